@@ -1,0 +1,180 @@
+/*
+ * talus_fem.h -- C ABI of the B200 deformable-body (tet FEM) step.
+ *
+ * This is the drop-in boundary for Talus's tet FEM step.  Each entry point
+ * names the reference interface it replaces (paths relative to the
+ * d-adel/talus project).  Plain pointers and sizes only; status codes, no
+ * exceptions.  The caller owns every host buffer; the library owns device
+ * memory behind opaque handles.  Implemented by talus_b200/libtalus_fem.so
+ * with hand-written sm_100a kernels; there is no CPU fallback: without a
+ * usable CUDA device every entry point that needs one returns
+ * TL_ERR_NO_DEVICE.
+ */
+#ifndef TALUS_FEM_H
+#define TALUS_FEM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TL_ABI_VERSION 1
+
+/* Status codes. */
+#define TL_OK 0
+#define TL_ERR_ARG 1            /* bad argument or size */
+#define TL_ERR_CUDA 2           /* a CUDA call failed */
+#define TL_ERR_NOT_CONVERGED 3  /* reported, not fatal: a PCG or Newton cap was hit */
+#define TL_ERR_NONFINITE 4      /* a NaN/Inf reached the state (StepReport::nonFinite, solver.h:278) */
+#define TL_ERR_TIMEOUT 5        /* a device-side wait ran out; the context stays usable */
+#define TL_ERR_UNSUPPORTED 6    /* feature outside this library's scope (e.g. floating bodies) */
+#define TL_ERR_NO_DEVICE 7      /* no CUDA device / extension unusable */
+
+/* Arithmetic of a resident system. */
+#define TL_FP64 0        /* plain FP64 GPU step */
+#define TL_FP32_MIXED 1  /* FP32 bulk; FP64 element kinematics, Dm^-1, J and reductions */
+
+/* Element law. */
+#define TL_LAW_COROTATED 0  /* reference tet law: corotated + J2 return map (material.cc:236-265, 978-1057) */
+#define TL_LAW_SNH 1        /* stable neo-Hookean (neohookean.cc:41-47, 183-192) at one point per tet */
+
+/* Host buffer element type for state transfer. */
+#define TL_DTYPE_F32 0
+#define TL_DTYPE_F64 1
+
+/* RigidSplit (solver.h:28-32). */
+#define TL_RIGID_SPLIT_OFF 0
+#define TL_RIGID_SPLIT_UNPROJECTED 1
+#define TL_RIGID_SPLIT_PROJECTED 2
+
+typedef struct tl_ctx tl_ctx;
+typedef struct tl_system tl_system;
+
+/* talus::PhysicalMaterial (src/talus/material.h:12-29): the fields the tet
+ * step reads (solver.cc:39-55: elasticOf, plasticOf). */
+typedef struct tl_material {
+  double density;
+  double youngs_modulus;
+  double poissons_ratio;
+  double stiffness_damping;  /* must be 0: stiffness damping is not implemented (TL_ERR_UNSUPPORTED) */
+  double yield_stress;       /* +inf: never yields (material.cc:747-749) */
+  double hardening_modulus;
+} tl_material;
+
+/* The tet fields of talus::PreparedMesh (src/talus/mesh.h:11-44) for one
+ * body, plus two extensions: a per-element Young's modulus override and a
+ * velocity for anchored nodes (zero reproduces the reference's fixed anchors,
+ * solver.cc:3784-3789, 5833-5838). */
+typedef struct tl_mesh_desc {
+  uint32_t nodes;
+  uint32_t tets;
+  const double* rest_positions;      /* [3*nodes] PreparedMesh::restPositions */
+  const double* node_mass;           /* [nodes]   PreparedMesh::nodeMass */
+  const uint8_t* anchored;           /* [nodes]   PreparedMesh::anchored */
+  const uint32_t* tet_nodes;         /* [4*tets]  PreparedTet::nodes */
+  const double* rest_inverse;        /* [9*tets]  PreparedTet::restInverse, row-major */
+  const double* volume;              /* [tets]    PreparedTet::volume */
+  const uint32_t* material;          /* [tets]    PreparedTet::material (lane) */
+  const tl_material* materials;      /* [lanes]   std::span<const PhysicalMaterial> */
+  uint32_t lanes;
+  const double* element_youngs;      /* [tets] or NULL */
+  const double* prescribed_velocity; /* [3*nodes] or NULL */
+} tl_mesh_desc;
+
+/* talus::deformable::Settings (src/talus/deformable/solver/solver.h:51-107):
+ * the fields the non-contact tet path reads. */
+typedef struct tl_settings {
+  uint32_t substeps;        /* 1   (solver.h:52) */
+  uint32_t cg_iterations;   /* 64  (solver.h:53) */
+  uint32_t plastic_passes;  /* 40  (solver.h:56) */
+  uint32_t rigid_split;     /* TL_RIGID_SPLIT_PROJECTED (solver.h:66) */
+  uint32_t law;             /* TL_LAW_* */
+  uint32_t reserved;
+  double tolerance;         /* 1e-3 (solver.h:64) */
+  double spectral_radius;   /* 0.5  (solver.h:65) */
+} tl_settings;
+
+/* talus::deformable::StepReport (solver.h:211-311): the counters of the
+ * non-contact tet path, per body, accumulated (+=) like the reference
+ * (solver.cc:3612-3615, 5881-5882). */
+typedef struct tl_step_report {
+  uint32_t nodes;
+  uint32_t elements;
+  uint32_t substeps;
+  uint32_t cg_iterations;
+  uint32_t cg_capped_solves;
+  uint32_t plastic_evaluations;
+  uint32_t plastic_solves;
+  uint32_t plastic_backtracks;
+  uint32_t plastic_capped;
+  uint32_t plastic_linear_reads;
+  uint32_t plastic_handoffs;
+  uint32_t plastic_fallbacks;
+  uint32_t plastic_fallback_rejections;
+  uint32_t operator_applications;
+  uint32_t yielding;
+  uint32_t plastic_growth;
+  uint32_t non_finite;
+  uint32_t kernel_launches;
+  double cg_worst_relative_residual;
+  double plastic_worst_residual;
+  double elastic_energy;
+  double kinetic_energy;
+  double min_volume_ratio;
+  double device_seconds;
+} tl_step_report;
+
+/* Library version (TL_ABI_VERSION); works without a device. */
+int32_t tl_abi_version(void);
+const char* tl_status_string(int32_t status);
+
+/* Device context: one CUDA device and one stream.  No reference
+ * counterpart: Talus is CPU-only. */
+int32_t tl_ctx_create(int32_t device, tl_ctx** out);
+int32_t tl_ctx_destroy(tl_ctx* ctx);
+const char* tl_ctx_last_error(const tl_ctx* ctx);
+
+/* Upload one or more bodies (a batch when count > 1) into one resident
+ * system.  Replaces buildMesh's output handling + refreshStiffness +
+ * buildIncidence (solver.cc:453-507, 1065-1101): the node->element CSR
+ * incidence is built here in the reference's element order. */
+int32_t tl_system_create(tl_ctx* ctx, const tl_mesh_desc* bodies, uint32_t count, int32_t precision,
+                         tl_system** out);
+int32_t tl_system_destroy(tl_system* system);
+int32_t tl_system_counts(const tl_system* system, uint32_t* bodies, uint64_t* nodes, uint64_t* tets);
+
+/* talus::DeformableState (mesh.h:56-62) transfer for one body.  position,
+ * velocity, acceleration: [3*nodes]; rotation: [9*tets] row-major
+ * CommittedTet::rotation or NULL; plastic: [10*tets] (PlasticPoint strain
+ * row-major, then equivalent) or NULL.  restState (solver.cc:2420-2453) is
+ * tl_state_set with rest positions and zero velocity/acceleration. */
+int32_t tl_state_set(tl_system* system, uint32_t body, int32_t dtype, const void* position, const void* velocity,
+                     const void* acceleration, const void* rotation, const void* plastic);
+int32_t tl_state_get(tl_system* system, uint32_t body, int32_t dtype, void* position, void* velocity,
+                     void* acceleration, void* rotation, void* plastic);
+
+/* talus::deformable::step (solver.h:451-462, solver.cc:3472-5901) for every
+ * body of the system, with no contacts, no rigid partners and no
+ * DeformableSolverState (block-Jacobi PCG).  reports: [bodies] or NULL,
+ * accumulated.  Returns TL_OK, or TL_ERR_NONFINITE when a body's state
+ * became non-finite (the step still completes, like the reference's
+ * nonFinite flag), or an error. */
+int32_t tl_step(tl_system* system, const tl_settings* settings, const double gravity[3], double dt,
+                tl_step_report* reports);
+
+/* Host-state convenience: upload the state, step, download it (the
+ * reference's calling convention, where DeformableState lives in host
+ * memory).  Same buffer layout as tl_state_set/get. */
+int32_t tl_step_host(tl_system* system, uint32_t body, int32_t dtype, void* position, void* velocity,
+                     void* acceleration, void* rotation, void* plastic, const tl_settings* settings,
+                     const double gravity[3], double dt, tl_step_report* report);
+
+/* Default settings (Settings{} in solver.h:51-107). */
+void tl_settings_default(tl_settings* settings);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TALUS_FEM_H */

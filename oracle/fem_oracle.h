@@ -1,0 +1,157 @@
+/*
+ * fem_oracle.h -- C API of the CPU oracle for the Talus tet FEM step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is a plain C++ restatement of
+ * talus::deformable::step (src/talus/deformable/solver/solver.cc:3472-5901,
+ * contact block excluded) and of the tet element laws it calls
+ * (src/talus/deformable/material/material.cc).  It exists so that tests,
+ * the smoke check and the timed CPU baseline have something to compare the
+ * CUDA path against.  Nothing in the product links or calls it.
+ *
+ * Parity status: the reference cannot be compiled here (GLM, Eigen and
+ * Catch2 are fetched at configure time, CMakeLists.txt:16-39), so this
+ * oracle is pinned by known-answer tests restated from the reference's own
+ * law tests (tests/neohookean_tests.cc:115-199, tests/dynamics_tests.cc:
+ * 119-336, tests/dynamics_strainstep_tests.cc:3090-3104) and by analytic
+ * cases of the generalized-alpha integrator; results at the GLM/Eigen
+ * boundary (glm::inverse, Eigen::JacobiSVD) are "parity unpinned".
+ *
+ * All arrays are caller-owned, row-major, double precision.  The
+ * `precision` argument selects the arithmetic the restatement runs in:
+ * OR_F32 reproduces the reference's own float arithmetic, OR_F64 is the
+ * FP64 oracle.
+ */
+#pragma once
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { OR_F32 = 0, OR_F64 = 1 };
+enum { OR_LAW_COROTATED = 0, OR_LAW_SNH = 1 };
+enum { OR_ROTATION_POLAR = 0, OR_ROTATION_INVERTIBLE = 1 };
+
+typedef struct or_material {
+  double density;
+  double youngs_modulus;
+  double poissons_ratio;
+  double stiffness_damping;
+  double yield_stress;
+  double hardening_modulus;
+} or_material;
+
+typedef struct or_mesh {
+  uint32_t nodes;
+  uint32_t tets;
+  const double* rest;          /* [3*nodes] */
+  const double* node_mass;     /* [nodes] */
+  const uint8_t* anchored;     /* [nodes] */
+  const uint32_t* tet_nodes;   /* [4*tets] */
+  const double* rest_inverse;  /* [9*tets], row-major Dm^-1 */
+  const double* volume;        /* [tets] */
+  const uint32_t* lane;        /* [tets] */
+  const double* element_youngs;/* [tets] or NULL: per-element E override */
+  const double* prescribed;    /* [3*nodes] or NULL: velocity of anchored nodes */
+} or_mesh;
+
+typedef struct or_settings {
+  uint32_t substeps;        /* Settings::substeps (solver.h:52) */
+  uint32_t cg_iterations;   /* Settings::cgIterations (solver.h:53) */
+  uint32_t plastic_passes;  /* Settings::plasticPasses (solver.h:56) */
+  uint32_t law;             /* OR_LAW_* */
+  double tolerance;         /* Settings::tolerance (solver.h:64) */
+  double spectral_radius;   /* Settings::spectralRadius (solver.h:65) */
+} or_settings;
+
+typedef struct or_state {
+  double* position;      /* [3*nodes] */
+  double* velocity;      /* [3*nodes] */
+  double* acceleration;  /* [3*nodes] */
+  double* rotation;      /* [9*tets] row-major CommittedTet::rotation */
+  double* plastic;       /* [10*tets]: strain row-major (9) + equivalent */
+} or_state;
+
+typedef struct or_report {
+  uint32_t substeps;
+  uint32_t cg_iterations;
+  uint32_t cg_capped_solves;
+  uint32_t plastic_evaluations;
+  uint32_t plastic_solves;
+  uint32_t plastic_backtracks;
+  uint32_t plastic_capped;
+  uint32_t plastic_linear_reads;
+  uint32_t plastic_handoffs;
+  uint32_t plastic_fallbacks;
+  uint32_t plastic_fallback_rejections;
+  uint32_t operator_applications;
+  uint32_t yielding;
+  uint32_t plastic_growth;
+  uint32_t non_finite;
+  uint32_t reserved;
+  double cg_worst_relative_residual;
+  double plastic_worst_residual;
+  double elastic_energy;
+  double kinetic_energy;
+  double seconds;
+} or_report;
+
+/* Synthetic Kuhn box grid: buildMesh (solver.cc:2185-2418) for a lattice whose
+ * every cell has fill 1.  Sizes: nodes = counted by or_grid_counts. */
+typedef struct or_grid {
+  uint32_t cells[3];
+  double voxel;            /* cube edge (m) */
+  double origin[3];
+  double jitter;           /* uniform +-jitter*voxel per coordinate */
+  uint64_t seed;
+  double density;
+  uint32_t anchor_axis;    /* 0,1,2; 3 = none */
+  uint32_t anchor_side;    /* 0 = low face, 1 = high face */
+} or_grid;
+
+int or_grid_counts(const or_grid* grid, uint32_t* nodes, uint32_t* tets);
+int or_grid_build(const or_grid* grid, double* rest, double* node_mass,
+                  uint8_t* anchored, uint32_t* tet_nodes, double* rest_inverse,
+                  double* volume, uint32_t* lane, uint32_t* grid_index);
+
+/* One talus::deformable::step (solver.cc:3472) with no contacts/partners. */
+int or_step(int precision, const or_mesh* mesh, or_state* state,
+            const or_material* materials, uint32_t lanes,
+            const or_settings* settings, const double gravity[3], double dt,
+            or_report* report);
+
+/* Element laws, one tet (material.cc).  deformed/rest: [12]; rest_inverse: [9];
+ * committed_plastic: [10]; outputs: force [12], rotation [9], plastic [10],
+ * tangent [144] (row-major 12x12 d(force)/d(x) sign convention of
+ * TetStiffness blocks, i.e. +K), scalars [4] = energy, plastic work,
+ * yielding, loading. */
+int or_tet_point_trial(int precision, const double* deformed, const double* rest,
+                       const double* rest_inverse, double volume,
+                       const or_material* material, const double* committed_plastic,
+                       double margin, int rotation_mode, int return_mapping,
+                       double* force, double* rotation, double* plastic,
+                       double* tangent, double* scalars);
+
+/* Corotated elastic trial (material.cc:236-265): force [12], rotation [9],
+ * energy [1]. */
+int or_tet_trial(int precision, const double* deformed, const double* rest,
+                 const double* rest_inverse, double volume,
+                 const or_material* material, int rotation_mode,
+                 double* force, double* rotation, double* energy);
+
+/* Stable neo-Hookean tet (P from neohookean.cc:183-184 at one point):
+ * force [12], energy [1], hessian_blocks [144] (Gauss-Newton blocks
+ * mu (g_a.g_b) I + (lambda+mu) b_a b_b^T, neohookean.cc:189-192). */
+int or_snh_tet(int precision, const double* deformed, const double* rest,
+               const double* rest_inverse, double volume,
+               const or_material* material, double* force, double* energy,
+               double* hessian_blocks);
+
+/* polarRotation (material.cc:168-197) and the Invertible rotation
+ * (material.cc:24-64). gradient/out: [9] row-major. */
+int or_rotation(int precision, const double* gradient, int rotation_mode,
+                double* out);
+
+#ifdef __cplusplus
+}
+#endif

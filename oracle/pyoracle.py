@@ -1,0 +1,286 @@
+"""ctypes binding of the CPU oracle (oracle/fem_oracle.cc).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / reference legs of bench.py as the checker.  The product package
+``talus_b200`` never imports it.
+
+The oracle restates talus::deformable::step (reference
+src/talus/deformable/solver/solver.cc:3472-5901, contact block excluded) and
+its tet laws (src/talus/deformable/material/material.cc).  Parity of the
+restatement is pinned by the known-answer tests in tests/test_oracle_laws.py.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libfem_oracle.so")
+
+F32, F64 = 0, 1
+LAW_COROTATED, LAW_SNH = 0, 1
+ROTATION_POLAR, ROTATION_INVERTIBLE = 0, 1
+
+
+class Material(C.Structure):
+    _fields_ = [
+        ("density", C.c_double),
+        ("youngs_modulus", C.c_double),
+        ("poissons_ratio", C.c_double),
+        ("stiffness_damping", C.c_double),
+        ("yield_stress", C.c_double),
+        ("hardening_modulus", C.c_double),
+    ]
+
+
+class _Mesh(C.Structure):
+    _fields_ = [
+        ("nodes", C.c_uint32),
+        ("tets", C.c_uint32),
+        ("rest", C.c_void_p),
+        ("node_mass", C.c_void_p),
+        ("anchored", C.c_void_p),
+        ("tet_nodes", C.c_void_p),
+        ("rest_inverse", C.c_void_p),
+        ("volume", C.c_void_p),
+        ("lane", C.c_void_p),
+        ("element_youngs", C.c_void_p),
+        ("prescribed", C.c_void_p),
+    ]
+
+
+class _Settings(C.Structure):
+    _fields_ = [
+        ("substeps", C.c_uint32),
+        ("cg_iterations", C.c_uint32),
+        ("plastic_passes", C.c_uint32),
+        ("law", C.c_uint32),
+        ("tolerance", C.c_double),
+        ("spectral_radius", C.c_double),
+    ]
+
+
+class _State(C.Structure):
+    _fields_ = [
+        ("position", C.c_void_p),
+        ("velocity", C.c_void_p),
+        ("acceleration", C.c_void_p),
+        ("rotation", C.c_void_p),
+        ("plastic", C.c_void_p),
+    ]
+
+
+class Report(C.Structure):
+    _fields_ = [
+        ("substeps", C.c_uint32),
+        ("cg_iterations", C.c_uint32),
+        ("cg_capped_solves", C.c_uint32),
+        ("plastic_evaluations", C.c_uint32),
+        ("plastic_solves", C.c_uint32),
+        ("plastic_backtracks", C.c_uint32),
+        ("plastic_capped", C.c_uint32),
+        ("plastic_linear_reads", C.c_uint32),
+        ("plastic_handoffs", C.c_uint32),
+        ("plastic_fallbacks", C.c_uint32),
+        ("plastic_fallback_rejections", C.c_uint32),
+        ("operator_applications", C.c_uint32),
+        ("yielding", C.c_uint32),
+        ("plastic_growth", C.c_uint32),
+        ("non_finite", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("cg_worst_relative_residual", C.c_double),
+        ("plastic_worst_residual", C.c_double),
+        ("elastic_energy", C.c_double),
+        ("kinetic_energy", C.c_double),
+        ("seconds", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class _Grid(C.Structure):
+    _fields_ = [
+        ("cells", C.c_uint32 * 3),
+        ("voxel", C.c_double),
+        ("origin", C.c_double * 3),
+        ("jitter", C.c_double),
+        ("seed", C.c_uint64),
+        ("density", C.c_double),
+        ("anchor_axis", C.c_uint32),
+        ("anchor_side", C.c_uint32),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"oracle library missing: {LIB_PATH} (run `make -C oracle`)")
+        _lib = C.CDLL(LIB_PATH)
+        _lib.or_grid_counts.argtypes = [C.POINTER(_Grid), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+        _lib.or_grid_build.argtypes = [C.POINTER(_Grid)] + [C.c_void_p] * 8
+        _lib.or_step.argtypes = [C.c_int, C.POINTER(_Mesh), C.POINTER(_State), C.POINTER(Material), C.c_uint32,
+                                 C.POINTER(_Settings), C.c_void_p, C.c_double, C.POINTER(Report)]
+        _lib.or_tet_point_trial.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                            C.POINTER(Material), C.c_void_p, C.c_double, C.c_int, C.c_int,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.or_tet_trial.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                      C.POINTER(Material), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.or_snh_tet.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                    C.POINTER(Material), C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.or_rotation.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def material(density=1000.0, youngs=1e6, poisson=0.3, damping=0.0, yield_stress=np.inf, hardening=0.0) -> Material:
+    return Material(density, youngs, poisson, damping, yield_stress, hardening)
+
+
+@dataclass
+class Mesh:
+    rest: np.ndarray            # [V,3] f64
+    node_mass: np.ndarray       # [V] f64
+    anchored: np.ndarray        # [V] u8
+    tet_nodes: np.ndarray       # [T,4] u32
+    rest_inverse: np.ndarray    # [T,3,3] f64 (row-major Dm^-1)
+    volume: np.ndarray          # [T] f64
+    lane: np.ndarray            # [T] u32
+    grid_index: np.ndarray | None = None   # [V] u32 lattice sample index
+    cells: tuple | None = None
+    element_youngs: np.ndarray | None = None
+    prescribed: np.ndarray | None = None   # [V,3] f64
+
+    @property
+    def nodes(self) -> int:
+        return int(self.rest.shape[0])
+
+    @property
+    def tets(self) -> int:
+        return int(self.tet_nodes.shape[0])
+
+    def lattice(self) -> np.ndarray:
+        """[V,3] integer lattice coordinates of each node."""
+        rx, ry = self.cells[0] + 1, self.cells[1] + 1
+        g = self.grid_index.astype(np.int64)
+        return np.stack([g % rx, (g // rx) % ry, g // (rx * ry)], axis=1)
+
+
+def build_grid(cells, voxel=0.1, origin=(0.0, 0.0, 0.0), jitter=0.0, seed=0, density=1000.0,
+               anchor_axis=1, anchor_side=0) -> Mesh:
+    g = _Grid((C.c_uint32 * 3)(*cells), voxel, (C.c_double * 3)(*origin), jitter, seed, density,
+              anchor_axis, anchor_side)
+    V, T = C.c_uint32(), C.c_uint32()
+    if lib().or_grid_counts(C.byref(g), C.byref(V), C.byref(T)) != 0:
+        raise ValueError("bad grid")
+    V, T = V.value, T.value
+    rest = np.zeros((V, 3)); mass = np.zeros(V); anchored = np.zeros(V, np.uint8)
+    tet = np.zeros((T, 4), np.uint32); rinv = np.zeros((T, 3, 3)); vol = np.zeros(T)
+    lane = np.zeros(T, np.uint32); gi = np.zeros(V, np.uint32)
+    rc = lib().or_grid_build(C.byref(g), _ptr(rest), _ptr(mass), _ptr(anchored), _ptr(tet), _ptr(rinv),
+                             _ptr(vol), _ptr(lane), _ptr(gi))
+    if rc != 0:
+        raise RuntimeError("or_grid_build failed")
+    return Mesh(rest, mass, anchored, tet, rinv, vol, lane, gi, tuple(cells))
+
+
+@dataclass
+class State:
+    position: np.ndarray
+    velocity: np.ndarray
+    acceleration: np.ndarray
+    rotation: np.ndarray   # [T,3,3]
+    plastic: np.ndarray    # [T,10]
+
+    @staticmethod
+    def rest(mesh: Mesh) -> "State":
+        """restState (solver.cc:2420-2453) at the identity pose; anchored nodes
+        start with their prescribed velocity."""
+        v = np.zeros((mesh.nodes, 3))
+        if mesh.prescribed is not None:
+            v[mesh.anchored != 0] = mesh.prescribed[mesh.anchored != 0]
+        return State(mesh.rest.copy(), v, np.zeros((mesh.nodes, 3)),
+                     np.tile(np.eye(3), (mesh.tets, 1, 1)), np.zeros((mesh.tets, 10)))
+
+    def copy(self) -> "State":
+        return State(self.position.copy(), self.velocity.copy(), self.acceleration.copy(), self.rotation.copy(),
+                     self.plastic.copy())
+
+
+@dataclass
+class Settings:
+    substeps: int = 1
+    cg_iterations: int = 64
+    plastic_passes: int = 40
+    law: int = LAW_COROTATED
+    tolerance: float = 1e-3
+    spectral_radius: float = 0.5
+
+
+def step(precision: int, mesh: Mesh, state: State, materials, settings: Settings, gravity=(0.0, -9.81, 0.0),
+         dt=1.0 / 60.0, report: Report | None = None) -> Report:
+    for a in (state.position, state.velocity, state.acceleration, state.rotation, state.plastic):
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+    m = _Mesh(mesh.nodes, mesh.tets, _ptr(mesh.rest), _ptr(mesh.node_mass), _ptr(mesh.anchored),
+              _ptr(mesh.tet_nodes), _ptr(mesh.rest_inverse), _ptr(mesh.volume), _ptr(mesh.lane),
+              _ptr(mesh.element_youngs), _ptr(mesh.prescribed))
+    s = _State(_ptr(state.position), _ptr(state.velocity), _ptr(state.acceleration), _ptr(state.rotation),
+               _ptr(state.plastic))
+    mats = (Material * len(materials))(*materials)
+    st = _Settings(settings.substeps, settings.cg_iterations, settings.plastic_passes, settings.law,
+                   settings.tolerance, settings.spectral_radius)
+    g = np.asarray(gravity, dtype=np.float64)
+    rep = report if report is not None else Report()
+    rc = lib().or_step(precision, C.byref(m), C.byref(s), mats, len(materials), C.byref(st), _ptr(g), dt,
+                       C.byref(rep))
+    if rc != 0:
+        raise RuntimeError(f"or_step failed: {rc}")
+    return rep
+
+
+def tet_point_trial(precision, deformed, rest, rest_inverse, volume, mat, committed=None, margin=0.0,
+                    rotation_mode=ROTATION_INVERTIBLE, return_mapping=True, tangent=True):
+    deformed = np.ascontiguousarray(deformed, np.float64); rest = np.ascontiguousarray(rest, np.float64)
+    rinv = np.ascontiguousarray(rest_inverse, np.float64)
+    committed = np.zeros(10) if committed is None else np.ascontiguousarray(committed, np.float64)
+    force = np.zeros((4, 3)); rot = np.zeros((3, 3)); plastic = np.zeros(10); scal = np.zeros(4)
+    tan = np.zeros((12, 12)) if tangent else None
+    lib().or_tet_point_trial(precision, _ptr(deformed), _ptr(rest), _ptr(rinv), volume, C.byref(mat),
+                             _ptr(committed), margin, rotation_mode, int(return_mapping), _ptr(force), _ptr(rot),
+                             _ptr(plastic), _ptr(tan), _ptr(scal))
+    return dict(force=force, rotation=rot, plastic=plastic, tangent=tan, energy=scal[0], plastic_work=scal[1],
+                yielding=int(scal[2]), loading=int(scal[3]))
+
+
+def tet_trial(precision, deformed, rest, rest_inverse, volume, mat, rotation_mode=ROTATION_INVERTIBLE):
+    deformed = np.ascontiguousarray(deformed, np.float64); rest = np.ascontiguousarray(rest, np.float64)
+    rinv = np.ascontiguousarray(rest_inverse, np.float64)
+    force = np.zeros((4, 3)); rot = np.zeros((3, 3)); energy = np.zeros(1)
+    lib().or_tet_trial(precision, _ptr(deformed), _ptr(rest), _ptr(rinv), volume, C.byref(mat), rotation_mode,
+                       _ptr(force), _ptr(rot), _ptr(energy))
+    return dict(force=force, rotation=rot, energy=energy[0])
+
+
+def snh_tet(precision, deformed, rest, rest_inverse, volume, mat):
+    deformed = np.ascontiguousarray(deformed, np.float64); rest = np.ascontiguousarray(rest, np.float64)
+    rinv = np.ascontiguousarray(rest_inverse, np.float64)
+    force = np.zeros((4, 3)); energy = np.zeros(1); hess = np.zeros((12, 12))
+    lib().or_snh_tet(precision, _ptr(deformed), _ptr(rest), _ptr(rinv), volume, C.byref(mat), _ptr(force),
+                     _ptr(energy), _ptr(hess))
+    return dict(force=force, energy=energy[0], hessian=hess)
+
+
+def rotation(precision, gradient, mode=ROTATION_INVERTIBLE):
+    g = np.ascontiguousarray(gradient, np.float64); out = np.zeros((3, 3))
+    lib().or_rotation(precision, _ptr(g), mode, _ptr(out))
+    return out

@@ -1,0 +1,1160 @@
+// tl_kernels.cuh -- sm_100a kernels of the tet FEM step.
+//
+// Layout in HBM (one resident "system" = one or more bodies, concatenated):
+//  * nodes: Vec4 records (x, y, z, w) so that one 16-byte (FP32) or 32-byte
+//    (FP64) load moves a node vector; the state is stored as DISPLACEMENT
+//    u = x - X from the rest position X, which keeps FP32 storage accurate
+//    for small motions of large bodies.  Each body's nodes are padded to a
+//    multiple of TILE; padding nodes are anchored with zero mass.
+//  * elements: structure-of-arrays planes (plane k of field f at
+//    f + k * Tp), so one warp reads 32 consecutive elements of a plane with
+//    one coalesced transaction; each body's elements are padded to TILE.
+//  * per-(element, corner) outputs (element force, diagonal block, matvec
+//    product) are Vec4 records at index 4 e + c, consumed by a
+//    node -> (element, corner) CSR gather in ascending element order: this
+//    reproduces the reference's serial scatter order per node
+//    (solver.cc:1354-1572, 904-1048) with no floating-point atomics.
+//
+// Reductions that feed decisions are deterministic: per-tile partial sums in
+// FP64 (warp shuffle, then a fixed shared-memory tree), summed over a body's
+// tiles in tile order.  Integer counts and flags use integer atomics.
+#pragma once
+
+#include "tl_math.cuh"
+
+namespace tl {
+
+constexpr int TILE = 256;  // nodes or elements per tile; one tile per 256-thread block pass
+
+template <class S> struct alignas(4 * sizeof(S)) Vec4 { S x, y, z, w; };
+
+template <class S> __device__ __forceinline__ Vec4<S> ld4(const Vec4<S>* p) { return *p; }
+template <class S> __device__ __forceinline__ Vec4<S> ld4cg(const Vec4<S>* p);
+template <> __device__ __forceinline__ Vec4<float> ld4cg<float>(const Vec4<float>* p) {
+  const float4 v = __ldcg(reinterpret_cast<const float4*>(p));
+  return {v.x, v.y, v.z, v.w};
+}
+template <> __device__ __forceinline__ Vec4<double> ld4cg<double>(const Vec4<double>* p) {
+  const double2 a = __ldcg(reinterpret_cast<const double2*>(p));
+  const double2 b = __ldcg(reinterpret_cast<const double2*>(p) + 1);
+  return {a.x, a.y, b.x, b.y};
+}
+// Read-only (non-coherent cache) loads of data no kernel writes during the launch.
+template <class S> __device__ __forceinline__ Vec4<S> ld4g(const Vec4<S>* p);
+template <> __device__ __forceinline__ Vec4<float> ld4g<float>(const Vec4<float>* p) {
+  const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+  return {v.x, v.y, v.z, v.w};
+}
+template <> __device__ __forceinline__ Vec4<double> ld4g<double>(const Vec4<double>* p) {
+  const double2 a = __ldg(reinterpret_cast<const double2*>(p));
+  const double2 b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+  return {a.x, a.y, b.x, b.y};
+}
+template <class S> __device__ __forceinline__ V3<S> xyz(Vec4<S> v) { return {v.x, v.y, v.z}; }
+template <class S> __device__ __forceinline__ Vec4<S> pack(V3<S> v, S w = S(0)) { return {v.x, v.y, v.z, w}; }
+template <class S, class T> __device__ __forceinline__ Vec4<S> packc(V3<T> v, T w = T(0)) {
+  return {S(v.x), S(v.y), S(v.z), S(w)};
+}
+
+struct BodyDev {
+  uint32_t node_begin, node_end;  // real nodes [begin, end) in global numbering
+  uint32_t node_tile_begin, node_tile_end;
+  uint32_t elem_begin, elem_end;  // real elements
+  uint32_t elem_tile_begin, elem_tile_end;
+};
+
+// Per-body generalized-alpha constants of the current step (solver.cc:531-566,
+// 3574-3583).  Computed on the host in the system's arithmetic.
+struct BodyStepDev {
+  uint32_t substeps;  // body takes part in pass p iff p < substeps
+  uint32_t limit;     // PCG iteration cap
+  double inner, carry, alpha_f, alpha_m, beta, gamma;
+  double inertia, hstep, scale;  // (1 - alpha_m), h_eff, h_eff^2
+  double gx, gy, gz;
+  double tolerance;
+  double check_inner, check_carry;  // predictor-inversion test at dt / configured
+};
+
+// Material lane (material.cc:71-78 with nu clamped to [0, 0.49]); lambda and mu
+// are youngs * unit.
+struct MatDev {
+  double lam_unit, mu_unit, youngs, yield, hardening;
+  uint32_t yields, pad;
+};
+
+// Per-body accumulators written by kernels (integer atomics) and by the
+// finalize kernel (FP64 sums over tiles).
+struct BodyAccDev {
+  uint32_t nonfinite, grew, inverts, pad;
+  unsigned long long min_j_key;  // order-preserving key of the smallest J seen
+  unsigned long long moved_key;  // max |increment| (non-negative double bits)
+  unsigned long long extent_key; // max |x_evaluated|
+  double energy, right_sq, kinetic;
+};
+
+struct CgBodyDev {
+  double squared, target, floor, length, stride, blend, start_res, rel_res;
+  uint32_t taken, done, pad0, pad1;
+};
+
+struct CgReportDev {
+  uint32_t iterations, capped, applications, solves;
+  double worst_rel;
+};
+
+struct GridSyncDev {
+  unsigned int arrive;
+  unsigned int generation;
+  int error;
+  int active;  // bodies still iterating in the current PCG solve
+};
+
+template <class S> struct Sys {
+  uint32_t bodies, Vp, Tp, node_tiles, elem_tiles;
+  const BodyDev* body;
+  const BodyStepDev* step;
+  const MatDev* mat;
+  const uint32_t* node_tile_body;
+  const uint32_t* elem_tile_body;
+  // nodes
+  const Vec4<S>* rest4;   // (X, Y, Z, mass)
+  const uint8_t* anch;
+  const Vec4<S>* pres;    // prescribed velocity of anchored nodes
+  Vec4<S>* u;             // displacement
+  Vec4<S>* v;
+  Vec4<S>* a;
+  Vec4<S>* carried;
+  Vec4<S>* shifted;
+  Vec4<S>* weighted;
+  Vec4<S>* total;
+  Vec4<S>* incr;
+  Vec4<S>* right;
+  Vec4<S>* pre0;          // block-Jacobi inverse (xx, yy, zz, xy)
+  Vec4<S>* pre1;          // (xz, yz, -, -)
+  Vec4<S>* r;
+  Vec4<S>* z;
+  Vec4<S>* p;
+  Vec4<S>* ap;
+  const uint32_t* start;  // [Vp + 1]
+  const uint32_t* entry;  // 4 e + c, ascending e per node
+  // elements
+  const uint4* tet;
+  const double* dm;       // 9 planes, FP64 Dm^-1 (row-major)
+  const S* dms;           // 9 planes, Dm^-1 in S (aliases dm in FP64)
+  const double* vold;     // volume (FP64)
+  const S* vols;          // volume in S
+  const uint32_t* lane;
+  const double* eyoung;   // per-element E override or null
+  S* op;                  // 9 planes: R (corotated) or F (SNH)
+  Vec4<S>* tan;           // 2 planes: (theta, thetaBar, nxx, nyy), (nzz, nxy, nxz, nyz)
+  S* snhc;                // SNH: (lambda + mu)(J - 1) - mu
+  Vec4<S>* plast;         // 2 planes: (exx, eyy, ezz, exy), (exz, eyz, equivalent, -)
+  Vec4<S>* fe;            // [4 Tp] (fx, fy, fz, Dxx)
+  Vec4<S>* de;            // [4 Tp] (Dyy, Dzz, Dxy, Dxz)
+  S* de2;                 // [4 Tp] Dyz
+  Vec4<S>* ye;            // [4 Tp] matvec products
+  // reductions
+  double* part;           // [node_tiles * 4] PCG partials
+  double* npart;          // [node_tiles * 2] right^2 (0), kinetic (1)
+  double* epart;          // [elem_tiles] elastic energy
+  uint32_t* loading;      // [bodies] per assemble: elements past the loading margin
+  uint32_t* yielding;     // [bodies] per assemble: elements on the yield surface
+  BodyAccDev* acc;
+  CgBodyDev* cg;
+  CgReportDev* cgrep;
+  unsigned int* counter;  // [bodies]
+  GridSyncDev* sync;
+};
+
+// ------------------------------------------------------------ helpers ----
+
+__device__ __forceinline__ unsigned long long minKey(double v) {
+  // order-preserving map double -> uint64 so that atomicMin finds the min
+  const unsigned long long b = __double_as_longlong(v);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+__host__ __device__ __forceinline__ double fromMinKey(unsigned long long k) {
+  const unsigned long long b = (k >> 63) ? (k & 0x7fffffffffffffffull) : ~k;
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double(b);
+#else
+  double d;
+  memcpy(&d, &b, 8);
+  return d;
+#endif
+}
+
+// Sum of N doubles over the 256-thread block in a fixed order; result valid
+// in thread 0.
+template <int N>
+__device__ __forceinline__ void blockSum(double (&v)[N]) {
+  __shared__ double red[N][8];
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < N; ++k) red[k][warp] = v[k];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      double s = 0.0;
+      for (int w = 0; w < (TILE >> 5); ++w) s += red[k][w];
+      v[k] = s;
+    }
+  }
+  __syncthreads();
+}
+
+template <class S>
+__device__ __forceinline__ V3<double> gradientsOf(const double* dm, uint32_t Tp, uint32_t e, V3<double> g[4]) {
+  double d[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) d[k] = __ldg(dm + size_t(k) * Tp + e);
+  g[1] = {d[0], d[1], d[2]};
+  g[2] = {d[3], d[4], d[5]};
+  g[3] = {d[6], d[7], d[8]};
+  g[0] = -(g[1] + g[2] + g[3]);  // material.cc:199-207
+  return g[0];
+}
+
+template <class S> __device__ __forceinline__ void gradientsS(const S* dms, uint32_t Tp, uint32_t e, V3<S> g[4]) {
+  S d[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) d[k] = __ldg(dms + size_t(k) * Tp + e);
+  g[1] = {d[0], d[1], d[2]};
+  g[2] = {d[3], d[4], d[5]};
+  g[3] = {d[6], d[7], d[8]};
+  g[0] = -(g[1] + g[2] + g[3]);
+}
+
+// Symmetric 3x3 stored as (xx, yy, zz, xy, xz, yz).
+template <class T> struct Sym { T xx, yy, zz, xy, xz, yz; };
+template <class T> __device__ __forceinline__ V3<T> symMul(const Sym<T>& s, V3<T> v) {
+  return {s.xx * v.x + s.xy * v.y + s.xz * v.z, s.xy * v.x + s.yy * v.y + s.yz * v.z,
+          s.xz * v.x + s.yz * v.y + s.zz * v.z};
+}
+template <class T> __device__ __forceinline__ T symTrace(const Sym<T>& s) { return s.xx + s.yy + s.zz; }
+template <class T> __device__ __forceinline__ T symContract(const Sym<T>& a, const Sym<T>& b) {
+  return a.xx * b.xx + a.yy * b.yy + a.zz * b.zz + T(2) * (a.xy * b.xy + a.xz * b.xz + a.yz * b.yz);
+}
+template <class T> __device__ __forceinline__ Sym<T> symOf(const M3<T>& m) {
+  return {m.m[0][0], m.m[1][1], m.m[2][2], T(0.5) * (m.m[0][1] + m.m[1][0]), T(0.5) * (m.m[0][2] + m.m[2][0]),
+          T(0.5) * (m.m[1][2] + m.m[2][1])};
+}
+
+// Tangent stress of the J2 law (material.cc:636-650) applied to a symmetric
+// strain: K tr(e) I + 2 mu theta dev(e) - 2 mu thetaBar (n : e) n.
+template <class T>
+__device__ __forceinline__ Sym<T> tangentStress(const Sym<T>& e, T bulk, T mu, T theta, T thetaBar, const Sym<T>& n) {
+  const T tr = symTrace(e);
+  const T third = tr / T(3);
+  const T a = T(2) * mu * theta;
+  const T ne = T(2) * mu * thetaBar * symContract(n, e);
+  Sym<T> s;
+  s.xx = bulk * tr + a * (e.xx - third) - ne * n.xx;
+  s.yy = bulk * tr + a * (e.yy - third) - ne * n.yy;
+  s.zz = bulk * tr + a * (e.zz - third) - ne * n.zz;
+  s.xy = a * e.xy - ne * n.xy;
+  s.xz = a * e.xz - ne * n.xz;
+  s.yz = a * e.yz - ne * n.yz;
+  return s;
+}
+
+template <class S> __device__ __forceinline__ bool bodyActive(const Sys<S>& s, uint32_t b, uint32_t pass) {
+  return pass < s.step[b].substeps;
+}
+
+__device__ __forceinline__ unsigned long long globalTimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Grid-wide barrier for a cooperative launch.  Every block arrives once per
+// barrier; the last arrival resets the counter and advances the generation.
+// Waiting is bounded: after TL_BARRIER_LIMIT_NS the waiting block records
+// an error in sync->error and returns false, and so does every block that
+// sees the error flag, so a stalled grid ends instead of hanging.
+#define TL_BARRIER_LIMIT_NS 2000000000ull
+__device__ __forceinline__ bool gridBarrier(GridSyncDev* sync) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int good = 1;
+    volatile unsigned int* gen = &sync->generation;
+    const unsigned int seen = *gen;
+    __threadfence();
+    const unsigned int prev = atomicAdd(&sync->arrive, 1u);
+    if (prev == gridDim.x - 1) {
+      atomicExch(&sync->arrive, 0u);
+      __threadfence();
+      atomicAdd(&sync->generation, 1u);
+    } else {
+      const unsigned long long t0 = globalTimer();
+      while (*gen == seen) {
+        if (*(volatile int*)&sync->error != 0) {
+          good = 0;
+          break;
+        }
+        __nanosleep(32);
+        if (globalTimer() - t0 > TL_BARRIER_LIMIT_NS) {
+          atomicExch(&sync->error, 5);  // TL_ERR_TIMEOUT
+          good = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+    ok = good && (*(volatile int*)&sync->error == 0);
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// Returns true in the block that processed the last tile of body b in this
+// phase (the tile's partials must already be written by thread 0).
+__device__ __forceinline__ bool lastTileOfBody(unsigned int* counter, uint32_t ntiles) {
+  __shared__ int last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int prev = atomicAdd(counter, 1u);
+    last = prev == ntiles - 1u;
+    if (last) {
+      atomicExch(counter, 0u);
+      __threadfence();
+    }
+  }
+  __syncthreads();
+  return last != 0;
+}
+
+// Fixed-order sum of field k of the partials of tiles [t0, t1).  Block-wide;
+// result valid in thread 0.
+template <int N>
+__device__ __forceinline__ void sumTiles(const double* part, uint32_t t0, uint32_t t1, double (&out)[N]) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) out[k] = 0.0;
+  for (uint32_t t = t0 + threadIdx.x; t < t1; t += TILE)
+#pragma unroll
+    for (int k = 0; k < N; ++k) out[k] += __ldcg(part + size_t(t) * 4 + k);
+  blockSum<N>(out);
+}
+
+// Block-wide integer sums (one atomic per block instead of one per thread).
+__device__ __forceinline__ uint32_t blockCount(bool flag) {
+  __shared__ uint32_t cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  const uint32_t w = __popc(__ballot_sync(0xffffffffu, flag));
+  if ((threadIdx.x & 31) == 0 && w) atomicAdd(&cnt, w);
+  __syncthreads();
+  const uint32_t r = cnt;
+  __syncthreads();
+  return r;
+}
+// Block-wide min / max of 64-bit keys; result valid in thread 0.
+__device__ __forceinline__ unsigned long long blockMinKey(unsigned long long k) {
+  __shared__ unsigned long long red[TILE / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long q = __shfl_down_sync(0xffffffffu, k, o);
+    k = q < k ? q : k;
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = k;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int w = 1; w < TILE / 32; ++w) k = red[w] < k ? red[w] : k;
+  __syncthreads();
+  return k;
+}
+__device__ __forceinline__ unsigned long long blockMaxKey(unsigned long long k) {
+  __shared__ unsigned long long red[TILE / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long q = __shfl_down_sync(0xffffffffu, k, o);
+    k = q > k ? q : k;
+  }
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = k;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int w = 1; w < TILE / 32; ++w) k = red[w] > k ? red[w] : k;
+  __syncthreads();
+  return k;
+}
+
+// ------------------------------------------------------------- kernels ----
+
+// Predictor (solver.cc:3691-3700): carried = a; shifted = u + h v + (1/2 - beta) h^2 a;
+// weighted = (1 - alpha_f) shifted + alpha_f u.
+template <class S>
+__global__ void __launch_bounds__(TILE) kPredict(Sys<S> s, uint32_t pass) {
+  const uint32_t tile = blockIdx.x, b = s.node_tile_body[tile];
+  if (!bodyActive(s, b, pass)) return;
+  const uint32_t n = tile * TILE + threadIdx.x;
+  if (n >= s.body[b].node_end) return;
+  const BodyStepDev& st = s.step[b];
+  const V3<double> u = cvt<double>(xyz(s.u[n])), v = cvt<double>(xyz(s.v[n])), a = cvt<double>(xyz(s.a[n]));
+  const V3<double> sh = u + st.inner * v + st.carry * a;
+  const V3<double> w = (1.0 - st.alpha_f) * sh + st.alpha_f * u;
+  s.carried[n] = s.a[n];
+  s.shifted[n] = packc<S>(sh);
+  s.weighted[n] = packc<S>(w);
+}
+
+// predictorInverts (solver.cc:568-623): does any tet of the body invert at the
+// predicted weighted position for h = dt / configured?
+template <class S>
+__global__ void __launch_bounds__(TILE) kInversionCheck(Sys<S> s) {
+  const uint32_t tile = blockIdx.x, b = s.elem_tile_body[tile];
+  const uint32_t e = tile * TILE + threadIdx.x;
+  if (e >= s.body[b].elem_end) return;
+  const BodyStepDev& st = s.step[b];
+  const uint4 t = __ldg(&s.tet[e]);
+  const uint32_t nodes[4] = {t.x, t.y, t.z, t.w};
+  V3<double> g[4];
+  gradientsOf<S>(s.dm, s.Tp, e, g);
+  M3<double> h = zero3<double>();
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const uint32_t n = nodes[c];
+    const V3<double> u = cvt<double>(xyz(s.u[n])), v = cvt<double>(xyz(s.v[n])), a = cvt<double>(xyz(s.a[n]));
+    const V3<double> sh = u + st.check_inner * v + st.check_carry * a;
+    addOuter(h, (1.0 - st.alpha_f) * sh + st.alpha_f * u, g[c]);
+  }
+  if (!(1.0 + volumeChange(h) > 0.0)) atomicOr(&s.acc[b].inverts, 1u);
+}
+
+enum ElementMode : uint32_t {
+  EM_KEEP = 1u,        // store the trial plastic point (assembleElastic's `keep`)
+  EM_CONSISTENT = 2u,  // scratch.stiffness is the consistent tangent (bindStiffness(true))
+  EM_MAPPING = 4u,     // returnMapping
+  EM_COMMIT = 8u,      // commitPlastic: plastic point only, no forces
+};
+
+// Element pass (assembleElastic, solver.cc:1354-1572; trial material.cc:236-265;
+// tetPointTrial material.cc:978-1057; SNH neohookean.cc:41-47, 183-192).
+// Kinematics and the law run in FP64 whatever S is; outputs are stored in S.
+// Positions are base + reach * dir (the reference's `evaluated`), in
+// displacement form.
+template <class S, int LAW>
+__global__ void __launch_bounds__(TILE)
+    kElement(Sys<S> s, const Vec4<S>* base, const Vec4<S>* dir, uint32_t pass, uint32_t mode, double margin) {
+  const uint32_t tile = blockIdx.x, b = s.elem_tile_body[tile];
+  if (!bodyActive(s, b, pass)) return;
+  const uint32_t e = tile * TILE + threadIdx.x;
+  const bool valid = e < s.body[b].elem_end;
+  double energy = 0.0;
+  bool isLoading = false, isYielding = false, grew = false, nonfinite = false;
+  unsigned long long jkey = ~0ull;
+  if (valid) {
+    const BodyStepDev& st = s.step[b];
+    const double reach = dir ? st.scale : 0.0;
+    const uint4 t = __ldg(&s.tet[e]);
+    const uint32_t nodes[4] = {t.x, t.y, t.z, t.w};
+    V3<double> g[4];
+    gradientsOf<S>(s.dm, s.Tp, e, g);
+    V3<double> X[4], U[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const uint32_t n = nodes[c];
+      X[c] = cvt<double>(xyz(ld4g(&s.rest4[n])));
+      V3<double> uu = cvt<double>(xyz(base[n]));
+      if (dir) uu = uu + reach * cvt<double>(xyz(dir[n]));
+      U[c] = uu;
+    }
+    M3<double> H = zero3<double>();
+#pragma unroll
+    for (int c = 0; c < 4; ++c) addOuter(H, U[c], g[c]);
+    const double vol = s.vold[e];
+    const MatDev m = s.mat[s.lane[e]];
+    const double youngs = s.eyoung ? s.eyoung[e] : m.youngs;
+    const double lam = youngs * m.lam_unit, mu = youngs * m.mu_unit;
+    const double change = volumeChange(H);
+    jkey = minKey(1.0 + change);
+    V3<double> force[4];
+    Sym<double> diag[4];
+    bool finite = true;
+    if (LAW == 0) {
+      M3<double> F = H;
+      F.m[0][0] += 1.0;
+      F.m[1][1] += 1.0;
+      F.m[2][2] += 1.0;
+      const M3<double> R = elementRotation(F, true);
+      // corotated offsets (material.cc:92-109), strain (material.cc:155-161)
+      V3<double> xc = {0, 0, 0}, uc = {0, 0, 0};
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        xc = xc + X[c];
+        uc = uc + U[c];
+      }
+      xc = 0.25 * xc;
+      uc = 0.25 * uc;
+      M3<double> D = zero3<double>();
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const V3<double> rel = X[c] - xc;
+        const V3<double> off = mulT(R, rel + (U[c] - uc)) - rel;
+        addOuter(D, off, g[c]);
+      }
+      const Sym<double> eps = symOf(D);
+      const bool yields = m.yields != 0u;
+      const double bulk = lam + 2.0 * mu / 3.0;
+      Sym<double> stress;
+      double theta = 1.0, thetaBar = 0.0;
+      Sym<double> normal = {0, 0, 0, 0, 0, 0};
+      if (yields) {
+        // returnMap (material.cc:594-634)
+        const Vec4<S> p0 = s.plast[e], p1 = s.plast[s.Tp + e];
+        const Sym<double> ep = {double(p0.x), double(p0.y), double(p0.z), double(p0.w), double(p1.x), double(p1.y)};
+        const double eq = double(p1.z);
+        const Sym<double> el = {eps.xx - ep.xx, eps.yy - ep.yy, eps.zz - ep.zz,
+                                eps.xy - ep.xy, eps.xz - ep.xz, eps.yz - ep.yz};
+        const double pressure = bulk * symTrace(el);
+        const double third = symTrace(el) / 3.0;
+        const Sym<double> tr = {2.0 * mu * (el.xx - third), 2.0 * mu * (el.yy - third), 2.0 * mu * (el.zz - third),
+                                2.0 * mu * el.xy, 2.0 * mu * el.xz, 2.0 * mu * el.yz};
+        const double norm = sqrt(symContract(tr, tr));
+        const double equivalent = sqrt(1.5) * norm;
+        const double radius = m.yield + fmax(m.hardening, 0.0) * eq;
+        const double hard = fmax(m.hardening, 0.0);
+        Sym<double> next = ep;
+        double nextEq = eq;
+        bool plastic = false;
+        double excess = 0.0;
+        if (!(mode & EM_MAPPING) || !(equivalent > radius) || !(norm > 0.0)) {
+          stress = {tr.xx + pressure, tr.yy + pressure, tr.zz + pressure, tr.xy, tr.xz, tr.yz};
+        } else {
+          const double gamma = (equivalent - radius) / (3.0 * mu + hard);
+          const double inv = 1.0 / norm;
+          const Sym<double> n = {tr.xx * inv, tr.yy * inv, tr.zz * inv, tr.xy * inv, tr.xz * inv, tr.yz * inv};
+          const double th = 1.0 - 3.0 * mu * gamma / equivalent;
+          stress = {th * tr.xx + pressure, th * tr.yy + pressure, th * tr.zz + pressure, th * tr.xy, th * tr.xz,
+                    th * tr.yz};
+          plastic = true;
+          excess = (equivalent - radius) / radius;
+          const double sg = sqrt(1.5) * gamma;
+          next = {ep.xx + sg * n.xx, ep.yy + sg * n.yy, ep.zz + sg * n.zz,
+                  ep.xy + sg * n.xy, ep.xz + sg * n.xz, ep.yz + sg * n.yz};
+          nextEq = eq + gamma;
+          const bool loading = excess > margin;
+          if (loading) {  // linearized = response (material.cc:1016-1017)
+            theta = th;
+            thetaBar = 3.0 * mu / (3.0 * mu + hard) - (1.0 - th);
+            normal = n;
+          }
+          isLoading = loading;
+          isYielding = true;
+        }
+        const Sym<double> rem = {eps.xx - next.xx, eps.yy - next.yy, eps.zz - next.zz,
+                                 eps.xy - next.xy, eps.xz - next.xz, eps.yz - next.yz};
+        energy = vol * 0.5 * symContract(stress, rem);
+        if ((mode & (EM_KEEP | EM_COMMIT)) != 0u) {
+          grew = nextEq > eq;
+          s.plast[e] = Vec4<S>{S(next.xx), S(next.yy), S(next.zz), S(next.xy)};
+          s.plast[s.Tp + e] = Vec4<S>{S(next.xz), S(next.yz), S(nextEq), S(0)};
+        }
+      } else {
+        const double tr = symTrace(eps);
+        stress = {lam * tr + 2.0 * mu * eps.xx, lam * tr + 2.0 * mu * eps.yy, lam * tr + 2.0 * mu * eps.zz,
+                  2.0 * mu * eps.xy, 2.0 * mu * eps.xz, 2.0 * mu * eps.yz};
+        energy = vol * 0.5 * symContract(stress, eps);
+      }
+      if (!(mode & EM_COMMIT)) {
+        const bool tangentDiag = (mode & EM_CONSISTENT) && yields;
+        const double th = tangentDiag ? theta : 1.0;
+        const double thb = tangentDiag ? thetaBar : 0.0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const V3<double> w = symMul(stress, g[c]);
+          force[c] = -(vol * mul(R, w));  // material.cc:1019-1027
+          // R K_cc R^T with K_cc = V[(K + mu theta/3) g g^T + mu theta |g|^2 I - 2 mu thetaBar (n g)(n g)^T]
+          const V3<double> rg = mul(R, g[c]);
+          const V3<double> rn = mul(R, symMul(normal, g[c]));
+          const double k1 = vol * (bulk + mu * th / 3.0), k2 = vol * mu * th * dot(g[c], g[c]);
+          const double k3 = -vol * 2.0 * mu * thb;
+          diag[c] = {k1 * rg.x * rg.x + k2 + k3 * rn.x * rn.x, k1 * rg.y * rg.y + k2 + k3 * rn.y * rn.y,
+                     k1 * rg.z * rg.z + k2 + k3 * rn.z * rn.z, k1 * rg.x * rg.y + k3 * rn.x * rn.y,
+                     k1 * rg.x * rg.z + k3 * rn.x * rn.z, k1 * rg.y * rg.z + k3 * rn.y * rn.z};
+        }
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) s.op[size_t(3 * i + j) * s.Tp + e] = S(R.m[i][j]);
+        if (mode & EM_CONSISTENT) {
+          s.tan[e] = Vec4<S>{S(th), S(thb), S(normal.xx), S(normal.yy)};
+          s.tan[s.Tp + e] = Vec4<S>{S(normal.zz), S(normal.xy), S(normal.xz), S(normal.yz)};
+        }
+      }
+    } else {
+      // SNH: P = mu (H + H^T - tr H I - cof H) + (lambda + mu)(J - 1) cof F
+      M3<double> F = H;
+      F.m[0][0] += 1.0;
+      F.m[1][1] += 1.0;
+      F.m[2][2] += 1.0;
+      const M3<double> C = cofactor(F), CH = cofactor(H);
+      const double shifted = lam + mu;
+      const double trH = trace3(H);
+      M3<double> P;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          P.m[i][j] = mu * (H.m[i][j] + H.m[j][i] - (i == j ? trH : 0.0) - CH.m[i][j]) + shifted * change * C.m[i][j];
+      const double squared = contract(H, H);
+      energy = vol * (0.5 * mu * squared - mu * (change - trH) + 0.5 * shifted * change * change);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        force[c] = -(vol * mul(P, g[c]));
+        const V3<double> bb = mul(C, g[c]);
+        const double k2 = vol * mu * dot(g[c], g[c]), k1 = vol * shifted;
+        diag[c] = {k1 * bb.x * bb.x + k2, k1 * bb.y * bb.y + k2, k1 * bb.z * bb.z + k2,
+                   k1 * bb.x * bb.y, k1 * bb.x * bb.z, k1 * bb.y * bb.z};
+      }
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) s.op[size_t(3 * i + j) * s.Tp + e] = S(F.m[i][j]);
+      s.snhc[e] = S(shifted * change - mu);
+    }
+    if (!(mode & EM_COMMIT)) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        finite = finite && isfinite(force[c].x) && isfinite(force[c].y) && isfinite(force[c].z);
+        s.fe[4 * e + c] = Vec4<S>{S(force[c].x), S(force[c].y), S(force[c].z), S(diag[c].xx)};
+        s.de[4 * e + c] = Vec4<S>{S(diag[c].yy), S(diag[c].zz), S(diag[c].xy), S(diag[c].xz)};
+        s.de2[4 * e + c] = S(diag[c].yz);
+      }
+      nonfinite = !finite;
+    }
+  }
+  const uint32_t nLoading = blockCount(isLoading), nYielding = blockCount(isYielding);
+  const uint32_t nGrew = blockCount(grew), nBad = blockCount(nonfinite);
+  const unsigned long long jmin = blockMinKey(jkey);
+  if (threadIdx.x == 0) {
+    if (mode & EM_COMMIT) {
+      if (nGrew) atomicOr(&s.acc[b].grew, 1u);
+    } else {
+      if (nLoading) atomicAdd(&s.loading[b], nLoading);
+      if (nYielding) atomicAdd(&s.yielding[b], nYielding);
+      if (nBad) atomicOr(&s.acc[b].nonfinite, 1u);
+      atomicMin(&s.acc[b].min_j_key, jmin);
+    }
+  }
+  if (mode & EM_COMMIT) return;
+  double v[1] = {energy};
+  blockSum<1>(v);
+  if (threadIdx.x == 0) s.epart[tile] = v[0];
+}
+
+// Node gather + balance (solver.cc:3746-3806) + guardPreconditioner
+// (solver.cc:1574-1593).  taken: the acceleration the right side subtracts
+// (null for the first read).
+template <class S>
+__global__ void __launch_bounds__(TILE) kNodeAssemble(Sys<S> s, const Vec4<S>* taken, uint32_t pass) {
+  const uint32_t tile = blockIdx.x, b = s.node_tile_body[tile];
+  if (!bodyActive(s, b, pass)) return;
+  const uint32_t n = tile * TILE + threadIdx.x;
+  double rr = 0.0;
+  if (n < s.body[b].node_end) {
+    const BodyStepDev& st = s.step[b];
+    const S scale = S(st.scale);
+    double f[3] = {0, 0, 0};
+    S d[6] = {0, 0, 0, 0, 0, 0};
+    const uint32_t k0 = s.start[n], k1 = s.start[n + 1];
+    for (uint32_t k = k0; k < k1; ++k) {
+      const uint32_t q = __ldg(&s.entry[k]);
+      const Vec4<S> a = s.fe[q], c = s.de[q];
+      const S c2 = s.de2[q];
+      f[0] += double(a.x);
+      f[1] += double(a.y);
+      f[2] += double(a.z);
+      d[0] += scale * a.w;
+      d[1] += scale * c.x;
+      d[2] += scale * c.y;
+      d[3] += scale * c.z;
+      d[4] += scale * c.w;
+      d[5] += scale * c2;
+    }
+    const Vec4<S> rest = ld4g(&s.rest4[n]);
+    if (s.anch[n]) {
+      s.v[n] = s.pres[n];
+      s.a[n] = Vec4<S>{0, 0, 0, 0};
+      s.right[n] = Vec4<S>{0, 0, 0, 0};
+      s.pre0[n] = Vec4<S>{1, 1, 1, 0};
+      s.pre1[n] = Vec4<S>{0, 0, 0, 0};
+    } else {
+      const double mass = double(rest.w);
+      const V3<double> car = cvt<double>(xyz(s.carried[n]));
+      V3<double> rhs = {f[0] + mass * st.gx - st.alpha_m * mass * car.x, f[1] + mass * st.gy - st.alpha_m * mass * car.y,
+                        f[2] + mass * st.gz - st.alpha_m * mass * car.z};
+      if (taken) rhs = rhs - (st.inertia * mass) * cvt<double>(xyz(taken[n]));
+      s.right[n] = packc<S>(rhs);
+      rr = dot(rhs, rhs);
+      const S im = S(st.inertia * mass);
+      const S xx = d[0] + im, yy = d[1] + im, zz = d[2] + im, xy = d[3], xz = d[4], yz = d[5];
+      // inverse of the symmetric block, identity unless det > 0
+      const S cxx = yy * zz - yz * yz, cxy = xz * yz - xy * zz, cxz = xy * yz - xz * yy;
+      const S det = xx * cxx + xy * cxy + xz * cxz;
+      if (det > S(0)) {
+        const S inv = S(1) / det;
+        s.pre0[n] = Vec4<S>{cxx * inv, (xx * zz - xz * xz) * inv, (xx * yy - xy * xy) * inv, cxy * inv};
+        s.pre1[n] = Vec4<S>{cxz * inv, (xy * xz - xx * yz) * inv, 0, 0};
+      } else {
+        s.pre0[n] = Vec4<S>{1, 1, 1, 0};
+        s.pre1[n] = Vec4<S>{0, 0, 0, 0};
+      }
+    }
+  }
+  const uint32_t nBad = blockCount(!isfinite(rr));
+  if (threadIdx.x == 0 && nBad) atomicOr(&s.acc[b].nonfinite, 1u);
+  double v[1] = {rr};
+  blockSum<1>(v);
+  if (threadIdx.x == 0) s.npart[size_t(tile) * 2] = v[0];
+}
+
+// Sum the per-tile partials of each body (one block per body) in tile order.
+// which: 0 = elastic energy (element tiles), 1 = right^2, 2 = kinetic (node tiles).
+__global__ void __launch_bounds__(TILE) kFinalize(const BodyDev* body, const double* epart, const double* npart,
+                                                  BodyAccDev* acc, uint32_t which) {
+  const uint32_t b = blockIdx.x;
+  const uint32_t t0 = which == 0 ? body[b].elem_tile_begin : body[b].node_tile_begin;
+  const uint32_t t1 = which == 0 ? body[b].elem_tile_end : body[b].node_tile_end;
+  double out[1] = {0.0};
+  for (uint32_t t = t0 + threadIdx.x; t < t1; t += TILE)
+    out[0] += which == 0 ? epart[t] : npart[size_t(t) * 2 + (which - 1)];
+  blockSum<1>(out);
+  if (threadIdx.x == 0) {
+    if (which == 0) acc[b].energy = out[0];
+    else if (which == 1) acc[b].right_sq = out[0];
+    else acc[b].kinetic = out[0];
+  }
+}
+
+// ---------------------------------------------------------------- PCG ----
+
+// +scale * R K R^T p_e for one tet (applyStiffness, material.cc:267-288, with
+// the consistent tangent of tetPointTrial when `tangent`), or the exact SNH
+// tangent dP for LAW 1.  Arithmetic in S.
+template <class S, int LAW>
+__device__ __forceinline__ void elementApply(const Sys<S>& s, uint32_t e, const V3<S> p[4], S scale, bool tangent,
+                                             V3<S> y[4]) {
+  V3<S> g[4];
+  gradientsS<S>(s.dms, s.Tp, e, g);
+  const MatDev m = s.mat[s.lane[e]];
+  const double youngs = s.eyoung ? s.eyoung[e] : m.youngs;
+  const S lam = S(youngs * m.lam_unit), mu = S(youngs * m.mu_unit);
+  const S w = scale * s.vols[e];
+  M3<S> O;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) O.m[i][j] = __ldg(s.op + size_t(3 * i + j) * s.Tp + e);
+  if (LAW == 0) {
+    M3<S> Hq = zero3<S>();
+#pragma unroll
+    for (int c = 0; c < 4; ++c) addOuter(Hq, mulT(O, p[c]), g[c]);
+    const Sym<S> eps = symOf(Hq);
+    Sym<S> sig;
+    if (tangent) {
+      const Vec4<S> t0 = ld4g(&s.tan[e]), t1 = ld4g(&s.tan[s.Tp + e]);
+      const Sym<S> n = {t0.z, t0.w, t1.x, t1.y, t1.z, t1.w};
+      sig = tangentStress(eps, lam + S(2) * mu / S(3), mu, t0.x, t0.y, n);
+    } else {
+      const S tr = symTrace(eps);
+      sig = {lam * tr + S(2) * mu * eps.xx, lam * tr + S(2) * mu * eps.yy, lam * tr + S(2) * mu * eps.zz,
+             S(2) * mu * eps.xy, S(2) * mu * eps.xz, S(2) * mu * eps.yz};
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) y[c] = w * mul(O, symMul(sig, g[c]));
+  } else {
+    // dP = mu dF + c dcof(F)[dF] + (lambda + mu)(cof F : dF) cof F
+    M3<S> dF = zero3<S>();
+#pragma unroll
+    for (int c = 0; c < 4; ++c) addOuter(dF, p[c], g[c]);
+    const M3<S> C = cofactor(O);
+    const S cc = __ldg(&s.snhc[e]);
+    const S k = (lam + mu) * contract(C, dF);
+    // columns of F and dF; column j of cof is F_{j+1} x F_{j+2}
+    V3<S> Fc[3], dc[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      Fc[j] = {O.m[0][j], O.m[1][j], O.m[2][j]};
+      dc[j] = {dF.m[0][j], dF.m[1][j], dF.m[2][j]};
+    }
+    M3<S> dP;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
+      const V3<S> dcof = cross(dc[j1], Fc[j2]) + cross(Fc[j1], dc[j2]);
+      dP.m[0][j] = mu * dF.m[0][j] + cc * dcof.x + k * C.m[0][j];
+      dP.m[1][j] = mu * dF.m[1][j] + cc * dcof.y + k * C.m[1][j];
+      dP.m[2][j] = mu * dF.m[2][j] + cc * dcof.z + k * C.m[2][j];
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) y[c] = w * mul(dP, g[c]);
+  }
+}
+
+// Reads a body's PCG scalars from L2 (they are written by other blocks).
+__device__ __forceinline__ CgBodyDev loadCg(const CgBodyDev* p) {
+  CgBodyDev c;
+  c.squared = __ldcg(&p->squared);
+  c.target = __ldcg(&p->target);
+  c.floor = __ldcg(&p->floor);
+  c.length = __ldcg(&p->length);
+  c.stride = __ldcg(&p->stride);
+  c.blend = __ldcg(&p->blend);
+  c.start_res = __ldcg(&p->start_res);
+  c.rel_res = __ldcg(&p->rel_res);
+  c.taken = __ldcg(&p->taken);
+  c.done = __ldcg(&p->done);
+  c.pad0 = c.pad1 = 0;
+  return c;
+}
+
+template <class S> __device__ __forceinline__ V3<S> fmaV(S a, V3<S> x, V3<S> y) {
+  return {fma(a, x.x, y.x), fma(a, x.y, y.y), fma(a, x.z, y.z)};
+}
+
+// Persistent PCG over every body of the system (conjugateGradient,
+// solver.cc:1904-2089, block-Jacobi branch).  One cooperative launch runs all
+// iterations; each body keeps its own scalars and stops on its own test, and
+// the launch ends when no body iterates.  Three grid barriers per iteration:
+//   A (element tiles) y_e = scale R K R^T p_e with p = z + blend p_prev formed on the fly
+//   B (node tiles)    p = z + blend p_prev; Ap = inertia m p + sum y_e; p.Ap
+//   C (node tiles)    x += stride p; r -= stride Ap; z = P r; r.z, r.r
+template <class S, int LAW>
+__global__ void __launch_bounds__(TILE, 2)
+    kPcg(Sys<S> s, Vec4<S>* X, uint32_t pass, uint32_t x0zero, uint32_t tangent) {
+  const uint32_t G = gridDim.x;
+  const S zero = S(0);
+  // ---- init: r = right - A x (anchored rows 0), z = P r, p_prev = 0
+  if (!x0zero) {
+    for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G) {
+      const uint32_t b = s.elem_tile_body[tile];
+      if (!bodyActive(s, b, pass)) continue;
+      const uint32_t e = tile * TILE + threadIdx.x;
+      if (e >= s.body[b].elem_end) continue;
+      const uint4 t = __ldg(&s.tet[e]);
+      const uint32_t nodes[4] = {t.x, t.y, t.z, t.w};
+      V3<S> pe[4], y[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) pe[c] = xyz(ld4cg(&X[nodes[c]]));
+      elementApply<S, LAW>(s, e, pe, S(s.step[b].scale), tangent != 0u, y);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) s.ye[4 * e + c] = pack(y[c]);
+    }
+    if (!gridBarrier(s.sync)) return;
+  }
+  for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
+    const uint32_t b = s.node_tile_body[tile];
+    if (!bodyActive(s, b, pass)) continue;
+    const uint32_t n = tile * TILE + threadIdx.x;
+    double sums[3] = {0.0, 0.0, 0.0};
+    if (n < s.body[b].node_end) {
+      const Vec4<S> rhs = s.right[n];
+      V3<S> r = {zero, zero, zero};
+      if (!s.anch[n]) {
+        V3<double> ax = {0, 0, 0};
+        if (!x0zero) {
+          const double im = s.step[b].inertia * double(ld4g(&s.rest4[n]).w);
+          ax = im * cvt<double>(xyz(ld4cg(&X[n])));
+          for (uint32_t k = s.start[n]; k < s.start[n + 1]; ++k) ax = ax + cvt<double>(xyz(ld4cg(&s.ye[__ldg(&s.entry[k])])));
+        }
+        r = cvt<S>(cvt<double>(xyz(rhs)) - ax);
+      }
+      const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
+      const Sym<S> P = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
+      const V3<S> z = symMul(P, r);
+      s.r[n] = pack(r);
+      s.z[n] = pack(z);
+      s.p[n] = Vec4<S>{zero, zero, zero, zero};
+      if (x0zero) X[n] = Vec4<S>{zero, zero, zero, zero};
+      sums[0] = dot(cvt<double>(r), cvt<double>(z));
+      sums[1] = dot(cvt<double>(r), cvt<double>(r));
+      sums[2] = dot(cvt<double>(xyz(rhs)), cvt<double>(xyz(rhs)));
+    }
+    blockSum<3>(sums);
+    if (threadIdx.x == 0) {
+      s.part[size_t(tile) * 4 + 0] = sums[0];
+      s.part[size_t(tile) * 4 + 1] = sums[1];
+      s.part[size_t(tile) * 4 + 2] = sums[2];
+    }
+    const BodyDev bd = s.body[b];
+    if (lastTileOfBody(&s.counter[b], bd.node_tile_end - bd.node_tile_begin)) {
+      double tot[3];
+      sumTiles<3>(s.part, bd.node_tile_begin, bd.node_tile_end, tot);
+      if (threadIdx.x == 0) {
+        CgBodyDev c;
+        const double reference = sqrt(tot[2]);
+        c.floor = fmax(reference, 1.1754943508222875e-38);  // std::numeric_limits<float>::min()
+        c.target = s.step[b].tolerance * c.floor;
+        c.squared = tot[0];
+        c.length = tot[1];
+        c.start_res = sqrt(tot[1]) / c.floor;
+        c.rel_res = c.start_res;
+        c.blend = 0.0;
+        c.stride = 0.0;
+        c.taken = 0;
+        c.done = (s.step[b].limit == 0u || sqrt(c.length) <= c.target) ? 1u : 0u;
+        c.pad0 = c.pad1 = 0;
+        s.cg[b] = c;
+        __threadfence();
+        if (c.done) atomicSub(&s.sync->active, 1);
+      }
+    }
+  }
+  if (!gridBarrier(s.sync)) return;
+  for (;;) {
+    if (*(volatile int*)&s.sync->active <= 0) break;  // uniform: no block decrements between here and barrier A
+    // ---- A
+    for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G) {
+      const uint32_t b = s.elem_tile_body[tile];
+      if (!bodyActive(s, b, pass) || __ldcg(&s.cg[b].done)) continue;
+      const uint32_t e = tile * TILE + threadIdx.x;
+      if (e >= s.body[b].elem_end) continue;
+      const S blend = S(__ldcg(&s.cg[b].blend));
+      const uint4 t = __ldg(&s.tet[e]);
+      const uint32_t nodes[4] = {t.x, t.y, t.z, t.w};
+      V3<S> pe[4], y[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        pe[c] = fmaV(blend, xyz(ld4cg(&s.p[nodes[c]])), xyz(ld4cg(&s.z[nodes[c]])));
+      elementApply<S, LAW>(s, e, pe, S(s.step[b].scale), tangent != 0u, y);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) s.ye[4 * e + c] = pack(y[c]);
+    }
+    if (!gridBarrier(s.sync)) return;
+    // ---- B
+    for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
+      const uint32_t b = s.node_tile_body[tile];
+      if (!bodyActive(s, b, pass) || __ldcg(&s.cg[b].done)) continue;
+      const uint32_t n = tile * TILE + threadIdx.x;
+      double sums[1] = {0.0};
+      if (n < s.body[b].node_end) {
+        const S blend = S(__ldcg(&s.cg[b].blend));
+        const V3<S> pn = fmaV(blend, xyz(ld4cg(&s.p[n])), xyz(ld4cg(&s.z[n])));
+        s.p[n] = pack(pn);
+        V3<S> apn = {zero, zero, zero};
+        if (!s.anch[n]) {
+          V3<double> acc = (s.step[b].inertia * double(ld4g(&s.rest4[n]).w)) * cvt<double>(pn);
+          for (uint32_t k = s.start[n]; k < s.start[n + 1]; ++k)
+            acc = acc + cvt<double>(xyz(ld4cg(&s.ye[__ldg(&s.entry[k])])));
+          apn = cvt<S>(acc);
+        }
+        s.ap[n] = pack(apn);
+        sums[0] = dot(cvt<double>(pn), cvt<double>(apn));
+      }
+      blockSum<1>(sums);
+      if (threadIdx.x == 0) s.part[size_t(tile) * 4 + 3] = sums[0];
+      const BodyDev bd = s.body[b];
+      if (lastTileOfBody(&s.counter[b], bd.node_tile_end - bd.node_tile_begin)) {
+        double tot[1];
+        double* base = s.part + 3;
+        sumTiles<1>(base, bd.node_tile_begin, bd.node_tile_end, tot);
+        if (threadIdx.x == 0) {
+          const double curvature = tot[0];
+          const double squared = __ldcg(&s.cg[b].squared);
+          if (!(curvature > 0.0) || !(squared > 0.0)) {
+            s.cg[b].done = 1u;
+            __threadfence();
+            atomicSub(&s.sync->active, 1);
+          } else {
+            s.cg[b].stride = squared / curvature;
+            __threadfence();
+          }
+        }
+      }
+    }
+    // No exit test here: phase C finalizers may already be decrementing the
+    // active count in other blocks.  The count is read only at the loop top,
+    // where every writer is ordered behind the previous barrier.
+    if (!gridBarrier(s.sync)) return;
+    // ---- C
+    for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
+      const uint32_t b = s.node_tile_body[tile];
+      if (!bodyActive(s, b, pass) || __ldcg(&s.cg[b].done)) continue;
+      const uint32_t n = tile * TILE + threadIdx.x;
+      double sums[2] = {0.0, 0.0};
+      if (n < s.body[b].node_end) {
+        const S stride = S(__ldcg(&s.cg[b].stride));
+        const V3<S> pn = xyz(ld4cg(&s.p[n]));
+        const V3<S> x = fmaV(stride, pn, xyz(ld4cg(&X[n])));
+        const V3<S> r = fmaV(-stride, xyz(ld4cg(&s.ap[n])), xyz(ld4cg(&s.r[n])));
+        const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
+        const Sym<S> P = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
+        const V3<S> z = symMul(P, r);
+        X[n] = pack(x);
+        s.r[n] = pack(r);
+        s.z[n] = pack(z);
+        sums[0] = dot(cvt<double>(r), cvt<double>(z));
+        sums[1] = dot(cvt<double>(r), cvt<double>(r));
+      }
+      blockSum<2>(sums);
+      if (threadIdx.x == 0) {
+        s.part[size_t(tile) * 4 + 0] = sums[0];
+        s.part[size_t(tile) * 4 + 1] = sums[1];
+      }
+      const BodyDev bd = s.body[b];
+      if (lastTileOfBody(&s.counter[b], bd.node_tile_end - bd.node_tile_begin)) {
+        double tot[2];
+        sumTiles<2>(s.part, bd.node_tile_begin, bd.node_tile_end, tot);
+        if (threadIdx.x == 0) {
+          CgBodyDev c = loadCg(&s.cg[b]);
+          c.blend = tot[0] / c.squared;
+          c.squared = tot[0];
+          c.length = tot[1];
+          c.taken += 1u;
+          c.done = (sqrt(c.length) <= c.target || c.taken >= s.step[b].limit) ? 1u : 0u;
+          s.cg[b] = c;
+          __threadfence();
+          if (c.done) atomicSub(&s.sync->active, 1);
+        }
+      }
+    }
+    if (!gridBarrier(s.sync)) return;
+  }
+  // ---- per-body results (block 0)
+  if (blockIdx.x == 0) {
+    for (uint32_t b = threadIdx.x; b < s.bodies; b += TILE) {
+      if (!bodyActive(s, b, pass)) continue;
+      CgBodyDev c = loadCg(&s.cg[b]);
+      const double residual = sqrt(c.length);
+      c.rel_res = residual / c.floor;
+      s.cg[b].rel_res = c.rel_res;
+      CgReportDev rep = s.cgrep[b];
+      rep.iterations += c.taken;
+      rep.capped += (c.taken == s.step[b].limit && residual > c.target) ? 1u : 0u;
+      rep.applications += c.taken + (x0zero ? 0u : 1u);
+      rep.solves += 1u;
+      rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
+      s.cgrep[b] = rep;
+    }
+  }
+}
+
+// Resets the PCG launch state: active body count, tile counters, barrier.
+template <class S>
+__global__ void kPcgPrepare(Sys<S> s, uint32_t pass) {
+  __shared__ int count;
+  if (threadIdx.x == 0) count = 0;
+  __syncthreads();
+  for (uint32_t b = threadIdx.x; b < s.bodies; b += blockDim.x) {
+    s.counter[b] = 0u;
+    if (bodyActive(s, b, pass)) atomicAdd(&count, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    s.sync->arrive = 0u;
+    s.sync->error = 0;
+    s.sync->active = count;
+  }
+}
+
+// a += incr on free nodes (solver.cc:3941-3945).
+template <class S>
+__global__ void __launch_bounds__(TILE) kAddIncrement(Sys<S> s, Vec4<S>* target, uint32_t pass) {
+  const uint32_t tile = blockIdx.x, b = s.node_tile_body[tile];
+  if (!bodyActive(s, b, pass)) return;
+  const uint32_t n = tile * TILE + threadIdx.x;
+  if (n >= s.body[b].node_end || s.anch[n]) return;
+  const Vec4<S> t = target[n], i = s.incr[n];
+  target[n] = Vec4<S>{t.x + i.x, t.y + i.y, t.z + i.z, t.w};
+}
+
+// Newton acceptance (solver.cc:4091-4107): total += increment on free nodes,
+// increment = 0 on anchored ones; max |increment| and max |x_evaluated|.
+template <class S>
+__global__ void __launch_bounds__(TILE) kNewtonAccept(Sys<S> s, uint32_t pass) {
+  const uint32_t tile = blockIdx.x, b = s.node_tile_body[tile];
+  if (!bodyActive(s, b, pass)) return;
+  const uint32_t n = tile * TILE + threadIdx.x;
+  unsigned long long moved = 0ull, extent = 0ull;
+  if (n < s.body[b].node_end) {
+    if (s.anch[n]) {
+      s.incr[n] = Vec4<S>{0, 0, 0, 0};
+    } else {
+      const BodyStepDev& st = s.step[b];
+      const V3<double> tot = cvt<double>(xyz(s.total[n]));
+      const V3<double> inc = cvt<double>(xyz(s.incr[n]));
+      const V3<double> ev = cvt<double>(xyz(s.rest4[n])) + cvt<double>(xyz(s.weighted[n])) + st.scale * tot;
+      s.total[n] = packc<S>(tot + inc);
+      moved = (unsigned long long)__double_as_longlong(sqrt(dot(inc, inc)));
+      extent = (unsigned long long)__double_as_longlong(sqrt(dot(ev, ev)));
+    }
+  }
+  moved = blockMaxKey(moved);
+  extent = blockMaxKey(extent);
+  if (threadIdx.x == 0) {
+    atomicMax(&s.acc[b].moved_key, moved);
+    atomicMax(&s.acc[b].extent_key, extent);
+  }
+}
+
+// Backtrack (solver.cc:4061-4070): increment *= 1/2; total -= increment.
+template <class S>
+__global__ void __launch_bounds__(TILE) kBacktrack(Sys<S> s, uint32_t pass) {
+  const uint32_t tile = blockIdx.x, b = s.node_tile_body[tile];
+  if (!bodyActive(s, b, pass)) return;
+  const uint32_t n = tile * TILE + threadIdx.x;
+  if (n >= s.body[b].node_end) return;
+  const Vec4<S> i = s.incr[n], t = s.total[n];
+  const Vec4<S> h = {i.x * S(0.5), i.y * S(0.5), i.z * S(0.5), S(0)};
+  s.incr[n] = h;
+  s.total[n] = Vec4<S>{t.x - h.x, t.y - h.y, t.z - h.z, t.w};
+}
+
+// Velocity and position update (solver.cc:4350-4369, 5829-5849).  Anchored
+// nodes move with their prescribed velocity (zero = the reference's fixed
+// anchors).
+template <class S>
+__global__ void __launch_bounds__(TILE) kUpdate(Sys<S> s, uint32_t pass) {
+  const uint32_t tile = blockIdx.x, b = s.node_tile_body[tile];
+  if (!bodyActive(s, b, pass)) return;
+  const uint32_t n = tile * TILE + threadIdx.x;
+  if (n >= s.body[b].node_end) return;
+  const BodyStepDev& st = s.step[b];
+  if (s.anch[n]) {
+    const Vec4<S> pv = s.pres[n];
+    s.v[n] = pv;
+    s.a[n] = Vec4<S>{0, 0, 0, 0};
+    const V3<double> u = cvt<double>(xyz(s.u[n])) + st.inner * cvt<double>(xyz(pv));
+    s.u[n] = packc<S>(u);
+    return;
+  }
+  const V3<double> a = cvt<double>(xyz(s.a[n]));
+  const V3<double> v = cvt<double>(xyz(s.v[n])) + st.inner * ((1.0 - st.gamma) * cvt<double>(xyz(s.carried[n])) + st.gamma * a);
+  const V3<double> u = cvt<double>(xyz(s.shifted[n])) + (st.beta * st.inner * st.inner) * a;
+  s.v[n] = packc<S>(v);
+  s.u[n] = packc<S>(u);
+}
+
+// Kinetic energy partials and the non-finite state check (solver.cc:5874-5879).
+template <class S>
+__global__ void __launch_bounds__(TILE) kStepEnd(Sys<S> s) {
+  const uint32_t tile = blockIdx.x, b = s.node_tile_body[tile];
+  const uint32_t n = tile * TILE + threadIdx.x;
+  double ke = 0.0;
+  bool bad = false;
+  if (n < s.body[b].node_end) {
+    const V3<double> v = cvt<double>(xyz(s.v[n]));
+    const V3<double> u = cvt<double>(xyz(s.u[n])), a = cvt<double>(xyz(s.a[n]));
+    ke = 0.5 * double(s.rest4[n].w) * dot(v, v);
+    const bool finite = isfinite(u.x) && isfinite(u.y) && isfinite(u.z) && isfinite(v.x) && isfinite(v.y) &&
+                        isfinite(v.z) && isfinite(a.x) && isfinite(a.y) && isfinite(a.z);
+    bad = !finite;
+  }
+  const uint32_t nBad = blockCount(bad);
+  if (threadIdx.x == 0 && nBad) atomicOr(&s.acc[b].nonfinite, 1u);
+  double sums[1] = {ke};
+  blockSum<1>(sums);
+  if (threadIdx.x == 0) s.npart[size_t(tile) * 2 + 1] = sums[0];
+}
+
+}  // namespace tl

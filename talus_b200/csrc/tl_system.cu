@@ -1,0 +1,1057 @@
+// tl_system.cu -- host side of the B200 tet FEM step: device memory of a
+// resident system, the step's control flow (generalized-alpha substeps, the
+// 3-read elastic path and the plastic Newton path of talus::deformable::step,
+// solver.cc:3472-4369, 5829-5900) over the kernels of tl_kernels.cuh, and the
+// C ABI of include/talus_fem.h.
+
+#include "../../include/talus_fem.h"
+#include "tl_kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+using namespace tl;
+
+namespace {
+
+struct CudaError {
+  cudaError_t code;
+  const char* what;
+};
+
+#define TL_CUDA(call)                                  \
+  do {                                                 \
+    const cudaError_t e_ = (call);                     \
+    if (e_ != cudaSuccess) throw CudaError{e_, #call}; \
+  } while (0)
+
+struct StatusError {
+  int32_t status;
+  std::string what;
+};
+
+template <class T>
+struct DevBuf {
+  T* ptr = nullptr;
+  size_t count = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() {
+    if (ptr) cudaFree(ptr);
+  }
+  void alloc(size_t n) {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    count = n;
+    if (n) TL_CUDA(cudaMalloc(&ptr, n * sizeof(T)));
+  }
+  void zero(cudaStream_t s) {
+    if (count) TL_CUDA(cudaMemsetAsync(ptr, 0, count * sizeof(T), s));
+  }
+  void upload(const T* host, size_t n, cudaStream_t s, size_t offset = 0) {
+    if (n) TL_CUDA(cudaMemcpyAsync(ptr + offset, host, n * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void download(T* host, size_t n, cudaStream_t s, size_t offset = 0) const {
+    if (n) TL_CUDA(cudaMemcpyAsync(host, ptr + offset, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+  }
+};
+
+template <class T>
+struct PinnedBuf {
+  T* ptr = nullptr;
+  size_t count = 0;
+  ~PinnedBuf() {
+    if (ptr) cudaFreeHost(ptr);
+  }
+  T* get(size_t n) {
+    if (n > count) {
+      if (ptr) cudaFreeHost(ptr);
+      ptr = nullptr;
+      TL_CUDA(cudaMallocHost(&ptr, n * sizeof(T)));
+      count = n;
+    }
+    return ptr;
+  }
+};
+
+uint32_t tilesOf(uint64_t n) { return uint32_t((n + TILE - 1) / TILE); }
+
+// Generalized-alpha rule (solver.cc:531-566) in double.
+struct Rule {
+  double alphaMass, alphaForce, beta, gamma;
+};
+Rule ruleOf(double spectral) {
+  const double held = std::clamp(spectral, 0.0, 1.0);
+  Rule r;
+  r.alphaMass = (2.0 * held - 1.0) / (held + 1.0);
+  r.alphaForce = held / (held + 1.0);
+  r.gamma = 0.5 - r.alphaMass + r.alphaForce;
+  r.beta = 0.25 * (1.0 - r.alphaMass + r.alphaForce) * (1.0 - r.alphaMass + r.alphaForce);
+  return r;
+}
+
+constexpr uint32_t ANCHORED_READS = 3u;       // solver.cc:11
+constexpr uint32_t INVERTED_SUBSTEPS = 4u;    // solver.cc:13
+constexpr double LOADING_MARGIN = 1.0e-3;     // solver.cc:372
+constexpr double PLASTIC_REDUCTION = 1.0e-2;  // solver.cc:374
+constexpr double PLASTIC_RESOLUTION = 8.0;    // solver.cc:380
+
+struct HostBody {
+  uint32_t nodes = 0, tets = 0;
+  bool anyAnchored = false, anyYields = false;
+  std::vector<double> rest;  // [3 V] for position <-> displacement
+};
+
+}  // namespace
+
+struct tl_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int sms = 0;
+  std::string last_error;
+};
+
+struct SystemBase {
+  virtual ~SystemBase() = default;
+  virtual void stateSet(uint32_t body, int32_t dtype, const void* x, const void* v, const void* a, const void* rot,
+                        const void* plastic) = 0;
+  virtual void stateGet(uint32_t body, int32_t dtype, void* x, void* v, void* a, void* rot, void* plastic) = 0;
+  virtual int32_t step(const tl_settings& set, const double g[3], double dt, tl_step_report* reports) = 0;
+  uint32_t bodies = 0;
+  uint64_t nodes = 0, tets = 0;
+};
+
+struct tl_system {
+  tl_ctx* ctx = nullptr;
+  std::unique_ptr<SystemBase> impl;
+};
+
+namespace {
+
+template <class S>
+struct System final : SystemBase {
+  tl_ctx* ctx;
+  cudaStream_t st;
+  uint32_t B = 0, Vp = 0, Tp = 0, nodeTiles = 0, elemTiles = 0;
+  std::vector<HostBody> hb;
+  std::vector<BodyDev> bodyHost;
+  uint32_t launches = 0;
+  // device buffers
+  DevBuf<BodyDev> dBody;
+  DevBuf<BodyStepDev> dStep;
+  DevBuf<MatDev> dMat;
+  DevBuf<uint32_t> dNodeTileBody, dElemTileBody;
+  DevBuf<Vec4<S>> rest4, pres, u, v, a, carried, shifted, weighted, total, incr, lowest, right, pre0, pre1, r, z, p, ap;
+  DevBuf<uint8_t> anch;
+  DevBuf<uint32_t> start, entry, lane;
+  DevBuf<uint4> tet;
+  DevBuf<double> dm, vold, eyoung;
+  DevBuf<S> dms, vols, op, snhc, de2;
+  DevBuf<Vec4<S>> tan, plast, fe, de, ye;
+  DevBuf<double> part, npart, epart;
+  DevBuf<uint32_t> loading, yielding, counter;
+  DevBuf<BodyAccDev> acc;
+  DevBuf<CgBodyDev> cg;
+  DevBuf<CgReportDev> cgrep;
+  DevBuf<GridSyncDev> sync;
+  bool hasEyoung = false;
+  int pcgGrid[2] = {0, 0};
+  PinnedBuf<BodyAccDev> hAcc;
+  PinnedBuf<uint32_t> hCount;
+  PinnedBuf<CgReportDev> hRep;
+  PinnedBuf<GridSyncDev> hSync;
+  PinnedBuf<BodyStepDev> hStep;
+  PinnedBuf<Vec4<S>> hNode;
+  PinnedBuf<S> hElem;
+  PinnedBuf<Vec4<S>> hElem4;
+
+  Sys<S> view() {
+    Sys<S> s;
+    s.bodies = B;
+    s.Vp = Vp;
+    s.Tp = Tp;
+    s.node_tiles = nodeTiles;
+    s.elem_tiles = elemTiles;
+    s.body = dBody.ptr;
+    s.step = dStep.ptr;
+    s.mat = dMat.ptr;
+    s.node_tile_body = dNodeTileBody.ptr;
+    s.elem_tile_body = dElemTileBody.ptr;
+    s.rest4 = rest4.ptr;
+    s.anch = anch.ptr;
+    s.pres = pres.ptr;
+    s.u = u.ptr;
+    s.v = v.ptr;
+    s.a = a.ptr;
+    s.carried = carried.ptr;
+    s.shifted = shifted.ptr;
+    s.weighted = weighted.ptr;
+    s.total = total.ptr;
+    s.incr = incr.ptr;
+    s.right = right.ptr;
+    s.pre0 = pre0.ptr;
+    s.pre1 = pre1.ptr;
+    s.r = r.ptr;
+    s.z = z.ptr;
+    s.p = p.ptr;
+    s.ap = ap.ptr;
+    s.start = start.ptr;
+    s.entry = entry.ptr;
+    s.tet = tet.ptr;
+    s.dm = dm.ptr;
+    s.vold = vold.ptr;
+    if constexpr (std::is_same_v<S, double>) {  // FP64: the S-typed copies are the FP64 arrays
+      s.dms = dm.ptr;
+      s.vols = vold.ptr;
+    } else {
+      s.dms = dms.ptr;
+      s.vols = vols.ptr;
+    }
+    s.lane = lane.ptr;
+    s.eyoung = hasEyoung ? eyoung.ptr : nullptr;
+    s.op = op.ptr;
+    s.tan = tan.ptr;
+    s.snhc = snhc.ptr;
+    s.plast = plast.ptr;
+    s.fe = fe.ptr;
+    s.de = de.ptr;
+    s.de2 = de2.ptr;
+    s.ye = ye.ptr;
+    s.part = part.ptr;
+    s.npart = npart.ptr;
+    s.epart = epart.ptr;
+    s.loading = loading.ptr;
+    s.yielding = yielding.ptr;
+    s.acc = acc.ptr;
+    s.cg = cg.ptr;
+    s.cgrep = cgrep.ptr;
+    s.counter = counter.ptr;
+    s.sync = sync.ptr;
+    return s;
+  }
+
+  System(tl_ctx* c, const tl_mesh_desc* descs, uint32_t count) : ctx(c), st(c->stream) {
+    B = count;
+    bodies = count;
+    hb.resize(B);
+    bodyHost.resize(B);
+    // ---- layout
+    uint64_t vp = 0, tp = 0, lanes = 0;
+    for (uint32_t b = 0; b < B; ++b) {
+      const tl_mesh_desc& d = descs[b];
+      if (d.nodes == 0 || d.tets == 0 || !d.rest_positions || !d.node_mass || !d.anchored || !d.tet_nodes ||
+          !d.rest_inverse || !d.volume || !d.material)
+        throw StatusError{TL_ERR_ARG, "mesh descriptor has an empty or missing field"};
+      BodyDev& bd = bodyHost[b];
+      bd.node_begin = uint32_t(vp);
+      bd.node_end = uint32_t(vp + d.nodes);
+      bd.node_tile_begin = uint32_t(vp / TILE);
+      vp += uint64_t(tilesOf(d.nodes)) * TILE;
+      bd.node_tile_end = uint32_t(vp / TILE);
+      bd.elem_begin = uint32_t(tp);
+      bd.elem_end = uint32_t(tp + d.tets);
+      bd.elem_tile_begin = uint32_t(tp / TILE);
+      tp += uint64_t(tilesOf(d.tets)) * TILE;
+      bd.elem_tile_end = uint32_t(tp / TILE);
+      lanes += d.lanes + 1;  // + the default lane (material.cc:9-16)
+      nodes += d.nodes;
+      tets += d.tets;
+      if (d.element_youngs) hasEyoung = true;
+    }
+    if (vp > 0xffffff00ull || tp * 4 > 0xffffff00ull) throw StatusError{TL_ERR_ARG, "system too large"};
+    Vp = uint32_t(vp);
+    Tp = uint32_t(tp);
+    nodeTiles = Vp / TILE;
+    elemTiles = Tp / TILE;
+    // ---- host staging
+    std::vector<Vec4<S>> hRest(Vp, Vec4<S>{0, 0, 0, 0}), hPres(Vp, Vec4<S>{0, 0, 0, 0});
+    std::vector<uint8_t> hAnch(Vp, 1u);
+    std::vector<uint32_t> hStart(size_t(Vp) + 1, 0u), hEntry(size_t(4) * tets);
+    std::vector<uint4> hTet(Tp);
+    std::vector<double> hDm(size_t(9) * Tp, 0.0), hVol(Tp, 0.0), hE(hasEyoung ? Tp : 0, 0.0);
+    std::vector<S> hDms(size_t(9) * Tp, S(0)), hVols(Tp, S(0));
+    std::vector<uint32_t> hLane(Tp, 0u), hNodeTileBody(nodeTiles), hElemTileBody(elemTiles);
+    std::vector<MatDev> hMat;
+    hMat.reserve(lanes);
+    for (uint32_t b = 0; b < B; ++b) {
+      const tl_mesh_desc& d = descs[b];
+      const BodyDev& bd = bodyHost[b];
+      HostBody& h = hb[b];
+      h.nodes = d.nodes;
+      h.tets = d.tets;
+      h.rest.assign(d.rest_positions, d.rest_positions + size_t(3) * d.nodes);
+      for (uint32_t t = bd.node_tile_begin; t < bd.node_tile_end; ++t) hNodeTileBody[t] = b;
+      for (uint32_t t = bd.elem_tile_begin; t < bd.elem_tile_end; ++t) hElemTileBody[t] = b;
+      const uint32_t laneBase = uint32_t(hMat.size());
+      for (uint32_t l = 0; l <= d.lanes; ++l) {
+        tl_material m = l < d.lanes ? d.materials[l]
+                                    : tl_material{1000.0, 0.0, 0.3, 0.0, std::numeric_limits<double>::infinity(), 0.0};
+        if (m.stiffness_damping > 0.0)
+          throw StatusError{TL_ERR_UNSUPPORTED, "stiffness damping is not implemented"};
+        const double nu = std::clamp(m.poissons_ratio, 0.0, 0.49);  // material.cc:71-78
+        MatDev md;
+        md.lam_unit = nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+        md.mu_unit = 1.0 / (2.0 * (1.0 + nu));
+        md.youngs = m.youngs_modulus;
+        md.yield = m.yield_stress;
+        md.hardening = m.hardening_modulus;
+        md.yields = (std::isfinite(m.yield_stress) && m.yield_stress > 0.0) ? 1u : 0u;  // material.cc:747-749
+        md.pad = 0;
+        hMat.push_back(md);
+      }
+      for (uint32_t n = 0; n < d.nodes; ++n) {
+        const uint32_t g = bd.node_begin + n;
+        hRest[g] = Vec4<S>{S(d.rest_positions[3 * n]), S(d.rest_positions[3 * n + 1]), S(d.rest_positions[3 * n + 2]),
+                           S(d.node_mass[n])};
+        hAnch[g] = d.anchored[n] ? 1u : 0u;
+        h.anyAnchored = h.anyAnchored || d.anchored[n] != 0;
+        if (d.prescribed_velocity && d.anchored[n])
+          hPres[g] = Vec4<S>{S(d.prescribed_velocity[3 * n]), S(d.prescribed_velocity[3 * n + 1]),
+                             S(d.prescribed_velocity[3 * n + 2]), S(0)};
+      }
+      for (uint32_t t = 0; t < d.tets; ++t) {
+        const uint32_t e = bd.elem_begin + t;
+        uint32_t q[4];
+        for (int k = 0; k < 4; ++k) {
+          q[k] = d.tet_nodes[4 * size_t(t) + k];
+          if (q[k] >= d.nodes) throw StatusError{TL_ERR_ARG, "tet node index out of range"};
+          q[k] += bd.node_begin;
+        }
+        hTet[e] = make_uint4(q[0], q[1], q[2], q[3]);
+        for (int k = 0; k < 9; ++k) {
+          hDm[size_t(k) * Tp + e] = d.rest_inverse[9 * size_t(t) + k];
+          hDms[size_t(k) * Tp + e] = S(d.rest_inverse[9 * size_t(t) + k]);
+        }
+        hVol[e] = d.volume[t];
+        hVols[e] = S(d.volume[t]);
+        const uint32_t l = d.material[t] < d.lanes ? d.material[t] : d.lanes;
+        hLane[e] = laneBase + l;
+        if (hMat[laneBase + l].yields) h.anyYields = true;
+        if (hasEyoung) hE[e] = d.element_youngs ? d.element_youngs[t] : hMat[laneBase + l].youngs;
+      }
+      for (uint32_t t = d.tets; t < bd.elem_tile_end * TILE - bd.elem_begin; ++t) {
+        const uint32_t e = bd.elem_begin + t;
+        hTet[e] = make_uint4(bd.node_begin, bd.node_begin, bd.node_begin, bd.node_begin);
+        hLane[e] = laneBase + d.lanes;
+      }
+    }
+    // ---- CSR node -> (element, corner), ascending element (solver.cc:1065-1101)
+    for (uint32_t e = 0; e < Tp; ++e) {
+      const uint32_t b = hElemTileBody[e / TILE];
+      if (e >= bodyHost[b].elem_end) continue;
+      const uint32_t q[4] = {hTet[e].x, hTet[e].y, hTet[e].z, hTet[e].w};
+      for (int k = 0; k < 4; ++k) ++hStart[q[k] + 1];
+    }
+    for (uint32_t n = 0; n < Vp; ++n) hStart[n + 1] += hStart[n];
+    {
+      std::vector<uint32_t> cursor(hStart.begin(), hStart.end() - 1);
+      for (uint32_t e = 0; e < Tp; ++e) {
+        const uint32_t b = hElemTileBody[e / TILE];
+        if (e >= bodyHost[b].elem_end) continue;
+        const uint32_t q[4] = {hTet[e].x, hTet[e].y, hTet[e].z, hTet[e].w};
+        for (int k = 0; k < 4; ++k) hEntry[cursor[q[k]]++] = 4 * e + uint32_t(k);
+      }
+    }
+    // ---- device
+    dBody.alloc(B);
+    dBody.upload(bodyHost.data(), B, st);
+    dStep.alloc(B);
+    dMat.alloc(hMat.size());
+    dMat.upload(hMat.data(), hMat.size(), st);
+    dNodeTileBody.alloc(nodeTiles);
+    dNodeTileBody.upload(hNodeTileBody.data(), nodeTiles, st);
+    dElemTileBody.alloc(elemTiles);
+    dElemTileBody.upload(hElemTileBody.data(), elemTiles, st);
+    rest4.alloc(Vp);
+    rest4.upload(hRest.data(), Vp, st);
+    pres.alloc(Vp);
+    pres.upload(hPres.data(), Vp, st);
+    anch.alloc(Vp);
+    anch.upload(hAnch.data(), Vp, st);
+    for (DevBuf<Vec4<S>>* buf : {&u, &v, &a, &carried, &shifted, &weighted, &total, &incr, &lowest, &right, &pre0,
+                                 &pre1, &r, &z, &p, &ap}) {
+      buf->alloc(Vp);
+      buf->zero(st);
+    }
+    start.alloc(hStart.size());
+    start.upload(hStart.data(), hStart.size(), st);
+    entry.alloc(hEntry.size());
+    entry.upload(hEntry.data(), hEntry.size(), st);
+    tet.alloc(Tp);
+    tet.upload(hTet.data(), Tp, st);
+    dm.alloc(hDm.size());
+    dm.upload(hDm.data(), hDm.size(), st);
+    if (sizeof(S) != sizeof(double)) {
+      dms.alloc(hDms.size());
+      dms.upload(hDms.data(), hDms.size(), st);
+      vols.alloc(Tp);
+      vols.upload(hVols.data(), Tp, st);
+    }
+    vold.alloc(Tp);
+    vold.upload(hVol.data(), Tp, st);
+    lane.alloc(Tp);
+    lane.upload(hLane.data(), Tp, st);
+    if (hasEyoung) {
+      eyoung.alloc(Tp);
+      eyoung.upload(hE.data(), Tp, st);
+    }
+    op.alloc(size_t(9) * Tp);
+    {
+      std::vector<S> ident(size_t(9) * Tp, S(0));
+      for (int k : {0, 4, 8}) std::fill(ident.begin() + size_t(k) * Tp, ident.begin() + size_t(k + 1) * Tp, S(1));
+      op.upload(ident.data(), ident.size(), st);
+      TL_CUDA(cudaStreamSynchronize(st));
+    }
+    tan.alloc(size_t(2) * Tp);
+    tan.zero(st);
+    snhc.alloc(Tp);
+    snhc.zero(st);
+    plast.alloc(size_t(2) * Tp);
+    plast.zero(st);
+    fe.alloc(size_t(4) * Tp);
+    de.alloc(size_t(4) * Tp);
+    de2.alloc(size_t(4) * Tp);
+    ye.alloc(size_t(4) * Tp);
+    part.alloc(size_t(4) * nodeTiles);
+    npart.alloc(size_t(2) * nodeTiles);
+    epart.alloc(elemTiles);
+    loading.alloc(B);
+    yielding.alloc(B);
+    counter.alloc(B);
+    counter.zero(st);
+    acc.alloc(B);
+    cg.alloc(B);
+    cg.zero(st);
+    cgrep.alloc(B);
+    sync.alloc(1);
+    sync.zero(st);
+    // cooperative grid sizes of the PCG kernel per law
+    int perSm = 0;
+    TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kPcg<S, 0>, TILE, 0));
+    pcgGrid[0] = std::max(1, std::min(perSm * ctx->sms, int(std::max(nodeTiles, elemTiles))));
+    if (perSm < 1) throw StatusError{TL_ERR_CUDA, "PCG kernel cannot be resident"};
+    TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kPcg<S, 1>, TILE, 0));
+    pcgGrid[1] = std::max(1, std::min(perSm * ctx->sms, int(std::max(nodeTiles, elemTiles))));
+    if (perSm < 1) throw StatusError{TL_ERR_CUDA, "PCG kernel cannot be resident"};
+    TL_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // ------------------------------------------------------------- state ----
+
+  template <class H>
+  void setNodes(const BodyDev& bd, const HostBody& h, DevBuf<Vec4<S>>& dst, const H* src, bool displacement) {
+    Vec4<S>* stage = hNode.get(h.nodes);
+    for (uint32_t n = 0; n < h.nodes; ++n) {
+      double x = double(src[3 * n]), y = double(src[3 * n + 1]), zz = double(src[3 * n + 2]);
+      if (displacement) {
+        x -= h.rest[3 * n];
+        y -= h.rest[3 * n + 1];
+        zz -= h.rest[3 * n + 2];
+      }
+      stage[n] = Vec4<S>{S(x), S(y), S(zz), S(0)};
+    }
+    dst.upload(stage, h.nodes, st, bd.node_begin);
+    TL_CUDA(cudaStreamSynchronize(st));
+  }
+  template <class H>
+  void getNodes(const BodyDev& bd, const HostBody& h, const DevBuf<Vec4<S>>& src, H* dst, bool displacement) {
+    Vec4<S>* stage = hNode.get(h.nodes);
+    src.download(stage, h.nodes, st, bd.node_begin);
+    TL_CUDA(cudaStreamSynchronize(st));
+    for (uint32_t n = 0; n < h.nodes; ++n) {
+      double x = double(stage[n].x), y = double(stage[n].y), zz = double(stage[n].z);
+      if (displacement) {
+        x += h.rest[3 * n];
+        y += h.rest[3 * n + 1];
+        zz += h.rest[3 * n + 2];
+      }
+      dst[3 * n] = H(x);
+      dst[3 * n + 1] = H(y);
+      dst[3 * n + 2] = H(zz);
+    }
+  }
+  template <class H>
+  void setElems(const BodyDev& bd, const HostBody& h, const H* rot, const H* plastic) {
+    const uint32_t T = h.tets;
+    if (rot) {
+      S* stage = hElem.get(size_t(9) * T);
+      for (int k = 0; k < 9; ++k)
+        for (uint32_t t = 0; t < T; ++t) stage[size_t(k) * T + t] = S(rot[9 * size_t(t) + k]);
+      for (int k = 0; k < 9; ++k) op.upload(stage + size_t(k) * T, T, st, size_t(k) * Tp + bd.elem_begin);
+    }
+    if (plastic) {
+      Vec4<S>* stage = hElem4.get(size_t(2) * T);
+      for (uint32_t t = 0; t < T; ++t) {
+        const H* q = plastic + 10 * size_t(t);
+        stage[t] = Vec4<S>{S(q[0]), S(q[4]), S(q[8]), S(0.5 * (double(q[1]) + double(q[3])))};
+        stage[T + t] = Vec4<S>{S(0.5 * (double(q[2]) + double(q[6]))), S(0.5 * (double(q[5]) + double(q[7]))), S(q[9]),
+                               S(0)};
+      }
+      plast.upload(stage, T, st, bd.elem_begin);
+      plast.upload(stage + T, T, st, size_t(Tp) + bd.elem_begin);
+    }
+    TL_CUDA(cudaStreamSynchronize(st));
+  }
+  template <class H>
+  void getElems(const BodyDev& bd, const HostBody& h, H* rot, H* plastic) {
+    const uint32_t T = h.tets;
+    if (rot) {
+      S* stage = hElem.get(size_t(9) * T);
+      for (int k = 0; k < 9; ++k) op.download(stage + size_t(k) * T, T, st, size_t(k) * Tp + bd.elem_begin);
+      TL_CUDA(cudaStreamSynchronize(st));
+      for (int k = 0; k < 9; ++k)
+        for (uint32_t t = 0; t < T; ++t) rot[9 * size_t(t) + k] = H(stage[size_t(k) * T + t]);
+    }
+    if (plastic) {
+      Vec4<S>* stage = hElem4.get(size_t(2) * T);
+      plast.download(stage, T, st, bd.elem_begin);
+      plast.download(stage + T, T, st, size_t(Tp) + bd.elem_begin);
+      TL_CUDA(cudaStreamSynchronize(st));
+      for (uint32_t t = 0; t < T; ++t) {
+        H* q = plastic + 10 * size_t(t);
+        const Vec4<S> a0 = stage[t], a1 = stage[T + t];
+        q[0] = H(a0.x); q[1] = H(a0.w); q[2] = H(a1.x);
+        q[3] = H(a0.w); q[4] = H(a0.y); q[5] = H(a1.y);
+        q[6] = H(a1.x); q[7] = H(a1.y); q[8] = H(a0.z);
+        q[9] = H(a1.z);
+      }
+    }
+  }
+
+  void stateSet(uint32_t b, int32_t dtype, const void* x, const void* vv, const void* aa, const void* rot,
+                const void* pl) override {
+    const BodyDev& bd = bodyHost[b];
+    const HostBody& h = hb[b];
+    if (dtype == TL_DTYPE_F64) {
+      if (x) setNodes(bd, h, u, static_cast<const double*>(x), true);
+      if (vv) setNodes(bd, h, v, static_cast<const double*>(vv), false);
+      if (aa) setNodes(bd, h, a, static_cast<const double*>(aa), false);
+      setElems(bd, h, static_cast<const double*>(rot), static_cast<const double*>(pl));
+    } else {
+      if (x) setNodes(bd, h, u, static_cast<const float*>(x), true);
+      if (vv) setNodes(bd, h, v, static_cast<const float*>(vv), false);
+      if (aa) setNodes(bd, h, a, static_cast<const float*>(aa), false);
+      setElems(bd, h, static_cast<const float*>(rot), static_cast<const float*>(pl));
+    }
+  }
+  void stateGet(uint32_t b, int32_t dtype, void* x, void* vv, void* aa, void* rot, void* pl) override {
+    const BodyDev& bd = bodyHost[b];
+    const HostBody& h = hb[b];
+    if (dtype == TL_DTYPE_F64) {
+      if (x) getNodes(bd, h, u, static_cast<double*>(x), true);
+      if (vv) getNodes(bd, h, v, static_cast<double*>(vv), false);
+      if (aa) getNodes(bd, h, a, static_cast<double*>(aa), false);
+      getElems(bd, h, static_cast<double*>(rot), static_cast<double*>(pl));
+    } else {
+      if (x) getNodes(bd, h, u, static_cast<float*>(x), true);
+      if (vv) getNodes(bd, h, v, static_cast<float*>(vv), false);
+      if (aa) getNodes(bd, h, a, static_cast<float*>(aa), false);
+      getElems(bd, h, static_cast<float*>(rot), static_cast<float*>(pl));
+    }
+  }
+
+  // ---------------------------------------------------------- launches ----
+
+  void check() {
+    TL_CUDA(cudaGetLastError());
+    ++launches;
+  }
+  void element(int law, const Vec4<S>* base, const Vec4<S>* dir, uint32_t pass, uint32_t mode, double margin) {
+    if (!(mode & EM_COMMIT)) {  // the counters describe the last assemble, not commitPlastic
+      loading.zero(st);
+      yielding.zero(st);
+    }
+    if (law == TL_LAW_SNH) kElement<S, 1><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass, mode, margin);
+    else kElement<S, 0><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass, mode, margin);
+    check();
+  }
+  void nodeAssemble(const Vec4<S>* taken, uint32_t pass) {
+    kNodeAssemble<S><<<nodeTiles, TILE, 0, st>>>(view(), taken, pass);
+    check();
+  }
+  void pcg(int law, Vec4<S>* X, uint32_t pass, bool x0zero, bool tangent) {
+    kPcgPrepare<S><<<1, TILE, 0, st>>>(view(), pass);
+    check();
+    Sys<S> s = view();
+    uint32_t ps = pass, xz = x0zero ? 1u : 0u, tg = tangent ? 1u : 0u;
+    void* args[] = {&s, &X, &ps, &xz, &tg};
+    const int idx = law == TL_LAW_SNH ? 1 : 0;
+    const void* fn = idx ? (const void*)kPcg<S, 1> : (const void*)kPcg<S, 0>;
+    TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(pcgGrid[idx]), dim3(TILE), args, 0, st));
+    ++launches;
+  }
+  void finalize(uint32_t which) {
+    kFinalize<<<B, TILE, 0, st>>>(dBody.ptr, epart.ptr, npart.ptr, acc.ptr, which);
+    check();
+  }
+  void nodeOp(void (*k)(Sys<S>, uint32_t), uint32_t pass) {
+    k<<<nodeTiles, TILE, 0, st>>>(view(), pass);
+    check();
+  }
+  void copy(DevBuf<Vec4<S>>& dst, const DevBuf<Vec4<S>>& src) {
+    TL_CUDA(cudaMemcpyAsync(dst.ptr, src.ptr, size_t(Vp) * sizeof(Vec4<S>), cudaMemcpyDeviceToDevice, st));
+  }
+  BodyAccDev readAcc(uint32_t b) {
+    BodyAccDev* h = hAcc.get(B);
+    acc.download(h, B, st);
+    TL_CUDA(cudaStreamSynchronize(st));
+    return h[b];
+  }
+  uint32_t readCount(DevBuf<uint32_t>& buf, uint32_t b) {
+    uint32_t* h = hCount.get(B);
+    buf.download(h, B, st);
+    TL_CUDA(cudaStreamSynchronize(st));
+    return h[b];
+  }
+
+  // -------------------------------------------------------------- step ----
+
+  int32_t step(const tl_settings& set, const double gvec[3], double dt, tl_step_report* reports) override {
+    if (set.law > 1u) throw StatusError{TL_ERR_ARG, "unknown law"};
+    const int law = int(set.law);
+    for (uint32_t b = 0; b < B; ++b)
+      if (!hb[b].anyAnchored && set.rigid_split != TL_RIGID_SPLIT_OFF)
+        throw StatusError{TL_ERR_UNSUPPORTED, "floating bodies (no anchored node, rigid split on) are not supported"};
+    launches = 0;
+    cudaEvent_t e0, e1;
+    TL_CUDA(cudaEventCreate(&e0));
+    TL_CUDA(cudaEventCreate(&e1));
+    TL_CUDA(cudaEventRecord(e0, st));
+    const uint32_t configured = std::max(set.substeps, 1u);
+    const Rule rule = ruleOf(set.spectral_radius);
+    const double checkInner = dt / double(configured);
+    // ---- per-body constants and the predictor-inversion test (solver.cc:3574-3583)
+    BodyStepDev* hs = hStep.get(B);
+    for (uint32_t b = 0; b < B; ++b) {
+      BodyStepDev& s = hs[b];
+      std::memset(&s, 0, sizeof(s));
+      s.substeps = configured;
+      s.limit = set.cg_iterations;
+      s.alpha_f = rule.alphaForce;
+      s.alpha_m = rule.alphaMass;
+      s.beta = rule.beta;
+      s.gamma = rule.gamma;
+      s.gx = gvec[0];
+      s.gy = gvec[1];
+      s.gz = gvec[2];
+      s.tolerance = set.tolerance;
+      s.check_inner = checkInner;
+      s.check_carry = (0.5 - rule.beta) * checkInner * checkInner;
+    }
+    dStep.upload(hs, B, st);
+    {
+      BodyAccDev* h = hAcc.get(B);
+      for (uint32_t b = 0; b < B; ++b) {
+        std::memset(&h[b], 0, sizeof(BodyAccDev));
+        h[b].min_j_key = ~0ull;
+      }
+      acc.upload(h, B, st);
+      cgrep.zero(st);
+    }
+    kInversionCheck<S><<<elemTiles, TILE, 0, st>>>(view());
+    check();
+    BodyAccDev* ha = hAcc.get(B);
+    acc.download(ha, B, st);
+    TL_CUDA(cudaStreamSynchronize(st));
+    uint32_t maxSub = 1;
+    bool anyNewton = false;
+    for (uint32_t b = 0; b < B; ++b) {
+      BodyStepDev& s = hs[b];
+      s.substeps = ha[b].inverts ? std::max(configured, INVERTED_SUBSTEPS) : configured;
+      s.inner = dt / double(s.substeps);
+      s.carry = (0.5 - rule.beta) * s.inner * s.inner;
+      s.inertia = 1.0 - rule.alphaMass;
+      s.hstep = std::sqrt((1.0 - rule.alphaForce) * rule.beta) * s.inner;
+      s.scale = s.hstep * s.hstep;
+      maxSub = std::max(maxSub, s.substeps);
+      const bool yieldsHere = hb[b].anyYields && law == TL_LAW_COROTATED;
+      anyNewton = anyNewton || (set.plastic_passes > 1u && yieldsHere);
+    }
+    if (anyNewton && B != 1u)
+      throw StatusError{TL_ERR_UNSUPPORTED, "the plastic Newton path runs one body per system"};
+    dStep.upload(hs, B, st);
+    const bool anyYields = std::any_of(hb.begin(), hb.end(), [](const HostBody& h) { return h.anyYields; }) &&
+                           law == TL_LAW_COROTATED;
+    std::vector<tl_step_report> local(B);
+    for (uint32_t pass = 0; pass < maxSub; ++pass) {
+      nodeOp(kPredict<S>, pass);
+      if (!anyNewton) {
+        elasticReads(law, pass);
+      } else {
+        newton(law, pass, set, rule, hs[0], local[0]);
+      }
+      nodeOp(kUpdate<S>, pass);
+      if (anyYields) element(law, u.ptr, nullptr, pass, EM_MAPPING | EM_COMMIT, 0.0);
+    }
+    kStepEnd<S><<<nodeTiles, TILE, 0, st>>>(view());
+    check();
+    finalize(0);
+    finalize(2);
+    TL_CUDA(cudaEventRecord(e1, st));
+    BodyAccDev* hacc = hAcc.get(B);
+    acc.download(hacc, B, st);
+    CgReportDev* hrep = hRep.get(B);
+    cgrep.download(hrep, B, st);
+    GridSyncDev* hsy = hSync.get(1);
+    sync.download(hsy, 1, st);
+    uint32_t* hy = hCount.get(B);
+    yielding.download(hy, B, st);
+    TL_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    TL_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int32_t status = TL_OK;
+    if (hsy->error != 0) throw StatusError{TL_ERR_TIMEOUT, "a PCG grid barrier ran out of time"};
+    for (uint32_t b = 0; b < B; ++b) {
+      if (!reports) continue;
+      tl_step_report& r = reports[b];
+      const tl_step_report& l = local[b];
+      r.nodes += hb[b].nodes;
+      r.elements += hb[b].tets;
+      r.substeps += hs[b].substeps;
+      r.cg_iterations += hrep[b].iterations;
+      r.cg_capped_solves += hrep[b].capped;
+      r.operator_applications += hrep[b].applications;
+      r.cg_worst_relative_residual = std::max(r.cg_worst_relative_residual, hrep[b].worst_rel);
+      r.plastic_evaluations += l.plastic_evaluations;
+      r.plastic_solves += l.plastic_solves;
+      r.plastic_backtracks += l.plastic_backtracks;
+      r.plastic_capped += l.plastic_capped;
+      r.plastic_linear_reads += l.plastic_linear_reads;
+      r.plastic_handoffs += l.plastic_handoffs;
+      r.plastic_fallbacks += l.plastic_fallbacks;
+      r.plastic_fallback_rejections += l.plastic_fallback_rejections;
+      r.plastic_worst_residual = std::max(r.plastic_worst_residual, l.plastic_worst_residual);
+      r.yielding = hy[b];
+      r.plastic_growth |= hacc[b].grew;
+      r.non_finite |= hacc[b].nonfinite;
+      r.elastic_energy += hacc[b].energy;
+      r.kinetic_energy += hacc[b].kinetic;
+      r.min_volume_ratio = fromMinKey(hacc[b].min_j_key);
+      r.device_seconds += double(ms) * 1e-3;
+      r.kernel_launches += launches;
+    }
+    for (uint32_t b = 0; b < B; ++b)
+      if (hacc[b].nonfinite) status = TL_ERR_NONFINITE;
+    return status;
+  }
+
+  // solver.cc:3914-3950: assemble at the predictor, solve for the
+  // acceleration, then two re-linearised increments.
+  void elasticReads(int law, uint32_t pass) {
+    element(law, weighted.ptr, nullptr, pass, EM_MAPPING, 0.0);
+    nodeAssemble(nullptr, pass);
+    pcg(law, a.ptr, pass, false, false);
+    for (uint32_t read = 1; read != ANCHORED_READS; ++read) {
+      element(law, weighted.ptr, a.ptr, pass, EM_MAPPING, 0.0);
+      nodeAssemble(a.ptr, pass);
+      pcg(law, incr.ptr, pass, true, false);
+      kAddIncrement<S><<<nodeTiles, TILE, 0, st>>>(view(), a.ptr, pass);
+      check();
+    }
+  }
+
+  // The plastic Newton loop of solver.cc:3951-4250 for one body (b = 0).
+  void newton(int law, uint32_t pass, const tl_settings& set, const Rule& rule, const BodyStepDev& bs,
+              tl_step_report& rep) {
+    const double travel = rule.beta * bs.inner * bs.inner;
+    const uint32_t plasticCap = set.plastic_passes;
+    bool consistent = false;  // bindStiffness(false) at step start (solver.cc:3521)
+    auto bind = [&](bool want) { consistent = want; };
+    auto assemble = [&](double margin, bool mapping = true) {
+      const uint32_t mode = (mapping ? uint32_t(EM_MAPPING) : 0u) | (consistent ? uint32_t(EM_CONSISTENT) : 0u);
+      element(law, weighted.ptr, total.ptr, pass, mode, margin);
+    };
+    auto balanceSquared = [&]() {
+      nodeAssemble(total.ptr, pass);
+      finalize(1);
+      const BodyAccDev h = readAcc(0);
+      return h.right_sq;
+    };
+    auto solve = [&](bool x0zero) { pcg(law, incr.ptr, pass, x0zero, consistent); };
+    auto addToTotal = [&]() {
+      kAddIncrement<S><<<nodeTiles, TILE, 0, st>>>(view(), total.ptr, pass);
+      check();
+    };
+    bool linearAllowed = true;
+    for (;;) {
+      total.zero(st);
+      double accepted = std::numeric_limits<double>::infinity();
+      double opening = 0.0;
+      double lowest = std::numeric_limits<double>::infinity();
+      uint32_t loadingBefore = 0, solves = 0;
+      bool converged = false, predictorUnloaded = false, handedOff = false;
+      for (uint32_t attempt = 0; attempt != plasticCap; ++attempt) {
+        if (attempt < 2u) bind(attempt != 0u);
+        assemble(LOADING_MARGIN);
+        ++rep.plastic_evaluations;
+        const double squared = balanceSquared();
+        const uint32_t loadingNow = readCount(loading, 0);
+        if (attempt != 0u) {
+          const double ranked = std::isfinite(squared) ? squared : std::numeric_limits<double>::infinity();
+          if (attempt == 1u || ranked < lowest) {
+            lowest = ranked;
+            copy(lowest_(), total);
+          }
+        }
+        if (attempt == 0u) predictorUnloaded = loadingNow == 0u;
+        if (attempt == 1u && linearAllowed && predictorUnloaded && std::isfinite(squared) && squared > accepted) {
+          ++rep.plastic_linear_reads;
+          bind(false);
+          for (uint32_t read = 1; read != ANCHORED_READS; ++read) {
+            assemble(LOADING_MARGIN);
+            ++rep.plastic_evaluations;
+            if (readCount(loading, 0) != 0u) {
+              handedOff = true;
+              break;
+            }
+            nodeAssemble(total.ptr, pass);
+            solve(true);
+            ++solves;
+            addToTotal();
+          }
+          converged = !handedOff;
+          break;
+        }
+        if (attempt != 0u && !(squared <= accepted)) {
+          nodeOp(kBacktrack<S>, pass);
+          ++rep.plastic_backtracks;
+          continue;
+        }
+        if (attempt != 0u && loadingBefore == 0u && loadingNow == 0u) {
+          converged = true;
+          break;
+        }
+        opening = attempt == 0u ? squared : opening;
+        accepted = squared;
+        loadingBefore = loadingNow;
+        if (attempt == 0u) copy(incr, a);
+        solve(attempt != 0u);
+        ++solves;
+        TL_CUDA(cudaMemsetAsync(&acc.ptr[0].moved_key, 0, 2 * sizeof(unsigned long long), st));
+        nodeOp(kNewtonAccept<S>, pass);
+        const BodyAccDev h = readAcc(0);
+        double moved, extent;
+        std::memcpy(&moved, &h.moved_key, 8);
+        std::memcpy(&extent, &h.extent_key, 8);
+        if (solves > 1u &&
+            travel * moved <= PLASTIC_RESOLUTION * double(std::numeric_limits<float>::epsilon()) * extent) {
+          converged = true;
+          break;
+        }
+      }
+      rep.plastic_solves += solves;
+      if (handedOff) {
+        ++rep.plastic_handoffs;
+        linearAllowed = false;
+        continue;
+      }
+      if (!converged) {
+        bind(false);
+        total.zero(st);
+        bool fellBack = true;
+        for (uint32_t read = 0; read != ANCHORED_READS; ++read) {
+          assemble(LOADING_MARGIN, read != 0u);
+          ++rep.plastic_evaluations;
+          if (readCount(loading, 0) != 0u) {
+            fellBack = false;
+            break;
+          }
+          nodeAssemble(total.ptr, pass);
+          if (read == 0u) copy(incr, a);
+          solve(read != 0u);
+          ++rep.plastic_solves;
+          addToTotal();
+        }
+        if (fellBack) {
+          assemble(LOADING_MARGIN);
+          ++rep.plastic_evaluations;
+          const double squared = balanceSquared();
+          fellBack = readCount(loading, 0) == 0u && squared <= PLASTIC_REDUCTION * PLASTIC_REDUCTION * opening;
+        }
+        if (fellBack) {
+          ++rep.plastic_fallbacks;
+          converged = true;
+        } else {
+          ++rep.plastic_fallback_rejections;
+          bind(true);
+          copy(total, lowest_());
+          assemble(LOADING_MARGIN);
+          ++rep.plastic_evaluations;
+          nodeAssemble(total.ptr, pass);
+          const double remaining = std::sqrt(lowest);
+          if (remaining >= rep.plastic_worst_residual) rep.plastic_worst_residual = remaining;
+        }
+      }
+      rep.plastic_capped += converged ? 0u : 1u;
+      copy(a, total);
+      break;
+    }
+  }
+  DevBuf<Vec4<S>>& lowest_() { return lowest; }
+};
+
+int32_t fail(tl_ctx* ctx, int32_t status, const std::string& what) {
+  if (ctx) ctx->last_error = what;
+  return status;
+}
+
+template <class F>
+int32_t guarded(tl_ctx* ctx, F&& body) {
+  try {
+    return body();
+  } catch (const StatusError& e) {
+    return fail(ctx, e.status, e.what);
+  } catch (const CudaError& e) {
+    return fail(ctx, TL_ERR_CUDA, std::string(e.what) + ": " + cudaGetErrorString(e.code));
+  } catch (const std::bad_alloc&) {
+    return fail(ctx, TL_ERR_ARG, "host allocation failed");
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t tl_abi_version(void) { return TL_ABI_VERSION; }
+
+const char* tl_status_string(int32_t status) {
+  switch (status) {
+    case TL_OK: return "ok";
+    case TL_ERR_ARG: return "invalid argument";
+    case TL_ERR_CUDA: return "CUDA error";
+    case TL_ERR_NOT_CONVERGED: return "not converged";
+    case TL_ERR_NONFINITE: return "non-finite state";
+    case TL_ERR_TIMEOUT: return "device wait timed out";
+    case TL_ERR_UNSUPPORTED: return "unsupported";
+    case TL_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown status";
+  }
+}
+
+void tl_settings_default(tl_settings* s) {
+  if (!s) return;
+  s->substeps = 1u;
+  s->cg_iterations = 64u;
+  s->plastic_passes = 40u;
+  s->rigid_split = TL_RIGID_SPLIT_PROJECTED;
+  s->law = TL_LAW_COROTATED;
+  s->reserved = 0u;
+  s->tolerance = 1.0e-3;
+  s->spectral_radius = 0.5;
+}
+
+int32_t tl_ctx_create(int32_t device, tl_ctx** out) {
+  if (!out) return TL_ERR_ARG;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= 0) return TL_ERR_NO_DEVICE;
+  if (device < 0 || device >= count) return TL_ERR_ARG;
+  auto ctx = std::make_unique<tl_ctx>();
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) return TL_ERR_NO_DEVICE;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return TL_ERR_NO_DEVICE;
+  if (prop.major < 10) return TL_ERR_NO_DEVICE;  // built for sm_100a only
+  int coop = 0;
+  cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+  if (!coop) return TL_ERR_NO_DEVICE;
+  ctx->sms = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return TL_ERR_CUDA;
+  *out = ctx.release();
+  return TL_OK;
+}
+
+int32_t tl_ctx_destroy(tl_ctx* ctx) {
+  if (!ctx) return TL_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return TL_OK;
+}
+
+const char* tl_ctx_last_error(const tl_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+int32_t tl_system_create(tl_ctx* ctx, const tl_mesh_desc* bodies, uint32_t count, int32_t precision,
+                         tl_system** out) {
+  if (!ctx || !bodies || !count || !out) return TL_ERR_ARG;
+  *out = nullptr;
+  return guarded(ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(ctx->device));
+    auto sys = std::make_unique<tl_system>();
+    sys->ctx = ctx;
+    if (precision == TL_FP64) sys->impl = std::make_unique<System<double>>(ctx, bodies, count);
+    else if (precision == TL_FP32_MIXED) sys->impl = std::make_unique<System<float>>(ctx, bodies, count);
+    else return fail(ctx, TL_ERR_ARG, "unknown precision");
+    *out = sys.release();
+    return TL_OK;
+  });
+}
+
+int32_t tl_system_destroy(tl_system* system) {
+  if (!system) return TL_ERR_ARG;
+  cudaSetDevice(system->ctx->device);
+  cudaStreamSynchronize(system->ctx->stream);
+  delete system;
+  return TL_OK;
+}
+
+int32_t tl_system_counts(const tl_system* system, uint32_t* bodies, uint64_t* nodes, uint64_t* tets) {
+  if (!system) return TL_ERR_ARG;
+  if (bodies) *bodies = system->impl->bodies;
+  if (nodes) *nodes = system->impl->nodes;
+  if (tets) *tets = system->impl->tets;
+  return TL_OK;
+}
+
+int32_t tl_state_set(tl_system* system, uint32_t body, int32_t dtype, const void* position, const void* velocity,
+                     const void* acceleration, const void* rotation, const void* plastic) {
+  if (!system || body >= system->impl->bodies || (dtype != TL_DTYPE_F32 && dtype != TL_DTYPE_F64)) return TL_ERR_ARG;
+  return guarded(system->ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(system->ctx->device));
+    system->impl->stateSet(body, dtype, position, velocity, acceleration, rotation, plastic);
+    return TL_OK;
+  });
+}
+
+int32_t tl_state_get(tl_system* system, uint32_t body, int32_t dtype, void* position, void* velocity,
+                     void* acceleration, void* rotation, void* plastic) {
+  if (!system || body >= system->impl->bodies || (dtype != TL_DTYPE_F32 && dtype != TL_DTYPE_F64)) return TL_ERR_ARG;
+  return guarded(system->ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(system->ctx->device));
+    system->impl->stateGet(body, dtype, position, velocity, acceleration, rotation, plastic);
+    return TL_OK;
+  });
+}
+
+int32_t tl_step(tl_system* system, const tl_settings* settings, const double gravity[3], double dt,
+                tl_step_report* reports) {
+  if (!system || !settings || !gravity || !(dt > 0.0)) return TL_ERR_ARG;
+  return guarded(system->ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(system->ctx->device));
+    return system->impl->step(*settings, gravity, dt, reports);
+  });
+}
+
+int32_t tl_step_host(tl_system* system, uint32_t body, int32_t dtype, void* position, void* velocity,
+                     void* acceleration, void* rotation, void* plastic, const tl_settings* settings,
+                     const double gravity[3], double dt, tl_step_report* report) {
+  if (!system || body >= system->impl->bodies || system->impl->bodies != 1u) return TL_ERR_ARG;
+  int32_t rc = tl_state_set(system, body, dtype, position, velocity, acceleration, rotation, plastic);
+  if (rc != TL_OK) return rc;
+  rc = tl_step(system, settings, gravity, dt, report);
+  if (rc != TL_OK && rc != TL_ERR_NONFINITE) return rc;
+  const int32_t got = tl_state_get(system, body, dtype, position, velocity, acceleration, rotation, plastic);
+  return got != TL_OK ? got : rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,260 @@
+"""Host mirror of talus::deformable's tet-step interface over the C ABI.
+
+Names and argument meaning follow the reference
+(src/talus/mesh.h, src/talus/material.h,
+src/talus/deformable/solver/solver.h):
+
+* ``PhysicalMaterial``  -- talus::PhysicalMaterial (material.h:12-29)
+* ``PreparedMesh``      -- the tet fields of talus::PreparedMesh (mesh.h:25-44)
+* ``DeformableState``   -- talus::DeformableState (mesh.h:56-62)
+* ``Settings``          -- the non-contact fields of deformable::Settings (solver.h:51-107)
+* ``StepReport``        -- the non-contact counters of deformable::StepReport (solver.h:211-311)
+* ``step``              -- deformable::step (solver.h:451-462) with no contacts,
+                           no rigid partners and no DeformableSolverState
+* ``rest_state``        -- deformable::restState (solver.h:331-334) at the identity pose
+
+Every call runs the CUDA kernels of libtalus_fem.so; nothing here computes
+physics.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _capi as capi
+from ._capi import check
+
+FP64 = capi.TL_FP64
+FP32_MIXED = capi.TL_FP32_MIXED
+COROTATED = capi.TL_LAW_COROTATED
+NEO_HOOKEAN = capi.TL_LAW_SNH
+
+
+@dataclass
+class PhysicalMaterial:
+    density: float = 1000.0
+    youngs_modulus: float = 0.0
+    poissons_ratio: float = 0.3
+    stiffness_damping: float = 0.0
+    yield_stress: float = math.inf
+    hardening_modulus: float = 0.0
+
+    def _c(self) -> capi.tl_material:
+        return capi.tl_material(self.density, self.youngs_modulus, self.poissons_ratio, self.stiffness_damping,
+                                self.yield_stress, self.hardening_modulus)
+
+
+@dataclass
+class PreparedMesh:
+    rest_positions: np.ndarray          # [V,3] float64
+    node_mass: np.ndarray               # [V]
+    anchored: np.ndarray                # [V] uint8
+    tet_nodes: np.ndarray               # [T,4] uint32
+    rest_inverse: np.ndarray            # [T,3,3] row-major Dm^-1
+    volume: np.ndarray                  # [T]
+    material: np.ndarray                # [T] uint32 lane
+    prescribed_velocity: np.ndarray | None = None   # [V,3] velocity of anchored nodes
+    element_youngs: np.ndarray | None = None        # [T] per-element E
+    lattice: np.ndarray | None = None               # [V,3] lattice coordinates (generator output)
+    cells: tuple | None = None
+
+    @property
+    def nodes(self) -> int:
+        return int(self.rest_positions.shape[0])
+
+    @property
+    def tets(self) -> int:
+        return int(self.tet_nodes.shape[0])
+
+    def face(self, axis: int, side: int) -> np.ndarray:
+        """Boolean mask of the nodes on one face of a generated box."""
+        value = 0 if side == 0 else self.cells[axis]
+        return self.lattice[:, axis] == value
+
+
+@dataclass
+class DeformableState:
+    position: np.ndarray      # [V,3]
+    velocity: np.ndarray      # [V,3]
+    acceleration: np.ndarray  # [V,3]
+    rotation: np.ndarray      # [T,3,3] CommittedTet::rotation
+    plastic: np.ndarray       # [T,10] PlasticPoint: strain (row-major 3x3), equivalent
+
+    def copy(self) -> "DeformableState":
+        return DeformableState(self.position.copy(), self.velocity.copy(), self.acceleration.copy(),
+                               self.rotation.copy(), self.plastic.copy())
+
+
+def rest_state(mesh: PreparedMesh) -> DeformableState:
+    """restState (solver.cc:2420-2453) at the identity pose.  Anchored nodes with
+    a prescribed velocity start moving with it."""
+    velocity = np.zeros((mesh.nodes, 3))
+    if mesh.prescribed_velocity is not None:
+        held = mesh.anchored != 0
+        velocity[held] = mesh.prescribed_velocity[held]
+    return DeformableState(mesh.rest_positions.astype(np.float64).copy(), velocity, np.zeros((mesh.nodes, 3)),
+                           np.tile(np.eye(3), (mesh.tets, 1, 1)), np.zeros((mesh.tets, 10)))
+
+
+@dataclass
+class Settings:
+    substeps: int = 1
+    cg_iterations: int = 64
+    plastic_passes: int = 40
+    tolerance: float = 1.0e-3
+    spectral_radius: float = 0.5
+    rigid_split: int = capi.TL_RIGID_SPLIT_PROJECTED
+    law: int = COROTATED
+
+    def _c(self) -> capi.tl_settings:
+        return capi.tl_settings(self.substeps, self.cg_iterations, self.plastic_passes, self.rigid_split, self.law, 0,
+                                self.tolerance, self.spectral_radius)
+
+
+class StepReport(capi.tl_step_report):
+    """Accumulated like the reference's StepReport (solver.cc:3612-3615)."""
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+class Context:
+    """One CUDA device + stream (tl_ctx)."""
+
+    def __init__(self, device: int = 0):
+        handle = C.c_void_p()
+        status = capi.lib().tl_ctx_create(device, C.byref(handle))
+        if status != capi.TL_OK:
+            raise capi.TalusError(status, "tl_ctx_create")
+        self.handle = handle
+
+    def close(self):
+        if self.handle:
+            capi.lib().tl_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_context: Context | None = None
+
+
+def default_context() -> Context:
+    global _default_context
+    if _default_context is None:
+        _default_context = Context(0)
+    return _default_context
+
+
+class _Body:
+    """Keeps a mesh's arrays alive in the layout the C ABI reads."""
+
+    def __init__(self, mesh: PreparedMesh, materials):
+        self.rest = np.ascontiguousarray(mesh.rest_positions, np.float64)
+        self.mass = np.ascontiguousarray(mesh.node_mass, np.float64)
+        self.anchored = np.ascontiguousarray(mesh.anchored, np.uint8)
+        self.tets = np.ascontiguousarray(mesh.tet_nodes, np.uint32)
+        self.rinv = np.ascontiguousarray(mesh.rest_inverse, np.float64)
+        self.volume = np.ascontiguousarray(mesh.volume, np.float64)
+        self.lane = np.ascontiguousarray(mesh.material, np.uint32)
+        self.youngs = None if mesh.element_youngs is None else np.ascontiguousarray(mesh.element_youngs, np.float64)
+        self.pres = None if mesh.prescribed_velocity is None else np.ascontiguousarray(mesh.prescribed_velocity,
+                                                                                       np.float64)
+        self.mats = (capi.tl_material * max(1, len(materials)))(*[m._c() for m in materials])
+        self.lanes = len(materials)
+        self.desc = capi.tl_mesh_desc(mesh.nodes, mesh.tets, _ptr(self.rest), _ptr(self.mass), _ptr(self.anchored),
+                                      _ptr(self.tets), _ptr(self.rinv), _ptr(self.volume), _ptr(self.lane),
+                                      self.mats, self.lanes, _ptr(self.youngs), _ptr(self.pres))
+
+
+class System:
+    """Bodies resident in device memory (tl_system).  ``count > 1`` bodies are
+    stepped together (the batched form)."""
+
+    def __init__(self, meshes, materials, precision: int = FP64, context: Context | None = None):
+        if isinstance(meshes, PreparedMesh):
+            meshes = [meshes]
+        if materials and isinstance(materials[0], PhysicalMaterial):
+            materials = [materials] * len(meshes)
+        self.context = context or default_context()
+        self.precision = precision
+        self.meshes = list(meshes)
+        self._bodies = [_Body(m, mats) for m, mats in zip(self.meshes, materials)]
+        descs = (capi.tl_mesh_desc * len(self._bodies))(*[b.desc for b in self._bodies])
+        handle = C.c_void_p()
+        check(capi.lib().tl_system_create(self.context.handle, descs, len(self._bodies), precision,
+                                          C.byref(handle)), self.context.handle)
+        self.handle = handle
+
+    def close(self):
+        if getattr(self, "handle", None):
+            capi.lib().tl_system_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, state: DeformableState, body: int = 0):
+        arrs = [np.ascontiguousarray(a, np.float64) for a in
+                (state.position, state.velocity, state.acceleration, state.rotation, state.plastic)]
+        check(capi.lib().tl_state_set(self.handle, body, capi.TL_DTYPE_F64, *[_ptr(a) for a in arrs]),
+              self.context.handle)
+
+    def get_state(self, body: int = 0) -> DeformableState:
+        m = self.meshes[body]
+        out = DeformableState(np.zeros((m.nodes, 3)), np.zeros((m.nodes, 3)), np.zeros((m.nodes, 3)),
+                              np.zeros((m.tets, 3, 3)), np.zeros((m.tets, 10)))
+        check(capi.lib().tl_state_get(self.handle, body, capi.TL_DTYPE_F64, _ptr(out.position), _ptr(out.velocity),
+                                      _ptr(out.acceleration), _ptr(out.rotation), _ptr(out.plastic)),
+              self.context.handle)
+        return out
+
+    def step(self, settings: Settings, gravity=(0.0, -9.81, 0.0), delta_time: float = 1.0 / 60.0, reports=None):
+        """One deformable::step of every body; returns the per-body reports
+        (accumulated into ``reports`` when given).  A non-finite state is
+        reported (report.non_finite), not raised, like the reference."""
+        if reports is None:
+            reports = (StepReport * len(self._bodies))()
+        g = np.asarray(gravity, np.float64)
+        status = capi.lib().tl_step(self.handle, C.byref(settings._c()), _ptr(g), float(delta_time), reports)
+        if status not in (capi.TL_OK, capi.TL_ERR_NONFINITE):
+            check(status, self.context.handle)
+        return reports
+
+
+_cache: dict = {}
+
+
+def step(mesh: PreparedMesh, state: DeformableState, materials, settings: Settings, gravity, delta_time: float,
+         report: StepReport | None = None, precision: int = FP64) -> StepReport:
+    """talus::deformable::step(mesh, state, materials, settings, gravity, deltaTime,
+    {}, {}, nullptr, report): advances ``state`` in place on the GPU."""
+    key = (id(mesh), precision, tuple((m.density, m.youngs_modulus, m.poissons_ratio, m.stiffness_damping,
+                                       m.yield_stress, m.hardening_modulus) for m in materials))
+    system = _cache.get(key)
+    if system is None:
+        system = System(mesh, list(materials), precision)
+        _cache[key] = system
+    system.set_state(state)
+    report = report if report is not None else StepReport()
+    reports = (StepReport * 1)(report)
+    system.step(settings, gravity, delta_time, reports)
+    C.memmove(C.addressof(report), C.addressof(reports[0]), C.sizeof(StepReport))
+    got = system.get_state()
+    state.position[...] = got.position
+    state.velocity[...] = got.velocity
+    state.acceleration[...] = got.acceleration
+    state.rotation[...] = got.rotation
+    state.plastic[...] = got.plastic
+    return report
