@@ -39,6 +39,10 @@ extern "C" {
 #define TL_LAW_COROTATED 0  /* reference tet law: corotated + J2 return map (material.cc:236-265, 978-1057) */
 #define TL_LAW_SNH 1        /* stable neo-Hookean (neohookean.cc:41-47, 183-192) at one point per tet */
 
+/* tl_settings.flags */
+#define TL_FLAG_PROFILE 1u  /* time the element pass, node assembly and PCG launches with CUDA events */
+#define TL_FLAG_TRACE 2u    /* record each PCG launch's iteration count (synchronises after every solve) */
+
 /* Host buffer element type for state transfer. */
 #define TL_DTYPE_F32 0
 #define TL_DTYPE_F64 1
@@ -90,7 +94,7 @@ typedef struct tl_settings {
   uint32_t plastic_passes;  /* 40  (solver.h:56) */
   uint32_t rigid_split;     /* TL_RIGID_SPLIT_PROJECTED (solver.h:66) */
   uint32_t law;             /* TL_LAW_* */
-  uint32_t reserved;
+  uint32_t flags;           /* TL_FLAG_* */
   double tolerance;         /* 1e-3 (solver.h:64) */
   double spectral_radius;   /* 0.5  (solver.h:65) */
 } tl_settings;
@@ -117,12 +121,17 @@ typedef struct tl_step_report {
   uint32_t plastic_growth;
   uint32_t non_finite;
   uint32_t kernel_launches;
+  uint32_t cg_tangent_iterations;  /* PCG iterations run with the consistent plastic tangent */
+  uint32_t cg_solves;
   double cg_worst_relative_residual;
   double plastic_worst_residual;
   double elastic_energy;
   double kinetic_energy;
   double min_volume_ratio;
   double device_seconds;
+  double element_seconds;   /* TL_FLAG_PROFILE: element-pass kernels */
+  double assemble_seconds;  /* TL_FLAG_PROFILE: node gather + balance kernels */
+  double pcg_seconds;       /* TL_FLAG_PROFILE: persistent PCG launches */
 } tl_step_report;
 
 /* Library version (TL_ABI_VERSION); works without a device. */
@@ -143,6 +152,12 @@ int32_t tl_system_create(tl_ctx* ctx, const tl_mesh_desc* bodies, uint32_t count
                          tl_system** out);
 int32_t tl_system_destroy(tl_system* system);
 int32_t tl_system_counts(const tl_system* system, uint32_t* bodies, uint64_t* nodes, uint64_t* tets);
+
+/* Diagnostics, no reference counterpart: iteration counts (body 0) of the
+ * PCG launches made while TL_FLAG_TRACE was set, oldest first, since the
+ * system was created.  Writes min(capacity, recorded) entries; *count gets
+ * the number recorded. */
+int32_t tl_system_trace(const tl_system* system, uint32_t* iterations, uint32_t capacity, uint32_t* count);
 
 /* talus::DeformableState (mesh.h:56-62) transfer for one body.  position,
  * velocity, acceleration: [3*nodes]; rotation: [9*tets] row-major

@@ -748,8 +748,9 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
     s.acceleration[n] = V3<R>(R(st->acceleration[3 * n]), R(st->acceleration[3 * n + 1]), R(st->acceleration[3 * n + 2]));
     anyAnchored = anyAnchored || s.anchored[n] != 0;
   }
-  // The floating (rigid split) path (solver.cc:2964-2971, 3659-3690) is out of scope.
-  if (!anyAnchored) return -2;
+  // The floating (rigid split) path (solver.cc:2964-2971, 3659-3690) is out of
+  // scope; with RigidSplit::Off an unanchored body takes the ordinary path.
+  if (!anyAnchored && settings->rigid_split != 0u) return -2;
   s.elements.resize(T);
   s.store.resize(T);
   s.rotation.resize(T);

@@ -62,6 +62,8 @@ typedef struct or_settings {
   uint32_t law;             /* OR_LAW_* */
   double tolerance;         /* Settings::tolerance (solver.h:64) */
   double spectral_radius;   /* Settings::spectralRadius (solver.h:65) */
+  uint32_t rigid_split;     /* Settings::rigidSplit (solver.h:66): 0 = Off */
+  uint32_t reserved;
 } or_settings;
 
 typedef struct or_state {

@@ -60,6 +60,8 @@ class _Settings(C.Structure):
         ("law", C.c_uint32),
         ("tolerance", C.c_double),
         ("spectral_radius", C.c_double),
+        ("rigid_split", C.c_uint32),
+        ("reserved", C.c_uint32),
     ]
 
 
@@ -225,6 +227,7 @@ class Settings:
     law: int = LAW_COROTATED
     tolerance: float = 1e-3
     spectral_radius: float = 0.5
+    rigid_split: int = 2
 
 
 def step(precision: int, mesh: Mesh, state: State, materials, settings: Settings, gravity=(0.0, -9.81, 0.0),
@@ -238,7 +241,7 @@ def step(precision: int, mesh: Mesh, state: State, materials, settings: Settings
                _ptr(state.plastic))
     mats = (Material * len(materials))(*materials)
     st = _Settings(settings.substeps, settings.cg_iterations, settings.plastic_passes, settings.law,
-                   settings.tolerance, settings.spectral_radius)
+                   settings.tolerance, settings.spectral_radius, settings.rigid_split, 0)
     g = np.asarray(gravity, dtype=np.float64)
     rep = report if report is not None else Report()
     rc = lib().or_step(precision, C.byref(m), C.byref(s), mats, len(materials), C.byref(st), _ptr(g), dt,

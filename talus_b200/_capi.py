@@ -30,6 +30,8 @@ TL_DTYPE_F64 = 1
 TL_RIGID_SPLIT_OFF = 0
 TL_RIGID_SPLIT_UNPROJECTED = 1
 TL_RIGID_SPLIT_PROJECTED = 2
+TL_FLAG_PROFILE = 1
+TL_FLAG_TRACE = 2
 
 
 class tl_material(C.Structure):
@@ -68,7 +70,7 @@ class tl_settings(C.Structure):
         ("plastic_passes", C.c_uint32),
         ("rigid_split", C.c_uint32),
         ("law", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("flags", C.c_uint32),
         ("tolerance", C.c_double),
         ("spectral_radius", C.c_double),
     ]
@@ -94,12 +96,17 @@ class tl_step_report(C.Structure):
         ("plastic_growth", C.c_uint32),
         ("non_finite", C.c_uint32),
         ("kernel_launches", C.c_uint32),
+        ("cg_tangent_iterations", C.c_uint32),
+        ("cg_solves", C.c_uint32),
         ("cg_worst_relative_residual", C.c_double),
         ("plastic_worst_residual", C.c_double),
         ("elastic_energy", C.c_double),
         ("kinetic_energy", C.c_double),
         ("min_volume_ratio", C.c_double),
         ("device_seconds", C.c_double),
+        ("element_seconds", C.c_double),
+        ("assemble_seconds", C.c_double),
+        ("pcg_seconds", C.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -118,6 +125,7 @@ SIGNATURES = {
     "tl_system_destroy": (C.c_int32, [C.c_void_p]),
     "tl_system_counts": (C.c_int32, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
                                      C.POINTER(C.c_uint64)]),
+    "tl_system_trace": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
     "tl_state_set": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_int32] + [C.c_void_p] * 5),
     "tl_state_get": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_int32] + [C.c_void_p] * 5),
     "tl_step": (C.c_int32, [C.c_void_p, C.POINTER(tl_settings), C.c_void_p, C.c_double,

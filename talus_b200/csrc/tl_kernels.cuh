@@ -98,7 +98,7 @@ struct CgBodyDev {
 };
 
 struct CgReportDev {
-  uint32_t iterations, capped, applications, solves;
+  uint32_t iterations, capped, applications, solves, tangent_iterations, pad;
   double worst_rel;
 };
 
@@ -1033,6 +1033,7 @@ __global__ void __launch_bounds__(TILE, 2)
       rep.capped += (c.taken == s.step[b].limit && residual > c.target) ? 1u : 0u;
       rep.applications += c.taken + (x0zero ? 0u : 1u);
       rep.solves += 1u;
+      rep.tangent_iterations += tangent ? c.taken : 0u;
       rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
       s.cgrep[b] = rep;
     }

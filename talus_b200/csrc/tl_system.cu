@@ -125,6 +125,7 @@ struct SystemBase {
                         const void* plastic) = 0;
   virtual void stateGet(uint32_t body, int32_t dtype, void* x, void* v, void* a, void* rot, void* plastic) = 0;
   virtual int32_t step(const tl_settings& set, const double g[3], double dt, tl_step_report* reports) = 0;
+  std::vector<uint32_t> trace;  // TL_FLAG_TRACE: iterations of each PCG launch (body 0)
   uint32_t bodies = 0;
   uint64_t nodes = 0, tets = 0;
 };
@@ -164,6 +165,32 @@ struct System final : SystemBase {
   DevBuf<GridSyncDev> sync;
   bool hasEyoung = false;
   int pcgGrid[2] = {0, 0};
+  // TL_FLAG_PROFILE: event pairs around kernel classes, resolved at step end
+  bool profiling = false;
+  bool tracing = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> evPool;
+  std::vector<std::pair<int, size_t>> evUsed;  // (class, pool index)
+  cudaEvent_t mark(int cls, bool begin) {
+    if (begin) {
+      if (evUsed.size() == evPool.size()) {
+        cudaEvent_t a, b;
+        TL_CUDA(cudaEventCreate(&a));
+        TL_CUDA(cudaEventCreate(&b));
+        evPool.emplace_back(a, b);
+      }
+      evUsed.emplace_back(cls, evUsed.size());
+      TL_CUDA(cudaEventRecord(evPool[evUsed.back().second].first, st));
+      return evPool[evUsed.back().second].first;
+    }
+    TL_CUDA(cudaEventRecord(evPool[evUsed.back().second].second, st));
+    return evPool[evUsed.back().second].second;
+  }
+  ~System() override {
+    for (auto& e : evPool) {
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+  }
   PinnedBuf<BodyAccDev> hAcc;
   PinnedBuf<uint32_t> hCount;
   PinnedBuf<CgReportDev> hRep;
@@ -569,13 +596,17 @@ struct System final : SystemBase {
       loading.zero(st);
       yielding.zero(st);
     }
+    if (profiling) mark(0, true);
     if (law == TL_LAW_SNH) kElement<S, 1><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass, mode, margin);
     else kElement<S, 0><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass, mode, margin);
     check();
+    if (profiling) mark(0, false);
   }
   void nodeAssemble(const Vec4<S>* taken, uint32_t pass) {
+    if (profiling) mark(1, true);
     kNodeAssemble<S><<<nodeTiles, TILE, 0, st>>>(view(), taken, pass);
     check();
+    if (profiling) mark(1, false);
   }
   void pcg(int law, Vec4<S>* X, uint32_t pass, bool x0zero, bool tangent) {
     kPcgPrepare<S><<<1, TILE, 0, st>>>(view(), pass);
@@ -585,8 +616,16 @@ struct System final : SystemBase {
     void* args[] = {&s, &X, &ps, &xz, &tg};
     const int idx = law == TL_LAW_SNH ? 1 : 0;
     const void* fn = idx ? (const void*)kPcg<S, 1> : (const void*)kPcg<S, 0>;
+    if (profiling) mark(2, true);
     TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(pcgGrid[idx]), dim3(TILE), args, 0, st));
     ++launches;
+    if (profiling) mark(2, false);
+    if (tracing) {
+      uint32_t taken = 0;
+      TL_CUDA(cudaMemcpyAsync(&taken, &cg.ptr[0].taken, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+      TL_CUDA(cudaStreamSynchronize(st));
+      trace.push_back(taken);
+    }
   }
   void finalize(uint32_t which) {
     kFinalize<<<B, TILE, 0, st>>>(dBody.ptr, epart.ptr, npart.ptr, acc.ptr, which);
@@ -621,6 +660,9 @@ struct System final : SystemBase {
       if (!hb[b].anyAnchored && set.rigid_split != TL_RIGID_SPLIT_OFF)
         throw StatusError{TL_ERR_UNSUPPORTED, "floating bodies (no anchored node, rigid split on) are not supported"};
     launches = 0;
+    profiling = (set.flags & TL_FLAG_PROFILE) != 0u;
+    tracing = (set.flags & TL_FLAG_TRACE) != 0u;
+    evUsed.clear();
     cudaEvent_t e0, e1;
     TL_CUDA(cudaEventCreate(&e0));
     TL_CUDA(cudaEventCreate(&e1));
@@ -707,6 +749,12 @@ struct System final : SystemBase {
     TL_CUDA(cudaStreamSynchronize(st));
     float ms = 0.f;
     TL_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    double classSeconds[3] = {0.0, 0.0, 0.0};
+    for (const auto& u : evUsed) {
+      float t = 0.f;
+      TL_CUDA(cudaEventElapsedTime(&t, evPool[u.second].first, evPool[u.second].second));
+      classSeconds[u.first] += double(t) * 1e-3;
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     int32_t status = TL_OK;
@@ -739,6 +787,11 @@ struct System final : SystemBase {
       r.min_volume_ratio = fromMinKey(hacc[b].min_j_key);
       r.device_seconds += double(ms) * 1e-3;
       r.kernel_launches += launches;
+      r.cg_tangent_iterations += hrep[b].tangent_iterations;
+      r.cg_solves += hrep[b].solves;
+      r.element_seconds += classSeconds[0];
+      r.assemble_seconds += classSeconds[1];
+      r.pcg_seconds += classSeconds[2];
     }
     for (uint32_t b = 0; b < B; ++b)
       if (hacc[b].nonfinite) status = TL_ERR_NONFINITE;
@@ -945,7 +998,7 @@ void tl_settings_default(tl_settings* s) {
   s->plastic_passes = 40u;
   s->rigid_split = TL_RIGID_SPLIT_PROJECTED;
   s->law = TL_LAW_COROTATED;
-  s->reserved = 0u;
+  s->flags = 0u;
   s->tolerance = 1.0e-3;
   s->spectral_radius = 0.5;
 }
@@ -1010,6 +1063,15 @@ int32_t tl_system_counts(const tl_system* system, uint32_t* bodies, uint64_t* no
   if (bodies) *bodies = system->impl->bodies;
   if (nodes) *nodes = system->impl->nodes;
   if (tets) *tets = system->impl->tets;
+  return TL_OK;
+}
+
+int32_t tl_system_trace(const tl_system* system, uint32_t* iterations, uint32_t capacity, uint32_t* count) {
+  if (!system || (capacity && !iterations)) return TL_ERR_ARG;
+  const std::vector<uint32_t>& t = system->impl->trace;
+  const size_t n = std::min<size_t>(capacity, t.size());
+  std::copy(t.begin(), t.begin() + n, iterations);
+  if (count) *count = uint32_t(t.size());
   return TL_OK;
 }
 

@@ -108,10 +108,13 @@ class Settings:
     spectral_radius: float = 0.5
     rigid_split: int = capi.TL_RIGID_SPLIT_PROJECTED
     law: int = COROTATED
+    profile: bool = False   # TL_FLAG_PROFILE: per-kernel-class device times in the report
+    trace: bool = False     # TL_FLAG_TRACE: record each PCG launch's iterations (System.trace)
 
     def _c(self) -> capi.tl_settings:
-        return capi.tl_settings(self.substeps, self.cg_iterations, self.plastic_passes, self.rigid_split, self.law, 0,
-                                self.tolerance, self.spectral_radius)
+        flags = (capi.TL_FLAG_PROFILE if self.profile else 0) | (capi.TL_FLAG_TRACE if self.trace else 0)
+        return capi.tl_settings(self.substeps, self.cg_iterations, self.plastic_passes, self.rigid_split, self.law,
+                                flags, self.tolerance, self.spectral_radius)
 
 
 class StepReport(capi.tl_step_report):
@@ -219,6 +222,15 @@ class System:
                                       _ptr(out.acceleration), _ptr(out.rotation), _ptr(out.plastic)),
               self.context.handle)
         return out
+
+    def trace(self) -> list:
+        """Iterations of every PCG launch made with Settings.trace, oldest first."""
+        count = C.c_uint32()
+        check(capi.lib().tl_system_trace(self.handle, None, 0, C.byref(count)), self.context.handle)
+        out = np.zeros(max(1, count.value), np.uint32)
+        check(capi.lib().tl_system_trace(self.handle, out.ctypes.data, count.value, C.byref(count)),
+              self.context.handle)
+        return out[:count.value].tolist()
 
     def step(self, settings: Settings, gravity=(0.0, -9.81, 0.0), delta_time: float = 1.0 / 60.0, reports=None):
         """One deformable::step of every body; returns the per-body reports

@@ -1,0 +1,46 @@
+"""Profiling driver: steps a benchmark workload and records, for every PCG
+launch, its iteration count, so that an ncu capture of one launch of
+tl::kPcg can be turned into DRAM bytes per PCG iteration.
+
+    python -m talus_b200.profile_run --workload plastic-block --steps 4 --precision mixed
+
+prints one JSON line {"pcg_iterations": [...], ...}; PCG launch i of the
+program (0-based, in launch order) made pcg_iterations[i] iterations.  The
+same command runs under `ncu -k regex:kPcg -s <i> -c 1`.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def main():
+    sys.path.insert(0, ROOT)
+    import bench
+    import talus_b200 as tb
+
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="plastic-block", choices=sorted(bench.WORKLOADS))
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    args = ap.parse_args()
+    spec = bench.WORKLOADS[args.workload]
+    mesh, mat = bench.make_mesh(spec)
+    precision = tb.FP32_MIXED if args.precision == "mixed" else tb.FP64
+    law = tb.NEO_HOOKEAN if spec["law"] == "snh" else tb.COROTATED
+    system = tb.System(mesh, [mat], precision)
+    system.set_state(tb.rest_state(mesh))
+    settings = tb.Settings(law=law, trace=True)
+    reports = [system.step(settings)[0].as_dict() for _ in range(args.steps)]
+    print(json.dumps({"workload": args.workload, "precision": args.precision, "tets": mesh.tets,
+                      "nodes": mesh.nodes, "pcg_iterations": system.trace(),
+                      "tangent_iterations": sum(r["cg_tangent_iterations"] for r in reports)}))
+    system.close()
+
+
+if __name__ == "__main__":
+    main()

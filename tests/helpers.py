@@ -22,7 +22,8 @@ def oracle_material(m: tb.PhysicalMaterial) -> po.Material:
 
 
 def oracle_settings(s: tb.Settings) -> po.Settings:
-    return po.Settings(s.substeps, s.cg_iterations, s.plastic_passes, s.law, s.tolerance, s.spectral_radius)
+    return po.Settings(s.substeps, s.cg_iterations, s.plastic_passes, s.law, s.tolerance, s.spectral_radius,
+                       s.rigid_split)
 
 
 def elastic_block(cells=(8, 8, 8), jitter=0.01, seed=1):
