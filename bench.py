@@ -118,17 +118,28 @@ class ClockSampler:
 
 # ------------------------------------------------------------ algorithmic --
 
-def pcg_bytes_per_iteration(T, V, s_bytes, tangent):
-    """Unique bytes one PCG iteration must move (kPcg phases A, B, C), per
-    the layout in talus_b200/csrc/tl_kernels.cuh.  s = 4 (FP32) or 8 (FP64)."""
+def tile_slots(mesh, tile=256):
+    """Slots of the two-level assembly: distinct nodes per 256-element tile."""
+    t = mesh.tet_nodes
+    total = 0
+    for k in range(0, t.shape[0], tile):
+        total += np.unique(t[k:k + tile]).size
+    return total
+
+
+def pcg_bytes_per_iteration(T, V, slots, s_bytes, tangent):
+    """Unique bytes one iteration of the single-body PCG (tl::kPcg1, phases A,
+    B, C) must move, per the layout in talus_b200/csrc/tl_kernels.cuh:
+    every array read or written once per phase.  s = 4 (FP32) or 8 (FP64)."""
     v4 = 4 * s_bytes
-    elem = 16 + 9 * s_bytes + 9 * s_bytes + s_bytes + 4 + (2 * v4 if tangent else 0)  # tet, R, Dm^-1, V, lane
-    elem += 4 * v4          # y_e write (phase A)
-    elem += 4 * 4 + 4 * v4  # CSR entries + y_e read (phase B)
-    node = 2 * v4           # p, z gathered (phase A)
-    node += 2 * v4 + v4 + 4 + v4 + 1 + v4  # B: p, z read; p write; start; rest(mass); anchored; Ap write
-    node += v4 + 2 * v4 + v4 + 2 * v4 + 2 * v4 + v4  # C: p, x r/w, Ap, r r/w, P (2 records), z write
-    return T * elem + V * node
+    # A, per element: tet 16, rotated gradients 9 s, coefficients v4, [flow normal 2 v4],
+    # tile CSR codes 4 x 2 B; per slot: offset 2 B + partial write v4; per node: p, z gathered
+    a = T * (16 + 9 * s_bytes + v4 + (2 * v4 if tangent else 0) + 8) + slots * (2 + v4) + V * 2 * v4
+    # B, per node: p, z read, p write, slot CSR start 4 + per slot id 4 and partial v4, mass record, anchor, Ap write
+    b = V * (2 * v4 + v4 + 4 + v4 + 1 + v4) + slots * (4 + v4)
+    # C, per node: p, x read+write, Ap, r read+write, preconditioner (2 records), z write
+    c = V * (v4 + 2 * v4 + v4 + 2 * v4 + 2 * v4 + v4)
+    return a + b + c
 
 
 def peaks():
@@ -291,8 +302,9 @@ def run_ours(args, spec, rank, world, dist):
     s_bytes = 4 if precision == tb.FP32_MIXED else 8
     iters = totals.cg_iterations
     tangent_iters = totals.cg_tangent_iterations
-    pcg_bytes = (pcg_bytes_per_iteration(mesh.tets, mesh.nodes, s_bytes, True) * tangent_iters +
-                 pcg_bytes_per_iteration(mesh.tets, mesh.nodes, s_bytes, False) * (iters - tangent_iters))
+    slots = tile_slots(mesh)
+    per_iter = {t: pcg_bytes_per_iteration(mesh.tets, mesh.nodes, slots, s_bytes, t) for t in (False, True)}
+    pcg_bytes = per_iter[True] * tangent_iters + per_iter[False] * (iters - tangent_iters)
     launches_pcg = totals.cg_solves
     pcg_time = totals.pcg_seconds
     peak, peak_kind = peaks()
@@ -318,7 +330,8 @@ def run_ours(args, spec, rank, world, dist):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
                 "steps": e2e_steps, "api": "tl_step_host (state in host memory, f32)"},
         "gpu_launches": int(totals.kernel_launches),
-        "roofline": {"bound": "hbm", "kernel": "tl::kPcg (persistent block-Jacobi PCG)", "achieved": achieved,
+        "roofline": {"bound": "hbm", "kernel": "tl::kPcg1 (persistent block-Jacobi PCG, two-level assembly)",
+                     "achieved": achieved,
                      "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                      "traffic": traffic, "launches": launches_pcg, "iterations": iters,
                      "algorithmic_bytes_per_launch": pcg_bytes / max(1, launches_pcg),

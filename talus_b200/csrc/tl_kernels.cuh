@@ -145,9 +145,10 @@ template <class S> struct Sys {
   const S* vols;          // volume in S
   const uint32_t* lane;
   const double* eyoung;   // per-element E override or null
-  S* op;                  // 9 planes: R (corotated) or F (SNH)
-  Vec4<S>* tan;           // 2 planes: (theta, thetaBar, nxx, nyy), (nzz, nxy, nxz, nyz)
-  S* snhc;                // SNH: (lambda + mu)(J - 1) - mu
+  S* op;                  // 9 planes: committed R (corotated) or F (SNH)
+  S* og;                  // 9 planes: matvec gradients R g_k (corotated) or g_k (SNH), k = 1..3
+  Vec4<S>* oc;            // matvec coefficients (a, b, c, -), h_eff^2 V folded in
+  Vec4<S>* on;            // 2 planes: rotated flow normal (xx, yy, zz, xy), (xz, yz, -, -)
   Vec4<S>* plast;         // 2 planes: (exx, eyy, ezz, exy), (exz, eyz, equivalent, -)
   Vec4<S>* fe;            // [4 Tp] (fx, fy, fz, Dxx)
   Vec4<S>* de;            // [4 Tp] (Dyy, Dzz, Dxy, Dxz)
@@ -164,7 +165,23 @@ template <class S> struct Sys {
   CgReportDev* cgrep;
   unsigned int* counter;  // [bodies]
   GridSyncDev* sync;
+  // two-level assembly (single-body PCG): per element tile, the distinct nodes
+  // it touches ("slots"), with a tile-local CSR of (local element, corner)
+  // codes; per node, the slots that hold its partial sums, in tile order.
+  const uint2* tile_meta;      // [elem_tiles] (first slot, slot count)
+  const uint16_t* tile_off;    // [elem_tiles][4 TILE + 1] offsets into tile_ent
+  const uint16_t* tile_ent;    // [elem_tiles][4 TILE] codes 4 * local element + corner
+  Vec4<S>* slot_part;          // [slots] tile-local sums of y_e
+  const uint32_t* tile_node;   // [slots] global node of each slot
+  const uint2* eloc;           // [Tp] an element's 4 corners as slot indices within its tile (4 x u16)
+  const uint4* ns_inline;      // [2][Vp] a node's first 8 slot ids (NO_SLOT when unused)
+  const uint32_t* ns_start;    // [Vp + 1] slots beyond the first 8 (overflow CSR)
+  const uint32_t* ns_slot;     // [overflow slots]
+  double* blk_part;            // [3 * grid] per-block partial sums
 };
+
+constexpr int TILE_OFF_STRIDE = 4 * TILE + 4;  // 4 TILE + 1 offsets, padded to 8-byte rows
+constexpr uint32_t NO_SLOT = 0xffffffffu;
 
 // ------------------------------------------------------------ helpers ----
 
@@ -586,9 +603,27 @@ __global__ void __launch_bounds__(TILE)
         for (int i = 0; i < 3; ++i)
 #pragma unroll
           for (int j = 0; j < 3; ++j) s.op[size_t(3 * i + j) * s.Tp + e] = S(R.m[i][j]);
+        // Matvec operator in the rotated frame: R K R^T p = sum over corners of
+        // V sigma_t(sym(sum_b p_b gh_b^T)) gh_a with gh = R g and the rotated
+        // normal R n R^T; h_eff^2 V folded into the coefficients.
+        const double sv = st.scale * vol;
+#pragma unroll
+        for (int k = 1; k < 4; ++k) {
+          const V3<double> gh = mul(R, g[k]);
+          s.og[size_t(3 * (k - 1) + 0) * s.Tp + e] = S(gh.x);
+          s.og[size_t(3 * (k - 1) + 1) * s.Tp + e] = S(gh.y);
+          s.og[size_t(3 * (k - 1) + 2) * s.Tp + e] = S(gh.z);
+        }
+        s.oc[e] = Vec4<S>{S(sv * (bulk - 2.0 * mu * th / 3.0)), S(sv * 2.0 * mu * th), S(sv * 2.0 * mu * thb), S(0)};
         if (mode & EM_CONSISTENT) {
-          s.tan[e] = Vec4<S>{S(th), S(thb), S(normal.xx), S(normal.yy)};
-          s.tan[s.Tp + e] = Vec4<S>{S(normal.zz), S(normal.xy), S(normal.xz), S(normal.yz)};
+          M3<double> nm;
+          nm.m[0][0] = normal.xx; nm.m[1][1] = normal.yy; nm.m[2][2] = normal.zz;
+          nm.m[0][1] = nm.m[1][0] = normal.xy;
+          nm.m[0][2] = nm.m[2][0] = normal.xz;
+          nm.m[1][2] = nm.m[2][1] = normal.yz;
+          const M3<double> nh = mul(mul(R, nm), transpose(R));
+          s.on[e] = Vec4<S>{S(nh.m[0][0]), S(nh.m[1][1]), S(nh.m[2][2]), S(nh.m[0][1])};
+          s.on[s.Tp + e] = Vec4<S>{S(nh.m[0][2]), S(nh.m[1][2]), S(0), S(0)};
         }
       }
     } else {
@@ -620,7 +655,16 @@ __global__ void __launch_bounds__(TILE)
       for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) s.op[size_t(3 * i + j) * s.Tp + e] = S(F.m[i][j]);
-      s.snhc[e] = S(shifted * change - mu);
+      // Matvec operator: dP = mu dF + ((lambda + mu)(J - 1) - mu) dcof + (lambda + mu)(cof : dF) cof,
+      // h_eff^2 V folded into the coefficients; unrotated gradients.
+      const double sv = st.scale * vol;
+#pragma unroll
+      for (int k = 1; k < 4; ++k) {
+        s.og[size_t(3 * (k - 1) + 0) * s.Tp + e] = S(g[k].x);
+        s.og[size_t(3 * (k - 1) + 1) * s.Tp + e] = S(g[k].y);
+        s.og[size_t(3 * (k - 1) + 2) * s.Tp + e] = S(g[k].z);
+      }
+      s.oc[e] = Vec4<S>{S(sv * mu), S(sv * (shifted * change - mu)), S(sv * shifted), S(0)};
     }
     if (!(mode & EM_COMMIT)) {
 #pragma unroll
@@ -738,67 +782,62 @@ __global__ void __launch_bounds__(TILE) kFinalize(const BodyDev* body, const dou
 
 // ---------------------------------------------------------------- PCG ----
 
-// +scale * R K R^T p_e for one tet (applyStiffness, material.cc:267-288, with
-// the consistent tangent of tetPointTrial when `tangent`), or the exact SNH
-// tangent dP for LAW 1.  Arithmetic in S.
-template <class S, int LAW>
-__device__ __forceinline__ void elementApply(const Sys<S>& s, uint32_t e, const V3<S> p[4], S scale, bool tangent,
-                                             V3<S> y[4]) {
+// h_eff^2 (R K R^T p)_e for one tet: applyStiffness (material.cc:267-288) with
+// the elastic blocks of tetStiffness (material.cc:209-234) or the consistent
+// tangent of tetPointTrial (material.cc:1033-1054), in the rotated frame where
+// gh = R g:  Q = sum_b p_b gh_b^T, e = sym(Q), sigma = a tr(e) I + b e -
+// c (nh : e) nh, y_a = sigma gh_a.  LAW 1: the exact SNH tangent dP(dF) g_a
+// with dF = sum_b p_b g_b^T.  (a, b, c) carry h_eff^2 V.  Arithmetic in S.
+template <class S, int LAW, bool TANGENT>
+__device__ __forceinline__ void elementApply(const Sys<S>& s, uint32_t e, const V3<S> p[4], V3<S> y[4]) {
   V3<S> g[4];
-  gradientsS<S>(s.dms, s.Tp, e, g);
-  const MatDev m = s.mat[s.lane[e]];
-  const double youngs = s.eyoung ? s.eyoung[e] : m.youngs;
-  const S lam = S(youngs * m.lam_unit), mu = S(youngs * m.mu_unit);
-  const S w = scale * s.vols[e];
-  M3<S> O;
+  gradientsS<S>(s.og, s.Tp, e, g);
+  const Vec4<S> k = ld4g(&s.oc[e]);
+  M3<S> Q = zero3<S>();
 #pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) O.m[i][j] = __ldg(s.op + size_t(3 * i + j) * s.Tp + e);
+  for (int c = 1; c < 4; ++c) addOuter(Q, p[c] - p[0], g[c]);  // sum_c g_c = 0
   if (LAW == 0) {
-    M3<S> Hq = zero3<S>();
-#pragma unroll
-    for (int c = 0; c < 4; ++c) addOuter(Hq, mulT(O, p[c]), g[c]);
-    const Sym<S> eps = symOf(Hq);
-    Sym<S> sig;
-    if (tangent) {
-      const Vec4<S> t0 = ld4g(&s.tan[e]), t1 = ld4g(&s.tan[s.Tp + e]);
-      const Sym<S> n = {t0.z, t0.w, t1.x, t1.y, t1.z, t1.w};
-      sig = tangentStress(eps, lam + S(2) * mu / S(3), mu, t0.x, t0.y, n);
-    } else {
-      const S tr = symTrace(eps);
-      sig = {lam * tr + S(2) * mu * eps.xx, lam * tr + S(2) * mu * eps.yy, lam * tr + S(2) * mu * eps.zz,
-             S(2) * mu * eps.xy, S(2) * mu * eps.xz, S(2) * mu * eps.yz};
+    const Sym<S> eps = symOf(Q);
+    const S tr = symTrace(eps);
+    const S at = k.x * tr;
+    Sym<S> sig = {at + k.y * eps.xx, at + k.y * eps.yy, at + k.y * eps.zz, k.y * eps.xy, k.y * eps.xz, k.y * eps.yz};
+    if (TANGENT) {
+      const Vec4<S> n0 = ld4g(&s.on[e]), n1 = ld4g(&s.on[s.Tp + e]);
+      const Sym<S> n = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y};
+      const S ne = k.z * symContract(n, eps);
+      sig.xx -= ne * n.xx;
+      sig.yy -= ne * n.yy;
+      sig.zz -= ne * n.zz;
+      sig.xy -= ne * n.xy;
+      sig.xz -= ne * n.xz;
+      sig.yz -= ne * n.yz;
     }
 #pragma unroll
-    for (int c = 0; c < 4; ++c) y[c] = w * mul(O, symMul(sig, g[c]));
+    for (int c = 1; c < 4; ++c) y[c] = symMul(sig, g[c]);
   } else {
-    // dP = mu dF + c dcof(F)[dF] + (lambda + mu)(cof F : dF) cof F
-    M3<S> dF = zero3<S>();
+    M3<S> F;
 #pragma unroll
-    for (int c = 0; c < 4; ++c) addOuter(dF, p[c], g[c]);
-    const M3<S> C = cofactor(O);
-    const S cc = __ldg(&s.snhc[e]);
-    const S k = (lam + mu) * contract(C, dF);
-    // columns of F and dF; column j of cof is F_{j+1} x F_{j+2}
-    V3<S> Fc[3], dc[3];
+    for (int i = 0; i < 3; ++i)
 #pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      Fc[j] = {O.m[0][j], O.m[1][j], O.m[2][j]};
-      dc[j] = {dF.m[0][j], dF.m[1][j], dF.m[2][j]};
-    }
+      for (int j = 0; j < 3; ++j) F.m[i][j] = __ldg(s.op + size_t(3 * i + j) * s.Tp + e);
+    const M3<S> C = cofactor(F);
+    const S kk = k.z * contract(C, Q);
+    // column j of cof F is F_{j+1} x F_{j+2}; its differential along Q
     M3<S> dP;
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
       const int j1 = (j + 1) % 3, j2 = (j + 2) % 3;
-      const V3<S> dcof = cross(dc[j1], Fc[j2]) + cross(Fc[j1], dc[j2]);
-      dP.m[0][j] = mu * dF.m[0][j] + cc * dcof.x + k * C.m[0][j];
-      dP.m[1][j] = mu * dF.m[1][j] + cc * dcof.y + k * C.m[1][j];
-      dP.m[2][j] = mu * dF.m[2][j] + cc * dcof.z + k * C.m[2][j];
+      const V3<S> f1 = {F.m[0][j1], F.m[1][j1], F.m[2][j1]}, f2 = {F.m[0][j2], F.m[1][j2], F.m[2][j2]};
+      const V3<S> d1 = {Q.m[0][j1], Q.m[1][j1], Q.m[2][j1]}, d2 = {Q.m[0][j2], Q.m[1][j2], Q.m[2][j2]};
+      const V3<S> dcof = cross(d1, f2) + cross(f1, d2);
+      dP.m[0][j] = k.x * Q.m[0][j] + k.y * dcof.x + kk * C.m[0][j];
+      dP.m[1][j] = k.x * Q.m[1][j] + k.y * dcof.y + kk * C.m[1][j];
+      dP.m[2][j] = k.x * Q.m[2][j] + k.y * dcof.z + kk * C.m[2][j];
     }
 #pragma unroll
-    for (int c = 0; c < 4; ++c) y[c] = w * mul(dP, g[c]);
+    for (int c = 1; c < 4; ++c) y[c] = mul(dP, g[c]);
   }
+  y[0] = -(y[1] + y[2] + y[3]);
 }
 
 // Reads a body's PCG scalars from L2 (they are written by other blocks).
@@ -846,7 +885,8 @@ __global__ void __launch_bounds__(TILE, 2)
       V3<S> pe[4], y[4];
 #pragma unroll
       for (int c = 0; c < 4; ++c) pe[c] = xyz(ld4cg(&X[nodes[c]]));
-      elementApply<S, LAW>(s, e, pe, S(s.step[b].scale), tangent != 0u, y);
+      if (tangent) elementApply<S, LAW, true>(s, e, pe, y);
+      else elementApply<S, LAW, false>(s, e, pe, y);
 #pragma unroll
       for (int c = 0; c < 4; ++c) s.ye[4 * e + c] = pack(y[c]);
     }
@@ -926,7 +966,8 @@ __global__ void __launch_bounds__(TILE, 2)
 #pragma unroll
       for (int c = 0; c < 4; ++c)
         pe[c] = fmaV(blend, xyz(ld4cg(&s.p[nodes[c]])), xyz(ld4cg(&s.z[nodes[c]])));
-      elementApply<S, LAW>(s, e, pe, S(s.step[b].scale), tangent != 0u, y);
+      if (tangent) elementApply<S, LAW, true>(s, e, pe, y);
+      else elementApply<S, LAW, false>(s, e, pe, y);
 #pragma unroll
       for (int c = 0; c < 4; ++c) s.ye[4 * e + c] = pack(y[c]);
     }
@@ -1037,6 +1078,301 @@ __global__ void __launch_bounds__(TILE, 2)
       rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
       s.cgrep[b] = rep;
     }
+  }
+}
+
+// ------------------------------------------------ single-body fast PCG ----
+
+__device__ __forceinline__ unsigned int atomAddRelease(unsigned int* p, unsigned int v) {
+  unsigned int old;
+  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ unsigned int ldAcquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Counting grid barrier: barrier k of a launch completes when the arrival
+// counter (zeroed before the launch) reaches gridDim.x * k.  Release on
+// arrival, acquire while polling; the wait is bounded by TL_BARRIER_LIMIT_NS,
+// after which the block records TL_ERR_TIMEOUT and every block leaves.
+__device__ __forceinline__ bool countBarrier(GridSyncDev* sync, unsigned int& k) {
+  __shared__ int ok;
+  ++k;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int good = 1;
+    const unsigned int goal = gridDim.x * k;
+    atomAddRelease(&sync->arrive, 1u);
+    if (ldAcquire(&sync->arrive) < goal) {
+      const unsigned long long t0 = globalTimer();
+      unsigned int polls = 0;
+      while (ldAcquire(&sync->arrive) < goal) {
+        if ((++polls & 255u) == 0u) {
+          if (*(volatile int*)&sync->error != 0) {
+            good = 0;
+            break;
+          }
+          if (globalTimer() - t0 > TL_BARRIER_LIMIT_NS) {
+            atomicExch(&sync->error, 5);  // TL_ERR_TIMEOUT
+            good = 0;
+            break;
+          }
+        }
+      }
+    }
+    ok = good;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// Sum of the per-block partials field f of every block, in block order; the
+// same value in every block (block-wide call, result broadcast).
+__device__ __forceinline__ double sumBlocks(const double* part, unsigned int field) {
+  __shared__ double total;
+  if (threadIdx.x < 32) {
+    double v = 0.0;
+    for (unsigned int b = threadIdx.x; b < gridDim.x; b += 32) v += __ldcg(part + size_t(field) * gridDim.x + b);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) total = v;
+  }
+  __syncthreads();
+  const double r = total;
+  __syncthreads();
+  return r;
+}
+
+// One element tile of the matvec: y_e = h_eff^2 (R K R^T p)_e for its 256
+// elements, then the tile-local sums of y_e per touched node, in ascending
+// element order, written to the tile's slots.  The tile's distinct nodes are
+// staged once in shared memory (p = z + blend p_prev formed once per node, or
+// X for the initial residual), elements read their corners from there by
+// local index, and the tile's local CSR is fetched while the elements compute.
+template <class S, int LAW, bool TANGENT>
+__device__ __forceinline__ void matvecTile(const Sys<S>& s, uint32_t tile, const Vec4<S>* X, S blend,
+                                           S (*buf)[4 * TILE], uint16_t* sOff, uint16_t* sEnt) {
+  const uint32_t e = tile * TILE + threadIdx.x;
+  const uint2 meta = __ldg(&s.tile_meta[tile]);
+  const uint2 entv = __ldg(reinterpret_cast<const uint2*>(s.tile_ent + size_t(tile) * 4 * TILE) + threadIdx.x);
+  const uint16_t* off = s.tile_off + size_t(tile) * TILE_OFF_STRIDE;
+  const uint2 offv = __ldg(reinterpret_cast<const uint2*>(off) + threadIdx.x);
+  const uint16_t offLast = threadIdx.x == 0 ? __ldg(&off[4 * TILE]) : uint16_t(0);
+  const bool live = e < s.body[0].elem_end;
+  const uint2 loc = live ? __ldg(&s.eloc[e]) : make_uint2(0u, 0u);
+  // stage the tile's nodes: buf[k][j] = component k of node j
+  for (uint32_t j = threadIdx.x; j < meta.y; j += TILE) {
+    const uint32_t n = __ldg(&s.tile_node[meta.x + j]);
+    V3<S> v;
+    if (X) v = xyz(ld4cg(&X[n]));
+    else v = fmaV(blend, xyz(ld4cg(&s.p[n])), xyz(ld4cg(&s.z[n])));
+    buf[0][j] = v.x;
+    buf[1][j] = v.y;
+    buf[2][j] = v.z;
+  }
+  __syncthreads();
+  V3<S> y[4] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  if (live) {
+    const uint32_t l[4] = {loc.x & 0xffffu, loc.x >> 16, loc.y & 0xffffu, loc.y >> 16};
+    V3<S> pe[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) pe[c] = {buf[0][l[c]], buf[1][l[c]], buf[2][l[c]]};
+    elementApply<S, LAW, TANGENT>(s, e, pe, y);
+  }
+  __syncthreads();  // node values consumed: buf now holds y, buf[k][c TILE + element]
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    buf[0][c * TILE + threadIdx.x] = y[c].x;
+    buf[1][c * TILE + threadIdx.x] = y[c].y;
+    buf[2][c * TILE + threadIdx.x] = y[c].z;
+  }
+  reinterpret_cast<uint2*>(sEnt)[threadIdx.x] = entv;
+  reinterpret_cast<uint2*>(sOff)[threadIdx.x] = offv;
+  if (threadIdx.x == 0) sOff[4 * TILE] = offLast;
+  __syncthreads();
+  for (uint32_t j = threadIdx.x; j < meta.y; j += TILE) {
+    const uint32_t k0 = sOff[j], k1 = sOff[j + 1];
+    S ax = 0, ay = 0, az = 0;
+    for (uint32_t k = k0; k < k1; ++k) {
+      const uint32_t code = sEnt[k];
+      const uint32_t q = (code & 3u) * TILE + (code >> 2);
+      ax += buf[0][q];
+      ay += buf[1][q];
+      az += buf[2][q];
+    }
+    s.slot_part[meta.x + j] = Vec4<S>{ax, ay, az, S(0)};
+  }
+  __syncthreads();
+}
+
+// Sum over node n's slots in ascending tile order, FP64 accumulation.  The
+// first eight slot ids sit inline with the node (two 16-byte records), so all
+// partial loads are issued at once; further slots come from the overflow CSR.
+template <class S> __device__ __forceinline__ V3<double> gatherSlots(const Sys<S>& s, uint32_t n) {
+  const uint4 i0 = __ldg(&s.ns_inline[n]), i1 = __ldg(&s.ns_inline[s.Vp + n]);
+  const uint32_t k0 = __ldg(&s.ns_start[n]), k1 = __ldg(&s.ns_start[n + 1]);
+  const uint32_t ids[8] = {i0.x, i0.y, i0.z, i0.w, i1.x, i1.y, i1.z, i1.w};
+  Vec4<S> v[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) v[k] = ids[k] != NO_SLOT ? ld4cg(&s.slot_part[ids[k]]) : Vec4<S>{0, 0, 0, 0};
+  V3<double> acc = {0, 0, 0};
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc = acc + cvt<double>(xyz(v[k]));
+  for (uint32_t k = k0; k < k1; ++k) acc = acc + cvt<double>(xyz(ld4cg(&s.slot_part[__ldg(&s.ns_slot[k])])));
+  return acc;
+}
+
+// Persistent PCG for a system holding ONE body (conjugateGradient,
+// solver.cc:1904-2089, block-Jacobi branch).  Per iteration:
+//   A (element tiles)  y_e and tile-local node sums (two-level assembly)
+//   B (node tiles)     p = z + blend p_prev; Ap = inertia m p + sum of slots; p.Ap
+//   C (node tiles)     x += stride p; r -= stride Ap; z = P r; r.z, r.r
+// with a grid barrier after each phase.  Every block accumulates its own
+// partial sums in a fixed order and, after the barrier, every block adds the
+// blocks' partials in block order, so all blocks take the same decisions
+// (convergence, breakdown) with no further communication.
+template <class S, int LAW, bool TANGENT>
+__global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, Vec4<S>* X, uint32_t x0zero) {
+  __shared__ S buf[3][4 * TILE];
+  __shared__ __align__(8) uint16_t sOff[TILE_OFF_STRIDE];
+  __shared__ __align__(8) uint16_t sEnt[4 * TILE];
+  const uint32_t G = gridDim.x;
+  unsigned int bar = 0;
+  const BodyDev bd = s.body[0];
+  const BodyStepDev st = s.step[0];
+  const S zero = S(0);
+  double* part = s.blk_part;
+  // ---- init: r = right - A x (anchored rows 0), z = P r, p_prev = 0
+  if (!x0zero) {
+    for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G) matvecTile<S, LAW, TANGENT>(s, tile, X, zero, buf, sOff, sEnt);
+    if (!countBarrier(s.sync, bar)) return;
+  }
+  {
+    double rz = 0.0, rr = 0.0, bb = 0.0;
+    for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
+      const uint32_t n = tile * TILE + threadIdx.x;
+      if (n >= bd.node_end) continue;
+      const Vec4<S> rhs = s.right[n];
+      V3<S> r = {zero, zero, zero};
+      if (!s.anch[n]) {
+        V3<double> ax = {0, 0, 0};
+        if (!x0zero) ax = (st.inertia * double(ld4g(&s.rest4[n]).w)) * cvt<double>(xyz(ld4cg(&X[n]))) + gatherSlots(s, n);
+        r = cvt<S>(cvt<double>(xyz(rhs)) - ax);
+      }
+      const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
+      const Sym<S> P = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
+      const V3<S> z = symMul(P, r);
+      s.r[n] = pack(r);
+      s.z[n] = pack(z);
+      s.p[n] = Vec4<S>{zero, zero, zero, zero};
+      if (x0zero) X[n] = Vec4<S>{zero, zero, zero, zero};
+      rz += dot(cvt<double>(r), cvt<double>(z));
+      rr += dot(cvt<double>(r), cvt<double>(r));
+      bb += dot(cvt<double>(xyz(rhs)), cvt<double>(xyz(rhs)));
+    }
+    double v[3] = {rz, rr, bb};
+    blockSum<3>(v);
+    if (threadIdx.x == 0) {
+      part[blockIdx.x] = v[0];
+      part[G + blockIdx.x] = v[1];
+      part[2 * G + blockIdx.x] = v[2];
+    }
+  }
+  if (!countBarrier(s.sync, bar)) return;
+  double squared = sumBlocks(part, 0);
+  double length = sumBlocks(part, 1);
+  const double reference = sqrt(sumBlocks(part, 2));
+  const double floor = fmax(reference, 1.1754943508222875e-38);  // std::numeric_limits<float>::min()
+  const double target = st.tolerance * floor;
+  const double startRes = sqrt(length) / floor;
+  double blend = 0.0;
+  uint32_t taken = 0;
+  if (!countBarrier(s.sync, bar)) return;  // every block has read the init partials
+  for (;;) {
+    if (taken >= st.limit || sqrt(length) <= target) break;
+    // ---- A
+    for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G)
+      matvecTile<S, LAW, TANGENT>(s, tile, nullptr, S(blend), buf, sOff, sEnt);
+    if (!countBarrier(s.sync, bar)) return;
+    // ---- B
+    double pap = 0.0;
+    for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
+      const uint32_t n = tile * TILE + threadIdx.x;
+      if (n >= bd.node_end) continue;
+      const V3<S> pn = fmaV(S(blend), xyz(ld4cg(&s.p[n])), xyz(ld4cg(&s.z[n])));
+      s.p[n] = pack(pn);
+      V3<S> apn = {zero, zero, zero};
+      if (!s.anch[n]) apn = cvt<S>((st.inertia * double(ld4g(&s.rest4[n]).w)) * cvt<double>(pn) + gatherSlots(s, n));
+      s.ap[n] = pack(apn);
+      pap += dot(cvt<double>(pn), cvt<double>(apn));
+    }
+    {
+      double v[1] = {pap};
+      blockSum<1>(v);
+      if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+    }
+    if (!countBarrier(s.sync, bar)) return;
+    const double curvature = sumBlocks(part, 0);
+    if (!(curvature > 0.0) || !(squared > 0.0)) break;
+    const double stride = squared / curvature;
+    // ---- C
+    double rz = 0.0, rr = 0.0;
+    for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
+      const uint32_t n = tile * TILE + threadIdx.x;
+      if (n >= bd.node_end) continue;
+      const V3<S> pn = xyz(ld4cg(&s.p[n]));
+      const V3<S> x = fmaV(S(stride), pn, xyz(ld4cg(&X[n])));
+      const V3<S> r = fmaV(S(-stride), xyz(ld4cg(&s.ap[n])), xyz(ld4cg(&s.r[n])));
+      const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
+      const Sym<S> P = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
+      const V3<S> z = symMul(P, r);
+      X[n] = pack(x);
+      s.r[n] = pack(r);
+      s.z[n] = pack(z);
+      rz += dot(cvt<double>(r), cvt<double>(z));
+      rr += dot(cvt<double>(r), cvt<double>(r));
+    }
+    {
+      double v[2] = {rz, rr};
+      blockSum<2>(v);
+      if (threadIdx.x == 0) {
+        part[G + blockIdx.x] = v[0];
+        part[2 * G + blockIdx.x] = v[1];
+      }
+    }
+    if (!countBarrier(s.sync, bar)) return;
+    const double next = sumBlocks(part, 1);
+    length = sumBlocks(part, 2);
+    blend = next / squared;
+    squared = next;
+    ++taken;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const double residual = sqrt(length);
+    CgBodyDev c;
+    c.squared = squared;
+    c.target = target;
+    c.floor = floor;
+    c.length = length;
+    c.stride = 0.0;
+    c.blend = blend;
+    c.start_res = startRes;
+    c.rel_res = residual / floor;
+    c.taken = taken;
+    c.done = 1u;
+    c.pad0 = c.pad1 = 0;
+    s.cg[0] = c;
+    CgReportDev rep = s.cgrep[0];
+    rep.iterations += taken;
+    rep.capped += (taken == st.limit && residual > target) ? 1u : 0u;
+    rep.applications += taken + (x0zero ? 0u : 1u);
+    rep.solves += 1u;
+    rep.tangent_iterations += TANGENT ? taken : 0u;
+    rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
+    s.cgrep[0] = rep;
   }
 }
 

@@ -155,8 +155,18 @@ struct System final : SystemBase {
   DevBuf<uint32_t> start, entry, lane;
   DevBuf<uint4> tet;
   DevBuf<double> dm, vold, eyoung;
-  DevBuf<S> dms, vols, op, snhc, de2;
-  DevBuf<Vec4<S>> tan, plast, fe, de, ye;
+  DevBuf<S> dms, vols, op, og, de2;
+  DevBuf<Vec4<S>> oc, on, plast, fe, de, ye;
+  // two-level assembly structures (single-body PCG)
+  DevBuf<uint2> tileMeta;
+  DevBuf<uint16_t> tileOff, tileEnt;
+  DevBuf<Vec4<S>> slotPart;
+  DevBuf<uint32_t> nsStart, nsSlot;
+  DevBuf<uint4> nsInline;
+  DevBuf<uint32_t> tileNode;
+  DevBuf<uint2> eloc;
+  DevBuf<double> blkPart;
+  int pcg1Grid[2][2] = {{0, 0}, {0, 0}};  // [law][tangent]
   DevBuf<double> part, npart, epart;
   DevBuf<uint32_t> loading, yielding, counter;
   DevBuf<BodyAccDev> acc;
@@ -245,8 +255,19 @@ struct System final : SystemBase {
     s.lane = lane.ptr;
     s.eyoung = hasEyoung ? eyoung.ptr : nullptr;
     s.op = op.ptr;
-    s.tan = tan.ptr;
-    s.snhc = snhc.ptr;
+    s.og = og.ptr;
+    s.oc = oc.ptr;
+    s.on = on.ptr;
+    s.tile_meta = tileMeta.ptr;
+    s.tile_off = tileOff.ptr;
+    s.tile_ent = tileEnt.ptr;
+    s.slot_part = slotPart.ptr;
+    s.ns_inline = nsInline.ptr;
+    s.tile_node = tileNode.ptr;
+    s.eloc = eloc.ptr;
+    s.ns_start = nsStart.ptr;
+    s.ns_slot = nsSlot.ptr;
+    s.blk_part = blkPart.ptr;
     s.plast = plast.ptr;
     s.fe = fe.ptr;
     s.de = de.ptr;
@@ -437,10 +458,12 @@ struct System final : SystemBase {
       op.upload(ident.data(), ident.size(), st);
       TL_CUDA(cudaStreamSynchronize(st));
     }
-    tan.alloc(size_t(2) * Tp);
-    tan.zero(st);
-    snhc.alloc(Tp);
-    snhc.zero(st);
+    og.alloc(size_t(9) * Tp);
+    og.zero(st);
+    oc.alloc(Tp);
+    oc.zero(st);
+    on.alloc(size_t(2) * Tp);
+    on.zero(st);
     plast.alloc(size_t(2) * Tp);
     plast.zero(st);
     fe.alloc(size_t(4) * Tp);
@@ -468,7 +491,108 @@ struct System final : SystemBase {
     TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kPcg<S, 1>, TILE, 0));
     pcgGrid[1] = std::max(1, std::min(perSm * ctx->sms, int(std::max(nodeTiles, elemTiles))));
     if (perSm < 1) throw StatusError{TL_ERR_CUDA, "PCG kernel cannot be resident"};
+    if (B == 1) buildTiles(hTet);
     TL_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // Two-level assembly structures: per element tile the distinct nodes it
+  // touches (its slots, ascending node) with a tile-local CSR of the
+  // (local element, corner) codes in ascending element order; per node the
+  // slots holding its partial sums, in ascending tile order.
+  void buildTiles(const std::vector<uint4>& hTet) {
+    std::vector<uint2> meta(elemTiles);
+    std::vector<uint16_t> off(size_t(elemTiles) * TILE_OFF_STRIDE, 0), ent(size_t(elemTiles) * 4 * TILE, 0);
+    std::vector<uint32_t> slotNode;
+    std::vector<uint16_t> cornerSlot(size_t(4) * Tp, 0);
+    std::vector<std::pair<uint32_t, uint32_t>> items;  // (node, code)
+    for (uint32_t t = 0; t < elemTiles; ++t) {
+      const BodyDev& bd = bodyHost[0];
+      const uint32_t e0 = t * TILE, e1 = std::min<uint32_t>(e0 + TILE, bd.elem_end);
+      items.clear();
+      for (uint32_t e = e0; e < e1; ++e) {
+        const uint32_t q[4] = {hTet[e].x, hTet[e].y, hTet[e].z, hTet[e].w};
+        for (uint32_t c = 0; c < 4; ++c) items.emplace_back(q[c], 4 * (e - e0) + c);
+      }
+      std::sort(items.begin(), items.end());
+      const uint32_t base = uint32_t(slotNode.size());
+      uint16_t* o = off.data() + size_t(t) * TILE_OFF_STRIDE;
+      uint16_t* en = ent.data() + size_t(t) * 4 * TILE;
+      uint32_t local = 0;
+      for (size_t k = 0; k < items.size(); ++k) {
+        if (k == 0 || items[k].first != items[k - 1].first) {
+          o[local++] = uint16_t(k);
+          slotNode.push_back(items[k].first);
+        }
+        en[k] = uint16_t(items[k].second);
+        // corner (element, c) of this item reads local node (local - 1)
+        const uint32_t le = items[k].second >> 2, c = items[k].second & 3u;
+        cornerSlot[size_t(e0 + le) * 4 + c] = uint16_t(local - 1);
+      }
+      o[local] = uint16_t(items.size());
+      meta[t] = make_uint2(base, local);
+    }
+    const size_t slots = slotNode.size();
+    std::vector<uint32_t> start(size_t(Vp) + 1, 0), list(slots);
+    for (uint32_t n : slotNode) ++start[n + 1];
+    for (uint32_t n = 0; n < Vp; ++n) start[n + 1] += start[n];
+    {
+      std::vector<uint32_t> cursor(start.begin(), start.end() - 1);
+      for (size_t k = 0; k < slots; ++k) list[cursor[slotNode[k]]++] = uint32_t(k);  // slots ascend with tiles
+    }
+    // the first 8 slots of each node inline, the rest in an overflow CSR
+    std::vector<uint4> inl(size_t(2) * Vp, make_uint4(NO_SLOT, NO_SLOT, NO_SLOT, NO_SLOT));
+    std::vector<uint32_t> ostart(size_t(Vp) + 1, 0), olist;
+    for (uint32_t n = 0; n < Vp; ++n) {
+      uint32_t ids[8] = {NO_SLOT, NO_SLOT, NO_SLOT, NO_SLOT, NO_SLOT, NO_SLOT, NO_SLOT, NO_SLOT};
+      for (uint32_t k = start[n]; k < start[n + 1]; ++k) {
+        if (k - start[n] < 8) ids[k - start[n]] = list[k];
+        else olist.push_back(list[k]);
+      }
+      inl[n] = make_uint4(ids[0], ids[1], ids[2], ids[3]);
+      inl[size_t(Vp) + n] = make_uint4(ids[4], ids[5], ids[6], ids[7]);
+      ostart[n + 1] = uint32_t(olist.size());
+    }
+    tileMeta.alloc(elemTiles);
+    tileMeta.upload(meta.data(), elemTiles, st);
+    tileOff.alloc(off.size());
+    tileOff.upload(off.data(), off.size(), st);
+    tileEnt.alloc(ent.size());
+    tileEnt.upload(ent.data(), ent.size(), st);
+    slotPart.alloc(std::max<size_t>(slots, 1));
+    tileNode.alloc(std::max<size_t>(slots, 1));
+    tileNode.upload(slotNode.data(), slots, st);
+    {
+      std::vector<uint2> loc(Tp);
+      for (uint32_t e = 0; e < Tp; ++e) {
+        const uint16_t* q = cornerSlot.data() + size_t(e) * 4;
+        loc[e] = make_uint2(uint32_t(q[0]) | (uint32_t(q[1]) << 16), uint32_t(q[2]) | (uint32_t(q[3]) << 16));
+      }
+      eloc.alloc(Tp);
+      eloc.upload(loc.data(), Tp, st);
+      TL_CUDA(cudaStreamSynchronize(st));
+    }
+    nsInline.alloc(inl.size());
+    nsInline.upload(inl.data(), inl.size(), st);
+    nsStart.alloc(ostart.size());
+    nsStart.upload(ostart.data(), ostart.size(), st);
+    nsSlot.alloc(std::max<size_t>(olist.size(), 1));
+    nsSlot.upload(olist.data(), olist.size(), st);
+    TL_CUDA(cudaStreamSynchronize(st));
+    // cooperative grid per kernel variant, bounded by the tile counts
+    auto grid = [&](const void* fn) {
+      int perSm = 0;
+      TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, TILE, 0));
+      if (perSm < 1) throw StatusError{TL_ERR_CUDA, "PCG kernel cannot be resident"};
+      return std::max(1, std::min(perSm * ctx->sms, int(std::max(nodeTiles, elemTiles))));
+    };
+    pcg1Grid[0][0] = grid((const void*)kPcg1<S, 0, false>);
+    pcg1Grid[0][1] = grid((const void*)kPcg1<S, 0, true>);
+    pcg1Grid[1][0] = grid((const void*)kPcg1<S, 1, false>);
+    pcg1Grid[1][1] = grid((const void*)kPcg1<S, 1, true>);
+    int most = 0;
+    for (auto& row : pcg1Grid)
+      for (int gsz : row) most = std::max(most, gsz);
+    blkPart.alloc(size_t(3) * most);
   }
 
   // ------------------------------------------------------------- state ----
@@ -613,11 +737,18 @@ struct System final : SystemBase {
     check();
     Sys<S> s = view();
     uint32_t ps = pass, xz = x0zero ? 1u : 0u, tg = tangent ? 1u : 0u;
-    void* args[] = {&s, &X, &ps, &xz, &tg};
     const int idx = law == TL_LAW_SNH ? 1 : 0;
-    const void* fn = idx ? (const void*)kPcg<S, 1> : (const void*)kPcg<S, 0>;
     if (profiling) mark(2, true);
-    TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(pcgGrid[idx]), dim3(TILE), args, 0, st));
+    if (B == 1) {  // single body: two-level assembly, per-block partials
+      void* args[] = {&s, &X, &xz};
+      const void* fn = idx ? (tangent ? (const void*)kPcg1<S, 1, true> : (const void*)kPcg1<S, 1, false>)
+                           : (tangent ? (const void*)kPcg1<S, 0, true> : (const void*)kPcg1<S, 0, false>);
+      TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(pcg1Grid[idx][tangent ? 1 : 0]), dim3(TILE), args, 0, st));
+    } else {
+      void* args[] = {&s, &X, &ps, &xz, &tg};
+      const void* fn = idx ? (const void*)kPcg<S, 1> : (const void*)kPcg<S, 0>;
+      TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(pcgGrid[idx]), dim3(TILE), args, 0, st));
+    }
     ++launches;
     if (profiling) mark(2, false);
     if (tracing) {
