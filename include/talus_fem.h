@@ -30,6 +30,7 @@ extern "C" {
 #define TL_ERR_TIMEOUT 5        /* a device-side wait ran out; the context stays usable */
 #define TL_ERR_UNSUPPORTED 6    /* feature outside this library's scope (e.g. floating bodies) */
 #define TL_ERR_NO_DEVICE 7      /* no CUDA device / extension unusable */
+#define TL_ERR_TOO_LARGE 8      /* input exceeds a fixed capacity (tl_step_noalloc) */
 
 /* Arithmetic of a resident system. */
 #define TL_FP64 0        /* plain FP64 GPU step */
@@ -187,6 +188,32 @@ int32_t tl_step_host(tl_system* system, uint32_t body, int32_t dtype, void* posi
 
 /* Default settings (Settings{} in solver.h:51-107). */
 void tl_settings_default(tl_settings* settings);
+
+/* No counterpart in the reference.  One step of one small body that allocates
+ * nothing, for callers that cannot call cudaMalloc: engines with a fixed GPU
+ * memory budget, code that runs while a CUDA graph is being captured (where
+ * allocation is not allowed), hosts that hand out device memory only through
+ * their own pool.  Same meaning of arguments and results as tl_step_host, with
+ * the mesh passed each call; the arithmetic is FP64.
+ *
+ * All device scratch lives in one fixed array inside the library
+ * (TL_NOALLOC_ARENA_BYTES on every GPU that loads it, held until the process
+ * exits); nothing is allocated on the device or the host heap.  Limits:
+ * TL_NOALLOC_MAX_NODES nodes, TL_NOALLOC_MAX_TETS tets, TL_NOALLOC_MAX_LANES
+ * material lanes (beyond them: TL_ERR_TOO_LARGE), and no plastic Newton loop
+ * (a yielding material with plastic_passes > 1: TL_ERR_UNSUPPORTED).  The
+ * first call on a device looks up the array's device address (once per
+ * device); make that first call before any stream capture begins.  Calls are
+ * serialised inside the library; GPU work of two overlapping calls would race
+ * on the shared array.  Runs on the legacy default stream and returns when the
+ * step has finished. */
+#define TL_NOALLOC_MAX_NODES 1024
+#define TL_NOALLOC_MAX_TETS 4096
+#define TL_NOALLOC_MAX_LANES 16
+#define TL_NOALLOC_ARENA_BYTES 4194304
+int32_t tl_step_noalloc(int32_t device, const tl_mesh_desc* mesh, int32_t dtype, void* position, void* velocity,
+                        void* acceleration, void* rotation, void* plastic, const tl_settings* settings,
+                        const double gravity[3], double dt, tl_step_report* report);
 
 #ifdef __cplusplus
 }

@@ -20,6 +20,7 @@ TL_ERR_NONFINITE = 4
 TL_ERR_TIMEOUT = 5
 TL_ERR_UNSUPPORTED = 6
 TL_ERR_NO_DEVICE = 7
+TL_ERR_TOO_LARGE = 8
 
 TL_FP64 = 0
 TL_FP32_MIXED = 1
@@ -133,6 +134,8 @@ SIGNATURES = {
     "tl_step_host": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_int32] + [C.c_void_p] * 5 +
                      [C.POINTER(tl_settings), C.c_void_p, C.c_double, C.POINTER(tl_step_report)]),
     "tl_settings_default": (None, [C.POINTER(tl_settings)]),
+    "tl_step_noalloc": (C.c_int32, [C.c_int32, C.POINTER(tl_mesh_desc), C.c_int32] + [C.c_void_p] * 5 +
+                        [C.POINTER(tl_settings), C.c_void_p, C.c_double, C.POINTER(tl_step_report)]),
 }
 
 _lib = None

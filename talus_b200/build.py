@@ -6,7 +6,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SOURCES = [os.path.join(HERE, "csrc", "tl_system.cu")]
+SOURCES = [os.path.join(HERE, "csrc", "tl_system.cu"), os.path.join(HERE, "csrc", "tl_noalloc.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("tl_kernels.cuh", "tl_math.cuh")] + [
     os.path.join(os.path.dirname(HERE), "include", "talus_fem.h")]
 OUTPUT = os.path.join(HERE, "libtalus_fem.so")

@@ -764,7 +764,7 @@ __global__ void __launch_bounds__(TILE) kNodeAssemble(Sys<S> s, const Vec4<S>* t
 
 // Sum the per-tile partials of each body (one block per body) in tile order.
 // which: 0 = elastic energy (element tiles), 1 = right^2, 2 = kinetic (node tiles).
-__global__ void __launch_bounds__(TILE) kFinalize(const BodyDev* body, const double* epart, const double* npart,
+static __global__ void __launch_bounds__(TILE) kFinalize(const BodyDev* body, const double* epart, const double* npart,
                                                   BodyAccDev* acc, uint32_t which) {
   const uint32_t b = blockIdx.x;
   const uint32_t t0 = which == 0 ? body[b].elem_tile_begin : body[b].node_tile_begin;

@@ -1118,6 +1118,7 @@ const char* tl_status_string(int32_t status) {
     case TL_ERR_TIMEOUT: return "device wait timed out";
     case TL_ERR_UNSUPPORTED: return "unsupported";
     case TL_ERR_NO_DEVICE: return "no CUDA device";
+    case TL_ERR_TOO_LARGE: return "input exceeds the fixed capacity of tl_step_noalloc";
     default: return "unknown status";
   }
 }
