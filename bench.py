@@ -3,15 +3,17 @@
 Workload (N=1), WORKLOADS["plastic-block"]: a 64x32x32-cube block (393,216
 tets, 70,785 nodes, 0.1 m cubes) of E=2e7 Pa, nu=0.35, rho=1000, yield 1e5 Pa,
 linear hardening 2e5 Pa, bottom face pinned, top face pushed down at 0.5 m/s,
-gravity 9.81, dt=1/60, FP32-mixed.  A step is one deformable::step (dt) of the full hot
-path: element pass, CSR gather assembly, PCG, plastic Newton control.  Inputs
-are synthetic (seeded generator of the reference's buildMesh layout).
+gravity 9.81, dt=1/60, FP32-mixed.  A step is one deformable::step (dt) of the
+full hot path: element pass, CSR gather assembly, PCG, plastic Newton control.
+Other workloads: "elastic-block" (8x8x8 neo-Hookean block) and "batch" (512
+uneven bodies in one system, one graph-captured launch sequence per step).
+Inputs are synthetic (seeded generator of the reference's buildMesh layout).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                        [--precision mixed|fp64] [--workload NAME]
-Under torchrun (N>1) every rank steps its own replica of the block (the path
-does not shard within one body; bodies are independent), no collective on
-the data path; time = max over ranks.
+Under torchrun (N>1) every rank steps its own replica of the workload (the
+path does not shard within one body; bodies are independent), no collective
+on the data path; time = max over ranks.
 """
 from __future__ import annotations
 
@@ -31,35 +33,24 @@ sys.path.insert(0, ROOT)
 METRIC = "elem-steps/s FP32-mixed vs FP64 GPU @rel-err<=1e-5; adjoint/forward time ratio"
 UNIT = "element-steps/s"
 
-WORKLOADS = {
-    # BASELINE configs[1]
-    "plastic-block": dict(cells=(64, 32, 32), youngs=2e7, poisson=0.35, yield_stress=1e5, hardening=2e5,
-                          push=0.5, jitter=0.0, law="corotated"),
-    # BASELINE configs[0]
-    "elastic-block": dict(cells=(8, 8, 8), youngs=1e6, poisson=0.3, yield_stress=float("inf"), hardening=0.0,
-                          push=0.0, jitter=0.01, law="snh"),
-}
+from talus_b200.workloads import WORKLOADS, make_bodies, make_mesh  # noqa: E402
 
 
-def make_mesh(spec, scale_cells=None):
-    import talus_b200 as tb
-
-    cells = scale_cells or spec["cells"]
-    mesh = tb.box_mesh(cells, voxel=0.1, jitter=spec["jitter"], seed=2)
-    if spec["push"]:
-        top = mesh.face(1, 1)
-        mesh.anchored[top] = 1
-        mesh.prescribed_velocity = np.zeros((mesh.nodes, 3))
-        # same strain rate as the full block when the sample is shorter
-        mesh.prescribed_velocity[top, 1] = -spec["push"] * cells[1] / spec["cells"][1]
-    mat = tb.PhysicalMaterial(density=1000.0, youngs_modulus=spec["youngs"], poissons_ratio=spec["poisson"],
-                              yield_stress=spec["yield_stress"], hardening_modulus=spec["hardening"])
-    return mesh, mat
-
-
-def sample_cells(spec):
-    """Bounded CPU sample of a workload: 1/64 of the cells (1/4 per axis)."""
-    return tuple(max(2, c // 4) for c in spec["cells"])
+def sample_bodies(spec, budget_tets=8000):
+    """Bounded CPU sample of a workload: a 1/64 sub-block (1/4 cells per axis,
+    same strain rate) of a single body; the first bodies of a batch up to
+    `budget_tets` tets."""
+    if spec.get("batch"):
+        meshes, mats = make_bodies(spec)
+        take, total = 0, 0
+        while take < len(meshes) and total + meshes[take].tets <= budget_tets or take == 0:
+            total += meshes[take].tets
+            take += 1
+        return meshes[:take], mats[:take], f"the first {take} bodies of the batch ({total} tets)"
+    cells = tuple(max(2, c // 4) for c in spec["cells"])
+    mesh, mat = make_mesh(spec, cells)
+    return [mesh], [[mat]], (f"{cells[0]}x{cells[1]}x{cells[2]} cells ({mesh.tets} tets, 1/64 of the workload, "
+                             f"same strain rate)")
 
 
 # ----------------------------------------------------------------- clocks --
@@ -128,8 +119,8 @@ def tile_slots(mesh, tile=256):
 
 
 def pcg_bytes_per_iteration(T, V, slots, s_bytes, tangent):
-    """Unique bytes one iteration of the single-body PCG (tl::kPcg1, phases A,
-    B, C) must move, per the layout in talus_b200/csrc/tl_kernels.cuh:
+    """Unique bytes one PCG iteration (tl::kPcg1 / kPcgBatch, phases A, B, C)
+    must move for one body, per the layout in talus_b200/csrc/tl_kernels.cuh:
     every array read or written once per phase.  s = 4 (FP32) or 8 (FP64)."""
     v4 = 4 * s_bytes
     # A, per element: tet 16, rotated gradients 9 s, coefficients v4, [flow normal 2 v4],
@@ -151,30 +142,15 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def tuning(workload, precision):
+    path = os.path.join(ROOT, "talus_b200", "tuning.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f).get(f"{workload}/{precision}")
+
+
 # --------------------------------------------------------------- CPU side --
-
-def cpu_sample(spec, steps_budget_s=15.0, max_steps=400):
-    """The oracle (the reference's algorithm restated, FP32 like the reference)
-    on a bounded sample of the workload, single-threaded like the reference
-    step (Settings::stepThreads is never read, solver.h:73-74)."""
-    from oracle import pyoracle as po
-    from tests.helpers import oracle_material, to_oracle
-
-    cells = sample_cells(spec)
-    mesh, mat = make_mesh(spec, cells)
-    om = to_oracle(mesh)
-    state = po.State.rest(om)
-    settings = po.Settings(law=po.LAW_SNH if spec["law"] == "snh" else po.LAW_COROTATED)
-    steps, t0 = 0, time.perf_counter()
-    while steps < max_steps and time.perf_counter() - t0 < steps_budget_s:
-        po.step(po.F32, om, state, [oracle_material(mat)], settings, (0.0, -9.81, 0.0), 1.0 / 60.0)
-        steps += 1
-    secs = time.perf_counter() - t0
-    return {"value": mesh.tets * steps / secs, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"oracle FP32 (reference arithmetic), {cells[0]}x{cells[1]}x{cells[2]} cells "
-                      f"({mesh.tets} tets, 1/64 of the workload, same strain rate), {steps} steps from rest, "
-                      f"1 thread, {secs:.1f} s"}
-
 
 def cpu_info():
     model = ""
@@ -189,33 +165,59 @@ def cpu_info():
     return model
 
 
+class OracleRun:
+    """The oracle (the reference's algorithm restated, FP32 like the
+    reference), single-threaded like the reference step
+    (Settings::stepThreads is never read, solver.h:73-74)."""
+
+    def __init__(self, spec):
+        from oracle import pyoracle as po
+        from tests.helpers import oracle_material, to_oracle
+
+        self.po = po
+        meshes, mats, self.sample = sample_bodies(spec)
+        self.bodies = []
+        for m, mat in zip(meshes, mats):
+            om = to_oracle(m)
+            self.bodies.append((om, po.State.rest(om), [oracle_material(x) for x in mat]))
+        self.tets = sum(m.tets for m in meshes)
+        self.settings = po.Settings(law=po.LAW_SNH if spec["law"] == "snh" else po.LAW_COROTATED)
+
+    def step(self):
+        for om, state, mats in self.bodies:
+            self.po.step(self.po.F32, om, state, mats, self.settings, (0.0, -9.81, 0.0), 1.0 / 60.0)
+
+
+def cpu_sample(spec, budget_s=15.0, max_steps=400):
+    run = OracleRun(spec)
+    steps, t0 = 0, time.perf_counter()
+    while steps < max_steps and time.perf_counter() - t0 < budget_s:
+        run.step()
+        steps += 1
+    secs = time.perf_counter() - t0
+    return {"value": run.tets * steps / secs, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"oracle FP32 (reference arithmetic), {run.sample}, {steps} steps from rest, 1 thread, "
+                      f"{secs:.1f} s"}
+
+
 def run_reference(args, spec, rank, world):
     if rank != 0:
         return
-    from oracle import pyoracle as po
-    from tests.helpers import oracle_material, to_oracle
-
-    cells = sample_cells(spec)
-    mesh, mat = make_mesh(spec, cells)
-    om = to_oracle(mesh)
-    state = po.State.rest(om)
-    settings = po.Settings(law=po.LAW_SNH if spec["law"] == "snh" else po.LAW_COROTATED)
-    mats = [oracle_material(mat)]
+    run = OracleRun(spec)
     for _ in range(args.warmup):
-        po.step(po.F32, om, state, mats, settings, (0.0, -9.81, 0.0), 1.0 / 60.0)
+        run.step()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        po.step(po.F32, om, state, mats, settings, (0.0, -9.81, 0.0), 1.0 / 60.0)
+        run.step()
     secs = time.perf_counter() - t0
-    value = mesh.tets * args.steps / secs
+    value = run.tets * args.steps / secs
     sample = (f"oracle FP32 restatement of deformable::step (the reference cannot be built here: GLM/Eigen "
-              f"fetched at configure time), {cells[0]}x{cells[1]}x{cells[2]} cells ({mesh.tets} tets, 1/64 of "
-              f"{args.workload}, same strain rate), 1 thread ({cpu_info()})")
+              f"fetched at configure time), {run.sample} of {args.workload}, 1 thread ({cpu_info()})")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.workload, "cells": list(cells), "tets": mesh.tets, "nodes": mesh.nodes},
+        "config": {"workload": args.workload, "tets": run.tets, "sample": run.sample},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -224,6 +226,8 @@ def run_reference(args, spec, rank, world):
 # --------------------------------------------------------------- GPU side --
 
 def run_ours(args, spec, rank, world, dist):
+    import ctypes as C
+
     import torch
 
     import talus_b200 as tb
@@ -232,12 +236,19 @@ def run_ours(args, spec, rank, world, dist):
     device = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(device)
     precision = tb.FP32_MIXED if args.precision == "mixed" else tb.FP64
-    mesh, mat = make_mesh(spec)
+    meshes, mats = make_bodies(spec)
+    B = len(meshes)
+    T = sum(m.tets for m in meshes)
+    V = sum(m.nodes for m in meshes)
     law = tb.NEO_HOOKEAN if spec["law"] == "snh" else tb.COROTATED
     settings = tb.Settings(law=law, profile=True)
     context = tb.Context(device)
-    system = tb.System(mesh, [mat], precision, context)
-    system.set_state(tb.rest_state(mesh))
+    system = tb.System(meshes, mats, precision, context)
+    tune = tuning(args.workload, args.precision)
+    if tune:
+        system.tune(tune["pcg_blocks_per_sm"], tune["graph"])
+    for i, m in enumerate(meshes):
+        system.set_state(tb.rest_state(m), i)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")  # > 126 MB L2
     for _ in range(args.warmup):
         system.step(settings)
@@ -248,65 +259,80 @@ def run_ours(args, spec, rank, world, dist):
             dist.barrier()
         torch.cuda.synchronize()
 
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     # ---- device-resident timing: per-step events inside the library, L2 flushed between steps
     barrier()
-    totals = capi.tl_step_report()
-    step_seconds = []
+    step_seconds, launches = [], 0
+    per_body = np.zeros((B, 4))  # cg iterations, tangent iterations, solves, plastic evaluations
+    totals = {"element": 0.0, "assemble": 0.0, "pcg": 0.0}
     with ClockSampler(device) as clocks:
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
-            rep = system.step(settings)[0]
-            step_seconds.append(rep.device_seconds)
-            for name, _ in rep._fields_:
-                if name in ("cg_worst_relative_residual", "plastic_worst_residual", "min_volume_ratio"):
-                    continue
-                setattr(totals, name, getattr(totals, name) + getattr(rep, name))
+            reps = system.step(settings)
+            step_seconds.append(reps[0].device_seconds)
+            launches += reps[0].kernel_launches
+            totals["element"] += reps[0].element_seconds
+            totals["assemble"] += reps[0].assemble_seconds
+            totals["pcg"] += reps[0].pcg_seconds
+            for b in range(B):
+                per_body[b] += (reps[b].cg_iterations, reps[b].cg_tangent_iterations, reps[b].cg_solves,
+                                reps[b].plastic_evaluations)
         barrier()
-    local = sum(step_seconds)
-    if dist is not None:
-        t = torch.tensor([local], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        local = float(t.item())
-    total_seconds = local
-    value = world * mesh.tets * args.steps / total_seconds
+    total_seconds = max_over_ranks(sum(step_seconds))
+    value = world * T * args.steps / total_seconds
 
-    # ---- end to end through the public host-state API (state in host memory every step)
-    state = system.get_state()
-    f32 = {k: np.ascontiguousarray(getattr(state, k), np.float32) for k in
-           ("position", "velocity", "acceleration", "rotation", "plastic")}
-    h2d = sum(a.nbytes for a in f32.values())
+    # ---- end to end through the public API: the state crosses the host boundary every step
+    f32 = []
+    for i in range(B):
+        st = system.get_state(i)
+        f32.append({k: np.ascontiguousarray(getattr(st, k), np.float32) for k in
+                    ("position", "velocity", "acceleration", "rotation", "plastic")})
+    h2d = sum(a.nbytes for d in f32 for a in d.values())
     lib = capi.lib()
     s_c = settings._c()
     g = np.asarray((0.0, -9.81, 0.0))
-    rep_e2e = capi.tl_step_report()
     e2e_steps = max(3, min(args.steps, 10))
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        st = lib.tl_step_host(system.handle, 0, capi.TL_DTYPE_F32, f32["position"].ctypes.data,
-                              f32["velocity"].ctypes.data, f32["acceleration"].ctypes.data,
-                              f32["rotation"].ctypes.data, f32["plastic"].ctypes.data, s_c, g.ctypes.data,
-                              1.0 / 60.0, rep_e2e)
+        if B == 1:
+            d = f32[0]
+            st = lib.tl_step_host(system.handle, 0, capi.TL_DTYPE_F32, d["position"].ctypes.data,
+                                  d["velocity"].ctypes.data, d["acceleration"].ctypes.data,
+                                  d["rotation"].ctypes.data, d["plastic"].ctypes.data, s_c, g.ctypes.data,
+                                  1.0 / 60.0, capi.tl_step_report())
+        else:
+            for i, d in enumerate(f32):
+                capi.check(lib.tl_state_set(system.handle, i, capi.TL_DTYPE_F32, *[d[k].ctypes.data for k in
+                           ("position", "velocity", "acceleration", "rotation", "plastic")]), context.handle)
+            reps = (capi.tl_step_report * B)()
+            st = lib.tl_step(system.handle, s_c, g.ctypes.data, 1.0 / 60.0, reps)
+            for i, d in enumerate(f32):
+                capi.check(lib.tl_state_get(system.handle, i, capi.TL_DTYPE_F32, *[d[k].ctypes.data for k in
+                           ("position", "velocity", "acceleration", "rotation", "plastic")]), context.handle)
         if st not in (capi.TL_OK, capi.TL_ERR_NONFINITE):
             capi.check(st, context.handle)
     barrier()
-    e2e_seconds = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_seconds], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_seconds = float(t.item())
-    e2e_value = world * mesh.tets * e2e_steps / e2e_seconds
+    e2e_seconds = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = world * T * e2e_steps / e2e_seconds
 
-    # ---- roofline of the dominant kernel (persistent PCG)
+    # ---- roofline of the dominant kernel (persistent PCG): algorithmic bytes of every iteration run
     s_bytes = 4 if precision == tb.FP32_MIXED else 8
-    iters = totals.cg_iterations
-    tangent_iters = totals.cg_tangent_iterations
-    slots = tile_slots(mesh)
-    per_iter = {t: pcg_bytes_per_iteration(mesh.tets, mesh.nodes, slots, s_bytes, t) for t in (False, True)}
-    pcg_bytes = per_iter[True] * tangent_iters + per_iter[False] * (iters - tangent_iters)
-    launches_pcg = totals.cg_solves
-    pcg_time = totals.pcg_seconds
+    pcg_bytes = 0.0
+    for b, m in enumerate(meshes):
+        slots = tile_slots(m)
+        it, tan = per_body[b, 0], per_body[b, 1]
+        pcg_bytes += (pcg_bytes_per_iteration(m.tets, m.nodes, slots, s_bytes, True) * tan +
+                      pcg_bytes_per_iteration(m.tets, m.nodes, slots, s_bytes, False) * (it - tan))
+    launches_pcg = int(per_body[:, 2].max())
+    pcg_time = totals["pcg"]
     peak, peak_kind = peaks()
     achieved = pcg_bytes / pcg_time / 1e9 if pcg_time > 0 else 0.0
     traffic = None
@@ -315,32 +341,36 @@ def run_ours(args, spec, rank, world, dist):
         with open(tpath) as f:
             tr = json.load(f)
         if tr.get("workload") == args.workload and tr.get("precision") == args.precision and launches_pcg:
-            # bytes per PCG iteration from one ncu capture, scaled to this run's average launch
-            traffic = tr["dram_bytes_per_iteration"] * iters / launches_pcg
+            traffic = tr["dram_bytes_per_iteration"] * per_body[:, 0].sum() / launches_pcg
 
+    kernel = ("tl::kPcg1 (persistent block-Jacobi PCG, two-level assembly)" if B == 1 else
+              "tl::kPcgBatch (persistent block-Jacobi PCG over all bodies, two-level assembly)")
+    config = {"workload": args.workload, "bodies": B, "tets": T, "nodes": V, "law": spec["law"],
+              "precision": args.precision, "dt": 1.0 / 60.0,
+              "parallelism": f"replicas{world}" if world > 1 else "single-gpu",
+              "l2": "flushed (256 MB write) between timed steps; working set > 126 MB"}
+    if not spec.get("batch"):
+        config["cells"] = list(spec["cells"])
+    if tune:
+        config["tuning"] = tune
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_seconds * 1e3 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32-mixed" if precision == tb.FP32_MIXED else "f64",
-        "data": "synthetic (seeded Kuhn grid in the reference buildMesh layout)",
-        "config": {"workload": args.workload, "cells": list(spec["cells"]), "tets": mesh.tets, "nodes": mesh.nodes,
-                   "law": spec["law"], "precision": args.precision, "dt": 1.0 / 60.0,
-                   "parallelism": f"replicas{world}" if world > 1 else "single-gpu",
-                   "l2": "flushed (256 MB write) between timed steps; working set > 126 MB"},
+        "data": "synthetic (seeded Kuhn grids in the reference buildMesh layout)",
+        "config": config,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": h2d,
-                "steps": e2e_steps, "api": "tl_step_host (state in host memory, f32)"},
-        "gpu_launches": int(totals.kernel_launches),
-        "roofline": {"bound": "hbm", "kernel": "tl::kPcg1 (persistent block-Jacobi PCG, two-level assembly)",
-                     "achieved": achieved,
-                     "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": traffic, "launches": launches_pcg, "iterations": iters,
+                "steps": e2e_steps,
+                "api": "tl_step_host (state in host memory, f32)" if B == 1 else "tl_state_set + tl_step + tl_state_get"},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": kernel, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic, "launches": launches_pcg,
+                     "iterations": int(per_body[:, 0].max()),
                      "algorithmic_bytes_per_launch": pcg_bytes / max(1, launches_pcg),
                      "avg_launch_ms": pcg_time * 1e3 / max(1, launches_pcg)},
-        "breakdown_ms_per_step": {"pcg": pcg_time * 1e3 / args.steps,
-                                  "element": totals.element_seconds * 1e3 / args.steps,
-                                  "assemble": totals.assemble_seconds * 1e3 / args.steps},
-        "solver": {"cg_iterations_per_step": iters / args.steps,
-                   "plastic_evaluations_per_step": totals.plastic_evaluations / args.steps},
+        "breakdown_ms_per_step": {k: v * 1e3 / args.steps for k, v in totals.items()},
+        "solver": {"cg_iterations_per_step": float(per_body[:, 0].sum() / args.steps),
+                   "plastic_evaluations_per_step": float(per_body[:, 3].sum() / args.steps)},
         "clocks": clocks.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

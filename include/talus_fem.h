@@ -154,6 +154,12 @@ int32_t tl_system_create(tl_ctx* ctx, const tl_mesh_desc* bodies, uint32_t count
 int32_t tl_system_destroy(tl_system* system);
 int32_t tl_system_counts(const tl_system* system, uint32_t* bodies, uint64_t* nodes, uint64_t* tets);
 
+/* Launch shape, no reference counterpart (chosen by talus_b200/autotune.py):
+ * pcg_blocks_per_sm caps the blocks per SM of the persistent PCG grid (0 =
+ * as many as can be resident); graph != 0 lets a batched system (count > 1)
+ * capture its elastic step in a CUDA graph and replay it every step. */
+int32_t tl_system_tune(tl_system* system, uint32_t pcg_blocks_per_sm, uint32_t graph);
+
 /* Diagnostics, no reference counterpart: iteration counts (body 0) of the
  * PCG launches made while TL_FLAG_TRACE was set, oldest first, since the
  * system was created.  Writes min(capacity, recorded) entries; *count gets

@@ -1,0 +1,93 @@
+"""Launch-shape autotuner of the step.
+
+For one workload it times every candidate launch shape on the device and
+records the fastest in a JSON table that ``bench.py`` and users read back
+through ``System.tune``:
+
+* ``pcg_blocks_per_sm``: how many 256-thread blocks of the persistent PCG
+  kernel share an SM (0 = as many as occupancy allows).  Fewer blocks make
+  the grid barriers cheaper; more blocks hide more load latency in the
+  element-tile matvec.
+* ``graph``: whether a batched elastic step is replayed from one captured CUDA
+  graph (device-side substep choice) or launched kernel by kernel.
+
+Every candidate starts from the same rest state and runs the same steps, so
+the candidates do the same physics; the score is device seconds per step.
+
+    python -m talus_b200.autotune --workload batch --precision mixed --out talus_b200/tuning.json
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def candidates(bodies: int):
+    shapes = [0, 1, 2, 3]
+    graphs = [True, False] if bodies > 1 else [False]
+    return [(k, g) for k in shapes for g in graphs]
+
+
+def time_candidate(system, meshes, settings, blocks, graph, warmup, steps):
+    import talus_b200 as tb
+
+    system.tune(blocks, graph)
+    for i, m in enumerate(meshes):
+        system.set_state(tb.rest_state(m), i)
+    for _ in range(warmup):
+        system.step(settings)
+    seconds, iterations = 0.0, 0
+    for _ in range(steps):
+        reps = system.step(settings)
+        seconds += reps[0].device_seconds
+        iterations += sum(r.cg_iterations for r in reps)
+    return seconds / steps, iterations / steps
+
+
+def tune(workload: str, precision_name: str, warmup: int = 2, steps: int = 4) -> dict:
+    sys.path.insert(0, ROOT)
+    import talus_b200 as tb
+    from talus_b200.workloads import WORKLOADS, make_bodies
+
+    spec = WORKLOADS[workload]
+    meshes, mats = make_bodies(spec)
+    precision = tb.FP32_MIXED if precision_name == "mixed" else tb.FP64
+    law = tb.NEO_HOOKEAN if spec["law"] == "snh" else tb.COROTATED
+    settings = tb.Settings(law=law)
+    system = tb.System(meshes, mats, precision)
+    results = []
+    for blocks, graph in candidates(len(meshes)):
+        sec, its = time_candidate(system, meshes, settings, blocks, graph, warmup, steps)
+        results.append({"pcg_blocks_per_sm": blocks, "graph": graph, "ms_per_step": sec * 1e3,
+                        "cg_iterations_per_step": its})
+        print(json.dumps(results[-1]), file=sys.stderr, flush=True)
+    system.close()
+    best = min(results, key=lambda r: r["ms_per_step"])
+    return {"pcg_blocks_per_sm": best["pcg_blocks_per_sm"], "graph": best["graph"],
+            "ms_per_step": best["ms_per_step"], "steps": steps, "candidates": results}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="batch")
+    ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--out", default=os.path.join(ROOT, "talus_b200", "tuning.json"))
+    args = ap.parse_args()
+    entry = tune(args.workload, args.precision, steps=args.steps)
+    table = {}
+    if os.path.exists(args.out):
+        with open(args.out) as f:
+            table = json.load(f)
+    table[f"{args.workload}/{args.precision}"] = entry
+    with open(args.out, "w") as f:
+        json.dump(table, f, indent=1, sort_keys=True)
+    print(json.dumps({k: v for k, v in entry.items() if k != "candidates"}))
+
+
+if __name__ == "__main__":
+    main()

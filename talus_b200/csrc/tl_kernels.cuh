@@ -1154,14 +1154,14 @@ __device__ __forceinline__ double sumBlocks(const double* part, unsigned int fie
 // local index, and the tile's local CSR is fetched while the elements compute.
 template <class S, int LAW, bool TANGENT>
 __device__ __forceinline__ void matvecTile(const Sys<S>& s, uint32_t tile, const Vec4<S>* X, S blend,
-                                           S (*buf)[4 * TILE], uint16_t* sOff, uint16_t* sEnt) {
+                                           S (*buf)[4 * TILE], uint16_t* sOff, uint16_t* sEnt, uint32_t elemEnd) {
   const uint32_t e = tile * TILE + threadIdx.x;
   const uint2 meta = __ldg(&s.tile_meta[tile]);
   const uint2 entv = __ldg(reinterpret_cast<const uint2*>(s.tile_ent + size_t(tile) * 4 * TILE) + threadIdx.x);
   const uint16_t* off = s.tile_off + size_t(tile) * TILE_OFF_STRIDE;
   const uint2 offv = __ldg(reinterpret_cast<const uint2*>(off) + threadIdx.x);
   const uint16_t offLast = threadIdx.x == 0 ? __ldg(&off[4 * TILE]) : uint16_t(0);
-  const bool live = e < s.body[0].elem_end;
+  const bool live = e < elemEnd;
   const uint2 loc = live ? __ldg(&s.eloc[e]) : make_uint2(0u, 0u);
   // stage the tile's nodes: buf[k][j] = component k of node j
   for (uint32_t j = threadIdx.x; j < meta.y; j += TILE) {
@@ -1247,7 +1247,7 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, 
   double* part = s.blk_part;
   // ---- init: r = right - A x (anchored rows 0), z = P r, p_prev = 0
   if (!x0zero) {
-    for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G) matvecTile<S, LAW, TANGENT>(s, tile, X, zero, buf, sOff, sEnt);
+    for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G) matvecTile<S, LAW, TANGENT>(s, tile, X, zero, buf, sOff, sEnt, bd.elem_end);
     if (!countBarrier(s.sync, bar)) return;
   }
   {
@@ -1295,7 +1295,7 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, 
     if (taken >= st.limit || sqrt(length) <= target) break;
     // ---- A
     for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G)
-      matvecTile<S, LAW, TANGENT>(s, tile, nullptr, S(blend), buf, sOff, sEnt);
+      matvecTile<S, LAW, TANGENT>(s, tile, nullptr, S(blend), buf, sOff, sEnt, bd.elem_end);
     if (!countBarrier(s.sync, bar)) return;
     // ---- B
     double pap = 0.0;
@@ -1374,6 +1374,218 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, 
     rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
     s.cgrep[0] = rep;
   }
+}
+
+// Persistent PCG for a system of MANY bodies (the batched form): the phases of
+// kPcg1 with the two-level assembly, but every body keeps its own scalars
+// (CgBodyDev) and stops on its own test.  Per-tile partials are summed over a
+// body's tiles, in tile order, by the block that finishes the body's last tile
+// (lastTileOfBody); the launch ends when no body iterates.  Bodies that are
+// done skip their tiles, so a batch costs the sum of its bodies' iterations,
+// not bodies x the slowest body.
+template <class S, int LAW, bool TANGENT>
+__global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2)
+    kPcgBatch(Sys<S> s, Vec4<S>* X, uint32_t pass, uint32_t x0zero) {
+  __shared__ S buf[3][4 * TILE];
+  __shared__ __align__(8) uint16_t sOff[TILE_OFF_STRIDE];
+  __shared__ __align__(8) uint16_t sEnt[4 * TILE];
+  const uint32_t G = gridDim.x;
+  const S zero = S(0);
+  // ---- init: r = right - A x (anchored rows 0), z = P r, p_prev = 0
+  if (!x0zero) {
+    for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G) {
+      const uint32_t b = s.elem_tile_body[tile];
+      if (!bodyActive(s, b, pass)) continue;
+      matvecTile<S, LAW, TANGENT>(s, tile, X, zero, buf, sOff, sEnt, s.body[b].elem_end);
+    }
+    if (!gridBarrier(s.sync)) return;
+  }
+  for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
+    const uint32_t b = s.node_tile_body[tile];
+    if (!bodyActive(s, b, pass)) continue;
+    const BodyDev bd = s.body[b];
+    const uint32_t n = tile * TILE + threadIdx.x;
+    double sums[3] = {0.0, 0.0, 0.0};
+    if (n < bd.node_end) {
+      const Vec4<S> rhs = s.right[n];
+      V3<S> r = {zero, zero, zero};
+      if (!s.anch[n]) {
+        V3<double> ax = {0, 0, 0};
+        if (!x0zero)
+          ax = (s.step[b].inertia * double(ld4g(&s.rest4[n]).w)) * cvt<double>(xyz(ld4cg(&X[n]))) + gatherSlots(s, n);
+        r = cvt<S>(cvt<double>(xyz(rhs)) - ax);
+      }
+      const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
+      const Sym<S> P = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
+      const V3<S> z = symMul(P, r);
+      s.r[n] = pack(r);
+      s.z[n] = pack(z);
+      s.p[n] = Vec4<S>{zero, zero, zero, zero};
+      if (x0zero) X[n] = Vec4<S>{zero, zero, zero, zero};
+      sums[0] = dot(cvt<double>(r), cvt<double>(z));
+      sums[1] = dot(cvt<double>(r), cvt<double>(r));
+      sums[2] = dot(cvt<double>(xyz(rhs)), cvt<double>(xyz(rhs)));
+    }
+    blockSum<3>(sums);
+    if (threadIdx.x == 0) {
+      s.part[size_t(tile) * 4 + 0] = sums[0];
+      s.part[size_t(tile) * 4 + 1] = sums[1];
+      s.part[size_t(tile) * 4 + 2] = sums[2];
+    }
+    if (lastTileOfBody(&s.counter[b], bd.node_tile_end - bd.node_tile_begin)) {
+      double tot[3];
+      sumTiles<3>(s.part, bd.node_tile_begin, bd.node_tile_end, tot);
+      if (threadIdx.x == 0) {
+        CgBodyDev c;
+        const double reference = sqrt(tot[2]);
+        c.floor = fmax(reference, 1.1754943508222875e-38);  // std::numeric_limits<float>::min()
+        c.target = s.step[b].tolerance * c.floor;
+        c.squared = tot[0];
+        c.length = tot[1];
+        c.start_res = sqrt(tot[1]) / c.floor;
+        c.rel_res = c.start_res;
+        c.blend = 0.0;
+        c.stride = 0.0;
+        c.taken = 0;
+        c.done = (s.step[b].limit == 0u || sqrt(c.length) <= c.target) ? 1u : 0u;
+        c.pad0 = c.pad1 = 0;
+        s.cg[b] = c;
+        __threadfence();
+        if (c.done) atomicSub(&s.sync->active, 1);
+      }
+    }
+  }
+  if (!gridBarrier(s.sync)) return;
+  for (;;) {
+    if (*(volatile int*)&s.sync->active <= 0) break;  // uniform: no block decrements between here and barrier A
+    // ---- A
+    for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G) {
+      const uint32_t b = s.elem_tile_body[tile];
+      if (!bodyActive(s, b, pass) || __ldcg(&s.cg[b].done)) continue;
+      matvecTile<S, LAW, TANGENT>(s, tile, nullptr, S(__ldcg(&s.cg[b].blend)), buf, sOff, sEnt, s.body[b].elem_end);
+    }
+    if (!gridBarrier(s.sync)) return;
+    // ---- B
+    for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
+      const uint32_t b = s.node_tile_body[tile];
+      if (!bodyActive(s, b, pass) || __ldcg(&s.cg[b].done)) continue;
+      const BodyDev bd = s.body[b];
+      const uint32_t n = tile * TILE + threadIdx.x;
+      double sums[1] = {0.0};
+      if (n < bd.node_end) {
+        const S blend = S(__ldcg(&s.cg[b].blend));
+        const V3<S> pn = fmaV(blend, xyz(ld4cg(&s.p[n])), xyz(ld4cg(&s.z[n])));
+        s.p[n] = pack(pn);
+        V3<S> apn = {zero, zero, zero};
+        if (!s.anch[n]) apn = cvt<S>((s.step[b].inertia * double(ld4g(&s.rest4[n]).w)) * cvt<double>(pn) + gatherSlots(s, n));
+        s.ap[n] = pack(apn);
+        sums[0] = dot(cvt<double>(pn), cvt<double>(apn));
+      }
+      blockSum<1>(sums);
+      if (threadIdx.x == 0) s.part[size_t(tile) * 4 + 3] = sums[0];
+      if (lastTileOfBody(&s.counter[b], bd.node_tile_end - bd.node_tile_begin)) {
+        double tot[1];
+        sumTiles<1>(s.part + 3, bd.node_tile_begin, bd.node_tile_end, tot);
+        if (threadIdx.x == 0) {
+          const double curvature = tot[0];
+          const double squared = __ldcg(&s.cg[b].squared);
+          if (!(curvature > 0.0) || !(squared > 0.0)) {
+            s.cg[b].done = 1u;
+            __threadfence();
+            atomicSub(&s.sync->active, 1);
+          } else {
+            s.cg[b].stride = squared / curvature;
+            __threadfence();
+          }
+        }
+      }
+    }
+    if (!gridBarrier(s.sync)) return;
+    // ---- C
+    for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
+      const uint32_t b = s.node_tile_body[tile];
+      if (!bodyActive(s, b, pass) || __ldcg(&s.cg[b].done)) continue;
+      const BodyDev bd = s.body[b];
+      const uint32_t n = tile * TILE + threadIdx.x;
+      double sums[2] = {0.0, 0.0};
+      if (n < bd.node_end) {
+        const S stride = S(__ldcg(&s.cg[b].stride));
+        const V3<S> pn = xyz(ld4cg(&s.p[n]));
+        const V3<S> x = fmaV(stride, pn, xyz(ld4cg(&X[n])));
+        const V3<S> r = fmaV(-stride, xyz(ld4cg(&s.ap[n])), xyz(ld4cg(&s.r[n])));
+        const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
+        const Sym<S> P = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
+        const V3<S> z = symMul(P, r);
+        X[n] = pack(x);
+        s.r[n] = pack(r);
+        s.z[n] = pack(z);
+        sums[0] = dot(cvt<double>(r), cvt<double>(z));
+        sums[1] = dot(cvt<double>(r), cvt<double>(r));
+      }
+      blockSum<2>(sums);
+      if (threadIdx.x == 0) {
+        s.part[size_t(tile) * 4 + 0] = sums[0];
+        s.part[size_t(tile) * 4 + 1] = sums[1];
+      }
+      if (lastTileOfBody(&s.counter[b], bd.node_tile_end - bd.node_tile_begin)) {
+        double tot[2];
+        sumTiles<2>(s.part, bd.node_tile_begin, bd.node_tile_end, tot);
+        if (threadIdx.x == 0) {
+          CgBodyDev c = loadCg(&s.cg[b]);
+          c.blend = tot[0] / c.squared;
+          c.squared = tot[0];
+          c.length = tot[1];
+          c.taken += 1u;
+          c.done = (sqrt(c.length) <= c.target || c.taken >= s.step[b].limit) ? 1u : 0u;
+          s.cg[b] = c;
+          __threadfence();
+          if (c.done) atomicSub(&s.sync->active, 1);
+        }
+      }
+    }
+    if (!gridBarrier(s.sync)) return;
+  }
+  if (blockIdx.x == 0) {
+    for (uint32_t b = threadIdx.x; b < s.bodies; b += TILE) {
+      if (!bodyActive(s, b, pass)) continue;
+      CgBodyDev c = loadCg(&s.cg[b]);
+      const double residual = sqrt(c.length);
+      c.rel_res = residual / c.floor;
+      s.cg[b].rel_res = c.rel_res;
+      CgReportDev rep = s.cgrep[b];
+      rep.iterations += c.taken;
+      rep.capped += (c.taken == s.step[b].limit && residual > c.target) ? 1u : 0u;
+      rep.applications += c.taken + (x0zero ? 0u : 1u);
+      rep.solves += 1u;
+      rep.tangent_iterations += TANGENT ? c.taken : 0u;
+      rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
+      s.cgrep[b] = rep;
+    }
+  }
+}
+
+// Step constants chosen on the device (graph-captured steps): variants[2 b]
+// holds body b's constants for the configured substeps, variants[2 b + 1] for
+// the inverted-predictor substeps (solver.cc:3574-3583).  mode 0 takes the
+// first (for the inversion test itself), mode 1 picks by the test's flag.
+static __global__ void kStepSelect(BodyStepDev* step, const BodyStepDev* variants, const BodyAccDev* acc,
+                                   uint32_t bodies, uint32_t mode) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= bodies) return;
+  step[b] = variants[2 * b + ((mode == 1u && acc[b].inverts) ? 1u : 0u)];
+}
+
+// Clears the per-body step accumulators (min J key to its largest value).
+static __global__ void kAccReset(BodyAccDev* acc, CgReportDev* rep, uint32_t bodies) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= bodies) return;
+  BodyAccDev z;
+  memset(&z, 0, sizeof(z));
+  z.min_j_key = ~0ull;
+  acc[b] = z;
+  CgReportDev r;
+  memset(&r, 0, sizeof(r));
+  rep[b] = r;
 }
 
 // Resets the PCG launch state: active body count, tile counters, barrier.

@@ -125,6 +125,7 @@ struct SystemBase {
                         const void* plastic) = 0;
   virtual void stateGet(uint32_t body, int32_t dtype, void* x, void* v, void* a, void* rot, void* plastic) = 0;
   virtual int32_t step(const tl_settings& set, const double g[3], double dt, tl_step_report* reports) = 0;
+  virtual void tune(uint32_t blocksPerSm, uint32_t graph) = 0;
   std::vector<uint32_t> trace;  // TL_FLAG_TRACE: iterations of each PCG launch (body 0)
   uint32_t bodies = 0;
   uint64_t nodes = 0, tets = 0;
@@ -166,7 +167,14 @@ struct System final : SystemBase {
   DevBuf<uint32_t> tileNode;
   DevBuf<uint2> eloc;
   DevBuf<double> blkPart;
-  int pcg1Grid[2][2] = {{0, 0}, {0, 0}};  // [law][tangent]
+  int pcg1PerSm[2][2] = {{0, 0}, {0, 0}};   // resident blocks per SM, [law][tangent]
+  int batchPerSm[2][2] = {{0, 0}, {0, 0}};
+  uint32_t tuneBlocksPerSm = 0;              // tl_system_tune: cap on the persistent grid (0 = occupancy)
+  bool tuneGraph = true;                     // tl_system_tune: capture batched elastic steps in a CUDA graph
+  int gridOf(int perSm) const {
+    const int use = tuneBlocksPerSm ? std::min<int>(perSm, int(tuneBlocksPerSm)) : perSm;
+    return std::max(1, std::min(use * ctx->sms, int(std::max(nodeTiles, elemTiles))));
+  }
   DevBuf<double> part, npart, epart;
   DevBuf<uint32_t> loading, yielding, counter;
   DevBuf<BodyAccDev> acc;
@@ -189,13 +197,23 @@ struct System final : SystemBase {
         evPool.emplace_back(a, b);
       }
       evUsed.emplace_back(cls, evUsed.size());
-      TL_CUDA(cudaEventRecord(evPool[evUsed.back().second].first, st));
+      record(evPool[evUsed.back().second].first);
       return evPool[evUsed.back().second].first;
     }
-    TL_CUDA(cudaEventRecord(evPool[evUsed.back().second].second, st));
+    record(evPool[evUsed.back().second].second);
     return evPool[evUsed.back().second].second;
   }
+  // Under stream capture a plain record only orders streams; the external
+  // flag makes it an event-record node that fires on every replay.
+  bool capturing = false;
+  void record(cudaEvent_t e) {
+    if (capturing)
+      TL_CUDA(cudaEventRecordWithFlags(e, st, cudaEventRecordExternal));
+    else
+      TL_CUDA(cudaEventRecord(e, st));
+  }
   ~System() override {
+    if (graphExec) cudaGraphExecDestroy(graphExec);
     for (auto& e : evPool) {
       cudaEventDestroy(e.first);
       cudaEventDestroy(e.second);
@@ -491,7 +509,7 @@ struct System final : SystemBase {
     TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kPcg<S, 1>, TILE, 0));
     pcgGrid[1] = std::max(1, std::min(perSm * ctx->sms, int(std::max(nodeTiles, elemTiles))));
     if (perSm < 1) throw StatusError{TL_ERR_CUDA, "PCG kernel cannot be resident"};
-    if (B == 1) buildTiles(hTet);
+    buildTiles(hTet, hElemTileBody);
     TL_CUDA(cudaStreamSynchronize(st));
   }
 
@@ -499,14 +517,14 @@ struct System final : SystemBase {
   // touches (its slots, ascending node) with a tile-local CSR of the
   // (local element, corner) codes in ascending element order; per node the
   // slots holding its partial sums, in ascending tile order.
-  void buildTiles(const std::vector<uint4>& hTet) {
+  void buildTiles(const std::vector<uint4>& hTet, const std::vector<uint32_t>& hElemTileBody) {
     std::vector<uint2> meta(elemTiles);
     std::vector<uint16_t> off(size_t(elemTiles) * TILE_OFF_STRIDE, 0), ent(size_t(elemTiles) * 4 * TILE, 0);
     std::vector<uint32_t> slotNode;
     std::vector<uint16_t> cornerSlot(size_t(4) * Tp, 0);
     std::vector<std::pair<uint32_t, uint32_t>> items;  // (node, code)
     for (uint32_t t = 0; t < elemTiles; ++t) {
-      const BodyDev& bd = bodyHost[0];
+      const BodyDev& bd = bodyHost[hElemTileBody[t]];
       const uint32_t e0 = t * TILE, e1 = std::min<uint32_t>(e0 + TILE, bd.elem_end);
       items.clear();
       for (uint32_t e = e0; e < e1; ++e) {
@@ -578,20 +596,25 @@ struct System final : SystemBase {
     nsSlot.alloc(std::max<size_t>(olist.size(), 1));
     nsSlot.upload(olist.data(), olist.size(), st);
     TL_CUDA(cudaStreamSynchronize(st));
-    // cooperative grid per kernel variant, bounded by the tile counts
-    auto grid = [&](const void* fn) {
-      int perSm = 0;
-      TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, TILE, 0));
-      if (perSm < 1) throw StatusError{TL_ERR_CUDA, "PCG kernel cannot be resident"};
-      return std::max(1, std::min(perSm * ctx->sms, int(std::max(nodeTiles, elemTiles))));
+    // resident blocks per SM of each cooperative kernel variant (the grid is
+    // that times the SM count, capped by tl_system_tune and the tile counts)
+    auto perSm = [&](const void* fn) {
+      int n = 0;
+      TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, TILE, 0));
+      if (n < 1) throw StatusError{TL_ERR_CUDA, "PCG kernel cannot be resident"};
+      return n;
     };
-    pcg1Grid[0][0] = grid((const void*)kPcg1<S, 0, false>);
-    pcg1Grid[0][1] = grid((const void*)kPcg1<S, 0, true>);
-    pcg1Grid[1][0] = grid((const void*)kPcg1<S, 1, false>);
-    pcg1Grid[1][1] = grid((const void*)kPcg1<S, 1, true>);
+    pcg1PerSm[0][0] = perSm((const void*)kPcg1<S, 0, false>);
+    pcg1PerSm[0][1] = perSm((const void*)kPcg1<S, 0, true>);
+    pcg1PerSm[1][0] = perSm((const void*)kPcg1<S, 1, false>);
+    pcg1PerSm[1][1] = perSm((const void*)kPcg1<S, 1, true>);
+    batchPerSm[0][0] = perSm((const void*)kPcgBatch<S, 0, false>);
+    batchPerSm[0][1] = perSm((const void*)kPcgBatch<S, 0, true>);
+    batchPerSm[1][0] = perSm((const void*)kPcgBatch<S, 1, false>);
+    batchPerSm[1][1] = perSm((const void*)kPcgBatch<S, 1, true>);
     int most = 0;
-    for (auto& row : pcg1Grid)
-      for (int gsz : row) most = std::max(most, gsz);
+    for (auto& row : pcg1PerSm)
+      for (int n : row) most = std::max(most, n * ctx->sms);
     blkPart.alloc(size_t(3) * most);
   }
 
@@ -739,15 +762,17 @@ struct System final : SystemBase {
     uint32_t ps = pass, xz = x0zero ? 1u : 0u, tg = tangent ? 1u : 0u;
     const int idx = law == TL_LAW_SNH ? 1 : 0;
     if (profiling) mark(2, true);
+    (void)tg;
     if (B == 1) {  // single body: two-level assembly, per-block partials
       void* args[] = {&s, &X, &xz};
       const void* fn = idx ? (tangent ? (const void*)kPcg1<S, 1, true> : (const void*)kPcg1<S, 1, false>)
                            : (tangent ? (const void*)kPcg1<S, 0, true> : (const void*)kPcg1<S, 0, false>);
-      TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(pcg1Grid[idx][tangent ? 1 : 0]), dim3(TILE), args, 0, st));
-    } else {
-      void* args[] = {&s, &X, &ps, &xz, &tg};
-      const void* fn = idx ? (const void*)kPcg<S, 1> : (const void*)kPcg<S, 0>;
-      TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(pcgGrid[idx]), dim3(TILE), args, 0, st));
+      TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(gridOf(pcg1PerSm[idx][tangent ? 1 : 0])), dim3(TILE), args, 0, st));
+    } else {  // batch: two-level assembly, per-body scalars
+      void* args[] = {&s, &X, &ps, &xz};
+      const void* fn = idx ? (tangent ? (const void*)kPcgBatch<S, 1, true> : (const void*)kPcgBatch<S, 1, false>)
+                           : (tangent ? (const void*)kPcgBatch<S, 0, true> : (const void*)kPcgBatch<S, 0, false>);
+      TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(gridOf(batchPerSm[idx][tangent ? 1 : 0])), dim3(TILE), args, 0, st));
     }
     ++launches;
     if (profiling) mark(2, false);
@@ -794,6 +819,15 @@ struct System final : SystemBase {
     profiling = (set.flags & TL_FLAG_PROFILE) != 0u;
     tracing = (set.flags & TL_FLAG_TRACE) != 0u;
     evUsed.clear();
+    {
+      const bool yieldsLaw = law == TL_LAW_COROTATED &&
+                             std::any_of(hb.begin(), hb.end(), [](const HostBody& h) { return h.anyYields; });
+      const bool newtonNeeded = set.plastic_passes > 1u && yieldsLaw;
+      if (B > 1 && !newtonNeeded && tuneGraph && !graphBroken && !tracing) {
+        const int32_t rc = stepGraph(set, gvec, dt, reports, law, yieldsLaw);
+        if (rc != TL_ERR_UNSUPPORTED) return rc;  // unsupported: capture refused, fall through to launches
+      }
+    }
     cudaEvent_t e0, e1;
     TL_CUDA(cudaEventCreate(&e0));
     TL_CUDA(cudaEventCreate(&e1));
@@ -927,6 +961,173 @@ struct System final : SystemBase {
     for (uint32_t b = 0; b < B; ++b)
       if (hacc[b].nonfinite) status = TL_ERR_NONFINITE;
     return status;
+  }
+
+  // ------------------------------------------------- graph-captured step ----
+  // A batched elastic step as one fixed launch sequence: the predictor
+  // inversion test and the substep count are decided on the device
+  // (kStepSelect), every body runs max(configured, 4) passes with the passes
+  // beyond its own substep count masked off, and the whole sequence is
+  // captured once into a CUDA graph and replayed every step.  The constants
+  // are copied from pinned host memory by a graph node, so dt and gravity may
+  // change between steps without re-capturing.
+  cudaGraphExec_t graphExec = nullptr;
+  uint64_t graphKey = ~0ull;
+  bool graphBroken = false;
+  DevBuf<BodyStepDev> dStepVar;
+  PinnedBuf<BodyStepDev> hStepVar, hStepOut;
+
+  void enqueueStep(int law, uint32_t passes, bool yieldsLaw) {
+    TL_CUDA(cudaMemcpyAsync(dStepVar.ptr, hStepVar.ptr, sizeof(BodyStepDev) * 2 * B, cudaMemcpyHostToDevice, st));
+    const uint32_t bb = (B + 255) / 256;
+    kAccReset<<<bb, 256, 0, st>>>(acc.ptr, cgrep.ptr, B);
+    kStepSelect<<<bb, 256, 0, st>>>(dStep.ptr, dStepVar.ptr, acc.ptr, B, 0u);
+    kInversionCheck<S><<<elemTiles, TILE, 0, st>>>(view());
+    kStepSelect<<<bb, 256, 0, st>>>(dStep.ptr, dStepVar.ptr, acc.ptr, B, 1u);
+    TL_CUDA(cudaGetLastError());
+    for (uint32_t pass = 0; pass < passes; ++pass) {
+      nodeOp(kPredict<S>, pass);
+      elasticReads(law, pass);
+      nodeOp(kUpdate<S>, pass);
+      if (yieldsLaw) element(law, u.ptr, nullptr, pass, EM_MAPPING | EM_COMMIT, 0.0);
+    }
+    kStepEnd<S><<<nodeTiles, TILE, 0, st>>>(view());
+    finalize(0);
+    finalize(2);
+    acc.download(hAcc.ptr, B, st);
+    cgrep.download(hRep.ptr, B, st);
+    sync.download(hSync.ptr, 1, st);
+    yielding.download(hCount.ptr, B, st);
+    dStep.download(hStepOut.ptr, B, st);
+  }
+
+  int32_t stepGraph(const tl_settings& set, const double gvec[3], double dt, tl_step_report* reports, int law,
+                    bool yieldsLaw) {
+    const uint32_t configured = std::max(set.substeps, 1u);
+    const uint32_t passes = std::max(configured, INVERTED_SUBSTEPS);
+    const Rule rule = ruleOf(set.spectral_radius);
+    if (!dStepVar.ptr) dStepVar.alloc(size_t(2) * B);
+    BodyStepDev* hv = hStepVar.get(size_t(2) * B);
+    hAcc.get(B);
+    hRep.get(B);
+    hSync.get(1);
+    hCount.get(B);
+    hStepOut.get(B);
+    for (uint32_t b = 0; b < B; ++b)
+      for (uint32_t k = 0; k < 2; ++k) {
+        BodyStepDev& s = hv[2 * b + k];
+        std::memset(&s, 0, sizeof(s));
+        s.substeps = k == 0 ? configured : std::max(configured, INVERTED_SUBSTEPS);
+        s.limit = set.cg_iterations;
+        s.alpha_f = rule.alphaForce;
+        s.alpha_m = rule.alphaMass;
+        s.beta = rule.beta;
+        s.gamma = rule.gamma;
+        s.gx = gvec[0];
+        s.gy = gvec[1];
+        s.gz = gvec[2];
+        s.tolerance = set.tolerance;
+        s.check_inner = dt / double(configured);
+        s.check_carry = (0.5 - rule.beta) * s.check_inner * s.check_inner;
+        s.inner = dt / double(s.substeps);
+        s.carry = (0.5 - rule.beta) * s.inner * s.inner;
+        s.inertia = 1.0 - rule.alphaMass;
+        s.hstep = std::sqrt((1.0 - rule.alphaForce) * rule.beta) * s.inner;
+        s.scale = s.hstep * s.hstep;
+      }
+    const uint64_t key = (uint64_t(law) << 48) | (uint64_t(yieldsLaw) << 40) | (uint64_t(profiling) << 36) |
+                         (uint64_t(configured) << 8) | uint64_t(tuneBlocksPerSm & 0xffu);
+    if (!graphExec || graphKey != key) {
+      if (graphExec) cudaGraphExecDestroy(graphExec);
+      graphExec = nullptr;
+      cudaGraph_t graph = nullptr;
+      evUsed.clear();  // profiling marks become event-record nodes of the graph
+      TL_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+      launches = 0;
+      capturing = true;
+      try {
+        enqueueStep(law, passes, yieldsLaw);
+      } catch (...) {
+        capturing = false;
+        cudaStreamEndCapture(st, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        graphBroken = true;
+        return TL_ERR_UNSUPPORTED;
+      }
+      capturing = false;
+      const cudaError_t ended = cudaStreamEndCapture(st, &graph);
+      if (ended != cudaSuccess || !graph ||
+          cudaGraphInstantiate(&graphExec, graph, 0) != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        graphExec = nullptr;
+        graphBroken = true;
+        return TL_ERR_UNSUPPORTED;
+      }
+      cudaGraphDestroy(graph);
+      graphKey = key;
+      graphLaunches = launches;
+      graphEv = evUsed;
+    }
+    cudaEvent_t e0, e1;
+    TL_CUDA(cudaEventCreate(&e0));
+    TL_CUDA(cudaEventCreate(&e1));
+    TL_CUDA(cudaEventRecord(e0, st));
+    TL_CUDA(cudaGraphLaunch(graphExec, st));
+    TL_CUDA(cudaEventRecord(e1, st));
+    TL_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    TL_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    double classSeconds[3] = {0.0, 0.0, 0.0};
+    if (profiling)
+      for (const auto& u : graphEv) {
+        float t = 0.f;
+        TL_CUDA(cudaEventElapsedTime(&t, evPool[u.second].first, evPool[u.second].second));
+        classSeconds[u.first] += double(t) * 1e-3;
+      }
+    if (hSync.ptr->error != 0) throw StatusError{TL_ERR_TIMEOUT, "a PCG grid barrier ran out of time"};
+    int32_t status = TL_OK;
+    for (uint32_t b = 0; b < B; ++b) {
+      if (hAcc.ptr[b].nonfinite) status = TL_ERR_NONFINITE;
+      if (reports) {
+        reports[b].element_seconds += classSeconds[0];
+        reports[b].assemble_seconds += classSeconds[1];
+        reports[b].pcg_seconds += classSeconds[2];
+      }
+      if (!reports) continue;
+      tl_step_report& r = reports[b];
+      r.nodes += hb[b].nodes;
+      r.elements += hb[b].tets;
+      r.substeps += hStepOut.ptr[b].substeps;
+      r.cg_iterations += hRep.ptr[b].iterations;
+      r.cg_capped_solves += hRep.ptr[b].capped;
+      r.operator_applications += hRep.ptr[b].applications;
+      r.cg_solves += hRep.ptr[b].solves;
+      r.cg_tangent_iterations += hRep.ptr[b].tangent_iterations;
+      r.cg_worst_relative_residual = std::max(r.cg_worst_relative_residual, hRep.ptr[b].worst_rel);
+      r.yielding = hCount.ptr[b];
+      r.plastic_growth |= hAcc.ptr[b].grew;
+      r.non_finite |= hAcc.ptr[b].nonfinite;
+      r.elastic_energy += hAcc.ptr[b].energy;
+      r.kinetic_energy += hAcc.ptr[b].kinetic;
+      r.min_volume_ratio = fromMinKey(hAcc.ptr[b].min_j_key);
+      r.device_seconds += double(ms) * 1e-3;
+      r.kernel_launches += graphLaunches;
+    }
+    return status;
+  }
+  uint32_t graphLaunches = 0;
+  std::vector<std::pair<int, size_t>> graphEv;  // event pairs recorded by the captured graph
+
+  void tune(uint32_t blocksPerSm, uint32_t graph) override {
+    tuneBlocksPerSm = blocksPerSm;
+    tuneGraph = graph != 0u;
+    if (graphExec) cudaGraphExecDestroy(graphExec);
+    graphExec = nullptr;
+    graphBroken = false;
   }
 
   // solver.cc:3914-3950: assemble at the predictor, solve for the
@@ -1196,6 +1397,15 @@ int32_t tl_system_counts(const tl_system* system, uint32_t* bodies, uint64_t* no
   if (nodes) *nodes = system->impl->nodes;
   if (tets) *tets = system->impl->tets;
   return TL_OK;
+}
+
+int32_t tl_system_tune(tl_system* system, uint32_t pcg_blocks_per_sm, uint32_t graph) {
+  if (!system || pcg_blocks_per_sm > 64u) return TL_ERR_ARG;
+  return guarded(system->ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(system->ctx->device));
+    system->impl->tune(pcg_blocks_per_sm, graph);
+    return TL_OK;
+  });
 }
 
 int32_t tl_system_trace(const tl_system* system, uint32_t* iterations, uint32_t capacity, uint32_t* count) {

@@ -223,6 +223,11 @@ class System:
               self.context.handle)
         return out
 
+    def tune(self, pcg_blocks_per_sm: int = 0, graph: bool = True):
+        """Launch shape (tl_system_tune): cap on persistent-PCG blocks per SM
+        (0 = occupancy limit) and CUDA-graph replay of batched elastic steps."""
+        check(capi.lib().tl_system_tune(self.handle, int(pcg_blocks_per_sm), 1 if graph else 0), self.context.handle)
+
     def trace(self) -> list:
         """Iterations of every PCG launch made with Settings.trace, oldest first."""
         count = C.c_uint32()

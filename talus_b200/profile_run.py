@@ -20,25 +20,27 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def main():
     sys.path.insert(0, ROOT)
-    import bench
     import talus_b200 as tb
+    from talus_b200.workloads import WORKLOADS, make_bodies
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="plastic-block", choices=sorted(bench.WORKLOADS))
+    ap.add_argument("--workload", default="plastic-block", choices=sorted(WORKLOADS))
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     args = ap.parse_args()
-    spec = bench.WORKLOADS[args.workload]
-    mesh, mat = bench.make_mesh(spec)
+    spec = WORKLOADS[args.workload]
+    meshes, mats = make_bodies(spec)
     precision = tb.FP32_MIXED if args.precision == "mixed" else tb.FP64
     law = tb.NEO_HOOKEAN if spec["law"] == "snh" else tb.COROTATED
-    system = tb.System(mesh, [mat], precision)
-    system.set_state(tb.rest_state(mesh))
+    system = tb.System(meshes, mats, precision)
+    for i, m in enumerate(meshes):
+        system.set_state(tb.rest_state(m), i)
     settings = tb.Settings(law=law, trace=True)
-    reports = [system.step(settings)[0].as_dict() for _ in range(args.steps)]
-    print(json.dumps({"workload": args.workload, "precision": args.precision, "tets": mesh.tets,
-                      "nodes": mesh.nodes, "pcg_iterations": system.trace(),
-                      "tangent_iterations": sum(r["cg_tangent_iterations"] for r in reports)}))
+    reports = [[r.as_dict() for r in system.step(settings)] for _ in range(args.steps)]
+    print(json.dumps({"workload": args.workload, "precision": args.precision,
+                      "tets": sum(m.tets for m in meshes), "nodes": sum(m.nodes for m in meshes),
+                      "pcg_iterations": system.trace(),
+                      "tangent_iterations": sum(r[0]["cg_tangent_iterations"] for r in reports)}))
     system.close()
 
 

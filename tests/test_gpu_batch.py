@@ -51,6 +51,56 @@ def test_batched_bodies_match_single_body_systems(law, precision, tol):
 
 
 @pytest.mark.parametrize("precision", [tb.FP64, tb.FP32_MIXED])
+def test_graph_replayed_batch_equals_launched_batch(precision):
+    """A batched elastic step replayed from a CUDA graph (device-side substep
+    choice, masked passes) gives bitwise the state of plain launches."""
+    meshes, mats = tb.mesh.batch_bodies(count=6, seed=11, lo=3, hi=6)
+    states = []
+    for graph in (True, False):
+        s = tb.System(meshes, mats, precision)
+        s.tune(graph=graph)
+        for i, m in enumerate(meshes):
+            s.set_state(tb.rest_state(m), i)
+        for _ in range(5):
+            reps = s.step(tb.Settings(), GRAVITY, DT)
+        assert all(r.cg_iterations > 0 for r in reps)
+        states.append(np.concatenate([s.get_state(i).position.ravel() for i in range(len(meshes))]))
+        s.close()
+    assert np.array_equal(states[0], states[1])
+
+
+def test_profiled_graph_step_reports_kernel_class_times():
+    """TL_FLAG_PROFILE events inside a captured graph fire on every replay."""
+    meshes, mats = tb.mesh.batch_bodies(count=4, seed=12, lo=3, hi=5)
+    s = tb.System(meshes, mats, tb.FP32_MIXED)
+    for i, m in enumerate(meshes):
+        s.set_state(tb.rest_state(m), i)
+    for _ in range(3):
+        reps = s.step(tb.Settings(profile=True), GRAVITY, DT)
+        r = reps[0]
+        assert r.element_seconds > 0 and r.pcg_seconds > 0
+        assert r.element_seconds + r.assemble_seconds + r.pcg_seconds <= r.device_seconds * 1.01
+    s.close()
+
+
+@pytest.mark.parametrize("blocks", [1, 2])
+def test_persistent_grid_shape_does_not_change_the_single_body_result(blocks):
+    """tl_system_tune caps the persistent grid; results stay within FP64 rounding."""
+    mesh, mat = elastic_block()
+    out = []
+    for cap in (0, blocks):
+        s = tb.System(mesh, [mat], tb.FP64)
+        s.tune(pcg_blocks_per_sm=cap)
+        s.set_state(tb.rest_state(mesh))
+        for _ in range(4):
+            s.step(tb.Settings(), GRAVITY, DT)
+        out.append(s.get_state().position)
+        s.close()
+    scale = np.linalg.norm(out[0] - mesh.rest_positions, axis=1).max()
+    assert np.linalg.norm(out[0] - out[1], axis=1).max() <= 1e-10 * scale
+
+
+@pytest.mark.parametrize("precision", [tb.FP64, tb.FP32_MIXED])
 def test_runs_are_bitwise_identical(precision):
     mesh, mat = plastic_block()
     results = []
