@@ -287,11 +287,11 @@ def run_ours(args, spec, rank, world, dist):
         barrier()
     total_seconds = max_over_ranks(sum(step_seconds))
     value = world * T * args.steps / total_seconds
+    finals = [system.get_state(i) for i in range(B)]
 
     # ---- end to end through the public API: the state crosses the host boundary every step
     f32 = []
-    for i in range(B):
-        st = system.get_state(i)
+    for st in finals:
         f32.append({k: np.ascontiguousarray(getattr(st, k), np.float32) for k in
                     ("position", "velocity", "acceleration", "rotation", "plastic")})
     h2d = sum(a.nbytes for d in f32 for a in d.values())
@@ -373,6 +373,21 @@ def run_ours(args, spec, rank, world, dist):
                    "plastic_evaluations_per_step": float(per_body[:, 3].sum() / args.steps)},
         "clocks": clocks.summary(),
     }
+    if precision == tb.FP32_MIXED:
+        # the plain FP64 GPU step on the same workload, and the FP32-mixed error against it
+        secs64, pos64 = run_fp64(meshes, mats, settings, args, flush, context)
+        secs64 = max_over_ranks(secs64)
+        worst = 0.0
+        for m, st, x64 in zip(meshes, finals, pos64):
+            scale = np.linalg.norm(x64 - m.rest_positions, axis=1).max()
+            worst = max(worst, float(np.linalg.norm(st.position - x64, axis=1).max() / max(scale, 1e-300)))
+        result["fp64"] = {"value": world * T * args.steps / secs64, "ms_per_step": secs64 * 1e3 / args.steps,
+                          "mixed_speedup": secs64 / total_seconds,
+                          "max_rel_displacement_error": worst,
+                          "note": f"same workload and steps from rest in FP64; error = max over bodies of "
+                                  f"max|x_mixed - x_fp64| / max|x_fp64 - X| after {args.warmup + args.steps} steps"}
+    if not args.no_adjoint:
+        result["adjoint"] = adjoint_ratio(precision, context)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_sample(spec)
         result["cpu_baseline"]["cpu"] = cpu_info()
@@ -380,6 +395,52 @@ def run_ours(args, spec, rank, world, dist):
         print(json.dumps(result), flush=True)
     system.close()
     context.close()
+
+
+def run_fp64(meshes, mats, settings, args, flush, context):
+    import torch
+
+    import talus_b200 as tb
+
+    system = tb.System(meshes, mats, tb.FP64, context)
+    tune = tuning(args.workload, "fp64")
+    if tune:
+        system.tune(tune["pcg_blocks_per_sm"], tune["graph"])
+    for i, m in enumerate(meshes):
+        system.set_state(tb.rest_state(m), i)
+    for _ in range(args.warmup):
+        system.step(settings)
+    secs = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        secs += system.step(settings)[0].device_seconds
+    pos = [system.get_state(i).position for i in range(len(meshes))]
+    system.close()
+    return secs, pos
+
+
+def adjoint_ratio(precision, context, repeats=3):
+    """Differentiable-rollout workload: 16^3 cubes (24,576 tets), 30 steps,
+    checkpoints every 5, loss |x_T - x_target|^2; device time of the adjoint
+    (checkpoint recomputation included) over that of the forward rollout."""
+    import talus_b200 as tb
+    from talus_b200 import gradcheck
+
+    tol = 1e-10 if precision == tb.FP64 else 1e-6
+    prob = gradcheck.make_problem(cells=16, steps=30, checkpoint_every=5, precision=precision, tolerance=tol,
+                                  context=context)
+    fwd, adj = [], []
+    for k in range(repeats + 1):
+        loss, g = prob.gradients(prob.youngs, prob.v0)
+        if k:
+            fwd.append(prob.roll.forward_seconds)
+            adj.append(g.seconds)
+    f, a = float(np.median(fwd)), float(np.median(adj))
+    prob.close()
+    return {"workload": "rollout 16x16x16 (24576 tets), 30 steps, checkpoints every 5, neo-Hookean",
+            "forward_ms": f * 1e3, "adjoint_ms": a * 1e3, "ratio": a / f, "loss": loss,
+            "precision": "fp64" if precision == tb.FP64 else "mixed", "pcg_tolerance": tol, "newton_reads": 4}
 
 
 def main():
@@ -391,6 +452,7 @@ def main():
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="plastic-block")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

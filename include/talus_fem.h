@@ -195,6 +195,49 @@ int32_t tl_step_host(tl_system* system, uint32_t body, int32_t dtype, void* posi
 /* Default settings (Settings{} in solver.h:51-107). */
 void tl_settings_default(tl_settings* settings);
 
+/* Per-element Young's modulus of one body ([tets], Pa), the
+ * PreparedMesh-side override that tl_mesh_desc::element_youngs sets at
+ * creation; lets a caller change E between rollouts without rebuilding the
+ * system.  No reference counterpart (the reference reads E from the lane). */
+int32_t tl_system_set_youngs(tl_system* system, uint32_t body, const double* youngs);
+
+/* Differentiable rollout, no reference counterpart (the reference has no
+ * differentiation).  A rollout is `steps` calls of tl_step on a one-body
+ * system whose law is TL_LAW_SNH and whose materials do not yield, starting
+ * from the state the system holds when tl_rollout_forward is called.  Each
+ * step runs `newton_reads` linearised reads (the reference takes 3,
+ * solver.cc:3914-3950) with the settings' PCG tolerance, so a tight
+ * tolerance and >= 3 reads give a converged implicit step, which is what the
+ * adjoint differentiates.  The forward keeps the state every
+ * `checkpoint_every` steps; the adjoint recomputes each segment from its
+ * checkpoint and runs the steps' vector-Jacobian products backwards (one
+ * element pass, one PCG solve with the step's own operator and one node
+ * update per step).  Steps that need more than one substep (predictor
+ * inversion, solver.cc:3574-3583) are refused with TL_ERR_UNSUPPORTED. */
+typedef struct tl_rollout tl_rollout;
+typedef struct tl_rollout_desc {
+  uint32_t steps;
+  uint32_t checkpoint_every;  /* >= 1 */
+  uint32_t newton_reads;      /* >= 1; 3 is the reference's count */
+  uint32_t pad;
+  double delta_time;
+  double gravity[3];
+} tl_rollout_desc;
+int32_t tl_rollout_create(tl_system* system, const tl_rollout_desc* desc, const tl_settings* settings,
+                          tl_rollout** out);
+/* A rollout holds on to its system: destroy it before the system (the destroy
+ * call itself touches only its own memory, so it is safe in any order). */
+int32_t tl_rollout_destroy(tl_rollout* rollout);
+/* Runs the rollout; the system ends in the final state.  report (or NULL) is
+ * accumulated over the steps; *device_seconds (or NULL) gets the GPU time. */
+int32_t tl_rollout_forward(tl_rollout* rollout, tl_step_report* report, double* device_seconds);
+/* Cotangents of the last forward rollout.  dl_dx_final: dL/dx_T [3*nodes];
+ * dl_dv_final: dL/dv_T [3*nodes] or NULL (zero).  Outputs: dl_dyoungs dL/dE
+ * [tets] (per element), dl_dv0 dL/dv_0 [3*nodes], dl_dx0 dL/dx_0 [3*nodes];
+ * each may be NULL.  The system is left in the final state of the forward. */
+int32_t tl_rollout_adjoint(tl_rollout* rollout, const double* dl_dx_final, const double* dl_dv_final,
+                           double* dl_dyoungs, double* dl_dv0, double* dl_dx0, double* device_seconds);
+
 /* No counterpart in the reference.  One step of one small body that allocates
  * nothing, for callers that cannot call cudaMalloc: engines with a fixed GPU
  * memory budget, code that runs while a CUDA graph is being captured (where

@@ -8,9 +8,10 @@ from . import _capi
 from .deformable import (COROTATED, FP32_MIXED, FP64, NEO_HOOKEAN, Context, DeformableState, PhysicalMaterial,
                          PreparedMesh, Settings, StepReport, System, rest_state, step)
 from .mesh import box_mesh
+from .rollout import Gradients, Rollout
 
 __all__ = ["COROTATED", "FP32_MIXED", "FP64", "NEO_HOOKEAN", "Context", "DeformableState", "PhysicalMaterial",
-           "PreparedMesh", "Settings", "StepReport", "System", "rest_state", "step", "box_mesh"]
+           "PreparedMesh", "Settings", "StepReport", "System", "rest_state", "step", "box_mesh", "Rollout", "Gradients"]
 
 
 def library():

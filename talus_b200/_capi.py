@@ -114,6 +114,17 @@ class tl_step_report(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class tl_rollout_desc(C.Structure):
+    _fields_ = [
+        ("steps", C.c_uint32),
+        ("checkpoint_every", C.c_uint32),
+        ("newton_reads", C.c_uint32),
+        ("pad", C.c_uint32),
+        ("delta_time", C.c_double),
+        ("gravity", C.c_double * 3),
+    ]
+
+
 # Every entry point of include/talus_fem.h: name -> (restype, argtypes).
 SIGNATURES = {
     "tl_abi_version": (C.c_int32, []),
@@ -135,6 +146,12 @@ SIGNATURES = {
     "tl_step_host": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_int32] + [C.c_void_p] * 5 +
                      [C.POINTER(tl_settings), C.c_void_p, C.c_double, C.POINTER(tl_step_report)]),
     "tl_settings_default": (None, [C.POINTER(tl_settings)]),
+    "tl_system_set_youngs": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p]),
+    "tl_rollout_create": (C.c_int32, [C.c_void_p, C.POINTER(tl_rollout_desc), C.POINTER(tl_settings),
+                                      C.POINTER(C.c_void_p)]),
+    "tl_rollout_destroy": (C.c_int32, [C.c_void_p]),
+    "tl_rollout_forward": (C.c_int32, [C.c_void_p, C.POINTER(tl_step_report), C.POINTER(C.c_double)]),
+    "tl_rollout_adjoint": (C.c_int32, [C.c_void_p] + [C.c_void_p] * 5 + [C.POINTER(C.c_double)]),
     "tl_step_noalloc": (C.c_int32, [C.c_int32, C.POINTER(tl_mesh_desc), C.c_int32] + [C.c_void_p] * 5 +
                         [C.POINTER(tl_settings), C.c_void_p, C.c_double, C.POINTER(tl_step_report)]),
 }

@@ -6,6 +6,7 @@
 
 #include "../../include/talus_fem.h"
 #include "tl_kernels.cuh"
+#include "tl_adjoint.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -119,8 +120,17 @@ struct tl_ctx {
   std::string last_error;
 };
 
+struct RolloutBase {
+  virtual ~RolloutBase() = default;
+  virtual void forward(tl_step_report* report, double* seconds) = 0;
+  virtual void adjoint(const double* dxT, const double* dvT, double* dE, double* dv0, double* dx0,
+                       double* seconds) = 0;
+};
+
 struct SystemBase {
   virtual ~SystemBase() = default;
+  virtual void setYoungs(uint32_t body, const double* youngs) = 0;
+  virtual std::unique_ptr<RolloutBase> rollout(const tl_rollout_desc& desc, const tl_settings& settings) = 0;
   virtual void stateSet(uint32_t body, int32_t dtype, const void* x, const void* v, const void* a, const void* rot,
                         const void* plastic) = 0;
   virtual void stateGet(uint32_t body, int32_t dtype, void* x, void* v, void* a, void* rot, void* plastic) = 0;
@@ -131,12 +141,23 @@ struct SystemBase {
   uint64_t nodes = 0, tets = 0;
 };
 
+// The destroy calls use only `device`, so handles may be destroyed in any
+// order (a garbage collector does not keep creation order).
 struct tl_system {
   tl_ctx* ctx = nullptr;
+  int device = 0;
   std::unique_ptr<SystemBase> impl;
 };
 
+struct tl_rollout {
+  tl_system* system = nullptr;
+  int device = 0;
+  std::unique_ptr<RolloutBase> impl;
+};
+
 namespace {
+
+template <class S> struct Rollout;
 
 template <class S>
 struct System final : SystemBase {
@@ -1132,11 +1153,13 @@ struct System final : SystemBase {
 
   // solver.cc:3914-3950: assemble at the predictor, solve for the
   // acceleration, then two re-linearised increments.
+  // newtonReads is ANCHORED_READS except inside a differentiable rollout.
+  uint32_t newtonReads = ANCHORED_READS;
   void elasticReads(int law, uint32_t pass) {
     element(law, weighted.ptr, nullptr, pass, EM_MAPPING, 0.0);
     nodeAssemble(nullptr, pass);
     pcg(law, a.ptr, pass, false, false);
-    for (uint32_t read = 1; read != ANCHORED_READS; ++read) {
+    for (uint32_t read = 1; read < newtonReads; ++read) {
       element(law, weighted.ptr, a.ptr, pass, EM_MAPPING, 0.0);
       nodeAssemble(a.ptr, pass);
       pcg(law, incr.ptr, pass, true, false);
@@ -1283,7 +1306,180 @@ struct System final : SystemBase {
     }
   }
   DevBuf<Vec4<S>>& lowest_() { return lowest; }
+
+  // Per-element E override (tl_system_set_youngs).  The first call gives
+  // every element its lane's modulus, then overwrites the body's elements.
+  void setYoungs(uint32_t b, const double* E) override {
+    const BodyDev& bd = bodyHost[b];
+    const HostBody& h = hb[b];
+    for (uint32_t t = 0; t < h.tets; ++t)
+      if (!(E[t] > 0.0) || !std::isfinite(E[t])) throw StatusError{TL_ERR_ARG, "Young's modulus must be positive"};
+    if (!hasEyoung) {
+      eyoung.alloc(Tp);
+      kLaneYoungs<<<elemTiles, TILE, 0, st>>>(view(), eyoung.ptr);
+      TL_CUDA(cudaGetLastError());
+      hasEyoung = true;
+      if (graphExec) cudaGraphExecDestroy(graphExec);  // the captured launches hold the old element view
+      graphExec = nullptr;
+    }
+    eyoung.upload(E, h.tets, st, bd.elem_begin);
+    TL_CUDA(cudaStreamSynchronize(st));
+  }
+
+  std::unique_ptr<RolloutBase> rollout(const tl_rollout_desc& desc, const tl_settings& settings) override;
 };
+
+// Checkpointed rollout and its adjoint (kernels and equations in
+// tl_adjoint.cuh).  State layout of a stored state: u, v, a, each [Vp].
+template <class S>
+struct Rollout final : RolloutBase {
+  System<S>& sys;
+  tl_rollout_desc d;
+  tl_settings set;
+  uint32_t segments = 0;
+  size_t stride = 0;  // elements of one stored state
+  DevBuf<Vec4<S>> ck, seg, fin, xb, vb, ab, lam;
+  DevBuf<double> ebar;
+  bool ran = false;
+
+  Rollout(System<S>& s, const tl_rollout_desc& desc, const tl_settings& settings) : sys(s), d(desc), set(settings) {
+    if (sys.B != 1u) throw StatusError{TL_ERR_UNSUPPORTED, "a rollout runs on a one-body system"};
+    if (settings.law != TL_LAW_SNH)
+      throw StatusError{TL_ERR_UNSUPPORTED, "the adjoint needs the exact tangent of TL_LAW_SNH"};
+    if (!desc.steps || !desc.checkpoint_every || !desc.newton_reads || !(desc.delta_time > 0.0))
+      throw StatusError{TL_ERR_ARG, "rollout needs steps, checkpoint_every, newton_reads >= 1 and dt > 0"};
+    segments = (desc.steps + desc.checkpoint_every - 1) / desc.checkpoint_every;
+    stride = size_t(3) * sys.Vp;
+    ck.alloc(stride * segments);
+    seg.alloc(stride * (size_t(std::min(desc.checkpoint_every, desc.steps)) + 1));
+    fin.alloc(stride);
+    for (DevBuf<Vec4<S>>* b : {&xb, &vb, &ab, &lam}) {
+      b->alloc(sys.Vp);
+      b->zero(sys.st);
+    }
+    ebar.alloc(sys.Tp);
+  }
+
+  void save(Vec4<S>* dst) {
+    const size_t bytes = size_t(sys.Vp) * sizeof(Vec4<S>);
+    TL_CUDA(cudaMemcpyAsync(dst, sys.u.ptr, bytes, cudaMemcpyDeviceToDevice, sys.st));
+    TL_CUDA(cudaMemcpyAsync(dst + sys.Vp, sys.v.ptr, bytes, cudaMemcpyDeviceToDevice, sys.st));
+    TL_CUDA(cudaMemcpyAsync(dst + 2 * size_t(sys.Vp), sys.a.ptr, bytes, cudaMemcpyDeviceToDevice, sys.st));
+  }
+  void load(const Vec4<S>* src) {
+    const size_t bytes = size_t(sys.Vp) * sizeof(Vec4<S>);
+    TL_CUDA(cudaMemcpyAsync(sys.u.ptr, src, bytes, cudaMemcpyDeviceToDevice, sys.st));
+    TL_CUDA(cudaMemcpyAsync(sys.v.ptr, src + sys.Vp, bytes, cudaMemcpyDeviceToDevice, sys.st));
+    TL_CUDA(cudaMemcpyAsync(sys.a.ptr, src + 2 * size_t(sys.Vp), bytes, cudaMemcpyDeviceToDevice, sys.st));
+  }
+
+  void stepOnce(tl_step_report* report) {
+    tl_step_report local;
+    std::memset(&local, 0, sizeof(local));
+    tl_step_report* r = report ? report : &local;
+    const uint64_t before = r->substeps;
+    sys.newtonReads = d.newton_reads;
+    int32_t rc;
+    try {
+      rc = sys.step(set, d.gravity, d.delta_time, r);
+    } catch (...) {
+      sys.newtonReads = ANCHORED_READS;
+      throw;
+    }
+    sys.newtonReads = ANCHORED_READS;
+    if (rc == TL_ERR_NONFINITE) throw StatusError{TL_ERR_NONFINITE, "the rollout state became non-finite"};
+    if (rc != TL_OK) throw StatusError{rc, "rollout step failed"};
+    if (r->substeps - before != 1u)
+      throw StatusError{TL_ERR_UNSUPPORTED, "a rollout step needed more than one substep (predictor inversion)"};
+  }
+
+  void forward(tl_step_report* report, double* seconds) override {
+    cudaEvent_t e0, e1;
+    TL_CUDA(cudaEventCreate(&e0));
+    TL_CUDA(cudaEventCreate(&e1));
+    TL_CUDA(cudaEventRecord(e0, sys.st));
+    save(ck.ptr);
+    const uint32_t C = d.checkpoint_every;
+    for (uint32_t n = 0; n < d.steps; ++n) {
+      stepOnce(report);
+      if ((n + 1) % C == 0 && n + 1 < d.steps) save(ck.ptr + stride * ((n + 1) / C));
+    }
+    save(fin.ptr);
+    TL_CUDA(cudaEventRecord(e1, sys.st));
+    TL_CUDA(cudaStreamSynchronize(sys.st));
+    float ms = 0.f;
+    TL_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (seconds) *seconds = double(ms) * 1e-3;
+    ran = true;
+  }
+
+  void adjoint(const double* dxT, const double* dvT, double* dE, double* dv0, double* dx0,
+               double* seconds) override {
+    if (!ran) throw StatusError{TL_ERR_ARG, "tl_rollout_adjoint needs a forward rollout first"};
+    const BodyDev& bd = sys.bodyHost[0];
+    const HostBody& h = sys.hb[0];
+    xb.zero(sys.st);
+    vb.zero(sys.st);
+    ab.zero(sys.st);
+    ebar.zero(sys.st);
+    if (dxT) sys.setNodes(bd, h, xb, dxT, false);
+    if (dvT) sys.setNodes(bd, h, vb, dvT, false);
+    cudaEvent_t e0, e1;
+    TL_CUDA(cudaEventCreate(&e0));
+    TL_CUDA(cudaEventCreate(&e1));
+    TL_CUDA(cudaEventRecord(e0, sys.st));
+    const uint32_t C = d.checkpoint_every;
+    for (uint32_t k = segments; k-- > 0;) {
+      const uint32_t s0 = k * C, s1 = std::min(d.steps, s0 + C), L = s1 - s0;
+      // recompute the segment from its checkpoint, keeping every state
+      load(ck.ptr + stride * k);
+      save(seg.ptr);
+      for (uint32_t j = 0; j < L; ++j) {
+        stepOnce(nullptr);
+        save(seg.ptr + stride * (j + 1));
+      }
+      for (uint32_t j = L; j-- > 0;) {
+        load(seg.ptr + stride * j);
+        const Vec4<S>* A = seg.ptr + stride * (j + 1) + 2 * size_t(sys.Vp);  // converged acceleration of step j
+        sys.nodeOp(kPredict<S>, 0);
+        sys.element(TL_LAW_SNH, sys.weighted.ptr, A, 0, EM_MAPPING, 0.0);
+        sys.nodeAssemble(A, 0);
+        kAdjointRight<S><<<sys.nodeTiles, TILE, 0, sys.st>>>(sys.view(), xb.ptr, vb.ptr, ab.ptr);
+        sys.check();
+        sys.pcg(TL_LAW_SNH, lam.ptr, 0, true, false);
+        kAdjointElement<S, 1><<<sys.elemTiles, TILE, 0, sys.st>>>(sys.view(), lam.ptr, ebar.ptr);
+        sys.check();
+        kAdjointNode<S><<<sys.nodeTiles, TILE, 0, sys.st>>>(sys.view(), lam.ptr, xb.ptr, vb.ptr, ab.ptr);
+        sys.check();
+      }
+      GridSyncDev* hs = sys.hSync.get(1);
+      sys.sync.download(hs, 1, sys.st);
+      TL_CUDA(cudaStreamSynchronize(sys.st));
+      if (hs->error != 0) throw StatusError{TL_ERR_TIMEOUT, "a PCG grid barrier ran out of time"};
+    }
+    load(fin.ptr);
+    TL_CUDA(cudaEventRecord(e1, sys.st));
+    TL_CUDA(cudaStreamSynchronize(sys.st));
+    float ms = 0.f;
+    TL_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (seconds) *seconds = double(ms) * 1e-3;
+    if (dE) {
+      ebar.download(dE, h.tets, sys.st, bd.elem_begin);
+      TL_CUDA(cudaStreamSynchronize(sys.st));
+    }
+    if (dv0) sys.getNodes(bd, h, vb, dv0, false);
+    if (dx0) sys.getNodes(bd, h, xb, dx0, false);
+  }
+};
+
+template <class S>
+std::unique_ptr<RolloutBase> System<S>::rollout(const tl_rollout_desc& desc, const tl_settings& settings) {
+  return std::make_unique<Rollout<S>>(*this, desc, settings);
+}
 
 int32_t fail(tl_ctx* ctx, int32_t status, const std::string& what) {
   if (ctx) ctx->last_error = what;
@@ -1375,6 +1571,7 @@ int32_t tl_system_create(tl_ctx* ctx, const tl_mesh_desc* bodies, uint32_t count
     TL_CUDA(cudaSetDevice(ctx->device));
     auto sys = std::make_unique<tl_system>();
     sys->ctx = ctx;
+    sys->device = ctx->device;
     if (precision == TL_FP64) sys->impl = std::make_unique<System<double>>(ctx, bodies, count);
     else if (precision == TL_FP32_MIXED) sys->impl = std::make_unique<System<float>>(ctx, bodies, count);
     else return fail(ctx, TL_ERR_ARG, "unknown precision");
@@ -1385,8 +1582,8 @@ int32_t tl_system_create(tl_ctx* ctx, const tl_mesh_desc* bodies, uint32_t count
 
 int32_t tl_system_destroy(tl_system* system) {
   if (!system) return TL_ERR_ARG;
-  cudaSetDevice(system->ctx->device);
-  cudaStreamSynchronize(system->ctx->stream);
+  cudaSetDevice(system->device);
+  cudaDeviceSynchronize();
   delete system;
   return TL_OK;
 }
@@ -1443,6 +1640,57 @@ int32_t tl_step(tl_system* system, const tl_settings* settings, const double gra
   return guarded(system->ctx, [&]() -> int32_t {
     TL_CUDA(cudaSetDevice(system->ctx->device));
     return system->impl->step(*settings, gravity, dt, reports);
+  });
+}
+
+int32_t tl_system_set_youngs(tl_system* system, uint32_t body, const double* youngs) {
+  if (!system || !youngs || body >= system->impl->bodies) return TL_ERR_ARG;
+  return guarded(system->ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(system->ctx->device));
+    system->impl->setYoungs(body, youngs);
+    return TL_OK;
+  });
+}
+
+int32_t tl_rollout_create(tl_system* system, const tl_rollout_desc* desc, const tl_settings* settings,
+                          tl_rollout** out) {
+  if (!system || !desc || !settings || !out) return TL_ERR_ARG;
+  *out = nullptr;
+  return guarded(system->ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(system->ctx->device));
+    auto r = std::make_unique<tl_rollout>();
+    r->system = system;
+    r->device = system->device;
+    r->impl = system->impl->rollout(*desc, *settings);
+    *out = r.release();
+    return TL_OK;
+  });
+}
+
+int32_t tl_rollout_destroy(tl_rollout* rollout) {
+  if (!rollout) return TL_ERR_ARG;
+  cudaSetDevice(rollout->device);
+  cudaDeviceSynchronize();
+  delete rollout;
+  return TL_OK;
+}
+
+int32_t tl_rollout_forward(tl_rollout* rollout, tl_step_report* report, double* device_seconds) {
+  if (!rollout) return TL_ERR_ARG;
+  return guarded(rollout->system->ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(rollout->system->ctx->device));
+    rollout->impl->forward(report, device_seconds);
+    return TL_OK;
+  });
+}
+
+int32_t tl_rollout_adjoint(tl_rollout* rollout, const double* dl_dx_final, const double* dl_dv_final,
+                           double* dl_dyoungs, double* dl_dv0, double* dl_dx0, double* device_seconds) {
+  if (!rollout) return TL_ERR_ARG;
+  return guarded(rollout->system->ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(rollout->system->ctx->device));
+    rollout->impl->adjoint(dl_dx_final, dl_dv_final, dl_dyoungs, dl_dv0, dl_dx0, device_seconds);
+    return TL_OK;
   });
 }
 

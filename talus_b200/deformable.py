@@ -223,6 +223,13 @@ class System:
               self.context.handle)
         return out
 
+    def set_youngs(self, youngs, body: int = 0):
+        """Per-element Young's modulus of one body (tl_system_set_youngs)."""
+        e = np.ascontiguousarray(youngs, np.float64)
+        if e.shape != (self.meshes[body].tets,):
+            raise ValueError("one modulus per tet")
+        check(capi.lib().tl_system_set_youngs(self.handle, body, _ptr(e)), self.context.handle)
+
     def tune(self, pcg_blocks_per_sm: int = 0, graph: bool = True):
         """Launch shape (tl_system_tune): cap on persistent-PCG blocks per SM
         (0 = occupancy limit) and CUDA-graph replay of batched elastic steps."""

@@ -35,7 +35,8 @@ def test_library_exports_every_declared_symbol():
 
 def test_struct_layout_matches_the_header():
     structs = {"tl_material": capi.tl_material, "tl_mesh_desc": capi.tl_mesh_desc,
-               "tl_settings": capi.tl_settings, "tl_step_report": capi.tl_step_report}
+               "tl_settings": capi.tl_settings, "tl_step_report": capi.tl_step_report,
+               "tl_rollout_desc": capi.tl_rollout_desc}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for name, cls in structs.items():
         lines.append(f'  printf("{name} size %zu\\n", sizeof({name}));')
@@ -77,6 +78,11 @@ def test_calls_without_device_work():
     assert lib.tl_step(None, None, None, 0.0, None) == capi.TL_ERR_ARG
     assert lib.tl_state_get(None, 0, 0, None, None, None, None, None) == capi.TL_ERR_ARG
     assert lib.tl_system_destroy(None) == capi.TL_ERR_ARG
+    assert lib.tl_system_set_youngs(None, 0, None) == capi.TL_ERR_ARG
+    assert lib.tl_rollout_create(None, None, None, None) == capi.TL_ERR_ARG
+    assert lib.tl_rollout_forward(None, None, None) == capi.TL_ERR_ARG
+    assert lib.tl_rollout_adjoint(None, None, None, None, None, None, None) == capi.TL_ERR_ARG
+    assert lib.tl_rollout_destroy(None) == capi.TL_ERR_ARG
 
 
 def _has_gpu():
