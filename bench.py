@@ -386,6 +386,8 @@ def run_ours(args, spec, rank, world, dist):
                           "max_rel_displacement_error": worst,
                           "note": f"same workload and steps from rest in FP64; error = max over bodies of "
                                   f"max|x_mixed - x_fp64| / max|x_fp64 - X| after {args.warmup + args.steps} steps"}
+        if not args.no_converged_check:
+            result["fp64"]["converged_check"] = converged_check(meshes, mats, law, context)
     if not args.no_adjoint:
         result["adjoint"] = adjoint_ratio(precision, context)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -418,6 +420,35 @@ def run_fp64(meshes, mats, settings, args, flush, context):
     pos = [system.get_state(i).position for i in range(len(meshes))]
     system.close()
     return secs, pos
+
+
+def converged_check(meshes, mats, law, context, steps=8, tolerance=1e-6, cap=3000, sample=24):
+    """FP32-mixed against FP64 with every PCG solve converged (relative
+    residual 1e-6): the arithmetic's own error, free of the iteration cap.
+    Batches use the stiffest bodies (worst conditioned) plus evenly spaced ones."""
+    import talus_b200 as tb
+
+    idx = list(range(len(meshes)))
+    if len(meshes) > sample:
+        youngs = np.array([m[0].youngs_modulus for m in mats])
+        stiff = list(np.argsort(-youngs)[:sample // 2])
+        spread = [i for i in np.linspace(0, len(meshes) - 1, sample - len(stiff)).astype(int) if i not in stiff]
+        idx = sorted(set(stiff + spread))
+    M, Mt = [meshes[i] for i in idx], [mats[i] for i in idx]
+    settings = tb.Settings(law=law, cg_iterations=cap, tolerance=tolerance)
+    out = []
+    for prec in (tb.FP32_MIXED, tb.FP64):
+        s = tb.System(M, Mt, prec, context)
+        for i, m in enumerate(M):
+            s.set_state(tb.rest_state(m), i)
+        for _ in range(steps):
+            s.step(settings)
+        out.append([s.get_state(i).position for i in range(len(M))])
+        s.close()
+    worst = max(float(np.linalg.norm(a - b, axis=1).max() / np.linalg.norm(b - m.rest_positions, axis=1).max())
+                for a, b, m in zip(out[0], out[1], M))
+    return {"bodies": len(M), "steps": steps, "pcg_tolerance": tolerance, "pcg_cap": cap,
+            "max_rel_displacement_error": worst}
 
 
 def adjoint_ratio(precision, context, repeats=3):
@@ -453,6 +484,7 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="plastic-block")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-converged-check", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -195,6 +195,15 @@ int32_t tl_step_host(tl_system* system, uint32_t body, int32_t dtype, void* posi
 /* Default settings (Settings{} in solver.h:51-107). */
 void tl_settings_default(tl_settings* settings);
 
+/* Internal forces of one body at the positions it holds: the element pass and
+ * vertex force gather of assembleElastic (solver.cc:1354-1572) with
+ * returnMapping on and no solve.  forces: [3*nodes] (N) or NULL; yielding:
+ * [tets] 1 where the trial state lies outside the yield surface, else 0, or
+ * NULL.  Changes no state (committed rotations and plastic points are kept).
+ * For comparing the arithmetic of two systems at one configuration. */
+int32_t tl_evaluate(tl_system* system, uint32_t body, const tl_settings* settings, double* forces,
+                    uint8_t* yielding);
+
 /* Per-element Young's modulus of one body ([tets], Pa), the
  * PreparedMesh-side override that tl_mesh_desc::element_youngs sets at
  * creation; lets a caller change E between rollouts without rebuilding the

@@ -147,6 +147,7 @@ SIGNATURES = {
                      [C.POINTER(tl_settings), C.c_void_p, C.c_double, C.POINTER(tl_step_report)]),
     "tl_settings_default": (None, [C.POINTER(tl_settings)]),
     "tl_system_set_youngs": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p]),
+    "tl_evaluate": (C.c_int32, [C.c_void_p, C.c_uint32, C.POINTER(tl_settings), C.c_void_p, C.c_void_p]),
     "tl_rollout_create": (C.c_int32, [C.c_void_p, C.POINTER(tl_rollout_desc), C.POINTER(tl_settings),
                                       C.POINTER(C.c_void_p)]),
     "tl_rollout_destroy": (C.c_int32, [C.c_void_p]),

@@ -96,6 +96,24 @@ __global__ void __launch_bounds__(TILE)
   ab[n] = packc<S>(c * x1 + (h * (1.0 - st.gamma)) * v1 + (keep * c) * wb - (st.alpha_m * mass) * l);
 }
 
+// Internal node forces of the last element pass, gathered in element order.
+template <class S>
+__global__ void __launch_bounds__(TILE) kGatherForces(Sys<S> s, double* out) {
+  const uint32_t tile = blockIdx.x, b = s.node_tile_body[tile];
+  const uint32_t n = tile * TILE + threadIdx.x;
+  if (n >= s.body[b].node_end) return;
+  double f[3] = {0, 0, 0};
+  for (uint32_t k = s.start[n], k1 = s.start[n + 1]; k < k1; ++k) {
+    const Vec4<S> a = s.fe[__ldg(&s.entry[k])];
+    f[0] += double(a.x);
+    f[1] += double(a.y);
+    f[2] += double(a.z);
+  }
+  out[3 * size_t(n)] = f[0];
+  out[3 * size_t(n) + 1] = f[1];
+  out[3 * size_t(n) + 2] = f[2];
+}
+
 // Per-element E from the element's material lane (the start of an override).
 template <class S>
 __global__ void __launch_bounds__(TILE) kLaneYoungs(Sys<S> s, double* youngs) {

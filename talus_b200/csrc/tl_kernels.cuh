@@ -178,6 +178,7 @@ template <class S> struct Sys {
   const uint32_t* ns_start;    // [Vp + 1] slots beyond the first 8 (overflow CSR)
   const uint32_t* ns_slot;     // [overflow slots]
   double* blk_part;            // [3 * grid] per-block partial sums
+  uint8_t* yflag;              // [Tp] 1 where the last element pass found the trial state yielding, or null
 };
 
 constexpr int TILE_OFF_STRIDE = 4 * TILE + 4;  // 4 TILE + 1 offsets, padded to 8-byte rows
@@ -677,6 +678,7 @@ __global__ void __launch_bounds__(TILE)
       nonfinite = !finite;
     }
   }
+  if (valid && s.yflag && !(mode & EM_COMMIT)) s.yflag[e] = isYielding ? 1u : 0u;
   const uint32_t nLoading = blockCount(isLoading), nYielding = blockCount(isYielding);
   const uint32_t nGrew = blockCount(grew), nBad = blockCount(nonfinite);
   const unsigned long long jmin = blockMinKey(jkey);

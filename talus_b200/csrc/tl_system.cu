@@ -130,6 +130,7 @@ struct RolloutBase {
 struct SystemBase {
   virtual ~SystemBase() = default;
   virtual void setYoungs(uint32_t body, const double* youngs) = 0;
+  virtual void evaluate(uint32_t body, const tl_settings& settings, double* forces, uint8_t* yielding) = 0;
   virtual std::unique_ptr<RolloutBase> rollout(const tl_rollout_desc& desc, const tl_settings& settings) = 0;
   virtual void stateSet(uint32_t body, int32_t dtype, const void* x, const void* v, const void* a, const void* rot,
                         const void* plastic) = 0;
@@ -322,6 +323,7 @@ struct System final : SystemBase {
     s.cgrep = cgrep.ptr;
     s.counter = counter.ptr;
     s.sync = sync.ptr;
+    s.yflag = yflagPtr;
     return s;
   }
 
@@ -1327,6 +1329,42 @@ struct System final : SystemBase {
   }
 
   std::unique_ptr<RolloutBase> rollout(const tl_rollout_desc& desc, const tl_settings& settings) override;
+
+  // tl_evaluate: one element pass at the resident positions and the force
+  // gather, with the committed rotations put back afterwards.
+  uint8_t* yflagPtr = nullptr;
+  void evaluate(uint32_t b, const tl_settings& set, double* forces, uint8_t* yielding) override {
+    if (set.law > 1u) throw StatusError{TL_ERR_ARG, "unknown law"};
+    const BodyDev& bd = bodyHost[b];
+    const HostBody& h = hb[b];
+    BodyStepDev* hs = hStep.get(B);
+    for (uint32_t k = 0; k < B; ++k) {
+      std::memset(&hs[k], 0, sizeof(BodyStepDev));
+      hs[k].substeps = 1;
+    }
+    dStep.upload(hs, B, st);
+    DevBuf<S> keepOp;
+    keepOp.alloc(size_t(9) * Tp);
+    TL_CUDA(cudaMemcpyAsync(keepOp.ptr, op.ptr, sizeof(S) * 9 * size_t(Tp), cudaMemcpyDeviceToDevice, st));
+    DevBuf<uint8_t> flags;
+    DevBuf<double> out;
+    flags.alloc(Tp);
+    out.alloc(size_t(3) * Vp);
+    yflagPtr = flags.ptr;
+    try {
+      element(int(set.law), u.ptr, nullptr, 0, EM_MAPPING, 0.0);
+    } catch (...) {
+      yflagPtr = nullptr;
+      throw;
+    }
+    yflagPtr = nullptr;
+    kGatherForces<S><<<nodeTiles, TILE, 0, st>>>(view(), out.ptr);
+    check();
+    TL_CUDA(cudaMemcpyAsync(op.ptr, keepOp.ptr, sizeof(S) * 9 * size_t(Tp), cudaMemcpyDeviceToDevice, st));
+    if (forces) out.download(forces, size_t(3) * h.nodes, st, size_t(3) * bd.node_begin);
+    if (yielding) flags.download(yielding, h.tets, st, bd.elem_begin);
+    TL_CUDA(cudaStreamSynchronize(st));
+  }
 };
 
 // Checkpointed rollout and its adjoint (kernels and equations in
@@ -1640,6 +1678,16 @@ int32_t tl_step(tl_system* system, const tl_settings* settings, const double gra
   return guarded(system->ctx, [&]() -> int32_t {
     TL_CUDA(cudaSetDevice(system->ctx->device));
     return system->impl->step(*settings, gravity, dt, reports);
+  });
+}
+
+int32_t tl_evaluate(tl_system* system, uint32_t body, const tl_settings* settings, double* forces,
+                    uint8_t* yielding) {
+  if (!system || !settings || body >= system->impl->bodies) return TL_ERR_ARG;
+  return guarded(system->ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(system->ctx->device));
+    system->impl->evaluate(body, *settings, forces, yielding);
+    return TL_OK;
   });
 }
 

@@ -223,6 +223,16 @@ class System:
               self.context.handle)
         return out
 
+    def evaluate(self, settings: Settings, body: int = 0):
+        """Internal node forces [V,3] and per-tet yield flags [T] at the
+        positions the body holds (tl_evaluate); no state changes."""
+        m = self.meshes[body]
+        forces = np.zeros((m.nodes, 3))
+        flags = np.zeros(m.tets, np.uint8)
+        check(capi.lib().tl_evaluate(self.handle, body, C.byref(settings._c()), _ptr(forces), _ptr(flags)),
+              self.context.handle)
+        return forces, flags
+
     def set_youngs(self, youngs, body: int = 0):
         """Per-element Young's modulus of one body (tl_system_set_youngs)."""
         e = np.ascontiguousarray(youngs, np.float64)
