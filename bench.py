@@ -118,6 +118,21 @@ def tile_slots(mesh, tile=256):
     return total
 
 
+def element_bytes(T, V, s_bytes, yields, commit=False):
+    """Unique bytes of one tl::kElement launch over a body (layout in
+    talus_b200/csrc/tl_kernels.cuh).  Per element it reads the tet (16 B),
+    Dm^-1 (9 FP64 planes, 72 B), the FP64 volume (8 B), the lane (4 B) and, for
+    a yielding material, the plastic point (2 Vec4 planes); per node the
+    evaluation point (base and direction records).  An evaluation writes the
+    committed rotation (9 S), the matvec operator (9 S gradients + Vec4
+    coefficients) and the per-corner force/diagonal records (4 x (2 Vec4 + S));
+    a commit pass writes only the plastic point."""
+    v4 = 4 * s_bytes
+    reads = T * (16 + 72 + 8 + 4 + (2 * v4 if yields else 0)) + V * 2 * v4
+    writes = T * (2 * v4) if commit else T * (9 * s_bytes + 9 * s_bytes + v4 + 4 * (2 * v4 + s_bytes))
+    return reads + writes
+
+
 def pcg_bytes_per_iteration(T, V, slots, s_bytes, tangent):
     """Unique bytes one PCG iteration (tl::kPcg1 / kPcgBatch, phases A, B, C)
     must move for one body, per the layout in talus_b200/csrc/tl_kernels.cuh:
@@ -270,6 +285,7 @@ def run_ours(args, spec, rank, world, dist):
     barrier()
     step_seconds, launches = [], 0
     per_body = np.zeros((B, 4))  # cg iterations, tangent iterations, solves, plastic evaluations
+    reps_substeps = np.zeros(B)
     totals = {"element": 0.0, "assemble": 0.0, "pcg": 0.0}
     with ClockSampler(device) as clocks:
         for _ in range(args.steps):
@@ -284,6 +300,7 @@ def run_ours(args, spec, rank, world, dist):
             for b in range(B):
                 per_body[b] += (reps[b].cg_iterations, reps[b].cg_tangent_iterations, reps[b].cg_solves,
                                 reps[b].plastic_evaluations)
+                reps_substeps[b] += reps[b].substeps
         barrier()
     total_seconds = max_over_ranks(sum(step_seconds))
     value = world * T * args.steps / total_seconds
@@ -368,6 +385,7 @@ def run_ours(args, spec, rank, world, dist):
                      "iterations": int(per_body[:, 0].max()),
                      "algorithmic_bytes_per_launch": pcg_bytes / max(1, launches_pcg),
                      "avg_launch_ms": pcg_time * 1e3 / max(1, launches_pcg)},
+        "element_pass": element_roofline(meshes, mats, per_body, reps_substeps, s_bytes, totals["element"], peak),
         "breakdown_ms_per_step": {k: v * 1e3 / args.steps for k, v in totals.items()},
         "solver": {"cg_iterations_per_step": float(per_body[:, 0].sum() / args.steps),
                    "plastic_evaluations_per_step": float(per_body[:, 3].sum() / args.steps)},
@@ -397,6 +415,27 @@ def run_ours(args, spec, rank, world, dist):
         print(json.dumps(result), flush=True)
     system.close()
     context.close()
+
+
+def element_roofline(meshes, mats, per_body, substeps, s_bytes, seconds, peak):
+    """Element pass (tl::kElement): algorithmic bytes of every launch in the
+    timed steps over the summed CUDA-event time of those launches.  Elastic
+    bodies take 3 evaluations per substep; yielding bodies take their Newton
+    evaluations plus one commit pass per substep."""
+    if seconds <= 0:
+        return None
+    total, launches = 0.0, 0.0
+    for b, m in enumerate(meshes):
+        yields = any(np.isfinite(x.yield_stress) and x.yield_stress > 0 for x in mats[b])
+        evals = per_body[b, 3] if yields else 3 * substeps[b]
+        total += evals * element_bytes(m.tets, m.nodes, s_bytes, yields)
+        if yields:
+            total += substeps[b] * element_bytes(m.tets, m.nodes, s_bytes, yields, commit=True)
+        launches = max(launches, evals + (substeps[b] if yields else 0))
+    achieved = total / seconds / 1e9
+    return {"kernel": "tl::kElement", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "launches": int(launches), "avg_launch_us": seconds * 1e6 / max(1.0, launches),
+            "algorithmic_bytes": total}
 
 
 def run_fp64(meshes, mats, settings, args, flush, context):

@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(TILE) kAdjointElement(Sys<S> s, const Vec4<S>*
   for (int c = 0; c < 4; ++c) {
     const Vec4<S> l = lam[nodes[c]];
     p[c] = xyz(l);
-    const Vec4<S> f = s.fe[4 * e + c];
+    const Vec4<S> f = s.fe[size_t(c) * s.Tp + e];
     eb += double(f.x) * double(l.x) + double(f.y) * double(l.y) + double(f.z) * double(l.z);
   }
   elementApply<S, LAW, false>(s, e, p, y);
@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(TILE) kGatherForces(Sys<S> s, double* out) {
   if (n >= s.body[b].node_end) return;
   double f[3] = {0, 0, 0};
   for (uint32_t k = s.start[n], k1 = s.start[n + 1]; k < k1; ++k) {
-    const Vec4<S> a = s.fe[__ldg(&s.entry[k])];
+    const Vec4<S> a = s.fe[cornerAt(__ldg(&s.entry[k]), s.Tp)];
     f[0] += double(a.x);
     f[1] += double(a.y);
     f[2] += double(a.z);

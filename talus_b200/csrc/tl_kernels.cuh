@@ -150,9 +150,9 @@ template <class S> struct Sys {
   Vec4<S>* oc;            // matvec coefficients (a, b, c, -), h_eff^2 V folded in
   Vec4<S>* on;            // 2 planes: rotated flow normal (xx, yy, zz, xy), (xz, yz, -, -)
   Vec4<S>* plast;         // 2 planes: (exx, eyy, ezz, exy), (exz, eyz, equivalent, -)
-  Vec4<S>* fe;            // [4 Tp] (fx, fy, fz, Dxx)
-  Vec4<S>* de;            // [4 Tp] (Dyy, Dzz, Dxy, Dxz)
-  S* de2;                 // [4 Tp] Dyz
+  Vec4<S>* fe;            // [4][Tp] corner planes: (fx, fy, fz, Dxx)
+  Vec4<S>* de;            // [4][Tp] (Dyy, Dzz, Dxy, Dxz)
+  S* de2;                 // [4][Tp] Dyz
   Vec4<S>* ye;            // [4 Tp] matvec products
   // reductions
   double* part;           // [node_tiles * 4] PCG partials
@@ -182,6 +182,12 @@ template <class S> struct Sys {
 };
 
 constexpr int TILE_OFF_STRIDE = 4 * TILE + 4;  // 4 TILE + 1 offsets, padded to 8-byte rows
+
+// Position of the (element, corner) record q = 4 e + c in the corner-major
+// planes of fe / de / de2 (a warp's stores of one corner are contiguous).
+__host__ __device__ __forceinline__ size_t cornerAt(uint32_t q, uint32_t Tp) {
+  return size_t(q & 3u) * Tp + (q >> 2);
+}
 constexpr uint32_t NO_SLOT = 0xffffffffu;
 
 // ------------------------------------------------------------ helpers ----
@@ -460,8 +466,11 @@ enum ElementMode : uint32_t {
 // Kinematics and the law run in FP64 whatever S is; outputs are stored in S.
 // Positions are base + reach * dir (the reference's `evaluated`), in
 // displacement form.
+#ifndef TL_ELEMENT_MIN_BLOCKS
+#define TL_ELEMENT_MIN_BLOCKS 2  // resident 256-thread blocks per SM the element pass is compiled for
+#endif
 template <class S, int LAW>
-__global__ void __launch_bounds__(TILE)
+__global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
     kElement(Sys<S> s, const Vec4<S>* base, const Vec4<S>* dir, uint32_t pass, uint32_t mode, double margin) {
   const uint32_t tile = blockIdx.x, b = s.elem_tile_body[tile];
   if (!bodyActive(s, b, pass)) return;
@@ -477,49 +486,44 @@ __global__ void __launch_bounds__(TILE)
     const uint32_t nodes[4] = {t.x, t.y, t.z, t.w};
     V3<double> g[4];
     gradientsOf<S>(s.dm, s.Tp, e, g);
-    V3<double> X[4], U[4];
+    M3<double> H = zero3<double>();  // displacement gradient, F = I + H
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       const uint32_t n = nodes[c];
-      X[c] = cvt<double>(xyz(ld4g(&s.rest4[n])));
       V3<double> uu = cvt<double>(xyz(base[n]));
       if (dir) uu = uu + reach * cvt<double>(xyz(dir[n]));
-      U[c] = uu;
+      addOuter(H, uu, g[c]);
     }
-    M3<double> H = zero3<double>();
-#pragma unroll
-    for (int c = 0; c < 4; ++c) addOuter(H, U[c], g[c]);
     const double vol = s.vold[e];
     const MatDev m = s.mat[s.lane[e]];
     const double youngs = s.eyoung ? s.eyoung[e] : m.youngs;
     const double lam = youngs * m.lam_unit, mu = youngs * m.mu_unit;
     const double change = volumeChange(H);
     jkey = minKey(1.0 + change);
-    V3<double> force[4];
-    Sym<double> diag[4];
     bool finite = true;
+    // per-corner force and diagonal block, stored as soon as they are formed
+    auto emit = [&](int c, const V3<double>& f, const Sym<double>& d) {
+      finite = finite && isfinite(f.x) && isfinite(f.y) && isfinite(f.z);
+      const size_t at = size_t(c) * s.Tp + e;
+      s.fe[at] = Vec4<S>{S(f.x), S(f.y), S(f.z), S(d.xx)};
+      s.de[at] = Vec4<S>{S(d.yy), S(d.zz), S(d.xy), S(d.xz)};
+      s.de2[at] = S(d.yz);
+    };
     if (LAW == 0) {
       M3<double> F = H;
       F.m[0][0] += 1.0;
       F.m[1][1] += 1.0;
       F.m[2][2] += 1.0;
       const M3<double> R = elementRotation(F, true);
-      // corotated offsets (material.cc:92-109), strain (material.cc:155-161)
-      V3<double> xc = {0, 0, 0}, uc = {0, 0, 0};
+      // Corotated strain (material.cc:92-109, 155-161): the offsets
+      // R^T (x_c - x_mean) - (X_c - X_mean) summed against g_c.  Because
+      // sum_c g_c = 0 and sum_c X_c g_c^T = Ds Dm^-1 = I, that sum is
+      // R^T F - I = R^T H + (R^T - I), formed here without the rest positions.
+      M3<double> D = mul(transpose(R), H);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        xc = xc + X[c];
-        uc = uc + U[c];
-      }
-      xc = 0.25 * xc;
-      uc = 0.25 * uc;
-      M3<double> D = zero3<double>();
+      for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const V3<double> rel = X[c] - xc;
-        const V3<double> off = mulT(R, rel + (U[c] - uc)) - rel;
-        addOuter(D, off, g[c]);
-      }
+        for (int j = 0; j < 3; ++j) D.m[i][j] += R.m[j][i] - (i == j ? 1.0 : 0.0);
       const Sym<double> eps = symOf(D);
       const bool yields = m.yields != 0u;
       const double bulk = lam + 2.0 * mu / 3.0;
@@ -590,15 +594,15 @@ __global__ void __launch_bounds__(TILE)
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
           const V3<double> w = symMul(stress, g[c]);
-          force[c] = -(vol * mul(R, w));  // material.cc:1019-1027
+          const V3<double> force = -(vol * mul(R, w));  // material.cc:1019-1027
           // R K_cc R^T with K_cc = V[(K + mu theta/3) g g^T + mu theta |g|^2 I - 2 mu thetaBar (n g)(n g)^T]
           const V3<double> rg = mul(R, g[c]);
           const V3<double> rn = mul(R, symMul(normal, g[c]));
           const double k1 = vol * (bulk + mu * th / 3.0), k2 = vol * mu * th * dot(g[c], g[c]);
           const double k3 = -vol * 2.0 * mu * thb;
-          diag[c] = {k1 * rg.x * rg.x + k2 + k3 * rn.x * rn.x, k1 * rg.y * rg.y + k2 + k3 * rn.y * rn.y,
-                     k1 * rg.z * rg.z + k2 + k3 * rn.z * rn.z, k1 * rg.x * rg.y + k3 * rn.x * rn.y,
-                     k1 * rg.x * rg.z + k3 * rn.x * rn.z, k1 * rg.y * rg.z + k3 * rn.y * rn.z};
+          emit(c, force, {k1 * rg.x * rg.x + k2 + k3 * rn.x * rn.x, k1 * rg.y * rg.y + k2 + k3 * rn.y * rn.y,
+                          k1 * rg.z * rg.z + k2 + k3 * rn.z * rn.z, k1 * rg.x * rg.y + k3 * rn.x * rn.y,
+                          k1 * rg.x * rg.z + k3 * rn.x * rn.z, k1 * rg.y * rg.z + k3 * rn.y * rn.z});
         }
 #pragma unroll
         for (int i = 0; i < 3; ++i)
@@ -644,13 +648,14 @@ __global__ void __launch_bounds__(TILE)
           P.m[i][j] = mu * (H.m[i][j] + H.m[j][i] - (i == j ? trH : 0.0) - CH.m[i][j]) + shifted * change * C.m[i][j];
       const double squared = contract(H, H);
       energy = vol * (0.5 * mu * squared - mu * (change - trH) + 0.5 * shifted * change * change);
+      if (!(mode & EM_COMMIT)) {
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        force[c] = -(vol * mul(P, g[c]));
-        const V3<double> bb = mul(C, g[c]);
-        const double k2 = vol * mu * dot(g[c], g[c]), k1 = vol * shifted;
-        diag[c] = {k1 * bb.x * bb.x + k2, k1 * bb.y * bb.y + k2, k1 * bb.z * bb.z + k2,
-                   k1 * bb.x * bb.y, k1 * bb.x * bb.z, k1 * bb.y * bb.z};
+        for (int c = 0; c < 4; ++c) {
+          const V3<double> bb = mul(C, g[c]);
+          const double k2 = vol * mu * dot(g[c], g[c]), k1 = vol * shifted;
+          emit(c, -(vol * mul(P, g[c])), {k1 * bb.x * bb.x + k2, k1 * bb.y * bb.y + k2, k1 * bb.z * bb.z + k2,
+                                          k1 * bb.x * bb.y, k1 * bb.x * bb.z, k1 * bb.y * bb.z});
+        }
       }
 #pragma unroll
       for (int i = 0; i < 3; ++i)
@@ -667,35 +672,55 @@ __global__ void __launch_bounds__(TILE)
       }
       s.oc[e] = Vec4<S>{S(sv * mu), S(sv * (shifted * change - mu)), S(sv * shifted), S(0)};
     }
-    if (!(mode & EM_COMMIT)) {
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        finite = finite && isfinite(force[c].x) && isfinite(force[c].y) && isfinite(force[c].z);
-        s.fe[4 * e + c] = Vec4<S>{S(force[c].x), S(force[c].y), S(force[c].z), S(diag[c].xx)};
-        s.de[4 * e + c] = Vec4<S>{S(diag[c].yy), S(diag[c].zz), S(diag[c].xy), S(diag[c].xz)};
-        s.de2[4 * e + c] = S(diag[c].yz);
-      }
-      nonfinite = !finite;
-    }
+    if (!(mode & EM_COMMIT)) nonfinite = !finite;
   }
   if (valid && s.yflag && !(mode & EM_COMMIT)) s.yflag[e] = isYielding ? 1u : 0u;
-  const uint32_t nLoading = blockCount(isLoading), nYielding = blockCount(isYielding);
-  const uint32_t nGrew = blockCount(grew), nBad = blockCount(nonfinite);
-  const unsigned long long jmin = blockMinKey(jkey);
-  if (threadIdx.x == 0) {
-    if (mode & EM_COMMIT) {
-      if (nGrew) atomicOr(&s.acc[b].grew, 1u);
-    } else {
-      if (nLoading) atomicAdd(&s.loading[b], nLoading);
-      if (nYielding) atomicAdd(&s.yielding[b], nYielding);
-      if (nBad) atomicOr(&s.acc[b].nonfinite, 1u);
-      atomicMin(&s.acc[b].min_j_key, jmin);
-    }
+  // All per-tile results in one fixed-order block reduction (one barrier):
+  // counts by warp ballots, the smallest J key and the energy by shuffles,
+  // then warps in order in thread 0.
+  __shared__ double redEnergy[TILE / 32];
+  __shared__ unsigned long long redKey[TILE / 32];
+  __shared__ uint32_t redCount[TILE / 32][4];
+  const unsigned full = 0xffffffffu;
+  const uint32_t c0 = __popc(__ballot_sync(full, isLoading)), c1 = __popc(__ballot_sync(full, isYielding));
+  const uint32_t c2 = __popc(__ballot_sync(full, grew)), c3 = __popc(__ballot_sync(full, nonfinite));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    energy += __shfl_down_sync(full, energy, o);
+    const unsigned long long q = __shfl_down_sync(full, jkey, o);
+    jkey = q < jkey ? q : jkey;
   }
-  if (mode & EM_COMMIT) return;
-  double v[1] = {energy};
-  blockSum<1>(v);
-  if (threadIdx.x == 0) s.epart[tile] = v[0];
+  const int warp = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    redEnergy[warp] = energy;
+    redKey[warp] = jkey;
+    redCount[warp][0] = c0;
+    redCount[warp][1] = c1;
+    redCount[warp][2] = c2;
+    redCount[warp][3] = c3;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double sum = 0.0;
+  unsigned long long jmin = ~0ull;
+  uint32_t nLoading = 0, nYielding = 0, nGrew = 0, nBad = 0;
+  for (int w = 0; w < TILE / 32; ++w) {
+    sum += redEnergy[w];
+    jmin = redKey[w] < jmin ? redKey[w] : jmin;
+    nLoading += redCount[w][0];
+    nYielding += redCount[w][1];
+    nGrew += redCount[w][2];
+    nBad += redCount[w][3];
+  }
+  if (mode & EM_COMMIT) {
+    if (nGrew) atomicOr(&s.acc[b].grew, 1u);
+    return;
+  }
+  if (nLoading) atomicAdd(&s.loading[b], nLoading);
+  if (nYielding) atomicAdd(&s.yielding[b], nYielding);
+  if (nBad) atomicOr(&s.acc[b].nonfinite, 1u);
+  atomicMin(&s.acc[b].min_j_key, jmin);
+  s.epart[tile] = sum;
 }
 
 // Node gather + balance (solver.cc:3746-3806) + guardPreconditioner
@@ -715,8 +740,9 @@ __global__ void __launch_bounds__(TILE) kNodeAssemble(Sys<S> s, const Vec4<S>* t
     const uint32_t k0 = s.start[n], k1 = s.start[n + 1];
     for (uint32_t k = k0; k < k1; ++k) {
       const uint32_t q = __ldg(&s.entry[k]);
-      const Vec4<S> a = s.fe[q], c = s.de[q];
-      const S c2 = s.de2[q];
+      const size_t at = cornerAt(q, s.Tp);
+      const Vec4<S> a = s.fe[at], c = s.de[at];
+      const S c2 = s.de2[at];
       f[0] += double(a.x);
       f[1] += double(a.y);
       f[2] += double(a.z);

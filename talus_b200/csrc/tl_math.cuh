@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cmath>
+#include <type_traits>
 
 #define TL_HD __host__ __device__ __forceinline__
 
@@ -220,10 +221,22 @@ template <class T> TL_HD M3<T> invertibleRotation(const M3<T>& fin) {
   return r;
 }
 
+#ifdef __CUDACC__
+// Out of line on the device: only inverted elements take this branch, and
+// inlined it would hold its Jacobi arrays and registers in every element
+// thread's frame.
+static __device__ __noinline__ M3<double> invertibleRotationOutOfLine(M3<double> f) {
+  return invertibleRotation(f);
+}
+#endif
+
 // material.cc:24-27: polar unless the element is inverted and the caller
 // asked for the invertible rotation.
 template <class T> TL_HD M3<T> elementRotation(const M3<T>& f, bool invertible) {
   if (!invertible || det3(f) > T(0)) return polarRotation(f);
+#ifdef __CUDA_ARCH__
+  if constexpr (std::is_same_v<T, double>) return invertibleRotationOutOfLine(f);
+#endif
   return invertibleRotation(f);
 }
 
