@@ -484,15 +484,17 @@ __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
     const double reach = dir ? st.scale : 0.0;
     const uint4 t = __ldg(&s.tet[e]);
     const uint32_t nodes[4] = {t.x, t.y, t.z, t.w};
-    V3<double> g[4];
-    gradientsOf<S>(s.dm, s.Tp, e, g);
     M3<double> H = zero3<double>();  // displacement gradient, F = I + H
+    {
+      V3<double> g0[4];
+      gradientsOf<S>(s.dm, s.Tp, e, g0);
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const uint32_t n = nodes[c];
-      V3<double> uu = cvt<double>(xyz(base[n]));
-      if (dir) uu = uu + reach * cvt<double>(xyz(dir[n]));
-      addOuter(H, uu, g[c]);
+      for (int c = 0; c < 4; ++c) {
+        const uint32_t n = nodes[c];
+        V3<double> uu = cvt<double>(xyz(base[n]));
+        if (dir) uu = uu + reach * cvt<double>(xyz(dir[n]));
+        addOuter(H, uu, g0[c]);
+      }
     }
     const double vol = s.vold[e];
     const MatDev m = s.mat[s.lane[e]];
@@ -502,7 +504,9 @@ __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
     jkey = minKey(1.0 + change);
     bool finite = true;
     // per-corner force and diagonal block, stored as soon as they are formed
-    auto emit = [&](int c, const V3<double>& f, const Sym<double>& d) {
+    // (forces in FP64; the diagonal blocks, like the matvec operator, are formed
+    // in the storage type S: they only precondition and are stored as S)
+    auto emit = [&](int c, const V3<double>& f, const Sym<S>& d) {
       finite = finite && isfinite(f.x) && isfinite(f.y) && isfinite(f.z);
       const size_t at = size_t(c) * s.Tp + e;
       s.fe[at] = Vec4<S>{S(f.x), S(f.y), S(f.z), S(d.xx)};
@@ -525,6 +529,20 @@ __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
 #pragma unroll
         for (int j = 0; j < 3; ++j) D.m[i][j] += R.m[j][i] - (i == j ? 1.0 : 0.0);
       const Sym<double> eps = symOf(D);
+      // The gradients are loaded again rather than kept live through the
+      // rotation; the empty asm keeps the compiler from merging the loads.
+      asm volatile("" ::: "memory");
+      V3<double> g[4];
+      {
+        const double* dmp = s.dm;
+        double d[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) d[k] = dmp[size_t(k) * s.Tp + e];
+        g[1] = {d[0], d[1], d[2]};
+        g[2] = {d[3], d[4], d[5]};
+        g[3] = {d[6], d[7], d[8]};
+        g[0] = -(g[1] + g[2] + g[3]);
+      }
       const bool yields = m.yields != 0u;
       const double bulk = lam + 2.0 * mu / 3.0;
       Sym<double> stress;
@@ -591,15 +609,22 @@ __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
         const bool tangentDiag = (mode & EM_CONSISTENT) && yields;
         const double th = tangentDiag ? theta : 1.0;
         const double thb = tangentDiag ? thetaBar : 0.0;
+        M3<S> Rw;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) Rw.m[i][j] = S(R.m[i][j]);
+        const Sym<S> nw = {S(normal.xx), S(normal.yy), S(normal.zz), S(normal.xy), S(normal.xz), S(normal.yz)};
+        const S k1 = S(vol * (bulk + mu * th / 3.0)), kmu = S(vol * mu * th), k3 = S(-vol * 2.0 * mu * thb);
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
           const V3<double> w = symMul(stress, g[c]);
           const V3<double> force = -(vol * mul(R, w));  // material.cc:1019-1027
           // R K_cc R^T with K_cc = V[(K + mu theta/3) g g^T + mu theta |g|^2 I - 2 mu thetaBar (n g)(n g)^T]
-          const V3<double> rg = mul(R, g[c]);
-          const V3<double> rn = mul(R, symMul(normal, g[c]));
-          const double k1 = vol * (bulk + mu * th / 3.0), k2 = vol * mu * th * dot(g[c], g[c]);
-          const double k3 = -vol * 2.0 * mu * thb;
+          const V3<S> gc = cvt<S>(g[c]);
+          const V3<S> rg = mul(Rw, gc);
+          const V3<S> rn = mul(Rw, symMul(nw, gc));
+          const S k2 = kmu * dot(gc, gc);
           emit(c, force, {k1 * rg.x * rg.x + k2 + k3 * rn.x * rn.x, k1 * rg.y * rg.y + k2 + k3 * rn.y * rn.y,
                           k1 * rg.z * rg.z + k2 + k3 * rn.z * rn.z, k1 * rg.x * rg.y + k3 * rn.x * rn.y,
                           k1 * rg.x * rg.z + k3 * rn.x * rn.z, k1 * rg.y * rg.z + k3 * rn.y * rn.z});
@@ -614,24 +639,26 @@ __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
         const double sv = st.scale * vol;
 #pragma unroll
         for (int k = 1; k < 4; ++k) {
-          const V3<double> gh = mul(R, g[k]);
-          s.og[size_t(3 * (k - 1) + 0) * s.Tp + e] = S(gh.x);
-          s.og[size_t(3 * (k - 1) + 1) * s.Tp + e] = S(gh.y);
-          s.og[size_t(3 * (k - 1) + 2) * s.Tp + e] = S(gh.z);
+          const V3<S> gh = mul(Rw, cvt<S>(g[k]));
+          s.og[size_t(3 * (k - 1) + 0) * s.Tp + e] = gh.x;
+          s.og[size_t(3 * (k - 1) + 1) * s.Tp + e] = gh.y;
+          s.og[size_t(3 * (k - 1) + 2) * s.Tp + e] = gh.z;
         }
         s.oc[e] = Vec4<S>{S(sv * (bulk - 2.0 * mu * th / 3.0)), S(sv * 2.0 * mu * th), S(sv * 2.0 * mu * thb), S(0)};
         if (mode & EM_CONSISTENT) {
-          M3<double> nm;
-          nm.m[0][0] = normal.xx; nm.m[1][1] = normal.yy; nm.m[2][2] = normal.zz;
-          nm.m[0][1] = nm.m[1][0] = normal.xy;
-          nm.m[0][2] = nm.m[2][0] = normal.xz;
-          nm.m[1][2] = nm.m[2][1] = normal.yz;
-          const M3<double> nh = mul(mul(R, nm), transpose(R));
-          s.on[e] = Vec4<S>{S(nh.m[0][0]), S(nh.m[1][1]), S(nh.m[2][2]), S(nh.m[0][1])};
-          s.on[s.Tp + e] = Vec4<S>{S(nh.m[0][2]), S(nh.m[1][2]), S(0), S(0)};
+          M3<S> nm;
+          nm.m[0][0] = nw.xx; nm.m[1][1] = nw.yy; nm.m[2][2] = nw.zz;
+          nm.m[0][1] = nm.m[1][0] = nw.xy;
+          nm.m[0][2] = nm.m[2][0] = nw.xz;
+          nm.m[1][2] = nm.m[2][1] = nw.yz;
+          const M3<S> nh = mul(mul(Rw, nm), transpose(Rw));
+          s.on[e] = Vec4<S>{nh.m[0][0], nh.m[1][1], nh.m[2][2], nh.m[0][1]};
+          s.on[s.Tp + e] = Vec4<S>{nh.m[0][2], nh.m[1][2], S(0), S(0)};
         }
       }
     } else {
+      V3<double> g[4];
+      gradientsOf<S>(s.dm, s.Tp, e, g);
       // SNH: P = mu (H + H^T - tr H I - cof H) + (lambda + mu)(J - 1) cof F
       M3<double> F = H;
       F.m[0][0] += 1.0;
@@ -651,8 +678,8 @@ __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
       if (!(mode & EM_COMMIT)) {
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-          const V3<double> bb = mul(C, g[c]);
-          const double k2 = vol * mu * dot(g[c], g[c]), k1 = vol * shifted;
+          const V3<S> bb = cvt<S>(mul(C, g[c]));
+          const S k2 = S(vol * mu * dot(g[c], g[c])), k1 = S(vol * shifted);
           emit(c, -(vol * mul(P, g[c])), {k1 * bb.x * bb.x + k2, k1 * bb.y * bb.y + k2, k1 * bb.z * bb.z + k2,
                                           k1 * bb.x * bb.y, k1 * bb.x * bb.z, k1 * bb.y * bb.z});
         }
@@ -816,11 +843,107 @@ static __global__ void __launch_bounds__(TILE) kFinalize(const BodyDev* body, co
 // gh = R g:  Q = sum_b p_b gh_b^T, e = sym(Q), sigma = a tr(e) I + b e -
 // c (nh : e) nh, y_a = sigma gh_a.  LAW 1: the exact SNH tangent dP(dF) g_a
 // with dF = sum_b p_b g_b^T.  (a, b, c) carry h_eff^2 V.  Arithmetic in S.
-template <class S, int LAW, bool TANGENT>
-__device__ __forceinline__ void elementApply(const Sys<S>& s, uint32_t e, const V3<S> p[4], V3<S> y[4]) {
+// The per-element matvec operator: rotated gradients gh_1..3 (g_0 = -sum),
+// coefficients k, and the flow normal (corotated tangent) or F (SNH).
+template <class S> struct ElementOperator {
   V3<S> g[4];
-  gradientsS<S>(s.og, s.Tp, e, g);
-  const Vec4<S> k = ld4g(&s.oc[e]);
+  Vec4<S> k;
+  Sym<S> n;
+  M3<S> F;
+};
+
+template <class S, int LAW, bool TANGENT>
+__device__ __forceinline__ ElementOperator<S> loadOperator(const Sys<S>& s, uint32_t e) {
+  ElementOperator<S> o;
+  gradientsS<S>(s.og, s.Tp, e, o.g);
+  o.k = ld4g(&s.oc[e]);
+  if (LAW == 0 && TANGENT) {
+    const Vec4<S> n0 = ld4g(&s.on[e]), n1 = ld4g(&s.on[s.Tp + e]);
+    o.n = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y};
+  }
+  if (LAW == 1) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) o.F.m[i][j] = __ldg(s.op + size_t(3 * i + j) * s.Tp + e);
+  }
+  return o;
+}
+
+// ---- shared-memory stage of one tile's operators, filled by cp.async ----
+// Layout: og [9][TILE] S, oc [TILE] Vec4<S>, then op [9][TILE] S (SNH) or
+// on [2][TILE] Vec4<S> (corotated tangent).  Thread t copies and later reads
+// only element t's entries, so its own cp.async.wait_group orders them.
+template <class S, int LAW, bool TANGENT> __host__ __device__ constexpr size_t stageBytes() {
+  return sizeof(S) * 9 * TILE + sizeof(Vec4<S>) * TILE +
+         (LAW == 1 ? sizeof(S) * 9 * TILE : (TANGENT ? sizeof(Vec4<S>) * 2 * TILE : 0));
+}
+template <int N> __device__ __forceinline__ void cpAsync(void* dst, const void* src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  if constexpr (N == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(N) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+template <class S, int LAW, bool TANGENT>
+__device__ __forceinline__ void stageOperator(const Sys<S>& s, uint32_t e, unsigned char* stage) {
+  const uint32_t t = threadIdx.x;
+  S* og = reinterpret_cast<S*>(stage);
+  Vec4<S>* oc = reinterpret_cast<Vec4<S>*>(stage + sizeof(S) * 9 * TILE);
+  unsigned char* extra = stage + sizeof(S) * 9 * TILE + sizeof(Vec4<S>) * TILE;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) cpAsync<sizeof(S)>(og + k * TILE + t, s.og + size_t(k) * s.Tp + e);
+#pragma unroll
+  for (int h = 0; h < int(sizeof(Vec4<S>) / 16); ++h)
+    cpAsync<16>(reinterpret_cast<unsigned char*>(oc + t) + 16 * h, reinterpret_cast<const unsigned char*>(s.oc + e) + 16 * h);
+  if (LAW == 1) {
+    S* op = reinterpret_cast<S*>(extra);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) cpAsync<sizeof(S)>(op + k * TILE + t, s.op + size_t(k) * s.Tp + e);
+  } else if (TANGENT) {
+    Vec4<S>* on = reinterpret_cast<Vec4<S>*>(extra);
+#pragma unroll
+    for (int q = 0; q < 2; ++q)
+#pragma unroll
+      for (int h = 0; h < int(sizeof(Vec4<S>) / 16); ++h)
+        cpAsync<16>(reinterpret_cast<unsigned char*>(on + q * TILE + t) + 16 * h,
+                    reinterpret_cast<const unsigned char*>(s.on + size_t(q) * s.Tp + e) + 16 * h);
+  }
+}
+
+template <class S, int LAW, bool TANGENT>
+__device__ __forceinline__ ElementOperator<S> stagedOperator(const unsigned char* stage) {
+  const uint32_t t = threadIdx.x;
+  const S* og = reinterpret_cast<const S*>(stage);
+  const Vec4<S>* oc = reinterpret_cast<const Vec4<S>*>(stage + sizeof(S) * 9 * TILE);
+  const unsigned char* extra = stage + sizeof(S) * 9 * TILE + sizeof(Vec4<S>) * TILE;
+  ElementOperator<S> o;
+  o.g[1] = {og[0 * TILE + t], og[1 * TILE + t], og[2 * TILE + t]};
+  o.g[2] = {og[3 * TILE + t], og[4 * TILE + t], og[5 * TILE + t]};
+  o.g[3] = {og[6 * TILE + t], og[7 * TILE + t], og[8 * TILE + t]};
+  o.g[0] = -(o.g[1] + o.g[2] + o.g[3]);
+  o.k = oc[t];
+  if (LAW == 1) {
+    const S* op = reinterpret_cast<const S*>(extra);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) o.F.m[i][j] = op[(3 * i + j) * TILE + t];
+  } else if (TANGENT) {
+    const Vec4<S>* on = reinterpret_cast<const Vec4<S>*>(extra);
+    const Vec4<S> n0 = on[t], n1 = on[TILE + t];
+    o.n = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y};
+  }
+  return o;
+}
+
+template <class S, int LAW, bool TANGENT>
+__device__ __forceinline__ void applyOperator(const ElementOperator<S>& o, const V3<S> p[4], V3<S> y[4]) {
+  const V3<S>* g = o.g;
+  const Vec4<S> k = o.k;
   M3<S> Q = zero3<S>();
 #pragma unroll
   for (int c = 1; c < 4; ++c) addOuter(Q, p[c] - p[0], g[c]);  // sum_c g_c = 0
@@ -830,8 +953,7 @@ __device__ __forceinline__ void elementApply(const Sys<S>& s, uint32_t e, const 
     const S at = k.x * tr;
     Sym<S> sig = {at + k.y * eps.xx, at + k.y * eps.yy, at + k.y * eps.zz, k.y * eps.xy, k.y * eps.xz, k.y * eps.yz};
     if (TANGENT) {
-      const Vec4<S> n0 = ld4g(&s.on[e]), n1 = ld4g(&s.on[s.Tp + e]);
-      const Sym<S> n = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y};
+      const Sym<S>& n = o.n;
       const S ne = k.z * symContract(n, eps);
       sig.xx -= ne * n.xx;
       sig.yy -= ne * n.yy;
@@ -843,11 +965,7 @@ __device__ __forceinline__ void elementApply(const Sys<S>& s, uint32_t e, const 
 #pragma unroll
     for (int c = 1; c < 4; ++c) y[c] = symMul(sig, g[c]);
   } else {
-    M3<S> F;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int j = 0; j < 3; ++j) F.m[i][j] = __ldg(s.op + size_t(3 * i + j) * s.Tp + e);
+    const M3<S>& F = o.F;
     const M3<S> C = cofactor(F);
     const S kk = k.z * contract(C, Q);
     // column j of cof F is F_{j+1} x F_{j+2}; its differential along Q
@@ -866,6 +984,11 @@ __device__ __forceinline__ void elementApply(const Sys<S>& s, uint32_t e, const 
     for (int c = 1; c < 4; ++c) y[c] = mul(dP, g[c]);
   }
   y[0] = -(y[1] + y[2] + y[3]);
+}
+
+template <class S, int LAW, bool TANGENT>
+__device__ __forceinline__ void elementApply(const Sys<S>& s, uint32_t e, const V3<S> p[4], V3<S> y[4]) {
+  applyOperator<S, LAW, TANGENT>(loadOperator<S, LAW, TANGENT>(s, e), p, y);
 }
 
 // Reads a body's PCG scalars from L2 (they are written by other blocks).
@@ -1180,16 +1303,25 @@ __device__ __forceinline__ double sumBlocks(const double* part, unsigned int fie
 // staged once in shared memory (p = z + blend p_prev formed once per node, or
 // X for the initial residual), elements read their corners from there by
 // local index, and the tile's local CSR is fetched while the elements compute.
-template <class S, int LAW, bool TANGENT>
+// STAGE: copy the element operators into shared memory (cp.async) while the
+// nodes are staged.  It pays on large batched systems (more loads in flight,
+// fewer registers); the single-body kernel, latency-bound on few tiles per
+// block, is faster loading them directly (measured on B200).
+template <class S, int LAW, bool TANGENT, bool STAGE>
 __device__ __forceinline__ void matvecTile(const Sys<S>& s, uint32_t tile, const Vec4<S>* X, S blend,
-                                           S (*buf)[4 * TILE], uint16_t* sOff, uint16_t* sEnt, uint32_t elemEnd) {
+                                           S (*buf)[4 * TILE], uint16_t* sOff, uint16_t* sEnt, uint32_t elemEnd,
+                                           unsigned char* stage) {
   const uint32_t e = tile * TILE + threadIdx.x;
+  const bool live = e < elemEnd;
+  if (STAGE) {
+    if (live) stageOperator<S, LAW, TANGENT>(s, e, stage);
+    cpAsyncCommit();
+  }
   const uint2 meta = __ldg(&s.tile_meta[tile]);
   const uint2 entv = __ldg(reinterpret_cast<const uint2*>(s.tile_ent + size_t(tile) * 4 * TILE) + threadIdx.x);
   const uint16_t* off = s.tile_off + size_t(tile) * TILE_OFF_STRIDE;
   const uint2 offv = __ldg(reinterpret_cast<const uint2*>(off) + threadIdx.x);
   const uint16_t offLast = threadIdx.x == 0 ? __ldg(&off[4 * TILE]) : uint16_t(0);
-  const bool live = e < elemEnd;
   const uint2 loc = live ? __ldg(&s.eloc[e]) : make_uint2(0u, 0u);
   // stage the tile's nodes: buf[k][j] = component k of node j
   for (uint32_t j = threadIdx.x; j < meta.y; j += TILE) {
@@ -1208,7 +1340,12 @@ __device__ __forceinline__ void matvecTile(const Sys<S>& s, uint32_t tile, const
     V3<S> pe[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) pe[c] = {buf[0][l[c]], buf[1][l[c]], buf[2][l[c]]};
-    elementApply<S, LAW, TANGENT>(s, e, pe, y);
+    if (STAGE) {
+      cpAsyncWaitAll();
+      applyOperator<S, LAW, TANGENT>(stagedOperator<S, LAW, TANGENT>(stage), pe, y);
+    } else {
+      elementApply<S, LAW, TANGENT>(s, e, pe, y);
+    }
   }
   __syncthreads();  // node values consumed: buf now holds y, buf[k][c TILE + element]
 #pragma unroll
@@ -1265,6 +1402,7 @@ template <class S> __device__ __forceinline__ V3<double> gatherSlots(const Sys<S
 template <class S, int LAW, bool TANGENT>
 __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, Vec4<S>* X, uint32_t x0zero) {
   __shared__ S buf[3][4 * TILE];
+
   __shared__ __align__(8) uint16_t sOff[TILE_OFF_STRIDE];
   __shared__ __align__(8) uint16_t sEnt[4 * TILE];
   const uint32_t G = gridDim.x;
@@ -1275,7 +1413,7 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, 
   double* part = s.blk_part;
   // ---- init: r = right - A x (anchored rows 0), z = P r, p_prev = 0
   if (!x0zero) {
-    for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G) matvecTile<S, LAW, TANGENT>(s, tile, X, zero, buf, sOff, sEnt, bd.elem_end);
+    for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G) matvecTile<S, LAW, TANGENT, false>(s, tile, X, zero, buf, sOff, sEnt, bd.elem_end, nullptr);
     if (!countBarrier(s.sync, bar)) return;
   }
   {
@@ -1323,7 +1461,7 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, 
     if (taken >= st.limit || sqrt(length) <= target) break;
     // ---- A
     for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G)
-      matvecTile<S, LAW, TANGENT>(s, tile, nullptr, S(blend), buf, sOff, sEnt, bd.elem_end);
+      matvecTile<S, LAW, TANGENT, false>(s, tile, nullptr, S(blend), buf, sOff, sEnt, bd.elem_end, nullptr);
     if (!countBarrier(s.sync, bar)) return;
     // ---- B
     double pap = 0.0;
@@ -1415,18 +1553,20 @@ template <class S, int LAW, bool TANGENT>
 __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2)
     kPcgBatch(Sys<S> s, Vec4<S>* X, uint32_t pass, uint32_t x0zero) {
   __shared__ S buf[3][4 * TILE];
+  extern __shared__ __align__(16) unsigned char tlStage[];  // stageBytes<S, LAW, TANGENT>()
   __shared__ __align__(8) uint16_t sOff[TILE_OFF_STRIDE];
   __shared__ __align__(8) uint16_t sEnt[4 * TILE];
   const uint32_t G = gridDim.x;
   const S zero = S(0);
+  unsigned int bar = 0;
   // ---- init: r = right - A x (anchored rows 0), z = P r, p_prev = 0
   if (!x0zero) {
     for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G) {
       const uint32_t b = s.elem_tile_body[tile];
       if (!bodyActive(s, b, pass)) continue;
-      matvecTile<S, LAW, TANGENT>(s, tile, X, zero, buf, sOff, sEnt, s.body[b].elem_end);
+      matvecTile<S, LAW, TANGENT, true>(s, tile, X, zero, buf, sOff, sEnt, s.body[b].elem_end, tlStage);
     }
-    if (!gridBarrier(s.sync)) return;
+    if (!countBarrier(s.sync, bar)) return;
   }
   for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
     const uint32_t b = s.node_tile_body[tile];
@@ -1483,16 +1623,16 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2)
       }
     }
   }
-  if (!gridBarrier(s.sync)) return;
+  if (!countBarrier(s.sync, bar)) return;
   for (;;) {
     if (*(volatile int*)&s.sync->active <= 0) break;  // uniform: no block decrements between here and barrier A
     // ---- A
     for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G) {
       const uint32_t b = s.elem_tile_body[tile];
       if (!bodyActive(s, b, pass) || __ldcg(&s.cg[b].done)) continue;
-      matvecTile<S, LAW, TANGENT>(s, tile, nullptr, S(__ldcg(&s.cg[b].blend)), buf, sOff, sEnt, s.body[b].elem_end);
+      matvecTile<S, LAW, TANGENT, true>(s, tile, nullptr, S(__ldcg(&s.cg[b].blend)), buf, sOff, sEnt, s.body[b].elem_end, tlStage);
     }
-    if (!gridBarrier(s.sync)) return;
+    if (!countBarrier(s.sync, bar)) return;
     // ---- B
     for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
       const uint32_t b = s.node_tile_body[tile];
@@ -1528,7 +1668,7 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2)
         }
       }
     }
-    if (!gridBarrier(s.sync)) return;
+    if (!countBarrier(s.sync, bar)) return;
     // ---- C
     for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
       const uint32_t b = s.node_tile_body[tile];
@@ -1571,7 +1711,7 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2)
         }
       }
     }
-    if (!gridBarrier(s.sync)) return;
+    if (!countBarrier(s.sync, bar)) return;
   }
   if (blockIdx.x == 0) {
     for (uint32_t b = threadIdx.x; b < s.bodies; b += TILE) {

@@ -621,20 +621,22 @@ struct System final : SystemBase {
     TL_CUDA(cudaStreamSynchronize(st));
     // resident blocks per SM of each cooperative kernel variant (the grid is
     // that times the SM count, capped by tl_system_tune and the tile counts)
-    auto perSm = [&](const void* fn) {
+    // (the batched variants take their operator stage as dynamic shared memory)
+    auto perSm = [&](const void* fn, size_t dyn) {
+      TL_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)));
       int n = 0;
-      TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, TILE, 0));
+      TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, TILE, dyn));
       if (n < 1) throw StatusError{TL_ERR_CUDA, "PCG kernel cannot be resident"};
       return n;
     };
-    pcg1PerSm[0][0] = perSm((const void*)kPcg1<S, 0, false>);
-    pcg1PerSm[0][1] = perSm((const void*)kPcg1<S, 0, true>);
-    pcg1PerSm[1][0] = perSm((const void*)kPcg1<S, 1, false>);
-    pcg1PerSm[1][1] = perSm((const void*)kPcg1<S, 1, true>);
-    batchPerSm[0][0] = perSm((const void*)kPcgBatch<S, 0, false>);
-    batchPerSm[0][1] = perSm((const void*)kPcgBatch<S, 0, true>);
-    batchPerSm[1][0] = perSm((const void*)kPcgBatch<S, 1, false>);
-    batchPerSm[1][1] = perSm((const void*)kPcgBatch<S, 1, true>);
+    pcg1PerSm[0][0] = perSm((const void*)kPcg1<S, 0, false>, 0);
+    pcg1PerSm[0][1] = perSm((const void*)kPcg1<S, 0, true>, 0);
+    pcg1PerSm[1][0] = perSm((const void*)kPcg1<S, 1, false>, 0);
+    pcg1PerSm[1][1] = perSm((const void*)kPcg1<S, 1, true>, 0);
+    batchPerSm[0][0] = perSm((const void*)kPcgBatch<S, 0, false>, stageBytes<S, 0, false>());
+    batchPerSm[0][1] = perSm((const void*)kPcgBatch<S, 0, true>, stageBytes<S, 0, true>());
+    batchPerSm[1][0] = perSm((const void*)kPcgBatch<S, 1, false>, stageBytes<S, 1, false>());
+    batchPerSm[1][1] = perSm((const void*)kPcgBatch<S, 1, true>, stageBytes<S, 1, true>());
     int most = 0;
     for (auto& row : pcg1PerSm)
       for (int n : row) most = std::max(most, n * ctx->sms);
@@ -786,6 +788,8 @@ struct System final : SystemBase {
     const int idx = law == TL_LAW_SNH ? 1 : 0;
     if (profiling) mark(2, true);
     (void)tg;
+    const size_t dyn = idx ? (tangent ? stageBytes<S, 1, true>() : stageBytes<S, 1, false>())
+                           : (tangent ? stageBytes<S, 0, true>() : stageBytes<S, 0, false>());
     if (B == 1) {  // single body: two-level assembly, per-block partials
       void* args[] = {&s, &X, &xz};
       const void* fn = idx ? (tangent ? (const void*)kPcg1<S, 1, true> : (const void*)kPcg1<S, 1, false>)
@@ -795,7 +799,7 @@ struct System final : SystemBase {
       void* args[] = {&s, &X, &ps, &xz};
       const void* fn = idx ? (tangent ? (const void*)kPcgBatch<S, 1, true> : (const void*)kPcgBatch<S, 1, false>)
                            : (tangent ? (const void*)kPcgBatch<S, 0, true> : (const void*)kPcgBatch<S, 0, false>);
-      TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(gridOf(batchPerSm[idx][tangent ? 1 : 0])), dim3(TILE), args, 0, st));
+      TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(gridOf(batchPerSm[idx][tangent ? 1 : 0])), dim3(TILE), args, dyn, st));
     }
     ++launches;
     if (profiling) mark(2, false);
