@@ -134,7 +134,8 @@ template <class S> struct Sys {
   Vec4<S>* r;
   Vec4<S>* z;
   Vec4<S>* p;
-  Vec4<S>* ap;
+  Vec4<S>* ap;            // A p (kPcgBatch); s = A p by recurrence (kPcg1)
+  Vec4<S>* w;             // A u (kPcg1)
   const uint32_t* start;  // [Vp + 1]
   const uint32_t* entry;  // 4 e + c, ascending e per node
   // elements
@@ -1280,6 +1281,39 @@ __device__ __forceinline__ bool countBarrier(GridSyncDev* sync, unsigned int& k)
   return ok != 0;
 }
 
+// Sums of fields [0, N) of every block's partials (field k of block b at
+// part[k G + b]) in one pass, the same in every block: all threads load at
+// once (thread t adds blocks t, t + TILE, ...), then a fixed shuffle tree per
+// warp and the warps in order, so a grid barrier is followed by one L2 round
+// trip instead of one per block stride.
+template <int N>
+__device__ __forceinline__ void sumBlocksAll(const double* part, double (&out)[N]) {
+  __shared__ double red[N][TILE / 32];
+  const unsigned G = gridDim.x;
+  double v[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) v[k] = 0.0;
+  for (unsigned b = threadIdx.x; b < G; b += TILE)
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] += __ldcg(part + size_t(k) * G + b);
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int k = 0; k < N; ++k) red[k][threadIdx.x >> 5] = v[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < TILE / 32; ++w) t += red[k][w];
+    out[k] = t;
+  }
+  __syncthreads();
+}
+
 // Sum of the per-block partials field f of every block, in block order; the
 // same value in every block (block-wide call, result broadcast).
 __device__ __forceinline__ double sumBlocks(const double* part, unsigned int field) {
@@ -1307,10 +1341,37 @@ __device__ __forceinline__ double sumBlocks(const double* part, unsigned int fie
 // nodes are staged.  It pays on large batched systems (more loads in flight,
 // fewer registers); the single-body kernel, latency-bound on few tiles per
 // block, is faster loading them directly (measured on B200).
-template <class S, int LAW, bool TANGENT, bool STAGE>
+// The preconditioned residual of kPcg1 after the deferred update
+//   s = w + beta s,  r = r - alpha s,  u = P r
+// from the stored vectors; every place that needs u (the matvec's node stage,
+// the node pass) forms it with this one function, so all agree bit for bit.
+template <class S>
+__device__ __forceinline__ V3<S> nextResidual(const Sys<S>& s, uint32_t n, S alpha, S beta, V3<S>& sOut, V3<S>& rOut) {
+  sOut = fmaV(beta, xyz(ld4cg(&s.ap[n])), xyz(ld4cg(&s.w[n])));
+  rOut = fmaV(-alpha, sOut, xyz(ld4cg(&s.r[n])));
+  const Vec4<S> q0 = ld4g(&s.pre0[n]), q1 = ld4g(&s.pre1[n]);
+  const Sym<S> P = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
+  return symMul(P, rOut);
+}
+
+// Node values a tile's matvec multiplies: X if given; else (CGU) u, formed by
+// nextResidual when `update` is set or read from z; else p = z + blend p_prev.
+template <class S, bool CGU>
+__device__ __forceinline__ V3<S> stagedValue(const Sys<S>& s, uint32_t n, const Vec4<S>* X, S blend, bool update,
+                                             S alpha) {
+  if (X) return xyz(ld4cg(&X[n]));
+  if (CGU) {
+    if (!update) return xyz(ld4cg(&s.z[n]));
+    V3<S> so, ro;
+    return nextResidual(s, n, alpha, blend, so, ro);
+  }
+  return fmaV(blend, xyz(ld4cg(&s.p[n])), xyz(ld4cg(&s.z[n])));
+}
+
+template <class S, int LAW, bool TANGENT, bool STAGE, bool CGU = false>
 __device__ __forceinline__ void matvecTile(const Sys<S>& s, uint32_t tile, const Vec4<S>* X, S blend,
                                            S (*buf)[4 * TILE], uint16_t* sOff, uint16_t* sEnt, uint32_t elemEnd,
-                                           unsigned char* stage) {
+                                           unsigned char* stage, bool update = false, S alpha = S(0)) {
   const uint32_t e = tile * TILE + threadIdx.x;
   const bool live = e < elemEnd;
   if (STAGE) {
@@ -1326,9 +1387,7 @@ __device__ __forceinline__ void matvecTile(const Sys<S>& s, uint32_t tile, const
   // stage the tile's nodes: buf[k][j] = component k of node j
   for (uint32_t j = threadIdx.x; j < meta.y; j += TILE) {
     const uint32_t n = __ldg(&s.tile_node[meta.x + j]);
-    V3<S> v;
-    if (X) v = xyz(ld4cg(&X[n]));
-    else v = fmaV(blend, xyz(ld4cg(&s.p[n])), xyz(ld4cg(&s.z[n])));
+    const V3<S> v = stagedValue<S, CGU>(s, n, X, blend, update, alpha);
     buf[0][j] = v.x;
     buf[1][j] = v.y;
     buf[2][j] = v.z;
@@ -1390,34 +1449,135 @@ template <class S> __device__ __forceinline__ V3<double> gatherSlots(const Sys<S
   return acc;
 }
 
-// Persistent PCG for a system holding ONE body (conjugateGradient,
-// solver.cc:1904-2089, block-Jacobi branch).  Per iteration:
-//   A (element tiles)  y_e and tile-local node sums (two-level assembly)
-//   B (node tiles)     p = z + blend p_prev; Ap = inertia m p + sum of slots; p.Ap
-//   C (node tiles)     x += stride p; r -= stride Ap; z = P r; r.z, r.r
-// with a grid barrier after each phase.  Every block accumulates its own
-// partial sums in a fixed order and, after the barrier, every block adds the
-// blocks' partials in block order, so all blocks take the same decisions
-// (convergence, breakdown) with no further communication.
+// Tile tables of one launch held in shared memory: a block of the
+// single-body PCG always works the same tiles (blockIdx.x + k gridDim.x), so
+// when it has at most CACHE_TILES of them it loads their local CSR, corner
+// slots and node lists once per launch instead of once per iteration.
+constexpr int CACHE_TILES = 4;
+struct TileCache {
+  uint2 meta[CACHE_TILES];
+  uint16_t ent[CACHE_TILES][4 * TILE];
+  uint16_t off[CACHE_TILES][TILE_OFF_STRIDE];
+  uint2 eloc[CACHE_TILES][TILE];
+  uint32_t node[CACHE_TILES][4 * TILE];
+};
+
+template <class S>
+__device__ __forceinline__ void fillTileCache(const Sys<S>& s, TileCache& c, uint32_t tiles) {
+  for (uint32_t k = 0; k < tiles; ++k) {
+    const uint32_t tile = blockIdx.x + k * gridDim.x;
+    const uint2 meta = __ldg(&s.tile_meta[tile]);
+    if (threadIdx.x == 0) c.meta[k] = meta;
+    reinterpret_cast<uint2*>(c.ent[k])[threadIdx.x] =
+        __ldg(reinterpret_cast<const uint2*>(s.tile_ent + size_t(tile) * 4 * TILE) + threadIdx.x);
+    const uint2* off = reinterpret_cast<const uint2*>(s.tile_off + size_t(tile) * TILE_OFF_STRIDE);
+    for (uint32_t q = threadIdx.x; q < TILE_OFF_STRIDE / 4; q += TILE) reinterpret_cast<uint2*>(c.off[k])[q] = __ldg(off + q);
+    c.eloc[k][threadIdx.x] = __ldg(&s.eloc[size_t(tile) * TILE + threadIdx.x]);
+    for (uint32_t j = threadIdx.x; j < meta.y; j += TILE) c.node[k][j] = __ldg(&s.tile_node[meta.x + j]);
+  }
+  __syncthreads();
+}
+
+// matvecTile with the tile tables of cache entry k: the element operator is
+// requested before the node stage, so the only dependent L2 round trip left
+// is the node values.
+template <class S, int LAW, bool TANGENT, bool CGU>
+__device__ __forceinline__ void matvecTileCached(const Sys<S>& s, const TileCache& c, uint32_t k, uint32_t tile,
+                                                 const Vec4<S>* X, S blend, S (*buf)[4 * TILE], uint32_t elemEnd,
+                                                 bool update, S alpha) {
+  const uint32_t e = tile * TILE + threadIdx.x;
+  const bool live = e < elemEnd;
+  ElementOperator<S> op;
+  if (live) op = loadOperator<S, LAW, TANGENT>(s, e);
+  const uint2 meta = c.meta[k];
+  for (uint32_t j = threadIdx.x; j < meta.y; j += TILE) {
+    const V3<S> v = stagedValue<S, CGU>(s, c.node[k][j], X, blend, update, alpha);
+    buf[0][j] = v.x;
+    buf[1][j] = v.y;
+    buf[2][j] = v.z;
+  }
+  __syncthreads();
+  V3<S> y[4] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  if (live) {
+    const uint2 loc = c.eloc[k][threadIdx.x];
+    const uint32_t l[4] = {loc.x & 0xffffu, loc.x >> 16, loc.y & 0xffffu, loc.y >> 16};
+    V3<S> pe[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) pe[q] = {buf[0][l[q]], buf[1][l[q]], buf[2][l[q]]};
+    applyOperator<S, LAW, TANGENT>(op, pe, y);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    buf[0][q * TILE + threadIdx.x] = y[q].x;
+    buf[1][q * TILE + threadIdx.x] = y[q].y;
+    buf[2][q * TILE + threadIdx.x] = y[q].z;
+  }
+  __syncthreads();
+  for (uint32_t j = threadIdx.x; j < meta.y; j += TILE) {
+    const uint32_t k0 = c.off[k][j], k1 = c.off[k][j + 1];
+    S ax = 0, ay = 0, az = 0;
+    for (uint32_t q = k0; q < k1; ++q) {
+      const uint32_t code = c.ent[k][q];
+      const uint32_t at = (code & 3u) * TILE + (code >> 2);
+      ax += buf[0][at];
+      ay += buf[1][at];
+      az += buf[2][at];
+    }
+    s.slot_part[meta.x + j] = Vec4<S>{ax, ay, az, S(0)};
+  }
+  __syncthreads();
+}
+
+// Persistent PCG for a system holding ONE body: conjugateGradient
+// (solver.cc:1904-2089, block-Jacobi branch) in the Chronopoulos-Gear
+// arrangement, which needs one reduction per iteration instead of two.  The
+// matvec is applied to u = P r rather than to p; p and s = A p follow by
+// recurrence:
+//   gamma = r.u, delta = u.A u, beta = gamma / gamma_prev,
+//   p.A p = delta - beta gamma / alpha_prev, alpha = gamma / p.A p,
+//   p = u + beta p, s = A u + beta s, x += alpha p, r -= alpha s, u = P r.
+// In exact arithmetic the iterates equal the reference's; the stopping test
+// (|r| <= tolerance |rhs| or the iteration cap, checked before each update),
+// the breakdown test (p.A p > 0 and r.z > 0) and the iteration count are the
+// reference's.  Per iteration:
+//   A (element tiles)  A u_i, u_i formed on the fly from the update of the
+//                      previous iteration (nextResidual), tile-local sums
+//   B (node tiles)     apply that update (p, s, x, r, u), gather w = A u,
+//                      partials of r.u, w.u, r.r
+// with a grid barrier after each.  A solve that stops on the tolerance has
+// computed one matvec more than the reference; one that reaches the cap
+// finishes with a node pass that applies the last update without a matvec.
+// Every block accumulates its partials in a fixed order and, after the
+// barrier, adds all blocks' partials in block order, so every block takes the
+// same decisions with no further communication.
 template <class S, int LAW, bool TANGENT>
 __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, Vec4<S>* X, uint32_t x0zero) {
   __shared__ S buf[3][4 * TILE];
-
   __shared__ __align__(8) uint16_t sOff[TILE_OFF_STRIDE];
   __shared__ __align__(8) uint16_t sEnt[4 * TILE];
+  extern __shared__ __align__(16) unsigned char tlDyn[];  // TileCache
+  TileCache& cache = *reinterpret_cast<TileCache*>(tlDyn);
   const uint32_t G = gridDim.x;
+  const uint32_t perBlock = (s.elem_tiles + G - 1) / G;  // the same in every block
+  const bool cached = perBlock <= uint32_t(CACHE_TILES);
+  if (cached) fillTileCache(s, cache, blockIdx.x < s.elem_tiles ? (s.elem_tiles - 1 - blockIdx.x) / G + 1 : 0u);
   unsigned int bar = 0;
   const BodyDev bd = s.body[0];
   const BodyStepDev st = s.step[0];
   const S zero = S(0);
   double* part = s.blk_part;
-  // ---- init: r = right - A x (anchored rows 0), z = P r, p_prev = 0
+  uint32_t applications = x0zero ? 0u : 1u;
+  // ---- init: r = right - A x (anchored rows 0), u = P r, p = s = 0
   if (!x0zero) {
-    for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G) matvecTile<S, LAW, TANGENT, false>(s, tile, X, zero, buf, sOff, sEnt, bd.elem_end, nullptr);
+    for (uint32_t tile = blockIdx.x, k = 0; tile < s.elem_tiles; tile += G, ++k) {
+      if (cached) matvecTileCached<S, LAW, TANGENT, true>(s, cache, k, tile, X, zero, buf, bd.elem_end, false, zero);
+      else matvecTile<S, LAW, TANGENT, false>(s, tile, X, zero, buf, sOff, sEnt, bd.elem_end, nullptr);
+    }
     if (!countBarrier(s.sync, bar)) return;
   }
   {
-    double rz = 0.0, rr = 0.0, bb = 0.0;
+    double rr = 0.0, bb = 0.0;
     for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
       const uint32_t n = tile * TILE + threadIdx.x;
       if (n >= bd.node_end) continue;
@@ -1430,101 +1590,136 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, 
       }
       const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
       const Sym<S> P = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
-      const V3<S> z = symMul(P, r);
       s.r[n] = pack(r);
-      s.z[n] = pack(z);
+      s.z[n] = pack(symMul(P, r));
       s.p[n] = Vec4<S>{zero, zero, zero, zero};
+      s.ap[n] = Vec4<S>{zero, zero, zero, zero};
       if (x0zero) X[n] = Vec4<S>{zero, zero, zero, zero};
-      rz += dot(cvt<double>(r), cvt<double>(z));
       rr += dot(cvt<double>(r), cvt<double>(r));
       bb += dot(cvt<double>(xyz(rhs)), cvt<double>(xyz(rhs)));
     }
-    double v[3] = {rz, rr, bb};
-    blockSum<3>(v);
+    double v[2] = {rr, bb};
+    blockSum<2>(v);
     if (threadIdx.x == 0) {
-      part[blockIdx.x] = v[0];
-      part[G + blockIdx.x] = v[1];
-      part[2 * G + blockIdx.x] = v[2];
+      part[G + blockIdx.x] = v[0];
+      part[2 * G + blockIdx.x] = v[1];
     }
   }
   if (!countBarrier(s.sync, bar)) return;
-  double squared = sumBlocks(part, 0);
-  double length = sumBlocks(part, 1);
-  const double reference = sqrt(sumBlocks(part, 2));
+  double init[3];
+  sumBlocksAll<3>(part, init);
+  double length = init[1];
+  const double reference = sqrt(init[2]);
   const double floor = fmax(reference, 1.1754943508222875e-38);  // std::numeric_limits<float>::min()
   const double target = st.tolerance * floor;
   const double startRes = sqrt(length) / floor;
-  double blend = 0.0;
+  double gamma = 0.0, alpha = 0.0, beta = 0.0;
   uint32_t taken = 0;
-  if (!countBarrier(s.sync, bar)) return;  // every block has read the init partials
-  for (;;) {
-    if (taken >= st.limit || sqrt(length) <= target) break;
-    // ---- A
-    for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G)
-      matvecTile<S, LAW, TANGENT, false>(s, tile, nullptr, S(blend), buf, sOff, sEnt, bd.elem_end, nullptr);
-    if (!countBarrier(s.sync, bar)) return;
-    // ---- B
-    double pap = 0.0;
+  // apply the update with (alpha, beta) on this block's nodes; partial r.r
+  auto applyUpdate = [&](double& rr) {
     for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
       const uint32_t n = tile * TILE + threadIdx.x;
       if (n >= bd.node_end) continue;
-      const V3<S> pn = fmaV(S(blend), xyz(ld4cg(&s.p[n])), xyz(ld4cg(&s.z[n])));
+      V3<S> sn, rn;
+      const V3<S> un = nextResidual(s, n, S(alpha), S(beta), sn, rn);
+      const V3<S> pn = fmaV(S(beta), xyz(ld4cg(&s.p[n])), xyz(ld4cg(&s.z[n])));
+      X[n] = pack(fmaV(S(alpha), pn, xyz(ld4cg(&X[n]))));
       s.p[n] = pack(pn);
-      V3<S> apn = {zero, zero, zero};
-      if (!s.anch[n]) apn = cvt<S>((st.inertia * double(ld4g(&s.rest4[n]).w)) * cvt<double>(pn) + gatherSlots(s, n));
-      s.ap[n] = pack(apn);
-      pap += dot(cvt<double>(pn), cvt<double>(apn));
+      s.ap[n] = pack(sn);
+      s.r[n] = pack(rn);
+      s.z[n] = pack(un);
+      rr += dot(cvt<double>(rn), cvt<double>(rn));
     }
-    {
-      double v[1] = {pap};
-      blockSum<1>(v);
-      if (threadIdx.x == 0) part[blockIdx.x] = v[0];
-    }
-    if (!countBarrier(s.sync, bar)) return;
-    const double curvature = sumBlocks(part, 0);
-    if (!(curvature > 0.0) || !(squared > 0.0)) break;
-    const double stride = squared / curvature;
-    // ---- C
-    double rz = 0.0, rr = 0.0;
-    for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
-      const uint32_t n = tile * TILE + threadIdx.x;
-      if (n >= bd.node_end) continue;
-      const V3<S> pn = xyz(ld4cg(&s.p[n]));
-      const V3<S> x = fmaV(S(stride), pn, xyz(ld4cg(&X[n])));
-      const V3<S> r = fmaV(S(-stride), xyz(ld4cg(&s.ap[n])), xyz(ld4cg(&s.r[n])));
-      const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
-      const Sym<S> P = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
-      const V3<S> z = symMul(P, r);
-      X[n] = pack(x);
-      s.r[n] = pack(r);
-      s.z[n] = pack(z);
-      rz += dot(cvt<double>(r), cvt<double>(z));
-      rr += dot(cvt<double>(r), cvt<double>(r));
-    }
-    {
-      double v[2] = {rz, rr};
-      blockSum<2>(v);
-      if (threadIdx.x == 0) {
-        part[G + blockIdx.x] = v[0];
-        part[2 * G + blockIdx.x] = v[1];
+  };
+  bool update = false;  // an update (alpha, beta) is pending
+  if (!(taken >= st.limit || sqrt(length) <= target)) {
+    for (;;) {
+      // ---- A: w = A u
+      for (uint32_t tile = blockIdx.x, k = 0; tile < s.elem_tiles; tile += G, ++k) {
+        if (cached)
+          matvecTileCached<S, LAW, TANGENT, true>(s, cache, k, tile, nullptr, S(beta), buf, bd.elem_end, update,
+                                                  S(alpha));
+        else
+          matvecTile<S, LAW, TANGENT, false, true>(s, tile, nullptr, S(beta), buf, sOff, sEnt, bd.elem_end, nullptr,
+                                                   update, S(alpha));
+      }
+      ++applications;
+      if (!countBarrier(s.sync, bar)) return;
+      // ---- B: the pending update, w = inertia m u + sum of slots, partials
+      double g = 0.0, d = 0.0, rr = 0.0;
+      for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
+        const uint32_t n = tile * TILE + threadIdx.x;
+        if (n >= bd.node_end) continue;
+        V3<S> un, rn;
+        if (update) {
+          V3<S> sn;
+          un = nextResidual(s, n, S(alpha), S(beta), sn, rn);
+          const V3<S> pn = fmaV(S(beta), xyz(ld4cg(&s.p[n])), xyz(ld4cg(&s.z[n])));
+          X[n] = pack(fmaV(S(alpha), pn, xyz(ld4cg(&X[n]))));
+          s.p[n] = pack(pn);
+          s.ap[n] = pack(sn);
+          s.r[n] = pack(rn);
+          s.z[n] = pack(un);
+        } else {
+          un = xyz(ld4cg(&s.z[n]));
+          rn = xyz(ld4cg(&s.r[n]));
+        }
+        V3<S> wn = {zero, zero, zero};
+        if (!s.anch[n]) wn = cvt<S>((st.inertia * double(ld4g(&s.rest4[n]).w)) * cvt<double>(un) + gatherSlots(s, n));
+        s.w[n] = pack(wn);
+        g += dot(cvt<double>(rn), cvt<double>(un));
+        d += dot(cvt<double>(wn), cvt<double>(un));
+        rr += dot(cvt<double>(rn), cvt<double>(rn));
+      }
+      {
+        double v[3] = {g, d, rr};
+        blockSum<3>(v);
+        if (threadIdx.x == 0) {
+          part[blockIdx.x] = v[0];
+          part[G + blockIdx.x] = v[1];
+          part[2 * G + blockIdx.x] = v[2];
+        }
+      }
+      if (!countBarrier(s.sync, bar)) return;
+      double sums[3];
+      sumBlocksAll<3>(part, sums);
+      const double gammaNext = sums[0], delta = sums[1];
+      length = sums[2];
+      if (update) {
+        ++taken;
+        if (taken >= st.limit || sqrt(length) <= target) break;  // the reference's loop-top test
+      }
+      const double b = update ? gammaNext / gamma : 0.0;
+      const double curvature = update ? delta - b * gammaNext / alpha : delta;  // p.A p
+      if (!(curvature > 0.0) || !(gammaNext > 0.0)) break;
+      beta = b;
+      alpha = gammaNext / curvature;
+      gamma = gammaNext;
+      update = true;
+      if (taken + 1 >= st.limit) {  // the last update the cap allows: no matvec after it
+        double rr2 = 0.0;
+        applyUpdate(rr2);
+        double v[1] = {rr2};
+        blockSum<1>(v);
+        if (threadIdx.x == 0) part[2 * G + blockIdx.x] = v[0];
+        if (!countBarrier(s.sync, bar)) return;
+        double fin[3];
+        sumBlocksAll<3>(part, fin);
+        length = fin[2];
+        ++taken;
+        break;
       }
     }
-    if (!countBarrier(s.sync, bar)) return;
-    const double next = sumBlocks(part, 1);
-    length = sumBlocks(part, 2);
-    blend = next / squared;
-    squared = next;
-    ++taken;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     const double residual = sqrt(length);
     CgBodyDev c;
-    c.squared = squared;
+    c.squared = gamma;
     c.target = target;
     c.floor = floor;
     c.length = length;
-    c.stride = 0.0;
-    c.blend = blend;
+    c.stride = alpha;
+    c.blend = beta;
     c.start_res = startRes;
     c.rel_res = residual / floor;
     c.taken = taken;
@@ -1534,7 +1729,7 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, 
     CgReportDev rep = s.cgrep[0];
     rep.iterations += taken;
     rep.capped += (taken == st.limit && residual > target) ? 1u : 0u;
-    rep.applications += taken + (x0zero ? 0u : 1u);
+    rep.applications += applications;
     rep.solves += 1u;
     rep.tangent_iterations += TANGENT ? taken : 0u;
     rep.worst_rel = fmax(rep.worst_rel, c.rel_res);

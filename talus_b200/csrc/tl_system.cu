@@ -173,7 +173,7 @@ struct System final : SystemBase {
   DevBuf<BodyStepDev> dStep;
   DevBuf<MatDev> dMat;
   DevBuf<uint32_t> dNodeTileBody, dElemTileBody;
-  DevBuf<Vec4<S>> rest4, pres, u, v, a, carried, shifted, weighted, total, incr, lowest, right, pre0, pre1, r, z, p, ap;
+  DevBuf<Vec4<S>> rest4, pres, u, v, a, carried, shifted, weighted, total, incr, lowest, right, pre0, pre1, r, z, p, ap, w;
   DevBuf<uint8_t> anch;
   DevBuf<uint32_t> start, entry, lane;
   DevBuf<uint4> tet;
@@ -280,6 +280,7 @@ struct System final : SystemBase {
     s.z = z.ptr;
     s.p = p.ptr;
     s.ap = ap.ptr;
+    s.w = w.ptr;
     s.start = start.ptr;
     s.entry = entry.ptr;
     s.tet = tet.ptr;
@@ -466,7 +467,7 @@ struct System final : SystemBase {
     anch.alloc(Vp);
     anch.upload(hAnch.data(), Vp, st);
     for (DevBuf<Vec4<S>>* buf : {&u, &v, &a, &carried, &shifted, &weighted, &total, &incr, &lowest, &right, &pre0,
-                                 &pre1, &r, &z, &p, &ap}) {
+                                 &pre1, &r, &z, &p, &ap, &w}) {
       buf->alloc(Vp);
       buf->zero(st);
     }
@@ -629,10 +630,10 @@ struct System final : SystemBase {
       if (n < 1) throw StatusError{TL_ERR_CUDA, "PCG kernel cannot be resident"};
       return n;
     };
-    pcg1PerSm[0][0] = perSm((const void*)kPcg1<S, 0, false>, 0);
-    pcg1PerSm[0][1] = perSm((const void*)kPcg1<S, 0, true>, 0);
-    pcg1PerSm[1][0] = perSm((const void*)kPcg1<S, 1, false>, 0);
-    pcg1PerSm[1][1] = perSm((const void*)kPcg1<S, 1, true>, 0);
+    pcg1PerSm[0][0] = perSm((const void*)kPcg1<S, 0, false>, sizeof(TileCache));
+    pcg1PerSm[0][1] = perSm((const void*)kPcg1<S, 0, true>, sizeof(TileCache));
+    pcg1PerSm[1][0] = perSm((const void*)kPcg1<S, 1, false>, sizeof(TileCache));
+    pcg1PerSm[1][1] = perSm((const void*)kPcg1<S, 1, true>, sizeof(TileCache));
     batchPerSm[0][0] = perSm((const void*)kPcgBatch<S, 0, false>, stageBytes<S, 0, false>());
     batchPerSm[0][1] = perSm((const void*)kPcgBatch<S, 0, true>, stageBytes<S, 0, true>());
     batchPerSm[1][0] = perSm((const void*)kPcgBatch<S, 1, false>, stageBytes<S, 1, false>());
@@ -794,7 +795,8 @@ struct System final : SystemBase {
       void* args[] = {&s, &X, &xz};
       const void* fn = idx ? (tangent ? (const void*)kPcg1<S, 1, true> : (const void*)kPcg1<S, 1, false>)
                            : (tangent ? (const void*)kPcg1<S, 0, true> : (const void*)kPcg1<S, 0, false>);
-      TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(gridOf(pcg1PerSm[idx][tangent ? 1 : 0])), dim3(TILE), args, 0, st));
+      TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(gridOf(pcg1PerSm[idx][tangent ? 1 : 0])), dim3(TILE), args,
+                                          sizeof(TileCache), st));
     } else {  // batch: two-level assembly, per-body scalars
       void* args[] = {&s, &X, &ps, &xz};
       const void* fn = idx ? (tangent ? (const void*)kPcgBatch<S, 1, true> : (const void*)kPcgBatch<S, 1, false>)
