@@ -33,6 +33,7 @@ sys.path.insert(0, ROOT)
 METRIC = "elem-steps/s FP32-mixed vs FP64 GPU @rel-err<=1e-5; adjoint/forward time ratio"
 UNIT = "element-steps/s"
 
+from talus_b200.shard import aggregate  # noqa: E402
 from talus_b200.workloads import WORKLOADS, make_bodies, make_mesh  # noqa: E402
 
 
@@ -251,7 +252,7 @@ def run_ours(args, spec, rank, world, dist):
     device = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(device)
     precision = tb.FP32_MIXED if args.precision == "mixed" else tb.FP64
-    meshes, mats = make_bodies(spec)
+    meshes, mats = make_bodies(spec, rank, world)
     B = len(meshes)
     T = sum(m.tets for m in meshes)
     V = sum(m.nodes for m in meshes)
@@ -302,8 +303,9 @@ def run_ours(args, spec, rank, world, dist):
                                 reps[b].plastic_evaluations)
                 reps_substeps[b] += reps[b].substeps
         barrier()
-    total_seconds = max_over_ranks(sum(step_seconds))
-    value = world * T * args.steps / total_seconds
+    # tets stepped by all ranks (replicas: world x T; shards: the whole batch) over the slowest rank
+    T_all, total_seconds = aggregate(T, sum(step_seconds), dist, f"cuda:{device}")
+    value = T_all * args.steps / total_seconds
     finals = [system.get_state(i) for i in range(B)]
 
     # ---- end to end through the public API: the state crosses the host boundary every step
@@ -338,7 +340,7 @@ def run_ours(args, spec, rank, world, dist):
             capi.check(st, context.handle)
     barrier()
     e2e_seconds = max_over_ranks(time.perf_counter() - t0)
-    e2e_value = world * T * e2e_steps / e2e_seconds
+    e2e_value = T_all * e2e_steps / e2e_seconds
 
     # ---- roofline of the dominant kernel (persistent PCG): algorithmic bytes of every iteration run
     s_bytes = 4 if precision == tb.FP32_MIXED else 8
@@ -364,8 +366,10 @@ def run_ours(args, spec, rank, world, dist):
               "tl::kPcgBatch (persistent block-Jacobi PCG over all bodies, two-level assembly)")
     config = {"workload": args.workload, "bodies": B, "tets": T, "nodes": V, "law": spec["law"],
               "precision": args.precision, "dt": 1.0 / 60.0,
-              "parallelism": f"replicas{world}" if world > 1 else "single-gpu",
+              "parallelism": "single-gpu" if world == 1 else (f"shards{world}" if spec.get("batch") else f"replicas{world}"),
               "l2": "flushed (256 MB write) between timed steps; working set > 126 MB"}
+    if world > 1:
+        config["tets_all_ranks"] = T_all
     if not spec.get("batch"):
         config["cells"] = list(spec["cells"])
     if tune:
@@ -399,7 +403,8 @@ def run_ours(args, spec, rank, world, dist):
         for m, st, x64 in zip(meshes, finals, pos64):
             scale = np.linalg.norm(x64 - m.rest_positions, axis=1).max()
             worst = max(worst, float(np.linalg.norm(st.position - x64, axis=1).max() / max(scale, 1e-300)))
-        result["fp64"] = {"value": world * T * args.steps / secs64, "ms_per_step": secs64 * 1e3 / args.steps,
+        worst = max_over_ranks(worst)
+        result["fp64"] = {"value": T_all * args.steps / secs64, "ms_per_step": secs64 * 1e3 / args.steps,
                           "mixed_speedup": secs64 / total_seconds,
                           "max_rel_displacement_error": worst,
                           "note": f"same workload and steps from rest in FP64; error = max over bodies of "

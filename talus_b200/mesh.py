@@ -47,16 +47,9 @@ def batch_bodies(count=512, seed=3, lo=4, hi=24, voxel=0.1):
     """Uneven bodies of the batched benchmark: cell counts per axis uniform in
     {lo..hi}, Young's modulus log-uniform in [1e5, 1e8] Pa, Poisson's ratio
     uniform in [0.25, 0.45], density 1000, base (y = 0) anchored; seeded."""
-    from .deformable import PhysicalMaterial
+    from .shard import batch_bodies_range
 
-    rng = np.random.default_rng(seed)
-    dims = rng.integers(lo, hi + 1, size=(count, 3))
-    youngs = np.exp(rng.uniform(np.log(1e5), np.log(1e8), size=count))
-    poisson = rng.uniform(0.25, 0.45, size=count)
-    meshes = [box_mesh(tuple(int(c) for c in d), voxel=voxel, seed=seed + i) for i, d in enumerate(dims)]
-    mats = [[PhysicalMaterial(density=1000.0, youngs_modulus=float(e), poissons_ratio=float(nu))]
-            for e, nu in zip(youngs, poisson)]
-    return meshes, mats
+    return batch_bodies_range(0, count, count, seed, lo, hi, voxel)
 
 
 def box_mesh(cells, voxel=0.1, origin=(0.0, 0.0, 0.0), jitter=0.0, seed=0, density=1000.0, anchor_axis=1,

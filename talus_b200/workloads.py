@@ -16,6 +16,7 @@ import numpy as np
 
 from .deformable import PhysicalMaterial
 from .mesh import batch_bodies, box_mesh
+from .shard import batch_bodies_range, batch_dims, partition, tets_of
 
 WORKLOADS = {
     "plastic-block": dict(cells=(64, 32, 32), youngs=2e7, poisson=0.35, yield_stress=1e5, hardening=2e5,
@@ -41,9 +42,17 @@ def make_mesh(spec, scale_cells=None):
     return mesh, mat
 
 
-def make_bodies(spec):
-    """(meshes, per-body material lists) of a workload."""
+def make_bodies(spec, rank=0, world=1):
+    """(meshes, per-body material lists) of a workload for one rank.  A batch
+    on `world` ranks is the batch of count * world bodies, each rank taking
+    its contiguous, tet-balanced share (talus_b200.shard); a single-body
+    workload is the same body on every rank (replicas)."""
     if spec.get("batch"):
-        return batch_bodies(spec["count"], spec["seed"], spec["lo"], spec["hi"])
+        if world == 1:
+            return batch_bodies(spec["count"], spec["seed"], spec["lo"], spec["hi"])
+        total = spec["count"] * world
+        dims = batch_dims(total, spec["seed"], spec["lo"], spec["hi"])
+        lo, hi = partition(tets_of(dims), world)[rank]
+        return batch_bodies_range(lo, hi, total, spec["seed"], spec["lo"], spec["hi"])
     mesh, mat = make_mesh(spec)
     return [mesh], [[mat]]
