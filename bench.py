@@ -373,7 +373,8 @@ def run_ours(args, spec, rank, world, dist):
     if not spec.get("batch"):
         config["cells"] = list(spec["cells"])
     if tune:
-        config["tuning"] = tune
+        config["tuning"] = {"pcg_blocks_per_sm": tune["pcg_blocks_per_sm"], "graph": tune["graph"],
+                            "source": "talus_b200/tuning.json (talus_b200.autotune)"}
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_seconds * 1e3 / args.steps, "higher_is_better": True,

@@ -1381,8 +1381,10 @@ __device__ __forceinline__ void matvecTile(const Sys<S>& s, uint32_t tile, const
   const uint2 meta = __ldg(&s.tile_meta[tile]);
   const uint2 entv = __ldg(reinterpret_cast<const uint2*>(s.tile_ent + size_t(tile) * 4 * TILE) + threadIdx.x);
   const uint16_t* off = s.tile_off + size_t(tile) * TILE_OFF_STRIDE;
-  const uint2 offv = __ldg(reinterpret_cast<const uint2*>(off) + threadIdx.x);
-  const uint16_t offLast = threadIdx.x == 0 ? __ldg(&off[4 * TILE]) : uint16_t(0);
+  // only offsets 0..meta.y are read: fetch the 4-entry groups that hold them
+  const uint2 offv = 4u * threadIdx.x <= meta.y ? __ldg(reinterpret_cast<const uint2*>(off) + threadIdx.x)
+                                                : make_uint2(0u, 0u);
+  const uint16_t offLast = threadIdx.x == 0 && meta.y >= 4u * TILE ? __ldg(&off[4 * TILE]) : uint16_t(0);
   const uint2 loc = live ? __ldg(&s.eloc[e]) : make_uint2(0u, 0u);
   // stage the tile's nodes: buf[k][j] = component k of node j
   for (uint32_t j = threadIdx.x; j < meta.y; j += TILE) {

@@ -27,8 +27,11 @@ def main():
     ap.add_argument("--workload", default="plastic-block", choices=sorted(WORKLOADS))
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
+    ap.add_argument("--count", type=int, default=0, help="bodies of a batch workload (0: the workload's own)")
     args = ap.parse_args()
-    spec = WORKLOADS[args.workload]
+    spec = dict(WORKLOADS[args.workload])
+    if args.count and spec.get("batch"):
+        spec["count"] = args.count
     meshes, mats = make_bodies(spec)
     precision = tb.FP32_MIXED if args.precision == "mixed" else tb.FP64
     law = tb.NEO_HOOKEAN if spec["law"] == "snh" else tb.COROTATED
