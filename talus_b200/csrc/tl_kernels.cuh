@@ -507,7 +507,7 @@ __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
     // per-corner force and diagonal block, stored as soon as they are formed
     // (forces in FP64; the diagonal blocks, like the matvec operator, are formed
     // in the storage type S: they only precondition and are stored as S)
-    auto emit = [&](int c, const V3<double>& f, const Sym<S>& d) {
+    auto emit = [&](int c, const V3<S>& f, const Sym<S>& d) {
       finite = finite && isfinite(f.x) && isfinite(f.y) && isfinite(f.z);
       const size_t at = size_t(c) * s.Tp + e;
       s.fe[at] = Vec4<S>{S(f.x), S(f.y), S(f.z), S(d.xx)};
@@ -544,85 +544,90 @@ __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
         g[3] = {d[6], d[7], d[8]};
         g[0] = -(g[1] + g[2] + g[3]);
       }
+      // From here on the arithmetic is the storage type S: the strain above
+      // needs FP64 (it is a small difference of O(1) quantities); the return
+      // map, stress and forces only need the relative accuracy of the S
+      // records they end in.  In FP64 systems nothing changes.
+      using C = S;
       const bool yields = m.yields != 0u;
-      const double bulk = lam + 2.0 * mu / 3.0;
-      Sym<double> stress;
-      double theta = 1.0, thetaBar = 0.0;
-      Sym<double> normal = {0, 0, 0, 0, 0, 0};
+      const C lamC = C(lam), muC = C(mu), volC = C(vol);
+      const C bulk = C(lam + 2.0 * mu / 3.0);
+      Sym<C> stress;
+      C theta = C(1), thetaBar = C(0);
+      Sym<C> normal = {0, 0, 0, 0, 0, 0};
       if (yields) {
         // returnMap (material.cc:594-634)
         const Vec4<S> p0 = s.plast[e], p1 = s.plast[s.Tp + e];
-        const Sym<double> ep = {double(p0.x), double(p0.y), double(p0.z), double(p0.w), double(p1.x), double(p1.y)};
-        const double eq = double(p1.z);
-        const Sym<double> el = {eps.xx - ep.xx, eps.yy - ep.yy, eps.zz - ep.zz,
-                                eps.xy - ep.xy, eps.xz - ep.xz, eps.yz - ep.yz};
-        const double pressure = bulk * symTrace(el);
-        const double third = symTrace(el) / 3.0;
-        const Sym<double> tr = {2.0 * mu * (el.xx - third), 2.0 * mu * (el.yy - third), 2.0 * mu * (el.zz - third),
-                                2.0 * mu * el.xy, 2.0 * mu * el.xz, 2.0 * mu * el.yz};
-        const double norm = sqrt(symContract(tr, tr));
-        const double equivalent = sqrt(1.5) * norm;
-        const double radius = m.yield + fmax(m.hardening, 0.0) * eq;
-        const double hard = fmax(m.hardening, 0.0);
-        Sym<double> next = ep;
-        double nextEq = eq;
-        bool plastic = false;
-        double excess = 0.0;
-        if (!(mode & EM_MAPPING) || !(equivalent > radius) || !(norm > 0.0)) {
+        const Sym<C> ep = {C(p0.x), C(p0.y), C(p0.z), C(p0.w), C(p1.x), C(p1.y)};
+        const C eq = C(p1.z);
+        const Sym<C> el = {C(eps.xx - double(p0.x)), C(eps.yy - double(p0.y)), C(eps.zz - double(p0.z)),
+                           C(eps.xy - double(p0.w)), C(eps.xz - double(p1.x)), C(eps.yz - double(p1.y))};
+        const C pressure = bulk * symTrace(el);
+        const C third = symTrace(el) / C(3);
+        const C twoMu = C(2) * muC;
+        const Sym<C> tr = {twoMu * (el.xx - third), twoMu * (el.yy - third), twoMu * (el.zz - third),
+                           twoMu * el.xy, twoMu * el.xz, twoMu * el.yz};
+        const C norm = sqrt(symContract(tr, tr));
+        const C equivalent = C(sqrt(1.5)) * norm;
+        const C hard = C(fmax(m.hardening, 0.0));
+        const C radius = C(m.yield) + hard * eq;
+        Sym<C> next = ep;
+        C nextEq = eq;
+        C excess = C(0);
+        if (!(mode & EM_MAPPING) || !(equivalent > radius) || !(norm > C(0))) {
           stress = {tr.xx + pressure, tr.yy + pressure, tr.zz + pressure, tr.xy, tr.xz, tr.yz};
         } else {
-          const double gamma = (equivalent - radius) / (3.0 * mu + hard);
-          const double inv = 1.0 / norm;
-          const Sym<double> n = {tr.xx * inv, tr.yy * inv, tr.zz * inv, tr.xy * inv, tr.xz * inv, tr.yz * inv};
-          const double th = 1.0 - 3.0 * mu * gamma / equivalent;
+          const C gamma = (equivalent - radius) / (C(3) * muC + hard);
+          const C inv = C(1) / norm;
+          const Sym<C> n = {tr.xx * inv, tr.yy * inv, tr.zz * inv, tr.xy * inv, tr.xz * inv, tr.yz * inv};
+          const C th = C(1) - C(3) * muC * gamma / equivalent;
           stress = {th * tr.xx + pressure, th * tr.yy + pressure, th * tr.zz + pressure, th * tr.xy, th * tr.xz,
                     th * tr.yz};
-          plastic = true;
           excess = (equivalent - radius) / radius;
-          const double sg = sqrt(1.5) * gamma;
+          const C sg = C(sqrt(1.5)) * gamma;
           next = {ep.xx + sg * n.xx, ep.yy + sg * n.yy, ep.zz + sg * n.zz,
                   ep.xy + sg * n.xy, ep.xz + sg * n.xz, ep.yz + sg * n.yz};
           nextEq = eq + gamma;
-          const bool loading = excess > margin;
+          const bool loading = double(excess) > margin;
           if (loading) {  // linearized = response (material.cc:1016-1017)
             theta = th;
-            thetaBar = 3.0 * mu / (3.0 * mu + hard) - (1.0 - th);
+            thetaBar = C(3) * muC / (C(3) * muC + hard) - (C(1) - th);
             normal = n;
           }
           isLoading = loading;
           isYielding = true;
         }
-        const Sym<double> rem = {eps.xx - next.xx, eps.yy - next.yy, eps.zz - next.zz,
-                                 eps.xy - next.xy, eps.xz - next.xz, eps.yz - next.yz};
-        energy = vol * 0.5 * symContract(stress, rem);
+        const Sym<C> rem = {C(eps.xx - double(next.xx)), C(eps.yy - double(next.yy)), C(eps.zz - double(next.zz)),
+                            C(eps.xy - double(next.xy)), C(eps.xz - double(next.xz)), C(eps.yz - double(next.yz))};
+        energy = double(volC * C(0.5) * symContract(stress, rem));
         if ((mode & (EM_KEEP | EM_COMMIT)) != 0u) {
           grew = nextEq > eq;
           s.plast[e] = Vec4<S>{S(next.xx), S(next.yy), S(next.zz), S(next.xy)};
           s.plast[s.Tp + e] = Vec4<S>{S(next.xz), S(next.yz), S(nextEq), S(0)};
         }
       } else {
-        const double tr = symTrace(eps);
-        stress = {lam * tr + 2.0 * mu * eps.xx, lam * tr + 2.0 * mu * eps.yy, lam * tr + 2.0 * mu * eps.zz,
-                  2.0 * mu * eps.xy, 2.0 * mu * eps.xz, 2.0 * mu * eps.yz};
-        energy = vol * 0.5 * symContract(stress, eps);
+        const Sym<C> ec = {C(eps.xx), C(eps.yy), C(eps.zz), C(eps.xy), C(eps.xz), C(eps.yz)};
+        const C tr = symTrace(ec);
+        stress = {lamC * tr + C(2) * muC * ec.xx, lamC * tr + C(2) * muC * ec.yy, lamC * tr + C(2) * muC * ec.zz,
+                  C(2) * muC * ec.xy, C(2) * muC * ec.xz, C(2) * muC * ec.yz};
+        energy = double(volC * C(0.5) * symContract(stress, ec));
       }
       if (!(mode & EM_COMMIT)) {
         const bool tangentDiag = (mode & EM_CONSISTENT) && yields;
-        const double th = tangentDiag ? theta : 1.0;
-        const double thb = tangentDiag ? thetaBar : 0.0;
+        const C th = tangentDiag ? theta : C(1);
+        const C thb = tangentDiag ? thetaBar : C(0);
         M3<S> Rw;
 #pragma unroll
         for (int i = 0; i < 3; ++i)
 #pragma unroll
           for (int j = 0; j < 3; ++j) Rw.m[i][j] = S(R.m[i][j]);
-        const Sym<S> nw = {S(normal.xx), S(normal.yy), S(normal.zz), S(normal.xy), S(normal.xz), S(normal.yz)};
-        const S k1 = S(vol * (bulk + mu * th / 3.0)), kmu = S(vol * mu * th), k3 = S(-vol * 2.0 * mu * thb);
+        const Sym<S> nw = normal;
+        const S k1 = volC * (bulk + muC * th / C(3)), kmu = volC * muC * th, k3 = -volC * C(2) * muC * thb;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
-          const V3<double> w = symMul(stress, g[c]);
-          const V3<double> force = -(vol * mul(R, w));  // material.cc:1019-1027
           // R K_cc R^T with K_cc = V[(K + mu theta/3) g g^T + mu theta |g|^2 I - 2 mu thetaBar (n g)(n g)^T]
           const V3<S> gc = cvt<S>(g[c]);
+          const V3<S> force = -(volC * mul(Rw, symMul(stress, gc)));  // material.cc:1019-1027
           const V3<S> rg = mul(Rw, gc);
           const V3<S> rn = mul(Rw, symMul(nw, gc));
           const S k2 = kmu * dot(gc, gc);
@@ -681,7 +686,7 @@ __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
         for (int c = 0; c < 4; ++c) {
           const V3<S> bb = cvt<S>(mul(C, g[c]));
           const S k2 = S(vol * mu * dot(g[c], g[c])), k1 = S(vol * shifted);
-          emit(c, -(vol * mul(P, g[c])), {k1 * bb.x * bb.x + k2, k1 * bb.y * bb.y + k2, k1 * bb.z * bb.z + k2,
+          emit(c, cvt<S>(-(vol * mul(P, g[c]))), {k1 * bb.x * bb.x + k2, k1 * bb.y * bb.y + k2, k1 * bb.z * bb.z + k2,
                                           k1 * bb.x * bb.y, k1 * bb.x * bb.z, k1 * bb.y * bb.z});
         }
       }
