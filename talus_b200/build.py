@@ -11,7 +11,7 @@ HEADERS = [os.path.join(HERE, "csrc", f) for f in ("tl_kernels.cuh", "tl_math.cu
     os.path.join(os.path.dirname(HERE), "include", "talus_fem.h")]
 OUTPUT = os.path.join(HERE, "libtalus_fem.so")
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
-              "-Xcompiler", "-fPIC", "-shared", "-Xptxas", "-v"]
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-pthread", "-shared", "-Xptxas", "-v"]
 
 
 def nvcc() -> str:

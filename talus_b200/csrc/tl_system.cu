@@ -16,6 +16,7 @@
 #include <memory>
 #include <string>
 #include <type_traits>
+#include <thread>
 #include <vector>
 
 using namespace tl;
@@ -104,6 +105,25 @@ constexpr uint32_t INVERTED_SUBSTEPS = 4u;    // solver.cc:13
 constexpr double LOADING_MARGIN = 1.0e-3;     // solver.cc:372
 constexpr double PLASTIC_REDUCTION = 1.0e-2;  // solver.cc:374
 constexpr double PLASTIC_RESOLUTION = 8.0;    // solver.cc:380
+
+// Host loops over [0, n) split across up to 16 threads (state conversion of
+// large bodies); small ranges run inline.  The body must not throw.
+template <class F>
+void parallelFor(size_t n, F&& body) {
+  const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  const size_t parts = n < (size_t(1) << 16) ? 1 : std::min<size_t>(hw, n >> 14);
+  if (parts <= 1) {
+    body(size_t(0), n);
+    return;
+  }
+  const size_t per = (n + parts - 1) / parts;
+  std::vector<std::thread> pool;
+  pool.reserve(parts - 1);
+  for (size_t p = 1; p < parts; ++p)
+    pool.emplace_back([&body, p, per, n] { body(p * per, std::min(n, (p + 1) * per)); });
+  body(size_t(0), std::min(n, per));
+  for (std::thread& t : pool) t.join();
+}
 
 struct HostBody {
   uint32_t nodes = 0, tets = 0;
@@ -246,7 +266,7 @@ struct System final : SystemBase {
   PinnedBuf<CgReportDev> hRep;
   PinnedBuf<GridSyncDev> hSync;
   PinnedBuf<BodyStepDev> hStep;
-  PinnedBuf<Vec4<S>> hNode;
+  PinnedBuf<Vec4<S>> hNode, hNodeV, hNodeA;
   PinnedBuf<S> hElem;
   PinnedBuf<Vec4<S>> hElem4;
 
@@ -648,81 +668,113 @@ struct System final : SystemBase {
 
   template <class H>
   void setNodes(const BodyDev& bd, const HostBody& h, DevBuf<Vec4<S>>& dst, const H* src, bool displacement) {
-    Vec4<S>* stage = hNode.get(h.nodes);
-    for (uint32_t n = 0; n < h.nodes; ++n) {
-      double x = double(src[3 * n]), y = double(src[3 * n + 1]), zz = double(src[3 * n + 2]);
-      if (displacement) {
-        x -= h.rest[3 * n];
-        y -= h.rest[3 * n + 1];
-        zz -= h.rest[3 * n + 2];
-      }
-      stage[n] = Vec4<S>{S(x), S(y), S(zz), S(0)};
-    }
-    dst.upload(stage, h.nodes, st, bd.node_begin);
+    stageNodes(bd, h, dst, src, displacement, hNode);
     TL_CUDA(cudaStreamSynchronize(st));
+  }
+  // Converts one node array into its pinned stage and queues the upload (the
+  // stage must not be reused before the stream has passed the copy).
+  template <class H>
+  void stageNodes(const BodyDev& bd, const HostBody& h, DevBuf<Vec4<S>>& dst, const H* src, bool displacement,
+                  PinnedBuf<Vec4<S>>& buf) {
+    Vec4<S>* stage = buf.get(h.nodes);
+    parallelFor(h.nodes, [&](size_t n0, size_t n1) {
+      for (size_t n = n0; n < n1; ++n) {
+        double x = double(src[3 * n]), y = double(src[3 * n + 1]), zz = double(src[3 * n + 2]);
+        if (displacement) {
+          x -= h.rest[3 * n];
+          y -= h.rest[3 * n + 1];
+          zz -= h.rest[3 * n + 2];
+        }
+        stage[n] = Vec4<S>{S(x), S(y), S(zz), S(0)};
+      }
+    });
+    dst.upload(stage, h.nodes, st, bd.node_begin);
   }
   template <class H>
   void getNodes(const BodyDev& bd, const HostBody& h, const DevBuf<Vec4<S>>& src, H* dst, bool displacement) {
     Vec4<S>* stage = hNode.get(h.nodes);
     src.download(stage, h.nodes, st, bd.node_begin);
     TL_CUDA(cudaStreamSynchronize(st));
-    for (uint32_t n = 0; n < h.nodes; ++n) {
-      double x = double(stage[n].x), y = double(stage[n].y), zz = double(stage[n].z);
-      if (displacement) {
-        x += h.rest[3 * n];
-        y += h.rest[3 * n + 1];
-        zz += h.rest[3 * n + 2];
+    unstageNodes(h, stage, dst, displacement);
+  }
+  template <class H>
+  void unstageNodes(const HostBody& h, const Vec4<S>* stage, H* dst, bool displacement) {
+    parallelFor(h.nodes, [&](size_t n0, size_t n1) {
+      for (size_t n = n0; n < n1; ++n) {
+        double x = double(stage[n].x), y = double(stage[n].y), zz = double(stage[n].z);
+        if (displacement) {
+          x += h.rest[3 * n];
+          y += h.rest[3 * n + 1];
+          zz += h.rest[3 * n + 2];
+        }
+        dst[3 * n] = H(x);
+        dst[3 * n + 1] = H(y);
+        dst[3 * n + 2] = H(zz);
       }
-      dst[3 * n] = H(x);
-      dst[3 * n + 1] = H(y);
-      dst[3 * n + 2] = H(zz);
-    }
+    });
   }
   template <class H>
   void setElems(const BodyDev& bd, const HostBody& h, const H* rot, const H* plastic) {
     const uint32_t T = h.tets;
     if (rot) {
       S* stage = hElem.get(size_t(9) * T);
-      for (int k = 0; k < 9; ++k)
-        for (uint32_t t = 0; t < T; ++t) stage[size_t(k) * T + t] = S(rot[9 * size_t(t) + k]);
+      parallelFor(T, [&](size_t t0, size_t t1) {  // one pass: each tet's 9 entries to the 9 planes
+        for (size_t t = t0; t < t1; ++t)
+          for (int k = 0; k < 9; ++k) stage[size_t(k) * T + t] = S(rot[9 * t + k]);
+      });
       for (int k = 0; k < 9; ++k) op.upload(stage + size_t(k) * T, T, st, size_t(k) * Tp + bd.elem_begin);
     }
     if (plastic) {
       Vec4<S>* stage = hElem4.get(size_t(2) * T);
-      for (uint32_t t = 0; t < T; ++t) {
-        const H* q = plastic + 10 * size_t(t);
-        stage[t] = Vec4<S>{S(q[0]), S(q[4]), S(q[8]), S(0.5 * (double(q[1]) + double(q[3])))};
-        stage[T + t] = Vec4<S>{S(0.5 * (double(q[2]) + double(q[6]))), S(0.5 * (double(q[5]) + double(q[7]))), S(q[9]),
-                               S(0)};
-      }
+      parallelFor(T, [&](size_t t0, size_t t1) {
+        for (size_t t = t0; t < t1; ++t) {
+          const H* q = plastic + 10 * t;
+          stage[t] = Vec4<S>{S(q[0]), S(q[4]), S(q[8]), S(0.5 * (double(q[1]) + double(q[3])))};
+          stage[T + t] = Vec4<S>{S(0.5 * (double(q[2]) + double(q[6]))), S(0.5 * (double(q[5]) + double(q[7]))),
+                                 S(q[9]), S(0)};
+        }
+      });
       plast.upload(stage, T, st, bd.elem_begin);
       plast.upload(stage + T, T, st, size_t(Tp) + bd.elem_begin);
     }
-    TL_CUDA(cudaStreamSynchronize(st));
   }
-  template <class H>
-  void getElems(const BodyDev& bd, const HostBody& h, H* rot, H* plastic) {
+  // Queues the downloads of a body's element state into the pinned stages.
+  void fetchElems(const BodyDev& bd, const HostBody& h, bool rot, bool plastic) {
     const uint32_t T = h.tets;
     if (rot) {
       S* stage = hElem.get(size_t(9) * T);
       for (int k = 0; k < 9; ++k) op.download(stage + size_t(k) * T, T, st, size_t(k) * Tp + bd.elem_begin);
-      TL_CUDA(cudaStreamSynchronize(st));
-      for (int k = 0; k < 9; ++k)
-        for (uint32_t t = 0; t < T; ++t) rot[9 * size_t(t) + k] = H(stage[size_t(k) * T + t]);
     }
     if (plastic) {
       Vec4<S>* stage = hElem4.get(size_t(2) * T);
       plast.download(stage, T, st, bd.elem_begin);
       plast.download(stage + T, T, st, size_t(Tp) + bd.elem_begin);
-      TL_CUDA(cudaStreamSynchronize(st));
-      for (uint32_t t = 0; t < T; ++t) {
-        H* q = plastic + 10 * size_t(t);
-        const Vec4<S> a0 = stage[t], a1 = stage[T + t];
-        q[0] = H(a0.x); q[1] = H(a0.w); q[2] = H(a1.x);
-        q[3] = H(a0.w); q[4] = H(a0.y); q[5] = H(a1.y);
-        q[6] = H(a1.x); q[7] = H(a1.y); q[8] = H(a0.z);
-        q[9] = H(a1.z);
-      }
+    }
+  }
+  // Converts the fetched element state (after the stream has finished).
+  template <class H>
+  void getElems(const BodyDev& bd, const HostBody& h, H* rot, H* plastic) {
+    (void)bd;
+    const uint32_t T = h.tets;
+    if (rot) {
+      S* stage = hElem.ptr;
+      parallelFor(T, [&](size_t t0, size_t t1) {
+        for (size_t t = t0; t < t1; ++t)
+          for (int k = 0; k < 9; ++k) rot[9 * t + k] = H(stage[size_t(k) * T + t]);
+      });
+    }
+    if (plastic) {
+      Vec4<S>* stage = hElem4.ptr;
+      parallelFor(T, [&](size_t t0, size_t t1) {
+        for (size_t t = t0; t < t1; ++t) {
+          H* q = plastic + 10 * t;
+          const Vec4<S> a0 = stage[t], a1 = stage[T + t];
+          q[0] = H(a0.x); q[1] = H(a0.w); q[2] = H(a1.x);
+          q[3] = H(a0.w); q[4] = H(a0.y); q[5] = H(a1.y);
+          q[6] = H(a1.x); q[7] = H(a1.y); q[8] = H(a0.z);
+          q[9] = H(a1.z);
+        }
+      });
     }
   }
 
@@ -730,30 +782,42 @@ struct System final : SystemBase {
                 const void* pl) override {
     const BodyDev& bd = bodyHost[b];
     const HostBody& h = hb[b];
+    // every array has its own pinned stage: conversions overlap the uploads
+    // queued before them, and the stream is waited on once
     if (dtype == TL_DTYPE_F64) {
-      if (x) setNodes(bd, h, u, static_cast<const double*>(x), true);
-      if (vv) setNodes(bd, h, v, static_cast<const double*>(vv), false);
-      if (aa) setNodes(bd, h, a, static_cast<const double*>(aa), false);
+      if (x) stageNodes(bd, h, u, static_cast<const double*>(x), true, hNode);
+      if (vv) stageNodes(bd, h, v, static_cast<const double*>(vv), false, hNodeV);
+      if (aa) stageNodes(bd, h, a, static_cast<const double*>(aa), false, hNodeA);
       setElems(bd, h, static_cast<const double*>(rot), static_cast<const double*>(pl));
     } else {
-      if (x) setNodes(bd, h, u, static_cast<const float*>(x), true);
-      if (vv) setNodes(bd, h, v, static_cast<const float*>(vv), false);
-      if (aa) setNodes(bd, h, a, static_cast<const float*>(aa), false);
+      if (x) stageNodes(bd, h, u, static_cast<const float*>(x), true, hNode);
+      if (vv) stageNodes(bd, h, v, static_cast<const float*>(vv), false, hNodeV);
+      if (aa) stageNodes(bd, h, a, static_cast<const float*>(aa), false, hNodeA);
       setElems(bd, h, static_cast<const float*>(rot), static_cast<const float*>(pl));
     }
+    TL_CUDA(cudaStreamSynchronize(st));
   }
   void stateGet(uint32_t b, int32_t dtype, void* x, void* vv, void* aa, void* rot, void* pl) override {
     const BodyDev& bd = bodyHost[b];
     const HostBody& h = hb[b];
+    // queue every download, wait once, then convert
+    Vec4<S>* sx = x ? hNode.get(h.nodes) : nullptr;
+    Vec4<S>* sv = vv ? hNodeV.get(h.nodes) : nullptr;
+    Vec4<S>* sa = aa ? hNodeA.get(h.nodes) : nullptr;
+    if (sx) u.download(sx, h.nodes, st, bd.node_begin);
+    if (sv) v.download(sv, h.nodes, st, bd.node_begin);
+    if (sa) a.download(sa, h.nodes, st, bd.node_begin);
+    fetchElems(bd, h, rot != nullptr, pl != nullptr);
+    TL_CUDA(cudaStreamSynchronize(st));
     if (dtype == TL_DTYPE_F64) {
-      if (x) getNodes(bd, h, u, static_cast<double*>(x), true);
-      if (vv) getNodes(bd, h, v, static_cast<double*>(vv), false);
-      if (aa) getNodes(bd, h, a, static_cast<double*>(aa), false);
+      if (x) unstageNodes(h, sx, static_cast<double*>(x), true);
+      if (vv) unstageNodes(h, sv, static_cast<double*>(vv), false);
+      if (aa) unstageNodes(h, sa, static_cast<double*>(aa), false);
       getElems(bd, h, static_cast<double*>(rot), static_cast<double*>(pl));
     } else {
-      if (x) getNodes(bd, h, u, static_cast<float*>(x), true);
-      if (vv) getNodes(bd, h, v, static_cast<float*>(vv), false);
-      if (aa) getNodes(bd, h, a, static_cast<float*>(aa), false);
+      if (x) unstageNodes(h, sx, static_cast<float*>(x), true);
+      if (vv) unstageNodes(h, sv, static_cast<float*>(vv), false);
+      if (aa) unstageNodes(h, sa, static_cast<float*>(aa), false);
       getElems(bd, h, static_cast<float*>(rot), static_cast<float*>(pl));
     }
   }
