@@ -37,17 +37,28 @@ from talus_b200.shard import aggregate  # noqa: E402
 from talus_b200.workloads import WORKLOADS, make_bodies, make_mesh  # noqa: E402
 
 
+def batch_sample_count(spec, budget_tets):
+    """Bodies at the start of the batch that fit `budget_tets` (at least one)."""
+    from talus_b200 import shard
+
+    tets = shard.tets_of(shard.batch_dims(spec["count"], spec["seed"], spec["lo"], spec["hi"]))
+    take, total = 0, 0
+    while take < len(tets) and (total + tets[take] <= budget_tets or take == 0):
+        total += int(tets[take])
+        take += 1
+    return take, total
+
+
 def sample_bodies(spec, budget_tets=8000):
     """Bounded CPU sample of a workload: a 1/64 sub-block (1/4 cells per axis,
     same strain rate) of a single body; the first bodies of a batch up to
     `budget_tets` tets."""
     if spec.get("batch"):
-        meshes, mats = make_bodies(spec)
-        take, total = 0, 0
-        while take < len(meshes) and total + meshes[take].tets <= budget_tets or take == 0:
-            total += meshes[take].tets
-            take += 1
-        return meshes[:take], mats[:take], f"the first {take} bodies of the batch ({total} tets)"
+        from talus_b200 import shard
+
+        take, total = batch_sample_count(spec, budget_tets)
+        meshes, mats = shard.batch_bodies_range(0, take, spec["count"], spec["seed"], spec["lo"], spec["hi"])
+        return meshes, mats, f"the first {take} bodies of the batch ({total} tets)"
     cells = tuple(max(2, c // 4) for c in spec["cells"])
     mesh, mat = make_mesh(spec, cells)
     return [mesh], [[mat]], (f"{cells[0]}x{cells[1]}x{cells[2]} cells ({mesh.tets} tets, 1/64 of the workload, "
@@ -181,10 +192,85 @@ def cpu_info():
     return model
 
 
+def _oracle_bodies(spec, indices):
+    """Oracle meshes, rest states and materials of the given batch bodies."""
+    from oracle import pyoracle as po
+    from talus_b200 import shard
+    from tests.helpers import oracle_material, to_oracle
+
+    out = []
+    for i in indices:
+        (m,), (mat,) = shard.batch_bodies_range(i, i + 1, spec["count"], spec["seed"], spec["lo"], spec["hi"])
+        om = to_oracle(m)
+        out.append((om, po.State.rest(om), [oracle_material(x) for x in mat]))
+    return out
+
+
+def _oracle_worker(conn, spec, indices):
+    """A host core stepping its share of the sampled batch bodies on request."""
+    from oracle import pyoracle as po
+
+    bodies = _oracle_bodies(spec, indices)
+    settings = po.Settings(law=po.LAW_SNH if spec["law"] == "snh" else po.LAW_COROTATED)
+    conn.send("ready")
+    while conn.recv() == "step":
+        for om, state, mats in bodies:
+            po.step(po.F32, om, state, mats, settings, (0.0, -9.81, 0.0), 1.0 / 60.0)
+        conn.send("done")
+
+
+class ParallelOracleRun:
+    """Batch bodies are independent, so the reference arm steps a batch sample
+    on every host core: one spawned process per core, each stepping its
+    round-robin share of the sampled bodies with the single-threaded oracle
+    step (the reference's own per-body step is serial)."""
+
+    def __init__(self, spec, workers, budget_tets_per_core=8000):
+        import multiprocessing as mp
+
+        from talus_b200 import shard
+
+        take, _ = batch_sample_count(spec, budget_tets_per_core * workers)
+        take = max(take, min(spec["count"], 4 * workers))  # several bodies per process, for balance
+        tets = shard.tets_of(shard.batch_dims(spec["count"], spec["seed"], spec["lo"], spec["hi"]))
+        self.tets = total = int(tets[:take].sum())
+        self.sample = f"the first {take} bodies of the batch ({total} tets)"
+        ctx = mp.get_context("spawn")
+        self.conns, self.procs = [], []
+        for w in range(workers):
+            parent, child = ctx.Pipe()
+            p = ctx.Process(target=_oracle_worker, args=(child, spec, list(range(w, take, workers))), daemon=True)
+            p.start()
+            self.conns.append(parent)
+            self.procs.append(p)
+        for c in self.conns:
+            if c.recv() != "ready":
+                raise RuntimeError("oracle worker failed")
+
+    def step(self):
+        for c in self.conns:
+            c.send("step")
+        for c in self.conns:
+            c.recv()
+
+    def close(self):
+        for c in self.conns:
+            c.send("stop")
+        for p in self.procs:
+            p.join(timeout=30)
+
+
+def host_workers():
+    return max(1, min(64, len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count() or 1))
+
+
 class OracleRun:
     """The oracle (the reference's algorithm restated, FP32 like the
     reference), single-threaded like the reference step
     (Settings::stepThreads is never read, solver.h:73-74)."""
+
+    def close(self):
+        pass
 
     def __init__(self, spec):
         from oracle import pyoracle as po
@@ -219,22 +305,25 @@ def cpu_sample(spec, budget_s=15.0, max_steps=400):
 def run_reference(args, spec, rank, world):
     if rank != 0:
         return
-    run = OracleRun(spec)
+    workers = host_workers() if spec.get("batch") else 1
+    run = ParallelOracleRun(spec, workers) if workers > 1 else OracleRun(spec)
     for _ in range(args.warmup):
         run.step()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         run.step()
     secs = time.perf_counter() - t0
+    run.close()
     value = run.tets * args.steps / secs
     sample = (f"oracle FP32 restatement of deformable::step (the reference cannot be built here: GLM/Eigen "
-              f"fetched at configure time), {run.sample} of {args.workload}, 1 thread ({cpu_info()})")
+              f"fetched at configure time), {run.sample} of {args.workload}, {workers} host "
+              f"{'process' if workers == 1 else 'processes'} ({cpu_info()})")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "tets": run.tets, "sample": run.sample},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
