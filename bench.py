@@ -59,6 +59,10 @@ def sample_bodies(spec, budget_tets=8000):
         take, total = batch_sample_count(spec, budget_tets)
         meshes, mats = shard.batch_bodies_range(0, take, spec["count"], spec["seed"], spec["lo"], spec["hi"])
         return meshes, mats, f"the first {take} bodies of the batch ({total} tets)"
+    full = 6 * spec["cells"][0] * spec["cells"][1] * spec["cells"][2]
+    if full <= 50000:  # small workloads are timed whole
+        mesh, mat = make_mesh(spec)
+        return [mesh], [[mat]], f"the whole workload ({mesh.tets} tets)"
     cells = tuple(max(2, c // 4) for c in spec["cells"])
     mesh, mat = make_mesh(spec, cells)
     return [mesh], [[mat]], (f"{cells[0]}x{cells[1]}x{cells[2]} cells ({mesh.tets} tets, 1/64 of the workload, "
