@@ -1744,6 +1744,128 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, 
   }
 }
 
+// ---- software-pipelined tile loop of the batched PCG ----
+// A block works through many tiles per phase.  While it computes tile k, its
+// threads copy tile k+1's tables (local CSR, corner slots, node list) and
+// element operators into the other half of a double-buffered shared stage
+// (cp.async), and tile k+2's slot range comes into a register, so a tile
+// waits for only one dependent L2/DRAM round trip: its node values.
+struct TileTables {
+  uint16_t ent[4 * TILE];
+  uint16_t off[TILE_OFF_STRIDE];
+  uint16_t pad[4];  // keeps the struct a multiple of 16 bytes
+  uint2 eloc[TILE];
+  uint32_t node[4 * TILE];
+};
+static_assert(sizeof(TileTables) % 16 == 0 && offsetof(TileTables, off) % 8 == 0 &&
+                  offsetof(TileTables, eloc) % 8 == 0 && offsetof(TileTables, node) % 4 == 0,
+              "cp.async destinations of the tile stage must stay aligned");
+template <class S, int LAW, bool TANGENT> __host__ __device__ constexpr size_t pipeBytes() {
+  return 2 * (sizeof(TileTables) + stageBytes<S, LAW, TANGENT>());
+}
+__device__ __forceinline__ void cpAsyncWaitNewest() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Queues the copies of one tile into a stage buffer (all threads take part).
+template <class S, int LAW, bool TANGENT>
+__device__ __forceinline__ void issueTile(const Sys<S>& s, uint32_t tile, uint2 meta, unsigned char* half) {
+  TileTables& tt = *reinterpret_cast<TileTables*>(half);
+  const uint32_t t = threadIdx.x, e = tile * TILE + t;  // e < Tp: padded elements have zeroed operators
+  stageOperator<S, LAW, TANGENT>(s, e, half + sizeof(TileTables));
+  cpAsync<8>(&tt.eloc[t], &s.eloc[e]);
+  cpAsync<8>(&tt.ent[4 * t], s.tile_ent + size_t(tile) * 4 * TILE + 4 * t);
+  const uint16_t* off = s.tile_off + size_t(tile) * TILE_OFF_STRIDE;
+  if (4u * t <= meta.y) cpAsync<8>(&tt.off[4 * t], off + 4 * t);
+  if (t == 0 && meta.y >= 4u * TILE) cpAsync<8>(&tt.off[4 * TILE], off + 4 * TILE);
+  for (uint32_t j = t; j < meta.y; j += TILE) cpAsync<4>(&tt.node[j], s.tile_node + meta.x + j);
+}
+
+// The matvec of one staged tile (same arithmetic and order as matvecTile).
+template <class S, int LAW, bool TANGENT>
+__device__ __forceinline__ void computeTile(const Sys<S>& s, uint32_t tile, uint2 meta, const unsigned char* half,
+                                            const Vec4<S>* X, S blend, S (*buf)[4 * TILE], uint32_t elemEnd) {
+  const TileTables& tt = *reinterpret_cast<const TileTables*>(half);
+  const uint32_t e = tile * TILE + threadIdx.x;
+  for (uint32_t j = threadIdx.x; j < meta.y; j += TILE) {
+    const V3<S> v = stagedValue<S, false>(s, tt.node[j], X, blend, false, S(0));
+    buf[0][j] = v.x;
+    buf[1][j] = v.y;
+    buf[2][j] = v.z;
+  }
+  __syncthreads();
+  V3<S> y[4] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  if (e < elemEnd) {
+    const uint2 loc = tt.eloc[threadIdx.x];
+    const uint32_t l[4] = {loc.x & 0xffffu, loc.x >> 16, loc.y & 0xffffu, loc.y >> 16};
+    V3<S> pe[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) pe[c] = {buf[0][l[c]], buf[1][l[c]], buf[2][l[c]]};
+    applyOperator<S, LAW, TANGENT>(stagedOperator<S, LAW, TANGENT>(half + sizeof(TileTables)), pe, y);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    buf[0][c * TILE + threadIdx.x] = y[c].x;
+    buf[1][c * TILE + threadIdx.x] = y[c].y;
+    buf[2][c * TILE + threadIdx.x] = y[c].z;
+  }
+  __syncthreads();
+  for (uint32_t j = threadIdx.x; j < meta.y; j += TILE) {
+    const uint32_t k0 = tt.off[j], k1 = tt.off[j + 1];
+    S ax = 0, ay = 0, az = 0;
+    for (uint32_t k = k0; k < k1; ++k) {
+      const uint32_t code = tt.ent[k];
+      const uint32_t q = (code & 3u) * TILE + (code >> 2);
+      ax += buf[0][q];
+      ay += buf[1][q];
+      az += buf[2][q];
+    }
+    s.slot_part[meta.x + j] = Vec4<S>{ax, ay, az, S(0)};
+  }
+  __syncthreads();
+}
+
+// Every tile of this block whose body takes part in the pass (and, when
+// skipDone, has not converged), in order, pipelined.  X: multiply X instead
+// of p = z + blend p_prev.  Done flags do not change during the phase.
+template <class S, int LAW, bool TANGENT>
+__device__ __forceinline__ void matvecPipelined(const Sys<S>& s, uint32_t pass, const Vec4<S>* X, bool skipDone,
+                                                unsigned char* dyn, S (*buf)[4 * TILE]) {
+  constexpr uint32_t NONE = 0xffffffffu;
+  constexpr size_t HALF = sizeof(TileTables) + stageBytes<S, LAW, TANGENT>();
+  const uint32_t G = gridDim.x;
+  auto next = [&](uint32_t t) -> uint32_t {
+    for (; t < s.elem_tiles; t += G) {
+      const uint32_t b = s.elem_tile_body[t];
+      if (bodyActive(s, b, pass) && !(skipDone && __ldcg(&s.cg[b].done))) return t;
+    }
+    return NONE;
+  };
+  uint32_t t0 = next(blockIdx.x);
+  if (t0 == NONE) return;
+  uint2 m0 = __ldg(&s.tile_meta[t0]);
+  uint32_t t1 = next(t0 + G);
+  uint2 m1 = t1 != NONE ? __ldg(&s.tile_meta[t1]) : make_uint2(0u, 0u);
+  issueTile<S, LAW, TANGENT>(s, t0, m0, dyn);
+  cpAsyncCommit();
+  for (uint32_t k = 0; t0 != NONE; ++k) {
+    unsigned char* cur = dyn + (k & 1u) * HALF;
+    if (t1 != NONE) issueTile<S, LAW, TANGENT>(s, t1, m1, dyn + ((k + 1u) & 1u) * HALF);
+    cpAsyncCommit();
+    const uint32_t t2 = t1 != NONE ? next(t1 + G) : NONE;
+    const uint2 m2 = t2 != NONE ? __ldg(&s.tile_meta[t2]) : make_uint2(0u, 0u);
+    cpAsyncWaitNewest();  // this thread's copies of tile t0 have landed
+    __syncthreads();      // and everyone else's
+    const uint32_t b0 = s.elem_tile_body[t0];
+    const S blend = X ? S(0) : S(__ldcg(&s.cg[b0].blend));
+    computeTile<S, LAW, TANGENT>(s, t0, m0, cur, X, blend, buf, s.body[b0].elem_end);
+    t0 = t1;
+    m0 = m1;
+    t1 = t2;
+    m1 = m2;
+  }
+  cpAsyncWaitAll();
+}
+
 // Persistent PCG for a system of MANY bodies (the batched form): the phases of
 // kPcg1 with the two-level assembly, but every body keeps its own scalars
 // (CgBodyDev) and stops on its own test.  Per-tile partials are summed over a
@@ -1755,19 +1877,13 @@ template <class S, int LAW, bool TANGENT>
 __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2)
     kPcgBatch(Sys<S> s, Vec4<S>* X, uint32_t pass, uint32_t x0zero) {
   __shared__ S buf[3][4 * TILE];
-  extern __shared__ __align__(16) unsigned char tlStage[];  // stageBytes<S, LAW, TANGENT>()
-  __shared__ __align__(8) uint16_t sOff[TILE_OFF_STRIDE];
-  __shared__ __align__(8) uint16_t sEnt[4 * TILE];
+  extern __shared__ __align__(16) unsigned char tlStage[];  // pipeBytes<S, LAW, TANGENT>()
   const uint32_t G = gridDim.x;
   const S zero = S(0);
   unsigned int bar = 0;
   // ---- init: r = right - A x (anchored rows 0), z = P r, p_prev = 0
   if (!x0zero) {
-    for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G) {
-      const uint32_t b = s.elem_tile_body[tile];
-      if (!bodyActive(s, b, pass)) continue;
-      matvecTile<S, LAW, TANGENT, true>(s, tile, X, zero, buf, sOff, sEnt, s.body[b].elem_end, tlStage);
-    }
+    matvecPipelined<S, LAW, TANGENT>(s, pass, X, false, tlStage, buf);
     if (!countBarrier(s.sync, bar)) return;
   }
   for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
@@ -1829,11 +1945,7 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2)
   for (;;) {
     if (*(volatile int*)&s.sync->active <= 0) break;  // uniform: no block decrements between here and barrier A
     // ---- A
-    for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += G) {
-      const uint32_t b = s.elem_tile_body[tile];
-      if (!bodyActive(s, b, pass) || __ldcg(&s.cg[b].done)) continue;
-      matvecTile<S, LAW, TANGENT, true>(s, tile, nullptr, S(__ldcg(&s.cg[b].blend)), buf, sOff, sEnt, s.body[b].elem_end, tlStage);
-    }
+    matvecPipelined<S, LAW, TANGENT>(s, pass, nullptr, true, tlStage, buf);
     if (!countBarrier(s.sync, bar)) return;
     // ---- B
     for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {

@@ -654,10 +654,10 @@ struct System final : SystemBase {
     pcg1PerSm[0][1] = perSm((const void*)kPcg1<S, 0, true>, sizeof(TileCache));
     pcg1PerSm[1][0] = perSm((const void*)kPcg1<S, 1, false>, sizeof(TileCache));
     pcg1PerSm[1][1] = perSm((const void*)kPcg1<S, 1, true>, sizeof(TileCache));
-    batchPerSm[0][0] = perSm((const void*)kPcgBatch<S, 0, false>, stageBytes<S, 0, false>());
-    batchPerSm[0][1] = perSm((const void*)kPcgBatch<S, 0, true>, stageBytes<S, 0, true>());
-    batchPerSm[1][0] = perSm((const void*)kPcgBatch<S, 1, false>, stageBytes<S, 1, false>());
-    batchPerSm[1][1] = perSm((const void*)kPcgBatch<S, 1, true>, stageBytes<S, 1, true>());
+    batchPerSm[0][0] = perSm((const void*)kPcgBatch<S, 0, false>, pipeBytes<S, 0, false>());
+    batchPerSm[0][1] = perSm((const void*)kPcgBatch<S, 0, true>, pipeBytes<S, 0, true>());
+    batchPerSm[1][0] = perSm((const void*)kPcgBatch<S, 1, false>, pipeBytes<S, 1, false>());
+    batchPerSm[1][1] = perSm((const void*)kPcgBatch<S, 1, true>, pipeBytes<S, 1, true>());
     int most = 0;
     for (auto& row : pcg1PerSm)
       for (int n : row) most = std::max(most, n * ctx->sms);
@@ -853,8 +853,8 @@ struct System final : SystemBase {
     const int idx = law == TL_LAW_SNH ? 1 : 0;
     if (profiling) mark(2, true);
     (void)tg;
-    const size_t dyn = idx ? (tangent ? stageBytes<S, 1, true>() : stageBytes<S, 1, false>())
-                           : (tangent ? stageBytes<S, 0, true>() : stageBytes<S, 0, false>());
+    const size_t dyn = idx ? (tangent ? pipeBytes<S, 1, true>() : pipeBytes<S, 1, false>())
+                           : (tangent ? pipeBytes<S, 0, true>() : pipeBytes<S, 0, false>());
     if (B == 1) {  // single body: two-level assembly, per-block partials
       void* args[] = {&s, &X, &xz};
       const void* fn = idx ? (tangent ? (const void*)kPcg1<S, 1, true> : (const void*)kPcg1<S, 1, false>)
