@@ -383,21 +383,7 @@ __device__ __forceinline__ uint32_t blockCount(bool flag) {
   __syncthreads();
   return r;
 }
-// Block-wide min / max of 64-bit keys; result valid in thread 0.
-__device__ __forceinline__ unsigned long long blockMinKey(unsigned long long k) {
-  __shared__ unsigned long long red[TILE / 32];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const unsigned long long q = __shfl_down_sync(0xffffffffu, k, o);
-    k = q < k ? q : k;
-  }
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = k;
-  __syncthreads();
-  if (threadIdx.x == 0)
-    for (int w = 1; w < TILE / 32; ++w) k = red[w] < k ? red[w] : k;
-  __syncthreads();
-  return k;
-}
+// Block-wide max of 64-bit keys; result valid in thread 0.
 __device__ __forceinline__ unsigned long long blockMaxKey(unsigned long long k) {
   __shared__ unsigned long long red[TILE / 32];
 #pragma unroll
@@ -1319,33 +1305,12 @@ __device__ __forceinline__ void sumBlocksAll(const double* part, double (&out)[N
   __syncthreads();
 }
 
-// Sum of the per-block partials field f of every block, in block order; the
-// same value in every block (block-wide call, result broadcast).
-__device__ __forceinline__ double sumBlocks(const double* part, unsigned int field) {
-  __shared__ double total;
-  if (threadIdx.x < 32) {
-    double v = 0.0;
-    for (unsigned int b = threadIdx.x; b < gridDim.x; b += 32) v += __ldcg(part + size_t(field) * gridDim.x + b);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (threadIdx.x == 0) total = v;
-  }
-  __syncthreads();
-  const double r = total;
-  __syncthreads();
-  return r;
-}
-
 // One element tile of the matvec: y_e = h_eff^2 (R K R^T p)_e for its 256
 // elements, then the tile-local sums of y_e per touched node, in ascending
 // element order, written to the tile's slots.  The tile's distinct nodes are
 // staged once in shared memory (p = z + blend p_prev formed once per node, or
 // X for the initial residual), elements read their corners from there by
 // local index, and the tile's local CSR is fetched while the elements compute.
-// STAGE: copy the element operators into shared memory (cp.async) while the
-// nodes are staged.  It pays on large batched systems (more loads in flight,
-// fewer registers); the single-body kernel, latency-bound on few tiles per
-// block, is faster loading them directly (measured on B200).
 // The preconditioned residual of kPcg1 after the deferred update
 //   s = w + beta s,  r = r - alpha s,  u = P r
 // from the stored vectors; every place that needs u (the matvec's node stage,
@@ -1373,16 +1338,12 @@ __device__ __forceinline__ V3<S> stagedValue(const Sys<S>& s, uint32_t n, const 
   return fmaV(blend, xyz(ld4cg(&s.p[n])), xyz(ld4cg(&s.z[n])));
 }
 
-template <class S, int LAW, bool TANGENT, bool STAGE, bool CGU = false>
+template <class S, int LAW, bool TANGENT, bool CGU = false>
 __device__ __forceinline__ void matvecTile(const Sys<S>& s, uint32_t tile, const Vec4<S>* X, S blend,
                                            S (*buf)[4 * TILE], uint16_t* sOff, uint16_t* sEnt, uint32_t elemEnd,
-                                           unsigned char* stage, bool update = false, S alpha = S(0)) {
+                                           bool update = false, S alpha = S(0)) {
   const uint32_t e = tile * TILE + threadIdx.x;
   const bool live = e < elemEnd;
-  if (STAGE) {
-    if (live) stageOperator<S, LAW, TANGENT>(s, e, stage);
-    cpAsyncCommit();
-  }
   const uint2 meta = __ldg(&s.tile_meta[tile]);
   const uint2 entv = __ldg(reinterpret_cast<const uint2*>(s.tile_ent + size_t(tile) * 4 * TILE) + threadIdx.x);
   const uint16_t* off = s.tile_off + size_t(tile) * TILE_OFF_STRIDE;
@@ -1406,12 +1367,7 @@ __device__ __forceinline__ void matvecTile(const Sys<S>& s, uint32_t tile, const
     V3<S> pe[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) pe[c] = {buf[0][l[c]], buf[1][l[c]], buf[2][l[c]]};
-    if (STAGE) {
-      cpAsyncWaitAll();
-      applyOperator<S, LAW, TANGENT>(stagedOperator<S, LAW, TANGENT>(stage), pe, y);
-    } else {
-      elementApply<S, LAW, TANGENT>(s, e, pe, y);
-    }
+    elementApply<S, LAW, TANGENT>(s, e, pe, y);
   }
   __syncthreads();  // node values consumed: buf now holds y, buf[k][c TILE + element]
 #pragma unroll
@@ -1579,7 +1535,7 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, 
   if (!x0zero) {
     for (uint32_t tile = blockIdx.x, k = 0; tile < s.elem_tiles; tile += G, ++k) {
       if (cached) matvecTileCached<S, LAW, TANGENT, true>(s, cache, k, tile, X, zero, buf, bd.elem_end, false, zero);
-      else matvecTile<S, LAW, TANGENT, false>(s, tile, X, zero, buf, sOff, sEnt, bd.elem_end, nullptr);
+      else matvecTile<S, LAW, TANGENT>(s, tile, X, zero, buf, sOff, sEnt, bd.elem_end);
     }
     if (!countBarrier(s.sync, bar)) return;
   }
@@ -1647,8 +1603,8 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, 
           matvecTileCached<S, LAW, TANGENT, true>(s, cache, k, tile, nullptr, S(beta), buf, bd.elem_end, update,
                                                   S(alpha));
         else
-          matvecTile<S, LAW, TANGENT, false, true>(s, tile, nullptr, S(beta), buf, sOff, sEnt, bd.elem_end, nullptr,
-                                                   update, S(alpha));
+          matvecTile<S, LAW, TANGENT, true>(s, tile, nullptr, S(beta), buf, sOff, sEnt, bd.elem_end, update,
+                                            S(alpha));
       }
       ++applications;
       if (!countBarrier(s.sync, bar)) return;

@@ -224,7 +224,6 @@ struct System final : SystemBase {
   DevBuf<CgReportDev> cgrep;
   DevBuf<GridSyncDev> sync;
   bool hasEyoung = false;
-  int pcgGrid[2] = {0, 0};
   // TL_FLAG_PROFILE: event pairs around kernel classes, resolved at step end
   bool profiling = false;
   bool tracing = false;
@@ -545,14 +544,6 @@ struct System final : SystemBase {
     cgrep.alloc(B);
     sync.alloc(1);
     sync.zero(st);
-    // cooperative grid sizes of the PCG kernel per law
-    int perSm = 0;
-    TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kPcg<S, 0>, TILE, 0));
-    pcgGrid[0] = std::max(1, std::min(perSm * ctx->sms, int(std::max(nodeTiles, elemTiles))));
-    if (perSm < 1) throw StatusError{TL_ERR_CUDA, "PCG kernel cannot be resident"};
-    TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kPcg<S, 1>, TILE, 0));
-    pcgGrid[1] = std::max(1, std::min(perSm * ctx->sms, int(std::max(nodeTiles, elemTiles))));
-    if (perSm < 1) throw StatusError{TL_ERR_CUDA, "PCG kernel cannot be resident"};
     buildTiles(hTet, hElemTileBody);
     TL_CUDA(cudaStreamSynchronize(st));
   }
