@@ -62,7 +62,8 @@ typedef struct tl_material {
   double density;
   double youngs_modulus;
   double poissons_ratio;
-  double stiffness_damping;  /* must be 0: stiffness damping is not implemented (TL_ERR_UNSUPPORTED) */
+  double stiffness_damping;  /* >0: rigid-motion-free stiffness damping, corotated law only (factor.cc:755-855);
+                                tl_step_noalloc returns TL_ERR_UNSUPPORTED for it */
   double yield_stress;       /* +inf: never yields (material.cc:747-749) */
   double hardening_modulus;
 } tl_material;

@@ -484,6 +484,122 @@ template <class R> M3<R> snhDiagonal(const V3<R>& g, const M3<R>& f, R volume, c
 
 // ------------------------------------------------------------- solver ----
 
+// ----------------------------------------------------------- damping ----
+// Stiffness damping (factor.cc:755-855, 183-272, 274-298; solver.cc:625-902):
+// per element with weight tau > 0, D(p) = P_rigid^perp R K R^T P_rigid^perp p,
+// where the projection removes the rigid motion fitted to the corners.
+
+// factor.cc:183-272: symmetric 3x3 pseudo-inverse by cyclic Jacobi rotations,
+// keeping the eigenvalues above `floor`.
+inline M3<double> pseudoInverse(const M3<double>& held, double floor) {
+  double reduced[3][3], basis[3][3];
+  for (int row = 0; row < 3; ++row)
+    for (int col = 0; col < 3; ++col) {
+      reduced[row][col] = held[col][row];
+      basis[row][col] = row == col ? 1.0 : 0.0;
+    }
+  const int pairs[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+  for (int sweep = 0; sweep < 64; ++sweep) {
+    double off = 0.0, size = 0.0;
+    for (int row = 0; row < 3; ++row) {
+      size += reduced[row][row] * reduced[row][row];
+      for (int col = row + 1; col < 3; ++col) off += reduced[row][col] * reduced[row][col];
+    }
+    if (!(off > 1.0e-30 * size)) break;
+    for (const auto& pr : pairs) {
+      const int p = pr[0], q = pr[1];
+      if (reduced[p][q] == 0.0) continue;
+      const double theta = (reduced[q][q] - reduced[p][p]) / (2.0 * reduced[p][q]);
+      const double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::abs(theta) + std::sqrt(theta * theta + 1.0));
+      const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+      for (int k = 0; k < 3; ++k) {
+        const double a = reduced[k][p], b = reduced[k][q];
+        reduced[k][p] = c * a - sn * b;
+        reduced[k][q] = sn * a + c * b;
+      }
+      for (int k = 0; k < 3; ++k) {
+        const double a = reduced[p][k], b = reduced[q][k];
+        reduced[p][k] = c * a - sn * b;
+        reduced[q][k] = sn * a + c * b;
+      }
+      for (int k = 0; k < 3; ++k) {
+        const double a = basis[k][p], b = basis[k][q];
+        basis[k][p] = c * a - sn * b;
+        basis[k][q] = sn * a + c * b;
+      }
+    }
+  }
+  M3<double> made(0.0);
+  for (int axis = 0; axis < 3; ++axis) {
+    const double value = reduced[axis][axis];
+    if (!(value > floor)) continue;
+    for (int row = 0; row < 3; ++row)
+      for (int col = 0; col < 3; ++col) made[col][row] += basis[row][axis] * basis[col][axis] / value;
+  }
+  return made;
+}
+
+template <class R> struct RigidFit { std::array<V3<R>, 4> arms{}; M3<R> inverse{R(0)}; };
+
+// factor.cc:780-817: arms from the centroid, inverse of the inertia tensor
+// sum |a|^2 I - a a^T (pseudo-inverse when it is near singular), in FP64.
+template <class R> RigidFit<R> rigidFit(const std::array<V3<R>, 4>& corners) {
+  RigidFit<R> fit;
+  V3<double> centre;
+  for (const V3<R>& c : corners) centre += V3<double>(double(c.x), double(c.y), double(c.z));
+  centre = (1.0 / 4.0) * centre;
+  M3<double> inertia(0.0);
+  for (int k = 0; k < 4; ++k) {
+    const V3<double> d = V3<double>(double(corners[k].x), double(corners[k].y), double(corners[k].z)) - centre;
+    fit.arms[k] = V3<R>(R(d.x), R(d.y), R(d.z));
+    const V3<double> a(double(fit.arms[k].x), double(fit.arms[k].y), double(fit.arms[k].z));
+    inertia = inertia + (dot(a, a) * M3<double>(1.0) - outer(a, a));
+  }
+  const double third = (inertia[0][0] + inertia[1][1] + inertia[2][2]) / 3.0;
+  const M3<double> inv = determinant(inertia) > 1.0e-6 * third * third * third ? inverse(inertia)
+                                                                                 : pseudoInverse(inertia, 1.0e-6 * third);
+  for (int col = 0; col < 3; ++col) fit.inverse[col] = V3<R>(R(inv[col].x), R(inv[col].y), R(inv[col].z));
+  return fit;
+}
+
+// factor.cc:819-841
+template <class R> void removeRigid(const RigidFit<R>& fit, std::array<V3<R>, 4>& values) {
+  V3<R> mean, moment;
+  for (int k = 0; k < 4; ++k) {
+    mean += values[k];
+    moment += cross(fit.arms[k], values[k]);
+  }
+  mean = (R(1) / R(4)) * mean;
+  const V3<R> spin = fit.inverse * moment;
+  for (int k = 0; k < 4; ++k) values[k] -= mean + cross(spin, fit.arms[k]);
+}
+
+// factor.cc:843-853
+template <class R>
+void applyDamping(const RigidFit<R>& fit, const M3<R>& rotation, const TetStiffness<R>& k,
+                  const std::array<V3<R>, 4>& direction, std::array<V3<R>, 4>& result) {
+  std::array<V3<R>, 4> relative = direction;
+  removeRigid(fit, relative);
+  applyStiffness(relative, rotation, k, result);
+  removeRigid(fit, result);
+}
+
+// factor.cc:274-298, 1041-1047: the diagonal corner blocks of D (columns from
+// unit directions).
+template <class R>
+std::array<M3<R>, 4> dampingDiagonal(const RigidFit<R>& fit, const M3<R>& rotation, const TetStiffness<R>& k) {
+  std::array<M3<R>, 4> out;
+  std::array<V3<R>, 4> unit, column;
+  for (int corner = 0; corner < 4; ++corner)
+    for (int axis = 0; axis < 3; ++axis) {
+      unit.fill(V3<R>());
+      unit[corner][axis] = R(1);
+      applyDamping(fit, rotation, k, unit, column);
+      out[corner][axis] = column[corner];
+    }
+  return out;
+}
+
 // solver.cc:531-566
 template <class R> struct IntegratorRule { R alphaMass{0}, alphaForce{0}, beta{0.25}, gamma{0.5}; };
 template <class R> IntegratorRule<R> integratorRule(R spectral) {
@@ -513,6 +629,7 @@ template <class R> struct Element {
   Lame<R> moduli;
   R yieldStress, hardening;
   bool yields;
+  R tau;  // stiffness damping weight (factor.cc:755-759)
 };
 
 template <class R> struct Solver {
@@ -531,6 +648,9 @@ template <class R> struct Solver {
   std::vector<V3<R>> position, velocity, acceleration;
   std::vector<M3<R>> rotation;
   std::vector<PlasticPoint<R>> plastic;
+  std::vector<RigidFit<R>> fits;         // Damping::fits at the last assemble
+  bool damped = false;
+  R dampScale{0};                        // Damping::scale = (1 - alpha_f) gamma h (solver.cc:3590)
   std::vector<M3<R>> snhGradient;        // SNH operator state: F per tet
   std::vector<R> snhChange;              // SNH operator state: J - 1 per tet
   // scratch (solver.cc:395-420)
@@ -604,7 +724,29 @@ template <class R> struct Solver {
         diagonal[el.nodes[n]][2] += scale * diag[n][2];
       }
     }
+    if (damped) {  // fitDamping, blockDamping, addDampingDiagonal (solver.cc:645-681, 755-804, 806-830)
+      for (uint32_t e = 0; e < T; ++e) {
+        const Element<R>& el = elements[e];
+        if (el.tau == R(0)) continue;
+        fits[e] = rigidFit(gather(at, el));
+        const std::array<M3<R>, 4> made = dampingDiagonal(fits[e], rotation[e], store[e]);
+        const R weight = dampScale * el.tau;
+        for (int n = 0; n < 4; ++n) diagonal[el.nodes[n]] = diagonal[el.nodes[n]] + weight * made[n];
+      }
+    }
     return out;
+  }
+
+  // addDamping (solver.cc:683-750): output += weight tau D(input) per element.
+  void addDamping(R weight, const std::vector<V3<R>>& input, std::vector<V3<R>>& output) {
+    std::array<V3<R>, 4> produced;
+    for (uint32_t e = 0; e < T; ++e) {
+      const Element<R>& el = elements[e];
+      if (el.tau == R(0)) continue;
+      applyDamping(fits[e], rotation[e], store[e], gather(input, el), produced);
+      const R scaled = weight * el.tau;
+      for (int n = 0; n < 4; ++n) output[el.nodes[n]] += scaled * produced[n];
+    }
   }
 
   // solver.cc:904-1048 applySystem (tets, no damping, not stressed)
@@ -622,6 +764,7 @@ template <class R> struct Solver {
       }
       for (int n = 0; n < 4; ++n) output[el.nodes[n]] += scale * produced[n];
     }
+    if (damped) addDamping(dampScale, input, output);  // solver.cc:1006-1007
     for (uint32_t n = 0; n < V; ++n)
       if (anchored[n]) output[n] = V3<R>();
     if (report) ++report->operator_applications;
@@ -765,7 +908,8 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
     el.restInverse = loadRowMajor<R>(mesh->rest_inverse + 9 * e);
     el.volume = R(mesh->volume[e]);
     const or_material& m = mesh->lane[e] < lanes ? materials[mesh->lane[e]] : DEFAULT;  // material.cc:9-16
-    if (m.stiffness_damping > 0.0) return -3;  // stiffness damping: not in this restatement
+    el.tau = std::isfinite(m.stiffness_damping) && m.stiffness_damping > 0.0 ? R(m.stiffness_damping) : R(0);
+    s.damped = s.damped || el.tau > R(0);
     const R youngs = mesh->element_youngs ? R(mesh->element_youngs[e]) : R(m.youngs_modulus);
     el.moduli = lame(youngs, R(m.poissons_ratio));
     el.yieldStress = R(m.yield_stress);
@@ -780,6 +924,9 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
     s.plastic[e] = p;
   }
   if (s.law == OR_LAW_SNH) anyYields = false;  // SNH runs elastic only
+  // damping is defined with the corotated stiffness and committed rotation
+  if (s.damped && s.law == OR_LAW_SNH) return -3;
+  if (s.damped) s.fits.assign(T, RigidFit<R>());
   auto sized = [&](std::vector<V3<R>>& v) { v.assign(V, V3<R>()); };
   sized(s.force); sized(s.right); sized(s.residual); sized(s.direction); sized(s.applied); sized(s.conditioned);
   sized(s.increment); sized(s.restart); sized(s.shifted); sized(s.weighted); sized(s.carried); sized(s.evaluated);
@@ -800,6 +947,8 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
   const R inner = dt / R(substeps);
   const EffectiveSystem<R> effective = effectiveSystem(rule, inner);
   const R carryScale = (R(0.5) - rule.beta) * inner * inner;
+  s.dampScale = (R(1) - rule.alphaForce) * rule.gamma * inner;
+  std::vector<V3<R>> viscous(s.damped ? V : 0u), viscousVelocity(s.damped ? V : 0u);
   const int mode = OR_ROTATION_INVERTIBLE;  // anchored meshes never float (solver.cc:3589-3590)
   report->substeps += substeps;
   R elastic = 0;
@@ -816,8 +965,21 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
     auto assemble = [&](const std::vector<V3<R>>& at, R margin, bool mapping = true) {
       return s.assemble(effective.step, at, false, margin, mode, mapping);
     };
-    // solver.cc:3746-3806 balance (no damping)
+    // solver.cc:3746-3806 balance
     auto balance = [&](const std::vector<V3<R>>* taken) {
+      if (s.damped) {  // viscous force of the lagged velocity (solver.cc:3747-3778)
+        const R lag = (R(1) - rule.alphaForce) * inner;
+        for (uint32_t n = 0; n < V; ++n) {
+          if (s.anchored[n]) {
+            viscousVelocity[n] = V3<R>();
+            continue;
+          }
+          viscousVelocity[n] = s.velocity[n] + (lag * (R(1) - rule.gamma)) * s.carried[n];
+          if (taken) viscousVelocity[n] += (lag * rule.gamma) * (*taken)[n];
+        }
+        std::fill(viscous.begin(), viscous.end(), V3<R>());
+        s.addDamping(R(1), viscousVelocity, viscous);
+      }
       for (uint32_t n = 0; n < V; ++n) {
         if (s.anchored[n]) {
           s.velocity[n] = s.prescribed[n];
@@ -828,6 +990,7 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
         const R m = s.mass[n];
         s.right[n] = s.force[n] + s.drive[n] - (rule.alphaMass * m) * s.carried[n];
         if (taken) s.right[n] -= (effective.inertia * m) * (*taken)[n];
+        if (s.damped) s.right[n] -= viscous[n];
         s.diagonal[n][0].x += effective.inertia * m;
         s.diagonal[n][1].y += effective.inertia * m;
         s.diagonal[n][2].z += effective.inertia * m;
@@ -1135,6 +1298,16 @@ constexpr uint32_t KUHN[6][4] = {{0, 1, 3, 7}, {0, 3, 2, 7}, {0, 2, 6, 7}, {0, 6
 
 }  // namespace
 
+template <class R>
+int dampingImpl(const double* at, const double* rotation, const double* rinv, double volume, const or_material* m,
+                const double* direction, double* out) {
+  const TetStiffness<R> k = tetStiffness(loadRowMajor<R>(rinv), R(volume), lame(R(m->youngs_modulus), R(m->poissons_ratio)));
+  std::array<V3<R>, 4> result;
+  applyDamping(rigidFit(corners<R>(at)), loadRowMajor<R>(rotation), k, corners<R>(direction), result);
+  storeCorners(result, out);
+  return 0;
+}
+
 extern "C" {
 
 int or_grid_counts(const or_grid* grid, uint32_t* nodes, uint32_t* tets) {
@@ -1257,6 +1430,12 @@ int or_snh_tet(int precision, const double* deformed, const double* rest, const 
   return precision == OR_F32
              ? snhImpl<float>(deformed, rest, rest_inverse, volume, material, force, energy, hessian_blocks)
              : snhImpl<double>(deformed, rest, rest_inverse, volume, material, force, energy, hessian_blocks);
+}
+
+int or_damping_apply(int precision, const double* corners, const double* rotation, const double* rest_inverse,
+                     double volume, const or_material* material, const double* direction, double* out) {
+  return precision == OR_F32 ? dampingImpl<float>(corners, rotation, rest_inverse, volume, material, direction, out)
+                             : dampingImpl<double>(corners, rotation, rest_inverse, volume, material, direction, out);
 }
 
 int or_rotation(int precision, const double* gradient, int rotation_mode, double* out) {

@@ -151,6 +151,12 @@ int or_snh_tet(int precision, const double* deformed, const double* rest,
 
 /* polarRotation (material.cc:168-197) and the Invertible rotation
  * (material.cc:24-64). gradient/out: [9] row-major. */
+/* Stiffness damping operator of one tet (factor.cc:780-853): out = D(direction),
+ * the elastic stiffness rotated by `rotation` between two removals of the
+ * rigid motion fitted to `corners`.  corners, direction, out: [12]. */
+int or_damping_apply(int precision, const double* corners, const double* rotation, const double* rest_inverse,
+                     double volume, const or_material* material, const double* direction, double* out);
+
 int or_rotation(int precision, const double* gradient, int rotation_mode,
                 double* out);
 

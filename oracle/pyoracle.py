@@ -138,6 +138,8 @@ def lib():
         _lib.or_snh_tet.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                     C.POINTER(Material), C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.or_rotation.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p]
+        _lib.or_damping_apply.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                          C.POINTER(Material), C.c_void_p, C.c_void_p]
     return _lib
 
 
@@ -281,6 +283,14 @@ def snh_tet(precision, deformed, rest, rest_inverse, volume, mat):
     lib().or_snh_tet(precision, _ptr(deformed), _ptr(rest), _ptr(rinv), volume, C.byref(mat), _ptr(force),
                      _ptr(energy), _ptr(hess))
     return dict(force=force, energy=energy[0], hessian=hess)
+
+
+def damping_apply(precision, corners, rotation, rest_inverse, volume, mat, direction):
+    """D(direction) of one tet with its rigid fit at `corners` (factor.cc:843-853)."""
+    a = [np.ascontiguousarray(x, np.float64) for x in (corners, rotation, rest_inverse, direction)]
+    out = np.zeros((4, 3))
+    lib().or_damping_apply(precision, _ptr(a[0]), _ptr(a[1]), _ptr(a[2]), volume, C.byref(mat), _ptr(a[3]), _ptr(out))
+    return out
 
 
 def rotation(precision, gradient, mode=ROTATION_INVERTIBLE):

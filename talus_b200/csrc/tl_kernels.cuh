@@ -180,6 +180,10 @@ template <class S> struct Sys {
   const uint32_t* ns_slot;     // [overflow slots]
   double* blk_part;            // [3 * grid] per-block partial sums
   uint8_t* yflag;              // [Tp] 1 where the last element pass found the trial state yielding, or null
+  // stiffness damping (null when no material of the system damps)
+  const S* dtau;               // [Tp] damping weight of each element's lane (0: undamped)
+  S* dfit;                     // [20][Tp] rigid fit at the last assemble: arms (12), inverse inertia
+                               // (xx, yy, zz, xy, xz, yz), damping coefficients (a, b)
 };
 
 constexpr int TILE_OFF_STRIDE = 4 * TILE + 4;  // 4 TILE + 1 offsets, padded to 8-byte rows
@@ -827,6 +831,211 @@ static __global__ void __launch_bounds__(TILE) kFinalize(const BodyDev* body, co
   }
 }
 
+// ------------------------------------------------------- stiffness damping ----
+// D(p) = Pi R K R^T Pi p per damped element (factor.cc:780-853): Pi removes the
+// rigid motion fitted to the corners (mean translation and the spin
+// I^-1 sum a x p about the centroid), K is the element's elastic stiffness
+// (the blocks of tetStiffness, material.cc:209-234) and R its committed
+// rotation.  The system operator gains (1 - alpha_f) gamma h tau D, the right
+// side loses tau D(v + lag ((1 - gamma) a_prev + gamma a)), lag = (1 - alpha_f) h
+// (solver.cc:1006-1007, 3747-3778), and the block-Jacobi diagonal gains the
+// corner blocks of (1 - alpha_f) gamma h tau D (solver.cc:755-830).
+
+template <class T>
+__device__ __forceinline__ void removeRigid(const V3<T> arm[4], const Sym<T>& inv, V3<T> v[4]) {
+  V3<T> mean = {0, 0, 0}, moment = {0, 0, 0};
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    mean = mean + v[c];
+    moment = moment + cross(arm[c], v[c]);
+  }
+  mean = T(0.25) * mean;
+  const V3<T> spin = symMul(inv, moment);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) v[c] = v[c] - (mean + cross(spin, arm[c]));
+}
+
+// R K R^T p in the rotated frame: gh_c = R g_c, sigma = a tr(e) I + b e with
+// e = sym(sum_b p_b gh_b^T), y_c = sigma gh_c  (a = lambda V, b = 2 mu V).
+template <class T>
+__device__ __forceinline__ void elasticProduct(const V3<T> gh[4], T a, T b, const V3<T> p[4], V3<T> y[4]) {
+  M3<T> Q = zero3<T>();
+#pragma unroll
+  for (int c = 0; c < 4; ++c) addOuter(Q, p[c], gh[c]);
+  const Sym<T> eps = symOf(Q);
+  const T at = a * symTrace(eps);
+  const Sym<T> sig = {at + b * eps.xx, at + b * eps.yy, at + b * eps.zz, b * eps.xy, b * eps.xz, b * eps.yz};
+#pragma unroll
+  for (int c = 0; c < 4; ++c) y[c] = symMul(sig, gh[c]);
+}
+
+template <class T>
+__device__ __forceinline__ void dampingApply(const V3<T> arm[4], const Sym<T>& inv, const V3<T> gh[4], T a, T b,
+                                             const V3<T> p[4], V3<T> y[4]) {
+  V3<T> rel[4] = {p[0], p[1], p[2], p[3]};
+  removeRigid(arm, inv, rel);
+  elasticProduct(gh, a, b, rel, y);
+  removeRigid(arm, inv, y);
+}
+
+// Inverse of the symmetric inertia tensor, or its pseudo-inverse keeping the
+// eigenvalues above `floor` (factor.cc:183-272, 806-814); out of line, the
+// degenerate branch is rare.
+static __device__ __noinline__ Sym<double> inertiaInverse(Sym<double> I) {
+  const double third = (I.xx + I.yy + I.zz) / 3.0;
+  M3<double> m;
+  m.m[0][0] = I.xx; m.m[1][1] = I.yy; m.m[2][2] = I.zz;
+  m.m[0][1] = m.m[1][0] = I.xy;
+  m.m[0][2] = m.m[2][0] = I.xz;
+  m.m[1][2] = m.m[2][1] = I.yz;
+  const double det = det3(m);
+  if (det > 1.0e-6 * third * third * third) {
+    const M3<double> c = cofactor(m);
+    const double inv = 1.0 / det;
+    return {c.m[0][0] * inv, c.m[1][1] * inv, c.m[2][2] * inv, c.m[0][1] * inv, c.m[0][2] * inv, c.m[1][2] * inv};
+  }
+  double a[3][3], v[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) a[i][j] = m.m[i][j];
+  jacobiEigen3(a, v);
+  Sym<double> out = {0, 0, 0, 0, 0, 0};
+  const double floor = 1.0e-6 * third;
+  for (int k = 0; k < 3; ++k) {
+    if (!(a[k][k] > floor)) continue;
+    const double w = 1.0 / a[k][k];
+    out.xx += w * v[0][k] * v[0][k];
+    out.yy += w * v[1][k] * v[1][k];
+    out.zz += w * v[2][k] * v[2][k];
+    out.xy += w * v[0][k] * v[1][k];
+    out.xz += w * v[0][k] * v[2][k];
+    out.yz += w * v[1][k] * v[2][k];
+  }
+  return out;
+}
+
+// After the element pass of an assemble (corotated law): for every damped
+// element, fit the rigid motion at the evaluated positions, keep the fit and
+// the scaled coefficients for the matvec, subtract tau D(viscous velocity)
+// from the corner forces and add the corner blocks of the damping operator to
+// the diagonal records.  FP64 arithmetic; records stay in S.
+template <class S>
+__global__ void __launch_bounds__(TILE) kDamping(Sys<S> s, const Vec4<S>* base, const Vec4<S>* dir, uint32_t pass) {
+  const uint32_t tile = blockIdx.x, b = s.elem_tile_body[tile];
+  if (!bodyActive(s, b, pass)) return;
+  const uint32_t e = tile * TILE + threadIdx.x;
+  if (e >= s.body[b].elem_end) return;
+  const double tau = double(s.dtau[e]);
+  if (tau == 0.0) return;
+  const BodyStepDev& st = s.step[b];
+  const double reach = dir ? st.scale : 0.0;
+  const uint4 t = __ldg(&s.tet[e]);
+  const uint32_t nodes[4] = {t.x, t.y, t.z, t.w};
+  // rigid fit at the evaluated corners (absolute positions)
+  V3<double> arm[4], centre = {0, 0, 0};
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    V3<double> x = cvt<double>(xyz(ld4g(&s.rest4[nodes[c]]))) + cvt<double>(xyz(base[nodes[c]]));
+    if (dir) x = x + reach * cvt<double>(xyz(dir[nodes[c]]));
+    arm[c] = x;
+    centre = centre + x;
+  }
+  centre = 0.25 * centre;
+  Sym<double> inertia = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    arm[c] = arm[c] - centre;
+    const V3<double>& q = arm[c];
+    const double qq = dot(q, q);
+    inertia.xx += qq - q.x * q.x;
+    inertia.yy += qq - q.y * q.y;
+    inertia.zz += qq - q.z * q.z;
+    inertia.xy -= q.x * q.y;
+    inertia.xz -= q.x * q.z;
+    inertia.yz -= q.y * q.z;
+  }
+  const Sym<double> inv = inertiaInverse(inertia);
+  // rotated gradients gh = R g from the committed rotation and Dm^-1
+  M3<double> R;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) R.m[i][j] = double(s.op[size_t(3 * i + j) * s.Tp + e]);
+  V3<double> g[4], gh[4];
+  gradientsOf<S>(s.dm, s.Tp, e, g);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) gh[c] = mul(R, g[c]);
+  const MatDev m = s.mat[s.lane[e]];
+  const double youngs = s.eyoung ? s.eyoung[e] : m.youngs;
+  const double vol = s.vold[e];
+  const double a = youngs * m.lam_unit * vol, bb = 2.0 * youngs * m.mu_unit * vol;
+  const double dscale = (1.0 - st.alpha_f) * st.gamma * st.inner;  // Damping::scale
+  // the fit and the scaled coefficients for the matvec
+  const double keep[20] = {arm[0].x, arm[0].y, arm[0].z, arm[1].x, arm[1].y, arm[1].z, arm[2].x, arm[2].y,
+                           arm[2].z, arm[3].x, arm[3].y, arm[3].z, inv.xx,   inv.yy,   inv.zz,   inv.xy,
+                           inv.xz,   inv.yz,   dscale * tau * a, dscale * tau * bb};
+#pragma unroll
+  for (int k = 0; k < 20; ++k) s.dfit[size_t(k) * s.Tp + e] = S(keep[k]);
+  // viscous force of the lagged velocity (anchored nodes: zero)
+  const double lag = (1.0 - st.alpha_f) * st.inner;
+  V3<double> vv[4], dv[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const uint32_t n = nodes[c];
+    if (s.anch[n]) {
+      vv[c] = {0, 0, 0};
+      continue;
+    }
+    vv[c] = cvt<double>(xyz(s.v[n])) + (lag * (1.0 - st.gamma)) * cvt<double>(xyz(s.carried[n]));
+    if (dir) vv[c] = vv[c] + (lag * st.gamma) * cvt<double>(xyz(dir[n]));
+  }
+  dampingApply(arm, inv, gh, a, bb, vv, dv);
+  // diagonal corner blocks of D, scaled like the element blocks (the node
+  // gather multiplies the records by h_eff^2)
+  const double wdiag = dscale * tau / st.scale;
+#pragma unroll 1
+  for (int c = 0; c < 4; ++c) {
+    M3<double> blk;
+#pragma unroll 1
+    for (int axis = 0; axis < 3; ++axis) {
+      V3<double> unit[4] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, col[4];
+      if (axis == 0) unit[c].x = 1.0;
+      else if (axis == 1) unit[c].y = 1.0;
+      else unit[c].z = 1.0;
+      dampingApply(arm, inv, gh, a, bb, unit, col);
+      blk.m[0][axis] = col[c].x;
+      blk.m[1][axis] = col[c].y;
+      blk.m[2][axis] = col[c].z;
+    }
+    const size_t at = size_t(c) * s.Tp + e;
+    const Vec4<S> f = s.fe[at], d = s.de[at];
+    s.fe[at] = Vec4<S>{S(double(f.x) - tau * dv[c].x), S(double(f.y) - tau * dv[c].y),
+                       S(double(f.z) - tau * dv[c].z), S(double(f.w) + wdiag * blk.m[0][0])};
+    s.de[at] = Vec4<S>{S(double(d.x) + wdiag * blk.m[1][1]), S(double(d.y) + wdiag * blk.m[2][2]),
+                       S(double(d.z) + wdiag * 0.5 * (blk.m[0][1] + blk.m[1][0])),
+                       S(double(d.w) + wdiag * 0.5 * (blk.m[0][2] + blk.m[2][0]))};
+    s.de2[at] = S(double(s.de2[at]) + wdiag * 0.5 * (blk.m[1][2] + blk.m[2][1]));
+  }
+}
+
+// Matvec share of damping for one element: y += (1 - alpha_f) gamma h tau D(p),
+// in S, from the fit kept by kDamping and the rotated gradients gh.  Only the
+// DAMP instantiations of the PCG kernels (systems with stiffness damping)
+// contain it.
+template <class S>
+__device__ __forceinline__ void dampingProduct(const Sys<S>& s, uint32_t e, const V3<S> gh[4], const V3<S> p[4],
+                                               V3<S> y[4]) {
+  if (s.dtau[e] == S(0)) return;
+  S k[20];
+#pragma unroll
+  for (int q = 0; q < 20; ++q) k[q] = s.dfit[size_t(q) * s.Tp + e];
+  const V3<S> arm[4] = {{k[0], k[1], k[2]}, {k[3], k[4], k[5]}, {k[6], k[7], k[8]}, {k[9], k[10], k[11]}};
+  const Sym<S> inv = {k[12], k[13], k[14], k[15], k[16], k[17]};
+  V3<S> d[4];
+  dampingApply(arm, inv, gh, k[18], k[19], p, d);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) y[c] = y[c] + d[c];
+}
+
 // ---------------------------------------------------------------- PCG ----
 
 // h_eff^2 (R K R^T p)_e for one tet: applyStiffness (material.cc:267-288) with
@@ -978,9 +1187,11 @@ __device__ __forceinline__ void applyOperator(const ElementOperator<S>& o, const
   y[0] = -(y[1] + y[2] + y[3]);
 }
 
-template <class S, int LAW, bool TANGENT>
+template <class S, int LAW, bool TANGENT, bool DAMP = false>
 __device__ __forceinline__ void elementApply(const Sys<S>& s, uint32_t e, const V3<S> p[4], V3<S> y[4]) {
-  applyOperator<S, LAW, TANGENT>(loadOperator<S, LAW, TANGENT>(s, e), p, y);
+  const ElementOperator<S> o = loadOperator<S, LAW, TANGENT>(s, e);
+  applyOperator<S, LAW, TANGENT>(o, p, y);
+  if (DAMP && LAW == 0) dampingProduct(s, e, o.g, p, y);
 }
 
 // Reads a body's PCG scalars from L2 (they are written by other blocks).
@@ -1338,7 +1549,7 @@ __device__ __forceinline__ V3<S> stagedValue(const Sys<S>& s, uint32_t n, const 
   return fmaV(blend, xyz(ld4cg(&s.p[n])), xyz(ld4cg(&s.z[n])));
 }
 
-template <class S, int LAW, bool TANGENT, bool CGU = false>
+template <class S, int LAW, bool TANGENT, bool CGU = false, bool DAMP = false>
 __device__ __forceinline__ void matvecTile(const Sys<S>& s, uint32_t tile, const Vec4<S>* X, S blend,
                                            S (*buf)[4 * TILE], uint16_t* sOff, uint16_t* sEnt, uint32_t elemEnd,
                                            bool update = false, S alpha = S(0)) {
@@ -1367,7 +1578,7 @@ __device__ __forceinline__ void matvecTile(const Sys<S>& s, uint32_t tile, const
     V3<S> pe[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) pe[c] = {buf[0][l[c]], buf[1][l[c]], buf[2][l[c]]};
-    elementApply<S, LAW, TANGENT>(s, e, pe, y);
+    elementApply<S, LAW, TANGENT, DAMP>(s, e, pe, y);
   }
   __syncthreads();  // node values consumed: buf now holds y, buf[k][c TILE + element]
 #pragma unroll
@@ -1444,7 +1655,7 @@ __device__ __forceinline__ void fillTileCache(const Sys<S>& s, TileCache& c, uin
 // matvecTile with the tile tables of cache entry k: the element operator is
 // requested before the node stage, so the only dependent L2 round trip left
 // is the node values.
-template <class S, int LAW, bool TANGENT, bool CGU>
+template <class S, int LAW, bool TANGENT, bool CGU, bool DAMP>
 __device__ __forceinline__ void matvecTileCached(const Sys<S>& s, const TileCache& c, uint32_t k, uint32_t tile,
                                                  const Vec4<S>* X, S blend, S (*buf)[4 * TILE], uint32_t elemEnd,
                                                  bool update, S alpha) {
@@ -1468,6 +1679,7 @@ __device__ __forceinline__ void matvecTileCached(const Sys<S>& s, const TileCach
 #pragma unroll
     for (int q = 0; q < 4; ++q) pe[q] = {buf[0][l[q]], buf[1][l[q]], buf[2][l[q]]};
     applyOperator<S, LAW, TANGENT>(op, pe, y);
+    if (DAMP && LAW == 0) dampingProduct(s, e, op.g, pe, y);
   }
   __syncthreads();
 #pragma unroll
@@ -1514,7 +1726,7 @@ __device__ __forceinline__ void matvecTileCached(const Sys<S>& s, const TileCach
 // Every block accumulates its partials in a fixed order and, after the
 // barrier, adds all blocks' partials in block order, so every block takes the
 // same decisions with no further communication.
-template <class S, int LAW, bool TANGENT>
+template <class S, int LAW, bool TANGENT, bool DAMP = false>
 __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, Vec4<S>* X, uint32_t x0zero) {
   __shared__ S buf[3][4 * TILE];
   __shared__ __align__(8) uint16_t sOff[TILE_OFF_STRIDE];
@@ -1534,8 +1746,8 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, 
   // ---- init: r = right - A x (anchored rows 0), u = P r, p = s = 0
   if (!x0zero) {
     for (uint32_t tile = blockIdx.x, k = 0; tile < s.elem_tiles; tile += G, ++k) {
-      if (cached) matvecTileCached<S, LAW, TANGENT, true>(s, cache, k, tile, X, zero, buf, bd.elem_end, false, zero);
-      else matvecTile<S, LAW, TANGENT>(s, tile, X, zero, buf, sOff, sEnt, bd.elem_end);
+      if (cached) matvecTileCached<S, LAW, TANGENT, true, DAMP>(s, cache, k, tile, X, zero, buf, bd.elem_end, false, zero);
+      else matvecTile<S, LAW, TANGENT, false, DAMP>(s, tile, X, zero, buf, sOff, sEnt, bd.elem_end);
     }
     if (!countBarrier(s.sync, bar)) return;
   }
@@ -1600,11 +1812,11 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, 
       // ---- A: w = A u
       for (uint32_t tile = blockIdx.x, k = 0; tile < s.elem_tiles; tile += G, ++k) {
         if (cached)
-          matvecTileCached<S, LAW, TANGENT, true>(s, cache, k, tile, nullptr, S(beta), buf, bd.elem_end, update,
-                                                  S(alpha));
+          matvecTileCached<S, LAW, TANGENT, true, DAMP>(s, cache, k, tile, nullptr, S(beta), buf, bd.elem_end,
+                                                        update, S(alpha));
         else
-          matvecTile<S, LAW, TANGENT, true>(s, tile, nullptr, S(beta), buf, sOff, sEnt, bd.elem_end, update,
-                                            S(alpha));
+          matvecTile<S, LAW, TANGENT, true, DAMP>(s, tile, nullptr, S(beta), buf, sOff, sEnt, bd.elem_end, update,
+                                                  S(alpha));
       }
       ++applications;
       if (!countBarrier(s.sync, bar)) return;
@@ -1736,7 +1948,7 @@ __device__ __forceinline__ void issueTile(const Sys<S>& s, uint32_t tile, uint2 
 }
 
 // The matvec of one staged tile (same arithmetic and order as matvecTile).
-template <class S, int LAW, bool TANGENT>
+template <class S, int LAW, bool TANGENT, bool DAMP>
 __device__ __forceinline__ void computeTile(const Sys<S>& s, uint32_t tile, uint2 meta, const unsigned char* half,
                                             const Vec4<S>* X, S blend, S (*buf)[4 * TILE], uint32_t elemEnd) {
   const TileTables& tt = *reinterpret_cast<const TileTables*>(half);
@@ -1755,7 +1967,9 @@ __device__ __forceinline__ void computeTile(const Sys<S>& s, uint32_t tile, uint
     V3<S> pe[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) pe[c] = {buf[0][l[c]], buf[1][l[c]], buf[2][l[c]]};
-    applyOperator<S, LAW, TANGENT>(stagedOperator<S, LAW, TANGENT>(half + sizeof(TileTables)), pe, y);
+    const ElementOperator<S> op = stagedOperator<S, LAW, TANGENT>(half + sizeof(TileTables));
+    applyOperator<S, LAW, TANGENT>(op, pe, y);
+    if (DAMP && LAW == 0) dampingProduct(s, e, op.g, pe, y);
   }
   __syncthreads();
 #pragma unroll
@@ -1783,7 +1997,7 @@ __device__ __forceinline__ void computeTile(const Sys<S>& s, uint32_t tile, uint
 // Every tile of this block whose body takes part in the pass (and, when
 // skipDone, has not converged), in order, pipelined.  X: multiply X instead
 // of p = z + blend p_prev.  Done flags do not change during the phase.
-template <class S, int LAW, bool TANGENT>
+template <class S, int LAW, bool TANGENT, bool DAMP>
 __device__ __forceinline__ void matvecPipelined(const Sys<S>& s, uint32_t pass, const Vec4<S>* X, bool skipDone,
                                                 unsigned char* dyn, S (*buf)[4 * TILE]) {
   constexpr uint32_t NONE = 0xffffffffu;
@@ -1813,7 +2027,7 @@ __device__ __forceinline__ void matvecPipelined(const Sys<S>& s, uint32_t pass, 
     __syncthreads();      // and everyone else's
     const uint32_t b0 = s.elem_tile_body[t0];
     const S blend = X ? S(0) : S(__ldcg(&s.cg[b0].blend));
-    computeTile<S, LAW, TANGENT>(s, t0, m0, cur, X, blend, buf, s.body[b0].elem_end);
+    computeTile<S, LAW, TANGENT, DAMP>(s, t0, m0, cur, X, blend, buf, s.body[b0].elem_end);
     t0 = t1;
     m0 = m1;
     t1 = t2;
@@ -1829,7 +2043,7 @@ __device__ __forceinline__ void matvecPipelined(const Sys<S>& s, uint32_t pass, 
 // (lastTileOfBody); the launch ends when no body iterates.  Bodies that are
 // done skip their tiles, so a batch costs the sum of its bodies' iterations,
 // not bodies x the slowest body.
-template <class S, int LAW, bool TANGENT>
+template <class S, int LAW, bool TANGENT, bool DAMP = false>
 __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2)
     kPcgBatch(Sys<S> s, Vec4<S>* X, uint32_t pass, uint32_t x0zero) {
   __shared__ S buf[3][4 * TILE];
@@ -1839,7 +2053,7 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2)
   unsigned int bar = 0;
   // ---- init: r = right - A x (anchored rows 0), z = P r, p_prev = 0
   if (!x0zero) {
-    matvecPipelined<S, LAW, TANGENT>(s, pass, X, false, tlStage, buf);
+    matvecPipelined<S, LAW, TANGENT, DAMP>(s, pass, X, false, tlStage, buf);
     if (!countBarrier(s.sync, bar)) return;
   }
   for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
@@ -1901,7 +2115,7 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2)
   for (;;) {
     if (*(volatile int*)&s.sync->active <= 0) break;  // uniform: no block decrements between here and barrier A
     // ---- A
-    matvecPipelined<S, LAW, TANGENT>(s, pass, nullptr, true, tlStage, buf);
+    matvecPipelined<S, LAW, TANGENT, DAMP>(s, pass, nullptr, true, tlStage, buf);
     if (!countBarrier(s.sync, bar)) return;
     // ---- B
     for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {

@@ -211,6 +211,8 @@ struct System final : SystemBase {
   DevBuf<double> blkPart;
   int pcg1PerSm[2][2] = {{0, 0}, {0, 0}};   // resident blocks per SM, [law][tangent]
   int batchPerSm[2][2] = {{0, 0}, {0, 0}};
+  int pcg1DampPerSm[2] = {0, 0};             // corotated law with stiffness damping, [tangent]
+  int batchDampPerSm[2] = {0, 0};
   uint32_t tuneBlocksPerSm = 0;              // tl_system_tune: cap on the persistent grid (0 = occupancy)
   bool tuneGraph = true;                     // tl_system_tune: capture batched elastic steps in a CUDA graph
   int gridOf(int perSm) const {
@@ -224,6 +226,9 @@ struct System final : SystemBase {
   DevBuf<CgReportDev> cgrep;
   DevBuf<GridSyncDev> sync;
   bool hasEyoung = false;
+  bool hasDamping = false;   // some element's lane has stiffness damping
+  bool evaluating = false;   // tl_evaluate: element forces only, no damping terms
+  DevBuf<S> dtau, dfit;
   // TL_FLAG_PROFILE: event pairs around kernel classes, resolved at step end
   bool profiling = false;
   bool tracing = false;
@@ -344,6 +349,8 @@ struct System final : SystemBase {
     s.counter = counter.ptr;
     s.sync = sync.ptr;
     s.yflag = yflagPtr;
+    s.dtau = hasDamping ? dtau.ptr : nullptr;
+    s.dfit = hasDamping ? dfit.ptr : nullptr;
     return s;
   }
 
@@ -389,6 +396,8 @@ struct System final : SystemBase {
     std::vector<S> hDms(size_t(9) * Tp, S(0)), hVols(Tp, S(0));
     std::vector<uint32_t> hLane(Tp, 0u), hNodeTileBody(nodeTiles), hElemTileBody(elemTiles);
     std::vector<MatDev> hMat;
+    std::vector<double> laneTau;        // damping weight per material lane
+    std::vector<S> hTau(Tp, S(0));      // and per element
     hMat.reserve(lanes);
     for (uint32_t b = 0; b < B; ++b) {
       const tl_mesh_desc& d = descs[b];
@@ -403,8 +412,8 @@ struct System final : SystemBase {
       for (uint32_t l = 0; l <= d.lanes; ++l) {
         tl_material m = l < d.lanes ? d.materials[l]
                                     : tl_material{1000.0, 0.0, 0.3, 0.0, std::numeric_limits<double>::infinity(), 0.0};
-        if (m.stiffness_damping > 0.0)
-          throw StatusError{TL_ERR_UNSUPPORTED, "stiffness damping is not implemented"};
+        // stiffnessDamping (factor.cc:755-759): finite and positive, else none
+        laneTau.push_back(std::isfinite(m.stiffness_damping) && m.stiffness_damping > 0.0 ? m.stiffness_damping : 0.0);
         const double nu = std::clamp(m.poissons_ratio, 0.0, 0.49);  // material.cc:71-78
         MatDev md;
         md.lam_unit = nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
@@ -443,6 +452,8 @@ struct System final : SystemBase {
         hVols[e] = S(d.volume[t]);
         const uint32_t l = d.material[t] < d.lanes ? d.material[t] : d.lanes;
         hLane[e] = laneBase + l;
+        hTau[e] = S(laneTau[laneBase + l]);
+        if (hTau[e] != S(0)) hasDamping = true;
         if (hMat[laneBase + l].yields) h.anyYields = true;
         if (hasEyoung) hE[e] = d.element_youngs ? d.element_youngs[t] : hMat[laneBase + l].youngs;
       }
@@ -508,6 +519,12 @@ struct System final : SystemBase {
     vold.upload(hVol.data(), Tp, st);
     lane.alloc(Tp);
     lane.upload(hLane.data(), Tp, st);
+    if (hasDamping) {
+      dtau.alloc(Tp);
+      dtau.upload(hTau.data(), Tp, st);
+      dfit.alloc(size_t(20) * Tp);
+      dfit.zero(st);
+    }
     if (hasEyoung) {
       eyoung.alloc(Tp);
       eyoung.upload(hE.data(), Tp, st);
@@ -649,9 +666,16 @@ struct System final : SystemBase {
     batchPerSm[0][1] = perSm((const void*)kPcgBatch<S, 0, true>, pipeBytes<S, 0, true>());
     batchPerSm[1][0] = perSm((const void*)kPcgBatch<S, 1, false>, pipeBytes<S, 1, false>());
     batchPerSm[1][1] = perSm((const void*)kPcgBatch<S, 1, true>, pipeBytes<S, 1, true>());
+    if (hasDamping) {
+      pcg1DampPerSm[0] = perSm((const void*)kPcg1<S, 0, false, true>, sizeof(TileCache));
+      pcg1DampPerSm[1] = perSm((const void*)kPcg1<S, 0, true, true>, sizeof(TileCache));
+      batchDampPerSm[0] = perSm((const void*)kPcgBatch<S, 0, false, true>, pipeBytes<S, 0, false>());
+      batchDampPerSm[1] = perSm((const void*)kPcgBatch<S, 0, true, true>, pipeBytes<S, 0, true>());
+    }
     int most = 0;
     for (auto& row : pcg1PerSm)
       for (int n : row) most = std::max(most, n * ctx->sms);
+    for (int n : pcg1DampPerSm) most = std::max(most, n * ctx->sms);
     blkPart.alloc(size_t(3) * most);
   }
 
@@ -825,9 +849,14 @@ struct System final : SystemBase {
       yielding.zero(st);
     }
     if (profiling) mark(0, true);
+    const bool damps = hasDamping && law == TL_LAW_COROTATED && !(mode & EM_COMMIT) && !evaluating;
     if (law == TL_LAW_SNH) kElement<S, 1><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass, mode, margin);
     else kElement<S, 0><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass, mode, margin);
     check();
+    if (damps) {
+      kDamping<S><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass);
+      check();
+    }
     if (profiling) mark(0, false);
   }
   void nodeAssemble(const Vec4<S>* taken, uint32_t pass) {
@@ -846,17 +875,23 @@ struct System final : SystemBase {
     (void)tg;
     const size_t dyn = idx ? (tangent ? pipeBytes<S, 1, true>() : pipeBytes<S, 1, false>())
                            : (tangent ? pipeBytes<S, 0, true>() : pipeBytes<S, 0, false>());
+    const bool damp = hasDamping && idx == 0;
     if (B == 1) {  // single body: two-level assembly, per-block partials
       void* args[] = {&s, &X, &xz};
       const void* fn = idx ? (tangent ? (const void*)kPcg1<S, 1, true> : (const void*)kPcg1<S, 1, false>)
-                           : (tangent ? (const void*)kPcg1<S, 0, true> : (const void*)kPcg1<S, 0, false>);
-      TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(gridOf(pcg1PerSm[idx][tangent ? 1 : 0])), dim3(TILE), args,
+                           : damp ? (tangent ? (const void*)kPcg1<S, 0, true, true> : (const void*)kPcg1<S, 0, false, true>)
+                                  : (tangent ? (const void*)kPcg1<S, 0, true> : (const void*)kPcg1<S, 0, false>);
+      const int perSm = damp ? pcg1DampPerSm[tangent ? 1 : 0] : pcg1PerSm[idx][tangent ? 1 : 0];
+      TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(gridOf(perSm)), dim3(TILE), args,
                                           sizeof(TileCache), st));
     } else {  // batch: two-level assembly, per-body scalars
       void* args[] = {&s, &X, &ps, &xz};
-      const void* fn = idx ? (tangent ? (const void*)kPcgBatch<S, 1, true> : (const void*)kPcgBatch<S, 1, false>)
-                           : (tangent ? (const void*)kPcgBatch<S, 0, true> : (const void*)kPcgBatch<S, 0, false>);
-      TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(gridOf(batchPerSm[idx][tangent ? 1 : 0])), dim3(TILE), args, dyn, st));
+      const void* fn =
+          idx ? (tangent ? (const void*)kPcgBatch<S, 1, true> : (const void*)kPcgBatch<S, 1, false>)
+              : damp ? (tangent ? (const void*)kPcgBatch<S, 0, true, true> : (const void*)kPcgBatch<S, 0, false, true>)
+                     : (tangent ? (const void*)kPcgBatch<S, 0, true> : (const void*)kPcgBatch<S, 0, false>);
+      const int perSm = damp ? batchDampPerSm[tangent ? 1 : 0] : batchPerSm[idx][tangent ? 1 : 0];
+      TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(gridOf(perSm)), dim3(TILE), args, dyn, st));
     }
     ++launches;
     if (profiling) mark(2, false);
@@ -895,6 +930,8 @@ struct System final : SystemBase {
 
   int32_t step(const tl_settings& set, const double gvec[3], double dt, tl_step_report* reports) override {
     if (set.law > 1u) throw StatusError{TL_ERR_ARG, "unknown law"};
+    if (hasDamping && set.law == TL_LAW_SNH)
+      throw StatusError{TL_ERR_UNSUPPORTED, "stiffness damping is defined with the corotated law"};
     const int law = int(set.law);
     for (uint32_t b = 0; b < B; ++b)
       if (!hb[b].anyAnchored && set.rigid_split != TL_RIGID_SPLIT_OFF)
@@ -1413,9 +1450,12 @@ struct System final : SystemBase {
     out.alloc(size_t(3) * Vp);
     yflagPtr = flags.ptr;
     try {
+      evaluating = true;
       element(int(set.law), u.ptr, nullptr, 0, EM_MAPPING, 0.0);
+      evaluating = false;
     } catch (...) {
       yflagPtr = nullptr;
+      evaluating = false;
       throw;
     }
     yflagPtr = nullptr;
