@@ -1,0 +1,314 @@
+// Assembled-operator PCG for a system holding one body.
+//
+// The element-by-element matvec of kPcg1 spends most of each iteration
+// moving element outputs back to the nodes through shared memory (bank
+// conflicts, warp divergence) and needs a grid barrier between the element
+// and the node phases.  Within one PCG solve the operator is fixed, so this
+// path assembles it once per solve into 3x3 node blocks (the sum over the
+// elements sharing two nodes of their h_eff^2 R K R^T blocks, plus
+// (1 - alpha_m) m I on the diagonal, solver.cc:904-1048) and runs the solve
+// on that matrix:
+//
+//   kSellAssemble  one thread per block position: the sum, in ascending
+//                  element order, of the element blocks that land there
+//                  (FP64 accumulation, stored in S);
+//   kPcgSell       persistent cooperative PCG in the pipelined arrangement
+//                  of Ghysels and Vanroose ("Hiding global synchronization
+//                  latency in the preconditioned conjugate gradient
+//                  algorithm", 2014), which overlaps the one reduction of an
+//                  iteration with its matvec, so each iteration needs one grid
+//                  barrier.  Each thread owns one node row and keeps its
+//                  vectors in FP64 registers; only the matvec input is
+//                  published (rounded to S, and used rounded on both sides).
+//
+// Layout: sliced ELL with 32 rows per slice (one warp).  Slice s holds its
+// rows' blocks in width_s columns; block position p = slice_start[s] +
+// 32 k + lane is column slot k of row 32 s + lane, and its 9 entries sit at
+// val[(p >> 5) 288 + 32 c + lane], so a warp reads each entry of 32 rows in
+// one 128-byte (FP32) transaction.  Column slots are the row's neighbour
+// nodes in ascending order; a row with fewer neighbours than its slice's
+// width pads with zero blocks on its own column (the mass term goes only to
+// the row's real diagonal position, diag[row]).
+#pragma once
+
+#include "tl_kernels.cuh"
+
+namespace tl {
+
+constexpr uint32_t SELL_ROWS = 32;   // rows per slice
+constexpr uint32_t SELL_SLICES_PER_BLOCK = TILE / SELL_ROWS;
+
+template <class S> struct SellDev {
+  uint32_t rows;                 // the body's nodes
+  uint32_t slices;               // ceil(rows / 32)
+  uint32_t positions;            // block positions, a multiple of 32
+  uint32_t stride;               // elements of one published vector (>= slices * 32)
+  const uint32_t* slice_start;   // [slices + 1]
+  const uint32_t* group_slice;   // [positions / 32] slice of each 32-position group
+  const uint32_t* col;           // [positions] column node
+  const uint32_t* diag;          // [rows] block position of each row's own column
+  const uint32_t* cstart;        // [positions + 1] contributor range of each position
+  const uint32_t* centry;        // (element << 4) | (row corner << 2) | column corner
+  S* val;                        // [positions / 32][9][32]
+  Vec4<S>* vec;                  // [2][stride] published matvec inputs
+};
+
+// Block (a, b) of one element's operator, d y_a / d p_b in FP64, where y is
+// the element matvec of elementApply.  Corotated law without damping in
+// closed form: with gh = R g, sigma(e) = k.x tr(e) I + k.y e - k.z (n : e) n
+// and e = sym(p_b gh_b^T),
+//   B_ij = k.x gh_a,i gh_b,j + k.y (delta_ij gh_a.gh_b + gh_b,i gh_a,j) / 2
+//          - k.z (n gh_a)_i (n gh_b)_j.
+// Otherwise the columns are the element operator applied to the three unit
+// vectors at corner b.
+template <class S, int LAW, bool TANGENT, bool DAMP>
+__device__ __forceinline__ void addElementBlock(const Sys<S>& s, uint32_t e, uint32_t a, uint32_t b,
+                                                double (&acc)[9]) {
+  const ElementOperator<S> o = loadOperator<S, LAW, TANGENT>(s, e);
+  if constexpr (LAW == 0 && !DAMP) {
+    const V3<double> ga = cvt<double>(o.g[a]), gb = cvt<double>(o.g[b]);
+    const double kx = double(o.k.x), hy = 0.5 * double(o.k.y);
+    const double gg = hy * dot(ga, gb);
+    V3<double> na = {0, 0, 0}, nb = {0, 0, 0};
+    if (TANGENT) {
+      const Sym<double> n = {double(o.n.xx), double(o.n.yy), double(o.n.zz),
+                             double(o.n.xy), double(o.n.xz), double(o.n.yz)};
+      const double kz = double(o.k.z);
+      na = kz * symMul(n, ga);
+      nb = symMul(n, gb);
+    }
+    const double A[3] = {ga.x, ga.y, ga.z}, Bv[3] = {gb.x, gb.y, gb.z};
+    const double NA[3] = {na.x, na.y, na.z}, NB[3] = {nb.x, nb.y, nb.z};
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        acc[3 * i + j] += kx * A[i] * Bv[j] + hy * Bv[i] * A[j] + (i == j ? gg : 0.0) - NA[i] * NB[j];
+  } else {
+#pragma unroll 1
+    for (int j = 0; j < 3; ++j) {
+      V3<S> p[4] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, y[4];
+      if (j == 0) p[b].x = S(1);
+      else if (j == 1) p[b].y = S(1);
+      else p[b].z = S(1);
+      applyOperator<S, LAW, TANGENT>(o, p, y);
+      if (DAMP && LAW == 0) dampingProduct(s, e, o.g, p, y);
+      acc[j] += double(y[a].x);
+      acc[3 + j] += double(y[a].y);
+      acc[6 + j] += double(y[a].z);
+    }
+  }
+}
+
+// One thread per block position; anchored rows and padding are zero blocks.
+template <class S, int LAW, bool TANGENT, bool DAMP>
+__global__ void __launch_bounds__(TILE) kSellAssemble(Sys<S> s, SellDev<S> g) {
+  const uint32_t pos = blockIdx.x * TILE + threadIdx.x;
+  if (pos >= g.positions) return;
+  const uint32_t group = pos >> 5, lane = pos & 31u;
+  const uint32_t row = g.group_slice[group] * SELL_ROWS + lane;
+  double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (row < g.rows && !s.anch[row]) {
+    const uint32_t q1 = g.cstart[pos + 1];
+    for (uint32_t q = g.cstart[pos]; q < q1; ++q) {
+      const uint32_t code = __ldg(&g.centry[q]);
+      addElementBlock<S, LAW, TANGENT, DAMP>(s, code >> 4, (code >> 2) & 3u, code & 3u, acc);
+    }
+    if (g.diag[row] == pos) {  // (1 - alpha_m) m I
+      const double m = s.step[0].inertia * double(ld4g(&s.rest4[row]).w);
+      acc[0] += m;
+      acc[4] += m;
+      acc[8] += m;
+    }
+  }
+  S* v = g.val + size_t(group) * 9 * SELL_ROWS + lane;
+#pragma unroll
+  for (int c = 0; c < 9; ++c) v[c * SELL_ROWS] = S(acc[c]);
+}
+
+// y = A in for the thread's row (0 for a thread without a row).
+template <class S>
+__device__ __forceinline__ V3<double> sellRow(const SellDev<S>& g, uint32_t slice, uint32_t lane,
+                                              const Vec4<S>* in) {
+  V3<double> acc = {0, 0, 0};
+  const uint32_t p1 = __ldg(&g.slice_start[slice + 1]);
+  for (uint32_t p = __ldg(&g.slice_start[slice]) + lane; p < p1; p += SELL_ROWS) {
+    const uint32_t c = __ldg(&g.col[p]);
+    const S* v = g.val + size_t(p >> 5) * 9 * SELL_ROWS + lane;
+    const V3<double> x = cvt<double>(xyz(ld4cg(&in[c])));
+    const double b0 = __ldg(v), b1 = __ldg(v + 32), b2 = __ldg(v + 64), b3 = __ldg(v + 96), b4 = __ldg(v + 128),
+                 b5 = __ldg(v + 160), b6 = __ldg(v + 192), b7 = __ldg(v + 224), b8 = __ldg(v + 256);
+    acc.x = fma(b0, x.x, fma(b1, x.y, fma(b2, x.z, acc.x)));
+    acc.y = fma(b3, x.x, fma(b4, x.y, fma(b5, x.z, acc.y)));
+    acc.z = fma(b6, x.x, fma(b7, x.y, fma(b8, x.z, acc.z)));
+  }
+  return acc;
+}
+
+template <class S> __device__ __forceinline__ V3<double> roundTo(V3<double> v) {
+  return cvt<double>(cvt<S>(v));
+}
+
+// Pipelined PCG (conjugateGradient, solver.cc:1904-2089, block-Jacobi
+// branch; Ghysels-Vanroose arrangement).  With u = P r, w = A u, m = P w,
+// n = A m, per iteration:
+//   gamma = r.u, delta = w.u                    (reduced at the barrier)
+//   beta = gamma / gamma_prev, p.A p = delta - beta gamma / alpha_prev,
+//   alpha = gamma / p.A p
+//   z = n + beta z, q = m + beta q, s = w + beta s, p = u + beta p,
+//   x += alpha p, r -= alpha s, u -= alpha q, w -= alpha z,
+// where n = A m is computed while the reduction of gamma, delta, r.r is in
+// flight.  In exact arithmetic the iterates are the reference's; the stopping
+// test (|r| <= tolerance |rhs| or the iteration cap, checked before each
+// update), the breakdown test (p.A p > 0 and r.u > 0) and the iteration
+// count are the reference's, and a solve that reaches the cap applies its
+// last update without a matvec.  Block partials are added in block order, so
+// every block takes the same decisions.  The slices of block b are
+// [b slices / G, (b + 1) slices / G), at most 8, one per warp.
+template <class S>
+__global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4<S>* X, uint32_t x0zero, uint32_t tangent) {
+  const uint32_t G = gridDim.x, lane = threadIdx.x & 31u;
+  const uint32_t s0 = uint32_t(uint64_t(blockIdx.x) * g.slices / G);
+  const uint32_t s1 = uint32_t(uint64_t(blockIdx.x + 1) * g.slices / G);
+  const uint32_t slice = s0 + (threadIdx.x >> 5);
+  const bool mine = slice < s1;
+  const uint32_t row = slice * SELL_ROWS + lane;
+  const bool live = mine && row < g.rows;
+  const bool freeRow = live && !s.anch[row];
+  const BodyStepDev st = s.step[0];
+  // Block partials alternate between two halves of blk_part by reduction
+  // parity: with one barrier per iteration, a block may write the next
+  // reduction's partials while another still sums the previous one.
+  double* const halves[2] = {s.blk_part, s.blk_part + 4 * size_t(G)};
+  uint32_t reductions = 0;
+  unsigned int bar = 0;
+  Sym<double> P = {1, 1, 1, 0, 0, 0};
+  V3<double> x = {0, 0, 0}, r = {0, 0, 0}, rhs = {0, 0, 0};
+  if (live) {
+    const Vec4<S> q0 = s.pre0[row], q1 = s.pre1[row];
+    P = {double(q0.x), double(q0.y), double(q0.z), double(q0.w), double(q1.x), double(q1.y)};
+    rhs = cvt<double>(xyz(s.right[row]));
+    if (!x0zero) x = cvt<double>(xyz(X[row]));
+  }
+  uint32_t applications = 0;
+  // ---- r = right - A x (anchored rows 0), u = P r, published to vec[1]
+  if (!x0zero) {
+    const V3<double> ax = mine ? sellRow(g, slice, lane, X) : V3<double>{0, 0, 0};
+    if (freeRow) r = rhs - ax;
+    ++applications;
+  } else if (freeRow) {
+    r = rhs;
+  }
+  V3<double> u = roundTo<S>(symMul(P, r));
+  Vec4<S>* vec0 = g.vec;
+  Vec4<S>* vec1 = g.vec + g.stride;
+  if (mine) vec1[row] = pack(cvt<S>(u));
+  if (!countBarrier(s.sync, bar)) return;
+  // ---- w = A u, m = P w published to vec[0], first reduction
+  V3<double> w = mine ? sellRow(g, slice, lane, vec1) : V3<double>{0, 0, 0};
+  ++applications;
+  V3<double> m = roundTo<S>(symMul(P, w));
+  if (mine) vec0[row] = pack(cvt<S>(m));
+  {
+    double v[4] = {dot(r, u), dot(w, u), dot(r, r), live ? dot(rhs, rhs) : 0.0};
+    blockSum<4>(v);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) halves[0][k * G + blockIdx.x] = v[k];
+  }
+  if (!countBarrier(s.sync, bar)) return;
+  double sums[4];
+  sumBlocksAll<4>(halves[0], sums);
+  ++reductions;
+  double gammaNext = sums[0], delta = sums[1], length = sums[2];
+  const double reference = sqrt(sums[3]);
+  const double floor = fmax(reference, 1.1754943508222875e-38);  // std::numeric_limits<float>::min()
+  const double target = st.tolerance * floor;
+  const double startRes = sqrt(length) / floor;
+  double gamma = 0.0, alpha = 0.0, beta = 0.0;
+  uint32_t taken = 0;
+  V3<double> zv = {0, 0, 0}, qv = {0, 0, 0}, sv = {0, 0, 0}, pv = {0, 0, 0};
+  for (;;) {
+    if (taken >= st.limit || sqrt(length) <= target) break;  // the reference's loop-top test
+    const double b = taken ? gammaNext / gamma : 0.0;
+    const double curvature = taken ? delta - b * gammaNext / alpha : delta;  // p.A p
+    if (!(curvature > 0.0) || !(gammaNext > 0.0)) break;
+    beta = b;
+    alpha = gammaNext / curvature;
+    gamma = gammaNext;
+    if (taken + 1 >= st.limit) {  // the last update the cap allows: no matvec after it
+      pv = u + beta * pv;
+      sv = w + beta * sv;
+      x = x + alpha * pv;
+      r = r - alpha * sv;
+      double* part = halves[reductions & 1u];
+      double v[3] = {0.0, 0.0, dot(r, r)};
+      blockSum<3>(v);
+      if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) part[k * G + blockIdx.x] = v[k];
+      if (!countBarrier(s.sync, bar)) return;
+      double fin[3];
+      sumBlocksAll<3>(part, fin);
+      length = fin[2];
+      ++taken;
+      break;
+    }
+    // n = A m with m of this iteration (vec[taken & 1]) while the scalars are fresh
+    const V3<double> n = mine ? sellRow(g, slice, lane, (taken & 1u) ? vec1 : vec0) : V3<double>{0, 0, 0};
+    ++applications;
+    zv = n + beta * zv;
+    qv = m + beta * qv;
+    sv = w + beta * sv;
+    pv = u + beta * pv;
+    x = x + alpha * pv;
+    r = r - alpha * sv;
+    u = u - alpha * qv;
+    w = w - alpha * zv;
+    m = roundTo<S>(symMul(P, w));
+    if (mine) ((taken & 1u) ? vec0 : vec1)[row] = pack(cvt<S>(m));
+    double* part = halves[reductions & 1u];
+    {
+      double v[3] = {dot(r, u), dot(w, u), dot(r, r)};
+      blockSum<3>(v);
+      if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) part[k * G + blockIdx.x] = v[k];
+    }
+    if (!countBarrier(s.sync, bar)) return;
+    double d[3];
+    sumBlocksAll<3>(part, d);
+    ++reductions;
+    gammaNext = d[0];
+    delta = d[1];
+    length = d[2];
+    ++taken;
+  }
+  if (live) X[row] = pack(cvt<S>(x));
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const double residual = sqrt(length);
+    CgBodyDev c;
+    c.squared = gamma;
+    c.target = target;
+    c.floor = floor;
+    c.length = length;
+    c.stride = alpha;
+    c.blend = beta;
+    c.start_res = startRes;
+    c.rel_res = residual / floor;
+    c.taken = taken;
+    c.done = 1u;
+    c.pad0 = c.pad1 = 0;
+    s.cg[0] = c;
+    CgReportDev rep = s.cgrep[0];
+    rep.iterations += taken;
+    rep.capped += (taken == st.limit && residual > target) ? 1u : 0u;
+    rep.applications += applications;
+    rep.solves += 1u;
+    rep.tangent_iterations += tangent ? taken : 0u;
+    rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
+    s.cgrep[0] = rep;
+  }
+}
+
+}  // namespace tl

@@ -7,6 +7,7 @@
 #include "../../include/talus_fem.h"
 #include "tl_kernels.cuh"
 #include "tl_adjoint.cuh"
+#include "tl_sell.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -209,6 +210,13 @@ struct System final : SystemBase {
   DevBuf<uint32_t> tileNode;
   DevBuf<uint2> eloc;
   DevBuf<double> blkPart;
+  // assembled block matrix of the single-body PCG (tl_sell.cuh)
+  bool sellReady = false;
+  uint32_t sellRows = 0, sellSlices = 0, sellPositions = 0, sellStride = 0;
+  int sellPerSm = 0;
+  DevBuf<uint32_t> sellSliceStart, sellGroupSlice, sellCol, sellDiag, sellCstart, sellCentry;
+  DevBuf<S> sellVal;
+  DevBuf<Vec4<S>> sellVec;
   int pcg1PerSm[2][2] = {{0, 0}, {0, 0}};   // resident blocks per SM, [law][tangent]
   int batchPerSm[2][2] = {{0, 0}, {0, 0}};
   int pcg1DampPerSm[2] = {0, 0};             // corotated law with stiffness damping, [tangent]
@@ -562,7 +570,150 @@ struct System final : SystemBase {
     sync.alloc(1);
     sync.zero(st);
     buildTiles(hTet, hElemTileBody);
+    if (B == 1) buildSell(hTet, hStart, hEntry);
     TL_CUDA(cudaStreamSynchronize(st));
+  }
+
+  // Sliced-ELL block structure of the single body's operator (tl_sell.cuh):
+  // each node row's neighbours (the nodes of its elements, ascending), slices
+  // of 32 rows padded to their widest row, and for every block position the
+  // (element, row corner, column corner) triples that add to it, in
+  // ascending element order (the node incidence lists ascend).
+  void buildSell(const std::vector<uint4>& hTet, const std::vector<uint32_t>& hStart,
+                 const std::vector<uint32_t>& hEntry) {
+    const uint32_t rows = bodyHost[0].node_end;
+    if (bodyHost[0].elem_end >= (1u << 28)) return;  // contributor codes hold the element in 28 bits
+    const uint32_t slices = (rows + SELL_ROWS - 1) / SELL_ROWS;
+    std::vector<uint32_t> nbStart(size_t(rows) + 1, 0), nb;
+    nb.reserve(size_t(rows) * 16);
+    std::vector<uint32_t> tmp;
+    for (uint32_t r = 0; r < rows; ++r) {
+      tmp.clear();
+      for (uint32_t k = hStart[r]; k < hStart[r + 1]; ++k) {
+        const uint4 t = hTet[hEntry[k] >> 2];
+        tmp.insert(tmp.end(), {t.x, t.y, t.z, t.w});
+      }
+      if (tmp.empty()) tmp.push_back(r);
+      std::sort(tmp.begin(), tmp.end());
+      tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+      nb.insert(nb.end(), tmp.begin(), tmp.end());
+      nbStart[r + 1] = uint32_t(nb.size());
+    }
+    std::vector<uint32_t> sliceStart(size_t(slices) + 1, 0);
+    for (uint32_t sl = 0; sl < slices; ++sl) {
+      uint32_t width = 1;
+      for (uint32_t r = sl * SELL_ROWS; r < std::min(rows, (sl + 1) * SELL_ROWS); ++r)
+        width = std::max(width, nbStart[r + 1] - nbStart[r]);
+      sliceStart[sl + 1] = sliceStart[sl] + width * SELL_ROWS;
+    }
+    const uint32_t positions = sliceStart[slices];
+    // contributors of (row, slot), ascending element: per row, codes keyed by slot
+    std::vector<uint32_t> slotStart(nb.size() + rows + 1, 0), codes;  // per row: slots + 1 offsets
+    std::vector<uint32_t> rowSlotBase(size_t(rows) + 1, 0);
+    codes.reserve(size_t(16) * tets);
+    std::vector<std::pair<uint32_t, uint32_t>> pairs;
+    for (uint32_t r = 0; r < rows; ++r) {
+      const uint32_t* nr = nb.data() + nbStart[r];
+      const uint32_t len = nbStart[r + 1] - nbStart[r];
+      pairs.clear();
+      for (uint32_t k = hStart[r]; k < hStart[r + 1]; ++k) {
+        const uint32_t e = hEntry[k] >> 2, a = hEntry[k] & 3u;
+        const uint32_t q[4] = {hTet[e].x, hTet[e].y, hTet[e].z, hTet[e].w};
+        for (uint32_t b = 0; b < 4; ++b) {
+          const uint32_t slot = uint32_t(std::lower_bound(nr, nr + len, q[b]) - nr);
+          pairs.emplace_back(slot, (e << 4) | (a << 2) | b);
+        }
+      }
+      std::stable_sort(pairs.begin(), pairs.end(),
+                       [](const std::pair<uint32_t, uint32_t>& x, const std::pair<uint32_t, uint32_t>& y) {
+                         return x.first < y.first;
+                       });
+      const uint32_t base = nbStart[r] + r;  // this row's len + 1 offsets
+      rowSlotBase[r] = base;
+      size_t j = 0;
+      for (uint32_t k = 0; k <= len; ++k) {
+        slotStart[base + k] = uint32_t(codes.size());
+        while (k < len && j < pairs.size() && pairs[j].first == k) codes.push_back(pairs[j++].second);
+      }
+    }
+    std::vector<uint32_t> col(positions, 0), cstart(size_t(positions) + 1, 0), centry, diag(rows, 0);
+    std::vector<uint32_t> groupSlice(positions / SELL_ROWS);
+    centry.reserve(codes.size());
+    for (uint32_t sl = 0; sl < slices; ++sl) {
+      const uint32_t width = (sliceStart[sl + 1] - sliceStart[sl]) / SELL_ROWS;
+      for (uint32_t k = 0; k < width; ++k) {
+        groupSlice[(sliceStart[sl] + k * SELL_ROWS) / SELL_ROWS] = sl;
+        for (uint32_t lane = 0; lane < SELL_ROWS; ++lane) {
+          const uint32_t pos = sliceStart[sl] + k * SELL_ROWS + lane, r = sl * SELL_ROWS + lane;
+          cstart[pos] = uint32_t(centry.size());
+          if (r >= rows) continue;  // padding row: column 0, zero block
+          const uint32_t len = nbStart[r + 1] - nbStart[r];
+          if (k >= len) {
+            col[pos] = r;  // padding slot: own column, zero block
+            continue;
+          }
+          col[pos] = nb[nbStart[r] + k];
+          if (col[pos] == r) diag[r] = pos;
+          const uint32_t* ss = slotStart.data() + rowSlotBase[r];
+          centry.insert(centry.end(), codes.begin() + ss[k], codes.begin() + ss[k + 1]);
+        }
+      }
+    }
+    cstart[positions] = uint32_t(centry.size());
+    sellRows = rows;
+    sellSlices = slices;
+    sellPositions = positions;
+    sellStride = std::max(Vp, slices * SELL_ROWS);
+    sellSliceStart.alloc(sliceStart.size());
+    sellSliceStart.upload(sliceStart.data(), sliceStart.size(), st);
+    sellGroupSlice.alloc(groupSlice.size());
+    sellGroupSlice.upload(groupSlice.data(), groupSlice.size(), st);
+    sellCol.alloc(col.size());
+    sellCol.upload(col.data(), col.size(), st);
+    sellDiag.alloc(diag.size());
+    sellDiag.upload(diag.data(), diag.size(), st);
+    sellCstart.alloc(cstart.size());
+    sellCstart.upload(cstart.data(), cstart.size(), st);
+    sellCentry.alloc(std::max<size_t>(centry.size(), 1));
+    sellCentry.upload(centry.data(), centry.size(), st);
+    sellVal.alloc(size_t(positions) * 9);
+    sellVec.alloc(size_t(2) * sellStride);
+    sellVec.zero(st);
+    TL_CUDA(cudaFuncSetAttribute((const void*)kPcgSell<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, 0));
+    TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sellPerSm, (const void*)kPcgSell<S>, TILE, 0));
+    // kPcgSell writes four partials per block into one of two halves
+    if (size_t(8) * sellPerSm * ctx->sms > blkPart.count) blkPart.alloc(size_t(8) * sellPerSm * ctx->sms);
+    TL_CUDA(cudaStreamSynchronize(st));
+    sellReady = sellPerSm > 0;
+  }
+  SellDev<S> sellView() {
+    SellDev<S> g;
+    g.rows = sellRows;
+    g.slices = sellSlices;
+    g.positions = sellPositions;
+    g.stride = sellStride;
+    g.slice_start = sellSliceStart.ptr;
+    g.group_slice = sellGroupSlice.ptr;
+    g.col = sellCol.ptr;
+    g.diag = sellDiag.ptr;
+    g.cstart = sellCstart.ptr;
+    g.centry = sellCentry.ptr;
+    g.val = sellVal.ptr;
+    g.vec = sellVec.ptr;
+    return g;
+  }
+  // Grid of kPcgSell: the occupancy (capped by tl_system_tune while every
+  // block still has at most one slice per warp), or 0 when the rows do not
+  // fit one per thread.
+  int sellGrid() const {
+    if (!sellReady) return 0;
+    const int full = std::min<int>(sellPerSm * ctx->sms, int(sellSlices));
+    const int capped = tuneBlocksPerSm ? std::min<int>(std::min<int>(sellPerSm, int(tuneBlocksPerSm)) * ctx->sms,
+                                                       int(sellSlices))
+                                       : full;
+    const auto fits = [&](int g) { return g > 0 && uint64_t(sellSlices) <= uint64_t(g) * SELL_SLICES_PER_BLOCK; };
+    if (fits(capped)) return capped;
+    return fits(full) ? full : 0;
   }
 
   // Two-level assembly structures: per element tile the distinct nodes it
@@ -872,11 +1023,28 @@ struct System final : SystemBase {
     uint32_t ps = pass, xz = x0zero ? 1u : 0u, tg = tangent ? 1u : 0u;
     const int idx = law == TL_LAW_SNH ? 1 : 0;
     if (profiling) mark(2, true);
-    (void)tg;
     const size_t dyn = idx ? (tangent ? pipeBytes<S, 1, true>() : pipeBytes<S, 1, false>())
                            : (tangent ? pipeBytes<S, 0, true>() : pipeBytes<S, 0, false>());
     const bool damp = hasDamping && idx == 0;
-    if (B == 1) {  // single body: two-level assembly, per-block partials
+    const int sellG = B == 1 ? sellGrid() : 0;
+    if (sellG > 0) {  // single body: assembled block matrix, pipelined PCG
+      SellDev<S> g = sellView();
+      const unsigned blocks = (sellPositions + TILE - 1) / TILE;
+      if (idx) {
+        if (tangent) kSellAssemble<S, 1, true, false><<<blocks, TILE, 0, st>>>(s, g);
+        else kSellAssemble<S, 1, false, false><<<blocks, TILE, 0, st>>>(s, g);
+      } else if (damp) {
+        if (tangent) kSellAssemble<S, 0, true, true><<<blocks, TILE, 0, st>>>(s, g);
+        else kSellAssemble<S, 0, false, true><<<blocks, TILE, 0, st>>>(s, g);
+      } else {
+        if (tangent) kSellAssemble<S, 0, true, false><<<blocks, TILE, 0, st>>>(s, g);
+        else kSellAssemble<S, 0, false, false><<<blocks, TILE, 0, st>>>(s, g);
+      }
+      check();
+      ++launches;
+      void* args[] = {&s, &g, &X, &xz, &tg};
+      TL_CUDA(cudaLaunchCooperativeKernel((const void*)kPcgSell<S>, dim3(sellG), dim3(TILE), args, 0, st));
+    } else if (B == 1) {  // single body: two-level assembly, per-block partials
       void* args[] = {&s, &X, &xz};
       const void* fn = idx ? (tangent ? (const void*)kPcg1<S, 1, true> : (const void*)kPcg1<S, 1, false>)
                            : damp ? (tangent ? (const void*)kPcg1<S, 0, true, true> : (const void*)kPcg1<S, 0, false, true>)
