@@ -164,6 +164,32 @@ def pcg_bytes_per_iteration(T, V, slots, s_bytes, tangent):
     return a + b + c
 
 
+def operator_blocks(mesh):
+    """Nonzero 3x3 blocks of the assembled single-body operator: the ordered
+    node pairs that share an element (the diagonal included)."""
+    t = mesh.tet_nodes.astype(np.int64)
+    pairs = (t[:, :, None] * mesh.nodes + t[:, None, :]).ravel()
+    return int(np.unique(pairs).size)
+
+
+def sell_bytes_per_iteration(blocks, V, s_bytes):
+    """Unique bytes of one tl::kPcgSell iteration (talus_b200/csrc/tl_sell.cuh):
+    every block of the matrix (9 S entries and its column index) and the
+    published matvec input read once, the next input written once.  The
+    iteration vectors stay in registers."""
+    v4 = 4 * s_bytes
+    return blocks * (9 * s_bytes + 4) + 2 * V * v4
+
+
+def sell_assembly_bytes(T, blocks, s_bytes, tangent):
+    """Unique bytes of one tl::kSellAssemble launch: the element matvec
+    operator (9 S gradients, Vec4 coefficients, [2 Vec4 flow normal]) and the
+    16 contributor codes of every element read once, each block written once
+    with its contributor range."""
+    v4 = 4 * s_bytes
+    return T * (9 * s_bytes + v4 + (2 * v4 if tangent else 0) + 16 * 4) + blocks * (9 * s_bytes + 4)
+
+
 def peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -438,11 +464,18 @@ def run_ours(args, spec, rank, world, dist):
     # ---- roofline of the dominant kernel (persistent PCG): algorithmic bytes of every iteration run
     s_bytes = 4 if precision == tb.FP32_MIXED else 8
     pcg_bytes = 0.0
+    assembly = None
     for b, m in enumerate(meshes):
-        slots = tile_slots(m)
         it, tan = per_body[b, 0], per_body[b, 1]
-        pcg_bytes += (pcg_bytes_per_iteration(m.tets, m.nodes, slots, s_bytes, True) * tan +
-                      pcg_bytes_per_iteration(m.tets, m.nodes, slots, s_bytes, False) * (it - tan))
+        if B == 1:  # assembled operator (tl_sell.cuh)
+            blocks = operator_blocks(m)
+            pcg_bytes += sell_bytes_per_iteration(blocks, m.nodes, s_bytes) * it
+            assembly = {"kernel": "tl::kSellAssemble (block matrix, once per solve)", "blocks": blocks,
+                        "algorithmic_bytes_per_launch": sell_assembly_bytes(m.tets, blocks, s_bytes, tan > 0)}
+        else:
+            slots = tile_slots(m)
+            pcg_bytes += (pcg_bytes_per_iteration(m.tets, m.nodes, slots, s_bytes, True) * tan +
+                          pcg_bytes_per_iteration(m.tets, m.nodes, slots, s_bytes, False) * (it - tan))
     launches_pcg = int(per_body[:, 2].max())
     pcg_time = totals["pcg"]
     peak, peak_kind = peaks()
@@ -452,10 +485,12 @@ def run_ours(args, spec, rank, world, dist):
     if os.path.exists(tpath):
         with open(tpath) as f:
             tr = json.load(f)
-        if tr.get("workload") == args.workload and tr.get("precision") == args.precision and launches_pcg:
+        same_kernel = tr.get("kernel", "").startswith("tl::kPcgSell" if B == 1 else "tl::kPcgBatch")
+        if tr.get("workload") == args.workload and tr.get("precision") == args.precision and same_kernel and launches_pcg:
             traffic = tr["dram_bytes_per_iteration"] * per_body[:, 0].sum() / launches_pcg
 
-    kernel = ("tl::kPcg1 (persistent block-Jacobi PCG, two-level assembly)" if B == 1 else
+    kernel = ("tl::kPcgSell (persistent pipelined block-Jacobi PCG on the assembled sliced-ELL block matrix)"
+              if B == 1 else
               "tl::kPcgBatch (persistent block-Jacobi PCG over all bodies, two-level assembly)")
     config = {"workload": args.workload, "bodies": B, "tets": T, "nodes": V, "law": spec["law"],
               "precision": args.precision, "dt": 1.0 / 60.0,
@@ -483,6 +518,7 @@ def run_ours(args, spec, rank, world, dist):
                      "iterations": int(per_body[:, 0].max()),
                      "algorithmic_bytes_per_launch": pcg_bytes / max(1, launches_pcg),
                      "avg_launch_ms": pcg_time * 1e3 / max(1, launches_pcg)},
+        "operator_assembly": assembly,
         "element_pass": element_roofline(meshes, mats, per_body, reps_substeps, s_bytes, totals["element"], peak),
         "breakdown_ms_per_step": {k: v * 1e3 / args.steps for k, v in totals.items()},
         "solver": {"cg_iterations_per_step": float(per_body[:, 0].sum() / args.steps),

@@ -132,7 +132,8 @@ typedef struct tl_step_report {
   double min_volume_ratio;
   double device_seconds;
   double element_seconds;   /* TL_FLAG_PROFILE: element-pass kernels */
-  double assemble_seconds;  /* TL_FLAG_PROFILE: node gather + balance kernels */
+  double assemble_seconds;  /* TL_FLAG_PROFILE: node gather + balance kernels, and the single-body
+                               PCG's block-matrix assembly */
   double pcg_seconds;       /* TL_FLAG_PROFILE: persistent PCG launches */
 } tl_step_report;
 

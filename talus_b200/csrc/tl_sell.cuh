@@ -9,9 +9,10 @@
 // (1 - alpha_m) m I on the diagonal, solver.cc:904-1048) and runs the solve
 // on that matrix:
 //
-//   kSellAssemble  one thread per block position: the sum, in ascending
-//                  element order, of the element blocks that land there
-//                  (FP64 accumulation, stored in S);
+//   kSellAssemble  one thread per block on or above the diagonal: the sum,
+//                  in ascending element order, of the element blocks that
+//                  land there (FP64 accumulation, stored in S), written with
+//                  its transpose below the diagonal;
 //   kPcgSell       persistent cooperative PCG in the pipelined arrangement
 //                  of Ghysels and Vanroose ("Hiding global synchronization
 //                  latency in the preconditioned conjugate gradient
@@ -27,8 +28,7 @@
 // val[(p >> 5) 288 + 32 c + lane], so a warp reads each entry of 32 rows in
 // one 128-byte (FP32) transaction.  Column slots are the row's neighbour
 // nodes in ascending order; a row with fewer neighbours than its slice's
-// width pads with zero blocks on its own column (the mass term goes only to
-// the row's real diagonal position, diag[row]).
+// width pads with zero blocks on its own column.
 #pragma once
 
 #include "tl_kernels.cuh"
@@ -46,7 +46,10 @@ template <class S> struct SellDev {
   const uint32_t* slice_start;   // [slices + 1]
   const uint32_t* group_slice;   // [positions / 32] slice of each 32-position group
   const uint32_t* col;           // [positions] column node
-  const uint32_t* diag;          // [rows] block position of each row's own column
+  uint32_t upper_count;          // block positions with row <= column
+  uint32_t col_cache;            // column slots per thread kept in shared memory by kPcgSell
+  const uint32_t* upper;         // [upper_count] those positions
+  const uint32_t* mirror;        // [upper_count] position of the transposed block (itself on the diagonal)
   const uint32_t* cstart;        // [positions + 1] contributor range of each position
   const uint32_t* centry;        // (element << 4) | (row corner << 2) | column corner
   S* val;                        // [positions / 32][9][32]
@@ -61,12 +64,19 @@ template <class S> struct SellDev {
 //          - k.z (n gh_a)_i (n gh_b)_j.
 // Otherwise the columns are the element operator applied to the three unit
 // vectors at corner b.
+// v_i for a run-time corner index, by selects (no local-memory array).
+template <class T>
+__device__ __forceinline__ V3<T> pick(const V3<T>& v0, const V3<T>& v1, const V3<T>& v2, const V3<T>& v3, uint32_t i) {
+  return i == 0 ? v0 : i == 1 ? v1 : i == 2 ? v2 : v3;
+}
+
 template <class S, int LAW, bool TANGENT, bool DAMP>
 __device__ __forceinline__ void addElementBlock(const Sys<S>& s, uint32_t e, uint32_t a, uint32_t b,
                                                 double (&acc)[9]) {
   const ElementOperator<S> o = loadOperator<S, LAW, TANGENT>(s, e);
   if constexpr (LAW == 0 && !DAMP) {
-    const V3<double> ga = cvt<double>(o.g[a]), gb = cvt<double>(o.g[b]);
+    const V3<double> ga = cvt<double>(pick(o.g[0], o.g[1], o.g[2], o.g[3], a)),
+                     gb = cvt<double>(pick(o.g[0], o.g[1], o.g[2], o.g[3], b));
     const double kx = double(o.k.x), hy = 0.5 * double(o.k.y);
     const double gg = hy * dot(ga, gb);
     V3<double> na = {0, 0, 0}, nb = {0, 0, 0};
@@ -87,61 +97,99 @@ __device__ __forceinline__ void addElementBlock(const Sys<S>& s, uint32_t e, uin
   } else {
 #pragma unroll 1
     for (int j = 0; j < 3; ++j) {
-      V3<S> p[4] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, y[4];
-      if (j == 0) p[b].x = S(1);
-      else if (j == 1) p[b].y = S(1);
-      else p[b].z = S(1);
+      const V3<S> unit = {S(j == 0), S(j == 1), S(j == 2)}, zero = {0, 0, 0};
+      V3<S> p[4], y[4];
+#pragma unroll
+      for (uint32_t c = 0; c < 4; ++c) p[c] = c == b ? unit : zero;
       applyOperator<S, LAW, TANGENT>(o, p, y);
       if (DAMP && LAW == 0) dampingProduct(s, e, o.g, p, y);
-      acc[j] += double(y[a].x);
-      acc[3 + j] += double(y[a].y);
-      acc[6 + j] += double(y[a].z);
+      const V3<S> ya = pick(y[0], y[1], y[2], y[3], a);
+      acc[j] += double(ya.x);
+      acc[3 + j] += double(ya.y);
+      acc[6 + j] += double(ya.z);
     }
   }
 }
 
-// One thread per block position; anchored rows and padding are zero blocks.
+// One thread per block (r, c) with r <= c: the sum over its contributors
+// (ascending element) is block (r, c), and its transpose is block (c, r),
+// since every element block satisfies B_ab = B_ba^T.  A block in an anchored
+// row is zero (its transpose, in a free row, is not).  Padding positions are
+// zero from the build and are never written.
 template <class S, int LAW, bool TANGENT, bool DAMP>
 __global__ void __launch_bounds__(TILE) kSellAssemble(Sys<S> s, SellDev<S> g) {
-  const uint32_t pos = blockIdx.x * TILE + threadIdx.x;
-  if (pos >= g.positions) return;
-  const uint32_t group = pos >> 5, lane = pos & 31u;
-  const uint32_t row = g.group_slice[group] * SELL_ROWS + lane;
+  const uint32_t i = blockIdx.x * TILE + threadIdx.x;
+  if (i >= g.upper_count) return;
+  const uint32_t pos = g.upper[i], mpos = g.mirror[i];
+  const uint32_t row = g.group_slice[pos >> 5] * SELL_ROWS + (pos & 31u), col = g.col[pos];
+  const bool rowFree = !s.anch[row], colFree = !s.anch[col];
   double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  if (row < g.rows && !s.anch[row]) {
+  if (rowFree || colFree) {
     const uint32_t q1 = g.cstart[pos + 1];
     for (uint32_t q = g.cstart[pos]; q < q1; ++q) {
       const uint32_t code = __ldg(&g.centry[q]);
       addElementBlock<S, LAW, TANGENT, DAMP>(s, code >> 4, (code >> 2) & 3u, code & 3u, acc);
     }
-    if (g.diag[row] == pos) {  // (1 - alpha_m) m I
+    if (row == col) {  // (1 - alpha_m) m I
       const double m = s.step[0].inertia * double(ld4g(&s.rest4[row]).w);
       acc[0] += m;
       acc[4] += m;
       acc[8] += m;
     }
   }
-  S* v = g.val + size_t(group) * 9 * SELL_ROWS + lane;
+  S* v = g.val + size_t(pos >> 5) * 9 * SELL_ROWS + (pos & 31u);
 #pragma unroll
-  for (int c = 0; c < 9; ++c) v[c * SELL_ROWS] = S(acc[c]);
+  for (int c = 0; c < 9; ++c) v[c * SELL_ROWS] = rowFree ? S(acc[c]) : S(0);
+  if (mpos != pos) {
+    S* t = g.val + size_t(mpos >> 5) * 9 * SELL_ROWS + (mpos & 31u);
+#pragma unroll
+    for (int i3 = 0; i3 < 3; ++i3)
+#pragma unroll
+      for (int j3 = 0; j3 < 3; ++j3) t[(3 * i3 + j3) * SELL_ROWS] = colFree ? S(acc[3 * j3 + i3]) : S(0);
+  }
 }
 
-// y = A in for the thread's row (0 for a thread without a row).
+// Column k of the thread's row: shared memory for the first col_cache slots
+// (filled once per launch by kPcgSell), global memory beyond.
+__device__ __forceinline__ uint32_t sellCol(const uint32_t* cols, uint32_t cache, uint32_t k, const uint32_t* gcol,
+                                            uint32_t p) {
+  return k < cache ? cols[k * TILE + threadIdx.x] : __ldg(&gcol[p]);
+}
+
+// One column slot of the thread's row: acc += block(p) x.
+template <class S>
+__device__ __forceinline__ void sellSlot(const SellDev<S>& g, uint32_t p, uint32_t lane, Vec4<S> xin,
+                                         V3<double>& acc) {
+  const S* v = g.val + size_t(p >> 5) * 9 * SELL_ROWS + lane;
+  const V3<double> x = cvt<double>(xyz(xin));
+  const double b0 = __ldg(v), b1 = __ldg(v + 32), b2 = __ldg(v + 64), b3 = __ldg(v + 96), b4 = __ldg(v + 128),
+               b5 = __ldg(v + 160), b6 = __ldg(v + 192), b7 = __ldg(v + 224), b8 = __ldg(v + 256);
+  acc.x = fma(b0, x.x, fma(b1, x.y, fma(b2, x.z, acc.x)));
+  acc.y = fma(b3, x.x, fma(b4, x.y, fma(b5, x.z, acc.y)));
+  acc.z = fma(b6, x.x, fma(b7, x.y, fma(b8, x.z, acc.z)));
+}
+
+// y = A in for the thread's row.  Column slots are taken U at a time (4 in
+// FP32, 2 in FP64): their input values and block entries are requested
+// together; the FMAs run slot by slot in order.
 template <class S>
 __device__ __forceinline__ V3<double> sellRow(const SellDev<S>& g, uint32_t slice, uint32_t lane,
-                                              const Vec4<S>* in) {
+                                              const Vec4<S>* in, const uint32_t* cols) {
+  constexpr uint32_t U = sizeof(S) == 4 ? 4u : 2u;
   V3<double> acc = {0, 0, 0};
   const uint32_t p1 = __ldg(&g.slice_start[slice + 1]);
-  for (uint32_t p = __ldg(&g.slice_start[slice]) + lane; p < p1; p += SELL_ROWS) {
-    const uint32_t c = __ldg(&g.col[p]);
-    const S* v = g.val + size_t(p >> 5) * 9 * SELL_ROWS + lane;
-    const V3<double> x = cvt<double>(xyz(ld4cg(&in[c])));
-    const double b0 = __ldg(v), b1 = __ldg(v + 32), b2 = __ldg(v + 64), b3 = __ldg(v + 96), b4 = __ldg(v + 128),
-                 b5 = __ldg(v + 160), b6 = __ldg(v + 192), b7 = __ldg(v + 224), b8 = __ldg(v + 256);
-    acc.x = fma(b0, x.x, fma(b1, x.y, fma(b2, x.z, acc.x)));
-    acc.y = fma(b3, x.x, fma(b4, x.y, fma(b5, x.z, acc.y)));
-    acc.z = fma(b6, x.x, fma(b7, x.y, fma(b8, x.z, acc.z)));
+  uint32_t p = __ldg(&g.slice_start[slice]) + lane, k = 0;
+  for (; p + (U - 1) * SELL_ROWS < p1; p += U * SELL_ROWS, k += U) {
+    uint32_t c[U];
+#pragma unroll
+    for (uint32_t i = 0; i < U; ++i) c[i] = sellCol(cols, g.col_cache, k + i, g.col, p + i * SELL_ROWS);
+    Vec4<S> xin[U];
+#pragma unroll
+    for (uint32_t i = 0; i < U; ++i) xin[i] = ld4cg(&in[c[i]]);
+#pragma unroll
+    for (uint32_t i = 0; i < U; ++i) sellSlot(g, p + i * SELL_ROWS, lane, xin[i], acc);
   }
+  for (; p < p1; p += SELL_ROWS, ++k) sellSlot(g, p, lane, ld4cg(&in[sellCol(cols, g.col_cache, k, g.col, p)]), acc);
   return acc;
 }
 
@@ -176,38 +224,49 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
   const bool live = mine && row < g.rows;
   const bool freeRow = live && !s.anch[row];
   const BodyStepDev st = s.step[0];
+  extern __shared__ uint32_t tlCols[];  // [col_cache][TILE] the first columns of each thread's row
+  if (mine) {
+    const uint32_t p0 = __ldg(&g.slice_start[slice]) + lane, p1 = __ldg(&g.slice_start[slice + 1]);
+    for (uint32_t k = 0, p = p0; k < g.col_cache && p < p1; ++k, p += SELL_ROWS)
+      tlCols[k * TILE + threadIdx.x] = __ldg(&g.col[p]);
+  }
+  __syncthreads();
   // Block partials alternate between two halves of blk_part by reduction
   // parity: with one barrier per iteration, a block may write the next
   // reduction's partials while another still sums the previous one.
   double* const halves[2] = {s.blk_part, s.blk_part + 4 * size_t(G)};
   uint32_t reductions = 0;
   unsigned int bar = 0;
-  Sym<double> P = {1, 1, 1, 0, 0, 0};
+  Sym<S> Ps = {1, 1, 1, 0, 0, 0};  // the row's preconditioner block, widened where used
+  const auto precondition = [&](V3<double> v) {
+    const Sym<double> P = {double(Ps.xx), double(Ps.yy), double(Ps.zz), double(Ps.xy), double(Ps.xz), double(Ps.yz)};
+    return roundTo<S>(symMul(P, v));
+  };
   V3<double> x = {0, 0, 0}, r = {0, 0, 0}, rhs = {0, 0, 0};
   if (live) {
     const Vec4<S> q0 = s.pre0[row], q1 = s.pre1[row];
-    P = {double(q0.x), double(q0.y), double(q0.z), double(q0.w), double(q1.x), double(q1.y)};
+    Ps = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
     rhs = cvt<double>(xyz(s.right[row]));
     if (!x0zero) x = cvt<double>(xyz(X[row]));
   }
   uint32_t applications = 0;
   // ---- r = right - A x (anchored rows 0), u = P r, published to vec[1]
   if (!x0zero) {
-    const V3<double> ax = mine ? sellRow(g, slice, lane, X) : V3<double>{0, 0, 0};
+    const V3<double> ax = mine ? sellRow(g, slice, lane, X, tlCols) : V3<double>{0, 0, 0};
     if (freeRow) r = rhs - ax;
     ++applications;
   } else if (freeRow) {
     r = rhs;
   }
-  V3<double> u = roundTo<S>(symMul(P, r));
+  V3<double> u = precondition(r);
   Vec4<S>* vec0 = g.vec;
   Vec4<S>* vec1 = g.vec + g.stride;
   if (mine) vec1[row] = pack(cvt<S>(u));
   if (!countBarrier(s.sync, bar)) return;
   // ---- w = A u, m = P w published to vec[0], first reduction
-  V3<double> w = mine ? sellRow(g, slice, lane, vec1) : V3<double>{0, 0, 0};
+  V3<double> w = mine ? sellRow(g, slice, lane, vec1, tlCols) : V3<double>{0, 0, 0};
   ++applications;
-  V3<double> m = roundTo<S>(symMul(P, w));
+  V3<double> m = precondition(w);
   if (mine) vec0[row] = pack(cvt<S>(m));
   {
     double v[4] = {dot(r, u), dot(w, u), dot(r, r), live ? dot(rhs, rhs) : 0.0};
@@ -217,6 +276,9 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
       for (int k = 0; k < 4; ++k) halves[0][k * G + blockIdx.x] = v[k];
   }
   if (!countBarrier(s.sync, bar)) return;
+  // n = A m for the first iteration, requested before the block sums so that
+  // their round trip overlaps it (unused if the solve stops here)
+  V3<double> n = mine ? sellRow(g, slice, lane, vec0, tlCols) : V3<double>{0, 0, 0};
   double sums[4];
   sumBlocksAll<4>(halves[0], sums);
   ++reductions;
@@ -254,9 +316,7 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
       ++taken;
       break;
     }
-    // n = A m with m of this iteration (vec[taken & 1]) while the scalars are fresh
-    const V3<double> n = mine ? sellRow(g, slice, lane, (taken & 1u) ? vec1 : vec0) : V3<double>{0, 0, 0};
-    ++applications;
+    ++applications;  // n = A m of this iteration, computed after the last barrier
     zv = n + beta * zv;
     qv = m + beta * qv;
     sv = w + beta * sv;
@@ -265,7 +325,7 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
     r = r - alpha * sv;
     u = u - alpha * qv;
     w = w - alpha * zv;
-    m = roundTo<S>(symMul(P, w));
+    m = precondition(w);
     if (mine) ((taken & 1u) ? vec0 : vec1)[row] = pack(cvt<S>(m));
     double* part = halves[reductions & 1u];
     {
@@ -276,6 +336,8 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
         for (int k = 0; k < 3; ++k) part[k * G + blockIdx.x] = v[k];
     }
     if (!countBarrier(s.sync, bar)) return;
+    // n = A m for the next iteration (m just published to vec[(taken + 1) & 1])
+    n = mine ? sellRow(g, slice, lane, (taken & 1u) ? vec0 : vec1, tlCols) : V3<double>{0, 0, 0};
     double d[3];
     sumBlocksAll<3>(part, d);
     ++reductions;

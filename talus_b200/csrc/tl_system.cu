@@ -214,7 +214,9 @@ struct System final : SystemBase {
   bool sellReady = false;
   uint32_t sellRows = 0, sellSlices = 0, sellPositions = 0, sellStride = 0;
   int sellPerSm = 0;
-  DevBuf<uint32_t> sellSliceStart, sellGroupSlice, sellCol, sellDiag, sellCstart, sellCentry;
+  DevBuf<uint32_t> sellSliceStart, sellGroupSlice, sellCol, sellCstart, sellCentry, sellUpper, sellMirror;
+  uint32_t sellUpperCount = 0, sellColCache = 0;
+  static constexpr uint32_t SELL_COL_CACHE_MAX = 32;  // column slots per thread in kPcgSell's shared memory
   DevBuf<S> sellVal;
   DevBuf<Vec4<S>> sellVec;
   int pcg1PerSm[2][2] = {{0, 0}, {0, 0}};   // resident blocks per SM, [law][tangent]
@@ -636,7 +638,7 @@ struct System final : SystemBase {
         while (k < len && j < pairs.size() && pairs[j].first == k) codes.push_back(pairs[j++].second);
       }
     }
-    std::vector<uint32_t> col(positions, 0), cstart(size_t(positions) + 1, 0), centry, diag(rows, 0);
+    std::vector<uint32_t> col(positions, 0), cstart(size_t(positions) + 1, 0), centry;
     std::vector<uint32_t> groupSlice(positions / SELL_ROWS);
     centry.reserve(codes.size());
     for (uint32_t sl = 0; sl < slices; ++sl) {
@@ -653,13 +655,36 @@ struct System final : SystemBase {
             continue;
           }
           col[pos] = nb[nbStart[r] + k];
-          if (col[pos] == r) diag[r] = pos;
           const uint32_t* ss = slotStart.data() + rowSlotBase[r];
           centry.insert(centry.end(), codes.begin() + ss[k], codes.begin() + ss[k + 1]);
         }
       }
     }
     cstart[positions] = uint32_t(centry.size());
+    // blocks on or above the diagonal and the positions of their transposes
+    std::vector<uint32_t> upper, mirror;
+    uint32_t widest = 1;
+    for (uint32_t sl = 0; sl < slices; ++sl) {
+      const uint32_t width = (sliceStart[sl + 1] - sliceStart[sl]) / SELL_ROWS;
+      widest = std::max(widest, width);
+      for (uint32_t k = 0; k < width; ++k)
+        for (uint32_t lane = 0; lane < SELL_ROWS; ++lane) {
+          const uint32_t pos = sliceStart[sl] + k * SELL_ROWS + lane, r = sl * SELL_ROWS + lane;
+          if (r >= rows || k >= nbStart[r + 1] - nbStart[r]) continue;
+          const uint32_t c = col[pos];
+          if (c < r) continue;
+          const uint32_t *nc = nb.data() + nbStart[c], *ncEnd = nb.data() + nbStart[c + 1];
+          const uint32_t kc = uint32_t(std::lower_bound(nc, ncEnd, r) - nc);
+          upper.push_back(pos);
+          mirror.push_back(sliceStart[c / SELL_ROWS] + kc * SELL_ROWS + c % SELL_ROWS);
+        }
+    }
+    sellUpperCount = uint32_t(upper.size());
+    sellColCache = std::min(widest, SELL_COL_CACHE_MAX);
+    sellUpper.alloc(std::max<size_t>(upper.size(), 1));
+    sellUpper.upload(upper.data(), upper.size(), st);
+    sellMirror.alloc(std::max<size_t>(mirror.size(), 1));
+    sellMirror.upload(mirror.data(), mirror.size(), st);
     sellRows = rows;
     sellSlices = slices;
     sellPositions = positions;
@@ -670,24 +695,29 @@ struct System final : SystemBase {
     sellGroupSlice.upload(groupSlice.data(), groupSlice.size(), st);
     sellCol.alloc(col.size());
     sellCol.upload(col.data(), col.size(), st);
-    sellDiag.alloc(diag.size());
-    sellDiag.upload(diag.data(), diag.size(), st);
     sellCstart.alloc(cstart.size());
     sellCstart.upload(cstart.data(), cstart.size(), st);
     sellCentry.alloc(std::max<size_t>(centry.size(), 1));
     sellCentry.upload(centry.data(), centry.size(), st);
     sellVal.alloc(size_t(positions) * 9);
+    sellVal.zero(st);  // padding blocks stay zero; kSellAssemble writes the others
     sellVec.alloc(size_t(2) * sellStride);
     sellVec.zero(st);
-    TL_CUDA(cudaFuncSetAttribute((const void*)kPcgSell<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, 0));
-    TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sellPerSm, (const void*)kPcgSell<S>, TILE, 0));
+    TL_CUDA(cudaFuncSetAttribute((const void*)kPcgSell<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(sellColBytes())));
+    TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sellPerSm, (const void*)kPcgSell<S>, TILE, sellColBytes()));
     // kPcgSell writes four partials per block into one of two halves
     if (size_t(8) * sellPerSm * ctx->sms > blkPart.count) blkPart.alloc(size_t(8) * sellPerSm * ctx->sms);
     TL_CUDA(cudaStreamSynchronize(st));
     sellReady = sellPerSm > 0;
   }
+  size_t sellColBytes() const { return size_t(sellColCache) * TILE * sizeof(uint32_t); }
   SellDev<S> sellView() {
     SellDev<S> g;
+    g.upper_count = sellUpperCount;
+    g.col_cache = sellColCache;
+    g.upper = sellUpper.ptr;
+    g.mirror = sellMirror.ptr;
     g.rows = sellRows;
     g.slices = sellSlices;
     g.positions = sellPositions;
@@ -695,7 +725,6 @@ struct System final : SystemBase {
     g.slice_start = sellSliceStart.ptr;
     g.group_slice = sellGroupSlice.ptr;
     g.col = sellCol.ptr;
-    g.diag = sellDiag.ptr;
     g.cstart = sellCstart.ptr;
     g.centry = sellCentry.ptr;
     g.val = sellVal.ptr;
@@ -1022,14 +1051,14 @@ struct System final : SystemBase {
     Sys<S> s = view();
     uint32_t ps = pass, xz = x0zero ? 1u : 0u, tg = tangent ? 1u : 0u;
     const int idx = law == TL_LAW_SNH ? 1 : 0;
-    if (profiling) mark(2, true);
     const size_t dyn = idx ? (tangent ? pipeBytes<S, 1, true>() : pipeBytes<S, 1, false>())
                            : (tangent ? pipeBytes<S, 0, true>() : pipeBytes<S, 0, false>());
     const bool damp = hasDamping && idx == 0;
     const int sellG = B == 1 ? sellGrid() : 0;
     if (sellG > 0) {  // single body: assembled block matrix, pipelined PCG
       SellDev<S> g = sellView();
-      const unsigned blocks = (sellPositions + TILE - 1) / TILE;
+      const unsigned blocks = (sellUpperCount + TILE - 1) / TILE;
+      if (profiling) mark(1, true);  // the operator assembly counts as assembly time
       if (idx) {
         if (tangent) kSellAssemble<S, 1, true, false><<<blocks, TILE, 0, st>>>(s, g);
         else kSellAssemble<S, 1, false, false><<<blocks, TILE, 0, st>>>(s, g);
@@ -1042,9 +1071,14 @@ struct System final : SystemBase {
       }
       check();
       ++launches;
+      if (profiling) {
+        mark(1, false);
+        mark(2, true);
+      }
       void* args[] = {&s, &g, &X, &xz, &tg};
-      TL_CUDA(cudaLaunchCooperativeKernel((const void*)kPcgSell<S>, dim3(sellG), dim3(TILE), args, 0, st));
+      TL_CUDA(cudaLaunchCooperativeKernel((const void*)kPcgSell<S>, dim3(sellG), dim3(TILE), args, sellColBytes(), st));
     } else if (B == 1) {  // single body: two-level assembly, per-block partials
+      if (profiling) mark(2, true);
       void* args[] = {&s, &X, &xz};
       const void* fn = idx ? (tangent ? (const void*)kPcg1<S, 1, true> : (const void*)kPcg1<S, 1, false>)
                            : damp ? (tangent ? (const void*)kPcg1<S, 0, true, true> : (const void*)kPcg1<S, 0, false, true>)
@@ -1053,6 +1087,7 @@ struct System final : SystemBase {
       TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(gridOf(perSm)), dim3(TILE), args,
                                           sizeof(TileCache), st));
     } else {  // batch: two-level assembly, per-body scalars
+      if (profiling) mark(2, true);
       void* args[] = {&s, &X, &ps, &xz};
       const void* fn =
           idx ? (tangent ? (const void*)kPcgBatch<S, 1, true> : (const void*)kPcgBatch<S, 1, false>)
