@@ -140,12 +140,12 @@ def element_bytes(T, V, s_bytes, yields, commit=False):
     Dm^-1 (9 FP64 planes, 72 B), the FP64 volume (8 B), the lane (4 B) and, for
     a yielding material, the plastic point (2 Vec4 planes); per node the
     evaluation point (base and direction records).  An evaluation writes the
-    committed rotation (9 S), the matvec operator (9 S gradients + Vec4
-    coefficients) and the per-corner force/diagonal records (4 x (2 Vec4 + S));
+    committed rotation (9 S), the matvec operator record (3 Vec4: gradients
+    and coefficients) and the per-corner force/diagonal records (4 x (2 Vec4 + S));
     a commit pass writes only the plastic point."""
     v4 = 4 * s_bytes
     reads = T * (16 + 72 + 8 + 4 + (2 * v4 if yields else 0)) + V * 2 * v4
-    writes = T * (2 * v4) if commit else T * (9 * s_bytes + 9 * s_bytes + v4 + 4 * (2 * v4 + s_bytes))
+    writes = T * (2 * v4) if commit else T * (9 * s_bytes + 3 * v4 + 4 * (2 * v4 + s_bytes))
     return reads + writes
 
 
@@ -154,9 +154,9 @@ def pcg_bytes_per_iteration(T, V, slots, s_bytes, tangent):
     must move for one body, per the layout in talus_b200/csrc/tl_kernels.cuh:
     every array read or written once per phase.  s = 4 (FP32) or 8 (FP64)."""
     v4 = 4 * s_bytes
-    # A, per element: tet 16, rotated gradients 9 s, coefficients v4, [flow normal 2 v4],
+    # A, per element: tet 16, operator record 3 v4 (gradients, coefficients), [flow normal 2 v4],
     # tile CSR codes 4 x 2 B; per slot: offset 2 B + partial write v4; per node: p, z gathered
-    a = T * (16 + 9 * s_bytes + v4 + (2 * v4 if tangent else 0) + 8) + slots * (2 + v4) + V * 2 * v4
+    a = T * (16 + 3 * v4 + (2 * v4 if tangent else 0) + 8) + slots * (2 + v4) + V * 2 * v4
     # B, per node: p, z read, p write, slot CSR start 4 + per slot id 4 and partial v4, mass record, anchor, Ap write
     b = V * (2 * v4 + v4 + 4 + v4 + 1 + v4) + slots * (4 + v4)
     # C, per node: p, x read+write, Ap, r read+write, preconditioner (2 records), z write
@@ -183,11 +183,11 @@ def sell_bytes_per_iteration(blocks, V, s_bytes):
 
 def sell_assembly_bytes(T, blocks, s_bytes, tangent):
     """Unique bytes of one tl::kSellAssemble launch: the element matvec
-    operator (9 S gradients, Vec4 coefficients, [2 Vec4 flow normal]) and the
-    16 contributor codes of every element read once, each block written once
-    with its contributor range."""
+    operator record (3 Vec4, [2 Vec4 flow normal]) and the 16 contributor
+    codes of every element read once, each block written once with its
+    contributor range."""
     v4 = 4 * s_bytes
-    return T * (9 * s_bytes + v4 + (2 * v4 if tangent else 0) + 16 * 4) + blocks * (9 * s_bytes + 4)
+    return T * (3 * v4 + (2 * v4 if tangent else 0) + 16 * 4) + blocks * (9 * s_bytes + 4)
 
 
 def peaks():

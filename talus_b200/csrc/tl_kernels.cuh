@@ -109,6 +109,17 @@ struct GridSyncDev {
   int active;  // bodies still iterating in the current PCG solve
 };
 
+// Per-element matvec operator, one record per element: the gradients
+// R g_k (corotated) or g_k (SNH), k = 1..3, and the coefficients (a, b, c),
+// h_eff^2 V folded in, as (g1x g1y g1z g2x) (g2y g2z g3x g3y) (g3z a b c).
+// A record is read whole by one thread, so a gather by element touches 3
+// contiguous 16-byte pieces.  The rotated flow normal of the corotated
+// consistent tangent, (xx yy zz xy) (xz yz - -), is a separate pair per
+// element (Sys::onorm), read only by tangent solves.
+template <class S> struct OpRec {
+  Vec4<S> q[3];
+};
+
 template <class S> struct Sys {
   uint32_t bodies, Vp, Tp, node_tiles, elem_tiles;
   const BodyDev* body;
@@ -147,9 +158,8 @@ template <class S> struct Sys {
   const uint32_t* lane;
   const double* eyoung;   // per-element E override or null
   S* op;                  // 9 planes: committed R (corotated) or F (SNH)
-  S* og;                  // 9 planes: matvec gradients R g_k (corotated) or g_k (SNH), k = 1..3
-  Vec4<S>* oc;            // matvec coefficients (a, b, c, -), h_eff^2 V folded in
-  Vec4<S>* on;            // 2 planes: rotated flow normal (xx, yy, zz, xy), (xz, yz, -, -)
+  OpRec<S>* orec;         // [Tp] per-element matvec operator records
+  Vec4<S>* onorm;         // [2 Tp] rotated flow normal pairs (corotated consistent tangent)
   Vec4<S>* plast;         // 2 planes: (exx, eyy, ezz, exy), (exz, eyz, equivalent, -)
   Vec4<S>* fe;            // [4][Tp] corner planes: (fx, fy, fz, Dxx)
   Vec4<S>* de;            // [4][Tp] (Dyy, Dzz, Dxy, Dxz)
@@ -633,14 +643,11 @@ __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
         // V sigma_t(sym(sum_b p_b gh_b^T)) gh_a with gh = R g and the rotated
         // normal R n R^T; h_eff^2 V folded into the coefficients.
         const double sv = st.scale * vol;
-#pragma unroll
-        for (int k = 1; k < 4; ++k) {
-          const V3<S> gh = mul(Rw, cvt<S>(g[k]));
-          s.og[size_t(3 * (k - 1) + 0) * s.Tp + e] = gh.x;
-          s.og[size_t(3 * (k - 1) + 1) * s.Tp + e] = gh.y;
-          s.og[size_t(3 * (k - 1) + 2) * s.Tp + e] = gh.z;
-        }
-        s.oc[e] = Vec4<S>{S(sv * (bulk - 2.0 * mu * th / 3.0)), S(sv * 2.0 * mu * th), S(sv * 2.0 * mu * thb), S(0)};
+        const V3<S> gh1 = mul(Rw, cvt<S>(g[1])), gh2 = mul(Rw, cvt<S>(g[2])), gh3 = mul(Rw, cvt<S>(g[3]));
+        OpRec<S>& rec = s.orec[e];
+        rec.q[0] = Vec4<S>{gh1.x, gh1.y, gh1.z, gh2.x};
+        rec.q[1] = Vec4<S>{gh2.y, gh2.z, gh3.x, gh3.y};
+        rec.q[2] = Vec4<S>{gh3.z, S(sv * (bulk - 2.0 * mu * th / 3.0)), S(sv * 2.0 * mu * th), S(sv * 2.0 * mu * thb)};
         if (mode & EM_CONSISTENT) {
           M3<S> nm;
           nm.m[0][0] = nw.xx; nm.m[1][1] = nw.yy; nm.m[2][2] = nw.zz;
@@ -648,8 +655,8 @@ __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
           nm.m[0][2] = nm.m[2][0] = nw.xz;
           nm.m[1][2] = nm.m[2][1] = nw.yz;
           const M3<S> nh = mul(mul(Rw, nm), transpose(Rw));
-          s.on[e] = Vec4<S>{nh.m[0][0], nh.m[1][1], nh.m[2][2], nh.m[0][1]};
-          s.on[s.Tp + e] = Vec4<S>{nh.m[0][2], nh.m[1][2], S(0), S(0)};
+          s.onorm[2 * size_t(e)] = Vec4<S>{nh.m[0][0], nh.m[1][1], nh.m[2][2], nh.m[0][1]};
+          s.onorm[2 * size_t(e) + 1] = Vec4<S>{nh.m[0][2], nh.m[1][2], S(0), S(0)};
         }
       }
     } else {
@@ -687,13 +694,10 @@ __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
       // Matvec operator: dP = mu dF + ((lambda + mu)(J - 1) - mu) dcof + (lambda + mu)(cof : dF) cof,
       // h_eff^2 V folded into the coefficients; unrotated gradients.
       const double sv = st.scale * vol;
-#pragma unroll
-      for (int k = 1; k < 4; ++k) {
-        s.og[size_t(3 * (k - 1) + 0) * s.Tp + e] = S(g[k].x);
-        s.og[size_t(3 * (k - 1) + 1) * s.Tp + e] = S(g[k].y);
-        s.og[size_t(3 * (k - 1) + 2) * s.Tp + e] = S(g[k].z);
-      }
-      s.oc[e] = Vec4<S>{S(sv * mu), S(sv * (shifted * change - mu)), S(sv * shifted), S(0)};
+      OpRec<S>& rec = s.orec[e];
+      rec.q[0] = Vec4<S>{S(g[1].x), S(g[1].y), S(g[1].z), S(g[2].x)};
+      rec.q[1] = Vec4<S>{S(g[2].y), S(g[2].z), S(g[3].x), S(g[3].y)};
+      rec.q[2] = Vec4<S>{S(g[3].z), S(sv * mu), S(sv * (shifted * change - mu)), S(sv * shifted)};
     }
     if (!(mode & EM_COMMIT)) nonfinite = !finite;
   }
@@ -1053,13 +1057,24 @@ template <class S> struct ElementOperator {
   M3<S> F;
 };
 
+// The operator from the record's pieces q0..q2 (the flow normal pair for the
+// corotated tangent; F from the op planes for SNH).
+template <class S>
+__device__ __forceinline__ void unpackOperator(ElementOperator<S>& o, Vec4<S> q0, Vec4<S> q1, Vec4<S> q2) {
+  o.g[1] = {q0.x, q0.y, q0.z};
+  o.g[2] = {q0.w, q1.x, q1.y};
+  o.g[3] = {q1.z, q1.w, q2.x};
+  o.g[0] = -(o.g[1] + o.g[2] + o.g[3]);
+  o.k = Vec4<S>{q2.y, q2.z, q2.w, S(0)};
+}
+
 template <class S, int LAW, bool TANGENT>
 __device__ __forceinline__ ElementOperator<S> loadOperator(const Sys<S>& s, uint32_t e) {
   ElementOperator<S> o;
-  gradientsS<S>(s.og, s.Tp, e, o.g);
-  o.k = ld4g(&s.oc[e]);
+  const OpRec<S>* rec = s.orec + e;
+  unpackOperator(o, ld4g(&rec->q[0]), ld4g(&rec->q[1]), ld4g(&rec->q[2]));
   if (LAW == 0 && TANGENT) {
-    const Vec4<S> n0 = ld4g(&s.on[e]), n1 = ld4g(&s.on[s.Tp + e]);
+    const Vec4<S> n0 = ld4g(&s.onorm[2 * size_t(e)]), n1 = ld4g(&s.onorm[2 * size_t(e) + 1]);
     o.n = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y};
   }
   if (LAW == 1) {
@@ -1072,12 +1087,17 @@ __device__ __forceinline__ ElementOperator<S> loadOperator(const Sys<S>& s, uint
 }
 
 // ---- shared-memory stage of one tile's operators, filled by cp.async ----
-// Layout: og [9][TILE] S, oc [TILE] Vec4<S>, then op [9][TILE] S (SNH) or
-// on [2][TILE] Vec4<S> (corotated tangent).  Thread t copies and later reads
-// only element t's entries, so its own cp.async.wait_group orders them.
+// Layout: the tile's records [TILE] OpRec<S>, then for the corotated tangent
+// its flow normal pairs [TILE][2] Vec4<S>, then for SNH op [9][TILE] S.
+// Records and pairs are contiguous both in global and in shared memory, so
+// each warp copies its 32 elements' span in 16-byte chunks with consecutive
+// lanes on consecutive chunks (a per-thread copy of its own 48-byte record
+// would fetch every 32-byte sector twice).  A thread then reads entries that
+// other lanes copied: the caller orders the copies with cp.async.wait_group
+// followed by a block barrier.
 template <class S, int LAW, bool TANGENT> __host__ __device__ constexpr size_t stageBytes() {
-  return sizeof(S) * 9 * TILE + sizeof(Vec4<S>) * TILE +
-         (LAW == 1 ? sizeof(S) * 9 * TILE : (TANGENT ? sizeof(Vec4<S>) * 2 * TILE : 0));
+  return sizeof(OpRec<S>) * TILE + (LAW == 0 && TANGENT ? sizeof(Vec4<S>) * 2 * TILE : 0) +
+         (LAW == 1 ? sizeof(S) * 9 * TILE : 0);
 }
 template <int N> __device__ __forceinline__ void cpAsync(void* dst, const void* src) {
   const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
@@ -1089,54 +1109,47 @@ template <int N> __device__ __forceinline__ void cpAsync(void* dst, const void* 
 __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
+// e: this thread's element (tile * TILE + threadIdx.x, below Tp).
 template <class S, int LAW, bool TANGENT>
 __device__ __forceinline__ void stageOperator(const Sys<S>& s, uint32_t e, unsigned char* stage) {
-  const uint32_t t = threadIdx.x;
-  S* og = reinterpret_cast<S*>(stage);
-  Vec4<S>* oc = reinterpret_cast<Vec4<S>*>(stage + sizeof(S) * 9 * TILE);
-  unsigned char* extra = stage + sizeof(S) * 9 * TILE + sizeof(Vec4<S>) * TILE;
+  const uint32_t t = threadIdx.x, lane = t & 31u, first = t & ~31u;  // the warp's first element in the tile
+  {
+    constexpr uint32_t CHUNKS = uint32_t(sizeof(OpRec<S>)) * 32u / 16u;
+    const unsigned char* src = reinterpret_cast<const unsigned char*>(s.orec + (e - lane));
+    unsigned char* dst = stage + size_t(first) * sizeof(OpRec<S>);
 #pragma unroll
-  for (int k = 0; k < 9; ++k) cpAsync<sizeof(S)>(og + k * TILE + t, s.og + size_t(k) * s.Tp + e);
+    for (uint32_t c = lane; c < CHUNKS; c += 32u) cpAsync<16>(dst + 16 * c, src + 16 * c);
+  }
+  if (LAW == 0 && TANGENT) {
+    constexpr uint32_t CHUNKS = uint32_t(sizeof(Vec4<S>)) * 2u * 32u / 16u;
+    const unsigned char* src = reinterpret_cast<const unsigned char*>(s.onorm + 2 * size_t(e - lane));
+    unsigned char* dst = stage + sizeof(OpRec<S>) * TILE + size_t(first) * 2 * sizeof(Vec4<S>);
 #pragma unroll
-  for (int h = 0; h < int(sizeof(Vec4<S>) / 16); ++h)
-    cpAsync<16>(reinterpret_cast<unsigned char*>(oc + t) + 16 * h, reinterpret_cast<const unsigned char*>(s.oc + e) + 16 * h);
+    for (uint32_t c = lane; c < CHUNKS; c += 32u) cpAsync<16>(dst + 16 * c, src + 16 * c);
+  }
   if (LAW == 1) {
-    S* op = reinterpret_cast<S*>(extra);
+    S* op = reinterpret_cast<S*>(stage + sizeof(OpRec<S>) * TILE);
 #pragma unroll
     for (int k = 0; k < 9; ++k) cpAsync<sizeof(S)>(op + k * TILE + t, s.op + size_t(k) * s.Tp + e);
-  } else if (TANGENT) {
-    Vec4<S>* on = reinterpret_cast<Vec4<S>*>(extra);
-#pragma unroll
-    for (int q = 0; q < 2; ++q)
-#pragma unroll
-      for (int h = 0; h < int(sizeof(Vec4<S>) / 16); ++h)
-        cpAsync<16>(reinterpret_cast<unsigned char*>(on + q * TILE + t) + 16 * h,
-                    reinterpret_cast<const unsigned char*>(s.on + size_t(q) * s.Tp + e) + 16 * h);
   }
 }
 
 template <class S, int LAW, bool TANGENT>
 __device__ __forceinline__ ElementOperator<S> stagedOperator(const unsigned char* stage) {
   const uint32_t t = threadIdx.x;
-  const S* og = reinterpret_cast<const S*>(stage);
-  const Vec4<S>* oc = reinterpret_cast<const Vec4<S>*>(stage + sizeof(S) * 9 * TILE);
-  const unsigned char* extra = stage + sizeof(S) * 9 * TILE + sizeof(Vec4<S>) * TILE;
+  const OpRec<S>& rec = reinterpret_cast<const OpRec<S>*>(stage)[t];
   ElementOperator<S> o;
-  o.g[1] = {og[0 * TILE + t], og[1 * TILE + t], og[2 * TILE + t]};
-  o.g[2] = {og[3 * TILE + t], og[4 * TILE + t], og[5 * TILE + t]};
-  o.g[3] = {og[6 * TILE + t], og[7 * TILE + t], og[8 * TILE + t]};
-  o.g[0] = -(o.g[1] + o.g[2] + o.g[3]);
-  o.k = oc[t];
+  unpackOperator(o, rec.q[0], rec.q[1], rec.q[2]);
+  if (LAW == 0 && TANGENT) {
+    const Vec4<S>* nq = reinterpret_cast<const Vec4<S>*>(stage + sizeof(OpRec<S>) * TILE) + 2 * size_t(t);
+    o.n = {nq[0].x, nq[0].y, nq[0].z, nq[0].w, nq[1].x, nq[1].y};
+  }
   if (LAW == 1) {
-    const S* op = reinterpret_cast<const S*>(extra);
+    const S* op = reinterpret_cast<const S*>(stage + sizeof(OpRec<S>) * TILE);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
       for (int j = 0; j < 3; ++j) o.F.m[i][j] = op[(3 * i + j) * TILE + t];
-  } else if (TANGENT) {
-    const Vec4<S>* on = reinterpret_cast<const Vec4<S>*>(extra);
-    const Vec4<S> n0 = on[t], n1 = on[TILE + t];
-    o.n = {n0.x, n0.y, n0.z, n0.w, n1.x, n1.y};
   }
   return o;
 }

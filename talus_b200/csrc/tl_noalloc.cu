@@ -74,10 +74,11 @@ struct Layout {
   MatDev* mat;
   uint32_t *nodeTileBody, *elemTileBody, *start, *entry, *lane, *loading, *yielding, *counter;
   Vec4<S> *rest4, *pres, *u, *v, *a, *carried, *shifted, *weighted, *total, *incr, *right, *pre0, *pre1, *r, *z, *p,
-      *ap, *fe, *de, *ye, *oc, *on, *plast;
+      *ap, *fe, *de, *ye, *plast, *onorm;
+  OpRec<S>* orec;
   uint8_t* anch;
   uint4* tet;
-  double *dm, *vold, *op, *og, *de2, *part, *npart, *epart;
+  double *dm, *vold, *op, *de2, *part, *npart, *epart;
   BodyAccDev* acc;
   CgBodyDev* cg;
   CgReportDev* cgrep;
@@ -104,9 +105,8 @@ Layout carve(unsigned char* base) {
   l.vold = c.take<double>(NA_TP);
   l.lane = c.take<uint32_t>(NA_TP);
   l.op = c.take<double>(size_t(9) * NA_TP);
-  l.og = c.take<double>(size_t(9) * NA_TP);
-  l.oc = c.take<Vec4<S>>(NA_TP);
-  l.on = c.take<Vec4<S>>(size_t(2) * NA_TP);
+  l.orec = c.take<OpRec<S>>(NA_TP);
+  l.onorm = c.take<Vec4<S>>(size_t(2) * NA_TP);
   l.plast = c.take<Vec4<S>>(size_t(2) * NA_TP);
   l.fe = c.take<Vec4<S>>(size_t(4) * NA_TP);
   l.de = c.take<Vec4<S>>(size_t(4) * NA_TP);
@@ -214,9 +214,8 @@ Sys<S> viewOf(const Layout& l, uint32_t Vp, uint32_t Tp) {
   s.lane = l.lane;
   s.eyoung = nullptr;
   s.op = l.op;
-  s.og = l.og;
-  s.oc = l.oc;
-  s.on = l.on;
+  s.orec = l.orec;
+  s.onorm = l.onorm;
   s.plast = l.plast;
   s.fe = l.fe;
   s.de = l.de;
@@ -387,9 +386,8 @@ int32_t stepLocked(int32_t device, const tl_mesh_desc& d, int32_t dtype, void* p
   NA_CUDA(cudaMemsetAsync(l.sync, 0, sizeof(GridSyncDev), st));
   NA_CUDA(cudaMemsetAsync(l.loading, 0, sizeof(uint32_t), st));
   NA_CUDA(cudaMemsetAsync(l.yielding, 0, sizeof(uint32_t), st));
-  NA_CUDA(cudaMemsetAsync(l.og, 0, sizeof(double) * 9 * Tp, st));
-  NA_CUDA(cudaMemsetAsync(l.oc, 0, sizeof(Vec4<S>) * Tp, st));
-  NA_CUDA(cudaMemsetAsync(l.on, 0, sizeof(Vec4<S>) * 2 * Tp, st));
+  NA_CUDA(cudaMemsetAsync(l.orec, 0, sizeof(OpRec<S>) * Tp, st));
+  NA_CUDA(cudaMemsetAsync(l.onorm, 0, sizeof(Vec4<S>) * 2 * Tp, st));
   const Sys<S> s = viewOf(l, Vp, Tp);
   const uint32_t nodeTiles = Vp / TILE, elemTiles = Tp / TILE;
   uint32_t launches = 0;

@@ -199,8 +199,9 @@ struct System final : SystemBase {
   DevBuf<uint32_t> start, entry, lane;
   DevBuf<uint4> tet;
   DevBuf<double> dm, vold, eyoung;
-  DevBuf<S> dms, vols, op, og, de2;
-  DevBuf<Vec4<S>> oc, on, plast, fe, de, ye;
+  DevBuf<S> dms, vols, op, de2;
+  DevBuf<Vec4<S>> plast, fe, de, ye, onorm;
+  DevBuf<OpRec<S>> orec;
   // two-level assembly structures (single-body PCG)
   DevBuf<uint2> tileMeta;
   DevBuf<uint16_t> tileOff, tileEnt;
@@ -330,9 +331,8 @@ struct System final : SystemBase {
     s.lane = lane.ptr;
     s.eyoung = hasEyoung ? eyoung.ptr : nullptr;
     s.op = op.ptr;
-    s.og = og.ptr;
-    s.oc = oc.ptr;
-    s.on = on.ptr;
+    s.orec = orec.ptr;
+    s.onorm = onorm.ptr;
     s.tile_meta = tileMeta.ptr;
     s.tile_off = tileOff.ptr;
     s.tile_ent = tileEnt.ptr;
@@ -546,12 +546,10 @@ struct System final : SystemBase {
       op.upload(ident.data(), ident.size(), st);
       TL_CUDA(cudaStreamSynchronize(st));
     }
-    og.alloc(size_t(9) * Tp);
-    og.zero(st);
-    oc.alloc(Tp);
-    oc.zero(st);
-    on.alloc(size_t(2) * Tp);
-    on.zero(st);
+    orec.alloc(Tp);
+    orec.zero(st);
+    onorm.alloc(size_t(2) * Tp);
+    onorm.zero(st);
     plast.alloc(size_t(2) * Tp);
     plast.zero(st);
     fe.alloc(size_t(4) * Tp);
