@@ -117,7 +117,7 @@ __device__ __forceinline__ void addElementBlock(const Sys<S>& s, uint32_t e, uin
 // row is zero (its transpose, in a free row, is not).  Padding positions are
 // zero from the build and are never written.
 template <class S, int LAW, bool TANGENT, bool DAMP>
-__global__ void __launch_bounds__(TILE) kSellAssemble(Sys<S> s, SellDev<S> g) {
+__global__ void __launch_bounds__(TILE, 4) kSellAssemble(Sys<S> s, SellDev<S> g) {
   const uint32_t i = blockIdx.x * TILE + threadIdx.x;
   if (i >= g.upper_count) return;
   const uint32_t pos = g.upper[i], mpos = g.mirror[i];

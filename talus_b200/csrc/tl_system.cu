@@ -158,6 +158,7 @@ struct SystemBase {
   virtual void stateGet(uint32_t body, int32_t dtype, void* x, void* v, void* a, void* rot, void* plastic) = 0;
   virtual int32_t step(const tl_settings& set, const double g[3], double dt, tl_step_report* reports) = 0;
   virtual void tune(uint32_t blocksPerSm, uint32_t graph) = 0;
+  virtual void setSolver(uint32_t form) = 0;
   std::vector<uint32_t> trace;  // TL_FLAG_TRACE: iterations of each PCG launch (body 0)
   uint32_t bodies = 0;
   uint64_t nodes = 0, tets = 0;
@@ -226,6 +227,7 @@ struct System final : SystemBase {
   int batchDampPerSm[2] = {0, 0};
   uint32_t tuneBlocksPerSm = 0;              // tl_system_tune: cap on the persistent grid (0 = occupancy)
   bool tuneGraph = true;                     // tl_system_tune: capture batched elastic steps in a CUDA graph
+  uint32_t solverForm = TL_SOLVER_AUTO;      // tl_system_set_solver
   int gridOf(int perSm) const {
     const int use = tuneBlocksPerSm ? std::min<int>(perSm, int(tuneBlocksPerSm)) : perSm;
     return std::max(1, std::min(use * ctx->sms, int(std::max(nodeTiles, elemTiles))));
@@ -677,6 +679,20 @@ struct System final : SystemBase {
           mirror.push_back(sliceStart[c / SELL_ROWS] + kc * SELL_ROWS + c % SELL_ROWS);
         }
     }
+    {  // longest contributor lists first, so warps take similar loop counts
+      std::vector<uint32_t> order(upper.size());
+      for (uint32_t i = 0; i < order.size(); ++i) order[i] = i;
+      std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+        return cstart[upper[x] + 1] - cstart[upper[x]] > cstart[upper[y] + 1] - cstart[upper[y]];
+      });
+      std::vector<uint32_t> u2(upper.size()), m2(upper.size());
+      for (uint32_t i = 0; i < order.size(); ++i) {
+        u2[i] = upper[order[i]];
+        m2[i] = mirror[order[i]];
+      }
+      upper.swap(u2);
+      mirror.swap(m2);
+    }
     sellUpperCount = uint32_t(upper.size());
     sellColCache = std::min(widest, SELL_COL_CACHE_MAX);
     sellUpper.alloc(std::max<size_t>(upper.size(), 1));
@@ -733,7 +749,7 @@ struct System final : SystemBase {
   // block still has at most one slice per warp), or 0 when the rows do not
   // fit one per thread.
   int sellGrid() const {
-    if (!sellReady) return 0;
+    if (!sellReady || solverForm == TL_SOLVER_ELEMENTWISE) return 0;
     const int full = std::min<int>(sellPerSm * ctx->sms, int(sellSlices));
     const int capped = tuneBlocksPerSm ? std::min<int>(std::min<int>(sellPerSm, int(tuneBlocksPerSm)) * ctx->sms,
                                                        int(sellSlices))
@@ -1444,6 +1460,7 @@ struct System final : SystemBase {
   uint32_t graphLaunches = 0;
   std::vector<std::pair<int, size_t>> graphEv;  // event pairs recorded by the captured graph
 
+  void setSolver(uint32_t form) override { solverForm = form; }
   void tune(uint32_t blocksPerSm, uint32_t graph) override {
     tuneBlocksPerSm = blocksPerSm;
     tuneGraph = graph != 0u;
@@ -1943,6 +1960,12 @@ int32_t tl_system_tune(tl_system* system, uint32_t pcg_blocks_per_sm, uint32_t g
     system->impl->tune(pcg_blocks_per_sm, graph);
     return TL_OK;
   });
+}
+
+int32_t tl_system_set_solver(tl_system* system, uint32_t form) {
+  if (!system || form > TL_SOLVER_ELEMENTWISE) return TL_ERR_ARG;
+  system->impl->setSolver(form);
+  return TL_OK;
 }
 
 int32_t tl_system_trace(const tl_system* system, uint32_t* iterations, uint32_t capacity, uint32_t* count) {

@@ -245,6 +245,13 @@ class System:
         (0 = occupancy limit) and CUDA-graph replay of batched elastic steps."""
         check(capi.lib().tl_system_tune(self.handle, int(pcg_blocks_per_sm), 1 if graph else 0), self.context.handle)
 
+    def set_solver(self, form: str = "auto"):
+        """PCG operator form of a single-body system (tl_system_set_solver):
+        "auto", "assembled" (3x3 node blocks assembled once per solve) or
+        "elementwise" (applied element by element every iteration)."""
+        code = {"auto": 0, "assembled": 1, "elementwise": 2}[form]
+        check(capi.lib().tl_system_set_solver(self.handle, code), self.context.handle)
+
     def trace(self) -> list:
         """Iterations of every PCG launch made with Settings.trace, oldest first."""
         count = C.c_uint32()

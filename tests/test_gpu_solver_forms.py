@@ -1,0 +1,67 @@
+"""The two forms of the single-body PCG operator (tl_system_set_solver): the
+assembled 3x3 node-block matrix and the element-by-element application of
+applySystem (solver.cc:904-1048).  They apply the same operator, so their
+trajectories agree to rounding, and each matches the FP64 oracle at the
+parity bars of test_gpu_parity."""
+import numpy as np
+import pytest
+
+import talus_b200 as tb
+from oracle import pyoracle as po
+from tests.helpers import DT, GRAVITY, elastic_block, plastic_block, relative_error, run_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def run(form, precision, mesh, mat, settings, steps):
+    s = tb.System(mesh, [mat], precision)
+    s.set_solver(form)
+    s.set_state(tb.rest_state(mesh))
+    reports = [s.step(settings, GRAVITY, DT)[0].as_dict() for _ in range(steps)]
+    x = s.get_state().position
+    s.close()
+    return x, reports
+
+
+@pytest.mark.parametrize("law", [tb.COROTATED, tb.NEO_HOOKEAN])
+def test_forms_agree_on_the_elastic_block(law):
+    mesh, mat = elastic_block()
+    settings = tb.Settings(law=law)
+    xa, ra = run("assembled", tb.FP64, mesh, mat, settings, 10)
+    xe, re = run("elementwise", tb.FP64, mesh, mat, settings, 10)
+    assert relative_error(xa, xe, mesh.rest_positions) <= 1e-10
+    assert [r["cg_iterations"] for r in ra] == [r["cg_iterations"] for r in re]
+
+
+def test_elementwise_form_matches_the_oracle():
+    mesh, mat = elastic_block()
+    ref, got = [], []
+    run_oracle(po.F64, mesh, mat, tb.Settings(), 8, record=ref)
+    s = tb.System(mesh, [mat], tb.FP64)
+    s.set_solver("elementwise")
+    s.set_state(tb.rest_state(mesh))
+    for _ in range(8):
+        s.step(tb.Settings(), GRAVITY, DT)
+        got.append(s.get_state().position)
+    s.close()
+    for step, (x, r) in enumerate(zip(got, ref)):
+        assert relative_error(x, r, mesh.rest_positions) <= 1e-9, step
+
+
+@pytest.mark.parametrize("precision,tol", [(tb.FP64, 1e-8), (tb.FP32_MIXED, 1e-5)])
+def test_forms_agree_on_the_plastic_block(precision, tol):
+    mesh, mat = plastic_block()
+    xa, ra = run("assembled", precision, mesh, mat, tb.Settings(), 6)
+    xe, re = run("elementwise", precision, mesh, mat, tb.Settings(), 6)
+    assert relative_error(xa, xe, mesh.rest_positions) <= tol
+    if precision == tb.FP64:
+        assert [r["plastic_evaluations"] for r in ra] == [r["plastic_evaluations"] for r in re]
+
+
+def test_unknown_form_is_rejected():
+    mesh, mat = elastic_block((3, 3, 3))
+    s = tb.System(mesh, [mat], tb.FP64)
+    with pytest.raises(tb._capi.TalusError) as e:
+        tb._capi.check(tb._capi.lib().tl_system_set_solver(s.handle, 3), s.context.handle)
+    assert e.value.status == tb._capi.TL_ERR_ARG
+    s.close()
