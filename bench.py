@@ -164,6 +164,9 @@ def pcg_bytes_per_iteration(T, V, slots, s_bytes, tangent):
     return a + b + c
 
 
+SELL_AUTO_MIN_TETS = 32768  # smallest body TL_SOLVER_AUTO assembles (talus_b200/csrc/tl_system.cu)
+
+
 def operator_blocks(mesh):
     """Nonzero 3x3 blocks of the assembled single-body operator: the ordered
     node pairs that share an element (the diagonal included)."""
@@ -465,9 +468,11 @@ def run_ours(args, spec, rank, world, dist):
     s_bytes = 4 if precision == tb.FP32_MIXED else 8
     pcg_bytes = 0.0
     assembly = None
+    # the form TL_SOLVER_AUTO takes: assembled for one body of >= 32,768 tets
+    assembled = B == 1 and meshes[0].tets >= SELL_AUTO_MIN_TETS
     for b, m in enumerate(meshes):
         it, tan = per_body[b, 0], per_body[b, 1]
-        if B == 1:  # assembled operator (tl_sell.cuh)
+        if assembled:  # assembled operator (tl_sell.cuh)
             blocks = operator_blocks(m)
             pcg_bytes += sell_bytes_per_iteration(blocks, m.nodes, s_bytes) * it
             assembly = {"kernel": "tl::kSellAssemble (block matrix, once per solve)", "blocks": blocks,
@@ -485,12 +490,14 @@ def run_ours(args, spec, rank, world, dist):
     if os.path.exists(tpath):
         with open(tpath) as f:
             tr = json.load(f)
-        same_kernel = tr.get("kernel", "").startswith("tl::kPcgSell" if B == 1 else "tl::kPcgBatch")
+        same_kernel = tr.get("kernel", "").startswith(
+            "tl::kPcgSell" if assembled else "tl::kPcg1" if B == 1 else "tl::kPcgBatch")
         if tr.get("workload") == args.workload and tr.get("precision") == args.precision and same_kernel and launches_pcg:
             traffic = tr["dram_bytes_per_iteration"] * per_body[:, 0].sum() / launches_pcg
 
     kernel = ("tl::kPcgSell (persistent pipelined block-Jacobi PCG on the assembled sliced-ELL block matrix)"
-              if B == 1 else
+              if assembled else
+              "tl::kPcg1 (persistent block-Jacobi PCG, element by element, two-level assembly)" if B == 1 else
               "tl::kPcgBatch (persistent block-Jacobi PCG over all bodies, two-level assembly)")
     config = {"workload": args.workload, "bodies": B, "tets": T, "nodes": V, "law": spec["law"],
               "precision": args.precision, "dt": 1.0 / 60.0,

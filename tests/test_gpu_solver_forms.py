@@ -58,6 +58,25 @@ def test_forms_agree_on_the_plastic_block(precision, tol):
         assert [r["plastic_evaluations"] for r in ra] == [r["plastic_evaluations"] for r in re]
 
 
+@pytest.mark.parametrize("precision,tol", [(tb.FP64, 1e-8), (tb.FP32_MIXED, 1e-5)])
+def test_assembled_form_matches_the_oracle_on_the_plastic_block(precision, tol):
+    mesh, mat = plastic_block()
+    ref, got = [], []
+    _, oreps = run_oracle(po.F64, mesh, mat, tb.Settings(), 6, record=ref)
+    s = tb.System(mesh, [mat], precision)
+    s.set_solver("assembled")
+    s.set_state(tb.rest_state(mesh))
+    greps = []
+    for _ in range(6):
+        greps.append(s.step(tb.Settings(), GRAVITY, DT)[0].as_dict())
+        got.append(s.get_state().position)
+    s.close()
+    for step, (x, r) in enumerate(zip(got, ref)):
+        assert relative_error(x, r, mesh.rest_positions) <= tol, step
+    if precision == tb.FP64:
+        assert [r["plastic_evaluations"] for r in greps] == [r["plastic_evaluations"] for r in oreps]
+
+
 def test_unknown_form_is_rejected():
     mesh, mat = elastic_block((3, 3, 3))
     s = tb.System(mesh, [mat], tb.FP64)
