@@ -28,6 +28,8 @@ def main():
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--count", type=int, default=0, help="bodies of a batch workload (0: the workload's own)")
+    ap.add_argument("--solver", choices=["auto", "assembled", "elementwise"], default="auto",
+                    help="PCG operator form of a single-body system (tl_system_set_solver)")
     args = ap.parse_args()
     spec = dict(WORKLOADS[args.workload])
     if args.count and spec.get("batch"):
@@ -36,6 +38,7 @@ def main():
     precision = tb.FP32_MIXED if args.precision == "mixed" else tb.FP64
     law = tb.NEO_HOOKEAN if spec["law"] == "snh" else tb.COROTATED
     system = tb.System(meshes, mats, precision)
+    system.set_solver(args.solver)
     for i, m in enumerate(meshes):
         system.set_state(tb.rest_state(m), i)
     settings = tb.Settings(law=law, trace=True)
