@@ -1040,6 +1040,50 @@ __device__ __forceinline__ void dampingProduct(const Sys<S>& s, uint32_t e, cons
   for (int c = 0; c < 4; ++c) y[c] = y[c] + d[c];
 }
 
+// ------------------------------------------------- state transfer ----
+// A body's committed rotations and plastic points between the caller's
+// per-tet layout (DeformableState, mesh.h:56-62: the rotation's 9 entries
+// row-major; the plastic strain's 9 entries row-major, then the equivalent
+// strain) and the element planes (op; plast as (exx, eyy, ezz, exy),
+// (exz, eyz, equivalent, -), off-diagonals averaged in FP64).  Tet t of the
+// body is element e0 + t; null arrays are skipped.
+template <class S, class H>
+__global__ void __launch_bounds__(TILE) kElemStateIn(Sys<S> s, uint32_t e0, uint32_t T, const H* rot,
+                                                     const H* plastic) {
+  const uint32_t t = blockIdx.x * TILE + threadIdx.x;
+  if (t >= T) return;
+  const size_t e = size_t(e0) + t;
+  if (rot) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) s.op[size_t(k) * s.Tp + e] = S(rot[9 * size_t(t) + k]);
+  }
+  if (plastic) {
+    const H* q = plastic + 10 * size_t(t);
+    s.plast[e] = Vec4<S>{S(q[0]), S(q[4]), S(q[8]), S(0.5 * (double(q[1]) + double(q[3])))};
+    s.plast[size_t(s.Tp) + e] = Vec4<S>{S(0.5 * (double(q[2]) + double(q[6]))),
+                                        S(0.5 * (double(q[5]) + double(q[7]))), S(q[9]), S(0)};
+  }
+}
+
+template <class S, class H>
+__global__ void __launch_bounds__(TILE) kElemStateOut(Sys<S> s, uint32_t e0, uint32_t T, H* rot, H* plastic) {
+  const uint32_t t = blockIdx.x * TILE + threadIdx.x;
+  if (t >= T) return;
+  const size_t e = size_t(e0) + t;
+  if (rot) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) rot[9 * size_t(t) + k] = H(s.op[size_t(k) * s.Tp + e]);
+  }
+  if (plastic) {
+    H* q = plastic + 10 * size_t(t);
+    const Vec4<S> a0 = s.plast[e], a1 = s.plast[size_t(s.Tp) + e];
+    q[0] = H(a0.x); q[1] = H(a0.w); q[2] = H(a1.x);
+    q[3] = H(a0.w); q[4] = H(a0.y); q[5] = H(a1.y);
+    q[6] = H(a1.x); q[7] = H(a1.y); q[8] = H(a0.z);
+    q[9] = H(a1.z);
+  }
+}
+
 // ---------------------------------------------------------------- PCG ----
 
 // h_eff^2 (R K R^T p)_e for one tet: applyStiffness (material.cc:267-288) with
