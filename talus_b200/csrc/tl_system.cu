@@ -353,6 +353,7 @@ struct System final : SystemBase {
   }
   ~System() override {
     if (graphExec) cudaGraphExecDestroy(graphExec);
+    for (cudaEvent_t e : xferEvents) cudaEventDestroy(e);
     for (auto& e : evPool) {
       cudaEventDestroy(e.first);
       cudaEventDestroy(e.second);
@@ -1017,6 +1018,32 @@ struct System final : SystemBase {
     host = reinterpret_cast<H*>(hXfer.get(bytes));
     dev = reinterpret_cast<H*>(dXfer.ptr);
   }
+  // Host <-> staging copies and DMA in chunks of XFER_CHUNK bytes: each
+  // chunk's DMA runs while the host copies the next one (uploads), or the
+  // host copies a chunk out while the later ones are still in flight
+  // (downloads, one event per chunk).
+  static constexpr size_t XFER_CHUNK = size_t(4) << 20;
+  std::vector<cudaEvent_t> xferEvents;
+  void upload(unsigned char* dev, unsigned char* stage, const unsigned char* src, size_t bytes) {
+    for (size_t o = 0; o < bytes; o += XFER_CHUNK) {
+      const size_t n = std::min(XFER_CHUNK, bytes - o);
+      parallelCopy(stage + o, src + o, n);
+      TL_CUDA(cudaMemcpyAsync(dev + o, stage + o, n, cudaMemcpyHostToDevice, st));
+    }
+  }
+  void queueDownload(unsigned char* stage, const unsigned char* dev, size_t bytes) {
+    const size_t chunks = (bytes + XFER_CHUNK - 1) / XFER_CHUNK;
+    while (xferEvents.size() < chunks) {
+      cudaEvent_t e;
+      TL_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      xferEvents.push_back(e);
+    }
+    for (size_t c = 0; c < chunks; ++c) {
+      const size_t o = c * XFER_CHUNK, n = std::min(XFER_CHUNK, bytes - o);
+      TL_CUDA(cudaMemcpyAsync(stage + o, dev + o, n, cudaMemcpyDeviceToHost, st));
+      TL_CUDA(cudaEventRecord(xferEvents[c], st));
+    }
+  }
   template <class H>
   void setElems(const BodyDev& bd, const HostBody& h, const H* rot, const H* plastic) {
     const uint32_t T = h.tets;
@@ -1024,14 +1051,10 @@ struct System final : SystemBase {
     if (!nR && !nP) return;
     H *stage, *dev;
     elemStaging<H>(nR + nP, stage, dev);
-    if (rot) {
-      parallelCopy(stage, rot, nR * sizeof(H));
-      TL_CUDA(cudaMemcpyAsync(dev, stage, nR * sizeof(H), cudaMemcpyHostToDevice, st));
-    }
-    if (plastic) {  // copied on the host while the rotations travel
-      parallelCopy(stage + nR, plastic, nP * sizeof(H));
-      TL_CUDA(cudaMemcpyAsync(dev + nR, stage + nR, nP * sizeof(H), cudaMemcpyHostToDevice, st));
-    }
+    auto bytes = [](auto* p) { return reinterpret_cast<unsigned char*>(p); };
+    if (rot) upload(bytes(dev), bytes(stage), reinterpret_cast<const unsigned char*>(rot), nR * sizeof(H));
+    if (plastic)
+      upload(bytes(dev + nR), bytes(stage + nR), reinterpret_cast<const unsigned char*>(plastic), nP * sizeof(H));
     kElemStateIn<S, H><<<(T + TILE - 1) / TILE, TILE, 0, st>>>(view(), bd.elem_begin, T, rot ? dev : nullptr,
                                                                plastic ? dev + nR : nullptr);
     check();
@@ -1048,16 +1071,27 @@ struct System final : SystemBase {
     kElemStateOut<S, H><<<(T + TILE - 1) / TILE, TILE, 0, st>>>(view(), bd.elem_begin, T, rot ? dev : nullptr,
                                                                 plastic ? dev + nR : nullptr);
     check();
-    TL_CUDA(cudaMemcpyAsync(stage, dev, (nR + nP) * sizeof(H), cudaMemcpyDeviceToHost, st));
+    queueDownload(reinterpret_cast<unsigned char*>(stage), reinterpret_cast<const unsigned char*>(dev),
+                  (nR + nP) * sizeof(H));
   }
-  // Copies the fetched element state out (after the stream has finished).
+  // Copies the fetched element state out, chunk by chunk as it arrives.
   template <class H>
   void getElems(const HostBody& h, H* rot, H* plastic) {
     const uint32_t T = h.tets;
     const size_t nR = rot ? size_t(9) * T : 0, nP = plastic ? size_t(10) * T : 0;
-    const H* stage = reinterpret_cast<const H*>(hXfer.ptr);
-    if (rot) parallelCopy(rot, stage, nR * sizeof(H));
-    if (plastic) parallelCopy(plastic, stage + nR, nP * sizeof(H));
+    const unsigned char* stage = hXfer.ptr;
+    if (!nR && !nP) return;
+    // the staging holds [rotations][plastic]; chunks may straddle the two
+    const size_t total = (nR + nP) * sizeof(H);
+    for (size_t o = 0, c = 0; o < total; o += XFER_CHUNK, ++c) {
+      TL_CUDA(cudaEventSynchronize(xferEvents[c]));
+      const size_t end = std::min(total, o + XFER_CHUNK), split = nR * sizeof(H);
+      if (o < split) parallelCopy(reinterpret_cast<unsigned char*>(rot) + o, stage + o, std::min(end, split) - o);
+      if (end > split) {
+        const size_t from = std::max(o, split);
+        parallelCopy(reinterpret_cast<unsigned char*>(plastic) + (from - split), stage + from, end - from);
+      }
+    }
   }
 
   void stateSet(uint32_t b, int32_t dtype, const void* x, const void* vv, const void* aa, const void* rot,
@@ -1091,17 +1125,19 @@ struct System final : SystemBase {
     if (sa) a.download(sa, h.nodes, st, bd.node_begin);
     if (dtype == TL_DTYPE_F64) fetchElems<double>(bd, h, rot != nullptr, pl != nullptr);
     else fetchElems<float>(bd, h, rot != nullptr, pl != nullptr);
+    // element state is copied out chunk by chunk as it arrives; the node
+    // records were queued first, so they have arrived once the stream ends
+    if (dtype == TL_DTYPE_F64) getElems(h, static_cast<double*>(rot), static_cast<double*>(pl));
+    else getElems(h, static_cast<float*>(rot), static_cast<float*>(pl));
     TL_CUDA(cudaStreamSynchronize(st));
     if (dtype == TL_DTYPE_F64) {
       if (x) unstageNodes(h, sx, static_cast<double*>(x), true);
       if (vv) unstageNodes(h, sv, static_cast<double*>(vv), false);
       if (aa) unstageNodes(h, sa, static_cast<double*>(aa), false);
-      getElems(h, static_cast<double*>(rot), static_cast<double*>(pl));
     } else {
       if (x) unstageNodes(h, sx, static_cast<float*>(x), true);
       if (vv) unstageNodes(h, sv, static_cast<float*>(vv), false);
       if (aa) unstageNodes(h, sa, static_cast<float*>(aa), false);
-      getElems(h, static_cast<float*>(rot), static_cast<float*>(pl));
     }
   }
 
