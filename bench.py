@@ -184,6 +184,16 @@ def sell_bytes_per_iteration(blocks, V, s_bytes):
     return blocks * (9 * s_bytes + 4) + 2 * V * v4
 
 
+def sell_batch_bytes_per_iteration(blocks, V, s_bytes):
+    """Unique bytes of one body's iteration in tl::kPcgBatchSell: the body's
+    matrix blocks (9 S entries and a column index) once; per node, the
+    previous direction and z gathered, the new direction and A p written
+    (phase AB), then direction, x, A p, r, the preconditioner (2 records)
+    read and x, r, z written (phase C)."""
+    v4 = 4 * s_bytes
+    return blocks * (9 * s_bytes + 4) + V * 13 * v4
+
+
 def sell_assembly_bytes(T, blocks, s_bytes, tangent):
     """Unique bytes of one tl::kSellAssemble launch: the element matvec
     operator record (3 Vec4, [2 Vec4 flow normal]) and the 16 contributor
@@ -468,15 +478,19 @@ def run_ours(args, spec, rank, world, dist):
     s_bytes = 4 if precision == tb.FP32_MIXED else 8
     pcg_bytes = 0.0
     assembly = None
-    # the form TL_SOLVER_AUTO takes: assembled for one body of >= 32,768 tets
-    assembled = B == 1 and meshes[0].tets >= SELL_AUTO_MIN_TETS
+    # the form TL_SOLVER_AUTO takes: assembled for a batch and for one body of >= 32,768 tets
+    assembled = B > 1 or meshes[0].tets >= SELL_AUTO_MIN_TETS
     for b, m in enumerate(meshes):
         it, tan = per_body[b, 0], per_body[b, 1]
         if assembled:  # assembled operator (tl_sell.cuh)
             blocks = operator_blocks(m)
-            pcg_bytes += sell_bytes_per_iteration(blocks, m.nodes, s_bytes) * it
-            assembly = {"kernel": "tl::kSellAssemble (block matrix, once per solve)", "blocks": blocks,
-                        "algorithmic_bytes_per_launch": sell_assembly_bytes(m.tets, blocks, s_bytes, tan > 0)}
+            per_it = (sell_bytes_per_iteration if B == 1 else sell_batch_bytes_per_iteration)(blocks, m.nodes, s_bytes)
+            pcg_bytes += per_it * it
+            if assembly is None:
+                assembly = {"kernel": "tl::kSellAssemble (block matrix, once per solve)", "blocks": 0,
+                            "algorithmic_bytes_per_launch": 0}
+            assembly["blocks"] += blocks
+            assembly["algorithmic_bytes_per_launch"] += sell_assembly_bytes(m.tets, blocks, s_bytes, tan > 0)
         else:
             slots = tile_slots(m)
             pcg_bytes += (pcg_bytes_per_iteration(m.tets, m.nodes, slots, s_bytes, True) * tan +
@@ -490,15 +504,17 @@ def run_ours(args, spec, rank, world, dist):
     if os.path.exists(tpath):
         with open(tpath) as f:
             tr = json.load(f)
-        same_kernel = tr.get("kernel", "").startswith(
-            "tl::kPcgSell" if assembled else "tl::kPcg1" if B == 1 else "tl::kPcgBatch")
+        prefix = ("tl::kPcgSell" if B == 1 else "tl::kPcgBatchSell") if assembled else (
+            "tl::kPcg1" if B == 1 else "tl::kPcgBatch<")
+        same_kernel = tr.get("kernel", "").startswith(prefix)
         if tr.get("workload") == args.workload and tr.get("precision") == args.precision and same_kernel and launches_pcg:
             traffic = tr["dram_bytes_per_iteration"] * per_body[:, 0].sum() / launches_pcg
 
-    kernel = ("tl::kPcgSell (persistent pipelined block-Jacobi PCG on the assembled sliced-ELL block matrix)"
-              if assembled else
-              "tl::kPcg1 (persistent block-Jacobi PCG, element by element, two-level assembly)" if B == 1 else
-              "tl::kPcgBatch (persistent block-Jacobi PCG over all bodies, two-level assembly)")
+    if B == 1:
+        kernel = ("tl::kPcgSell (persistent pipelined block-Jacobi PCG on the assembled sliced-ELL block matrix)"
+                  if assembled else "tl::kPcg1 (persistent block-Jacobi PCG, element by element, two-level assembly)")
+    else:
+        kernel = "tl::kPcgBatchSell (persistent block-Jacobi PCG over all bodies on the assembled block matrix)"
     config = {"workload": args.workload, "bodies": B, "tets": T, "nodes": V, "law": spec["law"],
               "precision": args.precision, "dt": 1.0 / 60.0,
               "parallelism": "single-gpu" if world == 1 else (f"shards{world}" if spec.get("batch") else f"replicas{world}"),

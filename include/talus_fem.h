@@ -162,16 +162,15 @@ int32_t tl_system_counts(const tl_system* system, uint32_t* bodies, uint64_t* no
  * capture its elastic step in a CUDA graph and replay it every step. */
 int32_t tl_system_tune(tl_system* system, uint32_t pcg_blocks_per_sm, uint32_t graph);
 
-/* Form of the PCG operator of a single-body system, no reference
- * counterpart (the reference applies it element by element, solver.cc:904-1048):
- * TL_SOLVER_ASSEMBLED assembles the 3x3 node blocks once per solve and
- * iterates on that matrix (about 40 bytes per nonzero block in FP32, 76 in
- * FP64) when every node row fits one thread of the persistent grid, and
- * otherwise falls back to the element-by-element form;
- * TL_SOLVER_ELEMENTWISE always iterates element by element; TL_SOLVER_AUTO
- * (default) is ASSEMBLED for bodies of at least 32,768 tets and ELEMENTWISE
- * below.  Batched systems always iterate element by element.  Both forms
- * apply the same operator; they differ in rounding. */
+/* Form of the PCG operator, no reference counterpart (the reference applies
+ * it element by element, solver.cc:904-1048): TL_SOLVER_ASSEMBLED assembles
+ * the 3x3 node blocks once per solve and iterates on that matrix (about 40
+ * bytes per nonzero block in FP32, 76 in FP64; for one body only when every
+ * node row fits one thread of the persistent grid, else element by
+ * element); TL_SOLVER_ELEMENTWISE always iterates element by element;
+ * TL_SOLVER_AUTO (default) is ASSEMBLED for batched systems and for single
+ * bodies of at least 32,768 tets, ELEMENTWISE for smaller single bodies.
+ * Both forms apply the same operator; they differ in rounding. */
 #define TL_SOLVER_AUTO 0u
 #define TL_SOLVER_ASSEMBLED 1u
 #define TL_SOLVER_ELEMENTWISE 2u

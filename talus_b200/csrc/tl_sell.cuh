@@ -117,11 +117,13 @@ __device__ __forceinline__ void addElementBlock(const Sys<S>& s, uint32_t e, uin
 // row is zero (its transpose, in a free row, is not).  Padding positions are
 // zero from the build and are never written.
 template <class S, int LAW, bool TANGENT, bool DAMP>
-__global__ void __launch_bounds__(TILE, 4) kSellAssemble(Sys<S> s, SellDev<S> g) {
+__global__ void __launch_bounds__(TILE, 4) kSellAssemble(Sys<S> s, SellDev<S> g, uint32_t pass) {
   const uint32_t i = blockIdx.x * TILE + threadIdx.x;
   if (i >= g.upper_count) return;
   const uint32_t pos = g.upper[i], mpos = g.mirror[i];
   const uint32_t row = g.group_slice[pos >> 5] * SELL_ROWS + (pos & 31u), col = g.col[pos];
+  const uint32_t body = s.node_tile_body[row / TILE];  // a block's two nodes share a body
+  if (!bodyActive(s, body, pass)) return;
   const bool rowFree = !s.anch[row], colFree = !s.anch[col];
   double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (rowFree || colFree) {
@@ -131,7 +133,7 @@ __global__ void __launch_bounds__(TILE, 4) kSellAssemble(Sys<S> s, SellDev<S> g)
       addElementBlock<S, LAW, TANGENT, DAMP>(s, code >> 4, (code >> 2) & 3u, code & 3u, acc);
     }
     if (row == col) {  // (1 - alpha_m) m I
-      const double m = s.step[0].inertia * double(ld4g(&s.rest4[row]).w);
+      const double m = s.step[body].inertia * double(ld4g(&s.rest4[row]).w);
       acc[0] += m;
       acc[4] += m;
       acc[8] += m;
@@ -172,9 +174,9 @@ __device__ __forceinline__ void sellSlot(const SellDev<S>& g, uint32_t p, uint32
 // y = A in for the thread's row.  Column slots are taken U at a time (4 in
 // FP32, 2 in FP64): their input values and block entries are requested
 // together; the FMAs run slot by slot in order.
-template <class S>
-__device__ __forceinline__ V3<double> sellRow(const SellDev<S>& g, uint32_t slice, uint32_t lane,
-                                              const Vec4<S>* in, const uint32_t* cols) {
+template <class S, class In>
+__device__ __forceinline__ V3<double> sellRowOf(const SellDev<S>& g, uint32_t slice, uint32_t lane, In in,
+                                                const uint32_t* cols) {
   constexpr uint32_t U = sizeof(S) == 4 ? 4u : 2u;
   V3<double> acc = {0, 0, 0};
   const uint32_t p1 = __ldg(&g.slice_start[slice + 1]);
@@ -185,12 +187,17 @@ __device__ __forceinline__ V3<double> sellRow(const SellDev<S>& g, uint32_t slic
     for (uint32_t i = 0; i < U; ++i) c[i] = sellCol(cols, g.col_cache, k + i, g.col, p + i * SELL_ROWS);
     Vec4<S> xin[U];
 #pragma unroll
-    for (uint32_t i = 0; i < U; ++i) xin[i] = ld4cg(&in[c[i]]);
+    for (uint32_t i = 0; i < U; ++i) xin[i] = in(c[i]);
 #pragma unroll
     for (uint32_t i = 0; i < U; ++i) sellSlot(g, p + i * SELL_ROWS, lane, xin[i], acc);
   }
-  for (; p < p1; p += SELL_ROWS, ++k) sellSlot(g, p, lane, ld4cg(&in[sellCol(cols, g.col_cache, k, g.col, p)]), acc);
+  for (; p < p1; p += SELL_ROWS, ++k) sellSlot(g, p, lane, in(sellCol(cols, g.col_cache, k, g.col, p)), acc);
   return acc;
+}
+template <class S>
+__device__ __forceinline__ V3<double> sellRow(const SellDev<S>& g, uint32_t slice, uint32_t lane,
+                                              const Vec4<S>* in, const uint32_t* cols) {
+  return sellRowOf(g, slice, lane, [in](uint32_t c) { return ld4cg(&in[c]); }, cols);
 }
 
 template <class S> __device__ __forceinline__ V3<double> roundTo(V3<double> v) {
@@ -370,6 +377,187 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
     rep.tangent_iterations += tangent ? taken : 0u;
     rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
     s.cgrep[0] = rep;
+  }
+}
+
+// Persistent PCG over every body of a batched system on the assembled block
+// matrix: kPcgBatch's per-body scalars, stopping tests and reports
+// (conjugateGradient, solver.cc:1904-2089, block-Jacobi branch), with the
+// element matvec and the node gather replaced by the rows of the matrix.
+// Per iteration, over node tiles:
+//   AB  p = z + beta p_prev and Ap = A p, each neighbour's p formed from its
+//       z and p_prev; p.Ap per body -> alpha (last tile of the body)
+//   C   x += alpha p, r -= alpha Ap, z = P r; r.z, r.r per body -> beta,
+//       stopping test
+// with a grid barrier after each.  AB reads the neighbours' previous p while
+// writing the new one, so p alternates between two buffers by iteration.
+template <class S>
+__global__ void __launch_bounds__(TILE, 2)
+    kPcgBatchSell(Sys<S> s, SellDev<S> g, Vec4<S>* X, Vec4<S>* p2, uint32_t pass, uint32_t x0zero, uint32_t tangent) {
+  const uint32_t G = gridDim.x, lane = threadIdx.x & 31u;
+  g.col_cache = 0;  // no per-launch column cache: a block walks many slices
+  const S zero = S(0);
+  unsigned int bar = 0;
+  Vec4<S>* const pbuf[2] = {s.p, p2};
+  // ---- init: r = right - A x (anchored rows 0), z = P r, p_prev = 0
+  for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
+    const uint32_t b = s.node_tile_body[tile];
+    if (!bodyActive(s, b, pass)) continue;
+    const BodyDev bd = s.body[b];
+    const uint32_t n = tile * TILE + threadIdx.x;
+    double sums[3] = {0.0, 0.0, 0.0};
+    if (n < bd.node_end) {
+      const Vec4<S> rhs = s.right[n];
+      V3<S> r = {zero, zero, zero};
+      if (!s.anch[n]) {
+        V3<double> ax = {0, 0, 0};
+        if (!x0zero) ax = sellRow(g, n >> 5, lane, X, nullptr);
+        r = cvt<S>(cvt<double>(xyz(rhs)) - ax);
+      }
+      const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
+      const Sym<S> P = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
+      const V3<S> z = symMul(P, r);
+      s.r[n] = pack(r);
+      s.z[n] = pack(z);
+      s.p[n] = Vec4<S>{zero, zero, zero, zero};
+      if (x0zero) X[n] = Vec4<S>{zero, zero, zero, zero};  // X is multiplied only when !x0zero
+      sums[0] = dot(cvt<double>(r), cvt<double>(z));
+      sums[1] = dot(cvt<double>(r), cvt<double>(r));
+      sums[2] = dot(cvt<double>(xyz(rhs)), cvt<double>(xyz(rhs)));
+    }
+    blockSum<3>(sums);
+    if (threadIdx.x == 0) {
+      s.part[size_t(tile) * 4 + 0] = sums[0];
+      s.part[size_t(tile) * 4 + 1] = sums[1];
+      s.part[size_t(tile) * 4 + 2] = sums[2];
+    }
+    if (lastTileOfBody(&s.counter[b], bd.node_tile_end - bd.node_tile_begin)) {
+      double tot[3];
+      sumTiles<3>(s.part, bd.node_tile_begin, bd.node_tile_end, tot);
+      if (threadIdx.x == 0) {
+        CgBodyDev c;
+        const double reference = sqrt(tot[2]);
+        c.floor = fmax(reference, 1.1754943508222875e-38);  // std::numeric_limits<float>::min()
+        c.target = s.step[b].tolerance * c.floor;
+        c.squared = tot[0];
+        c.length = tot[1];
+        c.start_res = sqrt(tot[1]) / c.floor;
+        c.rel_res = c.start_res;
+        c.blend = 0.0;
+        c.stride = 0.0;
+        c.taken = 0;
+        c.done = (s.step[b].limit == 0u || sqrt(c.length) <= c.target) ? 1u : 0u;
+        c.pad0 = c.pad1 = 0;
+        s.cg[b] = c;
+        __threadfence();
+        if (c.done) atomicSub(&s.sync->active, 1);
+      }
+    }
+  }
+  if (!countBarrier(s.sync, bar)) return;
+  for (uint32_t it = 0;; ++it) {
+    if (*(volatile int*)&s.sync->active <= 0) break;  // uniform: no block decrements between here and barrier AB
+    const Vec4<S>* pprev = pbuf[it & 1u];
+    Vec4<S>* pnew = pbuf[(it + 1u) & 1u];
+    // ---- AB
+    for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
+      const uint32_t b = s.node_tile_body[tile];
+      if (!bodyActive(s, b, pass) || __ldcg(&s.cg[b].done)) continue;
+      const BodyDev bd = s.body[b];
+      const uint32_t n = tile * TILE + threadIdx.x;
+      double sums[1] = {0.0};
+      if (n < bd.node_end) {
+        const S blend = S(__ldcg(&s.cg[b].blend));
+        const auto pOf = [&](uint32_t c) {
+          return pack(fmaV(blend, xyz(ld4cg(&pprev[c])), xyz(ld4cg(&s.z[c]))));
+        };
+        const V3<S> pn = xyz(pOf(n));
+        pnew[n] = pack(pn);
+        V3<S> apn = {zero, zero, zero};
+        if (!s.anch[n]) apn = cvt<S>(sellRowOf(g, n >> 5, lane, pOf, static_cast<const uint32_t*>(nullptr)));
+        s.ap[n] = pack(apn);
+        sums[0] = dot(cvt<double>(pn), cvt<double>(apn));
+      }
+      blockSum<1>(sums);
+      if (threadIdx.x == 0) s.part[size_t(tile) * 4 + 3] = sums[0];
+      if (lastTileOfBody(&s.counter[b], bd.node_tile_end - bd.node_tile_begin)) {
+        double tot[1];
+        sumTiles<1>(s.part + 3, bd.node_tile_begin, bd.node_tile_end, tot);
+        if (threadIdx.x == 0) {
+          const double curvature = tot[0];
+          const double squared = __ldcg(&s.cg[b].squared);
+          if (!(curvature > 0.0) || !(squared > 0.0)) {
+            s.cg[b].done = 1u;
+            __threadfence();
+            atomicSub(&s.sync->active, 1);
+          } else {
+            s.cg[b].stride = squared / curvature;
+            __threadfence();
+          }
+        }
+      }
+    }
+    if (!countBarrier(s.sync, bar)) return;
+    // ---- C
+    for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
+      const uint32_t b = s.node_tile_body[tile];
+      if (!bodyActive(s, b, pass) || __ldcg(&s.cg[b].done)) continue;
+      const BodyDev bd = s.body[b];
+      const uint32_t n = tile * TILE + threadIdx.x;
+      double sums[2] = {0.0, 0.0};
+      if (n < bd.node_end) {
+        const S stride = S(__ldcg(&s.cg[b].stride));
+        const V3<S> pn = xyz(ld4cg(&pnew[n]));
+        const V3<S> x = fmaV(stride, pn, xyz(ld4cg(&X[n])));
+        const V3<S> r = fmaV(-stride, xyz(ld4cg(&s.ap[n])), xyz(ld4cg(&s.r[n])));
+        const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
+        const Sym<S> P = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
+        const V3<S> z = symMul(P, r);
+        X[n] = pack(x);
+        s.r[n] = pack(r);
+        s.z[n] = pack(z);
+        sums[0] = dot(cvt<double>(r), cvt<double>(z));
+        sums[1] = dot(cvt<double>(r), cvt<double>(r));
+      }
+      blockSum<2>(sums);
+      if (threadIdx.x == 0) {
+        s.part[size_t(tile) * 4 + 0] = sums[0];
+        s.part[size_t(tile) * 4 + 1] = sums[1];
+      }
+      if (lastTileOfBody(&s.counter[b], bd.node_tile_end - bd.node_tile_begin)) {
+        double tot[2];
+        sumTiles<2>(s.part, bd.node_tile_begin, bd.node_tile_end, tot);
+        if (threadIdx.x == 0) {
+          CgBodyDev c = loadCg(&s.cg[b]);
+          c.blend = tot[0] / c.squared;
+          c.squared = tot[0];
+          c.length = tot[1];
+          c.taken += 1u;
+          c.done = (sqrt(c.length) <= c.target || c.taken >= s.step[b].limit) ? 1u : 0u;
+          s.cg[b] = c;
+          __threadfence();
+          if (c.done) atomicSub(&s.sync->active, 1);
+        }
+      }
+    }
+    if (!countBarrier(s.sync, bar)) return;
+  }
+  if (blockIdx.x == 0) {
+    for (uint32_t b = threadIdx.x; b < s.bodies; b += TILE) {
+      if (!bodyActive(s, b, pass)) continue;
+      CgBodyDev c = loadCg(&s.cg[b]);
+      const double residual = sqrt(c.length);
+      c.rel_res = residual / c.floor;
+      s.cg[b].rel_res = c.rel_res;
+      CgReportDev rep = s.cgrep[b];
+      rep.iterations += c.taken;
+      rep.capped += (c.taken == s.step[b].limit && residual > c.target) ? 1u : 0u;
+      rep.applications += c.taken + (x0zero ? 0u : 1u);
+      rep.solves += 1u;
+      rep.tangent_iterations += tangent ? c.taken : 0u;
+      rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
+      s.cgrep[b] = rep;
+    }
   }
 }
 

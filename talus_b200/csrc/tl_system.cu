@@ -294,7 +294,8 @@ struct System final : SystemBase {
   // assembled block matrix of the single-body PCG (tl_sell.cuh)
   bool sellReady = false;
   uint32_t sellRows = 0, sellSlices = 0, sellPositions = 0, sellStride = 0;
-  int sellPerSm = 0;
+  int sellPerSm = 0, batchSellPerSm = 0;
+  DevBuf<Vec4<S>> sellP2;  // kPcgBatchSell's second search-direction buffer
   DevBuf<uint32_t> sellSliceStart, sellGroupSlice, sellCol, sellCstart, sellCentry, sellUpper, sellMirror;
   uint32_t sellUpperCount = 0, sellColCache = 0;
   static constexpr uint32_t SELL_COL_CACHE_MAX = 32;  // column slots per thread in kPcgSell's shared memory
@@ -651,7 +652,7 @@ struct System final : SystemBase {
     sync.alloc(1);
     sync.zero(st);
     buildTiles(hTet, hElemTileBody);
-    if (B == 1) buildSell(hTet, hStart, hEntry);
+    buildSell(hTet, hStart, hEntry);
     TL_CUDA(cudaStreamSynchronize(st));
   }
 
@@ -662,8 +663,10 @@ struct System final : SystemBase {
   // ascending element order (the node incidence lists ascend).
   void buildSell(const std::vector<uint4>& hTet, const std::vector<uint32_t>& hStart,
                  const std::vector<uint32_t>& hEntry) {
-    const uint32_t rows = bodyHost[0].node_end;
-    if (bodyHost[0].elem_end >= (1u << 28)) return;  // contributor codes hold the element in 28 bits
+    // one body: its nodes; a batch: every node slot (tile padding rows have
+    // no elements and stay zero)
+    const uint32_t rows = B == 1 ? bodyHost[0].node_end : Vp;
+    if (Tp >= (1u << 28)) return;  // contributor codes hold the element in 28 bits
     const uint32_t slices = (rows + SELL_ROWS - 1) / SELL_ROWS;
     std::vector<uint32_t> nbStart(size_t(rows) + 1, 0), nb;
     nb.reserve(size_t(rows) * 16);
@@ -801,10 +804,28 @@ struct System final : SystemBase {
     TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sellPerSm, (const void*)kPcgSell<S>, TILE, sellColBytes()));
     // kPcgSell writes four partials per block into one of two halves
     if (size_t(8) * sellPerSm * ctx->sms > blkPart.count) blkPart.alloc(size_t(8) * sellPerSm * ctx->sms);
+    if (B > 1) {
+      sellP2.alloc(Vp);
+      sellP2.zero(st);
+      TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&batchSellPerSm, (const void*)kPcgBatchSell<S>, TILE, 0));
+    }
     TL_CUDA(cudaStreamSynchronize(st));
-    sellReady = sellPerSm > 0;
+    sellReady = B == 1 ? sellPerSm > 0 : batchSellPerSm > 0;
   }
   size_t sellColBytes() const { return size_t(sellColCache) * TILE * sizeof(uint32_t); }
+  void assembleSell(const Sys<S>& s, const SellDev<S>& g, unsigned blocks, int idx, bool damp, bool tangent,
+                    uint32_t pass) {
+    if (idx) {
+      if (tangent) kSellAssemble<S, 1, true, false><<<blocks, TILE, 0, st>>>(s, g, pass);
+      else kSellAssemble<S, 1, false, false><<<blocks, TILE, 0, st>>>(s, g, pass);
+    } else if (damp) {
+      if (tangent) kSellAssemble<S, 0, true, true><<<blocks, TILE, 0, st>>>(s, g, pass);
+      else kSellAssemble<S, 0, false, true><<<blocks, TILE, 0, st>>>(s, g, pass);
+    } else {
+      if (tangent) kSellAssemble<S, 0, true, false><<<blocks, TILE, 0, st>>>(s, g, pass);
+      else kSellAssemble<S, 0, false, false><<<blocks, TILE, 0, st>>>(s, g, pass);
+    }
+  }
   SellDev<S> sellView() {
     SellDev<S> g;
     g.upper_count = sellUpperCount;
@@ -1183,16 +1204,7 @@ struct System final : SystemBase {
       SellDev<S> g = sellView();
       const unsigned blocks = (sellUpperCount + TILE - 1) / TILE;
       if (profiling) mark(1, true);  // the operator assembly counts as assembly time
-      if (idx) {
-        if (tangent) kSellAssemble<S, 1, true, false><<<blocks, TILE, 0, st>>>(s, g);
-        else kSellAssemble<S, 1, false, false><<<blocks, TILE, 0, st>>>(s, g);
-      } else if (damp) {
-        if (tangent) kSellAssemble<S, 0, true, true><<<blocks, TILE, 0, st>>>(s, g);
-        else kSellAssemble<S, 0, false, true><<<blocks, TILE, 0, st>>>(s, g);
-      } else {
-        if (tangent) kSellAssemble<S, 0, true, false><<<blocks, TILE, 0, st>>>(s, g);
-        else kSellAssemble<S, 0, false, false><<<blocks, TILE, 0, st>>>(s, g);
-      }
+      assembleSell(s, g, blocks, idx, damp, tangent, ps);
       check();
       ++launches;
       if (profiling) {
@@ -1210,6 +1222,21 @@ struct System final : SystemBase {
       const int perSm = damp ? pcg1DampPerSm[tangent ? 1 : 0] : pcg1PerSm[idx][tangent ? 1 : 0];
       TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(gridOf(perSm)), dim3(TILE), args,
                                           sizeof(TileCache), st));
+    } else if (sellReady && solverForm != TL_SOLVER_ELEMENTWISE) {  // batch: assembled block matrix
+      SellDev<S> g = sellView();
+      const unsigned blocks = (sellUpperCount + TILE - 1) / TILE;
+      if (profiling) mark(1, true);
+      assembleSell(s, g, blocks, idx, damp, tangent, ps);
+      check();
+      ++launches;
+      if (profiling) {
+        mark(1, false);
+        mark(2, true);
+      }
+      Vec4<S>* p2 = sellP2.ptr;
+      void* args[] = {&s, &g, &X, &p2, &ps, &xz, &tg};
+      const int grid = std::max(1, std::min(batchSellPerSm * ctx->sms, int(nodeTiles)));
+      TL_CUDA(cudaLaunchCooperativeKernel((const void*)kPcgBatchSell<S>, dim3(grid), dim3(TILE), args, 0, st));
     } else {  // batch: two-level assembly, per-body scalars
       if (profiling) mark(2, true);
       void* args[] = {&s, &X, &ps, &xz};

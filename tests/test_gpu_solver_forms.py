@@ -77,6 +77,23 @@ def test_assembled_form_matches_the_oracle_on_the_plastic_block(precision, tol):
         assert [r["plastic_evaluations"] for r in greps] == [r["plastic_evaluations"] for r in oreps]
 
 
+def test_forms_agree_on_a_batch():
+    meshes, mats = tb.mesh.batch_bodies(count=5, seed=9, lo=3, hi=7)
+    out = []
+    for form in ("assembled", "elementwise"):
+        s = tb.System(meshes, mats, tb.FP64)
+        s.set_solver(form)
+        for i, m in enumerate(meshes):
+            s.set_state(tb.rest_state(m), i)
+        reps = [s.step(tb.Settings(), GRAVITY, DT) for _ in range(6)]
+        out.append(([s.get_state(i).position for i in range(len(meshes))],
+                    [[r.cg_iterations for r in rs] for rs in reps]))
+        s.close()
+    for i, m in enumerate(meshes):
+        assert relative_error(out[0][0][i], out[1][0][i], m.rest_positions) <= 1e-10, i
+    assert out[0][1] == out[1][1]
+
+
 def test_unknown_form_is_rejected():
     mesh, mat = elastic_block((3, 3, 3))
     s = tb.System(mesh, [mat], tb.FP64)
