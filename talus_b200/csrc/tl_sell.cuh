@@ -174,10 +174,9 @@ __device__ __forceinline__ void sellSlot(const SellDev<S>& g, uint32_t p, uint32
 // y = A in for the thread's row.  Column slots are taken U at a time (4 in
 // FP32, 2 in FP64): their input values and block entries are requested
 // together; the FMAs run slot by slot in order.
-template <class S, class In>
+template <class S, class In, uint32_t U = sizeof(S) == 4 ? 4u : 2u>
 __device__ __forceinline__ V3<double> sellRowOf(const SellDev<S>& g, uint32_t slice, uint32_t lane, In in,
                                                 const uint32_t* cols) {
-  constexpr uint32_t U = sizeof(S) == 4 ? 4u : 2u;
   V3<double> acc = {0, 0, 0};
   const uint32_t p1 = __ldg(&g.slice_start[slice + 1]);
   uint32_t p = __ldg(&g.slice_start[slice]) + lane, k = 0;
@@ -194,10 +193,16 @@ __device__ __forceinline__ V3<double> sellRowOf(const SellDev<S>& g, uint32_t sl
   for (; p < p1; p += SELL_ROWS, ++k) sellSlot(g, p, lane, in(sellCol(cols, g.col_cache, k, g.col, p)), acc);
   return acc;
 }
+// The matvec input read from a vector written during the launch (L2).
+template <class S> struct Ld4cg {
+  const Vec4<S>* v;
+  __device__ __forceinline__ Vec4<S> operator()(uint32_t c) const { return ld4cg(&v[c]); }
+};
+template <class S> __device__ __forceinline__ Ld4cg<S> ld4cgOf(const Vec4<S>* v) { return Ld4cg<S>{v}; }
 template <class S>
 __device__ __forceinline__ V3<double> sellRow(const SellDev<S>& g, uint32_t slice, uint32_t lane,
                                               const Vec4<S>* in, const uint32_t* cols) {
-  return sellRowOf(g, slice, lane, [in](uint32_t c) { return ld4cg(&in[c]); }, cols);
+  return sellRowOf(g, slice, lane, ld4cgOf(in), cols);
 }
 
 template <class S> __device__ __forceinline__ V3<double> roundTo(V3<double> v) {
@@ -392,7 +397,7 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
 // with a grid barrier after each.  AB reads the neighbours' previous p while
 // writing the new one, so p alternates between two buffers by iteration.
 template <class S>
-__global__ void __launch_bounds__(TILE, 2)
+__global__ void __launch_bounds__(TILE, 4)
     kPcgBatchSell(Sys<S> s, SellDev<S> g, Vec4<S>* X, Vec4<S>* p2, uint32_t pass, uint32_t x0zero, uint32_t tangent) {
   const uint32_t G = gridDim.x, lane = threadIdx.x & 31u;
   g.col_cache = 0;  // no per-launch column cache: a block walks many slices
@@ -411,7 +416,8 @@ __global__ void __launch_bounds__(TILE, 2)
       V3<S> r = {zero, zero, zero};
       if (!s.anch[n]) {
         V3<double> ax = {0, 0, 0};
-        if (!x0zero) ax = sellRow(g, n >> 5, lane, X, nullptr);
+        if (!x0zero)
+          ax = sellRowOf<S, decltype(ld4cgOf(X)), 2u>(g, n >> 5, lane, ld4cgOf(X), static_cast<const uint32_t*>(nullptr));
         r = cvt<S>(cvt<double>(xyz(rhs)) - ax);
       }
       const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
@@ -474,7 +480,8 @@ __global__ void __launch_bounds__(TILE, 2)
         const V3<S> pn = xyz(pOf(n));
         pnew[n] = pack(pn);
         V3<S> apn = {zero, zero, zero};
-        if (!s.anch[n]) apn = cvt<S>(sellRowOf(g, n >> 5, lane, pOf, static_cast<const uint32_t*>(nullptr)));
+        if (!s.anch[n])
+          apn = cvt<S>(sellRowOf<S, decltype(pOf), 2u>(g, n >> 5, lane, pOf, static_cast<const uint32_t*>(nullptr)));
         s.ap[n] = pack(apn);
         sums[0] = dot(cvt<double>(pn), cvt<double>(apn));
       }
