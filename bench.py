@@ -394,6 +394,7 @@ def run_ours(args, spec, rank, world, dist):
     system = tb.System(meshes, mats, precision, context)
     tune = tuning(args.workload, args.precision)
     if tune:
+        system.set_solver(tune.get("solver", "auto"))
         system.tune(tune["pcg_blocks_per_sm"], tune["graph"])
     for i, m in enumerate(meshes):
         system.set_state(tb.rest_state(m), i)
@@ -478,8 +479,9 @@ def run_ours(args, spec, rank, world, dist):
     s_bytes = 4 if precision == tb.FP32_MIXED else 8
     pcg_bytes = 0.0
     assembly = None
-    # the form TL_SOLVER_AUTO takes: assembled for a batch and for one body of >= 32,768 tets
-    assembled = B > 1 or meshes[0].tets >= SELL_AUTO_MIN_TETS
+    # the form the system took (TL_SOLVER_AUTO: assembled for a batch and for one body of >= 32,768 tets)
+    form = tune.get("solver", "auto") if tune else "auto"
+    assembled = form != "elementwise" and (B > 1 or form == "assembled" or meshes[0].tets >= SELL_AUTO_MIN_TETS)
     for b, m in enumerate(meshes):
         it, tan = per_body[b, 0], per_body[b, 1]
         if assembled:  # assembled operator (tl_sell.cuh)
@@ -524,7 +526,8 @@ def run_ours(args, spec, rank, world, dist):
     if not spec.get("batch"):
         config["cells"] = list(spec["cells"])
     if tune:
-        config["tuning"] = {"pcg_blocks_per_sm": tune["pcg_blocks_per_sm"], "graph": tune["graph"],
+        config["tuning"] = {"solver": tune.get("solver", "auto"), "pcg_blocks_per_sm": tune["pcg_blocks_per_sm"],
+                            "graph": tune["graph"],
                             "source": "talus_b200/tuning.json (talus_b200.autotune)"}
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -604,6 +607,7 @@ def run_fp64(meshes, mats, settings, args, flush, context):
     system = tb.System(meshes, mats, tb.FP64, context)
     tune = tuning(args.workload, "fp64")
     if tune:
+        system.set_solver(tune.get("solver", "auto"))
         system.tune(tune["pcg_blocks_per_sm"], tune["graph"])
     for i, m in enumerate(meshes):
         system.set_state(tb.rest_state(m), i)

@@ -10,6 +10,10 @@ through ``System.tune``:
   element-tile matvec.
 * ``graph``: whether a batched elastic step is replayed from one captured CUDA
   graph (device-side substep choice) or launched kernel by kernel.
+* ``solver``: the PCG operator form (``System.set_solver``): "auto" (the
+  block matrix assembled once per solve, for these workloads) or
+  "elementwise".  The block cap applies to the element-by-element kernels;
+  the assembled ones take their own occupancy, so they are timed at 0.
 
 Every candidate starts from the same rest state and runs the same steps, so
 the candidates do the same physics; the score is device seconds per step.
@@ -27,14 +31,15 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def candidates(bodies: int):
-    shapes = [0, 1, 2, 3]
     graphs = [True, False] if bodies > 1 else [False]
-    return [(k, g) for k in shapes for g in graphs]
+    out = [("elementwise", k, g) for k in (0, 1, 2, 3) for g in graphs]
+    return out + [("auto", 0, g) for g in graphs]
 
 
-def time_candidate(system, meshes, settings, blocks, graph, warmup, steps):
+def time_candidate(system, meshes, settings, solver, blocks, graph, warmup, steps):
     import talus_b200 as tb
 
+    system.set_solver(solver)
     system.tune(blocks, graph)
     for i, m in enumerate(meshes):
         system.set_state(tb.rest_state(m), i)
@@ -60,14 +65,14 @@ def tune(workload: str, precision_name: str, warmup: int = 2, steps: int = 4) ->
     settings = tb.Settings(law=law)
     system = tb.System(meshes, mats, precision)
     results = []
-    for blocks, graph in candidates(len(meshes)):
-        sec, its = time_candidate(system, meshes, settings, blocks, graph, warmup, steps)
-        results.append({"pcg_blocks_per_sm": blocks, "graph": graph, "ms_per_step": sec * 1e3,
+    for solver, blocks, graph in candidates(len(meshes)):
+        sec, its = time_candidate(system, meshes, settings, solver, blocks, graph, warmup, steps)
+        results.append({"solver": solver, "pcg_blocks_per_sm": blocks, "graph": graph, "ms_per_step": sec * 1e3,
                         "cg_iterations_per_step": its})
         print(json.dumps(results[-1]), file=sys.stderr, flush=True)
     system.close()
     best = min(results, key=lambda r: r["ms_per_step"])
-    return {"pcg_blocks_per_sm": best["pcg_blocks_per_sm"], "graph": best["graph"],
+    return {"solver": best["solver"], "pcg_blocks_per_sm": best["pcg_blocks_per_sm"], "graph": best["graph"],
             "ms_per_step": best["ms_per_step"], "steps": steps, "candidates": results}
 
 
