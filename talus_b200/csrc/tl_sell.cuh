@@ -32,10 +32,10 @@
 #pragma once
 
 #include "tl_kernels.cuh"
+#include "tl_sell_build.h"
 
 namespace tl {
 
-constexpr uint32_t SELL_ROWS = 32;   // rows per slice
 constexpr uint32_t SELL_SLICES_PER_BLOCK = TILE / SELL_ROWS;
 
 template <class S> struct SellDev {

@@ -8,6 +8,7 @@
 #include "tl_kernels.cuh"
 #include "tl_adjoint.cuh"
 #include "tl_sell.cuh"
+#include "tl_sell_build.h"
 
 #include <algorithm>
 #include <condition_variable>
@@ -656,125 +657,24 @@ struct System final : SystemBase {
     TL_CUDA(cudaStreamSynchronize(st));
   }
 
-  // Sliced-ELL block structure of the single body's operator (tl_sell.cuh):
-  // each node row's neighbours (the nodes of its elements, ascending), slices
-  // of 32 rows padded to their widest row, and for every block position the
-  // (element, row corner, column corner) triples that add to it, in
-  // ascending element order (the node incidence lists ascend).
+  // Sliced-ELL block structure of the operator (tl_sell.cuh), built on the
+  // host by buildSellHost (tl_sell_build.h).
   void buildSell(const std::vector<uint4>& hTet, const std::vector<uint32_t>& hStart,
                  const std::vector<uint32_t>& hEntry) {
     // one body: its nodes; a batch: every node slot (tile padding rows have
     // no elements and stay zero)
     const uint32_t rows = B == 1 ? bodyHost[0].node_end : Vp;
     if (Tp >= (1u << 28)) return;  // contributor codes hold the element in 28 bits
-    const uint32_t slices = (rows + SELL_ROWS - 1) / SELL_ROWS;
-    std::vector<uint32_t> nbStart(size_t(rows) + 1, 0), nb;
-    nb.reserve(size_t(rows) * 16);
-    std::vector<uint32_t> tmp;
-    for (uint32_t r = 0; r < rows; ++r) {
-      tmp.clear();
-      for (uint32_t k = hStart[r]; k < hStart[r + 1]; ++k) {
-        const uint4 t = hTet[hEntry[k] >> 2];
-        tmp.insert(tmp.end(), {t.x, t.y, t.z, t.w});
-      }
-      if (tmp.empty()) tmp.push_back(r);
-      std::sort(tmp.begin(), tmp.end());
-      tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
-      nb.insert(nb.end(), tmp.begin(), tmp.end());
-      nbStart[r + 1] = uint32_t(nb.size());
-    }
-    std::vector<uint32_t> sliceStart(size_t(slices) + 1, 0);
-    for (uint32_t sl = 0; sl < slices; ++sl) {
-      uint32_t width = 1;
-      for (uint32_t r = sl * SELL_ROWS; r < std::min(rows, (sl + 1) * SELL_ROWS); ++r)
-        width = std::max(width, nbStart[r + 1] - nbStart[r]);
-      sliceStart[sl + 1] = sliceStart[sl] + width * SELL_ROWS;
-    }
-    const uint32_t positions = sliceStart[slices];
-    // contributors of (row, slot), ascending element: per row, codes keyed by slot
-    std::vector<uint32_t> slotStart(nb.size() + rows + 1, 0), codes;  // per row: slots + 1 offsets
-    std::vector<uint32_t> rowSlotBase(size_t(rows) + 1, 0);
-    codes.reserve(size_t(16) * tets);
-    std::vector<std::pair<uint32_t, uint32_t>> pairs;
-    for (uint32_t r = 0; r < rows; ++r) {
-      const uint32_t* nr = nb.data() + nbStart[r];
-      const uint32_t len = nbStart[r + 1] - nbStart[r];
-      pairs.clear();
-      for (uint32_t k = hStart[r]; k < hStart[r + 1]; ++k) {
-        const uint32_t e = hEntry[k] >> 2, a = hEntry[k] & 3u;
-        const uint32_t q[4] = {hTet[e].x, hTet[e].y, hTet[e].z, hTet[e].w};
-        for (uint32_t b = 0; b < 4; ++b) {
-          const uint32_t slot = uint32_t(std::lower_bound(nr, nr + len, q[b]) - nr);
-          pairs.emplace_back(slot, (e << 4) | (a << 2) | b);
-        }
-      }
-      std::stable_sort(pairs.begin(), pairs.end(),
-                       [](const std::pair<uint32_t, uint32_t>& x, const std::pair<uint32_t, uint32_t>& y) {
-                         return x.first < y.first;
-                       });
-      const uint32_t base = nbStart[r] + r;  // this row's len + 1 offsets
-      rowSlotBase[r] = base;
-      size_t j = 0;
-      for (uint32_t k = 0; k <= len; ++k) {
-        slotStart[base + k] = uint32_t(codes.size());
-        while (k < len && j < pairs.size() && pairs[j].first == k) codes.push_back(pairs[j++].second);
-      }
-    }
-    std::vector<uint32_t> col(positions, 0), cstart(size_t(positions) + 1, 0), centry;
-    std::vector<uint32_t> groupSlice(positions / SELL_ROWS);
-    centry.reserve(codes.size());
-    for (uint32_t sl = 0; sl < slices; ++sl) {
-      const uint32_t width = (sliceStart[sl + 1] - sliceStart[sl]) / SELL_ROWS;
-      for (uint32_t k = 0; k < width; ++k) {
-        groupSlice[(sliceStart[sl] + k * SELL_ROWS) / SELL_ROWS] = sl;
-        for (uint32_t lane = 0; lane < SELL_ROWS; ++lane) {
-          const uint32_t pos = sliceStart[sl] + k * SELL_ROWS + lane, r = sl * SELL_ROWS + lane;
-          cstart[pos] = uint32_t(centry.size());
-          if (r >= rows) continue;  // padding row: column 0, zero block
-          const uint32_t len = nbStart[r + 1] - nbStart[r];
-          if (k >= len) {
-            col[pos] = r;  // padding slot: own column, zero block
-            continue;
-          }
-          col[pos] = nb[nbStart[r] + k];
-          const uint32_t* ss = slotStart.data() + rowSlotBase[r];
-          centry.insert(centry.end(), codes.begin() + ss[k], codes.begin() + ss[k + 1]);
-        }
-      }
-    }
-    cstart[positions] = uint32_t(centry.size());
-    // blocks on or above the diagonal and the positions of their transposes
-    std::vector<uint32_t> upper, mirror;
-    uint32_t widest = 1;
-    for (uint32_t sl = 0; sl < slices; ++sl) {
-      const uint32_t width = (sliceStart[sl + 1] - sliceStart[sl]) / SELL_ROWS;
-      widest = std::max(widest, width);
-      for (uint32_t k = 0; k < width; ++k)
-        for (uint32_t lane = 0; lane < SELL_ROWS; ++lane) {
-          const uint32_t pos = sliceStart[sl] + k * SELL_ROWS + lane, r = sl * SELL_ROWS + lane;
-          if (r >= rows || k >= nbStart[r + 1] - nbStart[r]) continue;
-          const uint32_t c = col[pos];
-          if (c < r) continue;
-          const uint32_t *nc = nb.data() + nbStart[c], *ncEnd = nb.data() + nbStart[c + 1];
-          const uint32_t kc = uint32_t(std::lower_bound(nc, ncEnd, r) - nc);
-          upper.push_back(pos);
-          mirror.push_back(sliceStart[c / SELL_ROWS] + kc * SELL_ROWS + c % SELL_ROWS);
-        }
-    }
-    {  // longest contributor lists first, so warps take similar loop counts
-      std::vector<uint32_t> order(upper.size());
-      for (uint32_t i = 0; i < order.size(); ++i) order[i] = i;
-      std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
-        return cstart[upper[x] + 1] - cstart[upper[x]] > cstart[upper[y] + 1] - cstart[upper[y]];
-      });
-      std::vector<uint32_t> u2(upper.size()), m2(upper.size());
-      for (uint32_t i = 0; i < order.size(); ++i) {
-        u2[i] = upper[order[i]];
-        m2[i] = mirror[order[i]];
-      }
-      upper.swap(u2);
-      mirror.swap(m2);
-    }
+    static_assert(sizeof(uint4) == 4 * sizeof(uint32_t), "tets are four node ids");
+    SellHost h = buildSellHost(rows, reinterpret_cast<const uint32_t*>(hTet.data()), hStart, hEntry);
+    const uint32_t slices = h.slices, positions = h.positions, widest = h.widest;
+    std::vector<uint32_t>& sliceStart = h.sliceStart;
+    std::vector<uint32_t>& groupSlice = h.groupSlice;
+    std::vector<uint32_t>& col = h.col;
+    std::vector<uint32_t>& cstart = h.cstart;
+    std::vector<uint32_t>& centry = h.centry;
+    std::vector<uint32_t>& upper = h.upper;
+    std::vector<uint32_t>& mirror = h.mirror;
     sellUpperCount = uint32_t(upper.size());
     sellColCache = std::min(widest, SELL_COL_CACHE_MAX);
     sellUpper.alloc(std::max<size_t>(upper.size(), 1));
