@@ -24,6 +24,8 @@
 #include <thread>
 #include <vector>
 
+#include <unistd.h>
+
 using namespace tl;
 
 namespace {
@@ -112,16 +114,19 @@ constexpr double PLASTIC_REDUCTION = 1.0e-2;  // solver.cc:374
 constexpr double PLASTIC_RESOLUTION = 8.0;    // solver.cc:380
 
 // Worker threads for the host side of state transfers, started on first use
-// and kept for the life of the process (up to 15 workers beside the calling
-// thread).  One job at a time: a job is a range split into contiguous parts,
-// part 0 run by the caller.
+// and kept until the process exits (up to 15 workers beside the calling
+// thread; the pool is never destroyed, so no worker is joined at exit).  One
+// job at a time: a job is a range split into contiguous parts, part 0 run by
+// the caller.
 class HostPool {
  public:
   static HostPool& instance() {
-    static HostPool pool;
-    return pool;
+    static HostPool* pool = new HostPool();
+    return *pool;
   }
-  size_t workers() const { return threads_.size(); }
+  // Workers usable from this process: none in a child forked after the pool
+  // started (its threads were not copied).
+  size_t workers() const { return getpid() == owner_ ? threads_.size() : 0; }
   // Runs body(part) for part in [0, parts), parts <= workers() + 1.
   void run(size_t parts, const std::function<void(size_t)>& body) {
     std::lock_guard<std::mutex> call(callMutex_);
@@ -139,17 +144,9 @@ class HostPool {
     done_.wait(lk, [&] { return pending_ == 0; });
     job_ = nullptr;
   }
-  ~HostPool() {
-    {
-      std::lock_guard<std::mutex> lk(m_);
-      stop_ = true;
-    }
-    cv_.notify_all();
-    for (std::thread& t : threads_) t.join();
-  }
 
  private:
-  HostPool() {
+  HostPool() : owner_(getpid()) {
     const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
     for (unsigned i = 1; i < hw; ++i) threads_.emplace_back([this] { loop(); });
   }
@@ -157,8 +154,7 @@ class HostPool {
     uint64_t seen = 0;
     for (;;) {
       std::unique_lock<std::mutex> lk(m_);
-      cv_.wait(lk, [&] { return stop_ || (generation_ != seen && next_ < parts_); });
-      if (stop_) return;
+      cv_.wait(lk, [&] { return generation_ != seen && next_ < parts_; });
       seen = generation_;
       while (next_ < parts_) {
         const size_t part = next_++;
@@ -176,7 +172,7 @@ class HostPool {
   const std::function<void(size_t)>* job_ = nullptr;
   size_t parts_ = 0, next_ = 0, pending_ = 0;
   uint64_t generation_ = 0;
-  bool stop_ = false;
+  pid_t owner_;
 };
 
 // Host loops over [0, n) split across the pool (state conversion of large
