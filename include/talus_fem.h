@@ -165,9 +165,8 @@ int32_t tl_system_tune(tl_system* system, uint32_t pcg_blocks_per_sm, uint32_t g
 /* Form of the PCG operator, no reference counterpart (the reference applies
  * it element by element, solver.cc:904-1048): TL_SOLVER_ASSEMBLED assembles
  * the 3x3 node blocks once per solve and iterates on that matrix (about 40
- * bytes per nonzero block in FP32, 76 in FP64; for one body only when every
- * node row fits one thread of the persistent grid, else element by
- * element); TL_SOLVER_ELEMENTWISE always iterates element by element;
+ * bytes per nonzero block in FP32, 76 in FP64);
+ * TL_SOLVER_ELEMENTWISE always iterates element by element;
  * TL_SOLVER_AUTO (default) is ASSEMBLED for batched systems and for single
  * bodies of at least 32,768 tets, ELEMENTWISE for smaller single bodies.
  * Both forms apply the same operator; they differ in rounding. */

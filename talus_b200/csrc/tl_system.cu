@@ -700,13 +700,12 @@ struct System final : SystemBase {
     TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sellPerSm, (const void*)kPcgSell<S>, TILE, sellColBytes()));
     // kPcgSell writes four partials per block into one of two halves
     if (size_t(8) * sellPerSm * ctx->sms > blkPart.count) blkPart.alloc(size_t(8) * sellPerSm * ctx->sms);
-    if (B > 1) {
-      sellP2.alloc(Vp);
-      sellP2.zero(st);
-      TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&batchSellPerSm, (const void*)kPcgBatchSell<S>, TILE, 0));
-    }
+    // kPcgBatchSell: every batch, and single bodies whose rows exceed one per thread of kPcgSell's grid
+    sellP2.alloc(Vp);
+    sellP2.zero(st);
+    TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&batchSellPerSm, (const void*)kPcgBatchSell<S>, TILE, 0));
     TL_CUDA(cudaStreamSynchronize(st));
-    sellReady = B == 1 ? sellPerSm > 0 : batchSellPerSm > 0;
+    sellReady = sellPerSm > 0 || batchSellPerSm > 0;
   }
   size_t sellColBytes() const { return size_t(sellColCache) * TILE * sizeof(uint32_t); }
   void assembleSell(const Sys<S>& s, const SellDev<S>& g, unsigned blocks, int idx, bool damp, bool tangent,
@@ -744,12 +743,16 @@ struct System final : SystemBase {
   // Grid of kPcgSell: the occupancy (capped by tl_system_tune while every
   // block still has at most one slice per warp), or 0 when the rows do not
   // fit one per thread.
+  // Whether this system's PCG runs on the assembled matrix.  TL_SOLVER_AUTO
+  // assembles batches, and single bodies large enough for the per-solve
+  // assembly to pay (measured on a B200: element-by-element 17% faster at
+  // 3,072 tets, even at 24,576, assembled 1.6x faster at 393,216).
+  bool assembledForm() const {
+    if (!sellReady || solverForm == TL_SOLVER_ELEMENTWISE) return false;
+    return B > 1 || solverForm == TL_SOLVER_ASSEMBLED || bodyHost[0].elem_end >= SELL_AUTO_MIN_TETS;
+  }
   int sellGrid() const {
-    if (!sellReady || solverForm == TL_SOLVER_ELEMENTWISE) return 0;
-    // TL_SOLVER_AUTO assembles only bodies large enough for the per-solve
-    // assembly to pay (measured on a B200: element-by-element 17% faster at
-    // 3,072 tets, even at 24,576, assembled 1.6x faster at 393,216)
-    if (solverForm == TL_SOLVER_AUTO && bodyHost[0].elem_end < SELL_AUTO_MIN_TETS) return 0;
+    if (B != 1 || sellPerSm < 1 || !assembledForm()) return 0;
     const int full = std::min<int>(sellPerSm * ctx->sms, int(sellSlices));
     const int capped = tuneBlocksPerSm ? std::min<int>(std::min<int>(sellPerSm, int(tuneBlocksPerSm)) * ctx->sms,
                                                        int(sellSlices))
@@ -1095,7 +1098,7 @@ struct System final : SystemBase {
     const size_t dyn = idx ? (tangent ? pipeBytes<S, 1, true>() : pipeBytes<S, 1, false>())
                            : (tangent ? pipeBytes<S, 0, true>() : pipeBytes<S, 0, false>());
     const bool damp = hasDamping && idx == 0;
-    const int sellG = B == 1 ? sellGrid() : 0;
+    const int sellG = sellGrid();
     if (sellG > 0) {  // single body: assembled block matrix, pipelined PCG
       SellDev<S> g = sellView();
       const unsigned blocks = (sellUpperCount + TILE - 1) / TILE;
@@ -1109,7 +1112,7 @@ struct System final : SystemBase {
       }
       void* args[] = {&s, &g, &X, &xz, &tg};
       TL_CUDA(cudaLaunchCooperativeKernel((const void*)kPcgSell<S>, dim3(sellG), dim3(TILE), args, sellColBytes(), st));
-    } else if (B == 1) {  // single body: two-level assembly, per-block partials
+    } else if (B == 1) {  // single body, element by element: two-level assembly, per-block partials
       if (profiling) mark(2, true);
       void* args[] = {&s, &X, &xz};
       const void* fn = idx ? (tangent ? (const void*)kPcg1<S, 1, true> : (const void*)kPcg1<S, 1, false>)
@@ -1118,7 +1121,7 @@ struct System final : SystemBase {
       const int perSm = damp ? pcg1DampPerSm[tangent ? 1 : 0] : pcg1PerSm[idx][tangent ? 1 : 0];
       TL_CUDA(cudaLaunchCooperativeKernel(fn, dim3(gridOf(perSm)), dim3(TILE), args,
                                           sizeof(TileCache), st));
-    } else if (sellReady && solverForm != TL_SOLVER_ELEMENTWISE) {  // batch: assembled block matrix
+    } else if (assembledForm() && batchSellPerSm > 0) {  // batch, or a body too large for kPcgSell
       SellDev<S> g = sellView();
       const unsigned blocks = (sellUpperCount + TILE - 1) / TILE;
       if (profiling) mark(1, true);

@@ -101,3 +101,16 @@ def test_unknown_form_is_rejected():
         tb._capi.check(tb._capi.lib().tl_system_set_solver(s.handle, 3), s.context.handle)
     assert e.value.status == tb._capi.TL_ERR_ARG
     s.close()
+
+
+def test_forms_agree_on_a_body_too_large_for_one_row_per_thread():
+    """A body with more node rows than the single-body assembled PCG has
+    threads (91,908 nodes) runs the assembled operator through the batched
+    kernel; it agrees with the element-by-element form."""
+    mesh = tb.box_mesh((68, 36, 35), voxel=0.1)
+    assert mesh.nodes > 2 * 148 * 256
+    mat = tb.PhysicalMaterial(density=1000.0, youngs_modulus=1e6, poissons_ratio=0.3)
+    xa, ra = run("assembled", tb.FP64, mesh, mat, tb.Settings(), 3)
+    xe, re = run("elementwise", tb.FP64, mesh, mat, tb.Settings(), 3)
+    assert relative_error(xa, xe, mesh.rest_positions) <= 1e-10
+    assert [r["cg_iterations"] for r in ra] == [r["cg_iterations"] for r in re]
