@@ -159,6 +159,8 @@ template <class S> struct Sys {
   const double* eyoung;   // per-element E override or null
   S* op;                  // 9 planes: committed R (corotated) or F (SNH)
   OpRec<S>* orec;         // [Tp] per-element matvec operator records
+  S* sell_val;                  // assembled operator's blocks (tl_sell.cuh) or null
+  const uint32_t* sell_diag;    // [rows] position of each node row's diagonal block, or null
   Vec4<S>* onorm;         // [2 Tp] rotated flow normal pairs (corotated consistent tangent)
   Vec4<S>* plast;         // 2 planes: (exx, eyy, ezz, exy), (exz, eyz, equivalent, -)
   Vec4<S>* fe;            // [4][Tp] corner planes: (fx, fy, fz, Dxx)
@@ -782,6 +784,11 @@ __global__ void __launch_bounds__(TILE) kNodeAssemble(Sys<S> s, const Vec4<S>* t
     }
     const Vec4<S> rest = ld4g(&s.rest4[n]);
     if (s.anch[n]) {
+      if (s.sell_diag) {  // anchored rows of the assembled operator are zero
+        S* v = s.sell_val + size_t(s.sell_diag[n] >> 5) * 9 * 32 + (s.sell_diag[n] & 31u);
+#pragma unroll
+        for (int c = 0; c < 9; ++c) v[c * 32] = S(0);
+      }
       s.v[n] = s.pres[n];
       s.a[n] = Vec4<S>{0, 0, 0, 0};
       s.right[n] = Vec4<S>{0, 0, 0, 0};
@@ -797,6 +804,12 @@ __global__ void __launch_bounds__(TILE) kNodeAssemble(Sys<S> s, const Vec4<S>* t
       rr = dot(rhs, rhs);
       const S im = S(st.inertia * mass);
       const S xx = d[0] + im, yy = d[1] + im, zz = d[2] + im, xy = d[3], xz = d[4], yz = d[5];
+      if (s.sell_diag) {  // the assembled operator's diagonal block is this one
+        S* v = s.sell_val + size_t(s.sell_diag[n] >> 5) * 9 * 32 + (s.sell_diag[n] & 31u);
+        const S m[9] = {xx, xy, xz, xy, yy, yz, xz, yz, zz};
+#pragma unroll
+        for (int c = 0; c < 9; ++c) v[c * 32] = m[c];
+      }
       // inverse of the symmetric block, identity unless det > 0
       const S cxx = yy * zz - yz * yz, cxy = xz * yz - xy * zz, cxz = xy * yz - xz * yy;
       const S det = xx * cxx + xy * cxy + xz * cxz;

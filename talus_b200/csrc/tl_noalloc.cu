@@ -215,6 +215,8 @@ Sys<S> viewOf(const Layout& l, uint32_t Vp, uint32_t Tp) {
   s.eyoung = nullptr;
   s.op = l.op;
   s.orec = l.orec;
+  s.sell_val = nullptr;
+  s.sell_diag = nullptr;
   s.onorm = l.onorm;
   s.plast = l.plast;
   s.fe = l.fe;

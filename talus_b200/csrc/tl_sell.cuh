@@ -9,7 +9,7 @@
 // (1 - alpha_m) m I on the diagonal, solver.cc:904-1048) and runs the solve
 // on that matrix:
 //
-//   kSellAssemble  one thread per block on or above the diagonal: the sum,
+//   kSellAssemble  one thread per block above the diagonal: the sum,
 //                  in ascending element order, of the element blocks that
 //                  land there (FP64 accumulation, stored in S), written with
 //                  its transpose below the diagonal;
@@ -111,11 +111,14 @@ __device__ __forceinline__ void addElementBlock(const Sys<S>& s, uint32_t e, uin
   }
 }
 
-// One thread per block (r, c) with r <= c: the sum over its contributors
+// One thread per block (r, c) with r < c: the sum over its contributors
 // (ascending element) is block (r, c), and its transpose is block (c, r),
 // since every element block satisfies B_ab = B_ba^T.  A block in an anchored
-// row is zero (its transpose, in a free row, is not).  Padding positions are
-// zero from the build and are never written.
+// row is zero (its transpose, in a free row, is not).  Diagonal blocks are
+// written by kNodeAssemble, whose diagonal block of a node (the sum of the
+// element pass's corner blocks plus (1 - alpha_m) m I, before its inversion
+// into the preconditioner) is this operator's.  Padding positions are zero
+// from the build and are never written.
 template <class S, int LAW, bool TANGENT, bool DAMP>
 __global__ void __launch_bounds__(TILE, 4) kSellAssemble(Sys<S> s, SellDev<S> g, uint32_t pass) {
   const uint32_t i = blockIdx.x * TILE + threadIdx.x;
@@ -131,12 +134,6 @@ __global__ void __launch_bounds__(TILE, 4) kSellAssemble(Sys<S> s, SellDev<S> g,
     for (uint32_t q = g.cstart[pos]; q < q1; ++q) {
       const uint32_t code = __ldg(&g.centry[q]);
       addElementBlock<S, LAW, TANGENT, DAMP>(s, code >> 4, (code >> 2) & 3u, code & 3u, acc);
-    }
-    if (row == col) {  // (1 - alpha_m) m I
-      const double m = s.step[body].inertia * double(ld4g(&s.rest4[row]).w);
-      acc[0] += m;
-      acc[4] += m;
-      acc[8] += m;
     }
   }
   S* v = g.val + size_t(pos >> 5) * 9 * SELL_ROWS + (pos & 31u);

@@ -20,8 +20,9 @@ struct SellHost {
   std::vector<uint32_t> col;         // [positions] column node (padding: own row, or 0 past the rows)
   std::vector<uint32_t> cstart;      // [positions + 1] contributor range of each position
   std::vector<uint32_t> centry;      // (element << 4) | (row corner << 2) | column corner, ascending element
-  std::vector<uint32_t> upper;       // block positions with row <= column, longest contributor lists first
+  std::vector<uint32_t> upper;       // block positions with row < column, longest contributor lists first
   std::vector<uint32_t> mirror;      // position of each upper block's transpose
+  std::vector<uint32_t> diag;        // [rows] position of each row's diagonal block
 };
 
 // rows: node rows [0, rows); tets4: 4 node ids per element; incStart /
@@ -119,7 +120,9 @@ inline SellHost buildSellHost(uint32_t rows, const uint32_t* tets4, const std::v
     }
   }
   h.cstart[positions] = uint32_t(h.centry.size());
-  // blocks on or above the diagonal and the positions of their transposes
+  // blocks above the diagonal and the positions of their transposes; the
+  // diagonal positions (their blocks are the node assembly's diagonal blocks)
+  h.diag.assign(rows, 0);
   for (uint32_t sl = 0; sl < slices; ++sl) {
     const uint32_t width = (h.sliceStart[sl + 1] - h.sliceStart[sl]) / SELL_ROWS;
     for (uint32_t k = 0; k < width; ++k)
@@ -127,7 +130,8 @@ inline SellHost buildSellHost(uint32_t rows, const uint32_t* tets4, const std::v
         const uint32_t pos = h.sliceStart[sl] + k * SELL_ROWS + lane, r = sl * SELL_ROWS + lane;
         if (r >= rows || k >= nbStart[r + 1] - nbStart[r]) continue;
         const uint32_t c = h.col[pos];
-        if (c < r) continue;
+        if (c == r) h.diag[r] = pos;
+        if (c <= r) continue;
         const uint32_t *nc = nb.data() + nbStart[c], *ncEnd = nb.data() + nbStart[c + 1];
         const uint32_t kc = uint32_t(std::lower_bound(nc, ncEnd, r) - nc);
         h.upper.push_back(pos);

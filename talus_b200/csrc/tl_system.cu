@@ -293,7 +293,7 @@ struct System final : SystemBase {
   uint32_t sellRows = 0, sellSlices = 0, sellPositions = 0, sellStride = 0;
   int sellPerSm = 0, batchSellPerSm = 0;
   DevBuf<Vec4<S>> sellP2;  // kPcgBatchSell's second search-direction buffer
-  DevBuf<uint32_t> sellSliceStart, sellGroupSlice, sellCol, sellCstart, sellCentry, sellUpper, sellMirror;
+  DevBuf<uint32_t> sellSliceStart, sellGroupSlice, sellCol, sellCstart, sellCentry, sellUpper, sellMirror, sellDiag;
   uint32_t sellUpperCount = 0, sellColCache = 0;
   static constexpr uint32_t SELL_COL_CACHE_MAX = 32;  // column slots per thread in kPcgSell's shared memory
   static constexpr uint32_t SELL_AUTO_MIN_TETS = 32768;  // TL_SOLVER_AUTO: smallest body that is assembled
@@ -411,6 +411,8 @@ struct System final : SystemBase {
     s.eyoung = hasEyoung ? eyoung.ptr : nullptr;
     s.op = op.ptr;
     s.orec = orec.ptr;
+    s.sell_val = sellReady ? sellVal.ptr : nullptr;
+    s.sell_diag = sellReady ? sellDiag.ptr : nullptr;
     s.onorm = onorm.ptr;
     s.tile_meta = tileMeta.ptr;
     s.tile_off = tileOff.ptr;
@@ -677,6 +679,8 @@ struct System final : SystemBase {
     sellUpper.upload(upper.data(), upper.size(), st);
     sellMirror.alloc(std::max<size_t>(mirror.size(), 1));
     sellMirror.upload(mirror.data(), mirror.size(), st);
+    sellDiag.alloc(std::max<size_t>(h.diag.size(), 1));
+    sellDiag.upload(h.diag.data(), h.diag.size(), st);
     sellRows = rows;
     sellSlices = slices;
     sellPositions = positions;

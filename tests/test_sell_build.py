@@ -2,9 +2,11 @@
 (talus_b200/csrc/tl_sell_build.h), compiled with g++ and checked on the CPU.
 
 A small driver restates on the host what the device does with the structure:
-the symmetric assembly of kSellAssemble (each block on or above the diagonal
-summed from its contributors, its transpose written at the mirror position)
-and the row matvec of kPcgSell, for random symmetric 12x12 element matrices.
+the diagonal blocks written by kNodeAssemble (each node's corner blocks
+summed), the symmetric assembly of kSellAssemble (each block above the
+diagonal summed from its contributors, its transpose written at the mirror
+position) and the row matvec of kPcgSell, for random symmetric 12x12 element
+matrices.
 The result must equal the element-by-element product
 y = sum_e K_e p_e (solver.cc:904-1048 applies the operator that way), on a
 Kuhn box and on a box with elements removed (uneven rows and slices).
@@ -40,8 +42,15 @@ int main(int argc, char** argv) {
   if (std::fread(p.data(), 8, p.size(), f) != p.size()) return 2;
   std::fclose(f);
   SellHost h = buildSellHost(rows, tets.data(), start, entry);
-  // symmetric assembly as kSellAssemble does it
+  // diagonal blocks as kNodeAssemble writes them: each node's corner blocks
   std::vector<double> val(size_t(h.positions) * 9, 0.0);
+  for (uint32_t e = 0; e < T; ++e)
+    for (int a = 0; a < 4; ++a) {
+      const uint32_t pos = h.diag[tets[4 * e + a]];
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) val[size_t(pos) * 9 + 3 * r + c] += K[size_t(e) * 144 + (3 * a + r) * 12 + 3 * a + c];
+    }
+  // the blocks above the diagonal and their transposes, as kSellAssemble writes them
   for (size_t i = 0; i < h.upper.size(); ++i) {
     const uint32_t pos = h.upper[i], mpos = h.mirror[i];
     double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -80,6 +89,8 @@ int main(int argc, char** argv) {
       scale = std::fmax(scale, std::fabs(ref[3 * size_t(row) + r]));
     }
   }
+  for (uint32_t row = 0; row < rows; ++row)
+    if (h.col[h.diag[row]] != row) return 4;
   size_t contributors = h.centry.size();
   std::printf("%.17g %.17g %zu %u %u %zu\n", err, scale, contributors, h.positions, h.widest, h.upper.size());
   return 0;
