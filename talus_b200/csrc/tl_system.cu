@@ -1537,11 +1537,18 @@ struct System final : SystemBase {
       const uint32_t mode = (mapping ? uint32_t(EM_MAPPING) : 0u) | (consistent ? uint32_t(EM_CONSISTENT) : 0u);
       element(law, weighted.ptr, total.ptr, pass, mode, margin);
     };
-    auto balanceSquared = [&]() {
+    // |right|^2 after the node assembly, and the loading count of the element
+    // pass before it, read back in one wait
+    auto balanceSquared = [&](uint32_t& loadingNow) {
       nodeAssemble(total.ptr, pass);
       finalize(1);
-      const BodyAccDev h = readAcc(0);
-      return h.right_sq;
+      BodyAccDev* ha = hAcc.get(B);
+      uint32_t* hc = hCount.get(B);
+      acc.download(ha, B, st);
+      loading.download(hc, B, st);
+      TL_CUDA(cudaStreamSynchronize(st));
+      loadingNow = hc[0];
+      return ha[0].right_sq;
     };
     auto solve = [&](bool x0zero) { pcg(law, incr.ptr, pass, x0zero, consistent); };
     auto addToTotal = [&]() {
@@ -1560,8 +1567,8 @@ struct System final : SystemBase {
         if (attempt < 2u) bind(attempt != 0u);
         assemble(LOADING_MARGIN);
         ++rep.plastic_evaluations;
-        const double squared = balanceSquared();
-        const uint32_t loadingNow = readCount(loading, 0);
+        uint32_t loadingNow = 0;
+        const double squared = balanceSquared(loadingNow);
         if (attempt != 0u) {
           const double ranked = std::isfinite(squared) ? squared : std::numeric_limits<double>::infinity();
           if (attempt == 1u || ranked < lowest) {
@@ -1641,8 +1648,9 @@ struct System final : SystemBase {
         if (fellBack) {
           assemble(LOADING_MARGIN);
           ++rep.plastic_evaluations;
-          const double squared = balanceSquared();
-          fellBack = readCount(loading, 0) == 0u && squared <= PLASTIC_REDUCTION * PLASTIC_REDUCTION * opening;
+          uint32_t loadingNow = 0;
+          const double squared = balanceSquared(loadingNow);
+          fellBack = loadingNow == 0u && squared <= PLASTIC_REDUCTION * PLASTIC_REDUCTION * opening;
         }
         if (fellBack) {
           ++rep.plastic_fallbacks;
