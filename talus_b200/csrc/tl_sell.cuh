@@ -46,10 +46,10 @@ template <class S> struct SellDev {
   const uint32_t* slice_start;   // [slices + 1]
   const uint32_t* group_slice;   // [positions / 32] slice of each 32-position group
   const uint32_t* col;           // [positions] column node
-  uint32_t upper_count;          // block positions with row <= column
+  uint32_t upper_count;          // block positions with row < column
   uint32_t col_cache;            // column slots per thread kept in shared memory by kPcgSell
   const uint32_t* upper;         // [upper_count] those positions
-  const uint32_t* mirror;        // [upper_count] position of the transposed block (itself on the diagonal)
+  const uint32_t* mirror;        // [upper_count] position of the transposed block
   const uint32_t* cstart;        // [positions + 1] contributor range of each position
   const uint32_t* centry;        // (element << 4) | (row corner << 2) | column corner
   S* val;                        // [positions / 32][9][32]
