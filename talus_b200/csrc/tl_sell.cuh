@@ -1,4 +1,4 @@
-// Assembled-operator PCG for a system holding one body.
+// PCG on the assembled operator.
 //
 // The element-by-element matvec of kPcg1 spends most of each iteration
 // moving element outputs back to the nodes through shared memory (bank
@@ -12,8 +12,12 @@
 //   kSellAssemble  one thread per block above the diagonal: the sum,
 //                  in ascending element order, of the element blocks that
 //                  land there (FP64 accumulation, stored in S), written with
-//                  its transpose below the diagonal;
-//   kPcgSell       persistent cooperative PCG in the pipelined arrangement
+//                  its transpose below the diagonal; the diagonal blocks are
+//                  written by kNodeAssemble;
+//   kPcgBatchSell  the batched PCG of kPcgBatch on this matrix, for batches
+//                  and for single bodies with more rows than kPcgSell's grid
+//                  has threads;
+//   kPcgSell       (one body) persistent cooperative PCG in the pipelined arrangement
 //                  of Ghysels and Vanroose ("Hiding global synchronization
 //                  latency in the preconditioned conjugate gradient
 //                  algorithm", 2014), which overlaps the one reduction of an
@@ -39,7 +43,7 @@ namespace tl {
 constexpr uint32_t SELL_SLICES_PER_BLOCK = TILE / SELL_ROWS;
 
 template <class S> struct SellDev {
-  uint32_t rows;                 // the body's nodes
+  uint32_t rows;                 // one body: its nodes; a batch: every node slot of the system
   uint32_t slices;               // ceil(rows / 32)
   uint32_t positions;            // block positions, a multiple of 32
   uint32_t stride;               // elements of one published vector (>= slices * 32)
