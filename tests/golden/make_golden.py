@@ -1,0 +1,142 @@
+"""Writes the golden fixtures of this directory from the oracle.
+
+The reference cannot be compiled here (it fetches GLM, Eigen and Catch2 at
+configure time, CMakeLists.txt:16-39) and none of its tests drives the tet
+step, so no fixture comes from the reference itself.  These arrays are the
+FP64 oracle's results (oracle/fem_oracle.cc, a restatement of
+deformable/solver/solver.cc and deformable/material/material.cc), with the
+oracle pinned by the law tests in tests/test_oracle_laws.py.  They freeze the
+oracle against later edits (tests/test_golden.py re-runs it) and give the GPU
+tests expected values that need no CPU solve (tests/test_gpu_golden.py).
+
+Each block fixture stores how its mesh is generated (talus_b200.box_mesh) and
+a checksum of the generated mesh, the positions after the first and the last
+step, and the step reports the GPU path must reproduce.  tet_laws.npz holds
+48 disconnected tets at seeded deformations (stretched, sheared, rotated,
+three inverted) with each law's element forces.
+
+Run from the repository root:  python -m tests.golden.make_golden
+"""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+
+import talus_b200 as tb
+from oracle import pyoracle as po
+from tests.helpers import elastic_block, oracle_material, plastic_block, run_oracle
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def mesh_checksum(mesh: tb.PreparedMesh) -> np.ndarray:
+    """Sums that change when the generator's nodes, tets or rest shapes do."""
+    order = np.arange(1, mesh.tets + 1, dtype=np.float64)
+    return np.array([mesh.rest_positions.sum(), np.abs(mesh.rest_positions).sum(),
+                     float(mesh.tet_nodes.astype(np.float64).ravel() @ np.tile(order, 4)),
+                     mesh.rest_inverse.sum(), np.abs(mesh.rest_inverse).sum(), mesh.volume.sum(),
+                     float(mesh.anchored.sum())])
+
+
+def material_array(m: tb.PhysicalMaterial) -> np.ndarray:
+    return np.array([m.density, m.youngs_modulus, m.poissons_ratio, m.stiffness_damping, m.yield_stress,
+                     m.hardening_modulus])
+
+
+def material_of(a) -> tb.PhysicalMaterial:
+    return tb.PhysicalMaterial(*(float(x) for x in a))
+
+
+BLOCKS = {
+    # name: (mesh builder, builder arguments, law, stiffness damping, steps)
+    "elastic_block_corotated": ("elastic", dict(cells=(8, 8, 8), jitter=0.01, seed=1), tb.COROTATED, 0.0, 12),
+    "elastic_block_snh": ("elastic", dict(cells=(8, 8, 8), jitter=0.01, seed=1), tb.NEO_HOOKEAN, 0.0, 12),
+    "damped_block": ("elastic", dict(cells=(8, 8, 8), jitter=0.01, seed=1), tb.COROTATED, 0.02, 12),
+    "plastic_block": ("plastic", dict(cells=(16, 8, 8), seed=2, speed=0.5), tb.COROTATED, 0.0, 10),
+}
+
+
+def block_case(name):
+    kind, args, law, damping, steps = BLOCKS[name]
+    mesh, mat = (elastic_block if kind == "elastic" else plastic_block)(**args)
+    mat.stiffness_damping = damping
+    return mesh, mat, tb.Settings(law=law), steps
+
+
+def write_block(name):
+    mesh, mat, settings, steps = block_case(name)
+    record = []
+    state, reports = run_oracle(po.F64, mesh, mat, settings, steps, record=record)
+    record32 = []
+    run_oracle(po.F32, mesh, mat, settings, steps, record=record32)
+    np.savez_compressed(
+        os.path.join(HERE, name + ".npz"),
+        mesh_checksum=mesh_checksum(mesh), material=material_array(mat), law=settings.law, steps=steps,
+        first=record[0], last=record[-1], last_fp32=record32[-1],
+        equivalent=state.plastic[:, 9],
+        cg_iterations=np.array([r["cg_iterations"] for r in reports]),
+        plastic_evaluations=np.array([r["plastic_evaluations"] for r in reports]))
+
+
+def single_tets(count=48, seed=11):
+    """`count` tets cut from a jittered Kuhn lattice, each with its own four
+    nodes, and a seeded deformation gradient per tet."""
+    base = tb.box_mesh((2, 2, 2), voxel=0.1, jitter=0.01, seed=seed)
+    rng = np.random.default_rng(seed)
+    pick = np.arange(count) % base.tets
+    corners = base.tet_nodes[pick]
+    rest = base.rest_positions[corners]                          # [count,4,3]
+    grads = []
+    for e in range(count):
+        scale = (0.001, 0.01, 0.05, 0.2)[e % 4]
+        f = np.eye(3) + scale * rng.standard_normal((3, 3))
+        if e % 8 == 5:                                           # a rigid turn on top
+            q = np.linalg.qr(rng.standard_normal((3, 3)))[0]
+            f = (q if np.linalg.det(q) > 0 else -q) @ f
+        if e in (7, 23, 39):                                     # inverted: one axis flipped through zero
+            f = f @ np.diag([1.0, 1.0, -0.3])
+        grads.append(f)
+    grads = np.array(grads)
+    centroid = rest.mean(axis=1, keepdims=True)
+    deformed = centroid + np.einsum("eij,ekj->eki", grads, rest - centroid)
+    return rest, base.rest_inverse[pick], base.volume[pick], deformed
+
+
+LAW_MATERIALS = {
+    "elastic": tb.PhysicalMaterial(density=1000.0, youngs_modulus=1e6, poissons_ratio=0.3),
+    "plastic": tb.PhysicalMaterial(density=1000.0, youngs_modulus=2e7, poissons_ratio=0.35, yield_stress=1e5,
+                                   hardening_modulus=2e5),
+}
+
+
+def write_tet_laws():
+    rest, rinv, volume, deformed = single_tets()
+    count = rest.shape[0]
+    el = oracle_material(LAW_MATERIALS["elastic"])
+    pl = oracle_material(LAW_MATERIALS["plastic"])
+    out = {k: np.zeros((count, 4, 3)) for k in ("corotated_force", "snh_force", "plastic_force")}
+    plastic_point = np.zeros((count, 10))
+    yielding = np.zeros(count, np.uint8)
+    for e in range(count):
+        args = (deformed[e], rest[e], rinv[e], volume[e])
+        out["corotated_force"][e] = po.tet_trial(po.F64, *args, el)["force"]
+        out["snh_force"][e] = po.snh_tet(po.F64, *args, el)["force"]
+        p = po.tet_point_trial(po.F64, *args, pl, tangent=False)
+        out["plastic_force"][e] = p["force"]
+        plastic_point[e] = p["plastic"]
+        yielding[e] = p["yielding"]
+    np.savez_compressed(os.path.join(HERE, "tet_laws.npz"), rest=rest, rest_inverse=rinv, volume=volume,
+                        deformed=deformed, elastic=material_array(LAW_MATERIALS["elastic"]),
+                        plastic=material_array(LAW_MATERIALS["plastic"]), plastic_point=plastic_point,
+                        yielding=yielding, **out)
+
+
+def main():
+    for name in BLOCKS:
+        write_block(name)
+    write_tet_laws()
+
+
+if __name__ == "__main__":
+    main()
