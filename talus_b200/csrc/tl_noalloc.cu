@@ -34,6 +34,7 @@
 
 #include "../../include/talus_fem.h"
 #include "tl_kernels.cuh"
+#include "tl_validate.h"
 
 #include <algorithm>
 #include <cmath>
@@ -248,12 +249,10 @@ int32_t stepLocked(int32_t device, const tl_mesh_desc& d, int32_t dtype, void* p
                    void* acceleration, void* rotation, void* plastic, const tl_settings& set, const double gvec[3],
                    double dt, tl_step_report* report) {
   // ---- validation (no allocation below this point, ever)
-  if (d.nodes == 0 || d.tets == 0 || !d.rest_positions || !d.node_mass || !d.anchored || !d.tet_nodes ||
-      !d.rest_inverse || !d.volume || !d.material || !position || !velocity || !acceleration)
-    return TL_ERR_ARG;
+  if (d.nodes == 0 || d.tets == 0 || !position || !velocity || !acceleration) return TL_ERR_ARG;
   if (d.nodes > TL_NOALLOC_MAX_NODES || d.tets > TL_NOALLOC_MAX_TETS || d.lanes > TL_NOALLOC_MAX_LANES)
     return TL_ERR_TOO_LARGE;
-  if (set.law > 1u || !(dt > 0.0)) return TL_ERR_ARG;
+  if (meshDescProblem(d) || set.law > 1u || !stepArgumentsValid(dt, gvec)) return TL_ERR_ARG;
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || device >= count) return TL_ERR_NO_DEVICE;
   NA_CUDA(cudaSetDevice(device));

@@ -9,6 +9,7 @@
 #include "tl_adjoint.cuh"
 #include "tl_sell.cuh"
 #include "tl_sell_build.h"
+#include "tl_validate.h"
 
 #include <algorithm>
 #include <condition_variable>
@@ -454,9 +455,7 @@ struct System final : SystemBase {
     uint64_t vp = 0, tp = 0, lanes = 0;
     for (uint32_t b = 0; b < B; ++b) {
       const tl_mesh_desc& d = descs[b];
-      if (d.nodes == 0 || d.tets == 0 || !d.rest_positions || !d.node_mass || !d.anchored || !d.tet_nodes ||
-          !d.rest_inverse || !d.volume || !d.material)
-        throw StatusError{TL_ERR_ARG, "mesh descriptor has an empty or missing field"};
+      if (const char* problem = meshDescProblem(d)) throw StatusError{TL_ERR_ARG, problem};
       BodyDev& bd = bodyHost[b];
       bd.node_begin = uint32_t(vp);
       bd.node_end = uint32_t(vp + d.nodes);
@@ -530,9 +529,7 @@ struct System final : SystemBase {
         const uint32_t e = bd.elem_begin + t;
         uint32_t q[4];
         for (int k = 0; k < 4; ++k) {
-          q[k] = d.tet_nodes[4 * size_t(t) + k];
-          if (q[k] >= d.nodes) throw StatusError{TL_ERR_ARG, "tet node index out of range"};
-          q[k] += bd.node_begin;
+          q[k] = d.tet_nodes[4 * size_t(t) + k] + bd.node_begin;  // in range: meshDescProblem
         }
         hTet[e] = make_uint4(q[0], q[1], q[2], q[3]);
         for (int k = 0; k < 9; ++k) {
@@ -2047,7 +2044,7 @@ int32_t tl_state_get(tl_system* system, uint32_t body, int32_t dtype, void* posi
 
 int32_t tl_step(tl_system* system, const tl_settings* settings, const double gravity[3], double dt,
                 tl_step_report* reports) {
-  if (!system || !settings || !gravity || !(dt > 0.0)) return TL_ERR_ARG;
+  if (!system || !settings || !gravity || !stepArgumentsValid(dt, gravity)) return TL_ERR_ARG;
   return guarded(system->ctx, [&]() -> int32_t {
     TL_CUDA(cudaSetDevice(system->ctx->device));
     return system->impl->step(*settings, gravity, dt, reports);
