@@ -150,7 +150,12 @@ const char* tl_ctx_last_error(const tl_ctx* ctx);
 /* Upload one or more bodies (a batch when count > 1) into one resident
  * system.  Replaces buildMesh's output handling + refreshStiffness +
  * buildIncidence (solver.cc:453-507, 1065-1101): the node->element CSR
- * incidence is built here in the reference's element order. */
+ * incidence is built here in the reference's element order.  A body must
+ * look like buildMesh output (solver.cc:2352-2356): finite rest positions,
+ * rest inverses and prescribed velocities, volumes > 0, masses >= 0, node
+ * indices < nodes, lanes with a finite E >= 0; otherwise TL_ERR_ARG and
+ * nothing is uploaded.  tl_step and tl_step_noalloc also refuse a dt that is
+ * not finite and positive, and non-finite gravity. */
 int32_t tl_system_create(tl_ctx* ctx, const tl_mesh_desc* bodies, uint32_t count, int32_t precision,
                          tl_system** out);
 int32_t tl_system_destroy(tl_system* system);
