@@ -2116,7 +2116,11 @@ int32_t tl_step_host(tl_system* system, uint32_t body, int32_t dtype, void* posi
                      void* acceleration, void* rotation, void* plastic, const tl_settings* settings,
                      const double gravity[3], double dt, tl_step_report* report) {
   if (!system || body >= system->impl->bodies || system->impl->bodies != 1u) return TL_ERR_ARG;
-  int32_t rc = tl_state_set(system, body, dtype, position, velocity, acceleration, rotation, plastic);
+  // The incoming rotations are not uploaded: every element pass writes each
+  // committed rotation before any kernel reads one (kElement, then kDamping
+  // and the matvec), as assembleElastic does in the reference
+  // (solver.cc:1404, 1446, 1500, 1547 before 745-987).  They are outputs only.
+  int32_t rc = tl_state_set(system, body, dtype, position, velocity, acceleration, nullptr, plastic);
   if (rc != TL_OK) return rc;
   rc = tl_step(system, settings, gravity, dt, report);
   if (rc != TL_OK && rc != TL_ERR_NONFINITE) return rc;

@@ -157,3 +157,38 @@ def test_smallest_bodies_in_a_ragged_batch_match_the_oracle(form):
     for i, (m, (_, ost)) in enumerate(zip(meshes, refs)):
         assert relative_error(batch.get_state(i).position, ost.position, m.rest_positions) <= 1e-9, i
     batch.close()
+
+
+@pytest.mark.parametrize("law,damping", [(tb.COROTATED, 0.0), (tb.COROTATED, 0.02), (tb.NEO_HOOKEAN, 0.0)])
+def test_host_step_treats_rotations_as_outputs(law, damping):
+    """tl_step_host does not upload the committed rotations (the step writes
+    each before reading it, solver.cc:1404-1547): NaN rotations in the caller's
+    buffer give bitwise the same step as the rotations of the previous step,
+    and come back overwritten."""
+    import ctypes as C
+    from talus_b200 import _capi as capi
+
+    mesh, mat = elastic_block((6, 5, 4), seed=8)
+    mat.stiffness_damping = damping
+    system = tb.System(mesh, [mat], tb.FP64)
+    settings = tb.Settings(law=law)
+    g = np.asarray(GRAVITY, np.float64)
+    results = []
+    for poison in (False, True):
+        st = tb.rest_state(mesh)
+        arrays = {k: np.ascontiguousarray(getattr(st, k), np.float64) for k in
+                  ("position", "velocity", "acceleration", "rotation", "plastic")}
+        for n in range(4):
+            if poison:
+                arrays["rotation"][:] = np.nan
+            rc = capi.lib().tl_step_host(system.handle, 0, capi.TL_DTYPE_F64,
+                                         *[arrays[k].ctypes.data for k in
+                                           ("position", "velocity", "acceleration", "rotation", "plastic")],
+                                         C.byref(settings._c()), g.ctypes.data, DT, C.byref(capi.tl_step_report()))
+            assert rc == capi.TL_OK, (poison, n, rc)
+        results.append(arrays)
+    system.close()
+    clean, poisoned = results
+    assert np.isfinite(poisoned["rotation"]).all()
+    for k in clean:
+        assert np.array_equal(clean[k], poisoned[k]), k
