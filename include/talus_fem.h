@@ -180,6 +180,28 @@ int32_t tl_system_tune(tl_system* system, uint32_t pcg_blocks_per_sm, uint32_t g
 #define TL_SOLVER_ELEMENTWISE 2u
 int32_t tl_system_set_solver(tl_system* system, uint32_t form);
 
+/* Plasticity of the yielding lanes.
+ * TL_PLASTICITY_SMALL_STRAIN (default): the tet law's J2 return on the small
+ * elastic strain inside the step, with the plastic Newton loop
+ * (material.cc:594-683, 978-1057; solver.cc:3951-4250).
+ * TL_PLASTICITY_HENCKY: the finite-strain flow of the reference's hex World
+ * path (plasticflow.cc:96-150, 184-247), at one point per tet.  Each step is
+ * elastic (corotated law) from the tet's plastic rest shape: Dm^-1 P and
+ * volume V / det P (plasticRest, plasticflow.cc:263-300).  After the solve,
+ * every yielding tet with det F > 0 returns F P radially in log-stretch
+ * space.  The yield stress is blended as (start + r q) / (1 + r), with
+ * r = H / (3 mu), and P and a hardening variable are kept per tet.  There is
+ * no crush and no plastic cap: tl_material has neither field, and the
+ * reference defaults for both are infinite.
+ * With HENCKY, the plastic slot of tl_state_set/get holds P (9 values,
+ * row-major) and then the hardening variable.  tl_step_report::yielding
+ * counts the tets that flowed.  Setting a mode resets every tet to P = I and
+ * hardening 0.  HENCKY needs TL_LAW_COROTATED and no stiffness damping, and
+ * does not run under rollouts (TL_ERR_UNSUPPORTED). */
+#define TL_PLASTICITY_SMALL_STRAIN 0u
+#define TL_PLASTICITY_HENCKY 1u
+int32_t tl_system_set_plasticity(tl_system* system, uint32_t mode);
+
 /* Diagnostics, no reference counterpart: iteration counts (body 0) of the
  * PCG launches made while TL_FLAG_TRACE was set, oldest first, since the
  * system was created.  Writes min(capacity, recorded) entries; *count gets

@@ -202,6 +202,93 @@ template <class R> M3<R> invertibleRotation(const M3<R>& gradient) {
   return out;
 }
 
+// ------------------------------------------------- finite-strain flow ----
+// plasticflow.cc:96-150 returnMap, FP64 like the reference.  The left stretch
+// B = F_e F_e^T (leftStretch, plasticflow.cc:22-38) is diagonalised by the
+// cyclic Jacobi solve above (Eigen::SelfAdjointEigenSolver in the reference;
+// the spectral function V f(L) V^T built from it does not depend on the order
+// or the signs of the eigenvectors).  Log strains 0.5 log(lambda_i), their
+// deviator d, q = sqrt(3/2) 2 mu |d|; past the yield stress the deviator is
+// scaled back by exp(d_i (yield / q - 1)) along the eigenvectors.
+struct HenckyReturn {
+  M3<double> elastic{1.0};
+  double strain = 0.0, trial = 0.0;
+  bool mapped = false;
+};
+
+// Log-strain deviator of F_e and the eigenvectors it is expressed in; false
+// when B is not positive definite.
+inline bool henckyDeviator(const M3<double>& fe, double dev[3], double vec[3][3], double& size) {
+  double a[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) a[i][j] = fe[0][i] * fe[0][j] + fe[1][i] * fe[1][j] + fe[2][i] * fe[2][j];
+  jacobiEigen(a, vec);
+  const double lo = std::min(a[0][0], std::min(a[1][1], a[2][2]));
+  if (!(lo > 0.0)) return false;
+  const double strain[3] = {0.5 * std::log(a[0][0]), 0.5 * std::log(a[1][1]), 0.5 * std::log(a[2][2])};
+  const double mean = (strain[0] + strain[1] + strain[2]) / 3.0;
+  for (int i = 0; i < 3; ++i) dev[i] = strain[i] - mean;
+  size = std::sqrt(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
+  return true;
+}
+
+// plasticflow.cc:96-108
+inline double henckyVonMises(const M3<double>& fe, double shear) {
+  double dev[3], vec[3][3], size = 0.0;
+  if (!henckyDeviator(fe, dev, vec, size)) return 0.0;
+  return std::sqrt(1.5) * 2.0 * shear * size;
+}
+
+// plasticflow.cc:110-150
+inline HenckyReturn henckyReturn(const M3<double>& fe, double shear, double yieldStress) {
+  HenckyReturn out;
+  double dev[3], vec[3][3], size = 0.0;
+  if (!henckyDeviator(fe, dev, vec, size)) return out;
+  const double stress = std::sqrt(1.5) * 2.0 * shear * size;
+  if (!(stress > yieldStress) || size <= 1.0e-15) return out;
+  M3<double> correction(0.0);
+  for (int k = 0; k < 3; ++k) {
+    const double scale = std::exp(dev[k] * (yieldStress / stress - 1.0));
+    const V3<double> v(vec[0][k], vec[1][k], vec[2][k]);
+    correction = correction + scale * outer(v, v);
+  }
+  out.elastic = correction * fe;
+  out.trial = stress;
+  out.strain = (stress - yieldStress) / (3.0 * shear);
+  out.mapped = true;
+  return out;
+}
+
+inline double oneNorm(const M3<double>& m) {
+  double total = 0.0;
+  for (int c = 0; c < 3; ++c) total += std::abs(m[c].x) + std::abs(m[c].y) + std::abs(m[c].z);
+  return total;
+}
+
+// plasticflow.cc:184-247 flowLattice at one point, without the crush and the
+// plastic cap (PhysicalMaterial::crushStress and plasticMax keep their
+// infinite defaults here): the elastic map F P returns with the yield stress
+// blended toward the trial stress, (start + r q) / (1 + r), r = H / (3 mu);
+// the plastic map becomes F^-1 F_e,returned and the hardening variable grows
+// by the returned strain.
+inline bool henckyFlow(const M3<double>& deformation, M3<double>& plastic, double& hardening, double shear,
+                       double yieldStress, double hardeningModulus) {
+  if (!(determinant(deformation) > 0.0)) return false;
+  const M3<double> elastic = deformation * plastic;
+  const double start = yieldStress + hardeningModulus * hardening;
+  const double ratio = hardeningModulus / (3.0 * shear);
+  const HenckyReturn trial = henckyReturn(elastic, shear, start);
+  if (!trial.mapped) return false;
+  const double yieldNow = (start + ratio * trial.trial) / (1.0 + ratio);
+  const HenckyReturn mapped = henckyReturn(elastic, shear, yieldNow);
+  if (!mapped.mapped) return false;
+  const M3<double> next = inverse(deformation) * mapped.elastic;
+  if (!(oneNorm(next - plastic) > 1.0e-12)) return false;
+  plastic = next;
+  hardening += mapped.strain;
+  return true;
+}
+
 // material.cc:24-27
 template <class R> M3<R> elementRotation(const M3<R>& gradient, int mode) {
   if (mode == OR_ROTATION_POLAR || determinant(gradient) > R(0)) return polarRotation(gradient);
@@ -651,6 +738,13 @@ template <class R> struct Solver {
   std::vector<RigidFit<R>> fits;         // Damping::fits at the last assemble
   bool damped = false;
   R dampScale{0};                        // Damping::scale = (1 - alpha_f) gamma h (solver.cc:3590)
+  // finite-strain flow (OR_PLASTICITY_HENCKY): Dm^-1 as given, the plastic
+  // map P = Fp^-1 and hardening variable per tet, and the corners of each
+  // tet's plastic rest shape Dm' = Fp Dm (plasticRest, plasticflow.cc:263-300)
+  bool hencky = false;
+  std::vector<M3<double>> authored, flowMap;
+  std::vector<double> hardeningOf;
+  std::vector<std::array<V3<R>, 4>> plasticCorners;
   std::vector<M3<R>> snhGradient;        // SNH operator state: F per tet
   std::vector<R> snhChange;              // SNH operator state: J - 1 per tet
   // scratch (solver.cc:395-420)
@@ -687,7 +781,8 @@ template <class R> struct Solver {
     for (uint32_t e = 0; e < T; ++e) {
       const Element<R>& el = elements[e];
       const std::array<V3<R>, 4> g = gather(at, el);
-      const std::array<V3<R>, 4> r = gather(rest, el);
+      // from the plastic rest shape the corotated offsets and K use Dm', V'
+      const std::array<V3<R>, 4> r = hencky ? plasticCorners[e] : gather(rest, el);
       std::array<V3<R>, 4> f;
       std::array<M3<R>, 4> diag;
       if (law == OR_LAW_SNH) {
@@ -698,7 +793,7 @@ template <class R> struct Solver {
         f = s.force;
         const std::array<V3<R>, 4> grad = shapeGradients(el.restInverse);
         for (int n = 0; n < 4; ++n) diag[n] = snhDiagonal(grad[n], s.gradient, el.volume, el.moduli);
-      } else if (el.yields) {
+      } else if (el.yields && !hencky) {
         const TetPointTrial<R> c = tetPointTrial(g, r, el.restInverse, el.volume, el.moduli, el.yieldStress,
                                                  el.hardening, plastic[e], margin, mode, mapping, consistent);
         rotation[e] = c.rotation;
@@ -900,6 +995,13 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
   s.plastic.resize(T);
   s.snhGradient.assign(T, M3<R>(R(1)));
   s.snhChange.assign(T, R(0));
+  s.hencky = settings->plasticity == OR_PLASTICITY_HENCKY;
+  if (s.hencky) {
+    s.authored.resize(T);
+    s.flowMap.resize(T);
+    s.hardeningOf.resize(T);
+    s.plasticCorners.resize(T);
+  }
   bool anyYields = false;
   static const or_material DEFAULT = {1000.0, 0.0, 0.3, 0.0, std::numeric_limits<double>::infinity(), 0.0};
   for (uint32_t e = 0; e < T; ++e) {
@@ -916,6 +1018,20 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
     el.hardening = R(m.hardening_modulus);
     el.yields = yieldsAt(el.yieldStress);
     anyYields = anyYields || el.yields;
+    if (s.hencky) {
+      const M3<double> given = loadRowMajor<double>(mesh->rest_inverse + 9 * e);
+      const M3<double> p = loadRowMajor<double>(st->plastic + 10 * e);
+      s.authored[e] = given;
+      s.flowMap[e] = p;
+      s.hardeningOf[e] = st->plastic[10 * e + 9];
+      double rowMajor[9];
+      storeRowMajor(given * p, rowMajor);  // Dm'^-1 = Dm^-1 P
+      el.restInverse = loadRowMajor<R>(rowMajor);
+      el.volume = R(mesh->volume[e] / determinant(p));  // V' = V det Fp
+      storeRowMajor(inverse(given * p), rowMajor);
+      const M3<R> shape = loadRowMajor<R>(rowMajor);
+      s.plasticCorners[e] = {V3<R>(), shape[0], shape[1], shape[2]};
+    }
     s.store[e] = tetStiffness(el.restInverse, el.volume, el.moduli);
     s.rotation[e] = loadRowMajor<R>(st->rotation + 9 * e);
     PlasticPoint<R> p;
@@ -924,6 +1040,10 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
     s.plastic[e] = p;
   }
   if (s.law == OR_LAW_SNH) anyYields = false;  // SNH runs elastic only
+  // the finite-strain flow is written for the corotated law without damping
+  if (s.hencky && (s.law == OR_LAW_SNH || s.damped)) return -3;
+  const bool anyFlows = s.hencky && anyYields;
+  if (s.hencky) anyYields = false;  // each step is elastic from the plastic rest
   // damping is defined with the corotated stiffness and committed rotation
   if (s.damped && s.law == OR_LAW_SNH) return -3;
   if (s.damped) s.fits.assign(T, RigidFit<R>());
@@ -1196,7 +1316,25 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
       s.position[n] = s.shifted[n] + (rule.beta * inner * inner) * s.acceleration[n];
     }
     // solver.cc:5860-5861
-    plasticGrowth = s.commitPlastic(mode) || plasticGrowth;
+    if (!s.hencky) plasticGrowth = s.commitPlastic(mode) || plasticGrowth;
+  }
+  // strainstep.cc:822-825: flowLattice once per step, after the solve
+  if (anyFlows) {
+    uint32_t flowed = 0;
+    for (uint32_t e = 0; e < T; ++e) {
+      const Element<R>& el = s.elements[e];
+      if (!el.yields) continue;
+      std::array<V3<double>, 4> x;
+      for (int k = 0; k < 4; ++k) {
+        const V3<R>& p = s.position[el.nodes[k]];
+        x[k] = V3<double>(double(p.x), double(p.y), double(p.z));
+      }
+      if (henckyFlow(deformationOf(x, s.authored[e]), s.flowMap[e], s.hardeningOf[e], double(el.moduli.second),
+                     double(el.yieldStress), double(el.hardening)))
+        ++flowed;
+    }
+    report->yielding = flowed;
+    plasticGrowth = plasticGrowth || flowed != 0u;
   }
   // solver.cc:5874-5882
   R kinetic = 0;
@@ -1216,6 +1354,11 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
   report->non_finite |= finite ? 0u : 1u;
   for (uint32_t e = 0; e < T; ++e) {
     storeRowMajor(s.rotation[e], st->rotation + 9 * e);
+    if (s.hencky) {
+      storeRowMajor(s.flowMap[e], st->plastic + 10 * e);
+      st->plastic[10 * e + 9] = s.hardeningOf[e];
+      continue;
+    }
     storeRowMajor(s.plastic[e].strain, st->plastic + 10 * e);
     st->plastic[10 * e + 9] = double(s.plastic[e].equivalent);
   }
@@ -1442,6 +1585,29 @@ int or_rotation(int precision, const double* gradient, int rotation_mode, double
   if (precision == OR_F32) storeRowMajor(elementRotation(loadRowMajor<float>(gradient), rotation_mode), out);
   else storeRowMajor(elementRotation(loadRowMajor<double>(gradient), rotation_mode), out);
   return 0;
+}
+
+int or_hencky_return(const double* elastic, double shear, double yield_stress, double* returned, double* strain,
+                     double* trial) {
+  const HenckyReturn r = henckyReturn(loadRowMajor<double>(elastic), shear, yield_stress);
+  if (!r.mapped) return 0;
+  storeRowMajor(r.elastic, returned);
+  *strain = r.strain;
+  *trial = r.trial;
+  return 1;
+}
+
+double or_hencky_von_mises(const double* elastic, double shear) {
+  return henckyVonMises(loadRowMajor<double>(elastic), shear);
+}
+
+int or_hencky_flow(const double* deformation, double* plastic, double* hardening, double shear, double yield_stress,
+                   double hardening_modulus) {
+  M3<double> p = loadRowMajor<double>(plastic);
+  const bool changed = henckyFlow(loadRowMajor<double>(deformation), p, *hardening, shear, yield_stress,
+                                  hardening_modulus);
+  storeRowMajor(p, plastic);
+  return changed ? 1 : 0;
 }
 
 }  // extern "C"

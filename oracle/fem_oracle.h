@@ -31,6 +31,11 @@ extern "C" {
 enum { OR_F32 = 0, OR_F64 = 1 };
 enum { OR_LAW_COROTATED = 0, OR_LAW_SNH = 1 };
 enum { OR_ROTATION_POLAR = 0, OR_ROTATION_INVERTIBLE = 1 };
+/* or_settings.plasticity: the tet law's small-strain J2 return inside the
+ * step (material.cc:594-683, 978-1057), or the finite-strain (Hencky) flow of
+ * the hex World path (plasticflow.cc:96-150, 184-247) after the step, from a
+ * per-tet plastic rest shape. */
+enum { OR_PLASTICITY_SMALL_STRAIN = 0, OR_PLASTICITY_HENCKY = 1 };
 
 typedef struct or_material {
   double density;
@@ -63,7 +68,9 @@ typedef struct or_settings {
   double tolerance;         /* Settings::tolerance (solver.h:64) */
   double spectral_radius;   /* Settings::spectralRadius (solver.h:65) */
   uint32_t rigid_split;     /* Settings::rigidSplit (solver.h:66): 0 = Off */
-  uint32_t reserved;
+  uint32_t plasticity;      /* OR_PLASTICITY_*; with HENCKY the state's plastic
+                               slot holds the plastic rest map P = Fp^-1
+                               row-major (9) and the hardening variable */
 } or_settings;
 
 typedef struct or_state {
@@ -159,6 +166,22 @@ int or_damping_apply(int precision, const double* corners, const double* rotatio
 
 int or_rotation(int precision, const double* gradient, int rotation_mode,
                 double* out);
+
+/* plasticflow.cc:96-150 returnMap of one point: elastic [9] row-major F_e,
+ * shear modulus, yield stress.  Returns 1 and writes the returned elastic
+ * map [9], strain = (q - yield) / (3 shear) and trial = q when the point is
+ * past its yield surface, else 0. */
+int or_hencky_return(const double* elastic, double shear, double yield_stress, double* returned, double* strain,
+                     double* trial);
+
+/* plasticflow.cc:96-108 vonMises: sqrt(3/2) 2 shear |dev log V_e|. */
+double or_hencky_von_mises(const double* elastic, double shear);
+
+/* plasticflow.cc:184-247 flowLattice for one point (no crush, no cap):
+ * deformation [9] F, plastic [9] P = Fp^-1 and *hardening updated in place.
+ * Returns 1 when P changed. */
+int or_hencky_flow(const double* deformation, double* plastic, double* hardening, double shear,
+                   double yield_stress, double hardening_modulus);
 
 #ifdef __cplusplus
 }

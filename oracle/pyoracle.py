@@ -23,6 +23,7 @@ LIB_PATH = os.path.join(HERE, "_build", "libfem_oracle.so")
 F32, F64 = 0, 1
 LAW_COROTATED, LAW_SNH = 0, 1
 ROTATION_POLAR, ROTATION_INVERTIBLE = 0, 1
+PLASTICITY_SMALL_STRAIN, PLASTICITY_HENCKY = 0, 1
 
 
 class Material(C.Structure):
@@ -61,7 +62,7 @@ class _Settings(C.Structure):
         ("tolerance", C.c_double),
         ("spectral_radius", C.c_double),
         ("rigid_split", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("plasticity", C.c_uint32),
     ]
 
 
@@ -140,6 +141,10 @@ def lib():
         _lib.or_rotation.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_void_p]
         _lib.or_damping_apply.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                           C.POINTER(Material), C.c_void_p, C.c_void_p]
+        _lib.or_hencky_return.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.or_hencky_von_mises.argtypes = [C.c_void_p, C.c_double]
+        _lib.or_hencky_von_mises.restype = C.c_double
+        _lib.or_hencky_flow.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double]
     return _lib
 
 
@@ -207,14 +212,17 @@ class State:
     plastic: np.ndarray    # [T,10]
 
     @staticmethod
-    def rest(mesh: Mesh) -> "State":
+    def rest(mesh: Mesh, hencky: bool = False) -> "State":
         """restState (solver.cc:2420-2453) at the identity pose; anchored nodes
-        start with their prescribed velocity."""
+        start with their prescribed velocity.  ``hencky``: the plastic slot holds
+        the identity plastic map P = I and hardening 0."""
         v = np.zeros((mesh.nodes, 3))
         if mesh.prescribed is not None:
             v[mesh.anchored != 0] = mesh.prescribed[mesh.anchored != 0]
-        return State(mesh.rest.copy(), v, np.zeros((mesh.nodes, 3)),
-                     np.tile(np.eye(3), (mesh.tets, 1, 1)), np.zeros((mesh.tets, 10)))
+        plastic = np.zeros((mesh.tets, 10))
+        if hencky:
+            plastic[:, [0, 4, 8]] = 1.0
+        return State(mesh.rest.copy(), v, np.zeros((mesh.nodes, 3)), np.tile(np.eye(3), (mesh.tets, 1, 1)), plastic)
 
     def copy(self) -> "State":
         return State(self.position.copy(), self.velocity.copy(), self.acceleration.copy(), self.rotation.copy(),
@@ -230,6 +238,7 @@ class Settings:
     tolerance: float = 1e-3
     spectral_radius: float = 0.5
     rigid_split: int = 2
+    plasticity: int = PLASTICITY_SMALL_STRAIN
 
 
 def step(precision: int, mesh: Mesh, state: State, materials, settings: Settings, gravity=(0.0, -9.81, 0.0),
@@ -243,7 +252,7 @@ def step(precision: int, mesh: Mesh, state: State, materials, settings: Settings
                _ptr(state.plastic))
     mats = (Material * len(materials))(*materials)
     st = _Settings(settings.substeps, settings.cg_iterations, settings.plastic_passes, settings.law,
-                   settings.tolerance, settings.spectral_radius, settings.rigid_split, 0)
+                   settings.tolerance, settings.spectral_radius, settings.rigid_split, settings.plasticity)
     g = np.asarray(gravity, dtype=np.float64)
     rep = report if report is not None else Report()
     rc = lib().or_step(precision, C.byref(m), C.byref(s), mats, len(materials), C.byref(st), _ptr(g), dt,
@@ -297,3 +306,27 @@ def rotation(precision, gradient, mode=ROTATION_INVERTIBLE):
     g = np.ascontiguousarray(gradient, np.float64); out = np.zeros((3, 3))
     lib().or_rotation(precision, _ptr(g), mode, _ptr(out))
     return out
+
+
+def hencky_return(elastic, shear, yield_stress):
+    """plasticflow.cc:110-150 returnMap of one point: None inside the yield
+    surface, else (returned elastic map, strain, trial stress)."""
+    fe = np.ascontiguousarray(elastic, np.float64)
+    out = np.zeros((3, 3)); strain = np.zeros(1); trial = np.zeros(1)
+    if not lib().or_hencky_return(_ptr(fe), shear, yield_stress, _ptr(out), _ptr(strain), _ptr(trial)):
+        return None
+    return out, float(strain[0]), float(trial[0])
+
+
+def hencky_von_mises(elastic, shear) -> float:
+    """plasticflow.cc:96-108 vonMises."""
+    return float(lib().or_hencky_von_mises(_ptr(np.ascontiguousarray(elastic, np.float64)), shear))
+
+
+def hencky_flow(deformation, plastic, hardening, shear, yield_stress, hardening_modulus):
+    """plasticflow.cc:184-247 flowLattice at one point: (changed, P, hardening)."""
+    f = np.ascontiguousarray(deformation, np.float64)
+    p = np.array(plastic, np.float64, order="C")
+    h = np.array([hardening], np.float64)
+    changed = lib().or_hencky_flow(_ptr(f), _ptr(p), _ptr(h), shear, yield_stress, hardening_modulus)
+    return bool(changed), p, float(h[0])

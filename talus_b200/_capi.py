@@ -140,6 +140,7 @@ SIGNATURES = {
     "tl_system_trace": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
     "tl_system_tune": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32]),
     "tl_system_set_solver": (C.c_int32, [C.c_void_p, C.c_uint32]),
+    "tl_system_set_plasticity": (C.c_int32, [C.c_void_p, C.c_uint32]),
     "tl_state_set": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_int32] + [C.c_void_p] * 5),
     "tl_state_get": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_int32] + [C.c_void_p] * 5),
     "tl_step": (C.c_int32, [C.c_void_p, C.POINTER(tl_settings), C.c_void_p, C.c_double,

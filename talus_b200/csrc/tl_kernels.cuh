@@ -196,6 +196,8 @@ template <class S> struct Sys {
   const S* dtau;               // [Tp] damping weight of each element's lane (0: undamped)
   S* dfit;                     // [20][Tp] rigid fit at the last assemble: arms (12), inverse inertia
                                // (xx, yy, zz, xy, xz, yz), damping coefficients (a, b)
+  // finite-strain plastic flow (null unless the system's plasticity is Hencky)
+  double* hk;                  // [10][Tp] plastic map P = Fp^-1 (9 planes, row-major), hardening variable
 };
 
 constexpr int TILE_OFF_STRIDE = 4 * TILE + 4;  // 4 TILE + 1 offsets, padded to 8-byte rows
@@ -472,9 +474,14 @@ enum ElementMode : uint32_t {
 #ifndef TL_ELEMENT_MIN_BLOCKS
 #define TL_ELEMENT_MIN_BLOCKS 2  // resident 256-thread blocks per SM the element pass is compiled for
 #endif
-template <class S, int LAW>
+// HK: the corotated law from each tet's plastic rest shape (finite-strain
+// flow): F' = F P, gradients g' = P^T g, volume V / det P, where P = Fp^-1 is
+// the tet's plastic map (plasticRest, plasticflow.cc:263-300: Dm' = Fp Dm,
+// V' = V det Fp); the small-strain return map is off.
+template <class S, int LAW, bool HK = false>
 __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
     kElement(Sys<S> s, const Vec4<S>* base, const Vec4<S>* dir, uint32_t pass, uint32_t mode, double margin) {
+  static_assert(!HK || LAW == 0, "the plastic rest shape is written for the corotated law");
   const uint32_t tile = blockIdx.x, b = s.elem_tile_body[tile];
   if (!bodyActive(s, b, pass)) return;
   const uint32_t e = tile * TILE + threadIdx.x;
@@ -499,7 +506,23 @@ __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
         addOuter(H, uu, g0[c]);
       }
     }
-    const double vol = s.vold[e];
+    double vol = s.vold[e];
+    if constexpr (HK) {  // H' = (I + H) P - I
+      M3<double> P;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) P.m[i][j] = s.hk[size_t(3 * i + j) * s.Tp + e];
+      M3<double> F = H;
+      F.m[0][0] += 1.0;
+      F.m[1][1] += 1.0;
+      F.m[2][2] += 1.0;
+      H = mul(F, P);
+      H.m[0][0] -= 1.0;
+      H.m[1][1] -= 1.0;
+      H.m[2][2] -= 1.0;
+      vol /= det3(P);
+    }
     const MatDev m = s.mat[s.lane[e]];
     const double youngs = s.eyoung ? s.eyoung[e] : m.youngs;
     const double lam = youngs * m.lam_unit, mu = youngs * m.mu_unit;
@@ -544,6 +567,15 @@ __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
         g[1] = {d[0], d[1], d[2]};
         g[2] = {d[3], d[4], d[5]};
         g[3] = {d[6], d[7], d[8]};
+        if constexpr (HK) {  // g' = P^T g (P reloaded: not kept live through the rotation)
+          double p[9];
+#pragma unroll
+          for (int k = 0; k < 9; ++k) p[k] = s.hk[size_t(k) * s.Tp + e];
+#pragma unroll
+          for (int c = 1; c < 4; ++c)
+            g[c] = {p[0] * g[c].x + p[3] * g[c].y + p[6] * g[c].z, p[1] * g[c].x + p[4] * g[c].y + p[7] * g[c].z,
+                    p[2] * g[c].x + p[5] * g[c].y + p[8] * g[c].z};
+        }
         g[0] = -(g[1] + g[2] + g[3]);
       }
       // From here on the arithmetic is the storage type S: the strain above
@@ -551,7 +583,7 @@ __global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
       // map, stress and forces only need the relative accuracy of the S
       // records they end in.  In FP64 systems nothing changes.
       using C = S;
-      const bool yields = m.yields != 0u;
+      const bool yields = !HK && m.yields != 0u;
       const C lamC = C(lam), muC = C(mu), volC = C(vol);
       const C bulk = C(lam + 2.0 * mu / 3.0);
       Sym<C> stress;
@@ -1070,7 +1102,10 @@ __global__ void __launch_bounds__(TILE) kElemStateIn(Sys<S> s, uint32_t e0, uint
 #pragma unroll
     for (int k = 0; k < 9; ++k) s.op[size_t(k) * s.Tp + e] = S(rot[9 * size_t(t) + k]);
   }
-  if (plastic) {
+  if (plastic && s.hk) {  // finite-strain flow: P row-major, hardening variable
+#pragma unroll
+    for (int k = 0; k < 10; ++k) s.hk[size_t(k) * s.Tp + e] = double(plastic[10 * size_t(t) + k]);
+  } else if (plastic) {
     const H* q = plastic + 10 * size_t(t);
     s.plast[e] = Vec4<S>{S(q[0]), S(q[4]), S(q[8]), S(0.5 * (double(q[1]) + double(q[3])))};
     s.plast[size_t(s.Tp) + e] = Vec4<S>{S(0.5 * (double(q[2]) + double(q[6]))),
@@ -1087,13 +1122,119 @@ __global__ void __launch_bounds__(TILE) kElemStateOut(Sys<S> s, uint32_t e0, uin
 #pragma unroll
     for (int k = 0; k < 9; ++k) rot[9 * size_t(t) + k] = H(s.op[size_t(k) * s.Tp + e]);
   }
-  if (plastic) {
+  if (plastic && s.hk) {
+#pragma unroll
+    for (int k = 0; k < 10; ++k) plastic[10 * size_t(t) + k] = H(s.hk[size_t(k) * s.Tp + e]);
+  } else if (plastic) {
     H* q = plastic + 10 * size_t(t);
     const Vec4<S> a0 = s.plast[e], a1 = s.plast[size_t(s.Tp) + e];
     q[0] = H(a0.x); q[1] = H(a0.w); q[2] = H(a1.x);
     q[3] = H(a0.w); q[4] = H(a0.y); q[5] = H(a1.y);
     q[6] = H(a1.x); q[7] = H(a1.y); q[8] = H(a0.z);
     q[9] = H(a1.z);
+  }
+}
+
+// -------------------------------------------- finite-strain plastic flow ----
+// returnMap (plasticflow.cc:110-150) of one point, FP64 like the reference:
+// the left stretch B = Fe Fe^T diagonalised by the cyclic Jacobi solve, log
+// strains 0.5 log(lambda), deviator d, q = sqrt(3/2) 2 mu |d|; past the yield
+// stress Fe <- V diag(exp(d (yield / q - 1))) V^T Fe.  False inside.
+__device__ inline bool henckyReturn(const M3<double>& fe, double shear, double yield, M3<double>& out,
+                                    double& strain, double& trial) {
+  double a[3][3], v[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      a[i][j] = fe.m[i][0] * fe.m[j][0] + fe.m[i][1] * fe.m[j][1] + fe.m[i][2] * fe.m[j][2];
+  jacobiEigen3(a, v);
+  if (!(fmin(a[0][0], fmin(a[1][1], a[2][2])) > 0.0)) return false;
+  const double l[3] = {0.5 * log(a[0][0]), 0.5 * log(a[1][1]), 0.5 * log(a[2][2])};
+  const double mean = (l[0] + l[1] + l[2]) / 3.0;
+  const double d[3] = {l[0] - mean, l[1] - mean, l[2] - mean};
+  const double size = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  const double stress = sqrt(1.5) * 2.0 * shear * size;
+  if (!(stress > yield) || size <= 1.0e-15) return false;
+  M3<double> c = zero3<double>();
+#pragma unroll
+  for (int k = 0; k < 3; ++k) addOuter(c, exp(d[k] * (yield / stress - 1.0)) * V3<double>{v[0][k], v[1][k], v[2][k]},
+                                       V3<double>{v[0][k], v[1][k], v[2][k]});
+  out = mul(c, fe);
+  trial = stress;
+  strain = (stress - yield) / (3.0 * shear);
+  return true;
+}
+
+// flowLattice (plasticflow.cc:184-247) once per step after the solve
+// (strainstep.cc:822-825), one point per tet, without the crush and the
+// plastic cap (tl_material has no crushStress / plasticMax; their defaults
+// are infinite).  The elastic map F P returns with the yield stress blended
+// toward the trial stress, (start + r q) / (1 + r), r = H / (3 mu); P becomes
+// F^-1 Fe,returned when it moves by more than 1e-12 (one-norm) and the
+// hardening variable grows by the returned strain.  Flowed tets are counted
+// into the body's yielding counter.
+template <class S>
+__global__ void __launch_bounds__(TILE) kHenckyFlow(Sys<S> s) {
+  const uint32_t tile = blockIdx.x, b = s.elem_tile_body[tile];
+  const uint32_t e = tile * TILE + threadIdx.x;
+  bool flowed = false;
+  if (e < s.body[b].elem_end) {
+    const MatDev m = s.mat[s.lane[e]];
+    if (m.yields) {
+      const uint4 t = __ldg(&s.tet[e]);
+      const uint32_t nodes[4] = {t.x, t.y, t.z, t.w};
+      V3<double> g[4];
+      gradientsOf<S>(s.dm, s.Tp, e, g);
+      M3<double> F = eye3<double>();
+#pragma unroll
+      for (int c = 0; c < 4; ++c) addOuter(F, cvt<double>(xyz(s.u[nodes[c]])), g[c]);
+      const double detF = det3(F);
+      if (detF > 0.0) {
+        M3<double> P;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) P.m[i][j] = s.hk[size_t(3 * i + j) * s.Tp + e];
+        const double hardening = s.hk[size_t(9) * s.Tp + e];
+        const double youngs = s.eyoung ? s.eyoung[e] : m.youngs;
+        const double mu = youngs * m.mu_unit;
+        const double hard = m.hardening;
+        const M3<double> fe = mul(F, P);
+        const double start = m.yield + hard * hardening;
+        M3<double> back;
+        double strain = 0.0, trial = 0.0;
+        if (henckyReturn(fe, mu, start, back, strain, trial)) {
+          const double ratio = hard / (3.0 * mu);
+          const double yieldNow = (start + ratio * trial) / (1.0 + ratio);
+          if (henckyReturn(fe, mu, yieldNow, back, strain, trial)) {
+            const M3<double> cof = cofactor(F);  // F^-1 = cof(F)^T / det F
+            M3<double> next = mul(transpose(cof), back);
+            double moved = 0.0;
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+              for (int j = 0; j < 3; ++j) {
+                next.m[i][j] /= detF;
+                moved += fabs(next.m[i][j] - P.m[i][j]);
+              }
+            if (moved > 1.0e-12) {
+#pragma unroll
+              for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) s.hk[size_t(3 * i + j) * s.Tp + e] = next.m[i][j];
+              s.hk[size_t(9) * s.Tp + e] = hardening + strain;
+              flowed = true;
+            }
+          }
+        }
+      }
+    }
+  }
+  const int n = __syncthreads_count(flowed);
+  if (threadIdx.x == 0 && n) {
+    atomicAdd(&s.yielding[b], uint32_t(n));
+    atomicOr(&s.acc[b].grew, 1u);
   }
 }
 

@@ -236,6 +236,7 @@ struct SystemBase {
   virtual int32_t step(const tl_settings& set, const double g[3], double dt, tl_step_report* reports) = 0;
   virtual void tune(uint32_t blocksPerSm, uint32_t graph) = 0;
   virtual void setSolver(uint32_t form) = 0;
+  virtual void setPlasticity(uint32_t mode) = 0;
   std::vector<uint32_t> trace;  // TL_FLAG_TRACE: iterations of each PCG launch (body 0)
   uint32_t bodies = 0;
   uint64_t nodes = 0, tets = 0;
@@ -319,6 +320,8 @@ struct System final : SystemBase {
   DevBuf<GridSyncDev> sync;
   bool hasEyoung = false;
   bool hasDamping = false;   // some element's lane has stiffness damping
+  bool hencky = false;       // TL_PLASTICITY_HENCKY: finite-strain flow from a per-tet plastic rest
+  DevBuf<double> hk;         // [10][Tp] plastic map P (row-major planes), hardening variable
   bool evaluating = false;   // tl_evaluate: element forces only, no damping terms
   DevBuf<S> dtau, dfit;
   // TL_FLAG_PROFILE: event pairs around kernel classes, resolved at step end
@@ -443,6 +446,7 @@ struct System final : SystemBase {
     s.yflag = yflagPtr;
     s.dtau = hasDamping ? dtau.ptr : nullptr;
     s.dfit = hasDamping ? dfit.ptr : nullptr;
+    s.hk = hencky ? hk.ptr : nullptr;
     return s;
   }
 
@@ -1076,6 +1080,7 @@ struct System final : SystemBase {
     if (profiling) mark(0, true);
     const bool damps = hasDamping && law == TL_LAW_COROTATED && !(mode & EM_COMMIT) && !evaluating;
     if (law == TL_LAW_SNH) kElement<S, 1><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass, mode, margin);
+    else if (hencky) kElement<S, 0, true><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass, mode, margin);
     else kElement<S, 0><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass, mode, margin);
     check();
     if (damps) {
@@ -1186,6 +1191,8 @@ struct System final : SystemBase {
     if (set.law > 1u) throw StatusError{TL_ERR_ARG, "unknown law"};
     if (hasDamping && set.law == TL_LAW_SNH)
       throw StatusError{TL_ERR_UNSUPPORTED, "stiffness damping is defined with the corotated law"};
+    if (hencky && (set.law != TL_LAW_COROTATED || hasDamping))
+      throw StatusError{TL_ERR_UNSUPPORTED, "the finite-strain flow is written for the corotated law without damping"};
     const int law = int(set.law);
     for (uint32_t b = 0; b < B; ++b)
       if (!hb[b].anyAnchored && set.rigid_split != TL_RIGID_SPLIT_OFF)
@@ -1195,10 +1202,10 @@ struct System final : SystemBase {
     tracing = (set.flags & TL_FLAG_TRACE) != 0u;
     evUsed.clear();
     {
-      const bool yieldsLaw = law == TL_LAW_COROTATED &&
+      const bool yieldsLaw = law == TL_LAW_COROTATED && !hencky &&
                              std::any_of(hb.begin(), hb.end(), [](const HostBody& h) { return h.anyYields; });
       const bool newtonNeeded = set.plastic_passes > 1u && yieldsLaw;
-      if (B > 1 && !newtonNeeded && tuneGraph && !graphBroken && !tracing) {
+      if (B > 1 && !newtonNeeded && tuneGraph && !graphBroken && !tracing && !hencky) {
         const int32_t rc = stepGraph(set, gvec, dt, reports, law, yieldsLaw);
         if (rc != TL_ERR_UNSUPPORTED) return rc;  // unsupported: capture refused, fall through to launches
       }
@@ -1254,14 +1261,14 @@ struct System final : SystemBase {
       s.hstep = std::sqrt((1.0 - rule.alphaForce) * rule.beta) * s.inner;
       s.scale = s.hstep * s.hstep;
       maxSub = std::max(maxSub, s.substeps);
-      const bool yieldsHere = hb[b].anyYields && law == TL_LAW_COROTATED;
+      const bool yieldsHere = hb[b].anyYields && law == TL_LAW_COROTATED && !hencky;
       anyNewton = anyNewton || (set.plastic_passes > 1u && yieldsHere);
     }
     if (anyNewton && B != 1u)
       throw StatusError{TL_ERR_UNSUPPORTED, "the plastic Newton path runs one body per system"};
     dStep.upload(hs, B, st);
     const bool anyYields = std::any_of(hb.begin(), hb.end(), [](const HostBody& h) { return h.anyYields; }) &&
-                           law == TL_LAW_COROTATED;
+                           law == TL_LAW_COROTATED && !hencky;
     std::vector<tl_step_report> local(B);
     for (uint32_t pass = 0; pass < maxSub; ++pass) {
       nodeOp(kPredict<S>, pass);
@@ -1272,6 +1279,11 @@ struct System final : SystemBase {
       }
       nodeOp(kUpdate<S>, pass);
       if (anyYields) element(law, u.ptr, nullptr, pass, EM_MAPPING | EM_COMMIT, 0.0);
+    }
+    if (hencky) {  // flowLattice once per step, after the solve (strainstep.cc:822-825)
+      yielding.zero(st);
+      kHenckyFlow<S><<<elemTiles, TILE, 0, st>>>(view());
+      check();
     }
     kStepEnd<S><<<nodeTiles, TILE, 0, st>>>(view());
     check();
@@ -1498,6 +1510,21 @@ struct System final : SystemBase {
   std::vector<std::pair<int, size_t>> graphEv;  // event pairs recorded by the captured graph
 
   void setSolver(uint32_t form) override { solverForm = form; }
+  // Every tet starts from its authored rest: P = I, hardening 0.
+  void setPlasticity(uint32_t mode) override {
+    if (mode != TL_PLASTICITY_HENCKY) {
+      hencky = false;
+      return;
+    }
+    if (!hk.ptr) hk.alloc(size_t(10) * Tp);
+    std::vector<double> h(size_t(10) * Tp, 0.0);
+    std::fill(h.begin(), h.begin() + Tp, 1.0);
+    std::fill(h.begin() + size_t(4) * Tp, h.begin() + size_t(5) * Tp, 1.0);
+    std::fill(h.begin() + size_t(8) * Tp, h.begin() + size_t(9) * Tp, 1.0);
+    hk.upload(h.data(), h.size(), st);
+    TL_CUDA(cudaStreamSynchronize(st));
+    hencky = true;
+  }
   void tune(uint32_t blocksPerSm, uint32_t graph) override {
     tuneBlocksPerSm = blocksPerSm;
     tuneGraph = graph != 0u;
@@ -1746,6 +1773,7 @@ struct Rollout final : RolloutBase {
 
   Rollout(System<S>& s, const tl_rollout_desc& desc, const tl_settings& settings) : sys(s), d(desc), set(settings) {
     if (sys.B != 1u) throw StatusError{TL_ERR_UNSUPPORTED, "a rollout runs on a one-body system"};
+    if (sys.hencky) throw StatusError{TL_ERR_UNSUPPORTED, "a rollout does not differentiate the plastic flow"};
     if (settings.law != TL_LAW_SNH)
       throw StatusError{TL_ERR_UNSUPPORTED, "the adjoint needs the exact tangent of TL_LAW_SNH"};
     if (!desc.steps || !desc.checkpoint_every || !desc.newton_reads || !(desc.delta_time > 0.0))
@@ -2011,6 +2039,15 @@ int32_t tl_system_set_solver(tl_system* system, uint32_t form) {
   if (!system || form > TL_SOLVER_ELEMENTWISE) return TL_ERR_ARG;
   system->impl->setSolver(form);
   return TL_OK;
+}
+
+int32_t tl_system_set_plasticity(tl_system* system, uint32_t mode) {
+  if (!system || mode > TL_PLASTICITY_HENCKY) return TL_ERR_ARG;
+  return guarded(system->ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(system->ctx->device));
+    system->impl->setPlasticity(mode);
+    return TL_OK;
+  });
 }
 
 int32_t tl_system_trace(const tl_system* system, uint32_t* iterations, uint32_t capacity, uint32_t* count) {

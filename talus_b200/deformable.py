@@ -88,15 +88,20 @@ class DeformableState:
                                self.rotation.copy(), self.plastic.copy())
 
 
-def rest_state(mesh: PreparedMesh) -> DeformableState:
+def rest_state(mesh: PreparedMesh, hencky: bool = False) -> DeformableState:
     """restState (solver.cc:2420-2453) at the identity pose.  Anchored nodes with
-    a prescribed velocity start moving with it."""
+    a prescribed velocity start moving with it.  ``hencky``: the plastic slot
+    holds the identity plastic map (P = I, hardening 0) that the finite-strain
+    flow starts from, instead of a zero plastic strain."""
     velocity = np.zeros((mesh.nodes, 3))
     if mesh.prescribed_velocity is not None:
         held = mesh.anchored != 0
         velocity[held] = mesh.prescribed_velocity[held]
+    plastic = np.zeros((mesh.tets, 10))
+    if hencky:
+        plastic[:, [0, 4, 8]] = 1.0
     return DeformableState(mesh.rest_positions.astype(np.float64).copy(), velocity, np.zeros((mesh.nodes, 3)),
-                           np.tile(np.eye(3), (mesh.tets, 1, 1)), np.zeros((mesh.tets, 10)))
+                           np.tile(np.eye(3), (mesh.tets, 1, 1)), plastic)
 
 
 @dataclass
@@ -251,6 +256,15 @@ class System:
         "elementwise" (applied element by element every iteration)."""
         code = {"auto": 0, "assembled": 1, "elementwise": 2}[form]
         check(capi.lib().tl_system_set_solver(self.handle, code), self.context.handle)
+
+    def set_plasticity(self, mode: str = "small_strain"):
+        """Plasticity of the yielding lanes (tl_system_set_plasticity):
+        "small_strain" (the tet law's J2 return inside the step) or "hencky"
+        (finite-strain flow after each step from a per-tet plastic rest
+        shape; the state's plastic slot then holds P = Fp^-1 row-major and
+        the hardening variable).  Resets every tet to P = I, hardening 0."""
+        code = {"small_strain": 0, "hencky": 1}[mode]
+        check(capi.lib().tl_system_set_plasticity(self.handle, code), self.context.handle)
 
     def trace(self) -> list:
         """Iterations of every PCG launch made with Settings.trace, oldest first."""
