@@ -190,9 +190,8 @@ int32_t tl_system_set_solver(tl_system* system, uint32_t form);
  * volume V / det P (plasticRest, plasticflow.cc:263-300).  After the solve,
  * every yielding tet with det F > 0 returns F P radially in log-stretch
  * space.  The yield stress is blended as (start + r q) / (1 + r), with
- * r = H / (3 mu), and P and a hardening variable are kept per tet.  There is
- * no crush and no plastic cap: tl_material has neither field, and the
- * reference defaults for both are infinite.
+ * r = H / (3 mu), and P and a hardening variable are kept per tet.  Crush
+ * and plastic cap come from tl_system_set_flow_limits.
  * With HENCKY, the plastic slot of tl_state_set/get holds P (9 values,
  * row-major) and then the hardening variable.  tl_step_report::yielding
  * counts the tets that flowed.  Setting a mode resets every tet to P = I and
@@ -201,6 +200,17 @@ int32_t tl_system_set_solver(tl_system* system, uint32_t form);
 #define TL_PLASTICITY_SMALL_STRAIN 0u
 #define TL_PLASTICITY_HENCKY 1u
 int32_t tl_system_set_plasticity(tl_system* system, uint32_t mode);
+
+/* PhysicalMaterial's crushStress, crushLimit and plasticMax (material.h:16-29)
+ * for material lane `lane` of body `body`, read by the finite-strain flow
+ * only (plasticflow.cc:196-240).  A lane with a finite crush stress and a
+ * crush limit < 1 compacts when squeezed below J = exp(-crushStress / K),
+ * until det Fp reaches the crush limit.  A finite plasticMax caps the
+ * Frobenius distance of Fp from I.  Defaults (no crush, no cap): +inf, 1,
+ * +inf.  crush_stress > 0, crush_limit in (0, 1], plastic_max > 0, else
+ * TL_ERR_ARG. */
+int32_t tl_system_set_flow_limits(tl_system* system, uint32_t body, uint32_t lane, double crush_stress,
+                                  double crush_limit, double plastic_max);
 
 /* Diagnostics, no reference counterpart: iteration counts (body 0) of the
  * PCG launches made while TL_FLAG_TRACE was set, oldest first, since the

@@ -265,27 +265,56 @@ inline double oneNorm(const M3<double>& m) {
   return total;
 }
 
-// plasticflow.cc:184-247 flowLattice at one point, without the crush and the
-// plastic cap (PhysicalMaterial::crushStress and plasticMax keep their
-// infinite defaults here): the elastic map F P returns with the yield stress
-// blended toward the trial stress, (start + r q) / (1 + r), r = H / (3 mu);
-// the plastic map becomes F^-1 F_e,returned and the hardening variable grows
-// by the returned strain.
+inline double frobenius(const M3<double>& m) {
+  return std::sqrt(dot(m[0], m[0]) + dot(m[1], m[1]) + dot(m[2], m[2]));
+}
+
+struct FlowLimits {
+  double crushStress = std::numeric_limits<double>::infinity(), crushLimit = 1.0;
+  double plasticMax = std::numeric_limits<double>::infinity();
+};
+
+// plasticflow.cc:184-247 flowLattice at one point.  The elastic map F P
+// returns with the yield stress blended toward the trial stress,
+// (start + r q) / (1 + r), r = H / (3 mu).  A crushable material
+// (finite crushStress, crushLimit < 1) squeezed below J = exp(-crushStress /
+// K) compacts by min(-crush - log J, room), room = -log(det P crushLimit).
+// The plastic map becomes F^-1 (grow F_e,returned); a plastic stretch Fp
+// further than plasticMax from I (Frobenius) is pulled back to that distance
+// at the same volume.  The hardening variable grows by the returned strain.
 inline bool henckyFlow(const M3<double>& deformation, M3<double>& plastic, double& hardening, double shear,
-                       double yieldStress, double hardeningModulus) {
+                       double bulk, double yieldStress, double hardeningModulus, const FlowLimits& limits) {
   if (!(determinant(deformation) > 0.0)) return false;
   const M3<double> elastic = deformation * plastic;
-  const double start = yieldStress + hardeningModulus * hardening;
   const double ratio = hardeningModulus / (3.0 * shear);
+  const bool crushable = std::isfinite(limits.crushStress) && limits.crushLimit < 1.0;
+  const double crush = limits.crushStress / bulk;
+  const double start = yieldStress + hardeningModulus * hardening;
+  const double room = crushable ? -std::log(determinant(plastic) * limits.crushLimit) : 0.0;
+  const bool squeezed = crushable && room > 0.0 && determinant(elastic) < std::exp(-crush);
   const HenckyReturn trial = henckyReturn(elastic, shear, start);
-  if (!trial.mapped) return false;
-  const double yieldNow = (start + ratio * trial.trial) / (1.0 + ratio);
-  const HenckyReturn mapped = henckyReturn(elastic, shear, yieldNow);
-  if (!mapped.mapped) return false;
-  const M3<double> next = inverse(deformation) * mapped.elastic;
+  const double yieldNow = trial.mapped ? (start + ratio * trial.trial) / (1.0 + ratio) : start;
+  const HenckyReturn mapped = trial.mapped ? henckyReturn(elastic, shear, yieldNow) : HenckyReturn{};
+  const M3<double> after = mapped.mapped ? mapped.elastic : elastic;
+  const double volume = determinant(after);
+  const double compaction = squeezed && volume > 0.0 ? std::min(-crush - std::log(volume), room) : 0.0;
+  if (!mapped.mapped && !(compaction > 0.0)) return false;
+  const double grow = compaction > 0.0 ? std::exp(compaction / 3.0) : 1.0;
+  M3<double> next = inverse(deformation) * (grow * after);
+  const double kept = determinant(next);
+  if (std::isfinite(limits.plasticMax) && kept > 0.0) {
+    const M3<double> stretch = inverse(next) - M3<double>(1.0);
+    const double size = frobenius(stretch);
+    if (size > limits.plasticMax) {
+      const M3<double> capped = M3<double>(1.0) + (limits.plasticMax / size) * stretch;
+      const double cappedVolume = determinant(capped);
+      if (!(cappedVolume > 1.0e-6)) return false;
+      next = std::cbrt(kept * cappedVolume) * inverse(capped);
+    }
+  }
   if (!(oneNorm(next - plastic) > 1.0e-12)) return false;
   plastic = next;
-  hardening += mapped.strain;
+  hardening += mapped.mapped ? mapped.strain : 0.0;
   return true;
 }
 
@@ -717,6 +746,7 @@ template <class R> struct Element {
   R yieldStress, hardening;
   bool yields;
   R tau;  // stiffness damping weight (factor.cc:755-759)
+  FlowLimits limits;  // finite-strain flow: crush and plastic cap
 };
 
 template <class R> struct Solver {
@@ -1003,7 +1033,9 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
     s.plasticCorners.resize(T);
   }
   bool anyYields = false;
-  static const or_material DEFAULT = {1000.0, 0.0, 0.3, 0.0, std::numeric_limits<double>::infinity(), 0.0};
+  static const or_material DEFAULT = {1000.0, 0.0, 0.3, 0.0, std::numeric_limits<double>::infinity(), 0.0,
+                                      std::numeric_limits<double>::infinity(), 1.0,
+                                      std::numeric_limits<double>::infinity()};
   for (uint32_t e = 0; e < T; ++e) {
     Element<R>& el = s.elements[e];
     for (int k = 0; k < 4; ++k) el.nodes[k] = mesh->tet_nodes[4 * e + k];
@@ -1017,6 +1049,7 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
     el.yieldStress = R(m.yield_stress);
     el.hardening = R(m.hardening_modulus);
     el.yields = yieldsAt(el.yieldStress);
+    el.limits = FlowLimits{m.crush_stress, m.crush_limit, m.plastic_max};
     anyYields = anyYields || el.yields;
     if (s.hencky) {
       const M3<double> given = loadRowMajor<double>(mesh->rest_inverse + 9 * e);
@@ -1329,8 +1362,9 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
         const V3<R>& p = s.position[el.nodes[k]];
         x[k] = V3<double>(double(p.x), double(p.y), double(p.z));
       }
-      if (henckyFlow(deformationOf(x, s.authored[e]), s.flowMap[e], s.hardeningOf[e], double(el.moduli.second),
-                     double(el.yieldStress), double(el.hardening)))
+      const double mu = double(el.moduli.second), bulk = double(el.moduli.first) + 2.0 * mu / 3.0;
+      if (henckyFlow(deformationOf(x, s.authored[e]), s.flowMap[e], s.hardeningOf[e], mu, bulk,
+                     double(el.yieldStress), double(el.hardening), el.limits))
         ++flowed;
     }
     report->yielding = flowed;
@@ -1601,11 +1635,12 @@ double or_hencky_von_mises(const double* elastic, double shear) {
   return henckyVonMises(loadRowMajor<double>(elastic), shear);
 }
 
-int or_hencky_flow(const double* deformation, double* plastic, double* hardening, double shear, double yield_stress,
-                   double hardening_modulus) {
+int or_hencky_flow(const double* deformation, double* plastic, double* hardening, double shear, double bulk,
+                   const or_material* material) {
   M3<double> p = loadRowMajor<double>(plastic);
-  const bool changed = henckyFlow(loadRowMajor<double>(deformation), p, *hardening, shear, yield_stress,
-                                  hardening_modulus);
+  const FlowLimits limits{material->crush_stress, material->crush_limit, material->plastic_max};
+  const bool changed = henckyFlow(loadRowMajor<double>(deformation), p, *hardening, shear, bulk, material->yield_stress,
+                                  material->hardening_modulus, limits);
   storeRowMajor(p, plastic);
   return changed ? 1 : 0;
 }

@@ -44,6 +44,11 @@ typedef struct or_material {
   double stiffness_damping;
   double yield_stress;
   double hardening_modulus;
+  /* finite-strain flow only (plasticflow.cc:196-240): PhysicalMaterial's
+   * crushStress (+inf: none), crushLimit (1: none) and plasticMax (+inf) */
+  double crush_stress;
+  double crush_limit;
+  double plastic_max;
 } or_material;
 
 typedef struct or_mesh {
@@ -177,11 +182,12 @@ int or_hencky_return(const double* elastic, double shear, double yield_stress, d
 /* plasticflow.cc:96-108 vonMises: sqrt(3/2) 2 shear |dev log V_e|. */
 double or_hencky_von_mises(const double* elastic, double shear);
 
-/* plasticflow.cc:184-247 flowLattice for one point (no crush, no cap):
- * deformation [9] F, plastic [9] P = Fp^-1 and *hardening updated in place.
- * Returns 1 when P changed. */
-int or_hencky_flow(const double* deformation, double* plastic, double* hardening, double shear,
-                   double yield_stress, double hardening_modulus);
+/* plasticflow.cc:184-247 flowLattice for one point: deformation [9] F,
+ * plastic [9] P = Fp^-1 and *hardening updated in place; shear and bulk
+ * moduli; the material's yield stress, hardening modulus, crush stress and
+ * limit and plastic cap.  Returns 1 when P changed. */
+int or_hencky_flow(const double* deformation, double* plastic, double* hardening, double shear, double bulk,
+                   const or_material* material);
 
 #ifdef __cplusplus
 }

@@ -34,6 +34,9 @@ class Material(C.Structure):
         ("stiffness_damping", C.c_double),
         ("yield_stress", C.c_double),
         ("hardening_modulus", C.c_double),
+        ("crush_stress", C.c_double),
+        ("crush_limit", C.c_double),
+        ("plastic_max", C.c_double),
     ]
 
 
@@ -144,7 +147,8 @@ def lib():
         _lib.or_hencky_return.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.or_hencky_von_mises.argtypes = [C.c_void_p, C.c_double]
         _lib.or_hencky_von_mises.restype = C.c_double
-        _lib.or_hencky_flow.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_double]
+        _lib.or_hencky_flow.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                        C.POINTER(Material)]
     return _lib
 
 
@@ -152,8 +156,9 @@ def _ptr(a):
     return None if a is None else a.ctypes.data
 
 
-def material(density=1000.0, youngs=1e6, poisson=0.3, damping=0.0, yield_stress=np.inf, hardening=0.0) -> Material:
-    return Material(density, youngs, poisson, damping, yield_stress, hardening)
+def material(density=1000.0, youngs=1e6, poisson=0.3, damping=0.0, yield_stress=np.inf, hardening=0.0,
+             crush_stress=np.inf, crush_limit=1.0, plastic_max=np.inf) -> Material:
+    return Material(density, youngs, poisson, damping, yield_stress, hardening, crush_stress, crush_limit, plastic_max)
 
 
 @dataclass
@@ -323,10 +328,11 @@ def hencky_von_mises(elastic, shear) -> float:
     return float(lib().or_hencky_von_mises(_ptr(np.ascontiguousarray(elastic, np.float64)), shear))
 
 
-def hencky_flow(deformation, plastic, hardening, shear, yield_stress, hardening_modulus):
-    """plasticflow.cc:184-247 flowLattice at one point: (changed, P, hardening)."""
+def hencky_flow(deformation, plastic, hardening, shear, bulk, mat: Material):
+    """plasticflow.cc:184-247 flowLattice at one point with the material's
+    yield stress, hardening, crush and plastic cap: (changed, P, hardening)."""
     f = np.ascontiguousarray(deformation, np.float64)
     p = np.array(plastic, np.float64, order="C")
     h = np.array([hardening], np.float64)
-    changed = lib().or_hencky_flow(_ptr(f), _ptr(p), _ptr(h), shear, yield_stress, hardening_modulus)
+    changed = lib().or_hencky_flow(_ptr(f), _ptr(p), _ptr(h), shear, bulk, C.byref(mat))
     return bool(changed), p, float(h[0])

@@ -198,6 +198,7 @@ template <class S> struct Sys {
                                // (xx, yy, zz, xy, xz, yz), damping coefficients (a, b)
   // finite-strain plastic flow (null unless the system's plasticity is Hencky)
   double* hk;                  // [10][Tp] plastic map P = Fp^-1 (9 planes, row-major), hardening variable
+  const double* flim;          // [3 lanes] per material lane: crush stress, crush limit, plastic cap
 };
 
 constexpr int TILE_OFF_STRIDE = 4 * TILE + 4;  // 4 TILE + 1 offsets, padded to 8-byte rows
@@ -1166,21 +1167,36 @@ __device__ inline bool henckyReturn(const M3<double>& fe, double shear, double y
   return true;
 }
 
+__device__ inline M3<double> inverse3(const M3<double>& a) {
+  const M3<double> c = cofactor(a);
+  const double inv = 1.0 / det3(a);
+  M3<double> r;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) r.m[i][j] = c.m[j][i] * inv;
+  return r;
+}
+
 // flowLattice (plasticflow.cc:184-247) once per step after the solve
-// (strainstep.cc:822-825), one point per tet, without the crush and the
-// plastic cap (tl_material has no crushStress / plasticMax; their defaults
-// are infinite).  The elastic map F P returns with the yield stress blended
-// toward the trial stress, (start + r q) / (1 + r), r = H / (3 mu); P becomes
-// F^-1 Fe,returned when it moves by more than 1e-12 (one-norm) and the
-// hardening variable grows by the returned strain.  Flowed tets are counted
-// into the body's yielding counter.
+// (strainstep.cc:822-825), one point per tet.  The elastic map F P returns
+// with the yield stress blended toward the trial stress, (start + r q) /
+// (1 + r), r = H / (3 mu).  A crushable lane (finite crush stress, crush
+// limit < 1) squeezed below J = exp(-crushStress / K) compacts by
+// min(-crush - log J, room), room = -log(det P crushLimit).  P becomes
+// F^-1 (grow Fe,returned); a plastic stretch Fp further than the lane's cap
+// from I (Frobenius) is pulled back to that distance at the same volume.  P
+// is written when it moves by more than 1e-12 (one-norm) and the hardening
+// variable grows by the returned strain.  Flowed tets are counted into the
+// body's yielding counter.
 template <class S>
 __global__ void __launch_bounds__(TILE) kHenckyFlow(Sys<S> s) {
   const uint32_t tile = blockIdx.x, b = s.elem_tile_body[tile];
   const uint32_t e = tile * TILE + threadIdx.x;
   bool flowed = false;
   if (e < s.body[b].elem_end) {
-    const MatDev m = s.mat[s.lane[e]];
+    const uint32_t lane = s.lane[e];
+    const MatDev m = s.mat[lane];
     if (m.yields) {
       const uint4 t = __ldg(&s.tet[e]);
       const uint32_t nodes[4] = {t.x, t.y, t.z, t.w};
@@ -1189,8 +1205,7 @@ __global__ void __launch_bounds__(TILE) kHenckyFlow(Sys<S> s) {
       M3<double> F = eye3<double>();
 #pragma unroll
       for (int c = 0; c < 4; ++c) addOuter(F, cvt<double>(xyz(s.u[nodes[c]])), g[c]);
-      const double detF = det3(F);
-      if (detF > 0.0) {
+      if (det3(F) > 0.0) {
         M3<double> P;
 #pragma unroll
         for (int i = 0; i < 3; ++i)
@@ -1198,34 +1213,72 @@ __global__ void __launch_bounds__(TILE) kHenckyFlow(Sys<S> s) {
           for (int j = 0; j < 3; ++j) P.m[i][j] = s.hk[size_t(3 * i + j) * s.Tp + e];
         const double hardening = s.hk[size_t(9) * s.Tp + e];
         const double youngs = s.eyoung ? s.eyoung[e] : m.youngs;
-        const double mu = youngs * m.mu_unit;
+        const double mu = youngs * m.mu_unit, bulk = youngs * m.lam_unit + 2.0 * mu / 3.0;
         const double hard = m.hardening;
+        const double crushStress = s.flim[3 * lane], crushLimit = s.flim[3 * lane + 1], cap = s.flim[3 * lane + 2];
+        const bool crushable = isfinite(crushStress) && crushLimit < 1.0;
+        const double crush = crushStress / bulk;
         const M3<double> fe = mul(F, P);
         const double start = m.yield + hard * hardening;
-        M3<double> back;
+        const double room = crushable ? -log(det3(P) * crushLimit) : 0.0;
+        const bool squeezed = crushable && room > 0.0 && det3(fe) < exp(-crush);
+        M3<double> back = fe;
         double strain = 0.0, trial = 0.0;
+        bool mapped = false;
         if (henckyReturn(fe, mu, start, back, strain, trial)) {
           const double ratio = hard / (3.0 * mu);
           const double yieldNow = (start + ratio * trial) / (1.0 + ratio);
-          if (henckyReturn(fe, mu, yieldNow, back, strain, trial)) {
-            const M3<double> cof = cofactor(F);  // F^-1 = cof(F)^T / det F
-            M3<double> next = mul(transpose(cof), back);
-            double moved = 0.0;
+          mapped = henckyReturn(fe, mu, yieldNow, back, strain, trial);
+        }
+        const M3<double> after = mapped ? back : fe;
+        const double volume = det3(after);
+        const double compaction = squeezed && volume > 0.0 ? fmin(-crush - log(volume), room) : 0.0;
+        if (mapped || compaction > 0.0) {
+          const double grow = compaction > 0.0 ? exp(compaction / 3.0) : 1.0;
+          M3<double> grown = after;
 #pragma unroll
-            for (int i = 0; i < 3; ++i)
+          for (int i = 0; i < 3; ++i)
 #pragma unroll
-              for (int j = 0; j < 3; ++j) {
-                next.m[i][j] /= detF;
-                moved += fabs(next.m[i][j] - P.m[i][j]);
-              }
-            if (moved > 1.0e-12) {
+            for (int j = 0; j < 3; ++j) grown.m[i][j] *= grow;
+          M3<double> next = mul(inverse3(F), grown);
+          const double kept = det3(next);
+          bool keep = true;
+          if (isfinite(cap) && kept > 0.0) {
+            M3<double> stretch = inverse3(next);
+            stretch.m[0][0] -= 1.0;
+            stretch.m[1][1] -= 1.0;
+            stretch.m[2][2] -= 1.0;
+            const double size = sqrt(contract(stretch, stretch));
+            if (size > cap) {
+              M3<double> capped;
 #pragma unroll
               for (int i = 0; i < 3; ++i)
 #pragma unroll
-                for (int j = 0; j < 3; ++j) s.hk[size_t(3 * i + j) * s.Tp + e] = next.m[i][j];
-              s.hk[size_t(9) * s.Tp + e] = hardening + strain;
-              flowed = true;
+                for (int j = 0; j < 3; ++j) capped.m[i][j] = (i == j ? 1.0 : 0.0) + (cap / size) * stretch.m[i][j];
+              const double cappedVolume = det3(capped);
+              keep = cappedVolume > 1.0e-6;
+              if (keep) {
+                const double scale = cbrt(kept * cappedVolume);
+                next = inverse3(capped);
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                  for (int j = 0; j < 3; ++j) next.m[i][j] *= scale;
+              }
             }
+          }
+          double moved = 0.0;
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) moved += fabs(next.m[i][j] - P.m[i][j]);
+          if (keep && moved > 1.0e-12) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+              for (int j = 0; j < 3; ++j) s.hk[size_t(3 * i + j) * s.Tp + e] = next.m[i][j];
+            s.hk[size_t(9) * s.Tp + e] = hardening + (mapped ? strain : 0.0);
+            flowed = true;
           }
         }
       }

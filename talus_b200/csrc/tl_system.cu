@@ -205,6 +205,7 @@ void parallelCopy(void* dst, const void* src, size_t bytes) {
 
 struct HostBody {
   uint32_t nodes = 0, tets = 0;
+  uint32_t laneBase = 0, lanes = 0;  // the body's material lanes in the system's lane table
   bool anyAnchored = false, anyYields = false;
   std::vector<double> rest;  // [3 V] for position <-> displacement
 };
@@ -237,6 +238,8 @@ struct SystemBase {
   virtual void tune(uint32_t blocksPerSm, uint32_t graph) = 0;
   virtual void setSolver(uint32_t form) = 0;
   virtual void setPlasticity(uint32_t mode) = 0;
+  virtual void setFlowLimits(uint32_t body, uint32_t lane, double crushStress, double crushLimit,
+                             double plasticMax) = 0;
   std::vector<uint32_t> trace;  // TL_FLAG_TRACE: iterations of each PCG launch (body 0)
   uint32_t bodies = 0;
   uint64_t nodes = 0, tets = 0;
@@ -272,6 +275,8 @@ struct System final : SystemBase {
   DevBuf<BodyDev> dBody;
   DevBuf<BodyStepDev> dStep;
   DevBuf<MatDev> dMat;
+  DevBuf<double> dFlim;          // [3 lanes] crush stress, crush limit, plastic cap (finite-strain flow)
+  std::vector<double> hFlim;
   DevBuf<uint32_t> dNodeTileBody, dElemTileBody;
   DevBuf<Vec4<S>> rest4, pres, u, v, a, carried, shifted, weighted, total, incr, lowest, right, pre0, pre1, r, z, p, ap, w;
   DevBuf<uint8_t> anch;
@@ -378,6 +383,7 @@ struct System final : SystemBase {
     s.body = dBody.ptr;
     s.step = dStep.ptr;
     s.mat = dMat.ptr;
+    s.flim = dFlim.ptr;
     s.node_tile_body = dNodeTileBody.ptr;
     s.elem_tile_body = dElemTileBody.ptr;
     s.rest4 = rest4.ptr;
@@ -503,6 +509,8 @@ struct System final : SystemBase {
       for (uint32_t t = bd.node_tile_begin; t < bd.node_tile_end; ++t) hNodeTileBody[t] = b;
       for (uint32_t t = bd.elem_tile_begin; t < bd.elem_tile_end; ++t) hElemTileBody[t] = b;
       const uint32_t laneBase = uint32_t(hMat.size());
+      h.laneBase = laneBase;
+      h.lanes = d.lanes;
       for (uint32_t l = 0; l <= d.lanes; ++l) {
         tl_material m = l < d.lanes ? d.materials[l]
                                     : tl_material{1000.0, 0.0, 0.3, 0.0, std::numeric_limits<double>::infinity(), 0.0};
@@ -578,6 +586,15 @@ struct System final : SystemBase {
     dStep.alloc(B);
     dMat.alloc(hMat.size());
     dMat.upload(hMat.data(), hMat.size(), st);
+    // PhysicalMaterial defaults (material.h:16-29): no crush, crush limit 1, no plastic cap
+    hFlim.resize(size_t(3) * hMat.size());
+    for (size_t l = 0; l < hMat.size(); ++l) {
+      hFlim[3 * l] = std::numeric_limits<double>::infinity();
+      hFlim[3 * l + 1] = 1.0;
+      hFlim[3 * l + 2] = std::numeric_limits<double>::infinity();
+    }
+    dFlim.alloc(hFlim.size());
+    dFlim.upload(hFlim.data(), hFlim.size(), st);
     dNodeTileBody.alloc(nodeTiles);
     dNodeTileBody.upload(hNodeTileBody.data(), nodeTiles, st);
     dElemTileBody.alloc(elemTiles);
@@ -1510,6 +1527,15 @@ struct System final : SystemBase {
   std::vector<std::pair<int, size_t>> graphEv;  // event pairs recorded by the captured graph
 
   void setSolver(uint32_t form) override { solverForm = form; }
+  void setFlowLimits(uint32_t b, uint32_t lane, double crushStress, double crushLimit, double plasticMax) override {
+    if (b >= B || lane >= hb[b].lanes) throw StatusError{TL_ERR_ARG, "no such body or material lane"};
+    const size_t at = size_t(3) * (hb[b].laneBase + lane);
+    hFlim[at] = crushStress;
+    hFlim[at + 1] = crushLimit;
+    hFlim[at + 2] = plasticMax;
+    dFlim.upload(hFlim.data() + at, 3, st, at);
+    TL_CUDA(cudaStreamSynchronize(st));
+  }
   // Every tet starts from its authored rest: P = I, hardening 0.
   void setPlasticity(uint32_t mode) override {
     if (mode != TL_PLASTICITY_HENCKY) {
@@ -2046,6 +2072,19 @@ int32_t tl_system_set_plasticity(tl_system* system, uint32_t mode) {
   return guarded(system->ctx, [&]() -> int32_t {
     TL_CUDA(cudaSetDevice(system->ctx->device));
     system->impl->setPlasticity(mode);
+    return TL_OK;
+  });
+}
+
+int32_t tl_system_set_flow_limits(tl_system* system, uint32_t body, uint32_t lane, double crush_stress,
+                                  double crush_limit, double plastic_max) {
+  // crushStress > 0 (+inf: none), crushLimit in (0, 1] (1: none), plasticMax > 0 (+inf: none)
+  if (!system || std::isnan(crush_stress) || !(crush_stress > 0.0) || !(crush_limit > 0.0) ||
+      !(crush_limit <= 1.0) || std::isnan(plastic_max) || !(plastic_max > 0.0))
+    return TL_ERR_ARG;
+  return guarded(system->ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(system->ctx->device));
+    system->impl->setFlowLimits(body, lane, crush_stress, crush_limit, plastic_max);
     return TL_OK;
   });
 }

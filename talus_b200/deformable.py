@@ -41,6 +41,11 @@ class PhysicalMaterial:
     stiffness_damping: float = 0.0
     yield_stress: float = math.inf
     hardening_modulus: float = 0.0
+    # finite-strain flow only (System.set_plasticity("hencky")); applied per
+    # lane through tl_system_set_flow_limits, not part of tl_material
+    crush_stress: float = math.inf
+    crush_limit: float = 1.0
+    plastic_max: float = math.inf
 
     def _c(self) -> capi.tl_material:
         return capi.tl_material(self.density, self.youngs_modulus, self.poissons_ratio, self.stiffness_damping,
@@ -201,6 +206,12 @@ class System:
         check(capi.lib().tl_system_create(self.context.handle, descs, len(self._bodies), precision,
                                           C.byref(handle)), self.context.handle)
         self.handle = handle
+        default = (math.inf, 1.0, math.inf)
+        for b, mats in enumerate(materials):
+            for lane, m in enumerate(mats):
+                limits = (m.crush_stress, m.crush_limit, m.plastic_max)
+                if limits != default:
+                    check(capi.lib().tl_system_set_flow_limits(handle, b, lane, *limits), self.context.handle)
 
     def close(self):
         if getattr(self, "handle", None):

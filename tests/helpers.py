@@ -18,7 +18,7 @@ def to_oracle(mesh: tb.PreparedMesh) -> po.Mesh:
 
 def oracle_material(m: tb.PhysicalMaterial) -> po.Material:
     return po.material(m.density, m.youngs_modulus, m.poissons_ratio, m.stiffness_damping, m.yield_stress,
-                       m.hardening_modulus)
+                       m.hardening_modulus, m.crush_stress, m.crush_limit, m.plastic_max)
 
 
 def oracle_settings(s: tb.Settings) -> po.Settings:

@@ -125,3 +125,44 @@ def test_hencky_refusals():
         d.step(tb.Settings(), GRAVITY, DT)
     assert err.value.status == capi.TL_ERR_UNSUPPORTED
     d.close()
+
+
+@pytest.mark.parametrize("limits", [dict(plastic_max=0.02), dict(crush_stress=2.0e4, crush_limit=0.95)],
+                         ids=["cap", "crush"])
+def test_flow_limits_match_the_oracle_and_hold(limits):
+    """A plastic cap (plasticMax) and a crushable lane (crushStress,
+    crushLimit) set through tl_system_set_flow_limits: FP64 parity with the
+    oracle, and the limits hold on every tet (plasticflow.cc:196-240)."""
+    mesh, mat = plastic_block()
+    for k, v in limits.items():
+        setattr(mat, k, v)
+    steps = 8
+    ost, ref, oflowed = oracle_run(mesh, mat, steps)
+    s = gpu_system([mesh], [[mat]], tb.FP64)
+    for n in range(steps):
+        rep = s.step(tb.Settings(), GRAVITY, DT)[0]
+        assert relative_error(s.get_state().position, ref[n], mesh.rest_positions) <= 1e-9, n
+        assert rep.yielding == oflowed[n], n
+    got = s.get_state()
+    s.close()
+    assert np.abs(got.plastic - ost.plastic).max() <= 1e-9 * max(1.0, np.abs(ost.plastic).max())
+    stretch = np.linalg.inv(got.plastic[:, :9].reshape(-1, 3, 3))
+    if "plastic_max" in limits:
+        distance = np.linalg.norm(stretch - np.eye(3), axis=(1, 2))
+        assert distance.max() <= limits["plastic_max"] + 1e-9 and distance.max() > 0.5 * limits["plastic_max"]
+    else:
+        kept = np.linalg.det(stretch)
+        assert kept.min() >= limits["crush_limit"] - 1e-9 and kept.min() < 0.999
+
+
+def test_flow_limit_arguments_are_checked():
+    mesh, mat = plastic_block((4, 3, 2))
+    s = gpu_system([mesh], [[mat]], tb.FP64)
+    lib = capi.lib()
+    assert lib.tl_system_set_flow_limits(s.handle, 0, 0, 1e3, 0.5, 1.0) == capi.TL_OK
+    assert lib.tl_system_set_flow_limits(s.handle, 0, 1, 1e3, 0.5, 1.0) == capi.TL_ERR_ARG  # one lane only
+    assert lib.tl_system_set_flow_limits(s.handle, 1, 0, 1e3, 0.5, 1.0) == capi.TL_ERR_ARG  # one body only
+    assert lib.tl_system_set_flow_limits(s.handle, 0, 0, -1.0, 0.5, 1.0) == capi.TL_ERR_ARG
+    assert lib.tl_system_set_flow_limits(s.handle, 0, 0, 1e3, 1.5, 1.0) == capi.TL_ERR_ARG
+    assert lib.tl_system_set_flow_limits(s.handle, 0, 0, 1e3, 0.5, float("nan")) == capi.TL_ERR_ARG
+    s.close()

@@ -1,11 +1,13 @@
 """The finite-strain (Hencky) plastic flow in the oracle, CPU.
 
 Known answers restated from the reference's own tests of returnMap and
-flowLattice (tests/dynamics_strainstep_tests.cc:3090-3135): a point inside
-its yield surface stays elastic; a point past it returns onto the surface and
-keeps its volume, with strain = (q - yield) / (3 mu); after a flow the
-elastic map's von Mises stress equals the hardened yield stress
-yield + H * hardening.  Then the flow inside the oracle's tet step
+flowLattice (tests/dynamics_strainstep_tests.cc:3090-3191), at one point: a
+point inside its yield surface stays elastic; a point past it returns onto
+the surface and keeps its volume, with strain = (q - yield) / (3 mu); after a
+flow the elastic map's von Mises stress equals the hardened yield stress
+yield + H * hardening; repeated pulls keep the plastic stretch within its cap;
+repeated squeezes crush no further than the crush limit.  Then the flow
+inside the oracle's tet step
 (plasticflow.cc:184-247 once per step, elastic steps from the plastic rest
 shape of plasticflow.cc:263-300).
 """
@@ -15,6 +17,14 @@ import pytest
 import talus_b200 as tb
 from oracle import pyoracle as po
 from tests.helpers import DT, GRAVITY, elastic_block, oracle_material, plastic_block, relative_error, to_oracle
+
+
+def moduli(youngs, poisson):
+    """(shear, bulk) of the tet law (lame, material.cc:71-78)."""
+    nu = min(max(poisson, 0.0), 0.49)
+    lam = youngs * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = youngs / (2 * (1 + nu))
+    return mu, lam + 2 * mu / 3
 
 
 def columns(*cols):
@@ -43,25 +53,53 @@ def test_point_past_yield_returns_onto_the_surface_and_keeps_its_volume():
 def test_flow_hardens_as_the_hardening_modulus_says(hardening):
     # dynamics_strainstep_tests.cc:3107-3135 at one point: a shear x += 0.2 y
     shear, yield_stress = 1.0e5, 2.0e3
+    mat = po.material(youngs=2.7e5, poisson=0.35, yield_stress=yield_stress, hardening=hardening)
     deformation = np.eye(3)
     deformation[0, 1] = 0.2
-    changed, plastic, alpha = po.hencky_flow(deformation, np.eye(3), 0.0, shear, yield_stress, hardening)
+    changed, plastic, alpha = po.hencky_flow(deformation, np.eye(3), 0.0, shear, 3e5, mat)
     assert changed and alpha > 0.0
     yield_now = yield_stress + hardening * alpha
     assert abs(po.hencky_von_mises(deformation @ plastic, shear) - yield_now) <= 1.0e-6 * yield_now
     # the return is deviatoric: the plastic map keeps volume
     assert abs(np.linalg.det(plastic) - 1.0) <= 1e-12
     # flowing again from the returned state moves nothing
-    again, plastic2, alpha2 = po.hencky_flow(deformation, plastic, alpha, shear, yield_stress, hardening)
+    again, plastic2, alpha2 = po.hencky_flow(deformation, plastic, alpha, shear, 3e5, mat)
     assert not again and np.array_equal(plastic2, plastic) and alpha2 == alpha
 
 
 def test_inverted_or_elastic_points_do_not_flow():
+    mat = po.material(youngs=2.7e5, poisson=0.35, yield_stress=1e3)
     flipped = np.diag([1.0, 1.0, -0.5])
-    assert not po.hencky_flow(flipped, np.eye(3), 0.0, 1e5, 1e3, 0.0)[0]
+    assert not po.hencky_flow(flipped, np.eye(3), 0.0, 1e5, 3e5, mat)[0]
     small = np.eye(3)
     small[0, 1] = 1e-4
-    assert not po.hencky_flow(small, np.eye(3), 0.0, 1e5, 1e3, 0.0)[0]
+    assert not po.hencky_flow(small, np.eye(3), 0.0, 1e5, 3e5, mat)[0]
+
+
+def test_plastic_stretch_stays_within_its_cap():
+    # dynamics_strainstep_tests.cc:3137-3167: clay(5e3, 50) (nu 0.35, plasticMax 1)
+    # pulled to stretch 2..7 along x, 1/stretch along y, one flow per pull
+    mat = po.material(youngs=5.0e3, poisson=0.35, yield_stress=50.0, plastic_max=1.0)
+    shear, bulk = moduli(5.0e3, 0.35)
+    plastic, alpha = np.eye(3), 0.0
+    for pull in range(1, 7):
+        stretch = 1.0 + pull
+        _, plastic, alpha = po.hencky_flow(np.diag([stretch, 1.0 / stretch, 1.0]), plastic, alpha, shear, bulk, mat)
+    distance = np.linalg.norm(np.linalg.inv(plastic) - np.eye(3))
+    assert distance > 0.5 and distance <= 1.0 + 1e-9
+
+
+def test_squeezed_point_crushes_no_further_than_its_limit():
+    # dynamics_strainstep_tests.cc:3169-3191: clay(1e5, 1e9), crushStress 1e3,
+    # crushLimit 0.7, squeezed to 0.6 of its size ten times
+    mat = po.material(youngs=1.0e5, poisson=0.35, yield_stress=1.0e9, crush_stress=1.0e3, crush_limit=0.7)
+    shear, bulk = moduli(1.0e5, 0.35)
+    plastic, alpha = np.eye(3), 0.0
+    for _ in range(10):
+        _, plastic, alpha = po.hencky_flow(0.6 * np.eye(3), plastic, alpha, shear, bulk, mat)
+    kept = np.linalg.det(np.linalg.inv(plastic))
+    assert kept < 0.99 and kept >= 0.7 - 1e-9
+    assert alpha == 0.0  # compaction alone: nothing returned, no hardening
 
 
 def run(mesh, mat, plasticity, steps, law=po.LAW_COROTATED):
