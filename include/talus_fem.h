@@ -147,6 +147,14 @@ int32_t tl_ctx_create(int32_t device, tl_ctx** out);
 int32_t tl_ctx_destroy(tl_ctx* ctx);
 const char* tl_ctx_last_error(const tl_ctx* ctx);
 
+/* Failure-detection self test, no reference counterpart.  Launches one block
+ * at the grid barrier of the persistent PCG kernels, waiting for an arrival
+ * that never comes.  The wait is bounded (2 s), so it runs out and the call
+ * returns TL_ERR_TIMEOUT, the status a stalled persistent kernel reports.
+ * The context stays usable.  Exercises the timeout path without faulting or
+ * hanging the GPU. */
+int32_t tl_ctx_check_wait_limit(tl_ctx* ctx);
+
 /* Upload one or more bodies (a batch when count > 1) into one resident
  * system.  Replaces buildMesh's output handling + refreshStiffness +
  * buildIncidence (solver.cc:453-507, 1065-1101): the node->element CSR

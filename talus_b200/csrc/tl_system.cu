@@ -2019,6 +2019,37 @@ int32_t tl_ctx_destroy(tl_ctx* ctx) {
 
 const char* tl_ctx_last_error(const tl_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
 
+}  // extern "C"
+
+namespace {
+// One block at the persistent kernels' grid barrier with one barrier already
+// counted: the goal (two arrivals) needs an arrival that never comes, so the
+// bounded wait runs out and records TL_ERR_TIMEOUT.
+__global__ void __launch_bounds__(TILE) kWaitLimitCheck(GridSyncDev* sync) {
+  unsigned int k = 1;
+  (void)countBarrier(sync, k);
+}
+}  // namespace
+
+extern "C" {
+
+int32_t tl_ctx_check_wait_limit(tl_ctx* ctx) {
+  if (!ctx) return TL_ERR_ARG;
+  return guarded(ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(ctx->device));
+    DevBuf<GridSyncDev> sync;
+    sync.alloc(1);
+    sync.zero(ctx->stream);
+    kWaitLimitCheck<<<1, TILE, 0, ctx->stream>>>(sync.ptr);
+    TL_CUDA(cudaGetLastError());
+    GridSyncDev h{};
+    sync.download(&h, 1, ctx->stream);
+    TL_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (h.error != 0) return fail(ctx, TL_ERR_TIMEOUT, "the grid barrier's bounded wait ran out (self test)");
+    return TL_OK;
+  });
+}
+
 int32_t tl_system_create(tl_ctx* ctx, const tl_mesh_desc* bodies, uint32_t count, int32_t precision,
                          tl_system** out) {
   if (!ctx || !bodies || !count || !out) return TL_ERR_ARG;

@@ -1,0 +1,38 @@
+"""Failure detection on the GPU without a GPU fault.
+
+Every spin in the persistent kernels is bounded (2 s on the grid barrier);
+when it runs out the kernel records TL_ERR_TIMEOUT in a status word the host
+reads, and the context stays usable.  tl_ctx_check_wait_limit makes that wait
+run out: one block waits at the barrier for an arrival that never comes.
+Afterwards the same context steps a body normally.  The host-side failure
+paths (a rank that raises, never joins) are covered with gloo ranks in
+test_shard.
+"""
+import time
+
+import numpy as np
+import pytest
+
+import talus_b200 as tb
+from talus_b200 import _capi as capi
+from tests.helpers import DT, GRAVITY, elastic_block
+
+pytestmark = pytest.mark.gpu
+
+
+def test_bounded_wait_runs_out_with_a_status_and_the_context_stays_usable():
+    ctx = tb.Context(0)
+    began = time.perf_counter()
+    rc = capi.lib().tl_ctx_check_wait_limit(ctx.handle)
+    waited = time.perf_counter() - began
+    assert rc == capi.TL_ERR_TIMEOUT
+    assert 1.5 < waited < 30.0
+    assert b"bounded wait" in capi.lib().tl_ctx_last_error(ctx.handle)
+    mesh, mat = elastic_block((4, 4, 4), seed=6)
+    system = tb.System(mesh, [mat], tb.FP64, context=ctx)
+    system.set_state(tb.rest_state(mesh))
+    report = system.step(tb.Settings(), GRAVITY, DT)[0]
+    assert report.cg_iterations > 0
+    assert np.isfinite(system.get_state().position).all()
+    system.close()
+    ctx.close()
