@@ -33,6 +33,11 @@ TL_RIGID_SPLIT_UNPROJECTED = 1
 TL_RIGID_SPLIT_PROJECTED = 2
 TL_FLAG_PROFILE = 1
 TL_FLAG_TRACE = 2
+TL_SOLVER_AUTO = 0
+TL_SOLVER_ASSEMBLED = 1
+TL_SOLVER_ELEMENTWISE = 2
+TL_PLASTICITY_SMALL_STRAIN = 0
+TL_PLASTICITY_HENCKY = 1
 
 
 class tl_material(C.Structure):

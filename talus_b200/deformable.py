@@ -265,7 +265,8 @@ class System:
         """PCG operator form of a single-body system (tl_system_set_solver):
         "auto", "assembled" (3x3 node blocks assembled once per solve) or
         "elementwise" (applied element by element every iteration)."""
-        code = {"auto": 0, "assembled": 1, "elementwise": 2}[form]
+        code = {"auto": capi.TL_SOLVER_AUTO, "assembled": capi.TL_SOLVER_ASSEMBLED,
+                "elementwise": capi.TL_SOLVER_ELEMENTWISE}[form]
         check(capi.lib().tl_system_set_solver(self.handle, code), self.context.handle)
 
     def set_plasticity(self, mode: str = "small_strain"):
@@ -274,7 +275,7 @@ class System:
         (finite-strain flow after each step from a per-tet plastic rest
         shape; the state's plastic slot then holds P = Fp^-1 row-major and
         the hardening variable).  Resets every tet to P = I, hardening 0."""
-        code = {"small_strain": 0, "hencky": 1}[mode]
+        code = {"small_strain": capi.TL_PLASTICITY_SMALL_STRAIN, "hencky": capi.TL_PLASTICITY_HENCKY}[mode]
         check(capi.lib().tl_system_set_plasticity(self.handle, code), self.context.handle)
 
     def trace(self) -> list:

@@ -55,6 +55,16 @@ def test_struct_layout_matches_the_header():
             assert table[(name, field)] == getattr(cls, field).offset, (name, field)
 
 
+def test_python_constants_match_the_header():
+    import re
+
+    defines = dict(re.findall(r"#define (TL_[A-Z0-9_]+) (\d+)u?\b", open(HEADER).read()))
+    named = {k: v for k, v in vars(capi).items() if k.startswith("TL_") and isinstance(v, int)}
+    assert named, "no TL_ constants in the binding"
+    for k, v in named.items():
+        assert k in defines and int(defines[k]) == v, k
+
+
 def test_header_compiles_as_c_and_cpp():
     with tempfile.TemporaryDirectory() as d:
         for comp, ext in (("gcc", "c"), ("g++", "cc")):
@@ -83,6 +93,9 @@ def test_calls_without_device_work():
     assert lib.tl_rollout_forward(None, None, None) == capi.TL_ERR_ARG
     assert lib.tl_rollout_adjoint(None, None, None, None, None, None, None) == capi.TL_ERR_ARG
     assert lib.tl_rollout_destroy(None) == capi.TL_ERR_ARG
+    assert lib.tl_system_set_plasticity(None, capi.TL_PLASTICITY_HENCKY) == capi.TL_ERR_ARG
+    assert lib.tl_system_set_flow_limits(None, 0, 0, 1e3, 0.5, 1.0) == capi.TL_ERR_ARG
+    assert lib.tl_ctx_check_wait_limit(None) == capi.TL_ERR_ARG
 
 
 def _has_gpu():
