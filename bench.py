@@ -572,6 +572,9 @@ def run_ours(args, spec, rank, world, dist):
             result["fp64"]["converged_check"] = converged_check(meshes, mats, law, context)
     if not args.no_adjoint:
         result["adjoint"] = adjoint_ratio(precision, context)
+    yields = any(np.isfinite(m.yield_stress) and m.yield_stress > 0 for ms in mats for m in ms)
+    if not args.no_hencky and not spec.get("batch") and yields:
+        result["hencky"] = hencky_form(meshes[0], mats[0], settings, context)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_sample(spec)
         result["cpu_baseline"]["cpu"] = cpu_info()
@@ -655,6 +658,38 @@ def converged_check(meshes, mats, law, context, steps=8, tolerance=1e-6, cap=300
             "max_rel_displacement_error": worst}
 
 
+def hencky_form(mesh, mats, settings, context, warmup=3, steps=10):
+    """The same body in the finite-strain plasticity mode
+    (tl_system_set_plasticity(TL_PLASTICITY_HENCKY): elastic steps from each
+    tet's plastic rest shape, then the flow kernel), FP32-mixed and FP64 from
+    rest: throughput from the library's per-step device time, and the mixed
+    error against FP64 after warmup + steps steps."""
+    import talus_b200 as tb
+
+    plain = tb.Settings(law=settings.law)
+    out, finals = {}, {}
+    for name, precision in (("mixed", tb.FP32_MIXED), ("fp64", tb.FP64)):
+        s = tb.System(mesh, mats, precision, context)
+        s.set_plasticity("hencky")
+        s.set_state(tb.rest_state(mesh, hencky=True))
+        seconds, flowed = 0.0, 0
+        for k in range(warmup + steps):
+            rep = s.step(plain)[0]
+            if k >= warmup:
+                seconds += rep.device_seconds
+                flowed = rep.yielding
+        finals[name] = s.get_state().position
+        s.close()
+        out[name] = {"value": mesh.tets * steps / seconds, "ms_per_step": seconds * 1e3 / steps,
+                     "flowed_tets_last_step": int(flowed)}
+    scale = np.linalg.norm(finals["fp64"] - mesh.rest_positions, axis=1).max()
+    out["max_rel_displacement_error"] = float(np.linalg.norm(finals["mixed"] - finals["fp64"], axis=1).max() / scale)
+    out["unit"] = UNIT
+    out["note"] = (f"plasticity mode 'hencky' on the same body; {warmup} warm-up and {steps} timed steps from rest; "
+                   f"device time per step from the step reports")
+    return out
+
+
 def adjoint_ratio(precision, context, repeats=3):
     """Differentiable-rollout workload: 16^3 cubes (24,576 tets), 30 steps,
     checkpoints every 5, loss |x_T - x_target|^2; device time of the adjoint
@@ -689,6 +724,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-converged-check", action="store_true")
+    ap.add_argument("--no-hencky", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -250,7 +250,10 @@ int32_t tl_step(tl_system* system, const tl_settings* settings, const double gra
  * memory).  Same buffer layout as tl_state_set/get.  The rotations are
  * written, not read: a step sets every committed rotation before it uses
  * one (assembleElastic, solver.cc:1404-1547), so they are not uploaded and
- * tl_state_set callers may pass NULL for them before tl_step. */
+ * tl_state_set callers may pass NULL for them before tl_step.  The plastic
+ * slot crosses only when the step uses it (a yielding lane under the
+ * corotated law, or TL_PLASTICITY_HENCKY); otherwise the caller's buffer is
+ * left as it is, which is the state the step leaves. */
 int32_t tl_step_host(tl_system* system, uint32_t body, int32_t dtype, void* position, void* velocity,
                      void* acceleration, void* rotation, void* plastic, const tl_settings* settings,
                      const double gravity[3], double dt, tl_step_report* report);

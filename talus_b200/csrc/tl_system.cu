@@ -238,6 +238,7 @@ struct SystemBase {
   virtual void tune(uint32_t blocksPerSm, uint32_t graph) = 0;
   virtual void setSolver(uint32_t form) = 0;
   virtual void setPlasticity(uint32_t mode) = 0;
+  virtual bool plasticUsed(uint32_t law) const = 0;
   virtual void setFlowLimits(uint32_t body, uint32_t lane, double crushStress, double crushLimit,
                              double plasticMax) = 0;
   std::vector<uint32_t> trace;  // TL_FLAG_TRACE: iterations of each PCG launch (body 0)
@@ -1536,6 +1537,12 @@ struct System final : SystemBase {
     dFlim.upload(hFlim.data() + at, 3, st, at);
     TL_CUDA(cudaStreamSynchronize(st));
   }
+  // Does a step under `law` read or write the plastic slot?
+  bool plasticUsed(uint32_t law) const override {
+    if (hencky) return true;
+    return law == TL_LAW_COROTATED &&
+           std::any_of(hb.begin(), hb.end(), [](const HostBody& h) { return h.anyYields; });
+  }
   // Every tet starts from its authored rest: P = I, hardening 0.
   void setPlasticity(uint32_t mode) override {
     if (mode != TL_PLASTICITY_HENCKY) {
@@ -2222,16 +2229,23 @@ int32_t tl_rollout_adjoint(tl_rollout* rollout, const double* dl_dx_final, const
 int32_t tl_step_host(tl_system* system, uint32_t body, int32_t dtype, void* position, void* velocity,
                      void* acceleration, void* rotation, void* plastic, const tl_settings* settings,
                      const double gravity[3], double dt, tl_step_report* report) {
-  if (!system || body >= system->impl->bodies || system->impl->bodies != 1u) return TL_ERR_ARG;
+  if (!system || !settings || body >= system->impl->bodies || system->impl->bodies != 1u) return TL_ERR_ARG;
   // The incoming rotations are not uploaded: every element pass writes each
   // committed rotation before any kernel reads one (kElement, then kDamping
   // and the matvec), as assembleElastic does in the reference
   // (solver.cc:1404, 1446, 1500, 1547 before 745-987).  They are outputs only.
-  int32_t rc = tl_state_set(system, body, dtype, position, velocity, acceleration, nullptr, plastic);
+  // The plastic slot crosses only when the step reads it: with no yielding
+  // lane under the corotated law (the SNH law runs elastic here) and the
+  // small-strain mode, the step leaves the plastic points as they are, so the
+  // caller's buffer already holds them.  In the finite-strain mode every tet's
+  // plastic map shapes its rest, so the slot always crosses.
+  const bool plasticUsed = system->impl->plasticUsed(settings->law);
+  void* pl = plasticUsed ? plastic : nullptr;
+  int32_t rc = tl_state_set(system, body, dtype, position, velocity, acceleration, nullptr, pl);
   if (rc != TL_OK) return rc;
   rc = tl_step(system, settings, gravity, dt, report);
   if (rc != TL_OK && rc != TL_ERR_NONFINITE) return rc;
-  const int32_t got = tl_state_get(system, body, dtype, position, velocity, acceleration, rotation, plastic);
+  const int32_t got = tl_state_get(system, body, dtype, position, velocity, acceleration, rotation, pl);
   return got != TL_OK ? got : rc;
 }
 

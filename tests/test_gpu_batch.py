@@ -192,3 +192,37 @@ def test_host_step_treats_rotations_as_outputs(law, damping):
     assert np.isfinite(poisoned["rotation"]).all()
     for k in clean:
         assert np.array_equal(clean[k], poisoned[k]), k
+
+
+def test_host_step_moves_plastic_state_only_when_the_step_uses_it():
+    """An elastic body: tl_step_host neither uploads nor downloads the plastic
+    slot (the step leaves it as it is), so a NaN-filled buffer stays as passed
+    and the step equals the resident one.  A yielding body's slot crosses."""
+    import ctypes as C
+    from talus_b200 import _capi as capi
+
+    def host_steps(mesh, mat, poison, n=3):
+        system = tb.System(mesh, [mat], tb.FP64)
+        st = tb.rest_state(mesh)
+        arrays = {k: np.ascontiguousarray(getattr(st, k), np.float64) for k in
+                  ("position", "velocity", "acceleration", "rotation", "plastic")}
+        if poison:
+            arrays["plastic"][:] = np.nan
+        g = np.asarray(GRAVITY, np.float64)
+        for _ in range(n):
+            rc = capi.lib().tl_step_host(system.handle, 0, capi.TL_DTYPE_F64,
+                                         *[arrays[k].ctypes.data for k in
+                                           ("position", "velocity", "acceleration", "rotation", "plastic")],
+                                         C.byref(tb.Settings()._c()), g.ctypes.data, DT,
+                                         C.byref(capi.tl_step_report()))
+            assert rc == capi.TL_OK
+        system.close()
+        return arrays
+
+    mesh, mat = elastic_block((5, 4, 4), seed=12)
+    clean, poisoned = host_steps(mesh, mat, False), host_steps(mesh, mat, True)
+    assert np.isnan(poisoned["plastic"]).all()
+    assert np.array_equal(clean["position"], poisoned["position"])
+    pmesh, pmat = plastic_block((8, 4, 4))
+    moved = host_steps(pmesh, pmat, False)
+    assert moved["plastic"][:, 9].max() > 0.0
