@@ -11,7 +11,9 @@ tests expected values that need no CPU solve (tests/test_gpu_golden.py).
 
 Each block fixture stores how its mesh is generated (talus_b200.box_mesh) and
 a checksum of the generated mesh, the positions after the first and the last
-step, and the step reports the GPU path must reproduce.  tet_laws.npz holds
+step, and the step reports the GPU path must reproduce.  hencky_block.npz is
+the plastic block in the finite-strain plasticity mode (plasticflow.cc), with
+its hardening variables and a sample of its plastic maps.  tet_laws.npz holds
 48 disconnected tets at seeded deformations (stretched, sheared, rotated,
 three inverted) with each law's element forces.
 
@@ -79,6 +81,30 @@ def write_block(name):
         plastic_evaluations=np.array([r["plastic_evaluations"] for r in reports]))
 
 
+# The plastic block in the finite-strain (Hencky) plasticity mode, P = I at rest.
+HENCKY_BLOCK = dict(cells=(16, 8, 8), seed=2, speed=0.5)
+HENCKY_STEPS = 8
+HENCKY_SAMPLE = 16  # every 16th tet's plastic map is stored
+
+
+def hencky_case():
+    mesh, mat = plastic_block(**HENCKY_BLOCK)
+    return mesh, mat, tb.Settings(), HENCKY_STEPS
+
+
+def write_hencky_block():
+    mesh, mat, settings, steps = hencky_case()
+    record = []
+    state, reports = run_oracle(po.F64, mesh, mat, settings, steps, record=record, plasticity=po.PLASTICITY_HENCKY)
+    np.savez_compressed(
+        os.path.join(HERE, "hencky_block.npz"),
+        mesh_checksum=mesh_checksum(mesh), material=material_array(mat), steps=steps,
+        first=record[0], last=record[-1], hardening=state.plastic[:, 9],
+        plastic_map_sample=state.plastic[::HENCKY_SAMPLE, :9],
+        flowed=np.array([r["yielding"] for r in reports]),
+        cg_iterations=np.array([r["cg_iterations"] for r in reports]))
+
+
 def single_tets(count=48, seed=11):
     """`count` tets cut from a jittered Kuhn lattice, each with its own four
     nodes, and a seeded deformation gradient per tet."""
@@ -135,6 +161,7 @@ def write_tet_laws():
 def main():
     for name in BLOCKS:
         write_block(name)
+    write_hencky_block()
     write_tet_laws()
 
 

@@ -45,12 +45,14 @@ def plastic_block(cells=(16, 8, 8), seed=2, speed=0.5):
     return mesh, mat
 
 
-def run_oracle(precision, mesh, mat, settings, steps, record=None):
+def run_oracle(precision, mesh, mat, settings, steps, record=None, plasticity=po.PLASTICITY_SMALL_STRAIN):
     om = to_oracle(mesh)
-    state = po.State.rest(om)
+    state = po.State.rest(om, hencky=plasticity == po.PLASTICITY_HENCKY)
+    osettings = oracle_settings(settings)
+    osettings.plasticity = plasticity
     reports = []
     for i in range(steps):
-        rep = po.step(precision, om, state, [oracle_material(mat)], oracle_settings(settings), GRAVITY, DT)
+        rep = po.step(precision, om, state, [oracle_material(mat)], osettings, GRAVITY, DT)
         reports.append(rep.as_dict())
         if record is not None:
             record.append(state.position.copy())

@@ -96,3 +96,22 @@ def test_single_tet_fixture_properties():
     assert inverted.sum() == 3
     # small deformations stay elastic, large ones yield
     assert g["yielding"][0::4].sum() == 0 and g["yielding"][3::4].all()
+
+
+def test_oracle_reproduces_the_finite_strain_fixture():
+    """hencky_block.npz: the plastic block in the finite-strain plasticity
+    mode (plasticflow.cc:96-150, 184-247 at one point per tet)."""
+    mesh, mat, settings, steps = mg.hencky_case()
+    g = load("hencky_block")
+    np.testing.assert_allclose(mg.mesh_checksum(mesh), g["mesh_checksum"], rtol=1e-12)
+    record = []
+    state, reports = run_oracle(po.F64, mesh, mat, settings, steps, record=record, plasticity=po.PLASTICITY_HENCKY)
+    assert relative_error(record[0], g["first"], mesh.rest_positions) <= 1e-10
+    assert relative_error(record[-1], g["last"], mesh.rest_positions) <= 1e-10
+    assert [r["yielding"] for r in reports] == list(g["flowed"])
+    assert [r["cg_iterations"] for r in reports] == list(g["cg_iterations"])
+    np.testing.assert_allclose(state.plastic[:, 9], g["hardening"], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(state.plastic[::mg.HENCKY_SAMPLE, :9], g["plastic_map_sample"], rtol=0, atol=1e-12)
+    # the flow is deviatoric: every stored plastic map keeps volume
+    maps = g["plastic_map_sample"].reshape(-1, 3, 3)
+    assert np.abs(np.linalg.det(maps) - 1.0).max() <= 1e-12

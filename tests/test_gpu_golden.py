@@ -86,3 +86,29 @@ def test_single_tet_forces_match_golden(law, material, key, precision):
     assert worst <= (1e-9 if precision == tb.FP64 else 1e-4), worst
     if material == "plastic" and precision == tb.FP64:
         np.testing.assert_array_equal(yielding, g["yielding"])
+
+
+@pytest.mark.parametrize("form", ["elementwise", "assembled"])
+@pytest.mark.parametrize("precision", [tb.FP64, tb.FP32_MIXED], ids=["fp64", "mixed"])
+def test_finite_strain_block_matches_golden(precision, form):
+    mesh, mat, settings, steps = mg.hencky_case()
+    g = load("hencky_block")
+    np.testing.assert_allclose(mg.mesh_checksum(mesh), g["mesh_checksum"], rtol=1e-12)
+    system = tb.System(mesh, [mat], precision)
+    system.set_solver(form)
+    system.set_plasticity("hencky")
+    system.set_state(tb.rest_state(mesh, hencky=True))
+    tol = 1e-9 if precision == tb.FP64 else 1e-5
+    flowed, first = [], None
+    for i in range(steps):
+        flowed.append(system.step(settings, GRAVITY, DT)[0].yielding)
+        if i == 0:
+            first = system.get_state().position
+    state = system.get_state()
+    system.close()
+    assert relative_error(first, g["first"], mesh.rest_positions) <= tol
+    assert relative_error(state.position, g["last"], mesh.rest_positions) <= tol
+    if precision == tb.FP64:
+        assert flowed == list(g["flowed"])
+        assert np.abs(state.plastic[:, 9] - g["hardening"]).max() <= 1e-9 * max(1.0, g["hardening"].max())
+        assert np.abs(state.plastic[::mg.HENCKY_SAMPLE, :9] - g["plastic_map_sample"]).max() <= 1e-9
