@@ -472,15 +472,20 @@ enum ElementMode : uint32_t {
 // Kinematics and the law run in FP64 whatever S is; outputs are stored in S.
 // Positions are base + reach * dir (the reference's `evaluated`), in
 // displacement form.
-#ifndef TL_ELEMENT_MIN_BLOCKS
-#define TL_ELEMENT_MIN_BLOCKS 2  // resident 256-thread blocks per SM the element pass is compiled for
-#endif
+// Resident 256-thread blocks per SM the element pass is compiled for: three
+// for the FP32-mixed corotated pass (80 registers; 4% less time per launch on
+// the 393,216-tet plastic block than two blocks at 128 registers, with
+// bitwise the same results), two for the others (the FP64 pass keeps its
+// 128 registers).
+template <class S, int LAW> constexpr int elementMinBlocks() {
+  return std::is_same_v<S, float> && LAW == 0 ? 3 : 2;
+}
 // HK: the corotated law from each tet's plastic rest shape (finite-strain
 // flow): F' = F P, gradients g' = P^T g, volume V / det P, where P = Fp^-1 is
 // the tet's plastic map (plasticRest, plasticflow.cc:263-300: Dm' = Fp Dm,
 // V' = V det Fp); the small-strain return map is off.
 template <class S, int LAW, bool HK = false>
-__global__ void __launch_bounds__(TILE, TL_ELEMENT_MIN_BLOCKS)
+__global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
     kElement(Sys<S> s, const Vec4<S>* base, const Vec4<S>* dir, uint32_t pass, uint32_t mode, double margin) {
   static_assert(!HK || LAW == 0, "the plastic rest shape is written for the corotated law");
   const uint32_t tile = blockIdx.x, b = s.elem_tile_body[tile];
