@@ -240,4 +240,34 @@ template <class T> TL_HD M3<T> elementRotation(const M3<T>& f, bool invertible) 
   return invertibleRotation(f);
 }
 
+// returnMap (plasticflow.cc:110-150) of one point, FP64 like the reference:
+// the left stretch B = Fe Fe^T diagonalised by the cyclic Jacobi solve, log
+// strains 0.5 log(lambda), deviator d, q = sqrt(3/2) 2 mu |d|; past the yield
+// stress Fe <- V diag(exp(d (yield / q - 1))) V^T Fe.  False inside.
+TL_HD bool henckyReturn(const M3<double>& fe, double shear, double yield, M3<double>& out,
+                                    double& strain, double& trial) {
+  double a[3][3], v[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      a[i][j] = fe.m[i][0] * fe.m[j][0] + fe.m[i][1] * fe.m[j][1] + fe.m[i][2] * fe.m[j][2];
+  jacobiEigen3(a, v);
+  if (!(fmin(a[0][0], fmin(a[1][1], a[2][2])) > 0.0)) return false;
+  const double l[3] = {0.5 * log(a[0][0]), 0.5 * log(a[1][1]), 0.5 * log(a[2][2])};
+  const double mean = (l[0] + l[1] + l[2]) / 3.0;
+  const double d[3] = {l[0] - mean, l[1] - mean, l[2] - mean};
+  const double size = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  const double stress = sqrt(1.5) * 2.0 * shear * size;
+  if (!(stress > yield) || size <= 1.0e-15) return false;
+  M3<double> c = zero3<double>();
+#pragma unroll
+  for (int k = 0; k < 3; ++k) addOuter(c, exp(d[k] * (yield / stress - 1.0)) * V3<double>{v[0][k], v[1][k], v[2][k]},
+                                       V3<double>{v[0][k], v[1][k], v[2][k]});
+  out = mul(c, fe);
+  trial = stress;
+  strain = (stress - yield) / (3.0 * shear);
+  return true;
+}
+
 }  // namespace tl
