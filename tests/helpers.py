@@ -27,13 +27,13 @@ def oracle_settings(s: tb.Settings) -> po.Settings:
 
 
 def elastic_block(cells=(8, 8, 8), jitter=0.01, seed=1):
-    """Config-1 shape: 8x8x8 cubes of 0.1 m, E=1e6, nu=0.3, rho=1000, bottom (y=0) pinned."""
+    """The elastic benchmark block: 8x8x8 cubes of 0.1 m, E=1e6, nu=0.3, rho=1000, bottom (y=0) pinned."""
     mesh = tb.box_mesh(cells, voxel=0.1, jitter=jitter, seed=seed)
     return mesh, tb.PhysicalMaterial(density=1000.0, youngs_modulus=1e6, poissons_ratio=0.3)
 
 
 def plastic_block(cells=(16, 8, 8), seed=2, speed=0.5):
-    """Config-2 shape at reduced size: E=2e7, nu=0.35, yield 1e5, H=2e5; bottom
+    """The plastic benchmark block at reduced size: E=2e7, nu=0.35, yield 1e5, H=2e5; bottom
     pinned, top face pushed down at `speed` m/s."""
     mesh = tb.box_mesh(cells, voxel=0.1, jitter=0.0, seed=seed)
     top = mesh.face(1, 1)
@@ -74,6 +74,6 @@ def run_gpu(precision, mesh, mat, settings, steps, record=None):
 
 
 def relative_error(x, ref, rest):
-    """max_n |x_n - ref_n| / max_n |ref_n - X_n| (the north-star displacement error)."""
+    """max_n |x_n - ref_n| / max_n |ref_n - X_n| (the relative displacement error the 1e-5 bar is stated in)."""
     scale = np.linalg.norm(ref - rest, axis=1).max()
     return float(np.linalg.norm(x - ref, axis=1).max() / max(scale, 1e-300))

@@ -3,7 +3,7 @@
 No CPU solve runs here: every expected value comes from a fixture the FP64
 oracle wrote (tests/golden/make_golden.py).  Bars as in test_gpu_parity:
 FP64 <= 1e-9 relative displacement error on the elastic and damped blocks and
-1e-8 on the plastic Newton path, FP32-mixed <= 1e-5 (the north-star
+1e-8 on the plastic Newton path, FP32-mixed <= 1e-5 (the FP32-mixed
 tolerance); each solver form (element-wise, assembled) meets them.  Single
 tets: element forces of each law through tl_evaluate, FP64 within 1e-9 of the
 tet's largest corner force and FP32-mixed within 1e-4 (the force tolerance of
