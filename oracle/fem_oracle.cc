@@ -1,7 +1,7 @@
 // fem_oracle.cc -- CPU restatement of the Talus tet FEM step.
 //
 // TEST INFRASTRUCTURE ONLY: used by tests/, __graft_entry__.smoke() and the
-// cpu_baseline leg of bench.py as the checker.  The product (talus_b200)
+// cpu_baseline leg of bench.py, for comparison.  The product (talus_b200)
 // never links or calls it.
 //
 // Every function names the reference lines it restates.  Paths are relative

@@ -1,7 +1,7 @@
 """ctypes binding of the CPU oracle (oracle/fem_oracle.cc).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
-cpu_baseline / reference legs of bench.py as the checker.  The product package
+cpu_baseline / reference legs of bench.py as the reference results.  The product package
 ``talus_b200`` never imports it.
 
 The oracle restates talus::deformable::step (reference

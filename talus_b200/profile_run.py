@@ -1,4 +1,4 @@
-"""Profiling driver: steps a benchmark workload and records, for every PCG
+"""Profiling run: steps a benchmark workload and records, for every PCG
 launch, its iteration count, so that an ncu capture of one launch of
 tl::kPcg can be turned into DRAM bytes per PCG iteration.
 

@@ -8,7 +8,7 @@
   E log-uniform in [1e5, 1e8] Pa, nu uniform in [0.25, 0.45], base pinned.
 
 All use 0.1 m cubes split into six Kuhn tets, density 1000, gravity 9.81 and
-dt = 1/60 (the driver of each workload passes those).
+dt = 1/60 (the code that steps each workload passes those).
 """
 from __future__ import annotations
 

@@ -1,5 +1,5 @@
 """Shared fixtures: synthetic meshes of the benchmark shapes and the oracle
-bridge.  The oracle (oracle/) is the checker, never the thing tested."""
+bridge.  The oracle (oracle/) is what the CUDA path is compared with, never the thing tested."""
 from __future__ import annotations
 
 import numpy as np

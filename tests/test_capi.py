@@ -115,7 +115,7 @@ def test_context_without_a_device_reports_no_device():
 
 
 def test_product_package_does_not_use_the_oracle():
-    """The oracle is the checker only: no product source links, imports or loads it."""
+    """The oracle is test infrastructure only: no product source links, imports or loads it."""
     banned = ("pyoracle", "fem_oracle", "from oracle", "import oracle", "libfem_oracle")
     for dirpath, _, files in os.walk(os.path.join(ROOT, "talus_b200")):
         for f in files:
