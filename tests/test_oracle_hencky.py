@@ -141,3 +141,24 @@ def test_hencky_is_refused_with_the_snh_law_and_with_damping():
     mat.stiffness_damping = 0.01
     with pytest.raises(RuntimeError):
         run(mesh, mat, po.PLASTICITY_HENCKY, 1)
+
+
+@pytest.mark.parametrize("limits", [dict(plastic_max=0.02), dict(crush_stress=2.0e4, crush_limit=0.95)],
+                         ids=["cap", "crush"])
+def test_flow_limits_hold_through_a_block_step(limits):
+    """In the oracle's step, the cap and the crush limit hold on every tet of a
+    pushed block, and a limit that binds changes the trajectory."""
+    mesh, mat = plastic_block()
+    free, _ = run(mesh, mat, po.PLASTICITY_HENCKY, 6)
+    for k, v in limits.items():
+        setattr(mat, k, v)
+    st, reports = run(mesh, mat, po.PLASTICITY_HENCKY, 6)
+    stretch = np.linalg.inv(st.plastic[:, :9].reshape(-1, 3, 3))
+    if "plastic_max" in limits:
+        assert np.linalg.norm(stretch - np.eye(3), axis=(1, 2)).max() <= limits["plastic_max"] + 1e-9
+        assert np.linalg.norm(np.linalg.inv(free.plastic[:, :9].reshape(-1, 3, 3)) - np.eye(3),
+                              axis=(1, 2)).max() > limits["plastic_max"]
+    else:
+        assert np.linalg.det(stretch).min() >= limits["crush_limit"] - 1e-9
+        assert np.linalg.det(stretch).min() < 0.999
+    assert relative_error(st.position, free.position, mesh.rest_positions) > 1e-6
