@@ -1756,6 +1756,8 @@ struct System final : SystemBase {
   uint8_t* yflagPtr = nullptr;
   void evaluate(uint32_t b, const tl_settings& set, double* forces, uint8_t* yielding) override {
     if (set.law > 1u) throw StatusError{TL_ERR_ARG, "unknown law"};
+    if (hencky && set.law != TL_LAW_COROTATED)
+      throw StatusError{TL_ERR_UNSUPPORTED, "the plastic rest shape is written for the corotated law"};
     const BodyDev& bd = bodyHost[b];
     const HostBody& h = hb[b];
     BodyStepDev* hs = hStep.get(B);
