@@ -155,6 +155,16 @@ const char* tl_ctx_last_error(const tl_ctx* ctx);
  * hanging the GPU. */
 int32_t tl_ctx_check_wait_limit(tl_ctx* ctx);
 
+/* Failure injection on the host, no reference counterpart.  Arms the next
+ * tl_step of `system` so that its PCG solve number `solve` (0 = the step's
+ * first solve; < 0 disarms) is preceded by the same bounded wait as
+ * tl_ctx_check_wait_limit on the system's barrier word: the wait runs out
+ * (about 2 s) and records TL_ERR_TIMEOUT, that solve and every later solve of
+ * the step leave at their first barrier, and the step returns TL_ERR_TIMEOUT.
+ * The arming is used once.  The system stays usable: the next step clears the
+ * record and runs normally.  No GPU fault or hang is involved. */
+int32_t tl_system_expire_wait(tl_system* system, int32_t solve);
+
 /* Upload one or more bodies (a batch when count > 1) into one resident
  * system.  Replaces buildMesh's output handling + refreshStiffness +
  * buildIncidence (solver.cc:453-507, 1065-1101): the node->element CSR
@@ -314,23 +324,26 @@ int32_t tl_rollout_adjoint(tl_rollout* rollout, const double* dl_dx_final, const
                            double* dl_dyoungs, double* dl_dv0, double* dl_dx0, double* device_seconds);
 
 /* No counterpart in the reference.  One step of one small body that allocates
- * nothing, for callers that cannot call cudaMalloc: engines with a fixed GPU
- * memory budget, code that runs while a CUDA graph is being captured (where
- * allocation is not allowed), hosts that hand out device memory only through
- * their own pool.  Same meaning of arguments and results as tl_step_host, with
- * the mesh passed each call; the arithmetic is FP64.
+ * nothing, for callers that cannot call cudaMalloc: engines that run inside a
+ * fixed GPU memory budget decided at start-up, and hosts that hand out device
+ * memory only through their own pool and forbid libraries to allocate behind
+ * their back.  Same meaning of arguments and results as tl_step_host, with
+ * the mesh passed each call (per-element Young's moduli included); the
+ * arithmetic is FP64.
  *
  * All device scratch lives in one fixed array inside the library
  * (TL_NOALLOC_ARENA_BYTES on every GPU that loads it, held until the process
  * exits); nothing is allocated on the device or the host heap.  Limits:
  * TL_NOALLOC_MAX_NODES nodes, TL_NOALLOC_MAX_TETS tets, TL_NOALLOC_MAX_LANES
- * material lanes (beyond them: TL_ERR_TOO_LARGE), and no plastic Newton loop
- * (a yielding material with plastic_passes > 1: TL_ERR_UNSUPPORTED).  The
- * first call on a device looks up the array's device address (once per
+ * material lanes (beyond them: TL_ERR_TOO_LARGE), no plastic Newton loop (a
+ * yielding material with plastic_passes > 1) and no stiffness damping on a
+ * lane an element uses (both TL_ERR_UNSUPPORTED).  The first call on a device
+ * looks up the array's device address and loads the step's kernels (once per
  * device); make that first call before any stream capture begins.  Calls are
  * serialised inside the library; GPU work of two overlapping calls would race
- * on the shared array.  Runs on the legacy default stream and returns when the
- * step has finished. */
+ * on the shared array.  Issues its copies and kernels on the legacy default
+ * stream (stream 0), synchronises it, and returns when the step has
+ * finished. */
 #define TL_NOALLOC_MAX_NODES 1024
 #define TL_NOALLOC_MAX_TETS 4096
 #define TL_NOALLOC_MAX_LANES 16

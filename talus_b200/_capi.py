@@ -147,6 +147,7 @@ SIGNATURES = {
     "tl_system_set_solver": (C.c_int32, [C.c_void_p, C.c_uint32]),
     "tl_system_set_plasticity": (C.c_int32, [C.c_void_p, C.c_uint32]),
     "tl_ctx_check_wait_limit": (C.c_int32, [C.c_void_p]),
+    "tl_system_expire_wait": (C.c_int32, [C.c_void_p, C.c_int32]),
     "tl_system_set_flow_limits": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_double, C.c_double,
                                               C.c_double]),
     "tl_state_set": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_int32] + [C.c_void_p] * 5),

@@ -12,7 +12,7 @@ HEADERS = [os.path.join(HERE, "csrc", f) for f in ("tl_kernels.cuh", "tl_math.cu
     os.path.join(os.path.dirname(HERE), "include", "talus_fem.h")]
 OUTPUT = os.path.join(HERE, "libtalus_fem.so")
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
-              "-Xcompiler", "-fPIC", "-Xcompiler", "-pthread", "-shared", "-Xptxas", "-v"]
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-pthread", "-Xptxas", "-v"]
 
 
 def nvcc() -> str:
@@ -31,14 +31,31 @@ def up_to_date() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and up_to_date():
         return OUTPUT
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", OUTPUT, *SOURCES]
-    res = subprocess.run(cmd, capture_output=True, text=True)
-    if verbose or res.returncode != 0:
-        sys.stderr.write(res.stdout + res.stderr)
-    if res.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({res.returncode})")
+    # each source compiles in its own nvcc process (in parallel), then one link
+    objects = [os.path.splitext(src)[0] + ".o" for src in SOURCES]
+    jobs = [subprocess.Popen([nvcc(), *NVCC_FLAGS, "-c", "-o", obj, src], stdout=subprocess.PIPE,
+                             stderr=subprocess.PIPE, text=True) for src, obj in zip(SOURCES, objects)]
+    logs = []
+    failed = 0
+    for job in jobs:
+        out, err = job.communicate()
+        logs.append(out + err)
+        failed = failed or job.returncode
+    if not failed:
+        link = subprocess.run([nvcc(), "-shared", "-Xcompiler", "-pthread", "-gencode",
+                               "arch=compute_100a,code=sm_100a", "-o", OUTPUT, *objects],
+                              capture_output=True, text=True)
+        logs.append(link.stdout + link.stderr)
+        failed = link.returncode
+    for obj in objects:
+        if os.path.exists(obj):
+            os.remove(obj)
+    if verbose or failed:
+        sys.stderr.write("".join(logs))
+    if failed:
+        raise RuntimeError(f"nvcc failed ({failed})")
     with open(os.path.join(HERE, "ptxas_info.txt"), "w") as f:
-        f.write(res.stderr)
+        f.write("".join(logs))
     return OUTPUT
 
 

@@ -2479,7 +2479,11 @@ static __global__ void kAccReset(BodyAccDev* acc, CgReportDev* rep, uint32_t bod
   rep[b] = r;
 }
 
-// Resets the PCG launch state: active body count, tile counters, barrier.
+// Resets the PCG launch state: active body count, tile counters, barrier
+// arrivals.  The error word is left as it is: a wait that ran out in any solve
+// of a step stays recorded until the host reads it at the step's end (the step
+// clears it once, before its first launch), and later solves of the same step
+// see it at their first barrier and leave at once.
 template <class S>
 __global__ void kPcgPrepare(Sys<S> s, uint32_t pass) {
   __shared__ int count;
@@ -2492,7 +2496,6 @@ __global__ void kPcgPrepare(Sys<S> s, uint32_t pass) {
   __syncthreads();
   if (threadIdx.x == 0) {
     s.sync->arrive = 0u;
-    s.sync->error = 0;
     s.sync->active = count;
   }
 }

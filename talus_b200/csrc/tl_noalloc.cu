@@ -1,21 +1,23 @@
 // tl_noalloc.cu -- tl_step_noalloc: one tet FEM step of one small body that
 // allocates nothing.
 //
-// Who needs this: code that may not allocate device memory at all -- a frame
-// loop of a game or robotics engine with a fixed memory budget, a thread that
-// runs while a CUDA graph is being captured (cudaMalloc/cudaFree are not
-// allowed inside a capture), or a host program that hands out GPU memory only
-// through its own pool.  Such callers cannot use tl_system_create, which
-// allocates the device buffers of a resident system.
+// Who needs this: callers that may not allocate device memory at all -- the
+// frame loop of a game or robotics engine that works inside a fixed GPU memory
+// budget decided at start-up, or a host program that hands out GPU memory only
+// through its own pool and forbids libraries to call cudaMalloc behind its
+// back.  Such callers cannot use tl_system_create, which allocates the device
+// buffers of a resident system.
 //
 // How: every device buffer of the step lives in one file-scope
 // `static __device__` array, tl_noalloc_arena, of a fixed size
 // (TL_NOALLOC_ARENA_BYTES; every GPU that loads the library holds it until the
 // process exits).  Host-side staging uses static host arrays.  The host code
-// never calls cudaMalloc, cudaFree, cudaMallocHost or the C++ heap.  The
-// arena's device address comes from cudaGetSymbolAddress, called once per
-// device (with that device current) by the first call on it; that first call
-// should therefore be made before any stream capture begins.
+// never calls cudaMalloc, cudaFree, cudaMallocHost or the C++ heap.  In host
+// code the array's name is only a host-side stand-in for it: its device
+// address comes from cudaGetSymbolAddress, called once per device (with that
+// device current) by the first call on it, which also loads every kernel the
+// step launches.  That first call should therefore be made before any stream
+// capture begins.
 //
 // Every call shares the one arena and the static host arrays: calls are
 // serialised by a host mutex, and the arena keeps the previous call's
@@ -27,10 +29,11 @@
 // Scope: FP64 arithmetic, one body, at most TL_NOALLOC_MAX_NODES nodes,
 // TL_NOALLOC_MAX_TETS tets and TL_NOALLOC_MAX_LANES material lanes, the
 // reference's step without its plastic Newton loop (plastic_passes <= 1 or no
-// yielding material); larger inputs are refused with TL_ERR_TOO_LARGE and the
-// Newton case with TL_ERR_UNSUPPORTED.  It runs the same kernels as tl_step
-// (kElement, kNodeAssemble, kPcg, ...) on the legacy default stream and
-// returns after the step has finished.
+// yielding material) and without stiffness damping; larger inputs are refused
+// with TL_ERR_TOO_LARGE, the Newton and damping cases with TL_ERR_UNSUPPORTED.
+// It runs the same kernels as tl_step (kElement, kNodeAssemble, kPcg, ...),
+// issues its copies and launches on the legacy default stream (stream 0),
+// synchronises that stream, and returns after the step has finished.
 
 #include "../../include/talus_fem.h"
 #include "tl_kernels.cuh"
@@ -79,7 +82,7 @@ struct Layout {
   OpRec<S>* orec;
   uint8_t* anch;
   uint4* tet;
-  double *dm, *vold, *op, *de2, *part, *npart, *epart;
+  double *dm, *vold, *eyoung, *op, *de2, *part, *npart, *epart;
   BodyAccDev* acc;
   CgBodyDev* cg;
   CgReportDev* cgrep;
@@ -104,6 +107,7 @@ Layout carve(unsigned char* base) {
   l.tet = c.take<uint4>(NA_TP);
   l.dm = c.take<double>(size_t(9) * NA_TP);
   l.vold = c.take<double>(NA_TP);
+  l.eyoung = c.take<double>(NA_TP);
   l.lane = c.take<uint32_t>(NA_TP);
   l.op = c.take<double>(size_t(9) * NA_TP);
   l.orec = c.take<OpRec<S>>(NA_TP);
@@ -142,7 +146,7 @@ Vec4<S> h_rest4[NA_VP], h_pres[NA_VP], h_node[3][NA_VP];
 uint8_t h_anch[NA_VP];
 uint32_t h_start[NA_VP + 1], h_cursor[NA_VP], h_entry[4 * NA_TP], h_lane[NA_TP], h_tileBody[NA_ELEM_TILES];
 uint4 h_tet[NA_TP];
-double h_dm[9 * NA_TP], h_vol[NA_TP], h_op[9 * NA_TP];
+double h_dm[9 * NA_TP], h_vol[NA_TP], h_eyoung[NA_TP], h_op[9 * NA_TP];
 Vec4<S> h_plast[2 * NA_TP];
 MatDev h_mat[NA_LANES];
 BodyDev h_body;
@@ -167,6 +171,17 @@ int32_t setupDevice(int32_t device, DeviceSetup*& out) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kPcg<S, 1>, TILE, 0) != cudaSuccess || perSm < 1)
       return TL_ERR_CUDA;
     d.pcgGrid[1] = std::min(perSm * sms, int(std::max(NA_NODE_TILES, NA_ELEM_TILES)));
+    // Every kernel a step can launch is loaded here, by the first call, so
+    // later calls load no module code (CUDA may load kernels lazily, on their
+    // first launch).
+    const void* kernels[] = {(const void*)kInversionCheck<S>, (const void*)kPcgPrepare<S>, (const void*)kPcg<S, 0>,
+                             (const void*)kPcg<S, 1>,          (const void*)kPredict<S>,     (const void*)kElement<S, 0>,
+                             (const void*)kElement<S, 1>,      (const void*)kNodeAssemble<S>, (const void*)kAddIncrement<S>,
+                             (const void*)kUpdate<S>,          (const void*)kStepEnd<S>,     (const void*)kFinalize};
+    for (const void* k : kernels) {
+      cudaFuncAttributes attr;
+      if (cudaFuncGetAttributes(&attr, k) != cudaSuccess) return TL_ERR_CUDA;
+    }
     d.arena = static_cast<unsigned char*>(ptr);
     d.ready = true;
   }
@@ -174,7 +189,7 @@ int32_t setupDevice(int32_t device, DeviceSetup*& out) {
   return TL_OK;
 }
 
-Sys<S> viewOf(const Layout& l, uint32_t Vp, uint32_t Tp) {
+Sys<S> viewOf(const Layout& l, uint32_t Vp, uint32_t Tp, bool perElementYoungs) {
   Sys<S> s;
   std::memset(&s, 0, sizeof(s));
   s.bodies = 1;
@@ -213,7 +228,7 @@ Sys<S> viewOf(const Layout& l, uint32_t Vp, uint32_t Tp) {
   s.vold = l.vold;
   s.vols = l.vold;
   s.lane = l.lane;
-  s.eyoung = nullptr;
+  s.eyoung = perElementYoungs ? l.eyoung : nullptr;
   s.op = l.op;
   s.orec = l.orec;
   s.sell_val = nullptr;
@@ -264,10 +279,12 @@ int32_t stepLocked(int32_t device, const tl_mesh_desc& d, int32_t dtype, void* p
   const int law = int(set.law);
   // ---- materials (material.cc:71-78, 747-749) and the default lane
   bool anyYields = false, anyAnchored = false;
+  bool laneDamps[NA_LANES];
   for (uint32_t k = 0; k <= d.lanes; ++k) {
     const tl_material m = k < d.lanes ? d.materials[k]
                                       : tl_material{1000.0, 0.0, 0.3, 0.0, std::numeric_limits<double>::infinity(), 0.0};
-    if (m.stiffness_damping > 0.0) return TL_ERR_UNSUPPORTED;
+    // stiffnessDamping counts when finite and positive (factor.cc:755-759), the rule tl_system_create applies
+    laneDamps[k] = std::isfinite(m.stiffness_damping) && m.stiffness_damping > 0.0;
     const double nu = std::clamp(m.poissons_ratio, 0.0, 0.49);
     h_mat[k] = MatDev{nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), 1.0 / (2.0 * (1.0 + nu)), m.youngs_modulus, m.yield_stress,
                       m.hardening_modulus, (std::isfinite(m.yield_stress) && m.yield_stress > 0.0) ? 1u : 0u, 0u};
@@ -313,6 +330,9 @@ int32_t stepLocked(int32_t device, const tl_mesh_desc& d, int32_t dtype, void* p
     h_vol[e] = real ? d.volume[e] : 0.0;
     const uint32_t ln = real && d.material[e] < d.lanes ? d.material[e] : d.lanes;
     h_lane[e] = ln;
+    // the damping fit planes are an allocation this entry point does not make
+    if (real && laneDamps[ln]) return TL_ERR_UNSUPPORTED;
+    h_eyoung[e] = (real && d.element_youngs) ? d.element_youngs[e] : h_mat[ln].youngs;
     anyYields = anyYields || (real && h_mat[ln].yields);
     for (int k = 0; k < 9; ++k)
       h_op[size_t(k) * Tp + e] = (real && rotation) ? (dtype == TL_DTYPE_F64 ? at<double>(rotation, 9 * size_t(e) + k)
@@ -375,6 +395,8 @@ int32_t stepLocked(int32_t device, const tl_mesh_desc& d, int32_t dtype, void* p
   NA_CUDA(cudaMemcpyAsync(l.tet, h_tet, sizeof(uint4) * Tp, cudaMemcpyHostToDevice, st));
   NA_CUDA(cudaMemcpyAsync(l.dm, h_dm, sizeof(double) * 9 * Tp, cudaMemcpyHostToDevice, st));
   NA_CUDA(cudaMemcpyAsync(l.vold, h_vol, sizeof(double) * Tp, cudaMemcpyHostToDevice, st));
+  if (d.element_youngs)
+    NA_CUDA(cudaMemcpyAsync(l.eyoung, h_eyoung, sizeof(double) * Tp, cudaMemcpyHostToDevice, st));
   NA_CUDA(cudaMemcpyAsync(l.lane, h_lane, sizeof(uint32_t) * Tp, cudaMemcpyHostToDevice, st));
   NA_CUDA(cudaMemcpyAsync(l.op, h_op, sizeof(double) * 9 * Tp, cudaMemcpyHostToDevice, st));
   NA_CUDA(cudaMemcpyAsync(l.plast, h_plast, sizeof(Vec4<S>) * 2 * Tp, cudaMemcpyHostToDevice, st));
@@ -389,7 +411,7 @@ int32_t stepLocked(int32_t device, const tl_mesh_desc& d, int32_t dtype, void* p
   NA_CUDA(cudaMemsetAsync(l.yielding, 0, sizeof(uint32_t), st));
   NA_CUDA(cudaMemsetAsync(l.orec, 0, sizeof(OpRec<S>) * Tp, st));
   NA_CUDA(cudaMemsetAsync(l.onorm, 0, sizeof(Vec4<S>) * 2 * Tp, st));
-  const Sys<S> s = viewOf(l, Vp, Tp);
+  const Sys<S> s = viewOf(l, Vp, Tp, d.element_youngs != nullptr);
   const uint32_t nodeTiles = Vp / TILE, elemTiles = Tp / TILE;
   uint32_t launches = 0;
   // ---- predictor inversion test -> substeps
@@ -417,24 +439,26 @@ int32_t stepLocked(int32_t device, const tl_mesh_desc& d, int32_t dtype, void* p
                ? TL_OK
                : TL_ERR_CUDA;
   };
-  auto element = [&](const Vec4<S>* base, const Vec4<S>* dir, uint32_t pass, uint32_t mode) {
+  auto element = [&](const Vec4<S>* base, const Vec4<S>* dir, uint32_t pass, uint32_t mode) -> int32_t {
     if (!(mode & EM_COMMIT)) {
-      cudaMemsetAsync(l.loading, 0, sizeof(uint32_t), st);
-      cudaMemsetAsync(l.yielding, 0, sizeof(uint32_t), st);
+      if (cudaMemsetAsync(l.loading, 0, sizeof(uint32_t), st) != cudaSuccess ||
+          cudaMemsetAsync(l.yielding, 0, sizeof(uint32_t), st) != cudaSuccess)
+        return TL_ERR_CUDA;
     }
     if (law == TL_LAW_SNH) kElement<S, 1><<<elemTiles, TILE, 0, st>>>(s, base, dir, pass, mode, 0.0);
     else kElement<S, 0><<<elemTiles, TILE, 0, st>>>(s, base, dir, pass, mode, 0.0);
     ++launches;
+    return cudaGetLastError() == cudaSuccess ? TL_OK : TL_ERR_CUDA;
   };
   // ---- substeps: predictor, the three anchored reads (solver.cc:3914-3950), update, plastic commit
   for (uint32_t pass = 0; pass < h_step.substeps; ++pass) {
     kPredict<S><<<nodeTiles, TILE, 0, st>>>(s, pass);
-    element(l.weighted, nullptr, pass, EM_MAPPING);
+    if (element(l.weighted, nullptr, pass, EM_MAPPING) != TL_OK) return TL_ERR_CUDA;
     kNodeAssemble<S><<<nodeTiles, TILE, 0, st>>>(s, nullptr, pass);
     launches += 2;
     if (pcg(l.a, pass, false) != TL_OK) return TL_ERR_CUDA;
     for (uint32_t read = 1; read != 3u; ++read) {
-      element(l.weighted, l.a, pass, EM_MAPPING);
+      if (element(l.weighted, l.a, pass, EM_MAPPING) != TL_OK) return TL_ERR_CUDA;
       kNodeAssemble<S><<<nodeTiles, TILE, 0, st>>>(s, l.a, pass);
       ++launches;
       if (pcg(l.incr, pass, true) != TL_OK) return TL_ERR_CUDA;
@@ -443,7 +467,7 @@ int32_t stepLocked(int32_t device, const tl_mesh_desc& d, int32_t dtype, void* p
     }
     kUpdate<S><<<nodeTiles, TILE, 0, st>>>(s, pass);
     ++launches;
-    if (anyYields) element(l.u, nullptr, pass, EM_MAPPING | EM_COMMIT);
+    if (anyYields && element(l.u, nullptr, pass, EM_MAPPING | EM_COMMIT) != TL_OK) return TL_ERR_CUDA;
   }
   kStepEnd<S><<<nodeTiles, TILE, 0, st>>>(s);
   kFinalize<<<1, TILE, 0, st>>>(l.body, l.epart, l.npart, l.acc, 0);

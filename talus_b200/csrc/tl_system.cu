@@ -238,6 +238,7 @@ struct SystemBase {
   virtual void tune(uint32_t blocksPerSm, uint32_t graph) = 0;
   virtual void setSolver(uint32_t form) = 0;
   virtual void setPlasticity(uint32_t mode) = 0;
+  virtual void expireWait(int32_t solve) = 0;
   virtual bool plasticUsed(uint32_t law) const = 0;
   virtual void setFlowLimits(uint32_t body, uint32_t lane, double crushStress, double crushLimit,
                              double plasticMax) = 0;
@@ -261,6 +262,14 @@ struct tl_rollout {
 };
 
 namespace {
+
+// One block at the persistent kernels' grid barrier with one barrier already
+// counted: the goal (two arrivals) needs an arrival that never comes, so the
+// bounded wait runs out and records TL_ERR_TIMEOUT.
+__global__ void __launch_bounds__(TILE) kWaitLimitCheck(GridSyncDev* sync) {
+  unsigned int k = 1;
+  (void)countBarrier(sync, k);
+}
 
 template <class S> struct Rollout;
 
@@ -1113,7 +1122,17 @@ struct System final : SystemBase {
     check();
     if (profiling) mark(1, false);
   }
+  // tl_system_expire_wait: the step's PCG solve number expireSolve (from 0)
+  // is preceded by the bounded-wait self test on this system's barrier word.
+  int64_t expireSolve = -1;
+  uint64_t solveCount = 0;  // PCG solves issued in the current step
   void pcg(int law, Vec4<S>* X, uint32_t pass, bool x0zero, bool tangent) {
+    if (expireSolve >= 0 && solveCount == uint64_t(expireSolve)) {
+      kWaitLimitCheck<<<1, TILE, 0, st>>>(sync.ptr);
+      check();
+      expireSolve = -1;
+    }
+    ++solveCount;
     kPcgPrepare<S><<<1, TILE, 0, st>>>(view(), pass);
     check();
     Sys<S> s = view();
@@ -1216,14 +1235,18 @@ struct System final : SystemBase {
       if (!hb[b].anyAnchored && set.rigid_split != TL_RIGID_SPLIT_OFF)
         throw StatusError{TL_ERR_UNSUPPORTED, "floating bodies (no anchored node, rigid split on) are not supported"};
     launches = 0;
+    solveCount = 0;
     profiling = (set.flags & TL_FLAG_PROFILE) != 0u;
     tracing = (set.flags & TL_FLAG_TRACE) != 0u;
     evUsed.clear();
+    // the barrier error word is cleared once per step; a wait that runs out in
+    // any of the step's solves is reported when the step ends
+    TL_CUDA(cudaMemsetAsync(&sync.ptr->error, 0, sizeof(int), st));
     {
       const bool yieldsLaw = law == TL_LAW_COROTATED && !hencky &&
                              std::any_of(hb.begin(), hb.end(), [](const HostBody& h) { return h.anyYields; });
       const bool newtonNeeded = set.plastic_passes > 1u && yieldsLaw;
-      if (B > 1 && !newtonNeeded && tuneGraph && !graphBroken && !tracing && !hencky) {
+      if (B > 1 && !newtonNeeded && tuneGraph && !graphBroken && !tracing && !hencky && expireSolve < 0) {
         const int32_t rc = stepGraph(set, gvec, dt, reports, law, yieldsLaw);
         if (rc != TL_ERR_UNSUPPORTED) return rc;  // unsupported: capture refused, fall through to launches
       }
@@ -1385,6 +1408,7 @@ struct System final : SystemBase {
   void enqueueStep(int law, uint32_t passes, bool yieldsLaw) {
     TL_CUDA(cudaMemcpyAsync(dStepVar.ptr, hStepVar.ptr, sizeof(BodyStepDev) * 2 * B, cudaMemcpyHostToDevice, st));
     const uint32_t bb = (B + 255) / 256;
+    TL_CUDA(cudaMemsetAsync(&sync.ptr->error, 0, sizeof(int), st));
     kAccReset<<<bb, 256, 0, st>>>(acc.ptr, cgrep.ptr, B);
     kStepSelect<<<bb, 256, 0, st>>>(dStep.ptr, dStepVar.ptr, acc.ptr, B, 0u);
     kInversionCheck<S><<<elemTiles, TILE, 0, st>>>(view());
@@ -1528,6 +1552,7 @@ struct System final : SystemBase {
   std::vector<std::pair<int, size_t>> graphEv;  // event pairs recorded by the captured graph
 
   void setSolver(uint32_t form) override { solverForm = form; }
+  void expireWait(int32_t solve) override { expireSolve = solve; }
   void setFlowLimits(uint32_t b, uint32_t lane, double crushStress, double crushLimit, double plasticMax) override {
     if (b >= B || lane >= hb[b].lanes) throw StatusError{TL_ERR_ARG, "no such body or material lane"};
     const size_t at = size_t(3) * (hb[b].laneBase + lane);
@@ -1889,6 +1914,7 @@ struct Rollout final : RolloutBase {
     vb.zero(sys.st);
     ab.zero(sys.st);
     ebar.zero(sys.st);
+    TL_CUDA(cudaMemsetAsync(&sys.sync.ptr->error, 0, sizeof(int), sys.st));
     if (dxT) sys.setNodes(bd, h, xb, dxT, false);
     if (dvT) sys.setNodes(bd, h, vb, dvT, false);
     cudaEvent_t e0, e1;
@@ -2030,16 +2056,6 @@ const char* tl_ctx_last_error(const tl_ctx* ctx) { return ctx ? ctx->last_error.
 
 }  // extern "C"
 
-namespace {
-// One block at the persistent kernels' grid barrier with one barrier already
-// counted: the goal (two arrivals) needs an arrival that never comes, so the
-// bounded wait runs out and records TL_ERR_TIMEOUT.
-__global__ void __launch_bounds__(TILE) kWaitLimitCheck(GridSyncDev* sync) {
-  unsigned int k = 1;
-  (void)countBarrier(sync, k);
-}
-}  // namespace
-
 extern "C" {
 
 int32_t tl_ctx_check_wait_limit(tl_ctx* ctx) {
@@ -2099,6 +2115,12 @@ int32_t tl_system_tune(tl_system* system, uint32_t pcg_blocks_per_sm, uint32_t g
     system->impl->tune(pcg_blocks_per_sm, graph);
     return TL_OK;
   });
+}
+
+int32_t tl_system_expire_wait(tl_system* system, int32_t solve) {
+  if (!system) return TL_ERR_ARG;
+  system->impl->expireWait(solve < 0 ? -1 : solve);
+  return TL_OK;
 }
 
 int32_t tl_system_set_solver(tl_system* system, uint32_t form) {

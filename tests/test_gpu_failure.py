@@ -8,6 +8,7 @@ Afterwards the same context steps a body normally.  The host-side failure
 paths (a rank that raises, never joins) are covered with gloo ranks in
 test_shard.
 """
+import ctypes as C
 import time
 
 import numpy as np
@@ -36,3 +37,23 @@ def test_bounded_wait_runs_out_with_a_status_and_the_context_stays_usable():
     assert np.isfinite(system.get_state().position).all()
     system.close()
     ctx.close()
+
+
+@pytest.mark.parametrize("solve", [0, 1])
+def test_a_wait_that_runs_out_in_an_early_solve_is_reported_at_the_step_end(solve):
+    """The elastic step runs three PCG solves.  When the barrier wait of an
+    early one runs out, the later solves of the same step must not erase the
+    record: the step returns TL_ERR_TIMEOUT.  The next step runs normally."""
+    mesh, mat = elastic_block((4, 4, 4), seed=6)
+    system = tb.System(mesh, [mat], tb.FP64)
+    system.set_state(tb.rest_state(mesh))
+    assert capi.lib().tl_system_expire_wait(system.handle, solve) == capi.TL_OK
+    reports = (tb.StepReport * 1)()
+    g = np.asarray(GRAVITY, np.float64)
+    rc = capi.lib().tl_step(system.handle, C.byref(tb.Settings()._c()), g.ctypes.data, DT, reports)
+    assert rc == capi.TL_ERR_TIMEOUT
+    system.set_state(tb.rest_state(mesh))
+    report = system.step(tb.Settings(), GRAVITY, DT)[0]
+    assert report.cg_iterations > 0
+    assert np.isfinite(system.get_state().position).all()
+    system.close()

@@ -85,3 +85,41 @@ def test_noalloc_refuses_meshes_beyond_its_capacity():
     rc = call_noalloc(body, arrays, tb.Settings(), capi.tl_step_report())
     assert rc == capi.TL_ERR_TOO_LARGE
     assert capi.lib().tl_status_string(rc) == b"input exceeds the fixed capacity of tl_step_noalloc"
+
+
+@pytest.mark.gpu
+def test_noalloc_step_honours_per_element_youngs_modulus():
+    """A mesh with per-element Young's moduli steps like the resident system
+    given the same moduli (and unlike the lane's own modulus)."""
+    mesh, mat = elastic_block((6, 6, 6), seed=4)
+    rng = np.random.default_rng(11)
+    mesh.element_youngs = mat.youngs_modulus * np.exp(0.3 * rng.standard_normal(mesh.tets))
+    settings = tb.Settings(law=tb.NEO_HOOKEAN)
+    body = _Body(mesh, [mat])
+    mine, ref = host_arrays(mesh), host_arrays(mesh)
+    system = tb.System(mesh, [mat], tb.FP64)
+    for call in range(2):
+        assert call_noalloc(body, mine, settings, capi.tl_step_report()) == capi.TL_OK
+        assert call_host(system, ref, settings, capi.tl_step_report()) == capi.TL_OK
+        assert relative_error(mine["position"], ref["position"], mesh.rest_positions) <= 1e-9, call
+    system.close()
+    mesh.element_youngs = None
+    lane_only = host_arrays(mesh)
+    plain = _Body(mesh, [mat])
+    for call in range(2):
+        assert call_noalloc(plain, lane_only, settings, capi.tl_step_report()) == capi.TL_OK
+    assert relative_error(lane_only["position"], ref["position"], mesh.rest_positions) > 1e-6
+
+
+@pytest.mark.gpu
+def test_noalloc_refuses_only_damping_an_element_uses():
+    """An unused damped lane, or one with infinite damping (no damping), is
+    accepted; a damped lane an element uses is refused before any work."""
+    mesh, mat = elastic_block((4, 4, 4))
+    damped = tb.PhysicalMaterial(density=1000.0, youngs_modulus=1e6, poissons_ratio=0.3, stiffness_damping=0.02)
+    endless = tb.PhysicalMaterial(density=1000.0, youngs_modulus=1e6, poissons_ratio=0.3,
+                                  stiffness_damping=float("inf"))
+    for lanes, want in (([mat, damped], capi.TL_OK), ([endless], capi.TL_OK), ([damped], capi.TL_ERR_UNSUPPORTED)):
+        arrays = host_arrays(mesh)
+        rc = call_noalloc(_Body(mesh, lanes), arrays, tb.Settings(), capi.tl_step_report())
+        assert rc == want, lanes
