@@ -988,6 +988,121 @@ template <class R> struct Solver {
   }
 };
 
+// ------------------------------------------------- floating frame ----
+// A body with no anchored node and RigidSplit != Off (floats, solver.cc:2964-2971)
+// is stepped in a frame that moves with its centre of mass and turns with its
+// rigid spin: the predictor, the drive of the fictitious forces, and the
+// end-of-substep momentum and torque projection (solver.cc:3657-3690,
+// 4265-4340).  The frame itself is FP64 like the reference's (floatingFrame,
+// solver.cc:3046-3142; rigidAdvance, solver.cc:2983-3036) and stored in R.
+
+constexpr double FLOATING_TOLERANCE = 1.0e-5;  // solver.cc:9
+constexpr uint32_t RIGID_PARTS = 8u;           // solver.h:109
+
+// solver.h:111-114 RigidMotion: angular momentum and accumulated turn
+struct RigidMotion { V3<double> momentum; M3<double> turn{1.0}; };
+
+// solver.cc:2973-2979 skew: skew(a) v = a x v
+inline M3<double> skew(const V3<double>& a) {
+  return M3<double>(V3<double>(0.0, a.z, -a.y), V3<double>(-a.z, 0.0, a.x), V3<double>(a.y, -a.x, 0.0));
+}
+
+// solver.cc:2983-2988 rigidRate: torque-free rigid body, inertia fixed in the world
+inline RigidMotion rigidRate(const M3<double>& inverseInertia, const RigidMotion& at) {
+  const V3<double> spin = inverseInertia * at.momentum;
+  return RigidMotion{cross(at.momentum, spin), at.turn * skew(spin)};
+}
+
+// solver.cc:2990-3030 rigidAdvance: `count` classic Runge-Kutta steps over
+// `span`, then three polar passes that pull the turn back to a rotation
+inline RigidMotion rigidAdvance(const M3<double>& inverseInertia, RigidMotion motion, double span, uint32_t count) {
+  const double part = span / double(count);
+  const auto moved = [](const RigidMotion& from, const RigidMotion& rate, double by) {
+    return RigidMotion{from.momentum + by * rate.momentum, from.turn + by * rate.turn};
+  };
+  for (uint32_t at = 0; at != count; ++at) {
+    const RigidMotion first = rigidRate(inverseInertia, motion);
+    const RigidMotion second = rigidRate(inverseInertia, moved(motion, first, 0.5 * part));
+    const RigidMotion third = rigidRate(inverseInertia, moved(motion, second, 0.5 * part));
+    const RigidMotion fourth = rigidRate(inverseInertia, moved(motion, third, part));
+    motion.momentum += (part / 6.0) * (first.momentum + 2.0 * second.momentum + 2.0 * third.momentum + fourth.momentum);
+    motion.turn = motion.turn + (part / 6.0) * (first.turn + 2.0 * second.turn + 2.0 * third.turn + fourth.turn);
+  }
+  for (uint32_t pass = 0; pass != 3u; ++pass) motion.turn = 0.5 * (motion.turn + transpose(inverse(motion.turn)));
+  return motion;
+}
+
+// solver.cc:2944-2961 FloatingFrame
+template <class R> struct FloatingFrame {
+  V3<R> centre, velocity, acceleration, nextCentre, nextVelocity, nextAcceleration, momentum, torque, spin, spinRate,
+      weightedSpin, weightedRate, endSpin, endRate;
+  M3<R> turn{R(1)}, weightedTurn{R(1)};
+};
+
+template <class R> V3<R> narrow(const V3<double>& v) { return V3<R>(R(v.x), R(v.y), R(v.z)); }
+template <class R> V3<double> widen(const V3<R>& v) { return V3<double>(double(v.x), double(v.y), double(v.z)); }
+template <class R> M3<R> narrow(const M3<double>& m) { return M3<R>(narrow<R>(m[0]), narrow<R>(m[1]), narrow<R>(m[2])); }
+
+// solver.cc:3038-3142 floatingFrame
+template <class R>
+FloatingFrame<R> floatingFrame(const std::vector<R>& nodeMass, const std::vector<V3<R>>& position,
+                               const std::vector<V3<R>>& velocity, const std::vector<V3<R>>& acceleration,
+                               const IntegratorRule<R>& rule, R inner, const V3<R>& gravity) {
+  V3<double> centre, vel, acc;
+  double total = 0.0;
+  for (size_t n = 0; n < position.size(); ++n) {
+    const double mass = double(nodeMass[n]);
+    total += mass;
+    centre += mass * widen(position[n]);
+    vel += mass * widen(velocity[n]);
+    acc += mass * widen(acceleration[n]);
+  }
+  const auto over = [](const V3<double>& v, double d) { return V3<double>(v.x / d, v.y / d, v.z / d); };
+  centre = over(centre, total);
+  vel = over(vel, total);
+  acc = over(acc, total);
+  M3<double> inertia(0.0);
+  V3<double> momentum, torque;
+  for (size_t n = 0; n < position.size(); ++n) {
+    const double mass = double(nodeMass[n]);
+    const V3<double> arm = widen(position[n]) - centre;
+    inertia = inertia + mass * (dot(arm, arm) * M3<double>(1.0) - outer(arm, arm));
+    momentum += mass * cross(arm, widen(velocity[n]) - vel);
+    torque += mass * cross(arm, widen(acceleration[n]) - acc);
+  }
+  FloatingFrame<R> made;
+  const double h = double(inner);
+  const double alphaMass = double(rule.alphaMass), beta = double(rule.beta), gamma = double(rule.gamma);
+  const V3<double> next = over(widen(gravity) - alphaMass * acc, 1.0 - alphaMass);
+  made.centre = narrow<R>(centre);
+  made.velocity = narrow<R>(vel);
+  made.acceleration = narrow<R>(acc);
+  made.nextAcceleration = narrow<R>(next);
+  made.nextCentre = narrow<R>(centre + h * vel + (h * h) * ((0.5 - beta) * acc + beta * next));
+  made.nextVelocity = narrow<R>(vel + h * ((1.0 - gamma) * acc + gamma * next));
+  made.momentum = narrow<R>(momentum + (h * (1.0 - gamma - gamma * alphaMass / (1.0 - alphaMass))) * torque);
+  made.torque = narrow<R>((-alphaMass / (1.0 - alphaMass)) * torque);
+  const double det = determinant(inertia);
+  const double scale = inertia[0][0] + inertia[1][1] + inertia[2][2];
+  if (!(det > 1.0e-12 * scale * scale * scale) || dot(momentum, momentum) == 0.0) return made;
+  const M3<double> inv = inverse(inertia);
+  const double weighted = (1.0 - double(rule.alphaForce)) * h;
+  const RigidMotion start{momentum, M3<double>(1.0)};
+  const RigidMotion middle = rigidAdvance(inv, start, weighted, RIGID_PARTS);
+  const RigidMotion end = rigidAdvance(inv, middle, h - weighted, RIGID_PARTS);
+  const auto spinOf = [&](const RigidMotion& at) { return inv * at.momentum; };
+  const auto rateOf = [&](const RigidMotion& at) { return inv * cross(at.momentum, inv * at.momentum); };
+  made.spin = narrow<R>(spinOf(start));
+  made.spinRate = narrow<R>(rateOf(start));
+  made.weightedSpin = narrow<R>(spinOf(middle));
+  made.weightedRate = narrow<R>(rateOf(middle));
+  made.endSpin = narrow<R>(end.turn * spinOf(end));
+  made.endRate = narrow<R>(end.turn * rateOf(end));
+  made.turn = narrow<R>(end.turn);
+  made.weightedTurn = narrow<R>(middle.turn);
+  return made;
+}
+
 template <class R>
 int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, uint32_t lanes, const or_settings* settings,
              const double gravity[3], double dtIn, or_report* report) {
@@ -1016,9 +1131,8 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
     s.acceleration[n] = V3<R>(R(st->acceleration[3 * n]), R(st->acceleration[3 * n + 1]), R(st->acceleration[3 * n + 2]));
     anyAnchored = anyAnchored || s.anchored[n] != 0;
   }
-  // The floating (rigid split) path (solver.cc:2964-2971, 3659-3690) is out of
-  // scope; with RigidSplit::Off an unanchored body takes the ordinary path.
-  if (!anyAnchored && settings->rigid_split != 0u) return -2;
+  // floats (solver.cc:2964-2971): no anchored node and the rigid split on
+  const bool floating = settings->rigid_split != 0u && V > 0u && !anyAnchored;
   s.elements.resize(T);
   s.store.resize(T);
   s.rotation.resize(T);
@@ -1094,26 +1208,55 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
   const bool newton = settings->plastic_passes > 1u && anyYields;
   const uint32_t plasticCap = settings->plastic_passes;
   s.bindStiffness(false, anyYields);
-  const R tolerance = R(settings->tolerance);
-  const uint32_t substeps =
-      s.predictorInverts(rule, dt / R(configured)) ? std::max(configured, INVERTED_SUBSTEPS) : configured;
+  // solver.cc:3560-3562, 3574-3583: a floating body solves to at most
+  // FLOATING_TOLERANCE and is not tested for predictor inversion
+  const R tolerance = floating ? std::min(R(settings->tolerance), R(FLOATING_TOLERANCE)) : R(settings->tolerance);
+  const uint32_t substeps = !floating && s.predictorInverts(rule, dt / R(configured))
+                                ? std::max(configured, INVERTED_SUBSTEPS)
+                                : configured;
   const R inner = dt / R(substeps);
   const EffectiveSystem<R> effective = effectiveSystem(rule, inner);
   const R carryScale = (R(0.5) - rule.beta) * inner * inner;
   s.dampScale = (R(1) - rule.alphaForce) * rule.gamma * inner;
   std::vector<V3<R>> viscous(s.damped ? V : 0u), viscousVelocity(s.damped ? V : 0u);
-  const int mode = OR_ROTATION_INVERTIBLE;  // anchored meshes never float (solver.cc:3589-3590)
+  const int mode = floating ? OR_ROTATION_POLAR : OR_ROTATION_INVERTIBLE;  // solver.cc:3587-3588
+  std::vector<V3<R>> relative(floating ? V : 0u), unconstrained(floating ? V : 0u);
   report->substeps += substeps;
   R elastic = 0;
   bool plasticGrowth = false;
 
   for (uint32_t pass = 0; pass != substeps; ++pass) {
-    // predictor, solver.cc:3691-3700 (anchored nodes move with their prescribed velocity)
-    for (uint32_t n = 0; n < V; ++n) {
-      s.carried[n] = s.acceleration[n];
-      s.shifted[n] = s.position[n] + inner * s.velocity[n] + carryScale * s.acceleration[n];
-      s.weighted[n] = (R(1) - rule.alphaForce) * s.shifted[n] + rule.alphaForce * s.position[n];
-      s.drive[n] = s.mass[n] * g;
+    const FloatingFrame<R> body = floating
+                                      ? floatingFrame(s.mass, s.position, s.velocity, s.acceleration, rule, inner, g)
+                                      : FloatingFrame<R>{};
+    if (floating) {
+      // solver.cc:3662-3690: relative velocity and acceleration in the frame
+      // that moves with the centre and turns with the spin; the drive holds
+      // the centrifugal, Euler and Coriolis forces at the weighted time
+      const V3<R> spin = body.spin, held = body.weightedSpin;
+      const R lag = (R(1) - rule.alphaForce) * (R(1) - rule.gamma) * inner;
+      for (uint32_t n = 0; n < V; ++n) {
+        const V3<R> arm = s.position[n] - body.centre;
+        const V3<R> moving = s.velocity[n] - body.velocity - cross(spin, arm);
+        const V3<R> turning = s.acceleration[n] - body.acceleration - cross(body.spinRate, arm) -
+                              cross(spin, cross(spin, arm)) - R(2) * cross(spin, moving);
+        const R m = s.mass[n];
+        relative[n] = moving;
+        s.carried[n] = turning;
+        s.shifted[n] = arm + inner * moving + carryScale * turning;
+        s.weighted[n] = (R(1) - rule.alphaForce) * s.shifted[n] + rule.alphaForce * arm;
+        s.drive[n] = -m * (cross(held, cross(held, s.weighted[n])) + cross(body.weightedRate, s.weighted[n]) +
+                           R(2) * cross(held, moving + lag * turning));
+        s.acceleration[n] = turning;
+      }
+    } else {
+      // predictor, solver.cc:3691-3700 (anchored nodes move with their prescribed velocity)
+      for (uint32_t n = 0; n < V; ++n) {
+        s.carried[n] = s.acceleration[n];
+        s.shifted[n] = s.position[n] + inner * s.velocity[n] + carryScale * s.acceleration[n];
+        s.weighted[n] = (R(1) - rule.alphaForce) * s.shifted[n] + rule.alphaForce * s.position[n];
+        s.drive[n] = s.mass[n] * g;
+      }
     }
     auto assemble = [&](const std::vector<V3<R>>& at, R margin, bool mapping = true) {
       return s.assemble(effective.step, at, false, margin, mode, mapping);
@@ -1127,7 +1270,7 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
             viscousVelocity[n] = V3<R>();
             continue;
           }
-          viscousVelocity[n] = s.velocity[n] + (lag * (R(1) - rule.gamma)) * s.carried[n];
+          viscousVelocity[n] = (floating ? relative[n] : s.velocity[n]) + (lag * (R(1) - rule.gamma)) * s.carried[n];
           if (taken) viscousVelocity[n] += (lag * rule.gamma) * (*taken)[n];
         }
         std::fill(viscous.begin(), viscous.end(), V3<R>());
@@ -1334,11 +1477,61 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
         break;
       }
     }
-    // solver.cc:4350-4369 velocity, solver.cc:5829-5849 position
-    for (uint32_t n = 0; n < V; ++n) {
-      if (s.anchored[n]) continue;
-      s.velocity[n] = s.velocity[n] + inner * ((R(1) - rule.gamma) * s.carried[n] + rule.gamma * s.acceleration[n]);
+    const R spanned = rule.beta * inner * inner;
+    if (floating) {
+      // solver.cc:4265-4340: back from the frame.  The frame's end turn
+      // carries the nodes' frame positions and velocities to the world, the
+      // centre moves on its own generalized-alpha path, and with the
+      // Projected split the body's angular momentum and torque are restored
+      // to the frame's rigid values.
+      V3<double> stray;
+      double weight = 0.0;
+      for (uint32_t n = 0; n < V; ++n) {
+        weight += double(s.mass[n]);
+        stray += double(s.mass[n]) * widen(s.acceleration[n]);
+      }
+      const V3<R> mean = narrow<R>(V3<double>(stray.x / weight, stray.y / weight, stray.z / weight));
+      const V3<R> spin = body.endSpin;
+      M3<double> inertia(0.0);
+      V3<double> momentum, torque;
+      for (uint32_t n = 0; n < V; ++n) {
+        const V3<R> turned = s.acceleration[n] - mean;
+        const V3<R> placed = body.turn * (s.shifted[n] + spanned * turned);
+        const V3<R> moved = body.turn * (relative[n] + inner * ((R(1) - rule.gamma) * s.carried[n] + rule.gamma * turned));
+        const V3<R> reached = body.nextCentre + placed;
+        const V3<R> acc = body.nextAcceleration + cross(body.endRate, placed) + cross(spin, cross(spin, placed)) +
+                          R(2) * cross(spin, moved) + body.turn * turned;
+        unconstrained[n] = body.nextVelocity + cross(spin, placed) + moved;
+        s.acceleration[n] = acc;
+        s.shifted[n] = reached - spanned * acc;
+        relative[n] = placed;
+        const double m = double(s.mass[n]);
+        const V3<double> arm = widen(placed);
+        inertia = inertia + m * (dot(arm, arm) * M3<double>(1.0) - outer(arm, arm));
+        momentum += m * cross(arm, widen(unconstrained[n] - body.nextVelocity));
+        torque += m * cross(arm, widen(acc - body.nextAcceleration));
+      }
+      if (settings->rigid_split == 2u && determinant(inertia) > 0.0) {  // RigidSplit::Projected
+        const M3<double> inv = inverse(inertia);
+        const V3<R> restore = narrow<R>(inv * (widen(body.momentum) - momentum));
+        const V3<R> settle = narrow<R>(inv * (widen(body.torque) - torque));
+        for (uint32_t n = 0; n < V; ++n) {
+          const V3<R> turning = cross(settle, relative[n]);
+          unconstrained[n] += cross(restore, relative[n]);
+          s.acceleration[n] += turning;
+          s.shifted[n] -= spanned * turning;
+        }
+      }
+      for (uint32_t n = 0; n < V; ++n) s.velocity[n] = unconstrained[n];
+      for (uint32_t e = 0; e < T; ++e) s.rotation[e] = body.turn * s.rotation[e];
+    } else {
+      // solver.cc:4341-4358 velocity
+      for (uint32_t n = 0; n < V; ++n) {
+        if (s.anchored[n]) continue;
+        s.velocity[n] = s.velocity[n] + inner * ((R(1) - rule.gamma) * s.carried[n] + rule.gamma * s.acceleration[n]);
+      }
     }
+    // solver.cc:5829-5849 position
     for (uint32_t n = 0; n < V; ++n) {
       if (s.anchored[n]) {
         s.velocity[n] = s.prescribed[n];
@@ -1346,7 +1539,7 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
         s.position[n] = s.position[n] + inner * s.prescribed[n];
         continue;
       }
-      s.position[n] = s.shifted[n] + (rule.beta * inner * inner) * s.acceleration[n];
+      s.position[n] = s.shifted[n] + spanned * s.acceleration[n];
     }
     // solver.cc:5860-5861
     if (!s.hencky) plasticGrowth = s.commitPlastic(mode) || plasticGrowth;

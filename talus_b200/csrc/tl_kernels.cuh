@@ -68,6 +68,8 @@ struct BodyDev {
 struct BodyStepDev {
   uint32_t substeps;  // body takes part in pass p iff p < substeps
   uint32_t limit;     // PCG iteration cap
+  uint32_t floating;  // floats (solver.cc:2964-2971): no anchored node, rigid split on
+  uint32_t projected; // RigidSplit::Projected: momentum and torque restored each substep
   double inner, carry, alpha_f, alpha_m, beta, gamma;
   double inertia, hstep, scale;  // (1 - alpha_m), h_eff, h_eff^2
   double gx, gy, gz;
@@ -101,6 +103,23 @@ struct CgReportDev {
   uint32_t iterations, capped, applications, solves, tangent_iterations, pad;
   double worst_rel;
 };
+
+// Floating frame of one body (FloatingFrame, solver.cc:2944-2961), FP64.
+// Positions are kept relative to the body's rest centre of mass X0 (fixed at
+// creation): `shift` is the current centre minus X0, so a node's arm from the
+// centre is (X - X0) + (u - shift) with no large coordinate in it.
+struct FrameDev {
+  double rest_centre[3];  // X0: mass-weighted rest centre
+  double mass;            // total mass
+  double shift[3], velocity[3], acceleration[3];
+  double next_shift[3], next_velocity[3], next_acceleration[3];
+  double momentum[3], torque[3];
+  double spin[3], spin_rate[3], weighted_spin[3], weighted_rate[3], end_spin[3], end_rate[3];
+  double turn[9];         // row-major end turn of the substep
+  double mean[3];         // mass-weighted mean of the solved frame acceleration
+  double restore[3], settle[3];
+};
+constexpr int FRAME_PART = 12;  // per node tile partial sums of the frame moments
 
 struct GridSyncDev {
   unsigned int arrive;
@@ -199,6 +218,11 @@ template <class S> struct Sys {
   // finite-strain plastic flow (null unless the system's plasticity is Hencky)
   double* hk;                  // [10][Tp] plastic map P = Fp^-1 (9 planes, row-major), hardening variable
   const double* flim;          // [3 lanes] per material lane: crush stress, crush limit, plastic cap
+  // floating bodies (null until a step has a floating body)
+  FrameDev* frame;             // [bodies]
+  double* fpart;               // [node_tiles][FRAME_PART] frame moment partials
+  Vec4<S>* relv;               // frame velocity of each node, then its world arm at the substep end
+  Vec4<S>* drive;              // external and fictitious force of each node (replaces m g)
 };
 
 constexpr int TILE_OFF_STRIDE = 4 * TILE + 4;  // 4 TILE + 1 offsets, padded to 8-byte rows
@@ -430,6 +454,36 @@ __global__ void __launch_bounds__(TILE) kPredict(Sys<S> s, uint32_t pass) {
   if (n >= s.body[b].node_end) return;
   const BodyStepDev& st = s.step[b];
   const V3<double> u = cvt<double>(xyz(s.u[n])), v = cvt<double>(xyz(s.v[n])), a = cvt<double>(xyz(s.a[n]));
+  if (st.floating) {
+    // solver.cc:3662-3690 in the frame of the body's centre and spin.  Frame
+    // positions are kept as displacements from the rest arm X - X0: uf = u - shift.
+    const FrameDev& f = s.frame[b];
+    const V3<double> rest = cvt<double>(xyz(s.rest4[n]));
+    const V3<double> restArm = rest - V3<double>{f.rest_centre[0], f.rest_centre[1], f.rest_centre[2]};
+    const V3<double> uf = u - V3<double>{f.shift[0], f.shift[1], f.shift[2]};
+    const V3<double> arm = restArm + uf;
+    const V3<double> spin = {f.spin[0], f.spin[1], f.spin[2]};
+    const V3<double> moving = v - V3<double>{f.velocity[0], f.velocity[1], f.velocity[2]} - cross(spin, arm);
+    const V3<double> turning = a - V3<double>{f.acceleration[0], f.acceleration[1], f.acceleration[2]} -
+                               cross(V3<double>{f.spin_rate[0], f.spin_rate[1], f.spin_rate[2]}, arm) -
+                               cross(spin, cross(spin, arm)) - 2.0 * cross(spin, moving);
+    const V3<double> sh = uf + st.inner * moving + st.carry * turning;
+    const V3<double> w = (1.0 - st.alpha_f) * sh + st.alpha_f * uf;
+    const V3<double> at = restArm + w;  // the reference's weighted frame position
+    const V3<double> held = {f.weighted_spin[0], f.weighted_spin[1], f.weighted_spin[2]};
+    const V3<double> rate = {f.weighted_rate[0], f.weighted_rate[1], f.weighted_rate[2]};
+    const double lag = (1.0 - st.alpha_f) * (1.0 - st.gamma) * st.inner;
+    const double mass = double(s.rest4[n].w);
+    const V3<double> drive =
+        -mass * (cross(held, cross(held, at)) + cross(rate, at) + 2.0 * cross(held, moving + lag * turning));
+    s.relv[n] = packc<S>(moving);
+    s.carried[n] = packc<S>(turning);
+    s.shifted[n] = packc<S>(sh);
+    s.weighted[n] = packc<S>(w);
+    s.drive[n] = packc<S>(drive);
+    s.a[n] = packc<S>(turning);
+    return;
+  }
   const V3<double> sh = u + st.inner * v + st.carry * a;
   const V3<double> w = (1.0 - st.alpha_f) * sh + st.alpha_f * u;
   s.carried[n] = s.a[n];
@@ -445,6 +499,7 @@ __global__ void __launch_bounds__(TILE) kInversionCheck(Sys<S> s) {
   const uint32_t e = tile * TILE + threadIdx.x;
   if (e >= s.body[b].elem_end) return;
   const BodyStepDev& st = s.step[b];
+  if (st.floating) return;  // a floating body is not tested (solver.cc:3574-3583)
   const uint4 t = __ldg(&s.tet[e]);
   const uint32_t nodes[4] = {t.x, t.y, t.z, t.w};
   V3<double> g[4];
@@ -550,7 +605,8 @@ __global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
       F.m[0][0] += 1.0;
       F.m[1][1] += 1.0;
       F.m[2][2] += 1.0;
-      const M3<double> R = elementRotation(F, true);
+      // ElementRotation::Polar for floating bodies, Invertible otherwise (solver.cc:3587-3588)
+      const M3<double> R = elementRotation(F, st.floating == 0u);
       // Corotated strain (material.cc:92-109, 155-161): the offsets
       // R^T (x_c - x_mean) - (X_c - X_mean) summed against g_c.  Because
       // sum_c g_c = 0 and sum_c X_c g_c^T = Ds Dm^-1 = I, that sum is
@@ -835,8 +891,11 @@ __global__ void __launch_bounds__(TILE) kNodeAssemble(Sys<S> s, const Vec4<S>* t
     } else {
       const double mass = double(rest.w);
       const V3<double> car = cvt<double>(xyz(s.carried[n]));
-      V3<double> rhs = {f[0] + mass * st.gx - st.alpha_m * mass * car.x, f[1] + mass * st.gy - st.alpha_m * mass * car.y,
-                        f[2] + mass * st.gz - st.alpha_m * mass * car.z};
+      // the drive: m g, or the frame's forces for a floating body (solver.cc:3683-3699)
+      const V3<double> drive = st.floating ? cvt<double>(xyz(s.drive[n])) : V3<double>{mass * st.gx, mass * st.gy,
+                                                                                        mass * st.gz};
+      V3<double> rhs = {f[0] + drive.x - st.alpha_m * mass * car.x, f[1] + drive.y - st.alpha_m * mass * car.y,
+                        f[2] + drive.z - st.alpha_m * mass * car.z};
       if (taken) rhs = rhs - (st.inertia * mass) * cvt<double>(xyz(taken[n]));
       s.right[n] = packc<S>(rhs);
       rr = dot(rhs, rhs);
@@ -1040,7 +1099,8 @@ __global__ void __launch_bounds__(TILE) kDamping(Sys<S> s, const Vec4<S>* base, 
       vv[c] = {0, 0, 0};
       continue;
     }
-    vv[c] = cvt<double>(xyz(s.v[n])) + (lag * (1.0 - st.gamma)) * cvt<double>(xyz(s.carried[n]));
+    // a floating body's viscous velocity is its frame velocity (solver.cc:3757-3759)
+    vv[c] = cvt<double>(xyz(st.floating ? s.relv[n] : s.v[n])) + (lag * (1.0 - st.gamma)) * cvt<double>(xyz(s.carried[n]));
     if (dir) vv[c] = vv[c] + (lag * st.gamma) * cvt<double>(xyz(dir[n]));
   }
   dampingApply(arm, inv, gh, a, bb, vv, dv);
@@ -2526,7 +2586,11 @@ __global__ void __launch_bounds__(TILE) kNewtonAccept(Sys<S> s, uint32_t pass) {
       const BodyStepDev& st = s.step[b];
       const V3<double> tot = cvt<double>(xyz(s.total[n]));
       const V3<double> inc = cvt<double>(xyz(s.incr[n]));
-      const V3<double> ev = cvt<double>(xyz(s.rest4[n])) + cvt<double>(xyz(s.weighted[n])) + st.scale * tot;
+      V3<double> ev = cvt<double>(xyz(s.rest4[n])) + cvt<double>(xyz(s.weighted[n])) + st.scale * tot;
+      if (st.floating) {  // frame positions are arms from the centre
+        const FrameDev& f = s.frame[b];
+        ev = ev - V3<double>{f.rest_centre[0], f.rest_centre[1], f.rest_centre[2]};
+      }
       s.total[n] = packc<S>(tot + inc);
       moved = (unsigned long long)__double_as_longlong(sqrt(dot(inc, inc)));
       extent = (unsigned long long)__double_as_longlong(sqrt(dot(ev, ev)));
@@ -2563,6 +2627,23 @@ __global__ void __launch_bounds__(TILE) kUpdate(Sys<S> s, uint32_t pass) {
   const uint32_t n = tile * TILE + threadIdx.x;
   if (n >= s.body[b].node_end) return;
   const BodyStepDev& st = s.step[b];
+  if (st.floating) {
+    // solver.cc:4325-4338, 5845-5847: the projection's spin corrections, then
+    // the position.  kFrameEnd left the unconstrained velocity in v, the world
+    // acceleration in a and the world arm in relv; restore and settle are
+    // zero unless the split is Projected.
+    const FrameDev& f = s.frame[b];
+    const V3<double> arm = cvt<double>(xyz(s.relv[n]));
+    const V3<double> turning = cross(V3<double>{f.settle[0], f.settle[1], f.settle[2]}, arm);
+    const double spanned = st.beta * st.inner * st.inner;
+    const V3<double> v = cvt<double>(xyz(s.v[n])) + cross(V3<double>{f.restore[0], f.restore[1], f.restore[2]}, arm);
+    const V3<double> a = cvt<double>(xyz(s.a[n])) + turning;
+    const V3<double> sh = cvt<double>(xyz(s.shifted[n])) - spanned * turning;
+    s.v[n] = packc<S>(v);
+    s.a[n] = packc<S>(a);
+    s.u[n] = packc<S>(sh + spanned * a);
+    return;
+  }
   if (s.anch[n]) {
     const Vec4<S> pv = s.pres[n];
     s.v[n] = pv;

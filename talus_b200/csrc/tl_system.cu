@@ -7,6 +7,7 @@
 #include "../../include/talus_fem.h"
 #include "tl_kernels.cuh"
 #include "tl_adjoint.cuh"
+#include "tl_floating.cuh"
 #include "tl_sell.cuh"
 #include "tl_sell_build.h"
 #include "tl_validate.h"
@@ -113,6 +114,7 @@ constexpr uint32_t INVERTED_SUBSTEPS = 4u;    // solver.cc:13
 constexpr double LOADING_MARGIN = 1.0e-3;     // solver.cc:372
 constexpr double PLASTIC_REDUCTION = 1.0e-2;  // solver.cc:374
 constexpr double PLASTIC_RESOLUTION = 8.0;    // solver.cc:380
+constexpr double FLOATING_TOLERANCE = 1.0e-5; // solver.cc:9
 
 // Worker threads for the host side of state transfers, started on first use
 // and kept until the process exits (up to 15 workers beside the calling
@@ -208,6 +210,10 @@ struct HostBody {
   uint32_t laneBase = 0, lanes = 0;  // the body's material lanes in the system's lane table
   bool anyAnchored = false, anyYields = false;
   std::vector<double> rest;  // [3 V] for position <-> displacement
+  double restCentre[3] = {0.0, 0.0, 0.0};  // mass-weighted rest centre (of the stored rest positions)
+  double mass = 0.0;
+  // floats (solver.cc:2964-2971): no anchored node and the rigid split on
+  bool floats(uint32_t split) const { return split != TL_RIGID_SPLIT_OFF && !anyAnchored; }
 };
 
 }  // namespace
@@ -339,6 +345,55 @@ struct System final : SystemBase {
   DevBuf<double> hk;         // [10][Tp] plastic map P (row-major planes), hardening variable
   bool evaluating = false;   // tl_evaluate: element forces only, no damping terms
   DevBuf<S> dtau, dfit;
+  // floating bodies: the frame of each body, moment partials, frame velocities
+  // and drives; allocated by the first step that has a floating body
+  DevBuf<FrameDev> dFrame;
+  DevBuf<double> fpart;
+  DevBuf<Vec4<S>> relv, drive;
+  void ensureFloating() {
+    if (dFrame.ptr) return;
+    std::vector<FrameDev> h(B);
+    for (uint32_t b = 0; b < B; ++b) {
+      std::memset(&h[b], 0, sizeof(FrameDev));
+      for (int k = 0; k < 3; ++k) h[b].rest_centre[k] = hb[b].restCentre[k];
+      h[b].mass = hb[b].mass;
+    }
+    dFrame.alloc(B);
+    dFrame.upload(h.data(), B, st);
+    fpart.alloc(size_t(nodeTiles) * FRAME_PART);
+    fpart.zero(st);
+    relv.alloc(Vp);
+    relv.zero(st);
+    drive.alloc(Vp);
+    drive.zero(st);
+    TL_CUDA(cudaStreamSynchronize(st));
+  }
+  // The frame before the predictor (floatingFrame, solver.cc:3658-3660).
+  void frameBegin(uint32_t pass) {
+    kFrameMoments<S><<<nodeTiles, TILE, 0, st>>>(view(), pass, 0u);
+    check();
+    kFrameSolve<S><<<B, TILE, 0, st>>>(view(), pass, 0u);
+    check();
+    kFrameMoments<S><<<nodeTiles, TILE, 0, st>>>(view(), pass, 1u);
+    check();
+    kFrameSolve<S><<<B, TILE, 0, st>>>(view(), pass, 1u);
+    check();
+  }
+  // Back to the world after the solve (solver.cc:4265-4340), before kUpdate.
+  void frameEnd(uint32_t pass) {
+    kFrameMoments<S><<<nodeTiles, TILE, 0, st>>>(view(), pass, 2u);
+    check();
+    kFrameSolve<S><<<B, TILE, 0, st>>>(view(), pass, 2u);
+    check();
+    kFrameEnd<S><<<nodeTiles, TILE, 0, st>>>(view(), pass);
+    check();
+    kFrameSolve<S><<<B, TILE, 0, st>>>(view(), pass, 3u);
+    check();
+  }
+  void frameTurn(uint32_t pass) {
+    kFrameTurn<S><<<elemTiles, TILE, 0, st>>>(view(), pass);
+    check();
+  }
   // TL_FLAG_PROFILE: event pairs around kernel classes, resolved at step end
   bool profiling = false;
   bool tracing = false;
@@ -463,6 +518,10 @@ struct System final : SystemBase {
     s.dtau = hasDamping ? dtau.ptr : nullptr;
     s.dfit = hasDamping ? dfit.ptr : nullptr;
     s.hk = hencky ? hk.ptr : nullptr;
+    s.frame = dFrame.ptr;
+    s.fpart = fpart.ptr;
+    s.relv = relv.ptr;
+    s.drive = drive.ptr;
     return s;
   }
 
@@ -537,16 +596,24 @@ struct System final : SystemBase {
         md.pad = 0;
         hMat.push_back(md);
       }
+      double centre[3] = {0.0, 0.0, 0.0};
       for (uint32_t n = 0; n < d.nodes; ++n) {
         const uint32_t g = bd.node_begin + n;
         hRest[g] = Vec4<S>{S(d.rest_positions[3 * n]), S(d.rest_positions[3 * n + 1]), S(d.rest_positions[3 * n + 2]),
                            S(d.node_mass[n])};
+        // rest centre of the stored (S) rest positions and masses, FP64
+        const double m = double(hRest[g].w);
+        h.mass += m;
+        centre[0] += m * double(hRest[g].x);
+        centre[1] += m * double(hRest[g].y);
+        centre[2] += m * double(hRest[g].z);
         hAnch[g] = d.anchored[n] ? 1u : 0u;
         h.anyAnchored = h.anyAnchored || d.anchored[n] != 0;
         if (d.prescribed_velocity && d.anchored[n])
           hPres[g] = Vec4<S>{S(d.prescribed_velocity[3 * n]), S(d.prescribed_velocity[3 * n + 1]),
                              S(d.prescribed_velocity[3 * n + 2]), S(0)};
       }
+      for (int k = 0; k < 3; ++k) h.restCentre[k] = h.mass > 0.0 ? centre[k] / h.mass : 0.0;
       for (uint32_t t = 0; t < d.tets; ++t) {
         const uint32_t e = bd.elem_begin + t;
         uint32_t q[4];
@@ -1231,9 +1298,14 @@ struct System final : SystemBase {
     if (hencky && (set.law != TL_LAW_COROTATED || hasDamping))
       throw StatusError{TL_ERR_UNSUPPORTED, "the finite-strain flow is written for the corotated law without damping"};
     const int law = int(set.law);
-    for (uint32_t b = 0; b < B; ++b)
-      if (!hb[b].anyAnchored && set.rigid_split != TL_RIGID_SPLIT_OFF)
-        throw StatusError{TL_ERR_UNSUPPORTED, "floating bodies (no anchored node, rigid split on) are not supported"};
+    if (set.rigid_split > TL_RIGID_SPLIT_PROJECTED) throw StatusError{TL_ERR_ARG, "unknown rigid split"};
+    bool anyFloating = false;
+    for (uint32_t b = 0; b < B; ++b) {
+      if (!hb[b].floats(set.rigid_split)) continue;
+      if (!(hb[b].mass > 0.0)) throw StatusError{TL_ERR_ARG, "a floating body needs a positive total mass"};
+      anyFloating = true;
+    }
+    if (anyFloating) ensureFloating();
     launches = 0;
     solveCount = 0;
     profiling = (set.flags & TL_FLAG_PROFILE) != 0u;
@@ -1247,7 +1319,7 @@ struct System final : SystemBase {
                              std::any_of(hb.begin(), hb.end(), [](const HostBody& h) { return h.anyYields; });
       const bool newtonNeeded = set.plastic_passes > 1u && yieldsLaw;
       if (B > 1 && !newtonNeeded && tuneGraph && !graphBroken && !tracing && !hencky && expireSolve < 0) {
-        const int32_t rc = stepGraph(set, gvec, dt, reports, law, yieldsLaw);
+        const int32_t rc = stepGraph(set, gvec, dt, reports, law, yieldsLaw, anyFloating);
         if (rc != TL_ERR_UNSUPPORTED) return rc;  // unsupported: capture refused, fall through to launches
       }
     }
@@ -1272,7 +1344,10 @@ struct System final : SystemBase {
       s.gx = gvec[0];
       s.gy = gvec[1];
       s.gz = gvec[2];
-      s.tolerance = set.tolerance;
+      s.floating = hb[b].floats(set.rigid_split) ? 1u : 0u;
+      s.projected = set.rigid_split == TL_RIGID_SPLIT_PROJECTED ? 1u : 0u;
+      // a floating body solves to at most FLOATING_TOLERANCE (solver.cc:3560-3562)
+      s.tolerance = s.floating ? std::min(set.tolerance, FLOATING_TOLERANCE) : set.tolerance;
       s.check_inner = checkInner;
       s.check_carry = (0.5 - rule.beta) * checkInner * checkInner;
     }
@@ -1312,13 +1387,16 @@ struct System final : SystemBase {
                            law == TL_LAW_COROTATED && !hencky;
     std::vector<tl_step_report> local(B);
     for (uint32_t pass = 0; pass < maxSub; ++pass) {
+      if (anyFloating) frameBegin(pass);
       nodeOp(kPredict<S>, pass);
       if (!anyNewton) {
         elasticReads(law, pass);
       } else {
         newton(law, pass, set, rule, hs[0], local[0]);
       }
+      if (anyFloating) frameEnd(pass);
       nodeOp(kUpdate<S>, pass);
+      if (anyFloating) frameTurn(pass);
       if (anyYields) element(law, u.ptr, nullptr, pass, EM_MAPPING | EM_COMMIT, 0.0);
     }
     if (hencky) {  // flowLattice once per step, after the solve (strainstep.cc:822-825)
@@ -1405,7 +1483,7 @@ struct System final : SystemBase {
   DevBuf<BodyStepDev> dStepVar;
   PinnedBuf<BodyStepDev> hStepVar, hStepOut;
 
-  void enqueueStep(int law, uint32_t passes, bool yieldsLaw) {
+  void enqueueStep(int law, uint32_t passes, bool yieldsLaw, bool anyFloating) {
     TL_CUDA(cudaMemcpyAsync(dStepVar.ptr, hStepVar.ptr, sizeof(BodyStepDev) * 2 * B, cudaMemcpyHostToDevice, st));
     const uint32_t bb = (B + 255) / 256;
     TL_CUDA(cudaMemsetAsync(&sync.ptr->error, 0, sizeof(int), st));
@@ -1415,9 +1493,12 @@ struct System final : SystemBase {
     kStepSelect<<<bb, 256, 0, st>>>(dStep.ptr, dStepVar.ptr, acc.ptr, B, 1u);
     TL_CUDA(cudaGetLastError());
     for (uint32_t pass = 0; pass < passes; ++pass) {
+      if (anyFloating) frameBegin(pass);
       nodeOp(kPredict<S>, pass);
       elasticReads(law, pass);
+      if (anyFloating) frameEnd(pass);
       nodeOp(kUpdate<S>, pass);
+      if (anyFloating) frameTurn(pass);
       if (yieldsLaw) element(law, u.ptr, nullptr, pass, EM_MAPPING | EM_COMMIT, 0.0);
     }
     kStepEnd<S><<<nodeTiles, TILE, 0, st>>>(view());
@@ -1431,7 +1512,7 @@ struct System final : SystemBase {
   }
 
   int32_t stepGraph(const tl_settings& set, const double gvec[3], double dt, tl_step_report* reports, int law,
-                    bool yieldsLaw) {
+                    bool yieldsLaw, bool anyFloating) {
     const uint32_t configured = std::max(set.substeps, 1u);
     const uint32_t passes = std::max(configured, INVERTED_SUBSTEPS);
     const Rule rule = ruleOf(set.spectral_radius);
@@ -1455,7 +1536,9 @@ struct System final : SystemBase {
         s.gx = gvec[0];
         s.gy = gvec[1];
         s.gz = gvec[2];
-        s.tolerance = set.tolerance;
+        s.floating = hb[b].floats(set.rigid_split) ? 1u : 0u;
+        s.projected = set.rigid_split == TL_RIGID_SPLIT_PROJECTED ? 1u : 0u;
+        s.tolerance = s.floating ? std::min(set.tolerance, FLOATING_TOLERANCE) : set.tolerance;
         s.check_inner = dt / double(configured);
         s.check_carry = (0.5 - rule.beta) * s.check_inner * s.check_inner;
         s.inner = dt / double(s.substeps);
@@ -1464,8 +1547,8 @@ struct System final : SystemBase {
         s.hstep = std::sqrt((1.0 - rule.alphaForce) * rule.beta) * s.inner;
         s.scale = s.hstep * s.hstep;
       }
-    const uint64_t key = (uint64_t(law) << 48) | (uint64_t(yieldsLaw) << 40) | (uint64_t(profiling) << 36) |
-                         (uint64_t(configured) << 8) | uint64_t(tuneBlocksPerSm & 0xffu);
+    const uint64_t key = (uint64_t(law) << 48) | (uint64_t(yieldsLaw) << 40) | (uint64_t(anyFloating) << 38) |
+                         (uint64_t(profiling) << 36) | (uint64_t(configured) << 8) | uint64_t(tuneBlocksPerSm & 0xffu);
     if (!graphExec || graphKey != key) {
       if (graphExec) cudaGraphExecDestroy(graphExec);
       graphExec = nullptr;
@@ -1475,7 +1558,7 @@ struct System final : SystemBase {
       launches = 0;
       capturing = true;
       try {
-        enqueueStep(law, passes, yieldsLaw);
+        enqueueStep(law, passes, yieldsLaw, anyFloating);
       } catch (...) {
         capturing = false;
         cudaStreamEndCapture(st, &graph);
@@ -1836,6 +1919,8 @@ struct Rollout final : RolloutBase {
     if (sys.hencky) throw StatusError{TL_ERR_UNSUPPORTED, "a rollout does not differentiate the plastic flow"};
     if (settings.law != TL_LAW_SNH)
       throw StatusError{TL_ERR_UNSUPPORTED, "the adjoint needs the exact tangent of TL_LAW_SNH"};
+    if (sys.hb[0].floats(settings.rigid_split))
+      throw StatusError{TL_ERR_UNSUPPORTED, "the adjoint does not differentiate the floating frame"};
     if (!desc.steps || !desc.checkpoint_every || !desc.newton_reads || !(desc.delta_time > 0.0))
       throw StatusError{TL_ERR_ARG, "rollout needs steps, checkpoint_every, newton_reads >= 1 and dt > 0"};
     segments = (desc.steps + desc.checkpoint_every - 1) / desc.checkpoint_every;

@@ -17,7 +17,11 @@ its hardening variables and a sample of its plastic maps.  tet_laws.npz holds
 48 disconnected tets at seeded deformations (stretched, sheared, rotated,
 three inverted) with each law's element forces.
 
-Run from the repository root:  python -m tests.golden.make_golden
+full_plastic_block.npz is the plastic benchmark block at its full size
+(393,216 tets) after two FP64 oracle steps: a sample of its node positions,
+sums over all nodes and the step counts.
+
+Run from the repository root:  python -m tests.golden.make_golden [name]
 """
 from __future__ import annotations
 
@@ -158,12 +162,57 @@ def write_tet_laws():
                         yielding=yielding, **out)
 
 
-def main():
+# The plastic benchmark block at its full size (64x32x32 cubes, 393,216 tets,
+# 70,785 nodes), two FP64 oracle steps from rest.  The oracle needs one to two
+# minutes per step there (17 and 33 Newton evaluations in these first steps),
+# so the result is stored instead of recomputed in the GPU test: every
+# FULL_SAMPLE-th node's position, and sums over all nodes.
+FULL_STEPS = 2
+FULL_SAMPLE = 8
+
+
+def full_block_case():
+    from talus_b200.workloads import WORKLOADS, make_mesh
+
+    mesh, mat = make_mesh(WORKLOADS["plastic-block"])
+    return mesh, mat, tb.Settings(), FULL_STEPS
+
+
+def position_sums(x, rest):
+    """Sums over every node that a wrong node anywhere would change."""
+    d = x - rest
+    return np.array([d.sum(), np.abs(d).sum(), (d * d).sum(), np.linalg.norm(d, axis=1).max()])
+
+
+def write_full_block():
+    mesh, mat, settings, steps = full_block_case()
+    record = []
+    state, reports = run_oracle(po.F64, mesh, mat, settings, steps, record=record)
+    np.savez_compressed(
+        os.path.join(HERE, "full_plastic_block.npz"),
+        mesh_checksum=mesh_checksum(mesh), material=material_array(mat), steps=steps, sample=FULL_SAMPLE,
+        positions=np.array([r[::FULL_SAMPLE] for r in record]),
+        sums=np.array([position_sums(r, mesh.rest_positions) for r in record]),
+        equivalent_sum=float(state.plastic[:, 9].sum()),
+        yielded=int((state.plastic[:, 9] > 0).sum()),
+        cg_iterations=np.array([r["cg_iterations"] for r in reports]),
+        plastic_evaluations=np.array([r["plastic_evaluations"] for r in reports]),
+        plastic_solves=np.array([r["plastic_solves"] for r in reports]))
+
+
+def main(which=None):
     for name in BLOCKS:
-        write_block(name)
-    write_hencky_block()
-    write_tet_laws()
+        if which in (None, name):
+            write_block(name)
+    if which in (None, "hencky_block"):
+        write_hencky_block()
+    if which in (None, "tet_laws"):
+        write_tet_laws()
+    if which in (None, "full_plastic_block"):
+        write_full_block()
 
 
 if __name__ == "__main__":
-    main()
+    import sys
+
+    main(sys.argv[1] if len(sys.argv) > 1 else None)

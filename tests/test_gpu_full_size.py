@@ -1,7 +1,15 @@
-"""The benchmark workloads at their full sizes, checked through properties
-that hold at any size (the oracle would need minutes per step there; its
-parity with the CUDA path is proven on the reduced blocks of
-test_gpu_parity and test_gpu_golden):
+"""The benchmark workloads at their full sizes.
+
+* plastic block against the FP64 oracle: the oracle's first two steps of the
+  393,216-tet block (17 and 33 Newton evaluations, one to two minutes per
+  step on one CPU core) are stored in tests/golden/full_plastic_block.npz
+  (every 8th node, sums over all nodes, the step counts).  The GPU steps the
+  block with the assembled operator (kSellAssemble, kPcgSell) at the tile,
+  slice and grid shapes the benchmark times: FP64 within 1e-8 relative
+  displacement with the same Newton evaluation and PCG iteration counts,
+  FP32-mixed within 1e-5.
+
+The rest is checked through properties that hold at any size:
 
 * plastic block, 64x32x32 cubes (393,216 tets, 70,785 nodes), 10 steps:
   FP32-mixed within 1e-5 relative displacement of FP64 at every step; the
@@ -13,11 +21,14 @@ test_gpu_parity and test_gpu_golden):
   1e-6, the iteration cap out of reach): FP32-mixed within 1e-5 of FP64 on
   every body, pinned bases at rest.
 """
+import os
+
 import numpy as np
 import pytest
 
 import talus_b200 as tb
 from talus_b200 import workloads
+from tests.golden import make_golden as mg
 from tests.helpers import DT, GRAVITY, relative_error
 
 pytestmark = pytest.mark.gpu
@@ -35,6 +46,36 @@ def run(meshes, mats, precision, settings, steps, record=False):
     states = [system.get_state(i) for i in range(len(meshes))]
     system.close()
     return states, history
+
+
+@pytest.mark.parametrize("precision", [tb.FP64, tb.FP32_MIXED], ids=["fp64", "mixed"])
+def test_plastic_block_at_full_size_matches_the_oracle(precision):
+    g = np.load(os.path.join(os.path.dirname(mg.__file__), "full_plastic_block.npz"))
+    mesh, mat, settings, steps = mg.full_block_case()
+    np.testing.assert_allclose(mg.mesh_checksum(mesh), g["mesh_checksum"], rtol=1e-12)
+    system = tb.System(mesh, [mat], precision)
+    system.set_solver("assembled")
+    system.set_state(tb.rest_state(mesh))
+    sample = int(g["sample"])
+    for k in range(steps):
+        rep = system.step(settings, GRAVITY, DT)[0]
+        x = system.get_state().position
+        want = g["positions"][k]
+        scale = g["sums"][k][3]  # max |x - X| over all nodes
+        err = np.linalg.norm(x[::sample] - want, axis=1).max() / scale
+        if precision == tb.FP64:
+            assert err <= 1e-8, (k, err)
+            np.testing.assert_allclose(mg.position_sums(x, mesh.rest_positions), g["sums"][k], rtol=1e-7)
+            assert rep.plastic_evaluations == g["plastic_evaluations"][k], k
+            assert rep.plastic_solves == g["plastic_solves"][k], k
+            assert rep.cg_iterations == g["cg_iterations"][k], k
+        else:
+            assert err <= 1e-5, (k, err)
+    state = system.get_state()
+    system.close()
+    if precision == tb.FP64:
+        assert int((state.plastic[:, 9] > 0).sum()) == int(g["yielded"])
+        assert state.plastic[:, 9].sum() == pytest.approx(float(g["equivalent_sum"]), rel=1e-8)
 
 
 def test_plastic_block_at_full_size():

@@ -232,17 +232,6 @@ def test_free_fall_follows_the_generalized_alpha_recurrence():
     assert np.abs(state.position[:, [0, 2]] - mesh.rest_positions[:, [0, 2]]).max() <= 1e-12
 
 
-def test_floating_body_with_rigid_split_is_refused():
-    import talus_b200 as tb
-
-    mesh = tb.box_mesh((2, 2, 2), voxel=0.1)
-    mesh.anchored[:] = 0
-    om = po.Mesh(mesh.rest_positions, mesh.node_mass, mesh.anchored, mesh.tet_nodes, mesh.rest_inverse,
-                 mesh.volume, mesh.material)
-    with pytest.raises(RuntimeError):
-        po.step(po.F64, om, po.State.rest(om), [RUBBER], po.Settings(rigid_split=2), (0, -9.81, 0), 1 / 60)
-
-
 def test_pinned_nodes_never_move_and_rest_stays_at_rest():
     import talus_b200 as tb
 
