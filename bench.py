@@ -49,10 +49,11 @@ def batch_sample_count(spec, budget_tets):
     return take, total
 
 
-def sample_bodies(spec, budget_tets=8000):
-    """Bounded CPU sample of a workload: a 1/64 sub-block (1/4 cells per axis,
-    same strain rate) of a single body; the first bodies of a batch up to
-    `budget_tets` tets."""
+def sample_bodies(spec, budget_tets=8000, divide=2):
+    """Bounded CPU sample of a workload: a sub-block with 1/`divide` of the
+    cells per axis (1/divide^3 of the workload, pushed at the same strain
+    rate) of a single body; the first bodies of a batch up to `budget_tets`
+    tets."""
     if spec.get("batch"):
         from talus_b200 import shard
 
@@ -63,10 +64,10 @@ def sample_bodies(spec, budget_tets=8000):
     if full <= 50000:  # small workloads are timed whole
         mesh, mat = make_mesh(spec)
         return [mesh], [[mat]], f"the whole workload ({mesh.tets} tets)"
-    cells = tuple(max(2, c // 4) for c in spec["cells"])
+    cells = tuple(max(2, c // divide) for c in spec["cells"])
     mesh, mat = make_mesh(spec, cells)
-    return [mesh], [[mat]], (f"{cells[0]}x{cells[1]}x{cells[2]} cells ({mesh.tets} tets, 1/64 of the workload, "
-                             f"same strain rate)")
+    return [mesh], [[mat]], (f"{cells[0]}x{cells[1]}x{cells[2]} cells ({mesh.tets} tets, 1/{divide ** 3} of the "
+                             f"workload, same strain rate)")
 
 
 # ----------------------------------------------------------------- clocks --
@@ -223,16 +224,22 @@ def tuning(workload, precision):
 # --------------------------------------------------------------- CPU side --
 
 def cpu_info():
-    model = ""
+    """Host CPU model, logical cores usable by this process and widest SIMD
+    (from the /proc/cpuinfo flags; the oracle is compiled -O2 without -march,
+    so it runs SSE2 code whatever the host offers)."""
+    model, flags = "", set()
     try:
         with open("/proc/cpuinfo") as f:
             for line in f:
-                if line.startswith("model name"):
+                if line.startswith("model name") and not model:
                     model = line.split(":", 1)[1].strip()
-                    break
+                elif line.startswith("flags") and not flags:
+                    flags = set(line.split(":", 1)[1].split())
     except OSError:
         pass
-    return model
+    simd = ("AVX-512 (512-bit)" if "avx512f" in flags else "AVX2 (256-bit)" if "avx2" in flags
+            else "SSE2 (128-bit)" if "sse2" in flags else "unknown")
+    return {"cpu": model, "nproc": host_workers(), "simd": simd, "oracle_simd": "SSE2 (128-bit, -O2, no -march)"}
 
 
 def _oracle_bodies(spec, indices):
@@ -250,10 +257,17 @@ def _oracle_bodies(spec, indices):
 
 
 def _oracle_worker(conn, spec, indices):
-    """A host core stepping its share of the sampled batch bodies on request."""
+    """A host core stepping its share of the sampled batch bodies, or its own
+    copy of a single body's sample sub-block (indices None), on request."""
     from oracle import pyoracle as po
+    from tests.helpers import oracle_material, to_oracle
 
-    bodies = _oracle_bodies(spec, indices)
+    if indices is None:
+        meshes, mats, _ = sample_bodies(spec)
+        bodies = [(to_oracle(m), po.State.rest(to_oracle(m)), [oracle_material(x) for x in mat])
+                  for m, mat in zip(meshes, mats)]
+    else:
+        bodies = _oracle_bodies(spec, indices)
     settings = po.Settings(law=po.LAW_SNH if spec["law"] == "snh" else po.LAW_COROTATED)
     conn.send("ready")
     while conn.recv() == "step":
@@ -263,26 +277,35 @@ def _oracle_worker(conn, spec, indices):
 
 
 class ParallelOracleRun:
-    """Batch bodies are independent, so the reference arm steps a batch sample
-    on every host core: one spawned process per core, each stepping its
-    round-robin share of the sampled bodies with the single-threaded oracle
-    step (the reference's own per-body step is serial)."""
+    """The reference's per-body step is serial (Settings::stepThreads is never
+    read, solver.h:73-74), so the host's cores are used the way a caller of
+    the reference would use them: one spawned process per core, each running
+    the single-threaded oracle step on independent bodies.  A batch sample is
+    split round-robin over the processes; a single-body workload gives every
+    process its own copy of the sample sub-block."""
 
     def __init__(self, spec, workers, budget_tets_per_core=8000):
         import multiprocessing as mp
 
         from talus_b200 import shard
 
-        take, _ = batch_sample_count(spec, budget_tets_per_core * workers)
-        take = max(take, min(spec["count"], 4 * workers))  # several bodies per process, for balance
-        tets = shard.tets_of(shard.batch_dims(spec["count"], spec["seed"], spec["lo"], spec["hi"]))
-        self.tets = total = int(tets[:take].sum())
-        self.sample = f"the first {take} bodies of the batch ({total} tets)"
+        if spec.get("batch"):
+            take, _ = batch_sample_count(spec, budget_tets_per_core * workers)
+            take = max(take, min(spec["count"], 4 * workers))  # several bodies per process, for balance
+            tets = shard.tets_of(shard.batch_dims(spec["count"], spec["seed"], spec["lo"], spec["hi"]))
+            self.tets = total = int(tets[:take].sum())
+            self.sample = f"the first {take} bodies of the batch ({total} tets)"
+            shares = [list(range(w, take, workers)) for w in range(workers)]
+        else:
+            meshes, _, sample = sample_bodies(spec)
+            self.tets = workers * sum(m.tets for m in meshes)
+            self.sample = f"{workers} independent copies of {sample}"
+            shares = [None] * workers
         ctx = mp.get_context("spawn")
         self.conns, self.procs = [], []
         for w in range(workers):
             parent, child = ctx.Pipe()
-            p = ctx.Process(target=_oracle_worker, args=(child, spec, list(range(w, take, workers))), daemon=True)
+            p = ctx.Process(target=_oracle_worker, args=(child, spec, shares[w]), daemon=True)
             p.start()
             self.conns.append(parent)
             self.procs.append(p)
@@ -315,12 +338,12 @@ class OracleRun:
     def close(self):
         pass
 
-    def __init__(self, spec):
+    def __init__(self, spec, divide=2):
         from oracle import pyoracle as po
         from tests.helpers import oracle_material, to_oracle
 
         self.po = po
-        meshes, mats, self.sample = sample_bodies(spec)
+        meshes, mats, self.sample = sample_bodies(spec, divide=divide)
         self.bodies = []
         for m, mat in zip(meshes, mats):
             om = to_oracle(m)
@@ -333,22 +356,46 @@ class OracleRun:
             self.po.step(self.po.F32, om, state, mats, self.settings, (0.0, -9.81, 0.0), 1.0 / 60.0)
 
 
-def cpu_sample(spec, budget_s=15.0, max_steps=400):
-    run = OracleRun(spec)
+def timed_steps(run, warmup, budget_s, min_steps=3, max_steps=400):
+    for _ in range(warmup):
+        run.step()
     steps, t0 = 0, time.perf_counter()
-    while steps < max_steps and time.perf_counter() - t0 < budget_s:
+    while steps < max_steps and (steps < min_steps or time.perf_counter() - t0 < budget_s):
         run.step()
         steps += 1
-    secs = time.perf_counter() - t0
-    return {"value": run.tets * steps / secs, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"oracle FP32 (reference arithmetic), {run.sample}, {steps} steps from rest, 1 thread, "
-                      f"{secs:.1f} s"}
+    return steps, time.perf_counter() - t0
+
+
+def cpu_sample(spec, budget_s=10.0):
+    """The reference arithmetic (oracle FP32) on the host, after 2 warm-up
+    steps from rest: one thread on the 1/8 sub-block (the reference's serial
+    step), one thread on the 1/64 sub-block (a cache-resident size, to show
+    what the smaller sample would inflate), and one process per host core on
+    independent 1/8 sub-blocks."""
+    info = cpu_info()
+    run = OracleRun(spec, divide=2)
+    steps, secs = timed_steps(run, 2, budget_s)
+    out = {"value": run.tets * steps / secs, "unit": UNIT, "cores": 1, "kind": "port",
+           "sample": f"oracle FP32 (reference arithmetic), {run.sample}, 2 warm-up and {steps} timed steps, 1 thread, "
+                     f"{secs:.1f} s", **info}
+    if not spec.get("batch") and 6 * int(np.prod(spec["cells"])) > 50000:
+        small = OracleRun(spec, divide=4)
+        s2, t2 = timed_steps(small, 2, budget_s / 2)
+        out["cache_resident_sample"] = {"value": small.tets * s2 / t2, "sample": small.sample, "steps": s2}
+    workers = host_workers()
+    if workers > 1:
+        par = ParallelOracleRun(spec, workers)
+        s3, t3 = timed_steps(par, 2, budget_s)
+        par.close()
+        out["all_cores"] = {"value": par.tets * s3 / t3, "cores": workers, "sample": par.sample, "steps": s3,
+                            "note": "one process per core, each the serial oracle step on its own bodies"}
+    return out
 
 
 def run_reference(args, spec, rank, world):
     if rank != 0:
         return
-    workers = host_workers() if spec.get("batch") else 1
+    workers = host_workers()
     run = ParallelOracleRun(spec, workers) if workers > 1 else OracleRun(spec)
     for _ in range(args.warmup):
         run.step()
@@ -358,15 +405,16 @@ def run_reference(args, spec, rank, world):
     secs = time.perf_counter() - t0
     run.close()
     value = run.tets * args.steps / secs
+    info = cpu_info()
     sample = (f"oracle FP32 restatement of deformable::step (the reference cannot be built here: GLM/Eigen "
               f"fetched at configure time), {run.sample} of {args.workload}, {workers} host "
-              f"{'process' if workers == 1 else 'processes'} ({cpu_info()})")
+              f"{'process' if workers == 1 else 'processes'} ({info['cpu']}, {info['simd']})")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.workload, "tets": run.tets, "sample": run.sample},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample, **info},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }), flush=True)
 
@@ -572,12 +620,13 @@ def run_ours(args, spec, rank, world, dist):
             result["fp64"]["converged_check"] = converged_check(meshes, mats, law, context)
     if not args.no_adjoint:
         result["adjoint"] = adjoint_ratio(precision, context)
+    if not args.no_batch and not spec.get("batch") and world == 1:
+        result["batch"] = batch_form(context, flush)
     yields = any(np.isfinite(m.yield_stress) and m.yield_stress > 0 for ms in mats for m in ms)
     if not args.no_hencky and not spec.get("batch") and yields:
         result["hencky"] = hencky_form(meshes[0], mats[0], settings, context)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_sample(spec)
-        result["cpu_baseline"]["cpu"] = cpu_info()
     if rank == 0:
         print(json.dumps(result), flush=True)
     system.close()
@@ -690,6 +739,57 @@ def hencky_form(mesh, mats, settings, context, warmup=3, steps=10):
     return out
 
 
+def batch_form(context, flush, warmup=2, steps=5, tolerance=1e-6, cap=4000):
+    """The batching form on its own workload: 512 uneven bodies (cells per
+    axis from U{4..24}, E log-uniform in [1e5, 1e8] Pa, nu in [0.25, 0.45],
+    7,907,508 tets) in one system, FP32-mixed and plain FP64, each from rest
+    with every PCG solve converged (relative residual `tolerance`, the cap out
+    of reach), so that the two arithmetics are compared on the same converged
+    answer.  Device time per step from the step reports (CUDA events), L2
+    flushed before every timed step; the error is the max over all 512 bodies
+    of max|x_mixed - x_fp64| / max|x_fp64 - X| after warmup + steps steps."""
+    import torch
+
+    import talus_b200 as tb
+
+    spec = WORKLOADS["batch"]
+    meshes, mats = make_bodies(spec)
+    settings = tb.Settings(cg_iterations=cap, tolerance=tolerance)
+    out, finals = {}, {}
+    for name, precision in (("mixed", tb.FP32_MIXED), ("fp64", tb.FP64)):
+        system = tb.System(meshes, mats, precision, context)
+        tune = tuning("batch", name)
+        if tune:
+            system.set_solver(tune.get("solver", "auto"))
+            system.tune(tune["pcg_blocks_per_sm"], tune["graph"])
+        for i, m in enumerate(meshes):
+            system.set_state(tb.rest_state(m), i)
+        for _ in range(warmup):
+            system.step(settings)
+        seconds, iters, launches, capped = 0.0, [], 0, 0
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            reps = system.step(settings)
+            seconds += reps[0].device_seconds
+            launches += reps[0].kernel_launches
+            iters.append(max(r.cg_iterations for r in reps))
+            capped += sum(r.cg_capped_solves for r in reps)
+        finals[name] = [system.get_state(i).position for i in range(len(meshes))]
+        system.close()
+        tets = sum(m.tets for m in meshes)
+        out[name] = {"value": tets * steps / seconds, "ms_per_step": seconds * 1e3 / steps,
+                     "max_body_cg_iterations_per_step": float(np.mean(iters)), "gpu_launches": launches,
+                     "capped_solves": capped, "tuning": tune}
+    worst = max(float(np.linalg.norm(a - b, axis=1).max() / np.linalg.norm(b - m.rest_positions, axis=1).max())
+                for a, b, m in zip(finals["mixed"], finals["fp64"], meshes))
+    return {"workload": f"batch, {len(meshes)} bodies, {sum(m.tets for m in meshes)} tets", "unit": UNIT,
+            "pcg_tolerance": tolerance, "pcg_cap": cap, "warmup": warmup, "steps": steps,
+            "mixed": out["mixed"], "fp64": out["fp64"], "mixed_speedup": out["fp64"]["ms_per_step"] /
+            out["mixed"]["ms_per_step"], "max_rel_displacement_error": worst, "bodies_checked": len(meshes),
+            "l2": "flushed (256 MB write) before each timed step"}
+
+
 def adjoint_ratio(precision, context, repeats=3):
     """Differentiable-rollout workload: 16^3 cubes (24,576 tets), 30 steps,
     checkpoints every 5, loss |x_T - x_target|^2; device time of the adjoint
@@ -725,6 +825,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-converged-check", action="store_true")
     ap.add_argument("--no-hencky", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -268,6 +268,16 @@ int32_t tl_step_host(tl_system* system, uint32_t body, int32_t dtype, void* posi
                      void* acceleration, void* rotation, void* plastic, const tl_settings* settings,
                      const double gravity[3], double dt, tl_step_report* report);
 
+/* The last tl_step's per-substep solve records of one body: the reference's
+ * StepReport::cgPerSubstep, cgStartResidual and cgEndResidual
+ * (solver.h:299-301, pushed once per substep at solver.cc:4253-4256).  Per
+ * substep: the PCG iterations summed over its solves, the first solve's
+ * starting relative residual and the last solve's final one.  Writes
+ * min(capacity, substeps, 16) entries of each non-NULL output; *count (or
+ * NULL) gets the substeps the step took (0 before the first step). */
+int32_t tl_step_substeps(const tl_system* system, uint32_t body, uint32_t* iterations, double* start_residual,
+                         double* end_residual, uint32_t capacity, uint32_t* count);
+
 /* Default settings (Settings{} in solver.h:51-107). */
 void tl_settings_default(tl_settings* settings);
 

@@ -13,6 +13,7 @@
 
 #include "talus_fem.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <span>
@@ -20,9 +21,14 @@
 
 namespace talus::deformable::b200 {
 
+// One PreparedMesh resident on the device, with the law its lanes select and
+// the host staging of the element state in the C ABI's row-major layout.
 struct DeviceBody {
   tl_ctx* ctx = nullptr;
   tl_system* system = nullptr;
+  uint32_t law = TL_LAW_COROTATED;
+  uint32_t nodes = 0u, tets = 0u;
+  std::vector<float> rotation, plastic;  // [9 T] committed rotations, [10 T] plastic points
   DeviceBody() = default;
   DeviceBody(const DeviceBody&) = delete;
   DeviceBody& operator=(const DeviceBody&) = delete;
@@ -32,6 +38,23 @@ struct DeviceBody {
   }
 };
 
+// PhysicalMaterial::elasticModel (material.h:7-10, 22) of the lanes the tets
+// use, as the step's law: Corotated is the reference tet law, NeoHookean the
+// stable neo-Hookean law at one point per tet.  A tet whose lane is out of
+// range takes the default material (material.cc:9-16), which is Corotated.
+// The step applies one law to a body, so a body whose tets mix the two
+// models is refused (TL_ERR_UNSUPPORTED).
+inline int32_t lawOf(const talus::PreparedMesh& mesh, std::span<const talus::PhysicalMaterial> lanes, uint32_t& law) {
+  bool corotated = false, neoHookean = false;
+  for (const talus::PreparedTet& t : mesh.tets) {
+    const bool snh = t.material < lanes.size() && lanes[t.material].elasticModel == talus::ElasticModel::NeoHookean;
+    (snh ? neoHookean : corotated) = true;
+  }
+  if (corotated && neoHookean) return TL_ERR_UNSUPPORTED;
+  law = neoHookean ? TL_LAW_SNH : TL_LAW_COROTATED;
+  return TL_OK;
+}
+
 // buildMesh's PreparedMesh (tets only) and its material lanes uploaded once:
 // the replacement for refreshStiffness and buildIncidence (solver.cc:453-507,
 // 1065-1101) on every step.  glm matrices are column-major; the ABI is
@@ -39,6 +62,8 @@ struct DeviceBody {
 inline int32_t upload(const talus::PreparedMesh& mesh, std::span<const talus::PhysicalMaterial> lanes,
                       DeviceBody& out, int32_t precision = TL_FP32_MIXED, int32_t device = 0) {
   const size_t V = mesh.restPositions.size(), T = mesh.tets.size();
+  int32_t rc = lawOf(mesh, lanes, out.law);
+  if (rc != TL_OK) return rc;
   std::vector<double> rest(3 * V), mass(V), rinv(9 * T), vol(T);
   std::vector<uint32_t> nodes(4 * T), lane(T);
   for (size_t n = 0; n < V; ++n) {
@@ -59,10 +84,12 @@ inline int32_t upload(const talus::PreparedMesh& mesh, std::span<const talus::Ph
                     m.hardeningModulus});
   const tl_mesh_desc d{uint32_t(V), uint32_t(T), rest.data(), mass.data(), mesh.anchored.data(), nodes.data(),
                        rinv.data(), vol.data(), lane.data(), mats.data(), uint32_t(mats.size()), nullptr, nullptr};
-  int32_t rc = tl_ctx_create(device, &out.ctx);
+  rc = tl_ctx_create(device, &out.ctx);
   if (rc != TL_OK) return rc;
   rc = tl_system_create(out.ctx, &d, 1, precision, &out.system);
   if (rc != TL_OK) return rc;
+  out.nodes = uint32_t(V);
+  out.tets = uint32_t(T);
   // the finite-strain flow's crush and plastic cap (material.h:16-29), for
   // lanes that set them; read only in TL_PLASTICITY_HENCKY
   for (size_t l = 0; l < lanes.size(); ++l) {
@@ -87,24 +114,77 @@ inline tl_settings settingsOf(const Settings& s) {
 }
 
 // deformable::step(mesh, state, materials, settings, gravity, dt, {}, {},
-// nullptr, report) (solver.h:451-462) with the state in host memory.  The
-// committed rotations are outputs of the step and the plastic points stay on
-// the device (pass them through tl_state_get when the host needs them); the
-// report is accumulated like the reference's (solver.cc:3612-3615).
+// nullptr, report) (solver.h:451-462) with the state in host memory, owned by
+// the caller as in the reference (mesh.h:56-62):
+//  * position, velocity and acceleration are read and written;
+//  * the plastic points (tet e in slot e, tetPoint solver.cc:1177-1190, for a
+//    mesh without hexes) are read every step, so a caller that restores a
+//    saved DeformableState steps from the plastic state it restored;
+//  * the committed rotations are written (the step sets each before reading
+//    it, assembleElastic solver.cc:1404-1547), sized to the tets if needed;
+//  * the report is accumulated like the reference's (solver.cc:3612-3615,
+//    5881-5882), with the per-substep lists appended (solver.cc:4253-4256).
 inline int32_t step(DeviceBody& body, talus::DeformableState& state, const Settings& s, const glm::vec3& gravity,
                     float dt, StepReport& report) {
-  const tl_settings t = settingsOf(s);
+  tl_settings t = settingsOf(s);
+  t.law = body.law;
+  const size_t T = body.tets;
+  body.rotation.assign(9 * T, 0.0f);
+  body.plastic.assign(10 * T, 0.0f);
+  for (size_t e = 0; e < T && e < state.plastic.size(); ++e) {
+    const talus::PlasticPoint& p = state.plastic[e];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) body.plastic[10 * e + 3 * r + c] = p.strain[c][r];
+    body.plastic[10 * e + 9] = p.equivalent;
+  }
   const double g[3] = {gravity.x, gravity.y, gravity.z};
   tl_step_report r{};
   const int32_t rc = tl_step_host(body.system, 0, TL_DTYPE_F32, state.position.data(), state.velocity.data(),
-                                  state.acceleration.data(), nullptr, nullptr, &t, g, dt, &r);
+                                  state.acceleration.data(), body.rotation.data(), body.plastic.data(), &t, g, dt, &r);
+  if (rc != TL_OK && rc != TL_ERR_NONFINITE) return rc;
+  if (state.committed.size() < T) state.committed.resize(T);
+  if (state.plastic.size() < T) state.plastic.resize(T);
+  for (size_t e = 0; e < T; ++e) {
+    for (int row = 0; row < 3; ++row)
+      for (int c = 0; c < 3; ++c) {
+        state.committed[e].rotation[c][row] = body.rotation[9 * e + 3 * row + c];
+        state.plastic[e].strain[c][row] = body.plastic[10 * e + 3 * row + c];
+      }
+    state.plastic[e].equivalent = body.plastic[10 * e + 9];
+  }
+  report.nodes += r.nodes;
+  report.elements += r.elements;
   report.cgIterations += r.cg_iterations;
   report.cgCappedSolves += r.cg_capped_solves;
   report.plasticEvaluations += r.plastic_evaluations;
+  report.plasticSolves += r.plastic_solves;
   report.plasticBacktracks += r.plastic_backtracks;
+  report.plasticCapped += r.plastic_capped;
+  report.plasticLinearReads += r.plastic_linear_reads;
+  report.plasticHandoffs += r.plastic_handoffs;
+  report.plasticFallbacks += r.plastic_fallbacks;
+  report.plasticFallbackRejections += r.plastic_fallback_rejections;
+  report.primaryCgOperatorApplications += r.operator_applications;
+  report.cgWorstRelativeResidual = std::max(report.cgWorstRelativeResidual, float(r.cg_worst_relative_residual));
+  report.plasticWorstResidual = std::max(report.plasticWorstResidual, float(r.plastic_worst_residual));
   report.elasticEnergy += float(r.elastic_energy);
   report.kineticEnergy += float(r.kinetic_energy);
   report.nonFinite = report.nonFinite || r.non_finite != 0;
+  report.plasticGrowth = report.plasticGrowth || r.plastic_growth != 0;
+  // device time of the element pass and the PCG (TL_FLAG_PROFILE) stand in
+  // for the reference's wall-clock stage timers
+  report.elasticSeconds += r.element_seconds;
+  report.primaryCgSeconds += r.pcg_seconds;
+  uint32_t iterations[16], count = 0u;
+  double start[16], end[16];
+  if (tl_step_substeps(body.system, 0, iterations, start, end, 16, &count) == TL_OK) {
+    for (uint32_t k = 0; k < count && k < 16u; ++k) {
+      report.cgPerSubstep.push_back(iterations[k]);
+      report.cgStartResidual.push_back(float(start[k]));
+      report.cgEndResidual.push_back(float(end[k]));
+      report.worstSubstep = std::max(report.worstSubstep, iterations[k]);
+    }
+  }
   return rc;
 }
 

@@ -143,6 +143,8 @@ SIGNATURES = {
     "tl_system_counts": (C.c_int32, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64),
                                      C.POINTER(C.c_uint64)]),
     "tl_system_trace": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)]),
+    "tl_step_substeps": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                     C.POINTER(C.c_uint32)]),
     "tl_system_tune": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32]),
     "tl_system_set_solver": (C.c_int32, [C.c_void_p, C.c_uint32]),
     "tl_system_set_plasticity": (C.c_int32, [C.c_void_p, C.c_uint32]),

@@ -102,7 +102,19 @@ struct CgBodyDev {
 struct CgReportDev {
   uint32_t iterations, capped, applications, solves, tangent_iterations, pad;
   double worst_rel;
+  // the current substep's solves (the reference's primaryResult, solver.cc:3919-3950, 4095-4097, 4245):
+  // iterations summed, the first solve's start residual, the last solve's end residual
+  uint32_t pass_iterations, pass_solves;
+  double pass_start, pass_end;
 };
+
+// One substep's record of the reference's per-substep report lists
+// (StepReport::cgPerSubstep, cgStartResidual, cgEndResidual, solver.h:299-301).
+struct SubstepRecordDev {
+  uint32_t iterations, pad;
+  double start_residual, end_residual;
+};
+constexpr uint32_t SUBSTEP_RECORDS = 16;  // substeps recorded per body and step
 
 // Floating frame of one body (FloatingFrame, solver.cc:2944-2961), FP64.
 // Positions are kept relative to the body's rest centre of mass X0 (fixed at
@@ -1729,6 +1741,10 @@ __global__ void __launch_bounds__(TILE, 2)
       rep.solves += 1u;
       rep.tangent_iterations += tangent ? c.taken : 0u;
       rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
+      if (rep.pass_solves == 0u) rep.pass_start = c.start_res;
+      rep.pass_end = c.rel_res;
+      rep.pass_iterations += c.taken;
+      rep.pass_solves += 1u;
       s.cgrep[b] = rep;
     }
   }
@@ -2207,6 +2223,10 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2) kPcg1(Sys<S> s, 
     rep.solves += 1u;
     rep.tangent_iterations += TANGENT ? taken : 0u;
     rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
+    if (rep.pass_solves == 0u) rep.pass_start = c.start_res;
+    rep.pass_end = c.rel_res;
+    rep.pass_iterations += c.taken;
+    rep.pass_solves += 1u;
     s.cgrep[0] = rep;
   }
 }
@@ -2510,6 +2530,10 @@ __global__ void __launch_bounds__(TILE, sizeof(S) == 4 ? 3 : 2)
       rep.solves += 1u;
       rep.tangent_iterations += TANGENT ? c.taken : 0u;
       rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
+      if (rep.pass_solves == 0u) rep.pass_start = c.start_res;
+      rep.pass_end = c.rel_res;
+      rep.pass_iterations += c.taken;
+      rep.pass_solves += 1u;
       s.cgrep[b] = rep;
     }
   }
@@ -2524,6 +2548,22 @@ static __global__ void kStepSelect(BodyStepDev* step, const BodyStepDev* variant
   const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= bodies) return;
   step[b] = variants[2 * b + ((mode == 1u && acc[b].inverts) ? 1u : 0u)];
+}
+
+// After substep `pass`: each active body's substep record from its report's
+// pass fields, which are then cleared for the next substep.
+template <class S>
+__global__ void kSubstepRecord(Sys<S> s, SubstepRecordDev* records, uint32_t pass) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= s.bodies || !bodyActive(s, b, pass)) return;
+  CgReportDev rep = s.cgrep[b];
+  if (pass < SUBSTEP_RECORDS)
+    records[size_t(b) * SUBSTEP_RECORDS + pass] = SubstepRecordDev{rep.pass_iterations, 0u, rep.pass_start, rep.pass_end};
+  rep.pass_iterations = 0u;
+  rep.pass_solves = 0u;
+  rep.pass_start = 0.0;
+  rep.pass_end = 0.0;
+  s.cgrep[b] = rep;
 }
 
 // Clears the per-body step accumulators (min J key to its largest value).

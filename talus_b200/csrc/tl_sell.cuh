@@ -382,6 +382,10 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
     rep.solves += 1u;
     rep.tangent_iterations += tangent ? taken : 0u;
     rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
+    if (rep.pass_solves == 0u) rep.pass_start = c.start_res;
+    rep.pass_end = c.rel_res;
+    rep.pass_iterations += c.taken;
+    rep.pass_solves += 1u;
     s.cgrep[0] = rep;
   }
 }
@@ -564,6 +568,10 @@ __global__ void __launch_bounds__(TILE, 4)
       rep.solves += 1u;
       rep.tangent_iterations += tangent ? c.taken : 0u;
       rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
+      if (rep.pass_solves == 0u) rep.pass_start = c.start_res;
+      rep.pass_end = c.rel_res;
+      rep.pass_iterations += c.taken;
+      rep.pass_solves += 1u;
       s.cgrep[b] = rep;
     }
   }

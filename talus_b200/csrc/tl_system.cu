@@ -249,6 +249,9 @@ struct SystemBase {
   virtual void setFlowLimits(uint32_t body, uint32_t lane, double crushStress, double crushLimit,
                              double plasticMax) = 0;
   std::vector<uint32_t> trace;  // TL_FLAG_TRACE: iterations of each PCG launch (body 0)
+  // the last step's per-substep records of every body ([bodies][SUBSTEP_RECORDS]) and substep counts
+  std::vector<SubstepRecordDev> substepRecords;
+  std::vector<uint32_t> substepCounts;
   uint32_t bodies = 0;
   uint64_t nodes = 0, tets = 0;
 };
@@ -339,6 +342,17 @@ struct System final : SystemBase {
   DevBuf<CgBodyDev> cg;
   DevBuf<CgReportDev> cgrep;
   DevBuf<GridSyncDev> sync;
+  DevBuf<SubstepRecordDev> subrec;   // [B][SUBSTEP_RECORDS] per-substep solve records of the current step
+  PinnedBuf<SubstepRecordDev> hSubrec;
+  void recordSubstep(uint32_t pass) {
+    kSubstepRecord<S><<<(B + 255) / 256, 256, 0, st>>>(view(), subrec.ptr, pass);
+    check();
+  }
+  // Keeps the downloaded records (hSubrec) and each body's substep count.
+  void keepSubsteps(const uint32_t* substeps) {
+    substepRecords.assign(hSubrec.ptr, hSubrec.ptr + size_t(B) * SUBSTEP_RECORDS);
+    substepCounts.assign(substeps, substeps + B);
+  }
   bool hasEyoung = false;
   bool hasDamping = false;   // some element's lane has stiffness damping
   bool hencky = false;       // TL_PLASTICITY_HENCKY: finite-strain flow from a per-tet plastic rest
@@ -745,6 +759,8 @@ struct System final : SystemBase {
     cgrep.alloc(B);
     sync.alloc(1);
     sync.zero(st);
+    subrec.alloc(size_t(B) * SUBSTEP_RECORDS);
+    subrec.zero(st);
     buildTiles(hTet, hElemTileBody);
     buildSell(hTet, hStart, hEntry);
     TL_CUDA(cudaStreamSynchronize(st));
@@ -1397,6 +1413,7 @@ struct System final : SystemBase {
       if (anyFloating) frameEnd(pass);
       nodeOp(kUpdate<S>, pass);
       if (anyFloating) frameTurn(pass);
+      recordSubstep(pass);
       if (anyYields) element(law, u.ptr, nullptr, pass, EM_MAPPING | EM_COMMIT, 0.0);
     }
     if (hencky) {  // flowLattice once per step, after the solve (strainstep.cc:822-825)
@@ -1417,7 +1434,13 @@ struct System final : SystemBase {
     sync.download(hsy, 1, st);
     uint32_t* hy = hCount.get(B);
     yielding.download(hy, B, st);
+    subrec.download(hSubrec.get(size_t(B) * SUBSTEP_RECORDS), size_t(B) * SUBSTEP_RECORDS, st);
     TL_CUDA(cudaStreamSynchronize(st));
+    {
+      std::vector<uint32_t> counts(B);
+      for (uint32_t b = 0; b < B; ++b) counts[b] = hs[b].substeps;
+      keepSubsteps(counts.data());
+    }
     float ms = 0.f;
     TL_CUDA(cudaEventElapsedTime(&ms, e0, e1));
     double classSeconds[3] = {0.0, 0.0, 0.0};
@@ -1499,6 +1522,7 @@ struct System final : SystemBase {
       if (anyFloating) frameEnd(pass);
       nodeOp(kUpdate<S>, pass);
       if (anyFloating) frameTurn(pass);
+      recordSubstep(pass);
       if (yieldsLaw) element(law, u.ptr, nullptr, pass, EM_MAPPING | EM_COMMIT, 0.0);
     }
     kStepEnd<S><<<nodeTiles, TILE, 0, st>>>(view());
@@ -1509,6 +1533,7 @@ struct System final : SystemBase {
     sync.download(hSync.ptr, 1, st);
     yielding.download(hCount.ptr, B, st);
     dStep.download(hStepOut.ptr, B, st);
+    subrec.download(hSubrec.ptr, size_t(B) * SUBSTEP_RECORDS, st);
   }
 
   int32_t stepGraph(const tl_settings& set, const double gvec[3], double dt, tl_step_report* reports, int law,
@@ -1523,6 +1548,7 @@ struct System final : SystemBase {
     hSync.get(1);
     hCount.get(B);
     hStepOut.get(B);
+    hSubrec.get(size_t(B) * SUBSTEP_RECORDS);
     for (uint32_t b = 0; b < B; ++b)
       for (uint32_t k = 0; k < 2; ++k) {
         BodyStepDev& s = hv[2 * b + k];
@@ -1601,6 +1627,11 @@ struct System final : SystemBase {
         classSeconds[u.first] += double(t) * 1e-3;
       }
     if (hSync.ptr->error != 0) throw StatusError{TL_ERR_TIMEOUT, "a PCG grid barrier ran out of time"};
+    {
+      std::vector<uint32_t> counts(B);
+      for (uint32_t b = 0; b < B; ++b) counts[b] = hStepOut.ptr[b].substeps;
+      keepSubsteps(counts.data());
+    }
     int32_t status = TL_OK;
     for (uint32_t b = 0; b < B; ++b) {
       if (hAcc.ptr[b].nonfinite) status = TL_ERR_NONFINITE;
@@ -2234,6 +2265,22 @@ int32_t tl_system_set_flow_limits(tl_system* system, uint32_t body, uint32_t lan
     system->impl->setFlowLimits(body, lane, crush_stress, crush_limit, plastic_max);
     return TL_OK;
   });
+}
+
+int32_t tl_step_substeps(const tl_system* system, uint32_t body, uint32_t* iterations, double* start_residual,
+                         double* end_residual, uint32_t capacity, uint32_t* count) {
+  if (!system || body >= system->impl->bodies) return TL_ERR_ARG;
+  const SystemBase& s = *system->impl;
+  const uint32_t taken = s.substepCounts.empty() ? 0u : s.substepCounts[body];
+  const uint32_t kept = std::min({capacity, taken, SUBSTEP_RECORDS});
+  for (uint32_t k = 0; k < kept; ++k) {
+    const SubstepRecordDev& r = s.substepRecords[size_t(body) * SUBSTEP_RECORDS + k];
+    if (iterations) iterations[k] = r.iterations;
+    if (start_residual) start_residual[k] = r.start_residual;
+    if (end_residual) end_residual[k] = r.end_residual;
+  }
+  if (count) *count = taken;
+  return TL_OK;
 }
 
 int32_t tl_system_trace(const tl_system* system, uint32_t* iterations, uint32_t capacity, uint32_t* count) {

@@ -287,6 +287,20 @@ class System:
               self.context.handle)
         return out[:count.value].tolist()
 
+    def substeps(self, body: int = 0):
+        """The last step's per-substep solve records of one body
+        (tl_step_substeps): PCG iterations, starting and final relative
+        residuals, like StepReport::cgPerSubstep / cgStartResidual /
+        cgEndResidual (solver.h:299-301)."""
+        count = C.c_uint32()
+        it = np.zeros(16, np.uint32)
+        start = np.zeros(16)
+        end = np.zeros(16)
+        check(capi.lib().tl_step_substeps(self.handle, body, it.ctypes.data, start.ctypes.data, end.ctypes.data, 16,
+                                          C.byref(count)), self.context.handle)
+        k = min(16, count.value)
+        return it[:k].tolist(), start[:k].tolist(), end[:k].tolist()
+
     def step(self, settings: Settings, gravity=(0.0, -9.81, 0.0), delta_time: float = 1.0 / 60.0, reports=None):
         """One deformable::step of every body; returns the per-body reports
         (accumulated into ``reports`` when given).  A non-finite state is

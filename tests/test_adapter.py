@@ -4,11 +4,13 @@ types, compiled and linked on the CPU.
 The adapter includes the reference's talus/deformable/solver/solver.h,
 which needs GLM and cannot be built here.  A stand-in header gives the
 fields the adapter touches, with the reference's names and layouts
-(mesh.h:11-62, material.h:12-29, solver.h:51-311; glm matrices
+(mesh.h:11-62, material.h:7-29, solver.h:51-311; glm matrices
 column-major).  The test program uploads one tet through the adapter and,
 without a device, gets TL_ERR_NO_DEVICE back from tl_ctx_create: the
 adapter compiles against those types, links against libtalus_fem.so and
-reaches the C ABI.
+reaches the C ABI.  A body whose lanes mix the two elastic models is refused
+before any device work.  tests/test_gpu_adapter.py steps blocks through the
+same adapter on the GPU against the oracle.
 """
 import os
 import shutil
@@ -44,6 +46,7 @@ struct mat3 {  // column-major: m[column][row]
 }  // namespace glm
 namespace talus {
 constexpr float kInf = std::numeric_limits<float>::infinity();
+enum class ElasticModel : uint32_t { Corotated, NeoHookean };
 struct PreparedTet { glm::uvec4 nodes; glm::mat3 restInverse; float volume = 0.0f; uint32_t material = 0u; };
 struct PreparedMesh {
   std::vector<glm::vec3> restPositions;
@@ -51,13 +54,20 @@ struct PreparedMesh {
   std::vector<uint8_t> anchored;
   std::vector<PreparedTet> tets;
 };
+struct PlasticPoint { glm::mat3 strain; float equivalent = 0.0f; };
+struct CommittedTet { glm::mat3 rotation; };
 struct PhysicalMaterial {
   float friction = 0.5f, restitution = 0.0f, density = 1000.0f, strength = kInf, youngsModulus = 0.0f,
         poissonsRatio = 0.3f, stiffnessDamping = 0.0f, yieldStress = kInf, hardeningModulus = 0.0f;
+  ElasticModel elasticModel = ElasticModel::Corotated;
   float hysteresis = 0.0f, dampingRatio = kInf, tearStrain = kInf, plasticMax = kInf, crushStress = kInf,
         crushLimit = 1.0f;
 };
-struct DeformableState { std::vector<glm::vec3> position, velocity, acceleration; };
+struct DeformableState {
+  std::vector<glm::vec3> position, velocity, acceleration;
+  std::vector<CommittedTet> committed;
+  std::vector<PlasticPoint> plastic;
+};
 namespace deformable {
 enum class RigidSplit { Off, Unprojected, Projected };
 struct Settings {
@@ -66,9 +76,17 @@ struct Settings {
   RigidSplit rigidSplit = RigidSplit::Projected;
 };
 struct StepReport {
-  uint32_t cgIterations = 0u, cgCappedSolves = 0u, plasticEvaluations = 0u, plasticBacktracks = 0u;
+  uint32_t nodes = 0u, elements = 0u, cgIterations = 0u, cgCappedSolves = 0u, plasticEvaluations = 0u,
+           plasticSolves = 0u, plasticBacktracks = 0u, plasticCapped = 0u, plasticLinearReads = 0u,
+           plasticHandoffs = 0u, plasticFallbacks = 0u, plasticFallbackRejections = 0u,
+           primaryCgOperatorApplications = 0u;
+  float cgWorstRelativeResidual = 0.0f, plasticWorstResidual = 0.0f;
+  double elasticSeconds = 0.0, primaryCgSeconds = 0.0;
   float elasticEnergy = 0.0f, kineticEnergy = 0.0f;
-  bool nonFinite = false;
+  bool nonFinite = false, plasticGrowth = false;
+  uint32_t worstSubstep = 0u;
+  std::vector<uint32_t> cgPerSubstep;
+  std::vector<float> cgStartResidual, cgEndResidual;
 };
 }  // namespace deformable
 }  // namespace talus
@@ -91,6 +109,16 @@ int main() {
   talus::PhysicalMaterial lanes[1];
   lanes[0].youngsModulus = 1.0e6f;
   lanes[0].plasticMax = 0.5f;
+  {  // lanes mixing the elastic models: refused before any device work
+    talus::PhysicalMaterial mixed[2];
+    mixed[1].elasticModel = talus::ElasticModel::NeoHookean;
+    talus::PreparedMesh two = mesh;
+    two.tets.push_back(tet);
+    two.tets[1].material = 1u;
+    d::b200::DeviceBody refused;
+    if (d::b200::upload(two, std::span<const talus::PhysicalMaterial>(mixed, 2), refused) != TL_ERR_UNSUPPORTED)
+      return 4;
+  }
   d::b200::DeviceBody body;
   const int32_t rc = d::b200::upload(mesh, std::span<const talus::PhysicalMaterial>(lanes, 1), body);
   if (rc == TL_OK) {  // with a device: one step through the adapter
