@@ -235,7 +235,24 @@ template <class S> struct Sys {
   double* fpart;               // [node_tiles][FRAME_PART] frame moment partials
   Vec4<S>* relv;               // frame velocity of each node, then its world arm at the substep end
   Vec4<S>* drive;              // external and fictitious force of each node (replaces m g)
+  // per-body gate of a batched plastic Newton round (null: every body takes part): a launch
+  // acts on body b only when gate[b] & gate_bit; the low bits carry the body's element-pass mode
+  const uint32_t* gate;
+  uint32_t gate_bit;
 };
+
+// Gate bits (above the ElementMode bits) of the batched Newton rounds.
+constexpr uint32_t GATE_ASSEMBLE = 1u << 8;
+constexpr uint32_t GATE_ZERO_TOTAL = 1u << 9;
+constexpr uint32_t GATE_TOTAL_FROM_LOWEST = 1u << 10;
+constexpr uint32_t GATE_BACKTRACK = 1u << 11;
+constexpr uint32_t GATE_LOWEST_FROM_TOTAL = 1u << 12;
+constexpr uint32_t GATE_INCR_FROM_A = 1u << 13;
+constexpr uint32_t GATE_ACCEPT = 1u << 14;
+constexpr uint32_t GATE_ADD = 1u << 15;
+constexpr uint32_t GATE_A_FROM_TOTAL = 1u << 16;
+constexpr uint32_t GATE_ELASTIC = 1u << 17;   // bodies on the three-read elastic path in a Newton batch
+constexpr uint32_t GATE_SOLVE0 = 1u << 20;    // + group (x0zero + 2 tangent): the four PCG launch groups
 
 constexpr int TILE_OFF_STRIDE = 4 * TILE + 4;  // 4 TILE + 1 offsets, padded to 8-byte rows
 
@@ -346,7 +363,7 @@ __device__ __forceinline__ Sym<T> tangentStress(const Sym<T>& e, T bulk, T mu, T
 }
 
 template <class S> __device__ __forceinline__ bool bodyActive(const Sys<S>& s, uint32_t b, uint32_t pass) {
-  return pass < s.step[b].substeps;
+  return pass < s.step[b].substeps && (!s.gate || (s.gate[b] & s.gate_bit) != 0u);
 }
 
 __device__ __forceinline__ unsigned long long globalTimer() {
@@ -557,6 +574,8 @@ __global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
   static_assert(!HK || LAW == 0, "the plastic rest shape is written for the corotated law");
   const uint32_t tile = blockIdx.x, b = s.elem_tile_body[tile];
   if (!bodyActive(s, b, pass)) return;
+  if (s.gate)  // a batched Newton round: the body's own mapping and tangent choice
+    mode = (mode & ~uint32_t(EM_CONSISTENT | EM_MAPPING)) | (s.gate[b] & uint32_t(EM_CONSISTENT | EM_MAPPING));
   const uint32_t e = tile * TILE + threadIdx.x;
   const bool valid = e < s.body[b].elem_end;
   double energy = 0.0;
@@ -2598,6 +2617,23 @@ __global__ void kPcgPrepare(Sys<S> s, uint32_t pass) {
     s.sync->arrive = 0u;
     s.sync->active = count;
   }
+}
+
+// dst = src on the nodes of the gated bodies (or zero when src is null).
+template <class S>
+__global__ void __launch_bounds__(TILE) kNodeCopy(Sys<S> s, Vec4<S>* dst, const Vec4<S>* src, uint32_t pass) {
+  const uint32_t tile = blockIdx.x, b = s.node_tile_body[tile];
+  if (!bodyActive(s, b, pass)) return;
+  const uint32_t n = tile * TILE + threadIdx.x;
+  dst[n] = src ? src[n] : Vec4<S>{0, 0, 0, 0};
+}
+
+// Clears the per-body Newton acceptance maxima before kNewtonAccept.
+static __global__ void kAccMovedReset(BodyAccDev* acc, uint32_t bodies) {
+  const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= bodies) return;
+  acc[b].moved_key = 0ull;
+  acc[b].extent_key = 0ull;
 }
 
 // a += incr on free nodes (solver.cc:3941-3945).

@@ -342,6 +342,10 @@ struct System final : SystemBase {
   DevBuf<CgBodyDev> cg;
   DevBuf<CgReportDev> cgrep;
   DevBuf<GridSyncDev> sync;
+  // batched plastic Newton: per-body gate words and the bit the next launches test (0: no gate)
+  DevBuf<uint32_t> gate;
+  PinnedBuf<uint32_t> hGate;
+  uint32_t gateBit = 0;
   DevBuf<SubstepRecordDev> subrec;   // [B][SUBSTEP_RECORDS] per-substep solve records of the current step
   PinnedBuf<SubstepRecordDev> hSubrec;
   void recordSubstep(uint32_t pass) {
@@ -536,6 +540,8 @@ struct System final : SystemBase {
     s.fpart = fpart.ptr;
     s.relv = relv.ptr;
     s.drive = drive.ptr;
+    s.gate = gateBit ? gate.ptr : nullptr;
+    s.gate_bit = gateBit;
     return s;
   }
 
@@ -1384,6 +1390,7 @@ struct System final : SystemBase {
     TL_CUDA(cudaStreamSynchronize(st));
     uint32_t maxSub = 1;
     bool anyNewton = false;
+    std::vector<uint8_t> newtonBody(B, 0u);
     for (uint32_t b = 0; b < B; ++b) {
       BodyStepDev& s = hs[b];
       s.substeps = ha[b].inverts ? std::max(configured, INVERTED_SUBSTEPS) : configured;
@@ -1394,10 +1401,9 @@ struct System final : SystemBase {
       s.scale = s.hstep * s.hstep;
       maxSub = std::max(maxSub, s.substeps);
       const bool yieldsHere = hb[b].anyYields && law == TL_LAW_COROTATED && !hencky;
-      anyNewton = anyNewton || (set.plastic_passes > 1u && yieldsHere);
+      newtonBody[b] = (set.plastic_passes > 1u && yieldsHere) ? 1u : 0u;
+      anyNewton = anyNewton || newtonBody[b];
     }
-    if (anyNewton && B != 1u)
-      throw StatusError{TL_ERR_UNSUPPORTED, "the plastic Newton path runs one body per system"};
     dStep.upload(hs, B, st);
     const bool anyYields = std::any_of(hb.begin(), hb.end(), [](const HostBody& h) { return h.anyYields; }) &&
                            law == TL_LAW_COROTATED && !hencky;
@@ -1407,8 +1413,10 @@ struct System final : SystemBase {
       nodeOp(kPredict<S>, pass);
       if (!anyNewton) {
         elasticReads(law, pass);
-      } else {
+      } else if (B == 1u) {
         newton(law, pass, set, rule, hs[0], local[0]);
+      } else {  // a batch: every yielding body's Newton loop at once, the others' elastic reads
+        newtonBatch(law, pass, set, rule, hs, local, newtonBody);
       }
       if (anyFloating) frameEnd(pass);
       nodeOp(kUpdate<S>, pass);
@@ -1473,7 +1481,7 @@ struct System final : SystemBase {
       r.plastic_fallbacks += l.plastic_fallbacks;
       r.plastic_fallback_rejections += l.plastic_fallback_rejections;
       r.plastic_worst_residual = std::max(r.plastic_worst_residual, l.plastic_worst_residual);
-      r.yielding = hy[b];
+      r.yielding = (B > 1u && newtonBody[b]) ? l.yielding : hy[b];
       r.plastic_growth |= hacc[b].grew;
       r.non_finite |= hacc[b].nonfinite;
       r.elastic_energy += hacc[b].energy;
@@ -1868,6 +1876,402 @@ struct System final : SystemBase {
     }
   }
   DevBuf<Vec4<S>>& lowest_() { return lowest; }
+
+  // ------------------------------------------- batched plastic Newton ----
+  // The plastic Newton loop of solver.cc:3951-4250 for every yielding body of
+  // a batch at once.  Each body runs the single-body control flow of newton()
+  // above as a state machine on the host; the device work is issued in
+  // rounds, each round one element pass and node assembly for the bodies
+  // that want one (gate GATE_ASSEMBLE) and one PCG solve for the bodies that
+  // want one (gates GATE_SOLVE0 + group), with per-body masked copies in
+  // between.  Every body therefore makes exactly the device calls it makes
+  // alone, in the same order; only bodies' calls are grouped.  Each round
+  // reads the per-body results back once after the assembly and once after
+  // the solves.
+  struct NewtonBody {
+    enum Stage : uint8_t {
+      START, ATTEMPT, ATTEMPT_GOT, ATTEMPT_SOLVED, LINEAR, LINEAR_GOT, LINEAR_SOLVED, AFTER, FALLBACK, FALLBACK_GOT,
+      FALLBACK_SOLVED, FALLBACK_CHECK_GOT, DECIDE, REJECT_GOT, FINISH, DONE
+    };
+    enum Need : uint8_t { NOTHING, ASSEMBLE, SOLVE };
+    Stage stage = DONE;
+    Need need = NOTHING;
+    // device requests of the coming round
+    bool mapping = true, consistent = false, x0zero = false, accept = false;
+    uint32_t ops = 0;  // GATE_* copies and updates
+    // newton()'s locals
+    bool linearAllowed = true, converged = false, predictorUnloaded = false, handedOff = false, fellBack = true;
+    double accepted = 0, opening = 0, lowest = 0;
+    uint32_t loadingBefore = 0, solves = 0, attempt = 0, read = 0;
+    tl_step_report rep{};
+  };
+
+  // Runs body `nb`'s control flow from its stage until it needs the device:
+  // an assembly (need ASSEMBLE), a solve (need SOLVE) or nothing (DONE).
+  // `squared`/`loadingNow` are the results of the assembly just made,
+  // `moved`/`extent` those of the acceptance after the solve just made.
+  void newtonAdvance(NewtonBody& nb, uint32_t cap, double travel, double squared, uint32_t loadingNow, double moved,
+                     double extent) {
+    using NB = NewtonBody;
+    nb.need = NB::NOTHING;
+    for (;;) {
+      switch (nb.stage) {
+        case NB::START:
+          nb.ops |= GATE_ZERO_TOTAL;
+          nb.accepted = std::numeric_limits<double>::infinity();
+          nb.opening = 0.0;
+          nb.lowest = std::numeric_limits<double>::infinity();
+          nb.loadingBefore = 0;
+          nb.solves = 0;
+          nb.converged = nb.predictorUnloaded = nb.handedOff = false;
+          nb.attempt = 0;
+          nb.stage = NB::ATTEMPT;
+          break;
+        case NB::ATTEMPT:
+          if (nb.attempt == cap) {
+            nb.stage = NB::AFTER;
+            break;
+          }
+          if (nb.attempt < 2u) nb.consistent = nb.attempt != 0u;
+          nb.need = NB::ASSEMBLE;
+          nb.mapping = true;
+          nb.stage = NB::ATTEMPT_GOT;
+          return;
+        case NB::ATTEMPT_GOT: {
+          ++nb.rep.plastic_evaluations;
+          if (nb.attempt != 0u) {
+            const double ranked = std::isfinite(squared) ? squared : std::numeric_limits<double>::infinity();
+            if (nb.attempt == 1u || ranked < nb.lowest) {
+              nb.lowest = ranked;
+              nb.ops |= GATE_LOWEST_FROM_TOTAL;
+            }
+          }
+          if (nb.attempt == 0u) nb.predictorUnloaded = loadingNow == 0u;
+          if (nb.attempt == 1u && nb.linearAllowed && nb.predictorUnloaded && std::isfinite(squared) &&
+              squared > nb.accepted) {
+            ++nb.rep.plastic_linear_reads;
+            nb.consistent = false;
+            nb.read = 1;
+            nb.stage = NB::LINEAR;
+            break;
+          }
+          if (nb.attempt != 0u && !(squared <= nb.accepted)) {
+            nb.ops |= GATE_BACKTRACK;
+            ++nb.rep.plastic_backtracks;
+            ++nb.attempt;
+            nb.stage = NB::ATTEMPT;
+            break;
+          }
+          if (nb.attempt != 0u && nb.loadingBefore == 0u && loadingNow == 0u) {
+            nb.converged = true;
+            nb.stage = NB::AFTER;
+            break;
+          }
+          nb.opening = nb.attempt == 0u ? squared : nb.opening;
+          nb.accepted = squared;
+          nb.loadingBefore = loadingNow;
+          if (nb.attempt == 0u) nb.ops |= GATE_INCR_FROM_A;
+          nb.need = NB::SOLVE;
+          nb.x0zero = nb.attempt != 0u;
+          nb.accept = true;
+          ++nb.solves;
+          nb.stage = NB::ATTEMPT_SOLVED;
+          return;
+        }
+        case NB::ATTEMPT_SOLVED:
+          if (nb.solves > 1u &&
+              travel * moved <= PLASTIC_RESOLUTION * double(std::numeric_limits<float>::epsilon()) * extent) {
+            nb.converged = true;
+            nb.stage = NB::AFTER;
+            break;
+          }
+          ++nb.attempt;
+          nb.stage = NB::ATTEMPT;
+          break;
+        case NB::LINEAR:
+          if (nb.read == ANCHORED_READS) {
+            nb.converged = !nb.handedOff;
+            nb.stage = NB::AFTER;
+            break;
+          }
+          nb.need = NB::ASSEMBLE;
+          nb.mapping = true;
+          nb.stage = NB::LINEAR_GOT;
+          return;
+        case NB::LINEAR_GOT:
+          ++nb.rep.plastic_evaluations;
+          if (loadingNow != 0u) {
+            nb.handedOff = true;
+            nb.converged = false;
+            nb.stage = NB::AFTER;
+            break;
+          }
+          nb.need = NB::SOLVE;
+          nb.x0zero = true;
+          nb.accept = false;
+          ++nb.solves;
+          nb.stage = NB::LINEAR_SOLVED;
+          return;
+        case NB::LINEAR_SOLVED:
+          ++nb.read;
+          nb.stage = NB::LINEAR;
+          break;
+        case NB::AFTER:
+          nb.rep.plastic_solves += nb.solves;
+          if (nb.handedOff) {
+            ++nb.rep.plastic_handoffs;
+            nb.linearAllowed = false;
+            nb.stage = NB::START;
+            break;
+          }
+          if (!nb.converged) {
+            nb.consistent = false;
+            nb.ops |= GATE_ZERO_TOTAL;
+            nb.fellBack = true;
+            nb.read = 0;
+            nb.stage = NB::FALLBACK;
+            break;
+          }
+          nb.stage = NB::FINISH;
+          break;
+        case NB::FALLBACK:
+          nb.need = NB::ASSEMBLE;
+          if (nb.read == ANCHORED_READS) {
+            nb.mapping = true;
+            nb.stage = NB::FALLBACK_CHECK_GOT;
+          } else {
+            nb.mapping = nb.read != 0u;
+            nb.stage = NB::FALLBACK_GOT;
+          }
+          return;
+        case NB::FALLBACK_GOT:
+          ++nb.rep.plastic_evaluations;
+          if (loadingNow != 0u) {
+            nb.fellBack = false;
+            nb.stage = NB::DECIDE;
+            break;
+          }
+          if (nb.read == 0u) nb.ops |= GATE_INCR_FROM_A;
+          nb.need = NB::SOLVE;
+          nb.x0zero = nb.read != 0u;
+          nb.accept = false;
+          ++nb.rep.plastic_solves;
+          nb.stage = NB::FALLBACK_SOLVED;
+          return;
+        case NB::FALLBACK_SOLVED:
+          ++nb.read;
+          nb.stage = NB::FALLBACK;
+          break;
+        case NB::FALLBACK_CHECK_GOT:
+          ++nb.rep.plastic_evaluations;
+          nb.fellBack = loadingNow == 0u && squared <= PLASTIC_REDUCTION * PLASTIC_REDUCTION * nb.opening;
+          nb.stage = NB::DECIDE;
+          break;
+        case NB::DECIDE:
+          if (nb.fellBack) {
+            ++nb.rep.plastic_fallbacks;
+            nb.converged = true;
+            nb.stage = NB::FINISH;
+            break;
+          }
+          ++nb.rep.plastic_fallback_rejections;
+          nb.consistent = true;
+          nb.ops |= GATE_TOTAL_FROM_LOWEST;
+          nb.need = NB::ASSEMBLE;
+          nb.mapping = true;
+          nb.stage = NB::REJECT_GOT;
+          return;
+        case NB::REJECT_GOT: {
+          ++nb.rep.plastic_evaluations;
+          const double remaining = std::sqrt(nb.lowest);
+          if (remaining >= nb.rep.plastic_worst_residual) nb.rep.plastic_worst_residual = remaining;
+          nb.stage = NB::FINISH;
+          break;
+        }
+        case NB::FINISH:
+          nb.rep.plastic_capped += nb.converged ? 0u : 1u;
+          nb.ops |= GATE_A_FROM_TOTAL;
+          nb.stage = NB::DONE;
+          return;
+        case NB::DONE:
+          return;
+      }
+    }
+  }
+
+  // Launches `k` for the bodies whose pending ops carry `bit` (once per round).
+  void gatedNodeCopy(uint32_t bit, DevBuf<Vec4<S>>& dst, const Vec4<S>* src, uint32_t pass) {
+    gateBit = bit;
+    kNodeCopy<S><<<nodeTiles, TILE, 0, st>>>(view(), dst.ptr, src, pass);
+    gateBit = 0;
+    check();
+  }
+  void uploadGates() {
+    gate.upload(hGate.ptr, B, st);
+  }
+
+  std::vector<NewtonBody> nbs;
+  std::vector<uint32_t> newtonYielding;  // each Newton body's yielding count at its last assembly
+
+  void newtonBatch(int law, uint32_t pass, const tl_settings& set, const Rule& rule, const BodyStepDev* hs,
+                   std::vector<tl_step_report>& local, const std::vector<uint8_t>& newtonBody) {
+    using NB = NewtonBody;
+    if (!gate.ptr) gate.alloc(B);
+    uint32_t* hg = hGate.get(B);
+    nbs.assign(B, NB{});
+    newtonYielding.assign(B, 0u);
+    bool anyElastic = false;
+    for (uint32_t b = 0; b < B; ++b) {
+      if (pass >= hs[b].substeps) continue;
+      if (!newtonBody[b]) {
+        anyElastic = true;
+        continue;
+      }
+      nbs[b].stage = NB::START;
+      newtonAdvance(nbs[b], set.plastic_passes, rule.beta * hs[b].inner * hs[b].inner, 0, 0, 0, 0);
+    }
+    // the batch's elastic bodies take the three reads on their own gate
+    if (anyElastic) {
+      for (uint32_t b = 0; b < B; ++b) hg[b] = (pass < hs[b].substeps && !newtonBody[b]) ? GATE_ELASTIC : 0u;
+      uploadGates();
+      gateBit = GATE_ELASTIC;
+      try {
+        elasticReads(law, pass);
+      } catch (...) {
+        gateBit = 0;
+        throw;
+      }
+      gateBit = 0;
+    }
+    for (;;) {
+      // ---- pre-assembly updates and the assembly
+      uint32_t orAll = 0;
+      bool anyAssemble = false;
+      for (uint32_t b = 0; b < B; ++b) {
+        NB& nb = nbs[b];
+        uint32_t w = nb.ops & (GATE_ZERO_TOTAL | GATE_TOTAL_FROM_LOWEST | GATE_BACKTRACK | GATE_A_FROM_TOTAL);
+        nb.ops &= ~w;
+        if (nb.need == NB::ASSEMBLE) {
+          w |= GATE_ASSEMBLE | (nb.mapping ? uint32_t(EM_MAPPING) : 0u) | (nb.consistent ? uint32_t(EM_CONSISTENT) : 0u);
+          anyAssemble = true;
+        }
+        hg[b] = w;
+        orAll |= w;
+      }
+      if (orAll) uploadGates();
+      if (orAll & GATE_ZERO_TOTAL) gatedNodeCopy(GATE_ZERO_TOTAL, total, nullptr, pass);
+      if (orAll & GATE_TOTAL_FROM_LOWEST) gatedNodeCopy(GATE_TOTAL_FROM_LOWEST, total, lowest.ptr, pass);
+      if (orAll & GATE_BACKTRACK) {
+        gateBit = GATE_BACKTRACK;
+        nodeOp(kBacktrack<S>, pass);
+        gateBit = 0;
+      }
+      if (orAll & GATE_A_FROM_TOTAL) gatedNodeCopy(GATE_A_FROM_TOTAL, a, total.ptr, pass);
+      if (anyAssemble) {
+        gateBit = GATE_ASSEMBLE;
+        try {
+          element(law, weighted.ptr, total.ptr, pass, EM_MAPPING, LOADING_MARGIN);
+          nodeAssemble(total.ptr, pass);
+        } catch (...) {
+          gateBit = 0;
+          throw;
+        }
+        gateBit = 0;
+        finalize(1);
+        BodyAccDev* ha = hAcc.get(B);
+        uint32_t* hc = hCount.get(2 * size_t(B));
+        acc.download(ha, B, st);
+        loading.download(hc, B, st);
+        yielding.download(hc + B, B, st);
+        TL_CUDA(cudaStreamSynchronize(st));
+        for (uint32_t b = 0; b < B; ++b) {
+          NB& nb = nbs[b];
+          if (nb.need != NB::ASSEMBLE) continue;
+          newtonYielding[b] = hc[B + b];
+          newtonAdvance(nb, set.plastic_passes, rule.beta * hs[b].inner * hs[b].inner, ha[b].right_sq, hc[b], 0, 0);
+        }
+      }
+      // ---- copies before the solves, the solves by launch group, the updates after them
+      orAll = 0;
+      bool anySolve = false, anyAccept = false;
+      uint32_t groups = 0;
+      for (uint32_t b = 0; b < B; ++b) {
+        NB& nb = nbs[b];
+        uint32_t w = nb.ops & (GATE_LOWEST_FROM_TOTAL | GATE_INCR_FROM_A | GATE_A_FROM_TOTAL);
+        nb.ops &= ~w;
+        if (nb.need == NB::SOLVE) {
+          const uint32_t g = (nb.x0zero ? 1u : 0u) + (nb.consistent ? 2u : 0u);
+          w |= (GATE_SOLVE0 << g) | (nb.accept ? GATE_ACCEPT : GATE_ADD);
+          groups |= 1u << g;
+          anySolve = true;
+          anyAccept = anyAccept || nb.accept;
+        }
+        hg[b] = w;
+        orAll |= w;
+      }
+      if (orAll) uploadGates();
+      if (orAll & GATE_LOWEST_FROM_TOTAL) gatedNodeCopy(GATE_LOWEST_FROM_TOTAL, lowest, total.ptr, pass);
+      if (orAll & GATE_INCR_FROM_A) gatedNodeCopy(GATE_INCR_FROM_A, incr, a.ptr, pass);
+      if (orAll & GATE_A_FROM_TOTAL) gatedNodeCopy(GATE_A_FROM_TOTAL, a, total.ptr, pass);
+      if (anySolve) {
+        for (uint32_t g = 0; g < 4u; ++g) {
+          if (!(groups & (1u << g))) continue;
+          gateBit = GATE_SOLVE0 << g;
+          try {
+            pcg(law, incr.ptr, pass, (g & 1u) != 0u, (g & 2u) != 0u);
+          } catch (...) {
+            gateBit = 0;
+            throw;
+          }
+          gateBit = 0;
+        }
+        if (anyAccept) {
+          kAccMovedReset<<<(B + 255) / 256, 256, 0, st>>>(acc.ptr, B);
+          check();
+          gateBit = GATE_ACCEPT;
+          nodeOp(kNewtonAccept<S>, pass);
+          gateBit = 0;
+        }
+        if (orAll & GATE_ADD) {
+          gateBit = GATE_ADD;
+          kAddIncrement<S><<<nodeTiles, TILE, 0, st>>>(view(), total.ptr, pass);
+          gateBit = 0;
+          check();
+        }
+        BodyAccDev* ha = hAcc.get(B);
+        acc.download(ha, B, st);
+        TL_CUDA(cudaStreamSynchronize(st));
+        for (uint32_t b = 0; b < B; ++b) {
+          NB& nb = nbs[b];
+          if (nb.need != NB::SOLVE) continue;
+          double moved = 0.0, extent = 0.0;
+          if (nb.accept) {
+            std::memcpy(&moved, &ha[b].moved_key, 8);
+            std::memcpy(&extent, &ha[b].extent_key, 8);
+          }
+          newtonAdvance(nb, set.plastic_passes, rule.beta * hs[b].inner * hs[b].inner, 0, 0, moved, extent);
+        }
+      }
+      bool pending = false;
+      for (const NB& nb : nbs) pending = pending || nb.need != NB::NOTHING || nb.ops != 0u;
+      if (!pending) break;
+    }
+    for (uint32_t b = 0; b < B; ++b) {
+      if (!newtonBody[b] || pass >= hs[b].substeps) continue;
+      const tl_step_report& r = nbs[b].rep;
+      tl_step_report& l = local[b];
+      l.plastic_evaluations += r.plastic_evaluations;
+      l.plastic_solves += r.plastic_solves;
+      l.plastic_backtracks += r.plastic_backtracks;
+      l.plastic_capped += r.plastic_capped;
+      l.plastic_linear_reads += r.plastic_linear_reads;
+      l.plastic_handoffs += r.plastic_handoffs;
+      l.plastic_fallbacks += r.plastic_fallbacks;
+      l.plastic_fallback_rejections += r.plastic_fallback_rejections;
+      l.plastic_worst_residual = std::max(l.plastic_worst_residual, r.plastic_worst_residual);
+      l.yielding = newtonYielding[b];
+    }
+  }
 
   // Per-element E override (tl_system_set_youngs).  The first call gives
   // every element its lane's modulus, then overwrites the body's elements.
