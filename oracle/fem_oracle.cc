@@ -1007,13 +1007,13 @@ inline M3<double> skew(const V3<double>& a) {
   return M3<double>(V3<double>(0.0, a.z, -a.y), V3<double>(-a.z, 0.0, a.x), V3<double>(a.y, -a.x, 0.0));
 }
 
-// solver.cc:2983-2988 rigidRate: torque-free rigid body, inertia fixed in the world
+// solver.cc:2983-2987 rigidRate: torque-free rigid body, inertia fixed in the world
 inline RigidMotion rigidRate(const M3<double>& inverseInertia, const RigidMotion& at) {
   const V3<double> spin = inverseInertia * at.momentum;
   return RigidMotion{cross(at.momentum, spin), at.turn * skew(spin)};
 }
 
-// solver.cc:2990-3030 rigidAdvance: `count` classic Runge-Kutta steps over
+// solver.cc:2989-3026 rigidAdvance: `count` classic Runge-Kutta steps over
 // `span`, then three polar passes that pull the turn back to a rotation
 inline RigidMotion rigidAdvance(const M3<double>& inverseInertia, RigidMotion motion, double span, uint32_t count) {
   const double part = span / double(count);
@@ -1043,7 +1043,7 @@ template <class R> V3<R> narrow(const V3<double>& v) { return V3<R>(R(v.x), R(v.
 template <class R> V3<double> widen(const V3<R>& v) { return V3<double>(double(v.x), double(v.y), double(v.z)); }
 template <class R> M3<R> narrow(const M3<double>& m) { return M3<R>(narrow<R>(m[0]), narrow<R>(m[1]), narrow<R>(m[2])); }
 
-// solver.cc:3038-3142 floatingFrame
+// solver.cc:3031-3142 floatingFrame
 template <class R>
 FloatingFrame<R> floatingFrame(const std::vector<R>& nodeMass, const std::vector<V3<R>>& position,
                                const std::vector<V3<R>>& velocity, const std::vector<V3<R>>& acceleration,

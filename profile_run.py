@@ -2,7 +2,7 @@
 launch, its iteration count, so that an ncu capture of one launch of
 tl::kPcg can be turned into DRAM bytes per PCG iteration.
 
-    python -m talus_b200.profile_run --workload plastic-block --steps 4 --precision mixed
+    python profile_run.py --workload plastic-block --steps 4 --precision mixed
 
 prints one JSON line {"pcg_iterations": [...], ...}; PCG launch i of the
 program (0-based, in launch order) made pcg_iterations[i] iterations.  The
@@ -15,7 +15,7 @@ import json
 import os
 import sys
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ROOT = os.path.dirname(os.path.abspath(__file__))
 
 
 def main():

@@ -3,7 +3,7 @@
 // A body with no anchored node, stepped with the rigid split on (floats,
 // solver.cc:2964-2971), is solved in a frame that moves with its centre of
 // mass and turns with its rigid spin:
-//   * floatingFrame (solver.cc:3038-3142): centre, mean velocity and
+//   * floatingFrame (solver.cc:3031-3142): centre, mean velocity and
 //     acceleration, inertia, angular momentum and torque about the centre;
 //     the centre's generalized-alpha step; the torque-free spin advanced by
 //     classic Runge-Kutta (rigidAdvance, solver.cc:2983-3036) to the weighted
@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(TILE) kFrameMoments(Sys<S> s, uint32_t pass, u
     for (int k = 0; k < FRAME_PART; ++k) s.fpart[size_t(tile) * FRAME_PART + k] = v[k];
 }
 
-// rigidRate (solver.cc:2981-2986): d(momentum) = m x w, d(turn) = turn skew(w),
+// rigidRate (solver.cc:2983-2987): d(momentum) = m x w, d(turn) = turn skew(w),
 // w = I^-1 m with the world inertia I fixed over the substep.
 struct RigidMotionDev {
   V3<double> momentum;
@@ -135,7 +135,7 @@ __device__ inline RigidMotionDev movedBy(const RigidMotionDev& from, const Rigid
     for (int j = 0; j < 3; ++j) r.turn.m[i][j] = from.turn.m[i][j] + by * rate.turn.m[i][j];
   return r;
 }
-// rigidAdvance (solver.cc:2988-3030): `count` Runge-Kutta steps over `span`,
+// rigidAdvance (solver.cc:2989-3026): `count` Runge-Kutta steps over `span`,
 // then three passes turn <- (turn + turn^-T) / 2.
 __device__ inline RigidMotionDev rigidAdvanceDev(const M3<double>& inv, RigidMotionDev motion, double span,
                                                  uint32_t count) {
@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(TILE) kFrameEnd(Sys<S> s, uint32_t pass) {
 }
 
 // The committed rotations of a floating body's tets turn with the frame
-// (solver.cc:4341-4343): R <- turn R.
+// (solver.cc:4343-4345): R <- turn R.
 template <class S>
 __global__ void __launch_bounds__(TILE) kFrameTurn(Sys<S> s, uint32_t pass) {
   const uint32_t tile = blockIdx.x, b = s.elem_tile_body[tile];

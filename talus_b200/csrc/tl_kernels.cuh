@@ -471,6 +471,18 @@ __device__ __forceinline__ unsigned long long blockMaxKey(unsigned long long k) 
   return k;
 }
 
+// Asynchronous global -> shared copies (cp.async, 4, 8 or 16 bytes; 16-byte
+// copies bypass L1).  Both addresses must be aligned to the copy size.
+template <int N> __device__ __forceinline__ void cpAsync(void* dst, const void* src) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  if constexpr (N == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(N) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // ------------------------------------------------------------- kernels ----
 
 // Predictor (solver.cc:3691-3700): carried = a; shifted = u + h v + (1/2 - beta) h^2 a;
@@ -549,6 +561,19 @@ enum ElementMode : uint32_t {
   EM_CONSISTENT = 2u,  // scratch.stiffness is the consistent tangent (bindStiffness(true))
   EM_MAPPING = 4u,     // returnMapping
   EM_COMMIT = 8u,      // commitPlastic: plastic point only, no forces
+  EM_YIELDING = 16u,   // some lane of the system yields: stage the plastic points
+};
+
+// One element tile's inputs in shared memory, filled by cp.async when the
+// element pass starts: one wave of coalesced copies per tile instead of
+// loads spread through the kernel, and the second read of Dm^-1 and the
+// plastic point (after the rotation) come from here, not from L2.
+template <class S> struct ElementStage {
+  double dm[9][TILE];       // Dm^-1 planes (FP64)
+  double vol[TILE];
+  uint4 tet[TILE];
+  Vec4<S> plast[2][TILE];
+  uint32_t lane[TILE];
 };
 
 // Element pass (assembleElastic, solver.cc:1354-1572; trial material.cc:236-265;
@@ -578,18 +603,44 @@ __global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
     mode = (mode & ~uint32_t(EM_CONSISTENT | EM_MAPPING)) | (s.gate[b] & uint32_t(EM_CONSISTENT | EM_MAPPING));
   const uint32_t e = tile * TILE + threadIdx.x;
   const bool valid = e < s.body[b].elem_end;
+  __shared__ ElementStage<S> stage;
+  const uint32_t me = threadIdx.x;
+  if (valid) {
+    cpAsync<16>(&stage.tet[me], &s.tet[e]);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) cpAsync<8>(&stage.dm[k][me], s.dm + size_t(k) * s.Tp + e);
+    cpAsync<8>(&stage.vol[me], s.vold + e);
+    cpAsync<4>(&stage.lane[me], s.lane + e);
+    if (LAW == 0 && !HK && (mode & EM_YIELDING)) {
+#pragma unroll
+      for (int k = 0; k < 2; ++k)
+#pragma unroll
+        for (int h = 0; h < int(sizeof(Vec4<S>)) / 16; ++h)
+          cpAsync<16>(reinterpret_cast<unsigned char*>(&stage.plast[k][me]) + 16 * h,
+                      reinterpret_cast<const unsigned char*>(&s.plast[size_t(k) * s.Tp + e]) + 16 * h);
+    }
+  }
+  cpAsyncCommit();
+  cpAsyncWaitAll();
+  __syncthreads();
+  const auto stagedGradients = [&](V3<double> g[4]) {
+    g[1] = {stage.dm[0][me], stage.dm[1][me], stage.dm[2][me]};
+    g[2] = {stage.dm[3][me], stage.dm[4][me], stage.dm[5][me]};
+    g[3] = {stage.dm[6][me], stage.dm[7][me], stage.dm[8][me]};
+    g[0] = -(g[1] + g[2] + g[3]);  // material.cc:199-207
+  };
   double energy = 0.0;
   bool isLoading = false, isYielding = false, grew = false, nonfinite = false;
   unsigned long long jkey = ~0ull;
   if (valid) {
     const BodyStepDev& st = s.step[b];
     const double reach = dir ? st.scale : 0.0;
-    const uint4 t = __ldg(&s.tet[e]);
+    const uint4 t = stage.tet[me];
     const uint32_t nodes[4] = {t.x, t.y, t.z, t.w};
     M3<double> H = zero3<double>();  // displacement gradient, F = I + H
     {
       V3<double> g0[4];
-      gradientsOf<S>(s.dm, s.Tp, e, g0);
+      stagedGradients(g0);
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         const uint32_t n = nodes[c];
@@ -598,7 +649,7 @@ __global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
         addOuter(H, uu, g0[c]);
       }
     }
-    double vol = s.vold[e];
+    double vol = stage.vol[me];
     if constexpr (HK) {  // H' = (I + H) P - I
       M3<double> P;
 #pragma unroll
@@ -615,7 +666,7 @@ __global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
       H.m[2][2] -= 1.0;
       vol /= det3(P);
     }
-    const MatDev m = s.mat[s.lane[e]];
+    const MatDev m = s.mat[stage.lane[me]];
     const double youngs = s.eyoung ? s.eyoung[e] : m.youngs;
     const double lam = youngs * m.lam_unit, mu = youngs * m.mu_unit;
     const double change = volumeChange(H);
@@ -653,13 +704,9 @@ __global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
       asm volatile("" ::: "memory");
       V3<double> g[4];
       {
-        const double* dmp = s.dm;
-        double d[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) d[k] = dmp[size_t(k) * s.Tp + e];
-        g[1] = {d[0], d[1], d[2]};
-        g[2] = {d[3], d[4], d[5]};
-        g[3] = {d[6], d[7], d[8]};
+        g[1] = {stage.dm[0][me], stage.dm[1][me], stage.dm[2][me]};
+        g[2] = {stage.dm[3][me], stage.dm[4][me], stage.dm[5][me]};
+        g[3] = {stage.dm[6][me], stage.dm[7][me], stage.dm[8][me]};
         if constexpr (HK) {  // g' = P^T g (P reloaded: not kept live through the rotation)
           double p[9];
 #pragma unroll
@@ -684,7 +731,7 @@ __global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
       Sym<C> normal = {0, 0, 0, 0, 0, 0};
       if (yields) {
         // returnMap (material.cc:594-634)
-        const Vec4<S> p0 = s.plast[e], p1 = s.plast[s.Tp + e];
+        const Vec4<S> p0 = stage.plast[0][me], p1 = stage.plast[1][me];
         const Sym<C> ep = {C(p0.x), C(p0.y), C(p0.z), C(p0.w), C(p1.x), C(p1.y)};
         const C eq = C(p1.z);
         const Sym<C> el = {C(eps.xx - double(p0.x)), C(eps.yy - double(p0.y)), C(eps.zz - double(p0.z)),
@@ -788,7 +835,7 @@ __global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
       }
     } else {
       V3<double> g[4];
-      gradientsOf<S>(s.dm, s.Tp, e, g);
+      stagedGradients(g);
       // SNH: P = mu (H + H^T - tr H I - cof H) + (lambda + mu)(J - 1) cof F
       M3<double> F = H;
       F.m[0][0] += 1.0;
@@ -1416,15 +1463,6 @@ template <class S, int LAW, bool TANGENT> __host__ __device__ constexpr size_t s
   return sizeof(OpRec<S>) * TILE + (LAW == 0 && TANGENT ? sizeof(Vec4<S>) * 2 * TILE : 0) +
          (LAW == 1 ? sizeof(S) * 9 * TILE : 0);
 }
-template <int N> __device__ __forceinline__ void cpAsync(void* dst, const void* src) {
-  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
-  if constexpr (N == 16)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-  else
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(N) : "memory");
-}
-__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cpAsyncWaitAll() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // e: this thread's element (tile * TILE + threadIdx.x, below Tp).
 template <class S, int LAW, bool TANGENT>

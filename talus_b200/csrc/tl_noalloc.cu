@@ -445,6 +445,7 @@ int32_t stepLocked(int32_t device, const tl_mesh_desc& d, int32_t dtype, void* p
           cudaMemsetAsync(l.yielding, 0, sizeof(uint32_t), st) != cudaSuccess)
         return TL_ERR_CUDA;
     }
+    if (anyYields) mode |= EM_YIELDING;
     if (law == TL_LAW_SNH) kElement<S, 1><<<elemTiles, TILE, 0, st>>>(s, base, dir, pass, mode, 0.0);
     else kElement<S, 0><<<elemTiles, TILE, 0, st>>>(s, base, dir, pass, mode, 0.0);
     ++launches;

@@ -1194,6 +1194,7 @@ struct System final : SystemBase {
       yielding.zero(st);
     }
     if (profiling) mark(0, true);
+    if (std::any_of(hb.begin(), hb.end(), [](const HostBody& h) { return h.anyYields; })) mode |= EM_YIELDING;
     const bool damps = hasDamping && law == TL_LAW_COROTATED && !(mode & EM_COMMIT) && !evaluating;
     if (law == TL_LAW_SNH) kElement<S, 1><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass, mode, margin);
     else if (hencky) kElement<S, 0, true><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass, mode, margin);

@@ -2,7 +2,7 @@
 
 A body with no anchored node, stepped with the rigid split on (floats,
 solver.cc:2964-2971), runs in the frame of its centre and rigid spin
-(floatingFrame solver.cc:3038-3142, predictor and drive solver.cc:3657-3690,
+(floatingFrame solver.cc:3031-3142, predictor and drive solver.cc:3657-3690,
 return to the world and momentum projection solver.cc:4265-4340).  Bars: FP64
 within 1e-9 relative displacement of the FP64 oracle with the same PCG
 iteration counts, FP32-mixed within 1e-5.
@@ -64,7 +64,7 @@ def test_spinning_free_body_fp64_matches_the_oracle(law, split):
     for o_it, g_it, _, _ in iters:
         assert o_it == g_it
     assert np.abs(got.velocity - want.velocity).max() <= 1e-9 * np.abs(want.velocity).max()
-    if law == tb.COROTATED:  # committed rotations turn with the frame (solver.cc:4341-4343)
+    if law == tb.COROTATED:  # committed rotations turn with the frame (solver.cc:4343-4345)
         assert np.abs(got.rotation - want.rotation).max() <= 1e-8
 
 

@@ -2,7 +2,7 @@
 
 A body with no anchored node and RigidSplit on (floats, solver.cc:2964-2971)
 is stepped in a frame that moves with its centre of mass and turns with its
-rigid spin (floatingFrame solver.cc:3038-3142, the predictor and drive
+rigid spin (floatingFrame solver.cc:3031-3142, the predictor and drive
 solver.cc:3657-3690, the return to the world and the momentum projection
 solver.cc:4265-4340).  The reference has no test of this path; these tests
 pin the restatement on what the equations must give:
