@@ -633,6 +633,19 @@ def run_ours(args, spec, rank, world, dist):
     context.close()
 
 
+def survey_element_bytes(T, V, s_bytes, yields):
+    """The element pass's algorithmic bytes per evaluation in the hot-path
+    byte model (tet indices 16, Dm^-1, volume and lane, the positions once
+    per node, the element force and the matvec's rotation, and the plastic
+    point read and written when the material yields): FP32-mixed elastic
+    180 + 12 r, plastic 260 + 12 r; FP64 344 + 24 r and 424 + 24 r bytes per
+    tet, r = nodes / tets."""
+    r = V / T
+    if s_bytes == 4:
+        return T * ((260.0 if yields else 180.0) + 12.0 * r)
+    return T * ((424.0 if yields else 344.0) + 24.0 * r)
+
+
 def element_roofline(meshes, mats, per_body, substeps, s_bytes, seconds, peak):
     """Element pass (tl::kElement): algorithmic bytes of every launch in the
     timed steps over the summed CUDA-event time of those launches.  Elastic
@@ -640,18 +653,26 @@ def element_roofline(meshes, mats, per_body, substeps, s_bytes, seconds, peak):
     evaluations plus one commit pass per substep."""
     if seconds <= 0:
         return None
-    total, launches = 0.0, 0.0
+    total, survey, launches = 0.0, 0.0, 0.0
     for b, m in enumerate(meshes):
         yields = any(np.isfinite(x.yield_stress) and x.yield_stress > 0 for x in mats[b])
         evals = per_body[b, 3] if yields else 3 * substeps[b]
         total += evals * element_bytes(m.tets, m.nodes, s_bytes, yields)
+        survey += evals * survey_element_bytes(m.tets, m.nodes, s_bytes, yields)
         if yields:
             total += substeps[b] * element_bytes(m.tets, m.nodes, s_bytes, yields, commit=True)
+            # a commit pass reads the element data and the positions and writes the plastic point
+            survey += substeps[b] * survey_element_bytes(m.tets, m.nodes, s_bytes, yields)
         launches = max(launches, evals + (substeps[b] if yields else 0))
     achieved = total / seconds / 1e9
+    achieved_model = survey / seconds / 1e9
     return {"kernel": "tl::kElement", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "launches": int(launches), "avg_launch_us": seconds * 1e6 / max(1.0, launches),
-            "algorithmic_bytes": total}
+            "algorithmic_bytes": total,
+            "hot_path_model": {"bytes": survey, "achieved": achieved_model, "frac": achieved_model / peak,
+                               "note": "bytes per tet of the hot-path byte model (FP32-mixed 180/260 + 12 r, FP64 "
+                                       "344/424 + 24 r; r = nodes / tets); 'frac' above counts every byte the "
+                                       "implementation moves (its per-corner diagonal records and operator record)"}}
 
 
 def run_fp64(meshes, mats, settings, args, flush, context):

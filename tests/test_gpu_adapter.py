@@ -14,7 +14,8 @@ reference's DeformableState (mesh.h:56-62):
   cgEndResidual, solver.h:299-301) are filled, one entry per substep;
 * restoring a saved DeformableState (plastic points included) and stepping
   again reproduces the steps taken from it bit for bit;
-* PhysicalMaterial::elasticModel = NeoHookean selects the neo-Hookean law.
+* PhysicalMaterial::elasticModel = NeoHookean selects the neo-Hookean law;
+* an Island steps anchored, floating and yielding bodies together.
 """
 import os
 import shutil
@@ -197,3 +198,134 @@ def test_neo_hookean_lanes_select_the_neo_hookean_law(program):
     assert relative_error(positions[-1], snh[-1], mesh.rest_positions) <= 1e-5
     assert relative_error(corotated[-1], snh[-1], mesh.rest_positions) > 1e-5  # the laws do differ here
     assert len(per) == steps and restored == 1
+
+
+ISLAND_PROGRAM = r"""
+#include "talus_fem_adapter.hpp"
+#include <cstdio>
+#include <fstream>
+namespace d = talus::deformable;
+template <class T> void get(std::ifstream& in, T* p, size_t n) { in.read(reinterpret_cast<char*>(p), sizeof(T) * n); }
+template <class T> void put(std::ofstream& out, const T* p, size_t n) {
+  out.write(reinterpret_cast<const char*>(p), sizeof(T) * n);
+}
+int main(int argc, char** argv) {
+  std::ifstream in(argv[1], std::ios::binary);
+  uint32_t count, steps;
+  get(in, &count, 1); get(in, &steps, 1);
+  std::vector<talus::PreparedMesh> meshes(count);
+  std::vector<talus::PhysicalMaterial> lanes(count);
+  std::vector<talus::DeformableState> states(count);
+  for (uint32_t b = 0; b < count; ++b) {
+    uint32_t V, T;
+    float mat[5];
+    get(in, &V, 1); get(in, &T, 1); get(in, mat, 5);
+    talus::PreparedMesh& mesh = meshes[b];
+    mesh.restPositions.resize(V); mesh.nodeMass.resize(V); mesh.anchored.resize(V); mesh.tets.resize(T);
+    for (auto& p : mesh.restPositions) get(in, &p.x, 3);
+    get(in, mesh.nodeMass.data(), V);
+    get(in, mesh.anchored.data(), V);
+    for (auto& t : mesh.tets) {
+      get(in, t.nodes.v, 4);
+      float rinv[9];
+      get(in, rinv, 9);
+      for (int r = 0; r < 3; ++r) for (int c = 0; c < 3; ++c) t.restInverse[c][r] = rinv[3 * r + c];
+      get(in, &t.volume, 1);
+    }
+    lanes[b].density = mat[0]; lanes[b].youngsModulus = mat[1]; lanes[b].poissonsRatio = mat[2];
+    lanes[b].yieldStress = mat[3]; lanes[b].hardeningModulus = mat[4];
+    states[b].position.resize(V); states[b].velocity.resize(V); states[b].acceleration.resize(V);
+    for (auto& p : states[b].position) get(in, &p.x, 3);
+    for (auto& p : states[b].velocity) get(in, &p.x, 3);
+  }
+  std::vector<d::b200::IslandBody> bodies(count);
+  for (uint32_t b = 0; b < count; ++b) bodies[b] = {&meshes[b], std::span<const talus::PhysicalMaterial>(&lanes[b], 1)};
+  d::b200::Island island;
+  int32_t rc = d::b200::upload(std::span<const d::b200::IslandBody>(bodies), island, TL_FP64);
+  if (rc != TL_OK) { std::printf("upload %d\n", rc); return 2; }
+  std::vector<talus::DeformableState*> ptrs(count);
+  for (uint32_t b = 0; b < count; ++b) ptrs[b] = &states[b];
+  std::vector<d::StepReport> reports(count);
+  std::ofstream out(argv[2], std::ios::binary);
+  for (uint32_t k = 0; k < steps; ++k) {
+    rc = d::b200::step(island, std::span<talus::DeformableState* const>(ptrs), d::Settings{},
+                       glm::vec3{0.0f, -9.81f, 0.0f}, 1.0f / 60.0f, std::span<d::StepReport>(reports));
+    if (rc != TL_OK) { std::printf("step %d\n", rc); return 3; }
+  }
+  for (uint32_t b = 0; b < count; ++b) {
+    for (auto& p : states[b].position) put(out, &p.x, 3);
+    for (auto& p : states[b].plastic) put(out, &p.equivalent, 1);
+    const uint32_t n = uint32_t(reports[b].cgPerSubstep.size());
+    put(out, &n, 1);
+    put(out, &reports[b].plasticEvaluations, 1);
+  }
+  return 0;
+}
+"""
+
+
+def test_island_of_anchored_floating_and_yielding_bodies(program):
+    """Every tet body of an island in one batched step through
+    talus::deformable::b200::Island: a yielding cantilever, a spinning free
+    block (floating frame, Projected split) and an elastic block, each
+    within 1e-5 of its own FP64 oracle run."""
+    work, _ = program
+    (work / "island.cc").write_text(ISLAND_PROGRAM)
+    exe = work / "island"
+    libdir = os.path.join(ROOT, "talus_b200")
+    subprocess.run(["g++", "-std=c++20", "-O2", "-Wall", "-Werror", f"-I{work}", f"-I{os.path.join(ROOT, 'include')}",
+                    "-o", str(exe), str(work / "island.cc"), f"-L{libdir}", "-ltalus_fem", f"-Wl,-rpath,{libdir}"],
+                   check=True)
+    cantilever = tb.box_mesh((6, 2, 2), voxel=0.1, jitter=0.01, seed=23, anchor_axis=0)
+    free = tb.box_mesh((3, 3, 4), voxel=0.1, jitter=0.01, seed=24, anchor_axis=3)
+    block = tb.box_mesh((4, 3, 3), voxel=0.1, jitter=0.01, seed=25)
+    meshes = (cantilever, free, block)
+    mats = [tb.PhysicalMaterial(density=1000.0, youngs_modulus=1e6, poissons_ratio=0.3, yield_stress=2e4,
+                                hardening_modulus=1e4),
+            tb.PhysicalMaterial(density=1000.0, youngs_modulus=5e5, poissons_ratio=0.3),
+            tb.PhysicalMaterial(density=1000.0, youngs_modulus=2e6, poissons_ratio=0.35)]
+    starts = []
+    for mesh in meshes:
+        st = tb.rest_state(mesh)
+        if mesh is free:
+            centre = (mesh.node_mass[:, None] * mesh.rest_positions).sum(0) / mesh.node_mass.sum()
+            st.velocity[...] = np.cross([0.5, 2.0, 0.0], mesh.rest_positions - centre) + np.array([0.2, 0.5, 0.0])
+        starts.append(st)
+    steps = 6
+    blob = struct.pack("<2I", 3, steps)
+    for mesh, mat, st in zip(meshes, mats, starts):
+        blob += struct.pack("<2I5f", mesh.nodes, mesh.tets, mat.density, mat.youngs_modulus, mat.poissons_ratio,
+                            mat.yield_stress, mat.hardening_modulus)
+        blob += mesh.rest_positions.astype(np.float32).tobytes() + mesh.node_mass.astype(np.float32).tobytes()
+        blob += mesh.anchored.astype(np.uint8).tobytes()
+        for e in range(mesh.tets):
+            blob += mesh.tet_nodes[e].astype(np.uint32).tobytes() + mesh.rest_inverse[e].astype(np.float32).tobytes()
+            blob += np.float32(mesh.volume[e]).tobytes()
+        blob += st.position.astype(np.float32).tobytes() + st.velocity.astype(np.float32).tobytes()
+    (work / "island.bin").write_bytes(blob)
+    out = subprocess.run([str(exe), str(work / "island.bin"), str(work / "island.out")], capture_output=True,
+                         text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    raw = (work / "island.out").read_bytes()
+    at = 0
+    for mesh, mat, st in zip(meshes, mats, starts):
+        pos = np.frombuffer(raw, np.float32, mesh.nodes * 3, at).reshape(-1, 3).astype(np.float64)
+        at += pos.size * 4
+        eq = np.frombuffer(raw, np.float32, mesh.tets, at)
+        at += eq.size * 4
+        n, evals = np.frombuffer(raw, np.uint32, 2, at)
+        at += 8
+        om = to_oracle(mesh)
+        ostate = po.State(st.position.copy(), st.velocity.copy(), st.acceleration.copy(), st.rotation.copy(),
+                          st.plastic.copy())
+        omat = po.material(mat.density, mat.youngs_modulus, mat.poissons_ratio, 0.0, mat.yield_stress,
+                           mat.hardening_modulus)
+        oevals = 0
+        for _ in range(steps):
+            oevals += po.step(po.F64, om, ostate, [omat], po.Settings(), GRAVITY, DT).plastic_evaluations
+        assert relative_error(pos, ostate.position, mesh.rest_positions) <= 1e-5
+        # the float host state rounds every step, which can move a Newton stopping decision by one
+        assert n == steps and abs(int(evals) - oevals) <= max(2, oevals // 5)
+        if np.isfinite(mat.yield_stress):
+            assert (ostate.plastic[:, 9] > 0).any()
+            assert np.abs(eq - ostate.plastic[:, 9]).max() <= 1e-4 * ostate.plastic[:, 9].max()
