@@ -1218,6 +1218,8 @@ struct System final : SystemBase {
   uint64_t solveCount = 0;  // PCG solves issued in the current step
   void pcg(int law, Vec4<S>* X, uint32_t pass, bool x0zero, bool tangent) {
     if (expireSolve >= 0 && solveCount == uint64_t(expireSolve)) {
+      // the previous solve left its arrivals in the counter: start the wait from zero
+      TL_CUDA(cudaMemsetAsync(&sync.ptr->arrive, 0, sizeof(unsigned int), st));
       kWaitLimitCheck<<<1, TILE, 0, st>>>(sync.ptr);
       check();
       expireSolve = -1;

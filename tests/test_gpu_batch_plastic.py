@@ -6,7 +6,8 @@ linear-read hand-off, the fallback and its rejection) as a state machine; the
 device work of all bodies is issued together in rounds, gated per body
 (tl_system.cu: newtonBatch).  A ragged batch of plastic blocks pushed from
 the top, with an elastic body among them, must give every body the result
-and the Newton counts it gets alone and from the FP64 oracle.
+and the Newton counts it gets alone (the plastic bar, 1e-8) and from the FP64
+oracle.
 """
 import numpy as np
 import pytest
@@ -69,8 +70,10 @@ def test_plastic_batch_equals_each_body_alone(form):
             assert (r.plastic_evaluations, r.plastic_solves, r.plastic_backtracks) == batch_counts[k][i], (i, k)
         got = alone.get_state()
         alone.close()
-        assert relative_error(batch[i].position, got.position, m.rest_positions) <= 1e-10, i
-        assert np.abs(batch[i].plastic[:, 9] - got.plastic[:, 9]).max() <= 1e-10 * max(1.0, got.plastic[:, 9].max())
+        # alone a body runs the single-body PCG kernels, in the batch the batched ones: the same
+        # operator summed in another order, so the plastic path's FP64 bar applies
+        assert relative_error(batch[i].position, got.position, m.rest_positions) <= 1e-8, i
+        assert np.abs(batch[i].plastic[:, 9] - got.plastic[:, 9]).max() <= 1e-8 * max(1e-30, got.plastic[:, 9].max())
     evaluations = sum(c[i][0] for c in batch_counts for i in range(len(meshes)))
     assert evaluations > 3 * steps * len(CELLS)  # the Newton path ran
 
