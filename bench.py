@@ -788,6 +788,7 @@ def batch_form(context, flush, warmup=2, steps=5, tolerance=1e-6, cap=4000):
         for _ in range(warmup):
             system.step(settings)
         seconds, iters, launches, capped = 0.0, [], 0, 0
+        body_iters = np.zeros(len(meshes))
         for _ in range(steps):
             flush.zero_()
             torch.cuda.synchronize()
@@ -795,12 +796,16 @@ def batch_form(context, flush, warmup=2, steps=5, tolerance=1e-6, cap=4000):
             seconds += reps[0].device_seconds
             launches += reps[0].kernel_launches
             iters.append(max(r.cg_iterations for r in reps))
+            body_iters += [r.cg_iterations for r in reps]
             capped += sum(r.cg_capped_solves for r in reps)
         finals[name] = [system.get_state(i).position for i in range(len(meshes))]
         system.close()
         tets = sum(m.tets for m in meshes)
         out[name] = {"value": tets * steps / seconds, "ms_per_step": seconds * 1e3 / steps,
                      "max_body_cg_iterations_per_step": float(np.mean(iters)), "gpu_launches": launches,
+                     "body_cg_iterations_per_step": {
+                         q: float(np.percentile(body_iters / steps, p)) for q, p in
+                         (("min", 0), ("median", 50), ("p90", 90), ("max", 100))},
                      "capped_solves": capped, "tuning": tune}
     worst = max(float(np.linalg.norm(a - b, axis=1).max() / np.linalg.norm(b - m.rest_positions, axis=1).max())
                 for a, b, m in zip(finals["mixed"], finals["fp64"], meshes))

@@ -568,13 +568,21 @@ enum ElementMode : uint32_t {
 // element pass starts: one wave of coalesced copies per tile instead of
 // loads spread through the kernel, and the second read of Dm^-1 and the
 // plastic point (after the rotation) come from here, not from L2.
+// The displacement gradient H is parked here across the corotated law's
+// rotation: the rotation's FP64 iteration needs every register it can get,
+// and values that spill instead go to local memory, which shares the L1
+// with this stage and misses it.
 template <class S> struct ElementStage {
   double dm[9][TILE];       // Dm^-1 planes (FP64)
+  double h[9][TILE];        // H (row-major planes) while the rotation runs
   double vol[TILE];
   uint4 tet[TILE];
   Vec4<S> plast[2][TILE];
   uint32_t lane[TILE];
 };
+// Dynamic shared memory of kElement (above the 48 KB a launch gets without
+// opting in; the host raises the limit once per instantiation).
+template <class S> constexpr size_t elementStageBytes() { return sizeof(ElementStage<S>); }
 
 // Element pass (assembleElastic, solver.cc:1354-1572; trial material.cc:236-265;
 // tetPointTrial material.cc:978-1057; SNH neohookean.cc:41-47, 183-192).
@@ -603,7 +611,8 @@ __global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
     mode = (mode & ~uint32_t(EM_CONSISTENT | EM_MAPPING)) | (s.gate[b] & uint32_t(EM_CONSISTENT | EM_MAPPING));
   const uint32_t e = tile * TILE + threadIdx.x;
   const bool valid = e < s.body[b].elem_end;
-  __shared__ ElementStage<S> stage;
+  extern __shared__ __align__(32) unsigned char tlElementStage[];
+  ElementStage<S>& stage = *reinterpret_cast<ElementStage<S>*>(tlElementStage);
   const uint32_t me = threadIdx.x;
   if (valid) {
     cpAsync<16>(&stage.tet[me], &s.tet[e]);
@@ -687,8 +696,19 @@ __global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
       F.m[0][0] += 1.0;
       F.m[1][1] += 1.0;
       F.m[2][2] += 1.0;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) stage.h[3 * i + j][me] = H.m[i][j];
       // ElementRotation::Polar for floating bodies, Invertible otherwise (solver.cc:3587-3588)
       const M3<double> R = elementRotation(F, st.floating == 0u);
+      // H comes back from shared memory (the clobber keeps the compiler from
+      // holding it in registers through the rotation instead)
+      asm volatile("" ::: "memory");
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) H.m[i][j] = stage.h[3 * i + j][me];
       // Corotated strain (material.cc:92-109, 155-161): the offsets
       // R^T (x_c - x_mean) - (X_c - X_mean) summed against g_c.  Because
       // sum_c g_c = 0 and sum_c X_c g_c^T = Ds Dm^-1 = I, that sum is
@@ -699,25 +719,17 @@ __global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
 #pragma unroll
         for (int j = 0; j < 3; ++j) D.m[i][j] += R.m[j][i] - (i == j ? 1.0 : 0.0);
       const Sym<double> eps = symOf(D);
-      // The gradients are loaded again rather than kept live through the
-      // rotation; the empty asm keeps the compiler from merging the loads.
-      asm volatile("" ::: "memory");
-      V3<double> g[4];
-      {
-        g[1] = {stage.dm[0][me], stage.dm[1][me], stage.dm[2][me]};
-        g[2] = {stage.dm[3][me], stage.dm[4][me], stage.dm[5][me]};
-        g[3] = {stage.dm[6][me], stage.dm[7][me], stage.dm[8][me]};
-        if constexpr (HK) {  // g' = P^T g (P reloaded: not kept live through the rotation)
-          double p[9];
+      // the rotation in S from here on (the committed rotation is stored in S)
+      M3<S> Rw;
 #pragma unroll
-          for (int k = 0; k < 9; ++k) p[k] = s.hk[size_t(k) * s.Tp + e];
+      for (int i = 0; i < 3; ++i)
 #pragma unroll
-          for (int c = 1; c < 4; ++c)
-            g[c] = {p[0] * g[c].x + p[3] * g[c].y + p[6] * g[c].z, p[1] * g[c].x + p[4] * g[c].y + p[7] * g[c].z,
-                    p[2] * g[c].x + p[5] * g[c].y + p[8] * g[c].z};
-        }
-        g[0] = -(g[1] + g[2] + g[3]);
-      }
+        for (int j = 0; j < 3; ++j) Rw.m[i][j] = S(R.m[i][j]);
+      if (!(mode & EM_COMMIT))
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) s.op[size_t(3 * i + j) * s.Tp + e] = Rw.m[i][j];
       // From here on the arithmetic is the storage type S: the strain above
       // needs FP64 (it is a small difference of O(1) quantities); the return
       // map, stress and forces only need the relative accuracy of the S
@@ -787,14 +799,29 @@ __global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
         energy = double(volC * C(0.5) * symContract(stress, ec));
       }
       if (!(mode & EM_COMMIT)) {
+        // The gradients are loaded again here rather than kept live through the
+        // rotation and the return map; the empty asm keeps the compiler from
+        // merging the loads with the first ones.
+        asm volatile("" ::: "memory");
+        V3<double> g[4];
+        {
+          g[1] = {stage.dm[0][me], stage.dm[1][me], stage.dm[2][me]};
+          g[2] = {stage.dm[3][me], stage.dm[4][me], stage.dm[5][me]};
+          g[3] = {stage.dm[6][me], stage.dm[7][me], stage.dm[8][me]};
+          if constexpr (HK) {  // g' = P^T g (P reloaded: not kept live through the rotation)
+            double p[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) p[k] = s.hk[size_t(k) * s.Tp + e];
+#pragma unroll
+            for (int c = 1; c < 4; ++c)
+              g[c] = {p[0] * g[c].x + p[3] * g[c].y + p[6] * g[c].z, p[1] * g[c].x + p[4] * g[c].y + p[7] * g[c].z,
+                      p[2] * g[c].x + p[5] * g[c].y + p[8] * g[c].z};
+          }
+          g[0] = -(g[1] + g[2] + g[3]);
+        }
         const bool tangentDiag = (mode & EM_CONSISTENT) && yields;
         const C th = tangentDiag ? theta : C(1);
         const C thb = tangentDiag ? thetaBar : C(0);
-        M3<S> Rw;
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-          for (int j = 0; j < 3; ++j) Rw.m[i][j] = S(R.m[i][j]);
         const Sym<S> nw = normal;
         const S k1 = volC * (bulk + muC * th / C(3)), kmu = volC * muC * th, k3 = -volC * C(2) * muC * thb;
 #pragma unroll
@@ -809,10 +836,6 @@ __global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
                           k1 * rg.z * rg.z + k2 + k3 * rn.z * rn.z, k1 * rg.x * rg.y + k3 * rn.x * rn.y,
                           k1 * rg.x * rg.z + k3 * rn.x * rn.z, k1 * rg.y * rg.z + k3 * rn.y * rn.z});
         }
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-          for (int j = 0; j < 3; ++j) s.op[size_t(3 * i + j) * s.Tp + e] = S(R.m[i][j]);
         // Matvec operator in the rotated frame: R K R^T p = sum over corners of
         // V sigma_t(sym(sum_b p_b gh_b^T)) gh_a with gh = R g and the rotated
         // normal R n R^T; h_eff^2 V folded into the coefficients.

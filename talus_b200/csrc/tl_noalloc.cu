@@ -182,6 +182,11 @@ int32_t setupDevice(int32_t device, DeviceSetup*& out) {
       cudaFuncAttributes attr;
       if (cudaFuncGetAttributes(&attr, k) != cudaSuccess) return TL_ERR_CUDA;
     }
+    // the element pass's shared-memory stage is above the default 48 KB
+    for (const void* k : {(const void*)kElement<S, 0>, (const void*)kElement<S, 1>})
+      if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, int(elementStageBytes<S>())) !=
+          cudaSuccess)
+        return TL_ERR_CUDA;
     d.arena = static_cast<unsigned char*>(ptr);
     d.ready = true;
   }
@@ -446,8 +451,8 @@ int32_t stepLocked(int32_t device, const tl_mesh_desc& d, int32_t dtype, void* p
         return TL_ERR_CUDA;
     }
     if (anyYields) mode |= EM_YIELDING;
-    if (law == TL_LAW_SNH) kElement<S, 1><<<elemTiles, TILE, 0, st>>>(s, base, dir, pass, mode, 0.0);
-    else kElement<S, 0><<<elemTiles, TILE, 0, st>>>(s, base, dir, pass, mode, 0.0);
+    if (law == TL_LAW_SNH) kElement<S, 1><<<elemTiles, TILE, elementStageBytes<S>(), st>>>(s, base, dir, pass, mode, 0.0);
+    else kElement<S, 0><<<elemTiles, TILE, elementStageBytes<S>(), st>>>(s, base, dir, pass, mode, 0.0);
     ++launches;
     return cudaGetLastError() == cudaSuccess ? TL_OK : TL_ERR_CUDA;
   };

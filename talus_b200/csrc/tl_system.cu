@@ -976,6 +976,9 @@ struct System final : SystemBase {
       if (n < 1) throw StatusError{TL_ERR_CUDA, "PCG kernel cannot be resident"};
       return n;
     };
+    // the element pass's shared-memory stage is above the default 48 KB
+    for (const void* fn : {(const void*)kElement<S, 0>, (const void*)kElement<S, 1>, (const void*)kElement<S, 0, true>})
+      TL_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(elementStageBytes<S>())));
     pcg1PerSm[0][0] = perSm((const void*)kPcg1<S, 0, false>, sizeof(TileCache));
     pcg1PerSm[0][1] = perSm((const void*)kPcg1<S, 0, true>, sizeof(TileCache));
     pcg1PerSm[1][0] = perSm((const void*)kPcg1<S, 1, false>, sizeof(TileCache));
@@ -1196,9 +1199,9 @@ struct System final : SystemBase {
     if (profiling) mark(0, true);
     if (std::any_of(hb.begin(), hb.end(), [](const HostBody& h) { return h.anyYields; })) mode |= EM_YIELDING;
     const bool damps = hasDamping && law == TL_LAW_COROTATED && !(mode & EM_COMMIT) && !evaluating;
-    if (law == TL_LAW_SNH) kElement<S, 1><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass, mode, margin);
-    else if (hencky) kElement<S, 0, true><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass, mode, margin);
-    else kElement<S, 0><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass, mode, margin);
+    if (law == TL_LAW_SNH) kElement<S, 1><<<elemTiles, TILE, elementStageBytes<S>(), st>>>(view(), base, dir, pass, mode, margin);
+    else if (hencky) kElement<S, 0, true><<<elemTiles, TILE, elementStageBytes<S>(), st>>>(view(), base, dir, pass, mode, margin);
+    else kElement<S, 0><<<elemTiles, TILE, elementStageBytes<S>(), st>>>(view(), base, dir, pass, mode, margin);
     check();
     if (damps) {
       kDamping<S><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass);
