@@ -192,10 +192,20 @@ int32_t tl_system_tune(tl_system* system, uint32_t pcg_blocks_per_sm, uint32_t g
  * TL_SOLVER_ELEMENTWISE always iterates element by element;
  * TL_SOLVER_AUTO (default) is ASSEMBLED for batched systems and for single
  * bodies of at least 32,768 tets, ELEMENTWISE for smaller single bodies.
- * Both forms apply the same operator; they differ in rounding. */
+ * Both forms apply the same operator; they differ in rounding.  On the
+ * assembled matrix a batch (or a body too large for the single-body grid)
+ * iterates in one of two orders with the same iterates in exact arithmetic:
+ * TL_SOLVER_ASSEMBLED_TWO_PHASE, the textbook order with two grid barriers
+ * per iteration, or TL_SOLVER_ASSEMBLED_PIPELINED, the pipelined order with
+ * one barrier per iteration and four more vectors per node (FP64 systems
+ * only: with its recurrences stored in FP32 the pipelined order drifts).
+ * ASSEMBLED and AUTO take the pipelined order in FP64 and the two-phase
+ * order in FP32-mixed, the faster of each on the 512-body batch. */
 #define TL_SOLVER_AUTO 0u
 #define TL_SOLVER_ASSEMBLED 1u
 #define TL_SOLVER_ELEMENTWISE 2u
+#define TL_SOLVER_ASSEMBLED_TWO_PHASE 3u
+#define TL_SOLVER_ASSEMBLED_PIPELINED 4u
 int32_t tl_system_set_solver(tl_system* system, uint32_t form);
 
 /* Plasticity of the yielding lanes.

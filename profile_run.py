@@ -28,8 +28,10 @@ def main():
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--count", type=int, default=0, help="bodies of a batch workload (0: the workload's own)")
-    ap.add_argument("--solver", choices=["auto", "assembled", "elementwise"], default="auto",
-                    help="PCG operator form of a single-body system (tl_system_set_solver)")
+    ap.add_argument("--solver", choices=["auto", "assembled", "assembled-two-phase", "elementwise"], default="auto",
+                    help="PCG operator form (tl_system_set_solver)")
+    ap.add_argument("--tolerance", type=float, default=1e-3, help="PCG relative tolerance")
+    ap.add_argument("--cap", type=int, default=64, help="PCG iteration cap")
     args = ap.parse_args()
     spec = dict(WORKLOADS[args.workload])
     if args.count and spec.get("batch"):
@@ -41,7 +43,7 @@ def main():
     system.set_solver(args.solver)
     for i, m in enumerate(meshes):
         system.set_state(tb.rest_state(m), i)
-    settings = tb.Settings(law=law, trace=True)
+    settings = tb.Settings(law=law, trace=True, tolerance=args.tolerance, cg_iterations=args.cap)
     reports = [[r.as_dict() for r in system.step(settings)] for _ in range(args.steps)]
     print(json.dumps({"workload": args.workload, "precision": args.precision,
                       "tets": sum(m.tets for m in meshes), "nodes": sum(m.nodes for m in meshes),

@@ -36,6 +36,8 @@ TL_FLAG_TRACE = 2
 TL_SOLVER_AUTO = 0
 TL_SOLVER_ASSEMBLED = 1
 TL_SOLVER_ELEMENTWISE = 2
+TL_SOLVER_ASSEMBLED_TWO_PHASE = 3
+TL_SOLVER_ASSEMBLED_PIPELINED = 4
 TL_PLASTICITY_SMALL_STRAIN = 0
 TL_PLASTICITY_HENCKY = 1
 

@@ -11,14 +11,18 @@ through ``System.tune``:
 * ``graph``: whether a batched elastic step is replayed from one captured CUDA
   graph (device-side substep choice) or launched kernel by kernel.
 * ``solver``: the PCG operator form (``System.set_solver``): "auto" (the
-  block matrix assembled once per solve, for these workloads) or
+  block matrix assembled once per solve, for these workloads), for a batch
+  "assembled-two-phase" (two grid barriers per iteration, fewer bytes) and,
+  in FP64, "assembled-pipelined" (one barrier per iteration), or
   "elementwise".  The block cap applies to the element-by-element kernels;
   the assembled ones take their own occupancy, so they are timed at 0.
 
 Every candidate starts from the same rest state and runs the same steps, so
 the candidates do the same physics; the score is device seconds per step.
+The PCG tolerance and cap are those of the run the table is for (the batched
+record solves every body to 1e-6 under a cap of 4000).
 
-    python -m talus_b200.autotune --workload batch --precision mixed --out talus_b200/tuning.json
+    python -m talus_b200.autotune --workload batch --precision mixed --tolerance 1e-6 --cap 4000
 """
 from __future__ import annotations
 
@@ -30,10 +34,13 @@ import sys
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def candidates(bodies: int):
+def candidates(bodies: int, fp64: bool):
     graphs = [True, False] if bodies > 1 else [False]
     out = [("elementwise", k, g) for k in (0, 1, 2, 3) for g in graphs]
-    return out + [("auto", 0, g) for g in graphs]
+    forms = ["auto"]
+    if bodies > 1:
+        forms = ["assembled-two-phase", "assembled-pipelined"] if fp64 else ["assembled-two-phase"]
+    return out + [(form, 0, g) for form in forms for g in graphs]
 
 
 def time_candidate(system, meshes, settings, solver, blocks, graph, warmup, steps):
@@ -53,7 +60,8 @@ def time_candidate(system, meshes, settings, solver, blocks, graph, warmup, step
     return seconds / steps, iterations / steps
 
 
-def tune(workload: str, precision_name: str, warmup: int = 2, steps: int = 4) -> dict:
+def tune(workload: str, precision_name: str, warmup: int = 2, steps: int = 4, tolerance: float = 1e-3,
+         cap: int = 64) -> dict:
     sys.path.insert(0, ROOT)
     import talus_b200 as tb
     from talus_b200.workloads import WORKLOADS, make_bodies
@@ -62,10 +70,10 @@ def tune(workload: str, precision_name: str, warmup: int = 2, steps: int = 4) ->
     meshes, mats = make_bodies(spec)
     precision = tb.FP32_MIXED if precision_name == "mixed" else tb.FP64
     law = tb.NEO_HOOKEAN if spec["law"] == "snh" else tb.COROTATED
-    settings = tb.Settings(law=law)
+    settings = tb.Settings(law=law, tolerance=tolerance, cg_iterations=cap)
     system = tb.System(meshes, mats, precision)
     results = []
-    for solver, blocks, graph in candidates(len(meshes)):
+    for solver, blocks, graph in candidates(len(meshes), precision == tb.FP64):
         sec, its = time_candidate(system, meshes, settings, solver, blocks, graph, warmup, steps)
         results.append({"solver": solver, "pcg_blocks_per_sm": blocks, "graph": graph, "ms_per_step": sec * 1e3,
                         "cg_iterations_per_step": its})
@@ -73,7 +81,8 @@ def tune(workload: str, precision_name: str, warmup: int = 2, steps: int = 4) ->
     system.close()
     best = min(results, key=lambda r: r["ms_per_step"])
     return {"solver": best["solver"], "pcg_blocks_per_sm": best["pcg_blocks_per_sm"], "graph": best["graph"],
-            "ms_per_step": best["ms_per_step"], "steps": steps, "candidates": results}
+            "ms_per_step": best["ms_per_step"], "steps": steps, "tolerance": tolerance, "cg_iterations": cap,
+            "candidates": results}
 
 
 def main():
@@ -81,9 +90,11 @@ def main():
     ap.add_argument("--workload", default="batch")
     ap.add_argument("--precision", choices=["mixed", "fp64"], default="mixed")
     ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--tolerance", type=float, default=1e-3)
+    ap.add_argument("--cap", type=int, default=64)
     ap.add_argument("--out", default=os.path.join(ROOT, "talus_b200", "tuning.json"))
     args = ap.parse_args()
-    entry = tune(args.workload, args.precision, steps=args.steps)
+    entry = tune(args.workload, args.precision, steps=args.steps, tolerance=args.tolerance, cap=args.cap)
     table = {}
     if os.path.exists(args.out):
         with open(args.out) as f:

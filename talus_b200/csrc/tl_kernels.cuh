@@ -137,7 +137,9 @@ struct GridSyncDev {
   unsigned int arrive;
   unsigned int generation;
   int error;
-  int active;  // bodies still iterating in the current PCG solve
+  int active;      // bodies still iterating in the current PCG solve
+  int active_odd;  // its copy for odd phases of the one-barrier batched PCG (kPcgBatchSellPipe)
+  int pad;
 };
 
 // Per-element matvec operator, one record per element: the gradients
@@ -1832,10 +1834,11 @@ __global__ void __launch_bounds__(TILE, 2)
 
 // ------------------------------------------------ single-body fast PCG ----
 
-__device__ __forceinline__ unsigned int atomAddRelease(unsigned int* p, unsigned int v) {
-  unsigned int old;
-  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
-  return old;
+// Release add without a returned value: the arriving block starts polling
+// without waiting for the atomic's reply (its own later load of the counter
+// sees the add, which precedes it in program order on the same address).
+__device__ __forceinline__ void redAddRelease(unsigned int* p, unsigned int v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 __device__ __forceinline__ unsigned int ldAcquire(const unsigned int* p) {
   unsigned int v;
@@ -1854,7 +1857,7 @@ __device__ __forceinline__ bool countBarrier(GridSyncDev* sync, unsigned int& k)
   if (threadIdx.x == 0) {
     int good = 1;
     const unsigned int goal = gridDim.x * k;
-    atomAddRelease(&sync->arrive, 1u);
+    redAddRelease(&sync->arrive, 1u);
     if (ldAcquire(&sync->arrive) < goal) {
       const unsigned long long t0 = globalTimer();
       unsigned int polls = 0;
@@ -1893,6 +1896,46 @@ __device__ __forceinline__ void sumBlocksAll(const double* part, double (&out)[N
   for (unsigned b = threadIdx.x; b < G; b += TILE)
 #pragma unroll
     for (int k = 0; k < N; ++k) v[k] += __ldcg(part + size_t(k) * G + b);
+#pragma unroll
+  for (int k = 0; k < N; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int k = 0; k < N; ++k) red[k][threadIdx.x >> 5] = v[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    double t = 0.0;
+#pragma unroll
+    for (int w = 0; w < TILE / 32; ++w) t += red[k][w];
+    out[k] = t;
+  }
+  __syncthreads();
+}
+
+// The first `fields` G partials of part (field k of block b at part[k G + b]),
+// requested into shared memory by cp.async in 16-byte pieces through L2 and
+// committed as one group; the caller waits for it (cp.async.wait_group 0),
+// then a block barrier, before sumStagedBlocks reads them.  part is 16-byte
+// aligned and holds at least fields G + 1 values.
+__device__ __forceinline__ void requestBlockPartials(const double* part, double* stage, unsigned fields) {
+  const unsigned pieces = (fields * gridDim.x + 1u) / 2u;
+  for (unsigned i = threadIdx.x; i < pieces; i += TILE) cpAsync<16>(stage + 2 * i, part + 2 * i);
+  cpAsyncCommit();
+}
+// sumBlocksAll on partials staged by requestBlockPartials: the same order of
+// additions, so the same sums.
+template <int N>
+__device__ __forceinline__ void sumStagedBlocks(const double* stage, double (&out)[N]) {
+  __shared__ double red[N][TILE / 32];
+  const unsigned G = gridDim.x;
+  double v[N];
+#pragma unroll
+  for (int k = 0; k < N; ++k) v[k] = 0.0;
+  for (unsigned b = threadIdx.x; b < G; b += TILE)
+#pragma unroll
+    for (int k = 0; k < N; ++k) v[k] += stage[size_t(k) * G + b];
 #pragma unroll
   for (int k = 0; k < N; ++k)
 #pragma unroll
@@ -2677,6 +2720,7 @@ __global__ void kPcgPrepare(Sys<S> s, uint32_t pass) {
   if (threadIdx.x == 0) {
     s.sync->arrive = 0u;
     s.sync->active = count;
+    s.sync->active_odd = count;
   }
 }
 

@@ -14,9 +14,12 @@
 //                  land there (FP64 accumulation, stored in S), written with
 //                  its transpose below the diagonal; the diagonal blocks are
 //                  written by kNodeAssemble;
-//   kPcgBatchSell  the batched PCG of kPcgBatch on this matrix, for batches
-//                  and for single bodies with more rows than kPcgSell's grid
-//                  has threads;
+//   kPcgBatchSellPipe  the batched PCG on this matrix, for batches and for
+//                  single bodies with more rows than kPcgSell's grid has
+//                  threads: kPcgSell's pipelined arrangement with per-body
+//                  scalars, one grid barrier per iteration;
+//   kPcgBatchSell  the same solve in the textbook order (two barriers per
+//                  iteration, fewer vectors; TL_SOLVER_ASSEMBLED_TWO_PHASE);
 //   kPcgSell       (one body) persistent cooperative PCG in the pipelined arrangement
 //                  of Ghysels and Vanroose ("Hiding global synchronization
 //                  latency in the preconditioned conjugate gradient
@@ -174,24 +177,33 @@ __device__ __forceinline__ void sellSlot(const SellDev<S>& g, uint32_t p, uint32
 
 // y = A in for the thread's row.  Column slots are taken U at a time (4 in
 // FP32, 2 in FP64): their input values and block entries are requested
-// together; the FMAs run slot by slot in order.
+// together, with the next group's column indices, so a group costs one
+// round trip to memory; the FMAs run slot by slot in order.
 template <class S, class In, uint32_t U = sizeof(S) == 4 ? 4u : 2u>
 __device__ __forceinline__ V3<double> sellRowOf(const SellDev<S>& g, uint32_t slice, uint32_t lane, In in,
                                                 const uint32_t* cols) {
   V3<double> acc = {0, 0, 0};
   const uint32_t p1 = __ldg(&g.slice_start[slice + 1]);
   uint32_t p = __ldg(&g.slice_start[slice]) + lane, k = 0;
-  for (; p + (U - 1) * SELL_ROWS < p1; p += U * SELL_ROWS, k += U) {
-    uint32_t c[U];
+  uint32_t c[U];
 #pragma unroll
-    for (uint32_t i = 0; i < U; ++i) c[i] = sellCol(cols, g.col_cache, k + i, g.col, p + i * SELL_ROWS);
+  for (uint32_t i = 0; i < U; ++i)
+    c[i] = p + i * SELL_ROWS < p1 ? sellCol(cols, g.col_cache, k + i, g.col, p + i * SELL_ROWS) : 0u;
+  for (; p + (U - 1) * SELL_ROWS < p1; p += U * SELL_ROWS, k += U) {
     Vec4<S> xin[U];
 #pragma unroll
     for (uint32_t i = 0; i < U; ++i) xin[i] = in(c[i]);
+    const uint32_t pn = p + U * SELL_ROWS;
+#pragma unroll
+    for (uint32_t i = 0; i < U; ++i)
+      c[i] = pn + i * SELL_ROWS < p1 ? sellCol(cols, g.col_cache, k + U + i, g.col, pn + i * SELL_ROWS) : 0u;
 #pragma unroll
     for (uint32_t i = 0; i < U; ++i) sellSlot(g, p + i * SELL_ROWS, lane, xin[i], acc);
   }
-  for (; p < p1; p += SELL_ROWS, ++k) sellSlot(g, p, lane, in(sellCol(cols, g.col_cache, k, g.col, p)), acc);
+  // fewer than U slots remain; their columns are in c already
+#pragma unroll
+  for (uint32_t i = 0; i + 1 < U; ++i)
+    if (p + i * SELL_ROWS < p1) sellSlot(g, p + i * SELL_ROWS, lane, in(c[i]), acc);
   return acc;
 }
 // The matvec input read from a vector written during the launch (L2).
@@ -204,6 +216,39 @@ template <class S>
 __device__ __forceinline__ V3<double> sellRow(const SellDev<S>& g, uint32_t slice, uint32_t lane,
                                               const Vec4<S>* in, const uint32_t* cols) {
   return sellRowOf(g, slice, lane, ld4cgOf(in), cols);
+}
+
+// y = A in for the thread's row, with the row's inputs gathered first: up to
+// sellGatherSlots column slots are requested at once by cp.async (16-byte
+// copies through L2, so values published by other blocks during the launch
+// are seen) into the thread's column of a shared stage, so the row waits one
+// round trip for all its inputs instead of one per group of slots.  Each
+// thread reads back only what it copied, so no block barrier is needed.  The
+// slots are summed in the order of sellRowOf, with the same result.
+template <class S> __host__ __device__ constexpr uint32_t sellGatherSlots() { return sizeof(S) == 4 ? 16u : 8u; }
+
+template <class S>
+__device__ __forceinline__ V3<double> sellRowStaged(const SellDev<S>& g, uint32_t slice, uint32_t lane,
+                                                    const Vec4<S>* in, const uint32_t* cols, Vec4<S>* stage) {
+  constexpr uint32_t GS = sellGatherSlots<S>();
+  V3<double> acc = {0, 0, 0};
+  const uint32_t p1 = __ldg(&g.slice_start[slice + 1]);
+  uint32_t p = __ldg(&g.slice_start[slice]) + lane, k = 0;
+  while (p < p1) {
+    uint32_t cnt = 0;
+    for (uint32_t q = p; q < p1 && cnt < GS; q += SELL_ROWS, ++cnt) {
+      const unsigned char* src =
+          reinterpret_cast<const unsigned char*>(in + sellCol(cols, g.col_cache, k + cnt, g.col, q));
+      unsigned char* dst = reinterpret_cast<unsigned char*>(&stage[cnt * TILE + threadIdx.x]);
+#pragma unroll
+      for (int h = 0; h < int(sizeof(Vec4<S>)) / 16; ++h) cpAsync<16>(dst + 16 * h, src + 16 * h);
+    }
+    cpAsyncCommit();
+    cpAsyncWaitAll();
+#pragma unroll 4
+    for (uint32_t i = 0; i < cnt; ++i, p += SELL_ROWS, ++k) sellSlot(g, p, lane, stage[i * TILE + threadIdx.x], acc);
+  }
+  return acc;
 }
 
 template <class S> __device__ __forceinline__ V3<double> roundTo(V3<double> v) {
@@ -238,6 +283,13 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
   const bool freeRow = live && !s.anch[row];
   const BodyStepDev st = s.step[0];
   extern __shared__ uint32_t tlCols[];  // [col_cache][TILE] the first columns of each thread's row
+  // then [sellGatherSlots][TILE] the matvec inputs of each thread's row
+  Vec4<S>* const stage = reinterpret_cast<Vec4<S>*>(tlCols + size_t(g.col_cache) * TILE);
+  // the block partials of each iteration's reduction, fetched while the matvec's inputs are
+  // (grids of up to SELL_PART_STAGE_BLOCKS blocks; larger ones read them from L2 after it)
+  constexpr unsigned SELL_PART_STAGE_BLOCKS = 320;
+  __shared__ __align__(16) double partStage[3 * SELL_PART_STAGE_BLOCKS + 2];
+  const bool stagedSums = G <= SELL_PART_STAGE_BLOCKS;
   if (mine) {
     const uint32_t p0 = __ldg(&g.slice_start[slice]) + lane, p1 = __ldg(&g.slice_start[slice + 1]);
     for (uint32_t k = 0, p = p0; k < g.col_cache && p < p1; ++k, p += SELL_ROWS)
@@ -265,7 +317,7 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
   uint32_t applications = 0;
   // ---- r = right - A x (anchored rows 0), u = P r, published to vec[1]
   if (!x0zero) {
-    const V3<double> ax = mine ? sellRow(g, slice, lane, X, tlCols) : V3<double>{0, 0, 0};
+    const V3<double> ax = mine ? sellRowStaged(g, slice, lane, X, tlCols, stage) : V3<double>{0, 0, 0};
     if (freeRow) r = rhs - ax;
     ++applications;
   } else if (freeRow) {
@@ -277,7 +329,7 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
   if (mine) vec1[row] = pack(cvt<S>(u));
   if (!countBarrier(s.sync, bar)) return;
   // ---- w = A u, m = P w published to vec[0], first reduction
-  V3<double> w = mine ? sellRow(g, slice, lane, vec1, tlCols) : V3<double>{0, 0, 0};
+  V3<double> w = mine ? sellRowStaged(g, slice, lane, vec1, tlCols, stage) : V3<double>{0, 0, 0};
   ++applications;
   V3<double> m = precondition(w);
   if (mine) vec0[row] = pack(cvt<S>(m));
@@ -291,7 +343,7 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
   if (!countBarrier(s.sync, bar)) return;
   // n = A m for the first iteration, requested before the block sums so that
   // their round trip overlaps it (unused if the solve stops here)
-  V3<double> n = mine ? sellRow(g, slice, lane, vec0, tlCols) : V3<double>{0, 0, 0};
+  V3<double> n = mine ? sellRowStaged(g, slice, lane, vec0, tlCols, stage) : V3<double>{0, 0, 0};
   double sums[4];
   sumBlocksAll<4>(halves[0], sums);
   ++reductions;
@@ -349,10 +401,18 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
         for (int k = 0; k < 3; ++k) part[k * G + blockIdx.x] = v[k];
     }
     if (!countBarrier(s.sync, bar)) return;
-    // n = A m for the next iteration (m just published to vec[(taken + 1) & 1])
-    n = mine ? sellRow(g, slice, lane, (taken & 1u) ? vec0 : vec1, tlCols) : V3<double>{0, 0, 0};
+    // n = A m for the next iteration (m just published to vec[(taken + 1) & 1]), with the
+    // block partials requested first so that both round trips overlap
+    if (stagedSums) requestBlockPartials(part, partStage, 3u);
+    n = mine ? sellRowStaged(g, slice, lane, (taken & 1u) ? vec0 : vec1, tlCols, stage) : V3<double>{0, 0, 0};
     double d[3];
-    sumBlocksAll<3>(part, d);
+    if (stagedSums) {
+      cpAsyncWaitAll();
+      __syncthreads();
+      sumStagedBlocks<3>(partStage, d);
+    } else {
+      sumBlocksAll<3>(part, d);
+    }
     ++reductions;
     gammaNext = d[0];
     delta = d[1];
@@ -401,22 +461,44 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
 //       stopping test
 // with a grid barrier after each.  AB reads the neighbours' previous p while
 // writing the new one, so p alternates between two buffers by iteration.
+//
+// A block's tiles are blockIdx.x + j G (slot j); their bodies and row counts
+// are read once per launch into shared memory (tlBatchSlots, 8 bytes per
+// slot), and the next live slot's stopping flag and scalar are requested
+// while the current tile is worked, so a tile starts without a round trip.
+// A body's flag changes within a phase only in its last-arriving tile, after
+// every tile of the body has read it.
+__device__ __forceinline__ uint32_t nextSlot(const uint32_t* slotBody, uint32_t j, uint32_t slots) {
+  while (j < slots && slotBody[j] == ~0u) ++j;
+  return j;
+}
+
 template <class S>
 __global__ void __launch_bounds__(TILE, 4)
     kPcgBatchSell(Sys<S> s, SellDev<S> g, Vec4<S>* X, Vec4<S>* p2, uint32_t pass, uint32_t x0zero, uint32_t tangent) {
+  extern __shared__ uint32_t tlBatchSlots[];  // [slots] body (~0u: not stepping), then [slots] rows
   const uint32_t G = gridDim.x, lane = threadIdx.x & 31u;
   g.col_cache = 0;  // no per-launch column cache: a block walks many slices
   const S zero = S(0);
   unsigned int bar = 0;
-  Vec4<S>* const pbuf[2] = {s.p, p2};
-  // ---- init: r = right - A x (anchored rows 0), z = P r, p_prev = 0
-  for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
+  const uint32_t slots = blockIdx.x < s.node_tiles ? (s.node_tiles - 1u - blockIdx.x) / G + 1u : 0u;
+  uint32_t* const slotBody = tlBatchSlots;
+  uint32_t* const slotRows = tlBatchSlots + slots;
+  for (uint32_t j = threadIdx.x; j < slots; j += TILE) {
+    const uint32_t tile = blockIdx.x + j * G;
     const uint32_t b = s.node_tile_body[tile];
-    if (!bodyActive(s, b, pass)) continue;
+    const bool live = bodyActive(s, b, pass);
+    slotBody[j] = live ? b : ~0u;
+    slotRows[j] = live ? min(TILE, s.body[b].node_end - tile * TILE) : 0u;
+  }
+  __syncthreads();
+  // ---- init: r = right - A x (anchored rows 0), z = P r, p_prev = 0
+  for (uint32_t j = nextSlot(slotBody, 0u, slots); j < slots; j = nextSlot(slotBody, j + 1u, slots)) {
+    const uint32_t b = slotBody[j], tile = blockIdx.x + j * G;
     const BodyDev bd = s.body[b];
     const uint32_t n = tile * TILE + threadIdx.x;
     double sums[3] = {0.0, 0.0, 0.0};
-    if (n < bd.node_end) {
+    if (threadIdx.x < slotRows[j]) {
       const Vec4<S> rhs = s.right[n];
       V3<S> r = {zero, zero, zero};
       if (!s.anch[n]) {
@@ -467,90 +549,131 @@ __global__ void __launch_bounds__(TILE, 4)
   }
   if (!countBarrier(s.sync, bar)) return;
   for (uint32_t it = 0;; ++it) {
-    if (*(volatile int*)&s.sync->active <= 0) break;  // uniform: no block decrements between here and barrier AB
-    const Vec4<S>* pprev = pbuf[it & 1u];
-    Vec4<S>* pnew = pbuf[(it + 1u) & 1u];
+    // uniform: the count changes only in C, whose barrier every block has passed
+    if (*(volatile int*)&s.sync->active <= 0) break;
+    const Vec4<S>* pprev = (it & 1u) ? p2 : s.p;
+    Vec4<S>* pnew = (it & 1u) ? s.p : p2;
     // ---- AB
-    for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
-      const uint32_t b = s.node_tile_body[tile];
-      if (!bodyActive(s, b, pass) || __ldcg(&s.cg[b].done)) continue;
-      const BodyDev bd = s.body[b];
-      const uint32_t n = tile * TILE + threadIdx.x;
-      double sums[1] = {0.0};
-      if (n < bd.node_end) {
-        const S blend = S(__ldcg(&s.cg[b].blend));
-        const auto pOf = [&](uint32_t c) {
-          return pack(fmaV(blend, xyz(ld4cg(&pprev[c])), xyz(ld4cg(&s.z[c]))));
-        };
-        const V3<S> pn = xyz(pOf(n));
-        pnew[n] = pack(pn);
-        V3<S> apn = {zero, zero, zero};
-        if (!s.anch[n])
-          apn = cvt<S>(sellRowOf<S, decltype(pOf), 2u>(g, n >> 5, lane, pOf, static_cast<const uint32_t*>(nullptr)));
-        s.ap[n] = pack(apn);
-        sums[0] = dot(cvt<double>(pn), cvt<double>(apn));
+    uint32_t j = nextSlot(slotBody, 0u, slots), done = 1u;
+    double blendNow = 0.0;
+    if (j < slots) {
+      done = __ldcg(&s.cg[slotBody[j]].done);
+      blendNow = __ldcg(&s.cg[slotBody[j]].blend);
+    }
+    while (j < slots) {
+      const uint32_t b = slotBody[j], tile = blockIdx.x + j * G, rows = slotRows[j];
+      const uint32_t jn = nextSlot(slotBody, j + 1u, slots);
+      uint32_t doneNext = 1u;
+      double blendNext = 0.0;
+      if (jn < slots) {
+        doneNext = __ldcg(&s.cg[slotBody[jn]].done);
+        blendNext = __ldcg(&s.cg[slotBody[jn]].blend);
       }
-      blockSum<1>(sums);
-      if (threadIdx.x == 0) s.part[size_t(tile) * 4 + 3] = sums[0];
-      if (lastTileOfBody(&s.counter[b], bd.node_tile_end - bd.node_tile_begin)) {
-        double tot[1];
-        sumTiles<1>(s.part + 3, bd.node_tile_begin, bd.node_tile_end, tot);
-        if (threadIdx.x == 0) {
-          const double curvature = tot[0];
-          const double squared = __ldcg(&s.cg[b].squared);
-          if (!(curvature > 0.0) || !(squared > 0.0)) {
-            s.cg[b].done = 1u;
-            __threadfence();
-            atomicSub(&s.sync->active, 1);
-          } else {
-            s.cg[b].stride = squared / curvature;
+      if (!done) {
+        const BodyDev bd = s.body[b];
+        const uint32_t n = tile * TILE + threadIdx.x;
+        double sums[1] = {0.0};
+        if (threadIdx.x < rows) {
+          const S blend = S(blendNow);
+          const auto pOf = [&](uint32_t c) {
+            return pack(fmaV(blend, xyz(ld4cg(&pprev[c])), xyz(ld4cg(&s.z[c]))));
+          };
+          const V3<S> pn = xyz(pOf(n));
+          pnew[n] = pack(pn);
+          V3<S> apn = {zero, zero, zero};
+          if (!s.anch[n])
+            apn = cvt<S>(sellRowOf<S, decltype(pOf), 2u>(g, n >> 5, lane, pOf, static_cast<const uint32_t*>(nullptr)));
+          s.ap[n] = pack(apn);
+          sums[0] = dot(cvt<double>(pn), cvt<double>(apn));
+        }
+        blockSum<1>(sums);
+        if (threadIdx.x == 0) s.part[size_t(tile) * 4 + 3] = sums[0];
+        if (lastTileOfBody(&s.counter[b], bd.node_tile_end - bd.node_tile_begin)) {
+          double tot[1];
+          sumTiles<1>(s.part + 3, bd.node_tile_begin, bd.node_tile_end, tot);
+          if (threadIdx.x == 0) {
+            const double curvature = tot[0];
+            const double squared = __ldcg(&s.cg[b].squared);
+            // a breakdown stops the body without an update; it is retired in C,
+            // so that no block changes the active count before this barrier
+            s.cg[b].pad0 = (!(curvature > 0.0) || !(squared > 0.0)) ? 1u : 0u;
+            s.cg[b].stride = s.cg[b].pad0 ? 0.0 : squared / curvature;
             __threadfence();
           }
         }
       }
+      j = jn;
+      done = doneNext;
+      blendNow = blendNext;
     }
     if (!countBarrier(s.sync, bar)) return;
     // ---- C
-    for (uint32_t tile = blockIdx.x; tile < s.node_tiles; tile += G) {
-      const uint32_t b = s.node_tile_body[tile];
-      if (!bodyActive(s, b, pass) || __ldcg(&s.cg[b].done)) continue;
-      const BodyDev bd = s.body[b];
-      const uint32_t n = tile * TILE + threadIdx.x;
-      double sums[2] = {0.0, 0.0};
-      if (n < bd.node_end) {
-        const S stride = S(__ldcg(&s.cg[b].stride));
-        const V3<S> pn = xyz(ld4cg(&pnew[n]));
-        const V3<S> x = fmaV(stride, pn, xyz(ld4cg(&X[n])));
-        const V3<S> r = fmaV(-stride, xyz(ld4cg(&s.ap[n])), xyz(ld4cg(&s.r[n])));
-        const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
-        const Sym<S> P = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
-        const V3<S> z = symMul(P, r);
-        X[n] = pack(x);
-        s.r[n] = pack(r);
-        s.z[n] = pack(z);
-        sums[0] = dot(cvt<double>(r), cvt<double>(z));
-        sums[1] = dot(cvt<double>(r), cvt<double>(r));
+    j = nextSlot(slotBody, 0u, slots);
+    done = 1u;
+    double strideNow = 0.0;
+    uint32_t brokenNow = 0u;
+    if (j < slots) {
+      done = __ldcg(&s.cg[slotBody[j]].done);
+      strideNow = __ldcg(&s.cg[slotBody[j]].stride);
+      brokenNow = __ldcg(&s.cg[slotBody[j]].pad0);
+    }
+    while (j < slots) {
+      const uint32_t b = slotBody[j], tile = blockIdx.x + j * G, rows = slotRows[j];
+      const uint32_t jn = nextSlot(slotBody, j + 1u, slots);
+      uint32_t doneNext = 1u, brokenNext = 0u;
+      double strideNext = 0.0;
+      if (jn < slots) {
+        doneNext = __ldcg(&s.cg[slotBody[jn]].done);
+        strideNext = __ldcg(&s.cg[slotBody[jn]].stride);
+        brokenNext = __ldcg(&s.cg[slotBody[jn]].pad0);
       }
-      blockSum<2>(sums);
-      if (threadIdx.x == 0) {
-        s.part[size_t(tile) * 4 + 0] = sums[0];
-        s.part[size_t(tile) * 4 + 1] = sums[1];
-      }
-      if (lastTileOfBody(&s.counter[b], bd.node_tile_end - bd.node_tile_begin)) {
-        double tot[2];
-        sumTiles<2>(s.part, bd.node_tile_begin, bd.node_tile_end, tot);
+      if (!done) {
+        const BodyDev bd = s.body[b];
+        const uint32_t n = tile * TILE + threadIdx.x;
+        double sums[2] = {0.0, 0.0};
+        if (threadIdx.x < rows && !brokenNow) {
+          const S stride = S(strideNow);
+          const V3<S> pn = xyz(ld4cg(&pnew[n]));
+          const V3<S> x = fmaV(stride, pn, xyz(ld4cg(&X[n])));
+          const V3<S> r = fmaV(-stride, xyz(ld4cg(&s.ap[n])), xyz(ld4cg(&s.r[n])));
+          const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
+          const Sym<S> P = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y};
+          const V3<S> z = symMul(P, r);
+          X[n] = pack(x);
+          s.r[n] = pack(r);
+          s.z[n] = pack(z);
+          sums[0] = dot(cvt<double>(r), cvt<double>(z));
+          sums[1] = dot(cvt<double>(r), cvt<double>(r));
+        }
+        blockSum<2>(sums);
         if (threadIdx.x == 0) {
-          CgBodyDev c = loadCg(&s.cg[b]);
-          c.blend = tot[0] / c.squared;
-          c.squared = tot[0];
-          c.length = tot[1];
-          c.taken += 1u;
-          c.done = (sqrt(c.length) <= c.target || c.taken >= s.step[b].limit) ? 1u : 0u;
-          s.cg[b] = c;
-          __threadfence();
-          if (c.done) atomicSub(&s.sync->active, 1);
+          s.part[size_t(tile) * 4 + 0] = sums[0];
+          s.part[size_t(tile) * 4 + 1] = sums[1];
+        }
+        if (lastTileOfBody(&s.counter[b], bd.node_tile_end - bd.node_tile_begin)) {
+          double tot[2];
+          sumTiles<2>(s.part, bd.node_tile_begin, bd.node_tile_end, tot);
+          if (threadIdx.x == 0) {
+            CgBodyDev c = loadCg(&s.cg[b]);
+            if (c.pad0) {  // broke down in AB: no update, the last residual stands
+              c.done = 1u;
+            } else {
+              c.blend = tot[0] / c.squared;
+              c.squared = tot[0];
+              c.length = tot[1];
+              c.taken += 1u;
+              c.done = (sqrt(c.length) <= c.target || c.taken >= s.step[b].limit) ? 1u : 0u;
+            }
+            s.cg[b] = c;
+            __threadfence();
+            if (c.done) atomicSub(&s.sync->active, 1);
+          }
         }
       }
+      j = jn;
+      done = doneNext;
+      strideNow = strideNext;
+      brokenNow = brokenNext;
     }
     if (!countBarrier(s.sync, bar)) return;
   }
@@ -565,6 +688,265 @@ __global__ void __launch_bounds__(TILE, 4)
       rep.iterations += c.taken;
       rep.capped += (c.taken == s.step[b].limit && residual > c.target) ? 1u : 0u;
       rep.applications += c.taken + (x0zero ? 0u : 1u);
+      rep.solves += 1u;
+      rep.tangent_iterations += tangent ? c.taken : 0u;
+      rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
+      if (rep.pass_solves == 0u) rep.pass_start = c.start_res;
+      rep.pass_end = c.rel_res;
+      rep.pass_iterations += c.taken;
+      rep.pass_solves += 1u;
+      s.cgrep[b] = rep;
+    }
+  }
+}
+
+// The batched PCG of kPcgBatchSell in kPcgSell's pipelined arrangement
+// (Ghysels-Vanroose): one grid barrier per iteration.  Each body keeps the
+// recurrences of kPcgSell, stored per node in S (x, r, u = P r, w = A u and
+// z, q, s, p), and m = P w is published for the next matvec n = A m, in two
+// buffers that alternate by phase.  Per phase, over the block's live tiles:
+//   n = A m; z = n + beta z, q = m + beta q, s = w + beta s, p = u + beta p,
+//   x += alpha p, r -= alpha s, u -= alpha q, w -= alpha z, m = P w;
+//   r.u, w.u, r.r per tile
+// and the last tile of each body to arrive sums the body's partials and takes
+// the next step of the body's control, as kPcgSell's loop top does: the
+// stopping test (|r| <= tolerance |rhs| or the cap), the breakdown test
+// (p.A p > 0 and r.u > 0), alpha and beta, and whether the next update is the
+// last one the cap allows (p, s, x and r only, no matvec).  A body's flags and
+// scalars (cg[b]: squared = gamma, stride = alpha, blend = beta, pad0 = the
+// kind of its next update, pad1 = operator applications, done = 1 + the phase
+// it stopped in) are read by its tiles after the barrier.
+//
+// The active count is read at the top of every phase by every block, while
+// last tiles of that same phase may already retire bodies, so it is kept in
+// two copies: phase k reads copy k & 1 and retires bodies from that copy
+// only; a body retired in phase k leaves copy (k + 1) & 1 in phase k + 1,
+// through the block that holds its first tile.
+constexpr uint32_t PIPE_FULL = 0u;  // kinds of a body's next update
+constexpr uint32_t PIPE_LAST = 1u;
+
+// kPcgSell's loop top for one body (thread 0 of its last tile): given the
+// sums gamma' = r.u, delta = w.u and |r|^2 of the current iterate, either stop
+// or set alpha, beta and the kind of the next update.
+__device__ __forceinline__ void pipeDecide(CgBodyDev& c, double gammaNext, double delta, uint32_t limit,
+                                           uint32_t phase) {
+  if (c.taken >= limit || sqrt(c.length) <= c.target) {
+    c.done = phase + 1u;
+    return;
+  }
+  const double b = c.taken ? gammaNext / c.squared : 0.0;
+  const double curvature = c.taken ? delta - b * gammaNext / c.stride : delta;  // p.A p
+  if (!(curvature > 0.0) || !(gammaNext > 0.0)) {
+    c.done = phase + 1u;
+    return;
+  }
+  c.blend = b;
+  c.stride = gammaNext / curvature;
+  c.squared = gammaNext;
+  c.pad0 = c.taken + 1u >= limit ? PIPE_LAST : PIPE_FULL;
+  if (c.pad0 == PIPE_FULL) c.pad1 += 1u;  // the matvec n = A m of the update
+}
+
+template <class S>
+__global__ void __launch_bounds__(TILE, 4)
+    kPcgBatchSellPipe(Sys<S> s, SellDev<S> g, Vec4<S>* X, Vec4<S>* zbuf, Vec4<S>* qbuf, uint32_t pass,
+                      uint32_t x0zero, uint32_t tangent) {
+  extern __shared__ uint32_t tlBatchSlots[];  // [slots] body (~0u: not stepping), then [slots] rows
+  const uint32_t G = gridDim.x, lane = threadIdx.x & 31u;
+  g.col_cache = 0;
+  unsigned int bar = 0;
+  const uint32_t slots = blockIdx.x < s.node_tiles ? (s.node_tiles - 1u - blockIdx.x) / G + 1u : 0u;
+  uint32_t* const slotBody = tlBatchSlots;
+  uint32_t* const slotRows = tlBatchSlots + slots;  // rows, | 0x80000000 on the first tile of its body
+  for (uint32_t j = threadIdx.x; j < slots; j += TILE) {
+    const uint32_t tile = blockIdx.x + j * G;
+    const uint32_t b = s.node_tile_body[tile];
+    const bool live = bodyActive(s, b, pass);
+    slotBody[j] = live ? b : ~0u;
+    const BodyDev bd = s.body[b];
+    slotRows[j] = live ? (min(TILE, bd.node_end - tile * TILE) | (tile == bd.node_tile_begin ? 0x80000000u : 0u)) : 0u;
+  }
+  __syncthreads();
+  Vec4<S>* const vecA = g.vec;             // m of even phases (and of phase 0)
+  Vec4<S>* const vecB = g.vec + g.stride;  // u of the start, then m of odd phases
+  Vec4<S>* const u = s.z;
+  Vec4<S>* const w = s.w;
+  Vec4<S>* const sv = s.ap;
+  Vec4<S>* const p = s.p;
+  const Vec4<S> zero4 = {S(0), S(0), S(0), S(0)};
+  const auto precondition = [&](uint32_t n, V3<double> v) {
+    const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
+    const Sym<double> P = {double(q0.x), double(q0.y), double(q0.z), double(q0.w), double(q1.x), double(q1.y)};
+    return roundTo<S>(symMul(P, v));
+  };
+  // ---- start: r = right - A x (anchored rows 0), u = P r published; the recurrences start at 0
+  for (uint32_t j = nextSlot(slotBody, 0u, slots); j < slots; j = nextSlot(slotBody, j + 1u, slots)) {
+    const uint32_t tile = blockIdx.x + j * G;
+    const uint32_t n = tile * TILE + threadIdx.x;
+    if (threadIdx.x >= (slotRows[j] & 0x7fffffffu)) continue;
+    V3<double> r = {0, 0, 0};
+    if (!s.anch[n]) {
+      V3<double> ax = {0, 0, 0};
+      if (!x0zero)
+        ax = sellRowOf<S, decltype(ld4cgOf(X)), 2u>(g, n >> 5, lane, ld4cgOf(X), static_cast<const uint32_t*>(nullptr));
+      r = cvt<double>(xyz(s.right[n])) - ax;
+    }
+    const V3<double> uu = precondition(n, r);
+    s.r[n] = pack(cvt<S>(r));
+    u[n] = pack(cvt<S>(uu));
+    vecB[n] = pack(cvt<S>(uu));
+    if (x0zero) X[n] = zero4;
+    zbuf[n] = zero4;
+    qbuf[n] = zero4;
+    sv[n] = zero4;
+    p[n] = zero4;
+  }
+  if (!countBarrier(s.sync, bar)) return;
+  // ---- phase 0: w = A u, m = P w published; r.u, w.u, r.r, rhs.rhs per body -> the first decision
+  for (uint32_t j = nextSlot(slotBody, 0u, slots); j < slots; j = nextSlot(slotBody, j + 1u, slots)) {
+    const uint32_t b = slotBody[j], tile = blockIdx.x + j * G;
+    const uint32_t n = tile * TILE + threadIdx.x;
+    double sums[4] = {0.0, 0.0, 0.0, 0.0};
+    if (threadIdx.x < (slotRows[j] & 0x7fffffffu)) {
+      V3<double> ww = {0, 0, 0};
+      if (!s.anch[n])
+        ww = sellRowOf<S, decltype(ld4cgOf(vecB)), 2u>(g, n >> 5, lane, ld4cgOf(vecB), static_cast<const uint32_t*>(nullptr));
+      const V3<double> m = precondition(n, ww);
+      w[n] = pack(cvt<S>(ww));
+      vecA[n] = pack(cvt<S>(m));
+      const V3<double> r = cvt<double>(xyz(s.r[n])), uu = cvt<double>(xyz(u[n]));
+      const V3<double> wr = cvt<double>(cvt<S>(ww));
+      const V3<double> rhs = cvt<double>(xyz(s.right[n]));
+      sums[0] = dot(r, uu);
+      sums[1] = dot(wr, uu);
+      sums[2] = dot(r, r);
+      sums[3] = dot(rhs, rhs);
+    }
+    blockSum<4>(sums);
+    if (threadIdx.x == 0) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) s.part[size_t(tile) * 4 + k] = sums[k];
+    }
+    const BodyDev bd = s.body[b];
+    if (lastTileOfBody(&s.counter[b], bd.node_tile_end - bd.node_tile_begin)) {
+      double tot[4];
+      sumTiles<4>(s.part, bd.node_tile_begin, bd.node_tile_end, tot);
+      if (threadIdx.x == 0) {
+        CgBodyDev c;
+        const double reference = sqrt(tot[3]);
+        c.floor = fmax(reference, 1.1754943508222875e-38);  // std::numeric_limits<float>::min()
+        c.target = s.step[b].tolerance * c.floor;
+        c.length = tot[2];
+        c.start_res = sqrt(tot[2]) / c.floor;
+        c.rel_res = c.start_res;
+        c.squared = 0.0;
+        c.stride = 0.0;
+        c.blend = 0.0;
+        c.taken = 0;
+        c.done = 0;
+        c.pad0 = PIPE_FULL;
+        c.pad1 = (x0zero ? 0u : 1u) + 1u;  // r = right - A x and w = A u
+        pipeDecide(c, tot[0], tot[1], s.step[b].limit, 0u);
+        s.cg[b] = c;
+        __threadfence();
+        if (c.done) atomicSub(&s.sync->active, 1);
+      }
+    }
+  }
+  if (!countBarrier(s.sync, bar)) return;
+  for (uint32_t phase = 1;; ++phase) {
+    // the count of phase - 1's copy: retirements of this phase go to the other copy
+    if (*(volatile int*)(((phase - 1u) & 1u) ? &s.sync->active_odd : &s.sync->active) <= 0) break;
+    int* const retire = (phase & 1u) ? &s.sync->active_odd : &s.sync->active;
+    const Vec4<S>* const mcur = (phase & 1u) ? vecA : vecB;
+    Vec4<S>* const mnext = (phase & 1u) ? vecB : vecA;
+    uint32_t j = nextSlot(slotBody, 0u, slots);
+    CgBodyDev cNow = {};
+    if (j < slots) cNow = loadCg(&s.cg[slotBody[j]]);
+    while (j < slots) {
+      const uint32_t b = slotBody[j], tile = blockIdx.x + j * G, rowsWord = slotRows[j];
+      const uint32_t jn = nextSlot(slotBody, j + 1u, slots);
+      CgBodyDev cNext = {};
+      if (jn < slots) cNext = loadCg(&s.cg[slotBody[jn]]);
+      if (cNow.done) {
+        // retired in the previous phase: leave this phase's copy of the count too
+        if (cNow.done == phase && (rowsWord & 0x80000000u) && threadIdx.x == 0) atomicSub(retire, 1);
+      } else {
+        const uint32_t n = tile * TILE + threadIdx.x;
+        const double alpha = cNow.stride, beta = cNow.blend;
+        double sums[3] = {0.0, 0.0, 0.0};
+        if (threadIdx.x < (rowsWord & 0x7fffffffu)) {
+          const bool full = cNow.pad0 == PIPE_FULL;
+          // the matvec first: its round trips are the phase's latency
+          V3<double> nn = {0, 0, 0};
+          if (full && !s.anch[n])
+            nn = sellRowOf<S, decltype(ld4cgOf(mcur)), 2u>(g, n >> 5, lane, ld4cgOf(mcur),
+                                                          static_cast<const uint32_t*>(nullptr));
+          const V3<double> uu = cvt<double>(xyz(u[n])), ww = cvt<double>(xyz(w[n]));
+          const V3<double> pp = cvt<double>(cvt<S>(uu + beta * cvt<double>(xyz(p[n]))));
+          const V3<double> ss = cvt<double>(cvt<S>(ww + beta * cvt<double>(xyz(sv[n]))));
+          const V3<double> x = cvt<double>(xyz(X[n])) + alpha * pp;
+          const V3<double> r = cvt<double>(cvt<S>(cvt<double>(xyz(s.r[n])) - alpha * ss));
+          p[n] = pack(cvt<S>(pp));
+          sv[n] = pack(cvt<S>(ss));
+          X[n] = pack(cvt<S>(x));
+          s.r[n] = pack(cvt<S>(r));
+          if (full) {
+            const V3<double> m = cvt<double>(xyz(ld4cg(&mcur[n])));
+            const V3<double> zz = cvt<double>(cvt<S>(nn + beta * cvt<double>(xyz(zbuf[n]))));
+            const V3<double> qq = cvt<double>(cvt<S>(m + beta * cvt<double>(xyz(qbuf[n]))));
+            const V3<double> u2 = cvt<double>(cvt<S>(uu - alpha * qq));
+            const V3<double> w2 = cvt<double>(cvt<S>(ww - alpha * zz));
+            zbuf[n] = pack(cvt<S>(zz));
+            qbuf[n] = pack(cvt<S>(qq));
+            u[n] = pack(cvt<S>(u2));
+            w[n] = pack(cvt<S>(w2));
+            mnext[n] = pack(cvt<S>(precondition(n, w2)));
+            sums[0] = dot(r, u2);
+            sums[1] = dot(w2, u2);
+          }
+          sums[2] = dot(r, r);
+        }
+        blockSum<3>(sums);
+        if (threadIdx.x == 0) {
+#pragma unroll
+          for (int k = 0; k < 3; ++k) s.part[size_t(tile) * 4 + k] = sums[k];
+        }
+        const BodyDev bd = s.body[b];
+        if (lastTileOfBody(&s.counter[b], bd.node_tile_end - bd.node_tile_begin)) {
+          double tot[3];
+          sumTiles<3>(s.part, bd.node_tile_begin, bd.node_tile_end, tot);
+          if (threadIdx.x == 0) {
+            CgBodyDev c = loadCg(&s.cg[b]);
+            c.length = tot[2];
+            c.taken += 1u;
+            if (c.pad0 == PIPE_LAST)
+              c.done = phase + 1u;
+            else
+              pipeDecide(c, tot[0], tot[1], s.step[b].limit, phase);
+            s.cg[b] = c;
+            __threadfence();
+            if (c.done) atomicSub(retire, 1);
+          }
+        }
+      }
+      j = jn;
+      cNow = cNext;
+    }
+    if (!countBarrier(s.sync, bar)) return;
+  }
+  if (blockIdx.x == 0) {
+    for (uint32_t b = threadIdx.x; b < s.bodies; b += TILE) {
+      if (!bodyActive(s, b, pass)) continue;
+      CgBodyDev c = loadCg(&s.cg[b]);
+      const double residual = sqrt(c.length);
+      c.rel_res = residual / c.floor;
+      s.cg[b].rel_res = c.rel_res;
+      s.cg[b].done = 1u;
+      CgReportDev rep = s.cgrep[b];
+      rep.iterations += c.taken;
+      rep.capped += (c.taken == s.step[b].limit && residual > c.target) ? 1u : 0u;
+      rep.applications += c.pad1;
       rep.solves += 1u;
       rep.tangent_iterations += tangent ? c.taken : 0u;
       rep.worst_rel = fmax(rep.worst_rel, c.rel_res);

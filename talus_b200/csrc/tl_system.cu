@@ -317,8 +317,9 @@ struct System final : SystemBase {
   // assembled block matrix of the single-body PCG (tl_sell.cuh)
   bool sellReady = false;
   uint32_t sellRows = 0, sellSlices = 0, sellPositions = 0, sellStride = 0;
-  int sellPerSm = 0, batchSellPerSm = 0;
-  DevBuf<Vec4<S>> sellP2;  // kPcgBatchSell's second search-direction buffer
+  int sellPerSm = 0, batchSellPerSm = 0, batchPipePerSm = 0;
+  DevBuf<Vec4<S>> sellP2;  // kPcgBatchSell's second search-direction buffer; z of kPcgBatchSellPipe
+  DevBuf<Vec4<S>> sellQ;   // q of kPcgBatchSellPipe
   DevBuf<uint32_t> sellSliceStart, sellGroupSlice, sellCol, sellCstart, sellCentry, sellUpper, sellMirror, sellDiag;
   uint32_t sellUpperCount = 0, sellColCache = 0;
   static constexpr uint32_t SELL_COL_CACHE_MAX = 32;  // column slots per thread in kPcgSell's shared memory
@@ -825,10 +826,19 @@ struct System final : SystemBase {
     sellP2.alloc(Vp);
     sellP2.zero(st);
     TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&batchSellPerSm, (const void*)kPcgBatchSell<S>, TILE, 0));
+    if (batchSellPerSm > 0) {
+      sellQ.alloc(Vp);
+      sellQ.zero(st);
+      TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&batchPipePerSm, (const void*)kPcgBatchSellPipe<S>, TILE, 0));
+      if (batchPipePerSm < 1) throw StatusError{TL_ERR_CUDA, "the pipelined batched PCG cannot be resident"};
+    }
     TL_CUDA(cudaStreamSynchronize(st));
     sellReady = sellPerSm > 0 || batchSellPerSm > 0;
   }
-  size_t sellColBytes() const { return size_t(sellColCache) * TILE * sizeof(uint32_t); }
+  // kPcgSell's dynamic shared memory: the column cache, then the gather stage
+  size_t sellColBytes() const {
+    return size_t(sellColCache) * TILE * sizeof(uint32_t) + size_t(sellGatherSlots<S>()) * TILE * sizeof(Vec4<S>);
+  }
   void assembleSell(const Sys<S>& s, const SellDev<S>& g, unsigned blocks, int idx, bool damp, bool tangent,
                     uint32_t pass) {
     if (idx) {
@@ -870,7 +880,8 @@ struct System final : SystemBase {
   // 3,072 tets, even at 24,576, assembled 1.6x faster at 393,216).
   bool assembledForm() const {
     if (!sellReady || solverForm == TL_SOLVER_ELEMENTWISE) return false;
-    return B > 1 || solverForm == TL_SOLVER_ASSEMBLED || bodyHost[0].elem_end >= SELL_AUTO_MIN_TETS;
+    return B > 1 || solverForm == TL_SOLVER_ASSEMBLED || solverForm == TL_SOLVER_ASSEMBLED_TWO_PHASE ||
+           solverForm == TL_SOLVER_ASSEMBLED_PIPELINED || bodyHost[0].elem_end >= SELL_AUTO_MIN_TETS;
   }
   int sellGrid() const {
     if (B != 1 || sellPerSm < 1 || !assembledForm()) return 0;
@@ -1271,9 +1282,26 @@ struct System final : SystemBase {
         mark(2, true);
       }
       Vec4<S>* p2 = sellP2.ptr;
-      void* args[] = {&s, &g, &X, &p2, &ps, &xz, &tg};
-      const int grid = std::max(1, std::min(batchSellPerSm * ctx->sms, int(nodeTiles)));
-      TL_CUDA(cudaLaunchCooperativeKernel((const void*)kPcgBatchSell<S>, dim3(grid), dim3(TILE), args, 0, st));
+      Vec4<S>* q = sellQ.ptr;
+      // the batch's order: measured on 512 uneven bodies solved to 1e-6, the pipelined
+      // order is the faster in FP64 and the two-phase one in FP32-mixed, whose FP32
+      // storage of the pipelined recurrences also drifts (more iterations, and a body
+      // that diverged); TL_SOLVER_ASSEMBLED_PIPELINED is refused for FP32 systems
+      const bool twoPhase = solverForm == TL_SOLVER_ASSEMBLED_TWO_PHASE ||
+                            (solverForm != TL_SOLVER_ASSEMBLED_PIPELINED && sizeof(S) == 4);
+      const int perSm = twoPhase ? batchSellPerSm : batchPipePerSm;
+      const int grid = std::max(1, std::min(perSm * ctx->sms, int(nodeTiles)));
+      // the block's slot table: body and row count of each of its tiles
+      const size_t slotBytes = size_t(2) * sizeof(uint32_t) * ((nodeTiles + grid - 1) / grid);
+      if (slotBytes > 48 * 1024) throw StatusError{TL_ERR_UNSUPPORTED, "too many node tiles for the batched PCG grid"};
+      if (twoPhase) {
+        void* args[] = {&s, &g, &X, &p2, &ps, &xz, &tg};
+        TL_CUDA(cudaLaunchCooperativeKernel((const void*)kPcgBatchSell<S>, dim3(grid), dim3(TILE), args, slotBytes, st));
+      } else {
+        void* args[] = {&s, &g, &X, &p2, &q, &ps, &xz, &tg};
+        TL_CUDA(cudaLaunchCooperativeKernel((const void*)kPcgBatchSellPipe<S>, dim3(grid), dim3(TILE), args, slotBytes,
+                                            st));
+      }
     } else {  // batch: two-level assembly, per-body scalars
       if (profiling) mark(2, true);
       void* args[] = {&s, &X, &ps, &xz};
@@ -1391,6 +1419,7 @@ struct System final : SystemBase {
     }
     kInversionCheck<S><<<elemTiles, TILE, 0, st>>>(view());
     check();
+    ++launches;
     BodyAccDev* ha = hAcc.get(B);
     acc.download(ha, B, st);
     TL_CUDA(cudaStreamSynchronize(st));
@@ -1520,7 +1549,10 @@ struct System final : SystemBase {
   DevBuf<BodyStepDev> dStepVar;
   PinnedBuf<BodyStepDev> hStepVar, hStepOut;
 
-  void enqueueStep(int law, uint32_t passes, bool yieldsLaw, bool anyFloating) {
+  // The step's opening, launched directly: the constants, the accumulators,
+  // the predictor-inversion test and each body's substep choice, whose
+  // largest count is read back to pick the graph.
+  uint32_t openStep() {
     TL_CUDA(cudaMemcpyAsync(dStepVar.ptr, hStepVar.ptr, sizeof(BodyStepDev) * 2 * B, cudaMemcpyHostToDevice, st));
     const uint32_t bb = (B + 255) / 256;
     TL_CUDA(cudaMemsetAsync(&sync.ptr->error, 0, sizeof(int), st));
@@ -1529,6 +1561,15 @@ struct System final : SystemBase {
     kInversionCheck<S><<<elemTiles, TILE, 0, st>>>(view());
     kStepSelect<<<bb, 256, 0, st>>>(dStep.ptr, dStepVar.ptr, acc.ptr, B, 1u);
     TL_CUDA(cudaGetLastError());
+    dStep.download(hStepOut.ptr, B, st);
+    TL_CUDA(cudaStreamSynchronize(st));
+    uint32_t passes = 1;
+    for (uint32_t b = 0; b < B; ++b) passes = std::max(passes, hStepOut.ptr[b].substeps);
+    return passes;
+  }
+  // The captured part: `passes` substeps (bodies with fewer are masked off in
+  // the later ones), the step's end and the downloads of its results.
+  void enqueueStep(int law, uint32_t passes, bool yieldsLaw, bool anyFloating) {
     for (uint32_t pass = 0; pass < passes; ++pass) {
       if (anyFloating) frameBegin(pass);
       nodeOp(kPredict<S>, pass);
@@ -1553,7 +1594,6 @@ struct System final : SystemBase {
   int32_t stepGraph(const tl_settings& set, const double gvec[3], double dt, tl_step_report* reports, int law,
                     bool yieldsLaw, bool anyFloating) {
     const uint32_t configured = std::max(set.substeps, 1u);
-    const uint32_t passes = std::max(configured, INVERTED_SUBSTEPS);
     const Rule rule = ruleOf(set.spectral_radius);
     if (!dStepVar.ptr) dStepVar.alloc(size_t(2) * B);
     BodyStepDev* hv = hStepVar.get(size_t(2) * B);
@@ -1587,8 +1627,16 @@ struct System final : SystemBase {
         s.hstep = std::sqrt((1.0 - rule.alphaForce) * rule.beta) * s.inner;
         s.scale = s.hstep * s.hstep;
       }
+    cudaEvent_t e0, e1;
+    TL_CUDA(cudaEventCreate(&e0));
+    TL_CUDA(cudaEventCreate(&e1));
+    TL_CUDA(cudaEventRecord(e0, st));
+    const uint32_t passes = openStep();
+    // one graph per substep count (the configured count, or the inverted
+    // predictor's four), so a step replays exactly the passes it takes
     const uint64_t key = (uint64_t(law) << 48) | (uint64_t(yieldsLaw) << 40) | (uint64_t(anyFloating) << 38) |
-                         (uint64_t(profiling) << 36) | (uint64_t(configured) << 8) | uint64_t(tuneBlocksPerSm & 0xffu);
+                         (uint64_t(profiling) << 36) | (uint64_t(passes) << 24) | (uint64_t(configured) << 8) |
+                         uint64_t(tuneBlocksPerSm & 0xffu);
     if (!graphExec || graphKey != key) {
       if (graphExec) cudaGraphExecDestroy(graphExec);
       graphExec = nullptr;
@@ -1605,6 +1653,8 @@ struct System final : SystemBase {
         if (graph) cudaGraphDestroy(graph);
         cudaGetLastError();
         graphBroken = true;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
         return TL_ERR_UNSUPPORTED;
       }
       capturing = false;
@@ -1615,6 +1665,8 @@ struct System final : SystemBase {
         cudaGetLastError();
         graphExec = nullptr;
         graphBroken = true;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
         return TL_ERR_UNSUPPORTED;
       }
       cudaGraphDestroy(graph);
@@ -1622,10 +1674,6 @@ struct System final : SystemBase {
       graphLaunches = launches;
       graphEv = evUsed;
     }
-    cudaEvent_t e0, e1;
-    TL_CUDA(cudaEventCreate(&e0));
-    TL_CUDA(cudaEventCreate(&e1));
-    TL_CUDA(cudaEventRecord(e0, st));
     TL_CUDA(cudaGraphLaunch(graphExec, st));
     TL_CUDA(cudaEventRecord(e1, st));
     TL_CUDA(cudaStreamSynchronize(st));
@@ -1672,14 +1720,19 @@ struct System final : SystemBase {
       r.kinetic_energy += hAcc.ptr[b].kinetic;
       r.min_volume_ratio = fromMinKey(hAcc.ptr[b].min_j_key);
       r.device_seconds += double(ms) * 1e-3;
-      r.kernel_launches += graphLaunches;
+      r.kernel_launches += graphLaunches + OPEN_LAUNCHES;
     }
     return status;
   }
   uint32_t graphLaunches = 0;
+  static constexpr uint32_t OPEN_LAUNCHES = 4;  // openStep's kernels
   std::vector<std::pair<int, size_t>> graphEv;  // event pairs recorded by the captured graph
 
-  void setSolver(uint32_t form) override { solverForm = form; }
+  void setSolver(uint32_t form) override {
+    if (form == TL_SOLVER_ASSEMBLED_PIPELINED && sizeof(S) == 4)
+      throw StatusError{TL_ERR_UNSUPPORTED, "the pipelined batched PCG keeps its recurrences in S: FP64 only"};
+    solverForm = form;
+  }
   void expireWait(int32_t solve) override { expireSolve = solve; }
   void setFlowLimits(uint32_t b, uint32_t lane, double crushStress, double crushLimit, double plasticMax) override {
     if (b >= B || lane >= hb[b].lanes) throw StatusError{TL_ERR_ARG, "no such body or material lane"};
@@ -2650,9 +2703,11 @@ int32_t tl_system_expire_wait(tl_system* system, int32_t solve) {
 }
 
 int32_t tl_system_set_solver(tl_system* system, uint32_t form) {
-  if (!system || form > TL_SOLVER_ELEMENTWISE) return TL_ERR_ARG;
-  system->impl->setSolver(form);
-  return TL_OK;
+  if (!system || form > TL_SOLVER_ASSEMBLED_PIPELINED) return TL_ERR_ARG;
+  return guarded(system->ctx, [&]() -> int32_t {
+    system->impl->setSolver(form);
+    return TL_OK;
+  });
 }
 
 int32_t tl_system_set_plasticity(tl_system* system, uint32_t mode) {

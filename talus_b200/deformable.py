@@ -262,10 +262,14 @@ class System:
         check(capi.lib().tl_system_tune(self.handle, int(pcg_blocks_per_sm), 1 if graph else 0), self.context.handle)
 
     def set_solver(self, form: str = "auto"):
-        """PCG operator form of a single-body system (tl_system_set_solver):
-        "auto", "assembled" (3x3 node blocks assembled once per solve) or
+        """PCG operator form of a system (tl_system_set_solver): "auto",
+        "assembled" (3x3 node blocks assembled once per solve),
+        "assembled-two-phase" / "assembled-pipelined" (the same matrix, a batch
+        iterating with two grid barriers per iteration or, FP64 only, one) or
         "elementwise" (applied element by element every iteration)."""
         code = {"auto": capi.TL_SOLVER_AUTO, "assembled": capi.TL_SOLVER_ASSEMBLED,
+                "assembled-two-phase": capi.TL_SOLVER_ASSEMBLED_TWO_PHASE,
+                "assembled-pipelined": capi.TL_SOLVER_ASSEMBLED_PIPELINED,
                 "elementwise": capi.TL_SOLVER_ELEMENTWISE}[form]
         check(capi.lib().tl_system_set_solver(self.handle, code), self.context.handle)
 

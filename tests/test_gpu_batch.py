@@ -50,6 +50,69 @@ def test_batched_bodies_match_single_body_systems(law, precision, tol):
         assert np.linalg.norm(x - ref, axis=1).max() <= tol * scale, i
 
 
+def run_batch_form(meshes, mats, precision, form, settings, steps):
+    s = tb.System(meshes, mats, precision)
+    s.set_solver(form)
+    for i, m in enumerate(meshes):
+        s.set_state(tb.rest_state(m), i)
+    counts = []
+    for _ in range(steps):
+        counts.append([r.cg_iterations for r in s.step(settings, GRAVITY, DT)])
+    states = [s.get_state(i).position for i in range(len(meshes))]
+    s.close()
+    return states, counts
+
+
+@pytest.mark.parametrize("law", [tb.COROTATED, tb.NEO_HOOKEAN])
+def test_pipelined_batched_pcg_equals_the_two_phase_order(law):
+    """The batched PCG on the assembled matrix in the pipelined arrangement
+    (one grid barrier per iteration, kPcgBatchSellPipe) and in the textbook
+    order (two barriers, kPcgBatchSell) take the same iterates in exact
+    arithmetic.  FP64, a ragged batch solved to 1e-4 (past the default cap of
+    64): the same iteration counts and positions within 1e-10."""
+    meshes, mats = tb.mesh.batch_bodies(count=7, seed=19, lo=3, hi=7)
+    settings = tb.Settings(law=law, tolerance=1e-4, cg_iterations=2000)
+    piped, piped_counts = run_batch_form(meshes, mats, tb.FP64, "assembled-pipelined", settings, 5)
+    split, split_counts = run_batch_form(meshes, mats, tb.FP64, "assembled-two-phase", settings, 5)
+    assert piped_counts == split_counts
+    assert max(max(c) for c in piped_counts) > 64
+    for i, m in enumerate(meshes):
+        scale = np.linalg.norm(split[i] - m.rest_positions, axis=1).max()
+        assert np.linalg.norm(piped[i] - split[i], axis=1).max() <= 1e-10 * scale, i
+
+
+def test_pipelined_and_two_phase_orders_agree_at_a_tight_tolerance():
+    """Solved to 1e-8 the two orders' residual recurrences (rounded
+    differently) may cross the tolerance an iteration apart; the converged
+    positions agree to the tolerance."""
+    meshes, mats = tb.mesh.batch_bodies(count=7, seed=19, lo=3, hi=7)
+    settings = tb.Settings(tolerance=1e-8, cg_iterations=4000)
+    piped, piped_counts = run_batch_form(meshes, mats, tb.FP64, "assembled-pipelined", settings, 4)
+    split, split_counts = run_batch_form(meshes, mats, tb.FP64, "assembled-two-phase", settings, 4)
+    for a, b in zip(piped_counts, split_counts):
+        assert max(abs(x - y) for x, y in zip(a, b)) <= 2
+    for i, m in enumerate(meshes):
+        scale = np.linalg.norm(split[i] - m.rest_positions, axis=1).max()
+        assert np.linalg.norm(piped[i] - split[i], axis=1).max() <= 1e-7 * scale, i
+
+
+def test_fp32_mixed_batch_follows_the_fp64_batch_at_a_converged_tolerance():
+    """The FP32-mixed batch (two-phase order) against the FP64 batch
+    (pipelined order), both solved to 1e-6 on soft bodies that move by
+    millimetres or more: within 1e-5 of the displacement, no solve at the cap."""
+    meshes, _ = tb.mesh.batch_bodies(count=7, seed=23, lo=3, hi=7)
+    mats = [[tb.PhysicalMaterial(density=1000.0, youngs_modulus=e, poissons_ratio=0.3)]
+            for e in (2e4, 5e4, 1e5, 3e4, 8e4, 4e4, 6e4)]
+    settings = tb.Settings(tolerance=1e-6, cg_iterations=4000)
+    ref, _ = run_batch_form(meshes, mats, tb.FP64, "assembled", settings, 5)
+    got, counts = run_batch_form(meshes, mats, tb.FP32_MIXED, "assembled", settings, 5)
+    assert max(max(c) for c in counts) < 4000
+    for i, m in enumerate(meshes):
+        scale = np.linalg.norm(ref[i] - m.rest_positions, axis=1).max()
+        assert scale > 1e-3
+        assert np.linalg.norm(got[i] - ref[i], axis=1).max() <= 1e-5 * scale, i
+
+
 @pytest.mark.parametrize("precision", [tb.FP64, tb.FP32_MIXED])
 def test_graph_replayed_batch_equals_launched_batch(precision):
     """A batched elastic step replayed from a CUDA graph (device-side substep

@@ -98,8 +98,20 @@ def test_unknown_form_is_rejected():
     mesh, mat = elastic_block((3, 3, 3))
     s = tb.System(mesh, [mat], tb.FP64)
     with pytest.raises(tb._capi.TalusError) as e:
-        tb._capi.check(tb._capi.lib().tl_system_set_solver(s.handle, 3), s.context.handle)
+        tb._capi.check(tb._capi.lib().tl_system_set_solver(s.handle, 5), s.context.handle)
     assert e.value.status == tb._capi.TL_ERR_ARG
+    s.close()
+
+
+def test_pipelined_batch_order_is_refused_in_fp32():
+    """The pipelined batched order keeps its recurrences in the system's
+    precision; in FP32 they drift, so an FP32-mixed system refuses it."""
+    mesh, mat = elastic_block((3, 3, 3))
+    s = tb.System(mesh, [mat], tb.FP32_MIXED)
+    with pytest.raises(tb._capi.TalusError) as e:
+        s.set_solver("assembled-pipelined")
+    assert e.value.status == tb._capi.TL_ERR_UNSUPPORTED
+    s.set_solver("assembled-two-phase")
     s.close()
 
 
