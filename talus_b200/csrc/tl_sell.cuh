@@ -177,33 +177,50 @@ __device__ __forceinline__ void sellSlot(const SellDev<S>& g, uint32_t p, uint32
 
 // y = A in for the thread's row.  Column slots are taken U at a time (4 in
 // FP32, 2 in FP64): their input values and block entries are requested
-// together, with the next group's column indices, so a group costs one
-// round trip to memory; the FMAs run slot by slot in order.
-template <class S, class In, uint32_t U = sizeof(S) == 4 ? 4u : 2u>
+// together; the FMAs run slot by slot in order.  With PREFETCH (columns read
+// from global memory, as in the batched kernels) the next group's column
+// indices are requested with this group's inputs, so a group costs one round
+// trip instead of two; kPcgSell reads its columns from shared memory and
+// goes without (the extra registers made it slower).
+template <class S, class In, uint32_t U = sizeof(S) == 4 ? 4u : 2u, bool PREFETCH = true>
 __device__ __forceinline__ V3<double> sellRowOf(const SellDev<S>& g, uint32_t slice, uint32_t lane, In in,
                                                 const uint32_t* cols) {
   V3<double> acc = {0, 0, 0};
   const uint32_t p1 = __ldg(&g.slice_start[slice + 1]);
   uint32_t p = __ldg(&g.slice_start[slice]) + lane, k = 0;
-  uint32_t c[U];
-#pragma unroll
-  for (uint32_t i = 0; i < U; ++i)
-    c[i] = p + i * SELL_ROWS < p1 ? sellCol(cols, g.col_cache, k + i, g.col, p + i * SELL_ROWS) : 0u;
-  for (; p + (U - 1) * SELL_ROWS < p1; p += U * SELL_ROWS, k += U) {
-    Vec4<S> xin[U];
-#pragma unroll
-    for (uint32_t i = 0; i < U; ++i) xin[i] = in(c[i]);
-    const uint32_t pn = p + U * SELL_ROWS;
+  if constexpr (PREFETCH) {
+    uint32_t c[U];
 #pragma unroll
     for (uint32_t i = 0; i < U; ++i)
-      c[i] = pn + i * SELL_ROWS < p1 ? sellCol(cols, g.col_cache, k + U + i, g.col, pn + i * SELL_ROWS) : 0u;
+      c[i] = p + i * SELL_ROWS < p1 ? sellCol(cols, g.col_cache, k + i, g.col, p + i * SELL_ROWS) : 0u;
+    for (; p + (U - 1) * SELL_ROWS < p1; p += U * SELL_ROWS, k += U) {
+      Vec4<S> xin[U];
 #pragma unroll
-    for (uint32_t i = 0; i < U; ++i) sellSlot(g, p + i * SELL_ROWS, lane, xin[i], acc);
+      for (uint32_t i = 0; i < U; ++i) xin[i] = in(c[i]);
+      const uint32_t pn = p + U * SELL_ROWS;
+#pragma unroll
+      for (uint32_t i = 0; i < U; ++i)
+        c[i] = pn + i * SELL_ROWS < p1 ? sellCol(cols, g.col_cache, k + U + i, g.col, pn + i * SELL_ROWS) : 0u;
+#pragma unroll
+      for (uint32_t i = 0; i < U; ++i) sellSlot(g, p + i * SELL_ROWS, lane, xin[i], acc);
+    }
+    // fewer than U slots remain; their columns are in c already
+#pragma unroll
+    for (uint32_t i = 0; i + 1 < U; ++i)
+      if (p + i * SELL_ROWS < p1) sellSlot(g, p + i * SELL_ROWS, lane, in(c[i]), acc);
+  } else {
+    for (; p + (U - 1) * SELL_ROWS < p1; p += U * SELL_ROWS, k += U) {
+      uint32_t c[U];
+#pragma unroll
+      for (uint32_t i = 0; i < U; ++i) c[i] = sellCol(cols, g.col_cache, k + i, g.col, p + i * SELL_ROWS);
+      Vec4<S> xin[U];
+#pragma unroll
+      for (uint32_t i = 0; i < U; ++i) xin[i] = in(c[i]);
+#pragma unroll
+      for (uint32_t i = 0; i < U; ++i) sellSlot(g, p + i * SELL_ROWS, lane, xin[i], acc);
+    }
+    for (; p < p1; p += SELL_ROWS, ++k) sellSlot(g, p, lane, in(sellCol(cols, g.col_cache, k, g.col, p)), acc);
   }
-  // fewer than U slots remain; their columns are in c already
-#pragma unroll
-  for (uint32_t i = 0; i + 1 < U; ++i)
-    if (p + i * SELL_ROWS < p1) sellSlot(g, p + i * SELL_ROWS, lane, in(c[i]), acc);
   return acc;
 }
 // The matvec input read from a vector written during the launch (L2).
@@ -212,43 +229,11 @@ template <class S> struct Ld4cg {
   __device__ __forceinline__ Vec4<S> operator()(uint32_t c) const { return ld4cg(&v[c]); }
 };
 template <class S> __device__ __forceinline__ Ld4cg<S> ld4cgOf(const Vec4<S>* v) { return Ld4cg<S>{v}; }
+// kPcgSell's row: columns from its shared-memory cache, no prefetch.
 template <class S>
 __device__ __forceinline__ V3<double> sellRow(const SellDev<S>& g, uint32_t slice, uint32_t lane,
                                               const Vec4<S>* in, const uint32_t* cols) {
-  return sellRowOf(g, slice, lane, ld4cgOf(in), cols);
-}
-
-// y = A in for the thread's row, with the row's inputs gathered first: up to
-// sellGatherSlots column slots are requested at once by cp.async (16-byte
-// copies through L2, so values published by other blocks during the launch
-// are seen) into the thread's column of a shared stage, so the row waits one
-// round trip for all its inputs instead of one per group of slots.  Each
-// thread reads back only what it copied, so no block barrier is needed.  The
-// slots are summed in the order of sellRowOf, with the same result.
-template <class S> __host__ __device__ constexpr uint32_t sellGatherSlots() { return sizeof(S) == 4 ? 16u : 8u; }
-
-template <class S>
-__device__ __forceinline__ V3<double> sellRowStaged(const SellDev<S>& g, uint32_t slice, uint32_t lane,
-                                                    const Vec4<S>* in, const uint32_t* cols, Vec4<S>* stage) {
-  constexpr uint32_t GS = sellGatherSlots<S>();
-  V3<double> acc = {0, 0, 0};
-  const uint32_t p1 = __ldg(&g.slice_start[slice + 1]);
-  uint32_t p = __ldg(&g.slice_start[slice]) + lane, k = 0;
-  while (p < p1) {
-    uint32_t cnt = 0;
-    for (uint32_t q = p; q < p1 && cnt < GS; q += SELL_ROWS, ++cnt) {
-      const unsigned char* src =
-          reinterpret_cast<const unsigned char*>(in + sellCol(cols, g.col_cache, k + cnt, g.col, q));
-      unsigned char* dst = reinterpret_cast<unsigned char*>(&stage[cnt * TILE + threadIdx.x]);
-#pragma unroll
-      for (int h = 0; h < int(sizeof(Vec4<S>)) / 16; ++h) cpAsync<16>(dst + 16 * h, src + 16 * h);
-    }
-    cpAsyncCommit();
-    cpAsyncWaitAll();
-#pragma unroll 4
-    for (uint32_t i = 0; i < cnt; ++i, p += SELL_ROWS, ++k) sellSlot(g, p, lane, stage[i * TILE + threadIdx.x], acc);
-  }
-  return acc;
+  return sellRowOf<S, Ld4cg<S>, sizeof(S) == 4 ? 4u : 2u, false>(g, slice, lane, ld4cgOf(in), cols);
 }
 
 template <class S> __device__ __forceinline__ V3<double> roundTo(V3<double> v) {
@@ -283,8 +268,6 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
   const bool freeRow = live && !s.anch[row];
   const BodyStepDev st = s.step[0];
   extern __shared__ uint32_t tlCols[];  // [col_cache][TILE] the first columns of each thread's row
-  // then [sellGatherSlots][TILE] the matvec inputs of each thread's row
-  Vec4<S>* const stage = reinterpret_cast<Vec4<S>*>(tlCols + size_t(g.col_cache) * TILE);
   // the block partials of each iteration's reduction, fetched while the matvec's inputs are
   // (grids of up to SELL_PART_STAGE_BLOCKS blocks; larger ones read them from L2 after it)
   constexpr unsigned SELL_PART_STAGE_BLOCKS = 320;
@@ -317,7 +300,7 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
   uint32_t applications = 0;
   // ---- r = right - A x (anchored rows 0), u = P r, published to vec[1]
   if (!x0zero) {
-    const V3<double> ax = mine ? sellRowStaged(g, slice, lane, X, tlCols, stage) : V3<double>{0, 0, 0};
+    const V3<double> ax = mine ? sellRow(g, slice, lane, X, tlCols) : V3<double>{0, 0, 0};
     if (freeRow) r = rhs - ax;
     ++applications;
   } else if (freeRow) {
@@ -329,7 +312,7 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
   if (mine) vec1[row] = pack(cvt<S>(u));
   if (!countBarrier(s.sync, bar)) return;
   // ---- w = A u, m = P w published to vec[0], first reduction
-  V3<double> w = mine ? sellRowStaged(g, slice, lane, vec1, tlCols, stage) : V3<double>{0, 0, 0};
+  V3<double> w = mine ? sellRow(g, slice, lane, vec1, tlCols) : V3<double>{0, 0, 0};
   ++applications;
   V3<double> m = precondition(w);
   if (mine) vec0[row] = pack(cvt<S>(m));
@@ -343,7 +326,7 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
   if (!countBarrier(s.sync, bar)) return;
   // n = A m for the first iteration, requested before the block sums so that
   // their round trip overlaps it (unused if the solve stops here)
-  V3<double> n = mine ? sellRowStaged(g, slice, lane, vec0, tlCols, stage) : V3<double>{0, 0, 0};
+  V3<double> n = mine ? sellRow(g, slice, lane, vec0, tlCols) : V3<double>{0, 0, 0};
   double sums[4];
   sumBlocksAll<4>(halves[0], sums);
   ++reductions;
@@ -404,7 +387,7 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
     // n = A m for the next iteration (m just published to vec[(taken + 1) & 1]), with the
     // block partials requested first so that both round trips overlap
     if (stagedSums) requestBlockPartials(part, partStage, 3u);
-    n = mine ? sellRowStaged(g, slice, lane, (taken & 1u) ? vec0 : vec1, tlCols, stage) : V3<double>{0, 0, 0};
+    n = mine ? sellRow(g, slice, lane, (taken & 1u) ? vec0 : vec1, tlCols) : V3<double>{0, 0, 0};
     double d[3];
     if (stagedSums) {
       cpAsyncWaitAll();

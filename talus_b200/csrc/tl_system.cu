@@ -835,10 +835,7 @@ struct System final : SystemBase {
     TL_CUDA(cudaStreamSynchronize(st));
     sellReady = sellPerSm > 0 || batchSellPerSm > 0;
   }
-  // kPcgSell's dynamic shared memory: the column cache, then the gather stage
-  size_t sellColBytes() const {
-    return size_t(sellColCache) * TILE * sizeof(uint32_t) + size_t(sellGatherSlots<S>()) * TILE * sizeof(Vec4<S>);
-  }
+  size_t sellColBytes() const { return size_t(sellColCache) * TILE * sizeof(uint32_t); }
   void assembleSell(const Sys<S>& s, const SellDev<S>& g, unsigned blocks, int idx, bool damp, bool tangent,
                     uint32_t pass) {
     if (idx) {
