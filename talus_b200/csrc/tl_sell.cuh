@@ -55,9 +55,9 @@ template <class S> struct SellDev {
   const uint32_t* col;           // [positions] column node
   uint32_t upper_count;          // block positions with row < column
   uint32_t col_cache;            // column slots per thread kept in shared memory by kPcgSell
-  const uint32_t* upper;         // [upper_count] those positions
-  const uint32_t* mirror;        // [upper_count] position of the transposed block
-  const uint32_t* cstart;        // [positions + 1] contributor range of each position
+  // [upper_count] per block above the diagonal: (position, its transpose's position, first
+  // contributor, contributor count | row free << 8 | column free << 9 | body << 10)
+  const uint4* urec;
   const uint32_t* centry;        // (element << 4) | (row corner << 2) | column corner
   S* val;                        // [positions / 32][9][32]
   Vec4<S>* vec;                  // [2][stride] published matvec inputs
@@ -130,16 +130,18 @@ template <class S, int LAW, bool TANGENT, bool DAMP>
 __global__ void __launch_bounds__(TILE, 4) kSellAssemble(Sys<S> s, SellDev<S> g, uint32_t pass) {
   const uint32_t i = blockIdx.x * TILE + threadIdx.x;
   if (i >= g.upper_count) return;
-  const uint32_t pos = g.upper[i], mpos = g.mirror[i];
-  const uint32_t row = g.group_slice[pos >> 5] * SELL_ROWS + (pos & 31u), col = g.col[pos];
-  const uint32_t body = s.node_tile_body[row / TILE];  // a block's two nodes share a body
+  // one record holds what the block needs, so its first contributor's code is requested
+  // together with the body's step flags: two dependent loads before the element records
+  const uint4 rec = __ldg(&g.urec[i]);
+  const uint32_t pos = rec.x, mpos = rec.y, q0 = rec.z, count = rec.w & 0xffu;
+  const bool rowFree = ((rec.w >> 8) & 1u) != 0u, colFree = ((rec.w >> 9) & 1u) != 0u;
+  const uint32_t body = rec.w >> 10;  // a block's two nodes share a body
+  const uint32_t first = count ? __ldg(&g.centry[q0]) : 0u;
   if (!bodyActive(s, body, pass)) return;
-  const bool rowFree = !s.anch[row], colFree = !s.anch[col];
   double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (rowFree || colFree) {
-    const uint32_t q1 = g.cstart[pos + 1];
-    for (uint32_t q = g.cstart[pos]; q < q1; ++q) {
-      const uint32_t code = __ldg(&g.centry[q]);
+    for (uint32_t q = 0; q < count; ++q) {
+      const uint32_t code = q ? __ldg(&g.centry[q0 + q]) : first;
       addElementBlock<S, LAW, TANGENT, DAMP>(s, code >> 4, (code >> 2) & 3u, code & 3u, acc);
     }
   }

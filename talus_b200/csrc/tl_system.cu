@@ -320,7 +320,8 @@ struct System final : SystemBase {
   int sellPerSm = 0, batchSellPerSm = 0, batchPipePerSm = 0;
   DevBuf<Vec4<S>> sellP2;  // kPcgBatchSell's second search-direction buffer; z of kPcgBatchSellPipe
   DevBuf<Vec4<S>> sellQ;   // q of kPcgBatchSellPipe
-  DevBuf<uint32_t> sellSliceStart, sellGroupSlice, sellCol, sellCstart, sellCentry, sellUpper, sellMirror, sellDiag;
+  DevBuf<uint32_t> sellSliceStart, sellGroupSlice, sellCol, sellCentry, sellDiag;
+  DevBuf<uint4> sellUrec;  // kSellAssemble's per-block records
   uint32_t sellUpperCount = 0, sellColCache = 0;
   static constexpr uint32_t SELL_COL_CACHE_MAX = 32;  // column slots per thread in kPcgSell's shared memory
   static constexpr uint32_t SELL_AUTO_MIN_TETS = 32768;  // TL_SOLVER_AUTO: smallest body that is assembled
@@ -769,14 +770,15 @@ struct System final : SystemBase {
     subrec.alloc(size_t(B) * SUBSTEP_RECORDS);
     subrec.zero(st);
     buildTiles(hTet, hElemTileBody);
-    buildSell(hTet, hStart, hEntry);
+    buildSell(hTet, hStart, hEntry, hAnch, hNodeTileBody);
     TL_CUDA(cudaStreamSynchronize(st));
   }
 
   // Sliced-ELL block structure of the operator (tl_sell.cuh), built on the
   // host by buildSellHost (tl_sell_build.h).
   void buildSell(const std::vector<uint4>& hTet, const std::vector<uint32_t>& hStart,
-                 const std::vector<uint32_t>& hEntry) {
+                 const std::vector<uint32_t>& hEntry, const std::vector<uint8_t>& hAnch,
+                 const std::vector<uint32_t>& hNodeTileBody) {
     // one body: its nodes; a batch: every node slot (tile padding rows have
     // no elements and stay zero)
     const uint32_t rows = B == 1 ? bodyHost[0].node_end : Vp;
@@ -793,10 +795,19 @@ struct System final : SystemBase {
     std::vector<uint32_t>& mirror = h.mirror;
     sellUpperCount = uint32_t(upper.size());
     sellColCache = std::min(widest, SELL_COL_CACHE_MAX);
-    sellUpper.alloc(std::max<size_t>(upper.size(), 1));
-    sellUpper.upload(upper.data(), upper.size(), st);
-    sellMirror.alloc(std::max<size_t>(mirror.size(), 1));
-    sellMirror.upload(mirror.data(), mirror.size(), st);
+    // one record per block above the diagonal, in the order of `upper`: its position, its
+    // mirror's, its first contributor and (count | row free << 8 | column free << 9 | body << 10)
+    std::vector<uint4> urec(std::max<size_t>(upper.size(), 1), make_uint4(0u, 0u, 0u, 0u));
+    for (size_t i = 0; i < upper.size(); ++i) {
+      const uint32_t pos = upper[i];
+      const uint32_t row = groupSlice[pos >> 5] * SELL_ROWS + (pos & 31u), c = col[pos];
+      const uint32_t count = cstart[pos + 1] - cstart[pos], body = hNodeTileBody[row / TILE];
+      if (count > 0xffu || body >= (1u << 22)) return;  // no assembled operator for such meshes
+      urec[i] = make_uint4(pos, mirror[i], cstart[pos],
+                           count | (hAnch[row] ? 0u : 1u << 8) | (hAnch[c] ? 0u : 1u << 9) | (body << 10));
+    }
+    sellUrec.alloc(urec.size());
+    sellUrec.upload(urec.data(), urec.size(), st);
     sellDiag.alloc(std::max<size_t>(h.diag.size(), 1));
     sellDiag.upload(h.diag.data(), h.diag.size(), st);
     sellRows = rows;
@@ -809,8 +820,6 @@ struct System final : SystemBase {
     sellGroupSlice.upload(groupSlice.data(), groupSlice.size(), st);
     sellCol.alloc(col.size());
     sellCol.upload(col.data(), col.size(), st);
-    sellCstart.alloc(cstart.size());
-    sellCstart.upload(cstart.data(), cstart.size(), st);
     sellCentry.alloc(std::max<size_t>(centry.size(), 1));
     sellCentry.upload(centry.data(), centry.size(), st);
     sellVal.alloc(size_t(positions) * 9);
@@ -853,8 +862,7 @@ struct System final : SystemBase {
     SellDev<S> g;
     g.upper_count = sellUpperCount;
     g.col_cache = sellColCache;
-    g.upper = sellUpper.ptr;
-    g.mirror = sellMirror.ptr;
+    g.urec = sellUrec.ptr;
     g.rows = sellRows;
     g.slices = sellSlices;
     g.positions = sellPositions;
@@ -862,7 +870,6 @@ struct System final : SystemBase {
     g.slice_start = sellSliceStart.ptr;
     g.group_slice = sellGroupSlice.ptr;
     g.col = sellCol.ptr;
-    g.cstart = sellCstart.ptr;
     g.centry = sellCentry.ptr;
     g.val = sellVal.ptr;
     g.vec = sellVec.ptr;
