@@ -444,6 +444,7 @@ def run_ours(args, spec, rank, world, dist):
     if tune:
         system.set_solver(tune.get("solver", "auto"))
         system.tune(tune["pcg_blocks_per_sm"], tune["graph"])
+        system.tune_shape(tune.get("row_group", 0), tune.get("batch_blocks", 0))
     for i, m in enumerate(meshes):
         system.set_state(tb.rest_state(m), i)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{device}")  # > 126 MB L2
@@ -578,7 +579,8 @@ def run_ours(args, spec, rank, world, dist):
         config["cells"] = list(spec["cells"])
     if tune:
         config["tuning"] = {"solver": tune.get("solver", "auto"), "pcg_blocks_per_sm": tune["pcg_blocks_per_sm"],
-                            "graph": tune["graph"],
+                            "graph": tune["graph"], "row_group": tune.get("row_group", 0),
+                            "batch_blocks": tune.get("batch_blocks", 0),
                             "source": "talus_b200/tuning.json (talus_b200.autotune)"}
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -685,6 +687,7 @@ def run_fp64(meshes, mats, settings, args, flush, context):
     if tune:
         system.set_solver(tune.get("solver", "auto"))
         system.tune(tune["pcg_blocks_per_sm"], tune["graph"])
+        system.tune_shape(tune.get("row_group", 0), tune.get("batch_blocks", 0))
     for i, m in enumerate(meshes):
         system.set_state(tb.rest_state(m), i)
     for _ in range(args.warmup):
@@ -783,6 +786,7 @@ def batch_form(context, flush, warmup=2, steps=5, tolerance=1e-6, cap=4000):
         if tune:
             system.set_solver(tune.get("solver", "auto"))
             system.tune(tune["pcg_blocks_per_sm"], tune["graph"])
+            system.tune_shape(tune.get("row_group", 0), tune.get("batch_blocks", 0))
         for i, m in enumerate(meshes):
             system.set_state(tb.rest_state(m), i)
         for _ in range(warmup):

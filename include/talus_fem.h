@@ -185,6 +185,17 @@ int32_t tl_system_counts(const tl_system* system, uint32_t* bodies, uint64_t* no
  * capture its elastic step in a CUDA graph and replay it every step. */
 int32_t tl_system_tune(tl_system* system, uint32_t pcg_blocks_per_sm, uint32_t graph);
 
+/* Launch shape of the assembled-operator PCG, no reference counterpart
+ * (chosen by talus_b200/autotune.py); results are bitwise the same for every
+ * shape. TL_SHAPE_ROW_GROUP: column slots of a matrix row whose inputs and
+ * blocks are requested per round trip, 2 or 4 (0 = the default: 4 in FP32
+ * and 2 in FP64 for a single body, 2 for batches). TL_SHAPE_BATCH_BLOCKS:
+ * resident 256-thread blocks per SM the batched kernels are compiled for,
+ * 3 or 4 (0 = 4). Other values return TL_ERR_ARG. */
+#define TL_SHAPE_ROW_GROUP 0u
+#define TL_SHAPE_BATCH_BLOCKS 1u
+int32_t tl_system_tune_shape(tl_system* system, uint32_t knob, uint32_t value);
+
 /* Form of the PCG operator, no reference counterpart (the reference applies
  * it element by element, solver.cc:904-1048): TL_SOLVER_ASSEMBLED assembles
  * the 3x3 node blocks once per solve and iterates on that matrix (about 40

@@ -38,6 +38,8 @@ TL_SOLVER_ASSEMBLED = 1
 TL_SOLVER_ELEMENTWISE = 2
 TL_SOLVER_ASSEMBLED_TWO_PHASE = 3
 TL_SOLVER_ASSEMBLED_PIPELINED = 4
+TL_SHAPE_ROW_GROUP = 0
+TL_SHAPE_BATCH_BLOCKS = 1
 TL_PLASTICITY_SMALL_STRAIN = 0
 TL_PLASTICITY_HENCKY = 1
 
@@ -148,6 +150,7 @@ SIGNATURES = {
     "tl_step_substeps": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
                                      C.POINTER(C.c_uint32)]),
     "tl_system_tune": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32]),
+    "tl_system_tune_shape": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32]),
     "tl_system_set_solver": (C.c_int32, [C.c_void_p, C.c_uint32]),
     "tl_system_set_plasticity": (C.c_int32, [C.c_void_p, C.c_uint32]),
     "tl_ctx_check_wait_limit": (C.c_int32, [C.c_void_p]),

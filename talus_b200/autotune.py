@@ -10,6 +10,11 @@ through ``System.tune``:
   element-tile matvec.
 * ``graph``: whether a batched elastic step is replayed from one captured CUDA
   graph (device-side substep choice) or launched kernel by kernel.
+* ``row_group`` and ``batch_blocks`` (``System.tune_shape``), for the
+  assembled forms: how many column slots of a matrix row have their inputs
+  and blocks requested per round trip (2 or 4), and how many blocks per SM the
+  batched kernels are compiled for (3 registers-richer, or 4).  They change
+  only the launch shape; the results are bitwise the same.
 * ``solver``: the PCG operator form (``System.set_solver``): "auto" (the
   block matrix assembled once per solve, for these workloads), for a batch
   "assembled-two-phase" (two grid barriers per iteration, fewer bytes) and,
@@ -35,19 +40,24 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def candidates(bodies: int, fp64: bool):
+    """(solver, PCG blocks per SM, graph, row group, batch blocks per SM)."""
     graphs = [True, False] if bodies > 1 else [False]
-    out = [("elementwise", k, g) for k in (0, 1, 2, 3) for g in graphs]
-    forms = ["auto"]
-    if bodies > 1:
-        forms = ["assembled-two-phase", "assembled-pipelined"] if fp64 else ["assembled-two-phase"]
-    return out + [(form, 0, g) for form in forms for g in graphs]
+    out = [("elementwise", k, g, 0, 0) for k in (0, 1, 2, 3) for g in graphs]
+    if bodies == 1:
+        return out + [("auto", 0, False, rg, 0) for rg in (2, 4)]
+    forms = ["assembled-two-phase", "assembled-pipelined"] if fp64 else ["assembled-two-phase"]
+    for form in forms:
+        out += [(form, 0, g, 0, 0) for g in graphs]
+        out += [(form, 0, False, rg, bb) for rg in (2, 4) for bb in (3, 4) if (rg, bb) != (2, 4)]
+    return out
 
 
-def time_candidate(system, meshes, settings, solver, blocks, graph, warmup, steps):
+def time_candidate(system, meshes, settings, solver, blocks, graph, row_group, batch_blocks, warmup, steps):
     import talus_b200 as tb
 
     system.set_solver(solver)
     system.tune(blocks, graph)
+    system.tune_shape(row_group, batch_blocks)
     for i, m in enumerate(meshes):
         system.set_state(tb.rest_state(m), i)
     for _ in range(warmup):
@@ -73,14 +83,15 @@ def tune(workload: str, precision_name: str, warmup: int = 2, steps: int = 4, to
     settings = tb.Settings(law=law, tolerance=tolerance, cg_iterations=cap)
     system = tb.System(meshes, mats, precision)
     results = []
-    for solver, blocks, graph in candidates(len(meshes), precision == tb.FP64):
-        sec, its = time_candidate(system, meshes, settings, solver, blocks, graph, warmup, steps)
-        results.append({"solver": solver, "pcg_blocks_per_sm": blocks, "graph": graph, "ms_per_step": sec * 1e3,
-                        "cg_iterations_per_step": its})
+    for solver, blocks, graph, rg, bb in candidates(len(meshes), precision == tb.FP64):
+        sec, its = time_candidate(system, meshes, settings, solver, blocks, graph, rg, bb, warmup, steps)
+        results.append({"solver": solver, "pcg_blocks_per_sm": blocks, "graph": graph, "row_group": rg,
+                        "batch_blocks": bb, "ms_per_step": sec * 1e3, "cg_iterations_per_step": its})
         print(json.dumps(results[-1]), file=sys.stderr, flush=True)
     system.close()
     best = min(results, key=lambda r: r["ms_per_step"])
     return {"solver": best["solver"], "pcg_blocks_per_sm": best["pcg_blocks_per_sm"], "graph": best["graph"],
+            "row_group": best["row_group"], "batch_blocks": best["batch_blocks"],
             "ms_per_step": best["ms_per_step"], "steps": steps, "tolerance": tolerance, "cg_iterations": cap,
             "candidates": results}
 

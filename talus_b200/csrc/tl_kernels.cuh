@@ -603,11 +603,11 @@ template <class S, int LAW> constexpr int elementMinBlocks() {
 // flow): F' = F P, gradients g' = P^T g, volume V / det P, where P = Fp^-1 is
 // the tet's plastic map (plasticRest, plasticflow.cc:263-300: Dm' = Fp Dm,
 // V' = V det Fp); the small-strain return map is off.
-template <class S, int LAW, bool HK = false>
-__global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
-    kElement(Sys<S> s, const Vec4<S>* base, const Vec4<S>* dir, uint32_t pass, uint32_t mode, double margin) {
+template <class S, int LAW, bool HK>
+__device__ __forceinline__ void elementTile(const Sys<S>& s, const Vec4<S>* base, const Vec4<S>* dir, uint32_t pass,
+                                            uint32_t mode, double margin, uint32_t tile) {
   static_assert(!HK || LAW == 0, "the plastic rest shape is written for the corotated law");
-  const uint32_t tile = blockIdx.x, b = s.elem_tile_body[tile];
+  const uint32_t b = s.elem_tile_body[tile];
   if (!bodyActive(s, b, pass)) return;
   if (s.gate)  // a batched Newton round: the body's own mapping and tangent choice
     mode = (mode & ~uint32_t(EM_CONSISTENT | EM_MAPPING)) | (s.gate[b] & uint32_t(EM_CONSISTENT | EM_MAPPING));
@@ -947,6 +947,18 @@ __global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
   if (nBad) atomicOr(&s.acc[b].nonfinite, 1u);
   atomicMin(&s.acc[b].min_j_key, jmin);
   s.epart[tile] = sum;
+}
+
+// The element pass over tiles blockIdx.x, blockIdx.x + gridDim.x, ...: a grid
+// of one block per tile, or a resident grid that walks the tiles (no block
+// launches between rounds); each tile is worked the same way either way.
+template <class S, int LAW, bool HK = false>
+__global__ void __launch_bounds__(TILE, elementMinBlocks<S, LAW>())
+    kElement(Sys<S> s, const Vec4<S>* base, const Vec4<S>* dir, uint32_t pass, uint32_t mode, double margin) {
+  for (uint32_t tile = blockIdx.x; tile < s.elem_tiles; tile += gridDim.x) {
+    elementTile<S, LAW, HK>(s, base, dir, pass, mode, margin, tile);
+    __syncthreads();  // the stage and the reduction arrays are reused by the next tile
+  }
 }
 
 // Node gather + balance (solver.cc:3746-3806) + guardPreconditioner

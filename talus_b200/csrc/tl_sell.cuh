@@ -231,12 +231,17 @@ template <class S> struct Ld4cg {
   __device__ __forceinline__ Vec4<S> operator()(uint32_t c) const { return ld4cg(&v[c]); }
 };
 template <class S> __device__ __forceinline__ Ld4cg<S> ld4cgOf(const Vec4<S>* v) { return Ld4cg<S>{v}; }
-// kPcgSell's row: columns from its shared-memory cache, no prefetch.
-template <class S>
+// kPcgSell's row: columns from its shared-memory cache, no prefetch, U slots per round trip.
+template <class S, uint32_t U>
 __device__ __forceinline__ V3<double> sellRow(const SellDev<S>& g, uint32_t slice, uint32_t lane,
                                               const Vec4<S>* in, const uint32_t* cols) {
-  return sellRowOf<S, Ld4cg<S>, sizeof(S) == 4 ? 4u : 2u, false>(g, slice, lane, ld4cgOf(in), cols);
+  return sellRowOf<S, Ld4cg<S>, U, false>(g, slice, lane, ld4cgOf(in), cols);
 }
+// Column slots per round trip of the assembled matvec rows (a launch shape
+// tl_system_tune_shape may change): kPcgSell's default, then the batched kernels'.
+template <class S> __host__ __device__ constexpr uint32_t sellRowGroup() { return sizeof(S) == 4 ? 4u : 2u; }
+constexpr uint32_t BATCH_ROW_GROUP = 2u;
+constexpr int BATCH_BLOCKS = 4;  // resident blocks per SM the batched kernels are compiled for by default
 
 template <class S> __device__ __forceinline__ V3<double> roundTo(V3<double> v) {
   return cvt<double>(cvt<S>(v));
@@ -258,7 +263,7 @@ template <class S> __device__ __forceinline__ V3<double> roundTo(V3<double> v) {
 // last update without a matvec.  Block partials are added in block order, so
 // every block takes the same decisions.  The slices of block b are
 // [b slices / G, (b + 1) slices / G), at most 8, one per warp.
-template <class S>
+template <class S, uint32_t U = sellRowGroup<S>()>
 __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4<S>* X, uint32_t x0zero, uint32_t tangent) {
   const uint32_t G = gridDim.x, lane = threadIdx.x & 31u;
   const uint32_t s0 = uint32_t(uint64_t(blockIdx.x) * g.slices / G);
@@ -302,7 +307,7 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
   uint32_t applications = 0;
   // ---- r = right - A x (anchored rows 0), u = P r, published to vec[1]
   if (!x0zero) {
-    const V3<double> ax = mine ? sellRow(g, slice, lane, X, tlCols) : V3<double>{0, 0, 0};
+    const V3<double> ax = mine ? sellRow<S, U>(g, slice, lane, X, tlCols) : V3<double>{0, 0, 0};
     if (freeRow) r = rhs - ax;
     ++applications;
   } else if (freeRow) {
@@ -314,7 +319,7 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
   if (mine) vec1[row] = pack(cvt<S>(u));
   if (!countBarrier(s.sync, bar)) return;
   // ---- w = A u, m = P w published to vec[0], first reduction
-  V3<double> w = mine ? sellRow(g, slice, lane, vec1, tlCols) : V3<double>{0, 0, 0};
+  V3<double> w = mine ? sellRow<S, U>(g, slice, lane, vec1, tlCols) : V3<double>{0, 0, 0};
   ++applications;
   V3<double> m = precondition(w);
   if (mine) vec0[row] = pack(cvt<S>(m));
@@ -328,7 +333,7 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
   if (!countBarrier(s.sync, bar)) return;
   // n = A m for the first iteration, requested before the block sums so that
   // their round trip overlaps it (unused if the solve stops here)
-  V3<double> n = mine ? sellRow(g, slice, lane, vec0, tlCols) : V3<double>{0, 0, 0};
+  V3<double> n = mine ? sellRow<S, U>(g, slice, lane, vec0, tlCols) : V3<double>{0, 0, 0};
   double sums[4];
   sumBlocksAll<4>(halves[0], sums);
   ++reductions;
@@ -389,7 +394,7 @@ __global__ void __launch_bounds__(TILE, 2) kPcgSell(Sys<S> s, SellDev<S> g, Vec4
     // n = A m for the next iteration (m just published to vec[(taken + 1) & 1]), with the
     // block partials requested first so that both round trips overlap
     if (stagedSums) requestBlockPartials(part, partStage, 3u);
-    n = mine ? sellRow(g, slice, lane, (taken & 1u) ? vec0 : vec1, tlCols) : V3<double>{0, 0, 0};
+    n = mine ? sellRow<S, U>(g, slice, lane, (taken & 1u) ? vec0 : vec1, tlCols) : V3<double>{0, 0, 0};
     double d[3];
     if (stagedSums) {
       cpAsyncWaitAll();
@@ -458,8 +463,8 @@ __device__ __forceinline__ uint32_t nextSlot(const uint32_t* slotBody, uint32_t 
   return j;
 }
 
-template <class S>
-__global__ void __launch_bounds__(TILE, 4)
+template <class S, uint32_t U = BATCH_ROW_GROUP, int MINB = BATCH_BLOCKS>
+__global__ void __launch_bounds__(TILE, MINB)
     kPcgBatchSell(Sys<S> s, SellDev<S> g, Vec4<S>* X, Vec4<S>* p2, uint32_t pass, uint32_t x0zero, uint32_t tangent) {
   extern __shared__ uint32_t tlBatchSlots[];  // [slots] body (~0u: not stepping), then [slots] rows
   const uint32_t G = gridDim.x, lane = threadIdx.x & 31u;
@@ -489,7 +494,7 @@ __global__ void __launch_bounds__(TILE, 4)
       if (!s.anch[n]) {
         V3<double> ax = {0, 0, 0};
         if (!x0zero)
-          ax = sellRowOf<S, decltype(ld4cgOf(X)), 2u>(g, n >> 5, lane, ld4cgOf(X), static_cast<const uint32_t*>(nullptr));
+          ax = sellRowOf<S, decltype(ld4cgOf(X)), U>(g, n >> 5, lane, ld4cgOf(X), static_cast<const uint32_t*>(nullptr));
         r = cvt<S>(cvt<double>(xyz(rhs)) - ax);
       }
       const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
@@ -567,7 +572,7 @@ __global__ void __launch_bounds__(TILE, 4)
           pnew[n] = pack(pn);
           V3<S> apn = {zero, zero, zero};
           if (!s.anch[n])
-            apn = cvt<S>(sellRowOf<S, decltype(pOf), 2u>(g, n >> 5, lane, pOf, static_cast<const uint32_t*>(nullptr)));
+            apn = cvt<S>(sellRowOf<S, decltype(pOf), U>(g, n >> 5, lane, pOf, static_cast<const uint32_t*>(nullptr)));
           s.ap[n] = pack(apn);
           sums[0] = dot(cvt<double>(pn), cvt<double>(apn));
         }
@@ -732,8 +737,8 @@ __device__ __forceinline__ void pipeDecide(CgBodyDev& c, double gammaNext, doubl
   if (c.pad0 == PIPE_FULL) c.pad1 += 1u;  // the matvec n = A m of the update
 }
 
-template <class S>
-__global__ void __launch_bounds__(TILE, 4)
+template <class S, uint32_t U = BATCH_ROW_GROUP, int MINB = BATCH_BLOCKS>
+__global__ void __launch_bounds__(TILE, MINB)
     kPcgBatchSellPipe(Sys<S> s, SellDev<S> g, Vec4<S>* X, Vec4<S>* zbuf, Vec4<S>* qbuf, uint32_t pass,
                       uint32_t x0zero, uint32_t tangent) {
   extern __shared__ uint32_t tlBatchSlots[];  // [slots] body (~0u: not stepping), then [slots] rows
@@ -773,7 +778,7 @@ __global__ void __launch_bounds__(TILE, 4)
     if (!s.anch[n]) {
       V3<double> ax = {0, 0, 0};
       if (!x0zero)
-        ax = sellRowOf<S, decltype(ld4cgOf(X)), 2u>(g, n >> 5, lane, ld4cgOf(X), static_cast<const uint32_t*>(nullptr));
+        ax = sellRowOf<S, decltype(ld4cgOf(X)), U>(g, n >> 5, lane, ld4cgOf(X), static_cast<const uint32_t*>(nullptr));
       r = cvt<double>(xyz(s.right[n])) - ax;
     }
     const V3<double> uu = precondition(n, r);
@@ -795,7 +800,7 @@ __global__ void __launch_bounds__(TILE, 4)
     if (threadIdx.x < (slotRows[j] & 0x7fffffffu)) {
       V3<double> ww = {0, 0, 0};
       if (!s.anch[n])
-        ww = sellRowOf<S, decltype(ld4cgOf(vecB)), 2u>(g, n >> 5, lane, ld4cgOf(vecB), static_cast<const uint32_t*>(nullptr));
+        ww = sellRowOf<S, decltype(ld4cgOf(vecB)), U>(g, n >> 5, lane, ld4cgOf(vecB), static_cast<const uint32_t*>(nullptr));
       const V3<double> m = precondition(n, ww);
       w[n] = pack(cvt<S>(ww));
       vecA[n] = pack(cvt<S>(m));
@@ -865,7 +870,7 @@ __global__ void __launch_bounds__(TILE, 4)
           // the matvec first: its round trips are the phase's latency
           V3<double> nn = {0, 0, 0};
           if (full && !s.anch[n])
-            nn = sellRowOf<S, decltype(ld4cgOf(mcur)), 2u>(g, n >> 5, lane, ld4cgOf(mcur),
+            nn = sellRowOf<S, decltype(ld4cgOf(mcur)), U>(g, n >> 5, lane, ld4cgOf(mcur),
                                                           static_cast<const uint32_t*>(nullptr));
           const V3<double> uu = cvt<double>(xyz(u[n])), ww = cvt<double>(xyz(w[n]));
           const V3<double> pp = cvt<double>(cvt<S>(uu + beta * cvt<double>(xyz(p[n]))));

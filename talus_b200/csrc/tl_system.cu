@@ -242,6 +242,7 @@ struct SystemBase {
   virtual void stateGet(uint32_t body, int32_t dtype, void* x, void* v, void* a, void* rot, void* plastic) = 0;
   virtual int32_t step(const tl_settings& set, const double g[3], double dt, tl_step_report* reports) = 0;
   virtual void tune(uint32_t blocksPerSm, uint32_t graph) = 0;
+  virtual void tuneShape(uint32_t knob, uint32_t value) = 0;
   virtual void setSolver(uint32_t form) = 0;
   virtual void setPlasticity(uint32_t mode) = 0;
   virtual void expireWait(int32_t solve) = 0;
@@ -318,6 +319,30 @@ struct System final : SystemBase {
   bool sellReady = false;
   uint32_t sellRows = 0, sellSlices = 0, sellPositions = 0, sellStride = 0;
   int sellPerSm = 0, batchSellPerSm = 0, batchPipePerSm = 0;
+  uint32_t elementGrid[3] = {0, 0, 0};  // resident element-pass grids: corotated, SNH, Hencky rest
+  // launch shapes of the assembled PCG (tl_system_tune_shape): column slots per round trip of a
+  // matrix row (0: the kernel's default) and resident blocks per SM of the batched kernels (0: 4)
+  uint32_t tuneRowGroup = 0, tuneBatchBlocks = 0;
+  int sellPerSmOf[2] = {0, 0};  // kPcgSell with row groups 2 and 4
+  uint32_t sellU() const { return tuneRowGroup ? tuneRowGroup : sellRowGroup<S>(); }
+  uint32_t batchU() const { return tuneRowGroup ? tuneRowGroup : BATCH_ROW_GROUP; }
+  int batchBlocks() const { return tuneBatchBlocks ? int(tuneBatchBlocks) : BATCH_BLOCKS; }
+  const void* sellKernel() const {
+    return sellU() == 2u ? (const void*)kPcgSell<S, 2> : (const void*)kPcgSell<S, 4>;
+  }
+  const void* batchKernel(bool twoPhase) const {
+    const bool u4 = batchU() == 4u, b3 = batchBlocks() == 3;
+    if (twoPhase)
+      return u4 ? (b3 ? (const void*)kPcgBatchSell<S, 4, 3> : (const void*)kPcgBatchSell<S, 4, 4>)
+                : (b3 ? (const void*)kPcgBatchSell<S, 2, 3> : (const void*)kPcgBatchSell<S, 2, 4>);
+    return u4 ? (b3 ? (const void*)kPcgBatchSellPipe<S, 4, 3> : (const void*)kPcgBatchSellPipe<S, 4, 4>)
+              : (b3 ? (const void*)kPcgBatchSellPipe<S, 2, 3> : (const void*)kPcgBatchSellPipe<S, 2, 4>);
+  }
+  int occupancyOf(const void* fn, size_t smem) const {
+    int perSm = 0;
+    TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, TILE, smem));
+    return perSm;
+  }
   DevBuf<Vec4<S>> sellP2;  // kPcgBatchSell's second search-direction buffer; z of kPcgBatchSellPipe
   DevBuf<Vec4<S>> sellQ;   // q of kPcgBatchSellPipe
   DevBuf<uint32_t> sellSliceStart, sellGroupSlice, sellCol, sellCentry, sellDiag;
@@ -826,19 +851,24 @@ struct System final : SystemBase {
     sellVal.zero(st);  // padding blocks stay zero; kSellAssemble writes the others
     sellVec.alloc(size_t(2) * sellStride);
     sellVec.zero(st);
-    TL_CUDA(cudaFuncSetAttribute((const void*)kPcgSell<S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(sellColBytes())));
-    TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sellPerSm, (const void*)kPcgSell<S>, TILE, sellColBytes()));
+    for (const void* fn : {(const void*)kPcgSell<S, 2>, (const void*)kPcgSell<S, 4>})
+      TL_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sellColBytes())));
+    sellPerSmOf[0] = occupancyOf((const void*)kPcgSell<S, 2>, sellColBytes());
+    sellPerSmOf[1] = occupancyOf((const void*)kPcgSell<S, 4>, sellColBytes());
+    sellPerSm = sellPerSmOf[sellU() == 4u ? 1 : 0];
     // kPcgSell writes four partials per block into one of two halves
-    if (size_t(8) * sellPerSm * ctx->sms > blkPart.count) blkPart.alloc(size_t(8) * sellPerSm * ctx->sms);
+    {
+      const size_t most = size_t(8) * std::max(sellPerSmOf[0], sellPerSmOf[1]) * ctx->sms;
+      if (most > blkPart.count) blkPart.alloc(most);
+    }
     // kPcgBatchSell: every batch, and single bodies whose rows exceed one per thread of kPcgSell's grid
     sellP2.alloc(Vp);
     sellP2.zero(st);
-    TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&batchSellPerSm, (const void*)kPcgBatchSell<S>, TILE, 0));
+    batchSellPerSm = occupancyOf(batchKernel(true), 0);
     if (batchSellPerSm > 0) {
       sellQ.alloc(Vp);
       sellQ.zero(st);
-      TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&batchPipePerSm, (const void*)kPcgBatchSellPipe<S>, TILE, 0));
+      batchPipePerSm = occupancyOf(batchKernel(false), 0);
       if (batchPipePerSm < 1) throw StatusError{TL_ERR_CUDA, "the pipelined batched PCG cannot be resident"};
     }
     TL_CUDA(cudaStreamSynchronize(st));
@@ -994,6 +1024,11 @@ struct System final : SystemBase {
     // the element pass's shared-memory stage is above the default 48 KB
     for (const void* fn : {(const void*)kElement<S, 0>, (const void*)kElement<S, 1>, (const void*)kElement<S, 0, true>})
       TL_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(elementStageBytes<S>())));
+    // the element pass runs as a resident grid that walks the tiles (no block launches between rounds)
+    elementGrid[0] = std::min<uint32_t>(std::max<uint32_t>(elemTiles, 1u), uint32_t(perSm((const void*)kElement<S, 0>, elementStageBytes<S>())) * ctx->sms);
+    elementGrid[1] = std::min<uint32_t>(std::max<uint32_t>(elemTiles, 1u), uint32_t(perSm((const void*)kElement<S, 1>, elementStageBytes<S>())) * ctx->sms);
+    elementGrid[2] =
+        std::min<uint32_t>(std::max<uint32_t>(elemTiles, 1u), uint32_t(perSm((const void*)kElement<S, 0, true>, elementStageBytes<S>())) * ctx->sms);
     pcg1PerSm[0][0] = perSm((const void*)kPcg1<S, 0, false>, sizeof(TileCache));
     pcg1PerSm[0][1] = perSm((const void*)kPcg1<S, 0, true>, sizeof(TileCache));
     pcg1PerSm[1][0] = perSm((const void*)kPcg1<S, 1, false>, sizeof(TileCache));
@@ -1214,9 +1249,12 @@ struct System final : SystemBase {
     if (profiling) mark(0, true);
     if (std::any_of(hb.begin(), hb.end(), [](const HostBody& h) { return h.anyYields; })) mode |= EM_YIELDING;
     const bool damps = hasDamping && law == TL_LAW_COROTATED && !(mode & EM_COMMIT) && !evaluating;
-    if (law == TL_LAW_SNH) kElement<S, 1><<<elemTiles, TILE, elementStageBytes<S>(), st>>>(view(), base, dir, pass, mode, margin);
-    else if (hencky) kElement<S, 0, true><<<elemTiles, TILE, elementStageBytes<S>(), st>>>(view(), base, dir, pass, mode, margin);
-    else kElement<S, 0><<<elemTiles, TILE, elementStageBytes<S>(), st>>>(view(), base, dir, pass, mode, margin);
+    if (law == TL_LAW_SNH)
+      kElement<S, 1><<<elementGrid[1], TILE, elementStageBytes<S>(), st>>>(view(), base, dir, pass, mode, margin);
+    else if (hencky)
+      kElement<S, 0, true><<<elementGrid[2], TILE, elementStageBytes<S>(), st>>>(view(), base, dir, pass, mode, margin);
+    else
+      kElement<S, 0><<<elementGrid[0], TILE, elementStageBytes<S>(), st>>>(view(), base, dir, pass, mode, margin);
     check();
     if (damps) {
       kDamping<S><<<elemTiles, TILE, 0, st>>>(view(), base, dir, pass);
@@ -1264,7 +1302,7 @@ struct System final : SystemBase {
         mark(2, true);
       }
       void* args[] = {&s, &g, &X, &xz, &tg};
-      TL_CUDA(cudaLaunchCooperativeKernel((const void*)kPcgSell<S>, dim3(sellG), dim3(TILE), args, sellColBytes(), st));
+      TL_CUDA(cudaLaunchCooperativeKernel(sellKernel(), dim3(sellG), dim3(TILE), args, sellColBytes(), st));
     } else if (B == 1) {  // single body, element by element: two-level assembly, per-block partials
       if (profiling) mark(2, true);
       void* args[] = {&s, &X, &xz};
@@ -1300,11 +1338,10 @@ struct System final : SystemBase {
       if (slotBytes > 48 * 1024) throw StatusError{TL_ERR_UNSUPPORTED, "too many node tiles for the batched PCG grid"};
       if (twoPhase) {
         void* args[] = {&s, &g, &X, &p2, &ps, &xz, &tg};
-        TL_CUDA(cudaLaunchCooperativeKernel((const void*)kPcgBatchSell<S>, dim3(grid), dim3(TILE), args, slotBytes, st));
+        TL_CUDA(cudaLaunchCooperativeKernel(batchKernel(true), dim3(grid), dim3(TILE), args, slotBytes, st));
       } else {
         void* args[] = {&s, &g, &X, &p2, &q, &ps, &xz, &tg};
-        TL_CUDA(cudaLaunchCooperativeKernel((const void*)kPcgBatchSellPipe<S>, dim3(grid), dim3(TILE), args, slotBytes,
-                                            st));
+        TL_CUDA(cudaLaunchCooperativeKernel(batchKernel(false), dim3(grid), dim3(TILE), args, slotBytes, st));
       }
     } else {  // batch: two-level assembly, per-body scalars
       if (profiling) mark(2, true);
@@ -1774,6 +1811,25 @@ struct System final : SystemBase {
     if (graphExec) cudaGraphExecDestroy(graphExec);
     graphExec = nullptr;
     graphBroken = false;
+  }
+  void tuneShape(uint32_t knob, uint32_t value) override {
+    if (knob == TL_SHAPE_ROW_GROUP) {
+      if (value != 0u && value != 2u && value != 4u) throw StatusError{TL_ERR_ARG, "row group is 0, 2 or 4"};
+      tuneRowGroup = value;
+    } else if (knob == TL_SHAPE_BATCH_BLOCKS) {
+      if (value != 0u && value != 3u && value != 4u) throw StatusError{TL_ERR_ARG, "batch blocks per SM are 0, 3 or 4"};
+      tuneBatchBlocks = value;
+    } else {
+      throw StatusError{TL_ERR_ARG, "no such launch-shape knob"};
+    }
+    if (sellReady) {
+      sellPerSm = sellPerSmOf[sellU() == 4u ? 1 : 0];
+      batchSellPerSm = occupancyOf(batchKernel(true), 0);
+      batchPipePerSm = occupancyOf(batchKernel(false), 0);
+      if (batchSellPerSm < 1 || batchPipePerSm < 1) throw StatusError{TL_ERR_CUDA, "shape cannot be resident"};
+    }
+    if (graphExec) cudaGraphExecDestroy(graphExec);  // the captured launches hold the old kernels
+    graphExec = nullptr;
   }
 
   // solver.cc:3914-3950: assemble at the predictor, solve for the
@@ -2696,6 +2752,15 @@ int32_t tl_system_tune(tl_system* system, uint32_t pcg_blocks_per_sm, uint32_t g
   return guarded(system->ctx, [&]() -> int32_t {
     TL_CUDA(cudaSetDevice(system->ctx->device));
     system->impl->tune(pcg_blocks_per_sm, graph);
+    return TL_OK;
+  });
+}
+
+int32_t tl_system_tune_shape(tl_system* system, uint32_t knob, uint32_t value) {
+  if (!system) return TL_ERR_ARG;
+  return guarded(system->ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(system->ctx->device));
+    system->impl->tuneShape(knob, value);
     return TL_OK;
   });
 }

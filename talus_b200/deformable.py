@@ -261,6 +261,15 @@ class System:
         (0 = occupancy limit) and CUDA-graph replay of batched elastic steps."""
         check(capi.lib().tl_system_tune(self.handle, int(pcg_blocks_per_sm), 1 if graph else 0), self.context.handle)
 
+    def tune_shape(self, row_group: int = 0, batch_blocks: int = 0):
+        """Launch shape of the assembled-operator PCG (tl_system_tune_shape):
+        column slots per round trip of a matrix row (2 or 4, 0 = default) and
+        resident blocks per SM of the batched kernels (3 or 4, 0 = 4).  The
+        results are bitwise the same for every shape."""
+        check(capi.lib().tl_system_tune_shape(self.handle, capi.TL_SHAPE_ROW_GROUP, int(row_group)), self.context.handle)
+        check(capi.lib().tl_system_tune_shape(self.handle, capi.TL_SHAPE_BATCH_BLOCKS, int(batch_blocks)),
+              self.context.handle)
+
     def set_solver(self, form: str = "auto"):
         """PCG operator form of a system (tl_system_set_solver): "auto",
         "assembled" (3x3 node blocks assembled once per solve),

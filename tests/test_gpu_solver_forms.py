@@ -126,3 +126,40 @@ def test_forms_agree_on_a_body_too_large_for_one_row_per_thread():
     xe, re = run("elementwise", tb.FP64, mesh, mat, tb.Settings(), 3)
     assert relative_error(xa, xe, mesh.rest_positions) <= 1e-10
     assert [r["cg_iterations"] for r in ra] == [r["cg_iterations"] for r in re]
+
+
+@pytest.mark.parametrize("precision", [tb.FP64, tb.FP32_MIXED])
+def test_launch_shapes_give_bitwise_the_same_step(precision):
+    """tl_system_tune_shape changes how many column slots of a matrix row are
+    requested per round trip and how many blocks per SM the batched kernels
+    run; the additions are the same, so the state is bitwise the same, for a
+    single body (kPcgSell) and a ragged batch (both batched orders)."""
+    mesh, mat = plastic_block()
+    meshes, mats = tb.mesh.batch_bodies(count=5, seed=31, lo=3, hi=6)
+    forms = ["assembled-two-phase"] + (["assembled-pipelined"] if precision == tb.FP64 else [])
+    cases = [([mesh], [[mat]], "assembled", [(0, 0), (2, 0), (4, 0)])]
+    cases += [(meshes, mats, form, [(0, 0), (4, 3), (2, 3), (4, 4)]) for form in forms]
+    for ms, mt, form, shapes in cases:
+        results = []
+        for rg, bb in shapes:
+            s = tb.System(ms, mt, precision)
+            s.set_solver(form)
+            s.tune_shape(rg, bb)
+            for i, m in enumerate(ms):
+                s.set_state(tb.rest_state(m), i)
+            for _ in range(3):
+                s.step(tb.Settings(), GRAVITY, DT)
+            results.append(np.concatenate([s.get_state(i).position.ravel() for i in range(len(ms))]))
+            s.close()
+        for r in results[1:]:
+            assert np.array_equal(r, results[0]), form
+
+
+def test_launch_shape_values_are_checked():
+    mesh, mat = elastic_block((3, 3, 3))
+    s = tb.System(mesh, [mat], tb.FP64)
+    for knob, value in ((tb._capi.TL_SHAPE_ROW_GROUP, 3), (tb._capi.TL_SHAPE_BATCH_BLOCKS, 5), (7, 0)):
+        with pytest.raises(tb._capi.TalusError) as e:
+            tb._capi.check(tb._capi.lib().tl_system_tune_shape(s.handle, knob, value), s.context.handle)
+        assert e.value.status == tb._capi.TL_ERR_ARG
+    s.close()
