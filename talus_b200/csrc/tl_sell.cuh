@@ -14,12 +14,13 @@
 //                  land there (FP64 accumulation, stored in S), written with
 //                  its transpose below the diagonal; the diagonal blocks are
 //                  written by kNodeAssemble;
-//   kPcgBatchSellPipe  the batched PCG on this matrix, for batches and for
+//   kPcgBatchSell  the batched PCG on this matrix, for batches and for
 //                  single bodies with more rows than kPcgSell's grid has
-//                  threads: kPcgSell's pipelined arrangement with per-body
-//                  scalars, one grid barrier per iteration;
-//   kPcgBatchSell  the same solve in the textbook order (two barriers per
-//                  iteration, fewer vectors; TL_SOLVER_ASSEMBLED_TWO_PHASE);
+//                  threads, in the textbook order (two grid barriers per
+//                  iteration): the order of FP32-mixed systems;
+//   kPcgBatchSellPipe  the same solve in kPcgSell's pipelined arrangement
+//                  with per-body scalars, one grid barrier per iteration and
+//                  four more vectors per node: the order of FP64 systems;
 //   kPcgSell       (one body) persistent cooperative PCG in the pipelined arrangement
 //                  of Ghysels and Vanroose ("Hiding global synchronization
 //                  latency in the preconditioned conjugate gradient
