@@ -763,6 +763,16 @@ def hencky_form(mesh, mats, settings, context, warmup=3, steps=10):
     return out
 
 
+def matrix_blocks(mesh):
+    """Nonzero 3x3 blocks of a body's assembled operator: its nodes (the
+    diagonal) plus both directions of every distinct edge of its tets."""
+    t = mesh.tet_nodes.astype(np.int64)
+    pairs = np.concatenate([t[:, [a, b]] for a, b in ((0, 1), (0, 2), (0, 3), (1, 2), (1, 3), (2, 3))])
+    pairs.sort(axis=1)
+    edges = np.unique(pairs[:, 0] * (int(pairs.max()) + 1) + pairs[:, 1]).size
+    return mesh.nodes + 2 * edges
+
+
 def batch_form(context, flush, warmup=2, steps=5, tolerance=1e-6, cap=4000):
     """The batching form on its own workload: 512 uneven bodies (cells per
     axis from U{4..24}, E log-uniform in [1e5, 1e8] Pa, nu in [0.25, 0.45],
@@ -778,6 +788,7 @@ def batch_form(context, flush, warmup=2, steps=5, tolerance=1e-6, cap=4000):
 
     spec = WORKLOADS["batch"]
     meshes, mats = make_bodies(spec)
+    blocks = [matrix_blocks(m) for m in meshes]
     settings = tb.Settings(cg_iterations=cap, tolerance=tolerance)
     out, finals = {}, {}
     for name, precision in (("mixed", tb.FP32_MIXED), ("fp64", tb.FP64)):
@@ -803,6 +814,25 @@ def batch_form(context, flush, warmup=2, steps=5, tolerance=1e-6, cap=4000):
             body_iters += [r.cg_iterations for r in reps]
             capped += sum(r.cg_capped_solves for r in reps)
         finals[name] = [system.get_state(i).position for i in range(len(meshes))]
+        # one more step with per-class device times: the batched PCG against its algorithmic bytes
+        # (per body-iteration: blocks (9s + 4) for the matrix and its columns, plus the node vectors
+        # each order moves: 13 (two-phase) or 19 (pipelined) four-wide vectors of s bytes)
+        flush.zero_()
+        torch.cuda.synchronize()
+        preps = system.step(tb.Settings(cg_iterations=cap, tolerance=tolerance, profile=True))
+        s_bytes = 4 if precision == tb.FP32_MIXED else 8
+        form = (tune or {}).get("solver", "auto")
+        piped = form == "assembled-pipelined" or (form in ("auto", "assembled") and precision == tb.FP64)
+        vectors = 19 if piped else 13
+        pcg_bytes = float(sum(r.cg_iterations * (blocks[i] * (9 * s_bytes + 4) + m.nodes * vectors * 4 * s_bytes)
+                              for i, (r, m) in enumerate(zip(preps, meshes))))
+        pcg_s = preps[0].pcg_seconds
+        peak, peak_kind = peaks()
+        pcg_roof = {"kernel": "tl::kPcgBatchSellPipe" if piped else "tl::kPcgBatchSell",
+                    "algorithmic_bytes_per_step": pcg_bytes, "pcg_ms_per_step": pcg_s * 1e3,
+                    "achieved": pcg_bytes / pcg_s / 1e9 if pcg_s > 0 else None, "peak": peak, "unit": "GB/s",
+                    "frac": pcg_bytes / pcg_s / 1e9 / peak if pcg_s > 0 else None, "peak_kind": peak_kind,
+                    "step_ms_with_events": preps[0].device_seconds * 1e3}
         system.close()
         tets = sum(m.tets for m in meshes)
         out[name] = {"value": tets * steps / seconds, "ms_per_step": seconds * 1e3 / steps,
@@ -810,7 +840,7 @@ def batch_form(context, flush, warmup=2, steps=5, tolerance=1e-6, cap=4000):
                      "body_cg_iterations_per_step": {
                          q: float(np.percentile(body_iters / steps, p)) for q, p in
                          (("min", 0), ("median", 50), ("p90", 90), ("max", 100))},
-                     "capped_solves": capped, "tuning": tune}
+                     "capped_solves": capped, "tuning": tune, "pcg_roofline": pcg_roof}
     worst = max(float(np.linalg.norm(a - b, axis=1).max() / np.linalg.norm(b - m.rest_positions, axis=1).max())
                 for a, b, m in zip(finals["mixed"], finals["fp64"], meshes))
     return {"workload": f"batch, {len(meshes)} bodies, {sum(m.tets for m in meshes)} tets", "unit": UNIT,
