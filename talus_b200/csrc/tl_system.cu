@@ -1331,11 +1331,22 @@ struct System final : SystemBase {
       // that diverged); TL_SOLVER_ASSEMBLED_PIPELINED is refused for FP32 systems
       const bool twoPhase = solverForm == TL_SOLVER_ASSEMBLED_TWO_PHASE ||
                             (solverForm != TL_SOLVER_ASSEMBLED_PIPELINED && sizeof(S) == 4);
-      const int perSm = twoPhase ? batchSellPerSm : batchPipePerSm;
-      const int grid = std::max(1, std::min(perSm * ctx->sms, int(nodeTiles)));
+      int perSm = twoPhase ? batchSellPerSm : batchPipePerSm;
+      int grid = std::max(1, std::min(perSm * ctx->sms, int(nodeTiles)));
       // the block's slot table: body and row count of each of its tiles
-      const size_t slotBytes = size_t(2) * sizeof(uint32_t) * ((nodeTiles + grid - 1) / grid);
+      size_t slotBytes = size_t(2) * sizeof(uint32_t) * ((nodeTiles + grid - 1) / grid);
       if (slotBytes > 48 * 1024) throw StatusError{TL_ERR_UNSUPPORTED, "too many node tiles for the batched PCG grid"};
+      if (slotBytes > 1024) {  // a large table may cost residency: size the cooperative grid with it
+        const int withTable = occupancyOf(batchKernel(twoPhase), slotBytes);
+        if (withTable < 1) throw StatusError{TL_ERR_UNSUPPORTED, "the batched PCG grid cannot be resident"};
+        if (withTable < perSm) {
+          perSm = withTable;
+          grid = std::max(1, std::min(perSm * ctx->sms, int(nodeTiles)));
+          slotBytes = size_t(2) * sizeof(uint32_t) * ((nodeTiles + grid - 1) / grid);
+          if (occupancyOf(batchKernel(twoPhase), slotBytes) < perSm)
+            throw StatusError{TL_ERR_UNSUPPORTED, "the batched PCG grid cannot be resident"};
+        }
+      }
       if (twoPhase) {
         void* args[] = {&s, &g, &X, &p2, &ps, &xz, &tg};
         TL_CUDA(cudaLaunchCooperativeKernel(batchKernel(true), dim3(grid), dim3(TILE), args, slotBytes, st));
