@@ -208,10 +208,10 @@ int32_t tl_system_tune_shape(tl_system* system, uint32_t knob, uint32_t value);
  * iterates in one of two orders with the same iterates in exact arithmetic:
  * TL_SOLVER_ASSEMBLED_TWO_PHASE, the textbook order with two grid barriers
  * per iteration, or TL_SOLVER_ASSEMBLED_PIPELINED, the pipelined order with
- * one barrier per iteration and four more vectors per node (FP64 systems
- * only: with its recurrences stored in FP32 the pipelined order drifts).
- * ASSEMBLED and AUTO take the pipelined order in FP64 and the two-phase
- * order in FP32-mixed, the faster of each on the 512-body batch. */
+ * one barrier per iteration and its recurrences kept in FP64 (eight vectors
+ * per node, in both precisions). ASSEMBLED and AUTO take the pipelined order
+ * in FP64 and the two-phase order in FP32-mixed, the faster of each on the
+ * 512-body batch. */
 #define TL_SOLVER_AUTO 0u
 #define TL_SOLVER_ASSEMBLED 1u
 #define TL_SOLVER_ELEMENTWISE 2u

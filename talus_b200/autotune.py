@@ -17,8 +17,8 @@ through ``System.tune``:
   only the launch shape; the results are bitwise the same.
 * ``solver``: the PCG operator form (``System.set_solver``): "auto" (the
   block matrix assembled once per solve, for these workloads), for a batch
-  "assembled-two-phase" (two grid barriers per iteration, fewer bytes) and,
-  in FP64, "assembled-pipelined" (one barrier per iteration), or
+  "assembled-two-phase" (two grid barriers per iteration, fewer bytes) and
+  "assembled-pipelined" (one barrier per iteration, FP64 recurrences), or
   "elementwise".  The block cap applies to the element-by-element kernels;
   the assembled ones take their own occupancy, so they are timed at 0.
 
@@ -45,7 +45,7 @@ def candidates(bodies: int, fp64: bool):
     out = [("elementwise", k, g, 0, 0) for k in (0, 1, 2, 3) for g in graphs]
     if bodies == 1:
         return out + [("auto", 0, False, rg, 0) for rg in (2, 4)]
-    forms = ["assembled-two-phase", "assembled-pipelined"] if fp64 else ["assembled-two-phase"]
+    forms = ["assembled-two-phase", "assembled-pipelined"]
     for form in forms:
         out += [(form, 0, g, 0, 0) for g in graphs]
         out += [(form, 0, False, rg, bb) for rg in (2, 4) for bb in (3, 4) if (rg, bb) != (2, 4)]

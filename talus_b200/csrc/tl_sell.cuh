@@ -20,7 +20,7 @@
 //                  iteration): the order of FP32-mixed systems;
 //   kPcgBatchSellPipe  the same solve in kPcgSell's pipelined arrangement
 //                  with per-body scalars, one grid barrier per iteration and
-//                  four more vectors per node: the order of FP64 systems;
+//                  its recurrences in FP64: the order of FP64 systems;
 //   kPcgSell       (one body) persistent cooperative PCG in the pipelined arrangement
 //                  of Ghysels and Vanroose ("Hiding global synchronization
 //                  latency in the preconditioned conjugate gradient
@@ -693,9 +693,10 @@ __global__ void __launch_bounds__(TILE, MINB)
 
 // The batched PCG of kPcgBatchSell in kPcgSell's pipelined arrangement
 // (Ghysels-Vanroose): one grid barrier per iteration.  Each body keeps the
-// recurrences of kPcgSell, stored per node in S (x, r, u = P r, w = A u and
-// z, q, s, p), and m = P w is published for the next matvec n = A m, in two
-// buffers that alternate by phase.  Per phase, over the block's live tiles:
+// recurrences of kPcgSell in FP64, as kPcgSell keeps them in registers, here
+// stored per node (x, r, u = P r, w = A u and z, q, s, p: eight planes of
+// Vec4<double>), and m = P w, rounded to S, is published for the next matvec
+// n = A m, in two buffers that alternate by phase; X follows x in S.  Per phase, over the block's live tiles:
 //   n = A m; z = n + beta z, q = m + beta q, s = w + beta s, p = u + beta p,
 //   x += alpha p, r -= alpha s, u -= alpha q, w -= alpha z, m = P w;
 //   r.u, w.u, r.r per tile
@@ -740,8 +741,8 @@ __device__ __forceinline__ void pipeDecide(CgBodyDev& c, double gammaNext, doubl
 
 template <class S, uint32_t U = BATCH_ROW_GROUP, int MINB = BATCH_BLOCKS>
 __global__ void __launch_bounds__(TILE, MINB)
-    kPcgBatchSellPipe(Sys<S> s, SellDev<S> g, Vec4<S>* X, Vec4<S>* zbuf, Vec4<S>* qbuf, uint32_t pass,
-                      uint32_t x0zero, uint32_t tangent) {
+    kPcgBatchSellPipe(Sys<S> s, SellDev<S> g, Vec4<S>* X, Vec4<double>* state, uint32_t pass, uint32_t x0zero,
+                      uint32_t tangent) {
   extern __shared__ uint32_t tlBatchSlots[];  // [slots] body (~0u: not stepping), then [slots] rows
   const uint32_t G = gridDim.x, lane = threadIdx.x & 31u;
   g.col_cache = 0;
@@ -760,11 +761,20 @@ __global__ void __launch_bounds__(TILE, MINB)
   __syncthreads();
   Vec4<S>* const vecA = g.vec;             // m of even phases (and of phase 0)
   Vec4<S>* const vecB = g.vec + g.stride;  // u of the start, then m of odd phases
-  Vec4<S>* const u = s.z;
-  Vec4<S>* const w = s.w;
-  Vec4<S>* const sv = s.ap;
-  Vec4<S>* const p = s.p;
+  // the FP64 recurrences, [8][Vp]: x, r, u, w, z, q, s, p (in an FP64 system x is X itself)
+  constexpr bool wide = std::is_same_v<S, double>;
+  Vec4<double>* const xd = wide ? reinterpret_cast<Vec4<double>*>(X) : state;
+  Vec4<double>* const rd = state + size_t(s.Vp);
+  Vec4<double>* const u = state + 2 * size_t(s.Vp);
+  Vec4<double>* const w = state + 3 * size_t(s.Vp);
+  Vec4<double>* const zbuf = state + 4 * size_t(s.Vp);
+  Vec4<double>* const qbuf = state + 5 * size_t(s.Vp);
+  Vec4<double>* const sv = state + 6 * size_t(s.Vp);
+  Vec4<double>* const p = state + 7 * size_t(s.Vp);
   const Vec4<S> zero4 = {S(0), S(0), S(0), S(0)};
+  const Vec4<double> zero4d = {0.0, 0.0, 0.0, 0.0};
+  const auto get = [](const Vec4<double>* v, uint32_t n) { return xyz(v[n]); };
+  const auto put = [](Vec4<double>* v, uint32_t n, V3<double> a) { v[n] = pack(a); };
   const auto precondition = [&](uint32_t n, V3<double> v) {
     const Vec4<S> q0 = s.pre0[n], q1 = s.pre1[n];
     const Sym<double> P = {double(q0.x), double(q0.y), double(q0.z), double(q0.w), double(q1.x), double(q1.y)};
@@ -783,14 +793,15 @@ __global__ void __launch_bounds__(TILE, MINB)
       r = cvt<double>(xyz(s.right[n])) - ax;
     }
     const V3<double> uu = precondition(n, r);
-    s.r[n] = pack(cvt<S>(r));
-    u[n] = pack(cvt<S>(uu));
+    put(rd, n, r);
+    put(u, n, uu);
     vecB[n] = pack(cvt<S>(uu));
     if (x0zero) X[n] = zero4;
-    zbuf[n] = zero4;
-    qbuf[n] = zero4;
-    sv[n] = zero4;
-    p[n] = zero4;
+    if (!wide) xd[n] = x0zero ? zero4d : pack(cvt<double>(xyz(X[n])));
+    zbuf[n] = zero4d;
+    qbuf[n] = zero4d;
+    sv[n] = zero4d;
+    p[n] = zero4d;
   }
   if (!countBarrier(s.sync, bar)) return;
   // ---- phase 0: w = A u, m = P w published; r.u, w.u, r.r, rhs.rhs per body -> the first decision
@@ -803,13 +814,12 @@ __global__ void __launch_bounds__(TILE, MINB)
       if (!s.anch[n])
         ww = sellRowOf<S, decltype(ld4cgOf(vecB)), U>(g, n >> 5, lane, ld4cgOf(vecB), static_cast<const uint32_t*>(nullptr));
       const V3<double> m = precondition(n, ww);
-      w[n] = pack(cvt<S>(ww));
+      put(w, n, ww);
       vecA[n] = pack(cvt<S>(m));
-      const V3<double> r = cvt<double>(xyz(s.r[n])), uu = cvt<double>(xyz(u[n]));
-      const V3<double> wr = cvt<double>(cvt<S>(ww));
+      const V3<double> r = get(rd, n), uu = get(u, n);
       const V3<double> rhs = cvt<double>(xyz(s.right[n]));
       sums[0] = dot(r, uu);
-      sums[1] = dot(wr, uu);
+      sums[1] = dot(ww, uu);
       sums[2] = dot(r, r);
       sums[3] = dot(rhs, rhs);
     }
@@ -873,25 +883,26 @@ __global__ void __launch_bounds__(TILE, MINB)
           if (full && !s.anch[n])
             nn = sellRowOf<S, decltype(ld4cgOf(mcur)), U>(g, n >> 5, lane, ld4cgOf(mcur),
                                                           static_cast<const uint32_t*>(nullptr));
-          const V3<double> uu = cvt<double>(xyz(u[n])), ww = cvt<double>(xyz(w[n]));
-          const V3<double> pp = cvt<double>(cvt<S>(uu + beta * cvt<double>(xyz(p[n]))));
-          const V3<double> ss = cvt<double>(cvt<S>(ww + beta * cvt<double>(xyz(sv[n]))));
-          const V3<double> x = cvt<double>(xyz(X[n])) + alpha * pp;
-          const V3<double> r = cvt<double>(cvt<S>(cvt<double>(xyz(s.r[n])) - alpha * ss));
-          p[n] = pack(cvt<S>(pp));
-          sv[n] = pack(cvt<S>(ss));
-          X[n] = pack(cvt<S>(x));
-          s.r[n] = pack(cvt<S>(r));
+          const V3<double> uu = get(u, n), ww = get(w, n);
+          const V3<double> pp = uu + beta * get(p, n);
+          const V3<double> ss = ww + beta * get(sv, n);
+          const V3<double> x = get(xd, n) + alpha * pp;
+          const V3<double> r = get(rd, n) - alpha * ss;
+          put(p, n, pp);
+          put(sv, n, ss);
+          put(xd, n, x);
+          if (!wide) X[n] = pack(cvt<S>(x));
+          put(rd, n, r);
           if (full) {
             const V3<double> m = cvt<double>(xyz(ld4cg(&mcur[n])));
-            const V3<double> zz = cvt<double>(cvt<S>(nn + beta * cvt<double>(xyz(zbuf[n]))));
-            const V3<double> qq = cvt<double>(cvt<S>(m + beta * cvt<double>(xyz(qbuf[n]))));
-            const V3<double> u2 = cvt<double>(cvt<S>(uu - alpha * qq));
-            const V3<double> w2 = cvt<double>(cvt<S>(ww - alpha * zz));
-            zbuf[n] = pack(cvt<S>(zz));
-            qbuf[n] = pack(cvt<S>(qq));
-            u[n] = pack(cvt<S>(u2));
-            w[n] = pack(cvt<S>(w2));
+            const V3<double> zz = nn + beta * get(zbuf, n);
+            const V3<double> qq = m + beta * get(qbuf, n);
+            const V3<double> u2 = uu - alpha * qq;
+            const V3<double> w2 = ww - alpha * zz;
+            put(zbuf, n, zz);
+            put(qbuf, n, qq);
+            put(u, n, u2);
+            put(w, n, w2);
             mnext[n] = pack(cvt<S>(precondition(n, w2)));
             sums[0] = dot(r, u2);
             sums[1] = dot(w2, u2);

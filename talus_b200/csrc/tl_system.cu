@@ -344,7 +344,7 @@ struct System final : SystemBase {
     return perSm;
   }
   DevBuf<Vec4<S>> sellP2;  // kPcgBatchSell's second search-direction buffer; z of kPcgBatchSellPipe
-  DevBuf<Vec4<S>> sellQ;   // q of kPcgBatchSellPipe
+  DevBuf<Vec4<double>> pipeState;  // kPcgBatchSellPipe's FP64 recurrences [8][Vp], allocated at its first use
   DevBuf<uint32_t> sellSliceStart, sellGroupSlice, sellCol, sellCentry, sellDiag;
   DevBuf<uint4> sellUrec;  // kSellAssemble's per-block records
   uint32_t sellUpperCount = 0, sellColCache = 0;
@@ -866,8 +866,6 @@ struct System final : SystemBase {
     sellP2.zero(st);
     batchSellPerSm = occupancyOf(batchKernel(true), 0);
     if (batchSellPerSm > 0) {
-      sellQ.alloc(Vp);
-      sellQ.zero(st);
       batchPipePerSm = occupancyOf(batchKernel(false), 0);
       if (batchPipePerSm < 1) throw StatusError{TL_ERR_CUDA, "the pipelined batched PCG cannot be resident"};
     }
@@ -1324,11 +1322,8 @@ struct System final : SystemBase {
         mark(2, true);
       }
       Vec4<S>* p2 = sellP2.ptr;
-      Vec4<S>* q = sellQ.ptr;
       // the batch's order: measured on 512 uneven bodies solved to 1e-6, the pipelined
-      // order is the faster in FP64 and the two-phase one in FP32-mixed, whose FP32
-      // storage of the pipelined recurrences also drifts (more iterations, and a body
-      // that diverged); TL_SOLVER_ASSEMBLED_PIPELINED is refused for FP32 systems
+      // order (FP64 recurrences) is the faster in FP64 and the two-phase one in FP32-mixed
       const bool twoPhase = solverForm == TL_SOLVER_ASSEMBLED_TWO_PHASE ||
                             (solverForm != TL_SOLVER_ASSEMBLED_PIPELINED && sizeof(S) == 4);
       int perSm = twoPhase ? batchSellPerSm : batchPipePerSm;
@@ -1351,7 +1346,9 @@ struct System final : SystemBase {
         void* args[] = {&s, &g, &X, &p2, &ps, &xz, &tg};
         TL_CUDA(cudaLaunchCooperativeKernel(batchKernel(true), dim3(grid), dim3(TILE), args, slotBytes, st));
       } else {
-        void* args[] = {&s, &g, &X, &p2, &q, &ps, &xz, &tg};
+        if (!pipeState.ptr) pipeState.alloc(size_t(8) * Vp);
+        Vec4<double>* state = pipeState.ptr;
+        void* args[] = {&s, &g, &X, &state, &ps, &xz, &tg};
         TL_CUDA(cudaLaunchCooperativeKernel(batchKernel(false), dim3(grid), dim3(TILE), args, slotBytes, st));
       }
     } else {  // batch: two-level assembly, per-body scalars
@@ -1780,11 +1777,7 @@ struct System final : SystemBase {
   static constexpr uint32_t OPEN_LAUNCHES = 4;  // openStep's kernels
   std::vector<std::pair<int, size_t>> graphEv;  // event pairs recorded by the captured graph
 
-  void setSolver(uint32_t form) override {
-    if (form == TL_SOLVER_ASSEMBLED_PIPELINED && sizeof(S) == 4)
-      throw StatusError{TL_ERR_UNSUPPORTED, "the pipelined batched PCG keeps its recurrences in S: FP64 only"};
-    solverForm = form;
-  }
+  void setSolver(uint32_t form) override { solverForm = form; }
   void expireWait(int32_t solve) override { expireSolve = solve; }
   void setFlowLimits(uint32_t b, uint32_t lane, double crushStress, double crushLimit, double plasticMax) override {
     if (b >= B || lane >= hb[b].lanes) throw StatusError{TL_ERR_ARG, "no such body or material lane"};

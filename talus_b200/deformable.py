@@ -274,7 +274,7 @@ class System:
         """PCG operator form of a system (tl_system_set_solver): "auto",
         "assembled" (3x3 node blocks assembled once per solve),
         "assembled-two-phase" / "assembled-pipelined" (the same matrix, a batch
-        iterating with two grid barriers per iteration or, FP64 only, one) or
+        iterating with two grid barriers per iteration or with one) or
         "elementwise" (applied element by element every iteration)."""
         code = {"auto": capi.TL_SOLVER_AUTO, "assembled": capi.TL_SOLVER_ASSEMBLED,
                 "assembled-two-phase": capi.TL_SOLVER_ASSEMBLED_TWO_PHASE,
