@@ -39,7 +39,7 @@ import sys
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def candidates(bodies: int, fp64: bool):
+def candidates(bodies: int):
     """(solver, PCG blocks per SM, graph, row group, batch blocks per SM)."""
     graphs = [True, False] if bodies > 1 else [False]
     out = [("elementwise", k, g, 0, 0) for k in (0, 1, 2, 3) for g in graphs]
@@ -83,7 +83,7 @@ def tune(workload: str, precision_name: str, warmup: int = 2, steps: int = 4, to
     settings = tb.Settings(law=law, tolerance=tolerance, cg_iterations=cap)
     system = tb.System(meshes, mats, precision)
     results = []
-    for solver, blocks, graph, rg, bb in candidates(len(meshes), precision == tb.FP64):
+    for solver, blocks, graph, rg, bb in candidates(len(meshes)):
         sec, its = time_candidate(system, meshes, settings, solver, blocks, graph, rg, bb, warmup, steps)
         results.append({"solver": solver, "pcg_blocks_per_sm": blocks, "graph": graph, "row_group": rg,
                         "batch_blocks": bb, "ms_per_step": sec * 1e3, "cg_iterations_per_step": its})
