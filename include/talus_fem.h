@@ -13,6 +13,7 @@
 #ifndef TALUS_FEM_H
 #define TALUS_FEM_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #ifdef __cplusplus
@@ -275,6 +276,15 @@ int32_t tl_state_get(tl_system* system, uint32_t body, int32_t dtype, void* posi
  * nonFinite flag), or an error. */
 int32_t tl_step(tl_system* system, const tl_settings* settings, const double gravity[3], double dt,
                 tl_step_report* reports);
+
+/* Page-locks a caller's host buffer (cudaHostRegister), no reference
+ * counterpart: the element state of tl_state_set/get and tl_step_host then
+ * moves by one DMA straight between that buffer and the device instead of
+ * through the library's pinned staging.  Register whole buffers, once, and
+ * unregister them before freeing them.  Either call may return TL_ERR_CUDA
+ * (a range already registered, or one that was never registered). */
+int32_t tl_host_register(tl_ctx* ctx, void* ptr, size_t bytes);
+int32_t tl_host_unregister(tl_ctx* ctx, void* ptr);
 
 /* Host-state convenience: upload the state, step, download it (the
  * reference's calling convention, where DeformableState lives in host

@@ -151,6 +151,8 @@ SIGNATURES = {
                                      C.POINTER(C.c_uint32)]),
     "tl_system_tune": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32]),
     "tl_system_tune_shape": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32]),
+    "tl_host_register": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_size_t]),
+    "tl_host_unregister": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "tl_system_set_solver": (C.c_int32, [C.c_void_p, C.c_uint32]),
     "tl_system_set_plasticity": (C.c_int32, [C.c_void_p, C.c_uint32]),
     "tl_ctx_check_wait_limit": (C.c_int32, [C.c_void_p]),

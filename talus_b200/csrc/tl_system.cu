@@ -197,6 +197,16 @@ void parallelFor(size_t n, F&& body) {
   pool.run(parts, job);
 }
 
+// Whether p is page-locked host memory (tl_host_register, cudaHostAlloc).
+bool pinnedHost(const void* p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
+
 // memcpy split across the pool.
 void parallelCopy(void* dst, const void* src, size_t bytes) {
   parallelFor(bytes, [&](size_t b0, size_t b1) {
@@ -1117,6 +1127,10 @@ struct System final : SystemBase {
   static constexpr size_t XFER_CHUNK = size_t(4) << 20;
   std::vector<cudaEvent_t> xferEvents;
   void upload(unsigned char* dev, unsigned char* stage, const unsigned char* src, size_t bytes) {
+    if (pinnedHost(src)) {  // the caller pinned its buffer (tl_host_register): one DMA, no staging
+      TL_CUDA(cudaMemcpyAsync(dev, src, bytes, cudaMemcpyHostToDevice, st));
+      return;
+    }
     for (size_t o = 0; o < bytes; o += XFER_CHUNK) {
       const size_t n = std::min(XFER_CHUNK, bytes - o);
       parallelCopy(stage + o, src + o, n);
@@ -1153,8 +1167,10 @@ struct System final : SystemBase {
   }
   // Queues the conversion of a body's element state and its download into
   // the pinned staging.
+  // With direct set (every requested caller buffer pinned), the state goes
+  // straight into the caller's buffers and getElems has nothing to copy.
   template <class H>
-  void fetchElems(const BodyDev& bd, const HostBody& h, bool rot, bool plastic) {
+  void fetchElems(const BodyDev& bd, const HostBody& h, H* rot, H* plastic, bool direct) {
     const uint32_t T = h.tets;
     const size_t nR = rot ? size_t(9) * T : 0, nP = plastic ? size_t(10) * T : 0;
     if (!nR && !nP) return;
@@ -1163,6 +1179,11 @@ struct System final : SystemBase {
     kElemStateOut<S, H><<<(T + TILE - 1) / TILE, TILE, 0, st>>>(view(), bd.elem_begin, T, rot ? dev : nullptr,
                                                                 plastic ? dev + nR : nullptr);
     check();
+    if (direct) {
+      if (nR) TL_CUDA(cudaMemcpyAsync(rot, dev, nR * sizeof(H), cudaMemcpyDeviceToHost, st));
+      if (nP) TL_CUDA(cudaMemcpyAsync(plastic, dev + nR, nP * sizeof(H), cudaMemcpyDeviceToHost, st));
+      return;
+    }
     queueDownload(reinterpret_cast<unsigned char*>(stage), reinterpret_cast<const unsigned char*>(dev),
                   (nR + nP) * sizeof(H));
   }
@@ -1215,12 +1236,17 @@ struct System final : SystemBase {
     if (sx) u.download(sx, h.nodes, st, bd.node_begin);
     if (sv) v.download(sv, h.nodes, st, bd.node_begin);
     if (sa) a.download(sa, h.nodes, st, bd.node_begin);
-    if (dtype == TL_DTYPE_F64) fetchElems<double>(bd, h, rot != nullptr, pl != nullptr);
-    else fetchElems<float>(bd, h, rot != nullptr, pl != nullptr);
+    const bool direct = (!rot || pinnedHost(rot)) && (!pl || pinnedHost(pl));
+    if (dtype == TL_DTYPE_F64)
+      fetchElems<double>(bd, h, static_cast<double*>(rot), static_cast<double*>(pl), direct);
+    else
+      fetchElems<float>(bd, h, static_cast<float*>(rot), static_cast<float*>(pl), direct);
     // element state is copied out chunk by chunk as it arrives; the node
     // records were queued first, so they have arrived once the stream ends
-    if (dtype == TL_DTYPE_F64) getElems(h, static_cast<double*>(rot), static_cast<double*>(pl));
-    else getElems(h, static_cast<float*>(rot), static_cast<float*>(pl));
+    if (!direct) {
+      if (dtype == TL_DTYPE_F64) getElems(h, static_cast<double*>(rot), static_cast<double*>(pl));
+      else getElems(h, static_cast<float*>(rot), static_cast<float*>(pl));
+    }
     TL_CUDA(cudaStreamSynchronize(st));
     if (dtype == TL_DTYPE_F64) {
       if (x) unstageNodes(h, sx, static_cast<double*>(x), true);
@@ -2916,6 +2942,24 @@ int32_t tl_rollout_adjoint(tl_rollout* rollout, const double* dl_dx_final, const
   return guarded(rollout->system->ctx, [&]() -> int32_t {
     TL_CUDA(cudaSetDevice(rollout->system->ctx->device));
     rollout->impl->adjoint(dl_dx_final, dl_dv_final, dl_dyoungs, dl_dv0, dl_dx0, device_seconds);
+    return TL_OK;
+  });
+}
+
+int32_t tl_host_register(tl_ctx* ctx, void* ptr, size_t bytes) {
+  if (!ctx || !ptr || !bytes) return TL_ERR_ARG;
+  return guarded(ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(ctx->device));
+    TL_CUDA(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
+    return TL_OK;
+  });
+}
+
+int32_t tl_host_unregister(tl_ctx* ctx, void* ptr) {
+  if (!ctx || !ptr) return TL_ERR_ARG;
+  return guarded(ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(ctx->device));
+    TL_CUDA(cudaHostUnregister(ptr));
     return TL_OK;
   });
 }

@@ -145,6 +145,14 @@ class Context:
             raise capi.TalusError(status, "tl_ctx_create")
         self.handle = handle
 
+    def pin(self, array):
+        """Page-locks a contiguous numpy array (tl_host_register), so state
+        crosses to and from it by one DMA instead of the library's staging."""
+        check(capi.lib().tl_host_register(self.handle, array.ctypes.data, array.nbytes), self.handle)
+
+    def unpin(self, array):
+        check(capi.lib().tl_host_unregister(self.handle, array.ctypes.data), self.handle)
+
     def close(self):
         if self.handle:
             capi.lib().tl_ctx_destroy(self.handle)
