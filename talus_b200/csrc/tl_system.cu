@@ -286,6 +286,38 @@ namespace {
 // One block at the persistent kernels' grid barrier with one barrier already
 // counted: the goal (two arrivals) needs an arrival that never comes, so the
 // bounded wait runs out and records TL_ERR_TIMEOUT.
+// A node array of the caller's layout ([3 count] of H) into the state
+// (displacement u = x - X when rest is given), in FP64 as the host
+// conversion does it, so both give the same bits.
+template <class S, class H>
+__global__ void __launch_bounds__(TILE) kNodeStateIn(Vec4<S>* dst, const H* src, const double* rest, uint32_t count) {
+  const uint32_t n = blockIdx.x * TILE + threadIdx.x;
+  if (n >= count) return;
+  double x = double(src[3 * size_t(n)]), y = double(src[3 * size_t(n) + 1]), z = double(src[3 * size_t(n) + 2]);
+  if (rest) {
+    x -= rest[3 * size_t(n)];
+    y -= rest[3 * size_t(n) + 1];
+    z -= rest[3 * size_t(n) + 2];
+  }
+  dst[n] = Vec4<S>{S(x), S(y), S(z), S(0)};
+}
+// And back (x = X + u when rest is given).
+template <class S, class H>
+__global__ void __launch_bounds__(TILE) kNodeStateOut(H* dst, const Vec4<S>* src, const double* rest, uint32_t count) {
+  const uint32_t n = blockIdx.x * TILE + threadIdx.x;
+  if (n >= count) return;
+  const Vec4<S> v = src[n];
+  double x = double(v.x), y = double(v.y), z = double(v.z);
+  if (rest) {
+    x += rest[3 * size_t(n)];
+    y += rest[3 * size_t(n) + 1];
+    z += rest[3 * size_t(n) + 2];
+  }
+  dst[3 * size_t(n)] = H(x);
+  dst[3 * size_t(n) + 1] = H(y);
+  dst[3 * size_t(n) + 2] = H(z);
+}
+
 __global__ void __launch_bounds__(TILE) kWaitLimitCheck(GridSyncDev* sync) {
   unsigned int k = 1;
   (void)countBarrier(sync, k);
@@ -492,6 +524,8 @@ struct System final : SystemBase {
   PinnedBuf<GridSyncDev> hSync;
   PinnedBuf<BodyStepDev> hStep;
   PinnedBuf<Vec4<S>> hNode, hNodeV, hNodeA;
+  DevBuf<double> dRest;                // [3 Vp] rest positions in FP64, for node arrays converted on the device
+  DevBuf<unsigned char> dNodeXfer[3];  // a node array in the caller's layout (position, velocity, acceleration)
 
   Sys<S> view() {
     Sys<S> s;
@@ -804,6 +838,13 @@ struct System final : SystemBase {
     sync.zero(st);
     subrec.alloc(size_t(B) * SUBSTEP_RECORDS);
     subrec.zero(st);
+    {
+      std::vector<double> rest(size_t(3) * Vp, 0.0);
+      for (uint32_t b = 0; b < B; ++b)
+        std::copy(hb[b].rest.begin(), hb[b].rest.end(), rest.begin() + size_t(3) * bodyHost[b].node_begin);
+      dRest.alloc(rest.size());
+      dRest.upload(rest.data(), rest.size(), st);
+    }
     buildTiles(hTet, hElemTileBody);
     buildSell(hTet, hStart, hEntry, hAnch, hNodeTileBody);
     TL_CUDA(cudaStreamSynchronize(st));
@@ -1070,6 +1111,18 @@ struct System final : SystemBase {
   template <class H>
   void stageNodes(const BodyDev& bd, const HostBody& h, DevBuf<Vec4<S>>& dst, const H* src, bool displacement,
                   PinnedBuf<Vec4<S>>& buf) {
+    if (pinnedHost(src)) {  // the caller pinned its buffer: one DMA, converted on the device
+      if (!h.nodes) return;
+      DevBuf<unsigned char>& xfer = nodeXfer(buf);
+      const size_t bytes = size_t(3) * h.nodes * sizeof(H);
+      if (xfer.count < bytes) xfer.alloc(bytes);
+      TL_CUDA(cudaMemcpyAsync(xfer.ptr, src, bytes, cudaMemcpyHostToDevice, st));
+      kNodeStateIn<S, H><<<(h.nodes + TILE - 1) / TILE, TILE, 0, st>>>(
+          dst.ptr + bd.node_begin, reinterpret_cast<const H*>(xfer.ptr),
+          displacement ? dRest.ptr + size_t(3) * bd.node_begin : nullptr, h.nodes);
+      check();
+      return;
+    }
     Vec4<S>* stage = buf.get(h.nodes);
     parallelFor(h.nodes, [&](size_t n0, size_t n1) {
       for (size_t n = n0; n < n1; ++n) {
@@ -1083,6 +1136,25 @@ struct System final : SystemBase {
       }
     });
     dst.upload(stage, h.nodes, st, bd.node_begin);
+  }
+  // The device scratch that goes with a node array's pinned stage.
+  DevBuf<unsigned char>& nodeXfer(const PinnedBuf<Vec4<S>>& buf) {
+    return dNodeXfer[&buf == &hNode ? 0 : &buf == &hNodeV ? 1 : 2];
+  }
+  // Converts a node array on the device and copies it straight into the
+  // caller's page-locked buffer.
+  template <class H>
+  void fetchNodesDirect(const BodyDev& bd, const HostBody& h, const DevBuf<Vec4<S>>& src, H* dst, bool displacement,
+                        const PinnedBuf<Vec4<S>>& buf) {
+    if (!h.nodes) return;
+    DevBuf<unsigned char>& xfer = nodeXfer(buf);
+    const size_t bytes = size_t(3) * h.nodes * sizeof(H);
+    if (xfer.count < bytes) xfer.alloc(bytes);
+    kNodeStateOut<S, H><<<(h.nodes + TILE - 1) / TILE, TILE, 0, st>>>(
+        reinterpret_cast<H*>(xfer.ptr), src.ptr + bd.node_begin,
+        displacement ? dRest.ptr + size_t(3) * bd.node_begin : nullptr, h.nodes);
+    check();
+    TL_CUDA(cudaMemcpyAsync(dst, xfer.ptr, bytes, cudaMemcpyDeviceToHost, st));
   }
   template <class H>
   void getNodes(const BodyDev& bd, const HostBody& h, const DevBuf<Vec4<S>>& src, H* dst, bool displacement) {
@@ -1229,13 +1301,25 @@ struct System final : SystemBase {
   void stateGet(uint32_t b, int32_t dtype, void* x, void* vv, void* aa, void* rot, void* pl) override {
     const BodyDev& bd = bodyHost[b];
     const HostBody& h = hb[b];
-    // queue every download, wait once, then convert
-    Vec4<S>* sx = x ? hNode.get(h.nodes) : nullptr;
-    Vec4<S>* sv = vv ? hNodeV.get(h.nodes) : nullptr;
-    Vec4<S>* sa = aa ? hNodeA.get(h.nodes) : nullptr;
+    // queue every download, wait once, then convert; a page-locked caller
+    // buffer gets its array converted on the device and copied straight in
+    auto direct_node = [&](void* p) { return p && pinnedHost(p); };
+    const bool dx = direct_node(x), dv = direct_node(vv), da = direct_node(aa);
+    Vec4<S>* sx = x && !dx ? hNode.get(h.nodes) : nullptr;
+    Vec4<S>* sv = vv && !dv ? hNodeV.get(h.nodes) : nullptr;
+    Vec4<S>* sa = aa && !da ? hNodeA.get(h.nodes) : nullptr;
     if (sx) u.download(sx, h.nodes, st, bd.node_begin);
     if (sv) v.download(sv, h.nodes, st, bd.node_begin);
     if (sa) a.download(sa, h.nodes, st, bd.node_begin);
+    if (dtype == TL_DTYPE_F64) {
+      if (dx) fetchNodesDirect(bd, h, u, static_cast<double*>(x), true, hNode);
+      if (dv) fetchNodesDirect(bd, h, v, static_cast<double*>(vv), false, hNodeV);
+      if (da) fetchNodesDirect(bd, h, a, static_cast<double*>(aa), false, hNodeA);
+    } else {
+      if (dx) fetchNodesDirect(bd, h, u, static_cast<float*>(x), true, hNode);
+      if (dv) fetchNodesDirect(bd, h, v, static_cast<float*>(vv), false, hNodeV);
+      if (da) fetchNodesDirect(bd, h, a, static_cast<float*>(aa), false, hNodeA);
+    }
     const bool direct = (!rot || pinnedHost(rot)) && (!pl || pinnedHost(pl));
     if (dtype == TL_DTYPE_F64)
       fetchElems<double>(bd, h, static_cast<double*>(rot), static_cast<double*>(pl), direct);
@@ -1249,13 +1333,13 @@ struct System final : SystemBase {
     }
     TL_CUDA(cudaStreamSynchronize(st));
     if (dtype == TL_DTYPE_F64) {
-      if (x) unstageNodes(h, sx, static_cast<double*>(x), true);
-      if (vv) unstageNodes(h, sv, static_cast<double*>(vv), false);
-      if (aa) unstageNodes(h, sa, static_cast<double*>(aa), false);
+      if (sx) unstageNodes(h, sx, static_cast<double*>(x), true);
+      if (sv) unstageNodes(h, sv, static_cast<double*>(vv), false);
+      if (sa) unstageNodes(h, sa, static_cast<double*>(aa), false);
     } else {
-      if (x) unstageNodes(h, sx, static_cast<float*>(x), true);
-      if (vv) unstageNodes(h, sv, static_cast<float*>(vv), false);
-      if (aa) unstageNodes(h, sa, static_cast<float*>(aa), false);
+      if (sx) unstageNodes(h, sx, static_cast<float*>(x), true);
+      if (sv) unstageNodes(h, sv, static_cast<float*>(vv), false);
+      if (sa) unstageNodes(h, sa, static_cast<float*>(aa), false);
     }
   }
 

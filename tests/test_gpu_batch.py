@@ -291,37 +291,41 @@ def test_host_step_moves_plastic_state_only_when_the_step_uses_it():
     assert moved["plastic"][:, 9].max() > 0.0
 
 
-def test_pinned_host_buffers_step_like_pageable_ones():
+@pytest.mark.parametrize("dtype", ["f32", "f64"])
+def test_pinned_host_buffers_step_like_pageable_ones(dtype):
     """tl_host_register page-locks the caller's state buffers; tl_step_host
-    then moves the element state by one DMA each way instead of through the
-    library's staging.  The states are bitwise the same either way, for a
-    yielding body (the plastic slot crosses both ways)."""
+    then moves every state array by one DMA each way instead of through the
+    library's staging, node arrays converted on the device.  The states are
+    bitwise the same either way, for a yielding body (the plastic slot
+    crosses both ways), in both caller precisions."""
     import ctypes as C
     from talus_b200 import _capi as capi
 
     mesh, mat = plastic_block()
     results = []
-    for pinned in (False, True):
+    # nothing pinned, everything pinned, and a mix (per-array choice)
+    for pinned in ((), ("position", "velocity", "acceleration", "rotation", "plastic"), ("position", "plastic")):
         system = tb.System(mesh, [mat], tb.FP32_MIXED)
         st = tb.rest_state(mesh)
-        arrays = {k: np.ascontiguousarray(getattr(st, k), np.float32) for k in
+        np_t = np.float32 if dtype == "f32" else np.float64
+        arrays = {k: np.ascontiguousarray(getattr(st, k), np_t) for k in
                   ("position", "velocity", "acceleration", "rotation", "plastic")}
-        if pinned:
-            for a in arrays.values():
-                system.context.pin(a)
+        for k in pinned:
+            system.context.pin(arrays[k])
         g = np.asarray(GRAVITY, np.float64)
         s_c = tb.Settings()._c()
         for _ in range(4):
-            rc = capi.lib().tl_step_host(system.handle, 0, capi.TL_DTYPE_F32,
+            rc = capi.lib().tl_step_host(system.handle, 0,
+                                         capi.TL_DTYPE_F32 if dtype == "f32" else capi.TL_DTYPE_F64,
                                          *[arrays[k].ctypes.data for k in
                                            ("position", "velocity", "acceleration", "rotation", "plastic")],
                                          C.byref(s_c), g.ctypes.data, DT, C.byref(capi.tl_step_report()))
             assert rc == capi.TL_OK
-        if pinned:
-            for a in arrays.values():
-                system.context.unpin(a)
+        for k in pinned:
+            system.context.unpin(arrays[k])
         results.append({k: a.copy() for k, a in arrays.items()})
         system.close()
-    for k in results[0]:
-        assert np.array_equal(results[0][k], results[1][k]), k
+    for r in results[1:]:
+        for k in results[0]:
+            assert np.array_equal(results[0][k], r[k]), k
     assert (results[1]["plastic"][:, 9] > 0).any()  # the plastic slot crossed
