@@ -220,6 +220,55 @@ int32_t tl_system_tune_shape(tl_system* system, uint32_t knob, uint32_t value);
 #define TL_SOLVER_ASSEMBLED_PIPELINED 4u
 int32_t tl_system_set_solver(tl_system* system, uint32_t form);
 
+/* The caller-held solver state of deformable::step (DeformableSolverState*,
+ * factor.h:205-210; solver.cc:3606-3655, 3808-3910, 4258-4263), held by the
+ * library for a one-body system.  While it is on, every step preconditions
+ * its PCG with the FP64 Cholesky factor of (1 - alpha_m) M + h^2 sum R K R^T
+ * made at the committed rotations of the last refresh (SystemFactor,
+ * factor.cc:318-618), applied in the body's rotation since then
+ * (bodyRotation, applyFactor, factor.cc:620-704).  The factor is made again
+ * when it is empty or the step's h or (1 - alpha_m) changed, and, with a
+ * second solve from the same start at the full iteration cap, when a solve
+ * that may refresh reaches factor_budget iterations (Settings::factorBudget,
+ * solver.h:54; 0: the iteration cap).  The factor is made on the host
+ * (nested-dissection order, block up-looking Cholesky) and applied on the
+ * device inside the PCG launch (kPcgFactor).  Needs a one-body system with
+ * the assembled operator available, the corotated law on the small-strain
+ * path and no stiffness damping: TL_ERR_UNSUPPORTED otherwise.  enable = 0 drops the state. */
+int32_t tl_system_use_factor(tl_system* system, uint32_t enable, uint32_t factor_budget);
+
+/* SolverStats (factor.h:28-38), the SystemFactor's size (factor.h:50-62) and
+ * the StepReport factor counters (solver.h:211-311; counts summed over
+ * steps, the spent / refreshed figures as last set).  factor_nonzeros counts
+ * this library's L (its own ordering); system_nonzeros counts the full
+ * scalar system as the reference's does. */
+typedef struct tl_factor_stats {
+  uint32_t factor_age;
+  uint32_t refactor_count;
+  uint32_t retry_count;
+  uint32_t substeps_since_refresh;
+  uint32_t refresh_requested;
+  uint32_t fresh_retry_failed;
+  double mean_iterations;
+  uint32_t rows;
+  uint32_t ready;
+  uint64_t system_nonzeros;
+  uint64_t generation;
+  uint32_t refresh_requests;
+  uint32_t refactors;
+  uint32_t retries;
+  uint32_t retries_failed;
+  uint32_t wasted_iterations;
+  uint32_t spent_before_refresh;
+  uint32_t spent_after_refresh;
+  uint32_t refreshed_at_age;
+  uint32_t factor_applications;
+  uint32_t reserved;
+  uint64_t factor_nonzeros;
+  double refactor_seconds;  /* host time spent making the factor */
+} tl_factor_stats;
+int32_t tl_system_factor_stats(tl_system* system, tl_factor_stats* out);
+
 /* Plasticity of the yielding lanes.
  * TL_PLASTICITY_SMALL_STRAIN (default): the tet law's J2 return on the small
  * elastic strain inside the step, with the plastic Newton loop

@@ -25,6 +25,29 @@
 #include <limits>
 #include <vector>
 
+// A caller-held solver state (DeformableSolverState, factor.h:205-210): the
+// system factor (SystemFactor::Held, factor.cc:302-314), its FactorReference
+// (factor.h:20-26) and SolverStats (factor.h:28-38).  The reference factors
+// with Eigen's SimplicialLLT under an AMD ordering; this restatement factors
+// the same FP64 matrix in its natural order inside its envelope (the row
+// profile), so L differs while L L^T, and so the applied inverse, agree to
+// rounding.
+struct or_solver {
+  uint32_t budget = 32u;              // Settings::factorBudget (solver.h:54)
+  uint32_t nodes = 0u;
+  bool analyzed = false, ready = false;
+  uint64_t born = 0u, systemNonZeros = 0u;
+  std::vector<uint32_t> first;         // envelope: first column of each row
+  std::vector<size_t> start;           // row offsets into env
+  std::vector<double> env;             // L, row by row, from first[i] to i
+  std::vector<uint8_t> anchored;
+  std::vector<double> refPosition;     // FactorReference::positions [3 nodes]
+  double refCentroid[3] = {0.0, 0.0, 0.0};
+  double refStep = 0.0, refInertia = 1.0;
+  or_solver_stats stats{};
+  float meanIterations = 0.0f;         // SolverStats::meanIterations is a float
+};
+
 namespace {
 
 // ---------------------------------------------------------------- math ----
@@ -749,6 +772,67 @@ template <class R> struct Element {
   FlowLimits limits;  // finite-strain flow: crush and plastic cap
 };
 
+// ----------------------------------------------------- system factor ----
+
+// L L^T x = b in place, with L in its envelope (the solve of applyFactor,
+// factor.cc:690).
+inline void envelopeSolve(const or_solver& f, std::vector<double>& b) {
+  const size_t n = f.first.size();
+  for (size_t i = 0; i < n; ++i) {
+    const double* row = &f.env[f.start[i]] - f.first[i];
+    double sum = b[i];
+    for (size_t k = f.first[i]; k < i; ++k) sum -= row[k] * b[k];
+    b[i] = sum / row[i];
+  }
+  for (size_t i = n; i-- > 0;) {
+    const double* row = &f.env[f.start[i]] - f.first[i];
+    b[i] /= row[i];
+    for (size_t k = f.first[i]; k < i; ++k) b[k] -= row[k] * b[i];
+  }
+}
+
+// factor.cc:669-704 applyFactor: turned into the factor's frame, packed to
+// FP64, solved, unpacked in the arithmetic of the step, turned back, anchored
+// nodes zero.
+template <class R>
+void applyFactor(const or_solver& f, const M3<R>& frame, std::vector<V3<R>>& vector) {
+  const M3<R> inverse = transpose(frame);
+  std::vector<double> packed(size_t(3) * f.nodes);
+  for (uint32_t n = 0; n < f.nodes; ++n) {
+    const V3<R> turned = inverse * vector[n];
+    packed[3 * n] = double(turned.x);
+    packed[3 * n + 1] = double(turned.y);
+    packed[3 * n + 2] = double(turned.z);
+  }
+  envelopeSolve(f, packed);
+  for (uint32_t n = 0; n < f.nodes; ++n) {
+    const V3<R> raw(R(packed[3 * n]), R(packed[3 * n + 1]), R(packed[3 * n + 2]));
+    vector[n] = f.anchored[n] != 0u ? V3<R>() : frame * raw;
+  }
+}
+
+// factor.cc:638-667 bodyRotation: the polar rotation of the mass-weighted
+// correlation of the positions now with those the factor was made at.
+template <class R>
+M3<R> bodyRotation(const std::vector<R>& mass, const std::vector<V3<R>>& position, const or_solver& f) {
+  if (f.refPosition.size() != size_t(3) * position.size()) return M3<R>(R(1));
+  V3<R> centre;
+  R total = 0;
+  for (size_t n = 0; n < position.size(); ++n) {
+    total += mass[n];
+    centre += mass[n] * position[n];
+  }
+  if (total > R(0)) centre = V3<R>(centre.x / total, centre.y / total, centre.z / total);
+  const V3<R> before0(R(f.refCentroid[0]), R(f.refCentroid[1]), R(f.refCentroid[2]));
+  M3<R> correlation(R(0));
+  for (size_t n = 0; n < position.size(); ++n) {
+    const V3<R> now = position[n] - centre;
+    const V3<R> before = V3<R>(R(f.refPosition[3 * n]), R(f.refPosition[3 * n + 1]), R(f.refPosition[3 * n + 2])) - before0;
+    correlation = correlation + mass[n] * outer(now, before);
+  }
+  return polarRotation(correlation);
+}
+
 template <class R> struct Solver {
   // inputs
   uint32_t V = 0, T = 0;
@@ -782,6 +866,22 @@ template <class R> struct Solver {
       carried, evaluated, total, lowestIterate, drive;
   std::vector<M3<R>> diagonal, preconditioner;
   or_report* report = nullptr;
+  // a caller-held factor (the prepared SystemFactor of solver.cc:3808-3812)
+  // and the frame it is applied in; block Jacobi while it is absent or empty
+  const or_solver* factor = nullptr;
+  M3<R> frame{R(1)};
+  uint32_t factorApplications = 0;
+
+  // solver.cc:1920-1952 condition
+  void condition() {
+    if (factor && factor->ready) {
+      conditioned = residual;
+      applyFactor(*factor, frame, conditioned);
+      ++factorApplications;
+      return;
+    }
+    for (uint32_t n = 0; n < V; ++n) conditioned[n] = preconditioner[n] * residual[n];
+  }
 
   const TetStiffness<R>& stiffnessOf(uint32_t e) const { return consistent ? working[e] : store[e]; }
 
@@ -906,18 +1006,25 @@ template <class R> struct Solver {
     }
   }
 
-  struct CgResult { uint32_t iterations = 0; R relativeResidual{0}, startResidual{0}; bool capped = false; };
+  // applications: the factor applications of this solve (CgResult::factorTiming, solver.cc:1926-1934)
+  struct CgResult {
+    uint32_t iterations = 0;
+    R relativeResidual{0}, startResidual{0};
+    bool capped = false;
+    uint32_t applications = 0;
+  };
 
-  // solver.cc:1904-2089 conjugateGradient (block Jacobi, no factor, no free modes)
+  // solver.cc:1904-2089 conjugateGradient (block Jacobi or the factor, no free modes)
   CgResult conjugateGradient(R inertia, R step, uint32_t limit, R tolerance, std::vector<V3<R>>& solution) {
     CgResult result;
+    const uint32_t applied0 = factorApplications;
     R reference = 0;
     for (uint32_t n = 0; n < V; ++n) reference += dot(right[n], right[n]);
     reference = std::sqrt(reference);
     applySystem(inertia, step, solution, applied);
     R squared = 0;
     for (uint32_t n = 0; n < V; ++n) residual[n] = anchored[n] ? V3<R>() : right[n] - applied[n];
-    for (uint32_t n = 0; n < V; ++n) conditioned[n] = preconditioner[n] * residual[n];
+    condition();
     for (uint32_t n = 0; n < V; ++n) {
       direction[n] = conditioned[n];
       squared += dot(residual[n], conditioned[n]);
@@ -942,7 +1049,7 @@ template <class R> struct Solver {
         residual[n] -= stride * applied[n];
       }
       R next = 0;
-      for (uint32_t n = 0; n < V; ++n) conditioned[n] = preconditioner[n] * residual[n];
+      condition();
       for (uint32_t n = 0; n < V; ++n) next += dot(residual[n], conditioned[n]);
       const R blend = next / squared;
       squared = next;
@@ -955,6 +1062,7 @@ template <class R> struct Solver {
     result.iterations = taken;
     result.relativeResidual = res / referenceFloor;
     result.capped = taken == limit && res > target;
+    result.applications = factorApplications - applied0;
     return result;
   }
 
@@ -1103,9 +1211,127 @@ FloatingFrame<R> floatingFrame(const std::vector<R>& nodeMass, const std::vector
   return made;
 }
 
+// factor.cc:21-30 preciseLame, 32-47 preciseTurned, 49-88 preciseTetBlocks:
+// step^2 R K R^T in FP64, with Dm and V recomputed from the rest positions.
+template <class R>
+std::array<M3<double>, 16> preciseTetBlocks(const Solver<R>& s, const Element<R>& el, double youngs, double poisson,
+                                            const M3<R>& rotation, R step) {
+  const auto wide = [](const V3<R>& v) { return V3<double>(double(v.x), double(v.y), double(v.z)); };
+  const V3<double> first = wide(s.rest[el.nodes[0]]);
+  const M3<double> shape(wide(s.rest[el.nodes[1]]) - first, wide(s.rest[el.nodes[2]]) - first,
+                         wide(s.rest[el.nodes[3]]) - first);
+  const double volume = determinant(shape) / 6.0;
+  const M3<double> rows = transpose(inverse(shape));
+  const std::array<V3<double>, 4> gradient{-(rows[0] + rows[1] + rows[2]), rows[0], rows[1], rows[2]};
+  const double nu = std::clamp(poisson, 0.0, 0.49);
+  const double lambda = youngs * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = youngs / (2.0 * (1.0 + nu));
+  M3<double> turn;
+  for (int c = 0; c < 3; ++c) turn[c] = wide(rotation[c]);
+  const M3<double> back = transpose(turn);
+  const double scale = double(step) * double(step);
+  std::array<M3<double>, 16> blocks;
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) {
+      const V3<double>& ga = gradient[a];
+      const V3<double>& gb = gradient[b];
+      const M3<double> k = volume * (lambda * outer(ga, gb) + mu * outer(gb, ga) + (mu * dot(ga, gb)) * M3<double>(1.0));
+      blocks[4 * a + b] = scale * (turn * k * back);
+    }
+  return blocks;
+}
+
+// factor.cc:318-460 gather, 549-565 analyzeSystem, 567-618 refreshFactor: the
+// system (1 - alpha_m) M + h^2 sum R K R^T at the committed rotations, anchored
+// rows and columns replaced by the identity, factored; the reference
+// positions and centroid are the state's.
+template <class R>
+void refreshFactor(or_solver& f, const Solver<R>& s, const std::vector<double>& youngs,
+                   const std::vector<double>& poisson, R step, R inertia) {
+  const uint32_t V = s.V;
+  const size_t n = size_t(3) * V;
+  if (f.analyzed && f.nodes != V) f.analyzed = false;
+  if (!f.analyzed) {
+    f.nodes = V;
+    f.anchored = s.anchored;
+    // stored entries of the full matrix: 9 per coupled pair of free nodes,
+    // 3 on the diagonal of every node
+    std::vector<std::vector<uint32_t>> pairs(V);
+    for (const Element<R>& el : s.elements)
+      for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b)
+          if (!s.anchored[el.nodes[a]] && !s.anchored[el.nodes[b]]) pairs[el.nodes[a]].push_back(el.nodes[b]);
+    uint64_t stored = 0;
+    for (uint32_t v = 0; v < V; ++v) {
+      std::sort(pairs[v].begin(), pairs[v].end());
+      pairs[v].erase(std::unique(pairs[v].begin(), pairs[v].end()), pairs[v].end());
+      const bool diagonalHeld = std::binary_search(pairs[v].begin(), pairs[v].end(), v);
+      stored += 9u * pairs[v].size() + (diagonalHeld ? 0u : 3u);
+    }
+    f.systemNonZeros = stored;
+    f.first.assign(n, 0u);
+    for (size_t i = 0; i < n; ++i) f.first[i] = uint32_t(i - i % 3);
+    for (const Element<R>& el : s.elements)
+      for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b) {
+          const uint32_t na = el.nodes[a], nb = el.nodes[b];
+          if (s.anchored[na] || s.anchored[nb]) continue;
+          for (int r = 0; r < 3; ++r) f.first[3 * na + r] = std::min(f.first[3 * na + r], 3u * nb);
+        }
+    f.start.assign(n + 1, 0u);
+    for (size_t i = 0; i < n; ++i) f.start[i + 1] = f.start[i] + (i - f.first[i] + 1);
+    f.analyzed = true;
+  }
+  f.env.assign(f.start[n], 0.0);
+  auto at = [&](size_t i, size_t j) -> double& { return f.env[f.start[i] + (j - f.first[i])]; };
+  for (uint32_t e = 0; e < s.T; ++e) {
+    const Element<R>& el = s.elements[e];
+    const std::array<M3<double>, 16> blocks = preciseTetBlocks(s, el, youngs[e], poisson[e], s.rotation[e], step);
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) {
+        const uint32_t na = el.nodes[a], nb = el.nodes[b];
+        if (s.anchored[na] || s.anchored[nb]) continue;
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c)
+            if (3u * nb + c <= 3u * na + r) at(3 * na + r, 3 * nb + c) += blocks[4 * a + b][c][r];
+      }
+  }
+  for (uint32_t v = 0; v < V; ++v) {
+    const double diagonal = s.anchored[v] ? 1.0 : double(inertia * s.mass[v]);
+    for (int k = 0; k < 3; ++k) at(3 * v + k, 3 * v + k) += diagonal;
+  }
+  // LL^T inside the envelope (SimplicialLLT::factorize fails on a pivot <= 0)
+  f.ready = true;
+  for (size_t i = 0; i < n && f.ready; ++i) {
+    double* row = &f.env[f.start[i]] - f.first[i];
+    for (size_t j = f.first[i]; j < i; ++j) {
+      const double* other = &f.env[f.start[j]] - f.first[j];
+      double sum = row[j];
+      for (size_t k = std::max(f.first[i], f.first[j]); k < j; ++k) sum -= row[k] * other[k];
+      row[j] = sum / other[j];
+    }
+    double d = row[i];
+    for (size_t k = f.first[i]; k < i; ++k) d -= row[k] * row[k];
+    if (!(d > 0.0)) f.ready = false;
+    else row[i] = std::sqrt(d);
+  }
+  ++f.born;
+  f.refStep = double(step);
+  f.refInertia = double(inertia);
+  f.refPosition.assign(n, 0.0);
+  V3<R> centroid;
+  R total = 0;
+  for (uint32_t v = 0; v < V; ++v) {
+    for (int k = 0; k < 3; ++k) f.refPosition[3 * v + k] = double(s.position[v][k]);
+    total += s.mass[v];
+    centroid += s.mass[v] * s.position[v];
+  }
+  if (total > R(0)) centroid = V3<R>(centroid.x / total, centroid.y / total, centroid.z / total);
+  for (int k = 0; k < 3; ++k) f.refCentroid[k] = double(centroid[k]);
+}
+
 template <class R>
 int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, uint32_t lanes, const or_settings* settings,
-             const double gravity[3], double dtIn, or_report* report) {
+             const double gravity[3], double dtIn, or_report* report, or_solver* solver) {
   const auto began = std::chrono::steady_clock::now();
   Solver<R> s;
   s.report = report;
@@ -1147,6 +1373,7 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
     s.plasticCorners.resize(T);
   }
   bool anyYields = false;
+  std::vector<double> factorYoungs(T), factorPoisson(T);  // the material of each tet, for the factor
   static const or_material DEFAULT = {1000.0, 0.0, 0.3, 0.0, std::numeric_limits<double>::infinity(), 0.0,
                                       std::numeric_limits<double>::infinity(), 1.0,
                                       std::numeric_limits<double>::infinity()};
@@ -1160,6 +1387,8 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
     s.damped = s.damped || el.tau > R(0);
     const R youngs = mesh->element_youngs ? R(mesh->element_youngs[e]) : R(m.youngs_modulus);
     el.moduli = lame(youngs, R(m.poissons_ratio));
+    factorYoungs[e] = double(youngs);
+    factorPoisson[e] = double(R(m.poissons_ratio));
     el.yieldStress = R(m.yield_stress);
     el.hardening = R(m.hardening_modulus);
     el.yields = yieldsAt(el.yieldStress);
@@ -1193,6 +1422,8 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
   if (s.hencky) anyYields = false;  // each step is elastic from the plastic rest
   // damping is defined with the corotated stiffness and committed rotation
   if (s.damped && s.law == OR_LAW_SNH) return -3;
+  // a factor is restated for undamped bodies on the small-strain path
+  if (solver && (s.damped || s.hencky)) return -3;
   if (s.damped) s.fits.assign(T, RigidFit<R>());
   auto sized = [&](std::vector<V3<R>>& v) { v.assign(V, V3<R>()); };
   sized(s.force); sized(s.right); sized(s.residual); sized(s.direction); sized(s.applied); sized(s.conditioned);
@@ -1224,6 +1455,14 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
   report->substeps += substeps;
   R elastic = 0;
   bool plasticGrowth = false;
+  // solver.cc:3639-3655: the caller's factor is made again when it is empty
+  // or was made for another step or inertia
+  if (solver && (!solver->ready || solver->refStep != double(effective.step) ||
+                 solver->refInertia != double(effective.inertia))) {
+    refreshFactor(*solver, s, factorYoungs, factorPoisson, effective.step, effective.inertia);
+    solver->stats.factor_age = 0u;
+    ++solver->stats.refactor_count;
+  }
 
   for (uint32_t pass = 0; pass != substeps; ++pass) {
     const FloatingFrame<R> body = floating
@@ -1298,9 +1537,45 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
       report->cg_capped_solves += r.capped ? 1u : 0u;
       report->cg_worst_relative_residual = std::max(report->cg_worst_relative_residual, double(r.relativeResidual));
     };
-    auto solvePrimary = [&](std::vector<V3<R>>& solution) {
+    // solver.cc:3808-3821: the prepared factor, its frame and the budget of a
+    // factored solve
+    s.factor = solver && solver->ready ? solver : nullptr;
+    s.frame = s.factor ? bodyRotation(s.mass, s.position, *solver) : M3<R>(R(1));
+    const uint32_t budget = s.factor && solver->budget != 0u ? std::min(solver->budget, settings->cg_iterations)
+                                                               : settings->cg_iterations;
+    uint32_t passIterations = 0;  // primaryResult.iterations of the substep
+    // solver.cc:3822-3910 solvePrimary: a capped factored solve that may
+    // refresh makes the factor again at the latest rotations and solves
+    // again from the same start with the full iteration cap
+    auto solvePrimary = [&](std::vector<V3<R>>& solution, bool refreshes) {
       s.restart = solution;
-      const auto r = s.conjugateGradient(effective.inertia, effective.step, settings->cg_iterations, tolerance, solution);
+      auto r = s.conjugateGradient(effective.inertia, effective.step, budget, tolerance, solution);
+      if (r.capped && s.factor && refreshes) {
+        or_solver_stats& fs = solver->stats;
+        ++fs.refresh_requests;
+        fs.refreshed_at_age = fs.substeps_since_refresh;
+        fs.spent_before_refresh = r.iterations;
+        fs.wasted_iterations += r.iterations;
+        fs.refresh_requested = 1u;
+        solution = s.restart;
+        refreshFactor(*solver, s, factorYoungs, factorPoisson, effective.step, effective.inertia);
+        ++fs.refactors;
+        ++fs.retries;
+        ++fs.refactor_count;
+        ++fs.retry_count;
+        fs.factor_age = 0u;
+        fs.substeps_since_refresh = 0u;
+        s.frame = M3<R>(R(1));
+        s.factor = solver;
+        r = s.conjugateGradient(effective.inertia, effective.step, settings->cg_iterations, tolerance, solution);
+        fs.spent_after_refresh = r.iterations;
+        if (r.capped) {
+          ++fs.retries_failed;
+          fs.fresh_retry_failed = 1u;
+        }
+      }
+      passIterations += r.iterations;
+      if (solver) solver->stats.factor_applications += r.applications;  // recordCg: the result's own
       recordCg(r);
       return r;
     };
@@ -1316,7 +1591,7 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
       elastic = first.energy;
       report->yielding = first.yielding;
       balance(nullptr);
-      solvePrimary(s.acceleration);
+      solvePrimary(s.acceleration, true);
       for (uint32_t read = 1; read != ANCHORED_READS; ++read) {
         for (uint32_t n = 0; n < V; ++n) s.evaluated[n] = s.weighted[n] + reach * s.acceleration[n];
         const auto again = assemble(s.evaluated, R(0));
@@ -1324,7 +1599,7 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
         report->yielding = again.yielding;
         balance(&s.acceleration);
         std::fill(s.increment.begin(), s.increment.end(), V3<R>());
-        solvePrimary(s.increment);
+        solvePrimary(s.increment, false);
         for (uint32_t n = 0; n < V; ++n)
           if (!s.anchored[n]) s.acceleration[n] += s.increment[n];
       }
@@ -1372,7 +1647,7 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
               }
               balance(&s.total);
               std::fill(s.increment.begin(), s.increment.end(), V3<R>());
-              const auto solved = solvePrimary(s.increment);
+              const auto solved = solvePrimary(s.increment, false);
               spent += solved.iterations;
               ++solves;
               for (uint32_t n = 0; n < V; ++n)
@@ -1398,7 +1673,7 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
           loadingBefore = assembled.loading;
           if (attempt == 0u) s.increment = s.acceleration;
           else std::fill(s.increment.begin(), s.increment.end(), V3<R>());
-          const auto solved = solvePrimary(s.increment);
+          const auto solved = solvePrimary(s.increment, attempt == 0u);
           spent += solved.iterations;
           ++solves;
           R moved = 0, extent = 0;
@@ -1439,7 +1714,7 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
             balance(&s.total);
             if (read == 0u) s.increment = s.acceleration;
             else std::fill(s.increment.begin(), s.increment.end(), V3<R>());
-            const auto solved = solvePrimary(s.increment);
+            const auto solved = solvePrimary(s.increment, read == 0u);
             spent += solved.iterations;
             ++report->plastic_solves;
             for (uint32_t n = 0; n < V; ++n)
@@ -1476,6 +1751,10 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
         s.acceleration = s.total;
         break;
       }
+    }
+    if (solver) {  // solver.cc:4258-4263
+      ++solver->stats.substeps_since_refresh;
+      solver->meanIterations = 0.9f * solver->meanIterations + 0.1f * float(passIterations);
     }
     const R spanned = rule.beta * inner * inner;
     if (floating) {
@@ -1769,11 +2048,36 @@ int or_grid_build(const or_grid* grid, double* rest, double* node_mass, uint8_t*
   return int(t == T ? 0 : -1);
 }
 
+int or_step_solver(int precision, const or_mesh* mesh, or_state* state, const or_material* materials, uint32_t lanes,
+                   const or_settings* settings, const double gravity[3], double dt, or_report* report,
+                   or_solver* solver) {
+  if (!mesh || !state || !settings || !report) return -1;
+  return precision == OR_F32 ? stepImpl<float>(mesh, state, materials, lanes, settings, gravity, dt, report, solver)
+                             : stepImpl<double>(mesh, state, materials, lanes, settings, gravity, dt, report, solver);
+}
+
 int or_step(int precision, const or_mesh* mesh, or_state* state, const or_material* materials, uint32_t lanes,
             const or_settings* settings, const double gravity[3], double dt, or_report* report) {
-  if (!mesh || !state || !settings || !report) return -1;
-  return precision == OR_F32 ? stepImpl<float>(mesh, state, materials, lanes, settings, gravity, dt, report)
-                             : stepImpl<double>(mesh, state, materials, lanes, settings, gravity, dt, report);
+  return or_step_solver(precision, mesh, state, materials, lanes, settings, gravity, dt, report, nullptr);
+}
+
+or_solver* or_solver_create(uint32_t factor_budget) {
+  or_solver* s = new or_solver();
+  s->budget = factor_budget;
+  return s;
+}
+
+void or_solver_destroy(or_solver* solver) { delete solver; }
+
+int or_solver_get_stats(const or_solver* solver, or_solver_stats* out) {
+  if (!solver || !out) return -1;
+  *out = solver->stats;
+  out->mean_iterations = double(solver->meanIterations);
+  out->rows = 3u * solver->nodes;
+  out->ready = solver->ready ? 1u : 0u;
+  out->system_nonzeros = solver->systemNonZeros;
+  out->generation = solver->born;
+  return 0;
 }
 
 int or_tet_point_trial(int precision, const double* deformed, const double* rest, const double* rest_inverse,

@@ -129,6 +129,49 @@ int or_grid_build(const or_grid* grid, double* rest, double* node_mass,
                   double* volume, uint32_t* lane, uint32_t* grid_index);
 
 /* One talus::deformable::step (solver.cc:3472) with no contacts/partners. */
+/* A caller-held solver state (talus::deformable::DeformableSolverState,
+ * factor.h:205-210): the FP64 Cholesky preconditioner SystemFactor and its
+ * SolverStats.  factor_budget is Settings::factorBudget (solver.h:54). */
+typedef struct or_solver or_solver;
+
+typedef struct or_solver_stats {
+  /* SolverStats (factor.h:30-40) */
+  uint32_t factor_age;
+  uint32_t refactor_count;
+  uint32_t retry_count;
+  uint32_t substeps_since_refresh;
+  uint32_t refresh_requested;
+  uint32_t fresh_retry_failed;
+  double mean_iterations;
+  /* SystemFactor (factor.h:50-62) */
+  uint32_t rows;
+  uint32_t ready;
+  uint64_t system_nonzeros;
+  uint64_t generation;
+  /* StepReport's factor counters (solver.h:211-311): the counts summed over
+   * steps, the spent/refreshed figures as last set */
+  uint32_t refresh_requests;
+  uint32_t refactors;
+  uint32_t retries;
+  uint32_t retries_failed;
+  uint32_t wasted_iterations;
+  uint32_t spent_before_refresh;
+  uint32_t spent_after_refresh;
+  uint32_t refreshed_at_age;
+  uint32_t factor_applications;
+  uint32_t reserved;
+} or_solver_stats;
+
+or_solver* or_solver_create(uint32_t factor_budget);
+void or_solver_destroy(or_solver* solver);
+int or_solver_get_stats(const or_solver* solver, or_solver_stats* out);
+
+/* or_step with a solver state (NULL: or_step). */
+int or_step_solver(int precision, const or_mesh* mesh, or_state* state,
+                   const or_material* materials, uint32_t lanes,
+                   const or_settings* settings, const double gravity[3], double dt,
+                   or_report* report, or_solver* solver);
+
 int or_step(int precision, const or_mesh* mesh, or_state* state,
             const or_material* materials, uint32_t lanes,
             const or_settings* settings, const double gravity[3], double dt,

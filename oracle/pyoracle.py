@@ -108,6 +108,42 @@ class Report(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class SolverStats(C.Structure):
+    """or_solver_stats: SolverStats (factor.h:28-38), the SystemFactor's size
+    and the StepReport's factor counters."""
+    _fields_ = [(n, C.c_uint32) for n in ("factor_age", "refactor_count", "retry_count", "substeps_since_refresh",
+                                          "refresh_requested", "fresh_retry_failed")] + \
+               [("mean_iterations", C.c_double), ("rows", C.c_uint32), ("ready", C.c_uint32),
+                ("system_nonzeros", C.c_uint64), ("generation", C.c_uint64)] + \
+               [(n, C.c_uint32) for n in ("refresh_requests", "refactors", "retries", "retries_failed",
+                                          "wasted_iterations", "spent_before_refresh", "spent_after_refresh",
+                                          "refreshed_at_age", "factor_applications", "reserved")]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class Solver:
+    """A caller-held solver state (DeformableSolverState, factor.h:205-210)
+    with its FP64 Cholesky factor; factor_budget is Settings::factorBudget."""
+
+    def __init__(self, factor_budget: int = 32):
+        self.handle = lib().or_solver_create(factor_budget)
+
+    def stats(self) -> dict:
+        out = SolverStats()
+        lib().or_solver_get_stats(self.handle, C.byref(out))
+        return out.as_dict()
+
+    def close(self):
+        if self.handle:
+            lib().or_solver_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+
 class _Grid(C.Structure):
     _fields_ = [
         ("cells", C.c_uint32 * 3),
@@ -134,6 +170,12 @@ def lib():
         _lib.or_grid_build.argtypes = [C.POINTER(_Grid)] + [C.c_void_p] * 8
         _lib.or_step.argtypes = [C.c_int, C.POINTER(_Mesh), C.POINTER(_State), C.POINTER(Material), C.c_uint32,
                                  C.POINTER(_Settings), C.c_void_p, C.c_double, C.POINTER(Report)]
+        _lib.or_step_solver.argtypes = list(_lib.or_step.argtypes) + [C.c_void_p]
+        _lib.or_solver_create.argtypes = [C.c_uint32]
+        _lib.or_solver_create.restype = C.c_void_p
+        _lib.or_solver_destroy.argtypes = [C.c_void_p]
+        _lib.or_solver_destroy.restype = None
+        _lib.or_solver_get_stats.argtypes = [C.c_void_p, C.POINTER(SolverStats)]
         _lib.or_tet_point_trial.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                             C.POINTER(Material), C.c_void_p, C.c_double, C.c_int, C.c_int,
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -247,7 +289,7 @@ class Settings:
 
 
 def step(precision: int, mesh: Mesh, state: State, materials, settings: Settings, gravity=(0.0, -9.81, 0.0),
-         dt=1.0 / 60.0, report: Report | None = None) -> Report:
+         dt=1.0 / 60.0, report: Report | None = None, solver: "Solver | None" = None) -> Report:
     for a in (state.position, state.velocity, state.acceleration, state.rotation, state.plastic):
         assert a.dtype == np.float64 and a.flags.c_contiguous
     m = _Mesh(mesh.nodes, mesh.tets, _ptr(mesh.rest), _ptr(mesh.node_mass), _ptr(mesh.anchored),
@@ -260,8 +302,8 @@ def step(precision: int, mesh: Mesh, state: State, materials, settings: Settings
                    settings.tolerance, settings.spectral_radius, settings.rigid_split, settings.plasticity)
     g = np.asarray(gravity, dtype=np.float64)
     rep = report if report is not None else Report()
-    rc = lib().or_step(precision, C.byref(m), C.byref(s), mats, len(materials), C.byref(st), _ptr(g), dt,
-                       C.byref(rep))
+    rc = lib().or_step_solver(precision, C.byref(m), C.byref(s), mats, len(materials), C.byref(st), _ptr(g), dt,
+                              C.byref(rep), solver.handle if solver is not None else None)
     if rc != 0:
         raise RuntimeError(f"or_step failed: {rc}")
     return rep

@@ -123,6 +123,22 @@ class tl_step_report(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class tl_factor_stats(C.Structure):
+    """SolverStats (factor.h:28-38), the SystemFactor's size and the
+    StepReport factor counters of a system's solver state."""
+    _fields_ = [(n, C.c_uint32) for n in ("factor_age", "refactor_count", "retry_count", "substeps_since_refresh",
+                                          "refresh_requested", "fresh_retry_failed")] + \
+               [("mean_iterations", C.c_double), ("rows", C.c_uint32), ("ready", C.c_uint32),
+                ("system_nonzeros", C.c_uint64), ("generation", C.c_uint64)] + \
+               [(n, C.c_uint32) for n in ("refresh_requests", "refactors", "retries", "retries_failed",
+                                          "wasted_iterations", "spent_before_refresh", "spent_after_refresh",
+                                          "refreshed_at_age", "factor_applications", "reserved")] + \
+               [("factor_nonzeros", C.c_uint64), ("refactor_seconds", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+
+
 class tl_rollout_desc(C.Structure):
     _fields_ = [
         ("steps", C.c_uint32),
@@ -154,6 +170,8 @@ SIGNATURES = {
     "tl_host_register": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_size_t]),
     "tl_host_unregister": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "tl_system_set_solver": (C.c_int32, [C.c_void_p, C.c_uint32]),
+    "tl_system_use_factor": (C.c_int32, [C.c_void_p, C.c_uint32, C.c_uint32]),
+    "tl_system_factor_stats": (C.c_int32, [C.c_void_p, C.POINTER(tl_factor_stats)]),
     "tl_system_set_plasticity": (C.c_int32, [C.c_void_p, C.c_uint32]),
     "tl_ctx_check_wait_limit": (C.c_int32, [C.c_void_p]),
     "tl_system_expire_wait": (C.c_int32, [C.c_void_p, C.c_int32]),

@@ -1,0 +1,364 @@
+// tl_factor.cuh -- the caller-held Cholesky preconditioner on the device.
+//
+// A system with a solver state (DeformableSolverState, factor.h:205-210)
+// preconditions its PCG with the FP64 factor of
+//   A = (1 - alpha_m) M + h^2 sum_e R_e K_e R_e^T   (anchored rows: identity)
+// made at the rotations and positions of its last refresh (SystemFactor,
+// factor.cc:318-460, 567-618), applied in the frame that turns the body from
+// those positions to the current ones (applyFactor, factor.cc:669-704;
+// bodyRotation, factor.cc:620-667).  The factor is L with P A P^T = L L^T
+// in 3x3 node blocks under a nested-dissection order P, made on the host.
+//
+// Kernels:
+//   kFactorFrame  (one block) the body rotation: polar of the mass-weighted
+//                 correlation of the positions now with the factor's
+//   kPcgFactor    persistent cooperative PCG in the reference's order with
+//                 the factor as preconditioner, operator = the assembled block
+//                 matrix of kSellAssemble.  The two triangular solves of each
+//                 application run inside the launch: every warp takes node
+//                 rows by an atomic ticket, forward rows in increasing order,
+//                 then backward rows in decreasing order, and waits (bounded)
+//                 for the flags of the rows its row reads.  Rows are handed out
+//                 only to running warps in dependency order, so the smallest
+//                 unfinished ticket can always finish.
+#pragma once
+
+#include "tl_sell.cuh"
+
+namespace tl {
+
+// The factor in the layout of the two triangular solves, FP64.
+struct FactorDev {
+  uint32_t nodes;
+  const uint32_t* perm;       // [nodes] factor order -> node
+  const uint32_t* iperm;      // [nodes] node -> factor order
+  const uint32_t* row_start;  // [nodes + 1] strictly lower blocks of row i of L
+  const uint32_t* row_col;    // [row blocks] their columns
+  const double* row_blk;      // [9 per block] L_ij row-major
+  const uint32_t* col_start;  // [nodes + 1] strictly lower blocks of column i of L
+  const uint32_t* col_row;    // [col blocks] their rows
+  const double* col_blk;      // [9 per block] L_ji row-major
+  const double* diag_inv;     // [9 per node] L_ii^-1 row-major (lower triangular)
+  Vec4<double>* y;            // [nodes] forward solve
+  Vec4<double>* w;            // [nodes] backward solve
+  uint32_t* fwd_flag;         // [nodes] application epoch of y
+  uint32_t* bwd_flag;         // [nodes] application epoch of w
+  uint32_t* ticket;           // [3] row tickets, by application mod 3
+  uint32_t* epoch;            // [1] applications made so far (flags start at 0)
+  const double* frame;        // [9] row-major rotation the factor is applied in
+  double* part;               // [8 G] block partials, two halves
+};
+
+__device__ __forceinline__ void stRelease(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Bounded wait for flag == epoch.  Gives up after TL_BARRIER_LIMIT_NS
+// (recording TL_ERR_TIMEOUT) or once another wait or barrier has given up.
+__device__ __forceinline__ bool waitFlag(const uint32_t* flag, uint32_t epoch, GridSyncDev* sync) {
+  if (ldAcquire(flag) == epoch) return true;
+  const unsigned long long t0 = globalTimer();
+  unsigned int polls = 0;
+  while (ldAcquire(flag) != epoch) {
+    if ((++polls & 255u) == 0u) {
+      if (*(volatile int*)&sync->error != 0) return false;
+      if (globalTimer() - t0 > TL_BARRIER_LIMIT_NS) {
+        atomicExch(&sync->error, 5);  // TL_ERR_TIMEOUT
+        return false;
+      }
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ V3<double> warpSum3(V3<double> v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    v.x += __shfl_xor_sync(0xffffffffu, v.x, o);
+    v.y += __shfl_xor_sync(0xffffffffu, v.y, o);
+    v.z += __shfl_xor_sync(0xffffffffu, v.z, o);
+  }
+  return v;
+}
+
+// z = frame (L L^T)^-1 P (frame^T r) of applyFactor, y and w in factor order;
+// every warp of the grid takes part.  r is read at the forward rows (written
+// before the launch's last grid barrier); the caller turns w back.
+template <class S>
+__device__ void factorSolve(const FactorDev& f, GridSyncDev* sync, const Vec4<S>* r, const M3<S>& frame,
+                            uint32_t epoch, uint32_t* ticket) {
+  const uint32_t lane = threadIdx.x & 31u, V = f.nodes;
+  bool ok = true;
+  for (;;) {
+    uint32_t t = 0;
+    if (lane == 0) t = atomicAdd(ticket, 1u);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= 2u * V) break;
+    V3<double> acc = {0, 0, 0};
+    if (t < V) {  // forward row i: y_i = L_ii^-1 (b_i - sum_j L_ij y_j)
+      const uint32_t i = t, k1 = __ldg(&f.row_start[i + 1]);
+      for (uint32_t k = __ldg(&f.row_start[i]) + lane; k < k1; k += 32u) {
+        const uint32_t j = __ldg(&f.row_col[k]);
+        ok = ok && waitFlag(&f.fwd_flag[j], epoch, sync);
+        const Vec4<double> yj = ld4cg(&f.y[j]);
+        const double* L = f.row_blk + size_t(9) * k;
+        acc.x += __ldg(L) * yj.x + __ldg(L + 1) * yj.y + __ldg(L + 2) * yj.z;
+        acc.y += __ldg(L + 3) * yj.x + __ldg(L + 4) * yj.y + __ldg(L + 5) * yj.z;
+        acc.z += __ldg(L + 6) * yj.x + __ldg(L + 7) * yj.y + __ldg(L + 8) * yj.z;
+      }
+      acc = warpSum3(acc);
+      if (lane == 0) {
+        const uint32_t o = __ldg(&f.perm[i]);
+        const V3<S> turned = mulT(frame, xyz(ld4cg(&r[o])));  // frame^T r in the step's arithmetic
+        const V3<double> b = cvt<double>(turned) - acc;
+        const double* D = f.diag_inv + size_t(9) * i;
+        const V3<double> y = {__ldg(D) * b.x, __ldg(D + 3) * b.x + __ldg(D + 4) * b.y,
+                              __ldg(D + 6) * b.x + __ldg(D + 7) * b.y + __ldg(D + 8) * b.z};
+        f.y[i] = Vec4<double>{y.x, y.y, y.z, 0.0};
+        stRelease(&f.fwd_flag[i], epoch);
+      }
+    } else {  // backward row i: w_i = L_ii^-T (y_i - sum_{j > i} L_ji^T w_j)
+      const uint32_t i = 2u * V - 1u - t, k1 = __ldg(&f.col_start[i + 1]);
+      for (uint32_t k = __ldg(&f.col_start[i]) + lane; k < k1; k += 32u) {
+        const uint32_t j = __ldg(&f.col_row[k]);
+        ok = ok && waitFlag(&f.bwd_flag[j], epoch, sync);
+        const Vec4<double> wj = ld4cg(&f.w[j]);
+        const double* L = f.col_blk + size_t(9) * k;
+        acc.x += __ldg(L) * wj.x + __ldg(L + 3) * wj.y + __ldg(L + 6) * wj.z;
+        acc.y += __ldg(L + 1) * wj.x + __ldg(L + 4) * wj.y + __ldg(L + 7) * wj.z;
+        acc.z += __ldg(L + 2) * wj.x + __ldg(L + 5) * wj.y + __ldg(L + 8) * wj.z;
+      }
+      acc = warpSum3(acc);
+      if (lane == 0) {
+        ok = ok && waitFlag(&f.fwd_flag[i], epoch, sync);
+        const Vec4<double> yi = ld4cg(&f.y[i]);
+        const V3<double> b = {yi.x - acc.x, yi.y - acc.y, yi.z - acc.z};
+        const double* D = f.diag_inv + size_t(9) * i;
+        const V3<double> w = {__ldg(D) * b.x + __ldg(D + 3) * b.y + __ldg(D + 6) * b.z,
+                              __ldg(D + 4) * b.y + __ldg(D + 7) * b.z, __ldg(D + 8) * b.z};
+        f.w[i] = Vec4<double>{w.x, w.y, w.z, 0.0};
+        stRelease(&f.bwd_flag[i], epoch);
+      }
+    }
+  }
+  (void)ok;  // a wait that gave up has recorded it; the next grid barrier ends the launch
+}
+
+// bodyRotation (factor.cc:620-667) of one body (nodes [0, V)): the polar
+// rotation of sum_n m_n (x_n - c)(x0_n - c0)^T, x = rest + u now, x0 the
+// positions at the refresh and c, c0 the mass-weighted centres.  One block.
+template <class S>
+__global__ void __launch_bounds__(TILE) kFactorFrame(Sys<S> s, uint32_t V, const Vec4<double>* ref, double* frame) {
+  __shared__ double centre[3];
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (uint32_t n = threadIdx.x; n < V; n += TILE) {
+    const Vec4<S> r4 = s.rest4[n], u = s.u[n];
+    const double m = double(r4.w);
+    v[0] += m;
+    v[1] += m * (double(r4.x) + double(u.x));
+    v[2] += m * (double(r4.y) + double(u.y));
+    v[3] += m * (double(r4.z) + double(u.z));
+  }
+  blockSum<4>(v);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) centre[k] = v[0] > 0.0 ? v[k + 1] / v[0] : v[k + 1];
+  __syncthreads();
+  // ref[V] holds the centre of the refresh positions
+  const Vec4<double> c0 = ref[V];
+  double c[9];
+  for (int k = 0; k < 9; ++k) c[k] = 0.0;
+  for (uint32_t n = threadIdx.x; n < V; n += TILE) {
+    const Vec4<S> r4 = s.rest4[n], u = s.u[n];
+    const Vec4<double> x0 = ref[n];
+    const double m = double(r4.w);
+    const double now[3] = {double(r4.x) + double(u.x) - centre[0], double(r4.y) + double(u.y) - centre[1],
+                           double(r4.z) + double(u.z) - centre[2]};
+    const double before[3] = {x0.x - c0.x, x0.y - c0.y, x0.z - c0.z};
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) c[3 * i + j] += m * now[i] * before[j];
+  }
+  blockSum<9>(c);
+  if (threadIdx.x == 0) {
+    M3<double> corr;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) corr.m[i][j] = c[3 * i + j];
+    const M3<double> rot = polarRotation(corr);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) frame[3 * i + j] = rot.m[i][j];
+  }
+}
+
+// Sum of N doubles over the grid: block partials into half `h` of part, a
+// grid barrier, then the same block-ordered sum in every block.
+template <int N>
+__device__ __forceinline__ bool gridSum(double (&v)[N], double* part, uint32_t& h, GridSyncDev* sync,
+                                        unsigned int& bar, double (&out)[N]) {
+  double* half = part + size_t(4) * gridDim.x * (h++ & 1u);
+  blockSum<N>(v);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < N; ++k) half[size_t(k) * gridDim.x + blockIdx.x] = v[k];
+  if (!countBarrier(sync, bar)) return false;
+  sumBlocksAll<N>(half, out);
+  return true;
+}
+
+// Persistent PCG of one body preconditioned by the factor (conjugateGradient,
+// solver.cc:1904-2089, with condition = applyFactor): the reference's order,
+// loop-top stopping test, breakdown test and cap.  Vectors live in global
+// memory (x in X; r, d, q, z in the four planes given); rows are the
+// assembled matrix's, a warp per 32-row slice, grid-strided; dots are FP64.
+template <class S>
+__global__ void __launch_bounds__(TILE) kPcgFactor(Sys<S> s, SellDev<S> g, FactorDev f, Vec4<S>* X, Vec4<S>* R,
+                                                   Vec4<S>* D, Vec4<S>* Q, Vec4<S>* Z, uint32_t x0zero, uint32_t limit) {
+  const uint32_t warps = gridDim.x * (TILE / 32u), gw = blockIdx.x * (TILE / 32u) + (threadIdx.x >> 5);
+  const uint32_t lane = threadIdx.x & 31u;
+  const BodyStepDev st = s.step[0];
+  g.col_cache = 0;  // columns from global memory
+  M3<S> frame;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) frame.m[i][j] = S(__ldcg(&f.frame[3 * i + j]));
+  const uint32_t epoch0 = __ldcg(f.epoch);
+  if (blockIdx.x == 0 && threadIdx.x < 3) f.ticket[threadIdx.x] = 0u;
+  unsigned int bar = 0;
+  uint32_t h = 0, apps = 0;
+  // the rows of this thread: slices gw, gw + warps, ...; lane = row in slice
+  auto forRows = [&](auto&& fn) {
+    for (uint32_t slice = gw; slice < g.slices; slice += warps) {
+      const uint32_t row = slice * SELL_ROWS + lane;
+      fn(slice, row, row < g.rows && !s.anch[row], row < g.rows);
+    }
+  };
+  auto matvec = [&](uint32_t slice, const Vec4<S>* in) {
+    return sellRowOf<S, Ld4cg<S>, sellRowGroup<S>(), false>(g, slice, lane, ld4cgOf(in), nullptr);
+  };
+  // one application: z = frame (LL^T)^-1 frame^T r, anchored rows zero
+  auto condition = [&](double& rz, double& rr) -> bool {
+    if (blockIdx.x == 0 && threadIdx.x == 0) f.ticket[(apps + 1u) % 3u] = 0u;
+    factorSolve<S>(f, s.sync, R, frame, epoch0 + apps + 1u, &f.ticket[apps % 3u]);
+    ++apps;
+    if (!countBarrier(s.sync, bar)) return false;
+    rz = 0.0;
+    rr = 0.0;
+    forRows([&](uint32_t, uint32_t row, bool freeRow, bool live) {
+      if (!live) return;
+      V3<S> z = {0, 0, 0};
+      if (freeRow) {
+        const Vec4<double> w = ld4cg(&f.w[__ldg(&f.iperm[row])]);
+        z = mul(frame, V3<S>{S(w.x), S(w.y), S(w.z)});
+      }
+      Z[row] = pack(z);
+      const V3<double> r = cvt<double>(xyz(R[row])), zd = cvt<double>(z);
+      rz += dot(r, zd);
+      rr += dot(r, r);
+    });
+    return true;
+  };
+  // ---- r = right - A x (anchored rows 0), |right|
+  double v0[1] = {0.0};
+  forRows([&](uint32_t slice, uint32_t row, bool freeRow, bool live) {
+    V3<double> r = {0, 0, 0};
+    const V3<double> rhs = live ? cvt<double>(xyz(s.right[row])) : V3<double>{0, 0, 0};
+    if (x0zero) {
+      if (live) X[row] = Vec4<S>{0, 0, 0, 0};
+      if (freeRow) r = rhs;
+    } else {
+      const V3<double> ax = matvec(slice, X);
+      if (freeRow) r = rhs - ax;
+    }
+    if (live) {
+      R[row] = pack(cvt<S>(r));
+      v0[0] += dot(rhs, rhs);
+    }
+  });
+  double refSq[1];
+  if (!gridSum<1>(v0, f.part, h, s.sync, bar, refSq)) return;
+  const double reference = sqrt(refSq[0]);
+  double rz = 0.0, rr = 0.0;
+  if (!condition(rz, rr)) return;
+  forRows([&](uint32_t, uint32_t row, bool, bool live) {
+    if (live) D[row] = Z[row];
+  });
+  double v1[2] = {rz, rr}, s1[2];
+  if (!gridSum<2>(v1, f.part, h, s.sync, bar, s1)) return;
+  double squared = s1[0], length = s1[1];
+  const double floor = fmax(reference, 1.1754943508222875e-38);  // std::numeric_limits<float>::min()
+  const double target = st.tolerance * floor;
+  const double startRes = sqrt(length) / floor;
+  double stride = 0.0, blend = 0.0;
+  uint32_t taken = 0;
+  for (uint32_t iteration = 0; iteration != limit; ++iteration) {
+    if (sqrt(length) <= target) break;
+    double vc[1] = {0.0}, curv[1];
+    forRows([&](uint32_t slice, uint32_t row, bool freeRow, bool live) {
+      const V3<double> q = matvec(slice, D);
+      if (!live) return;
+      const V3<S> qs = freeRow ? cvt<S>(q) : V3<S>{0, 0, 0};
+      Q[row] = pack(qs);
+      vc[0] += dot(cvt<double>(xyz(D[row])), cvt<double>(qs));
+    });
+    if (!gridSum<1>(vc, f.part, h, s.sync, bar, curv)) return;
+    if (!(curv[0] > 0.0) || !(squared > 0.0)) break;
+    stride = squared / curv[0];
+    forRows([&](uint32_t, uint32_t row, bool, bool live) {
+      if (!live) return;
+      const V3<double> d = cvt<double>(xyz(D[row]));
+      X[row] = pack(cvt<S>(cvt<double>(xyz(X[row])) + stride * d));
+      R[row] = pack(cvt<S>(cvt<double>(xyz(R[row])) - stride * cvt<double>(xyz(Q[row]))));
+    });
+    if (!countBarrier(s.sync, bar)) return;
+    if (!condition(rz, rr)) return;
+    double vn[2] = {rz, rr}, sn[2];
+    if (!gridSum<2>(vn, f.part, h, s.sync, bar, sn)) return;
+    blend = sn[0] / squared;
+    squared = sn[0];
+    length = sn[1];
+    forRows([&](uint32_t, uint32_t row, bool, bool live) {
+      if (!live) return;
+      D[row] = pack(cvt<S>(cvt<double>(xyz(Z[row])) + blend * cvt<double>(xyz(D[row]))));
+    });
+    ++taken;
+    if (!countBarrier(s.sync, bar)) return;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const double residual = sqrt(length);
+    CgBodyDev c;
+    c.squared = squared;
+    c.target = target;
+    c.floor = floor;
+    c.length = length;
+    c.stride = stride;
+    c.blend = blend;
+    c.start_res = startRes;
+    c.rel_res = residual / floor;
+    c.taken = taken;
+    c.done = 1u;
+    c.pad0 = (taken == limit && residual > target) ? 1u : 0u;  // capped
+    c.pad1 = apps;                                               // factor applications
+    s.cg[0] = c;
+    *f.epoch = epoch0 + apps;
+  }
+}
+
+// The report of a finished factored solve (the recordCg of solver.cc:3621-3637
+// for the result solvePrimary returns), as kPcgSell writes it.
+template <class S>
+__global__ void kFactorRecord(Sys<S> s, uint32_t tangent) {
+  const CgBodyDev c = s.cg[0];
+  CgReportDev rep = s.cgrep[0];
+  rep.iterations += c.taken;
+  rep.capped += c.pad0;
+  rep.applications += c.taken + 1u;
+  rep.solves += 1u;
+  rep.tangent_iterations += tangent ? c.taken : 0u;
+  rep.worst_rel = fmax(rep.worst_rel, c.rel_res);
+  if (rep.pass_solves == 0u) rep.pass_start = c.start_res;
+  rep.pass_end = c.rel_res;
+  rep.pass_iterations += c.taken;
+  rep.pass_solves += 1u;
+  s.cgrep[0] = rep;
+}
+
+}  // namespace tl

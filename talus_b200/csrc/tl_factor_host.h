@@ -1,0 +1,246 @@
+// tl_factor_host.h -- the block Cholesky factor of a solver state, made on the host.
+//
+// The system of SystemFactor (factor.cc:318-460) in 3x3 node blocks:
+//   A_nn = (1 - alpha_m) m_n I + sum_e h^2 R K_nn R^T, A_nm = sum_e h^2 R K_nm R^T
+// over free nodes, anchored nodes carrying the identity and no coupling.
+// The reference factors it with Eigen's SimplicialLLT under an AMD ordering
+// (factor.cc:302-314); here a nested dissection of the node graph by
+// coordinate bisection orders it, the elimination tree and row patterns are
+// found once per mesh (analyze), and the numeric factor is an up-looking
+// block Cholesky, row by row (factor).  L L^T equals P A P^T to rounding
+// whatever the order, so the applied inverse is the reference's.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <numeric>
+#include <vector>
+
+namespace tl {
+
+struct BlockFactor {
+  uint32_t nodes = 0;
+  bool analyzed = false, ready = false;
+  uint64_t systemNonZeros = 0;  // stored entries of the full scalar system, as the reference counts them
+  std::vector<uint32_t> perm, iperm;          // factor order -> node, node -> factor order
+  std::vector<uint32_t> rowStart, rowCol;     // strictly lower blocks of L by rows, columns ascending
+  std::vector<uint32_t> colStart, colRow;     // the same blocks by columns, rows ascending
+  std::vector<double> rowBlk, colBlk, diagInv;  // [9 per block] row-major; L_ii^-1 per node
+
+  uint64_t factorNonZeros() const {  // scalar entries of L: 9 per off-diagonal block, 6 per diagonal block
+    return ready ? uint64_t(9) * rowCol.size() + uint64_t(6) * nodes : 0u;
+  }
+
+  // Order and symbolic factor of a mesh: tets [4 T] node ids, rest [3 V].
+  void analyze(uint32_t V, const uint8_t* anchored, const std::vector<uint32_t>& tets, const double* rest) {
+    nodes = V;
+    const size_t T = tets.size() / 4;
+    // free-free couplings, both directions, without the node itself
+    std::vector<std::vector<uint32_t>> adj(V);
+    for (size_t e = 0; e < T; ++e)
+      for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b) {
+          const uint32_t na = tets[4 * e + a], nb = tets[4 * e + b];
+          if (na != nb && !anchored[na] && !anchored[nb]) adj[na].push_back(nb);
+        }
+    uint64_t stored = 0;
+    for (uint32_t v = 0; v < V; ++v) {
+      auto& l = adj[v];
+      std::sort(l.begin(), l.end());
+      l.erase(std::unique(l.begin(), l.end()), l.end());
+      stored += 9u * l.size() + (anchored[v] ? 3u : 9u);
+    }
+    // a free node outside every tet holds its 3 diagonal entries only
+    std::vector<uint8_t> inTet(V, 0);
+    for (size_t e = 0; e < T; ++e)
+      for (int a = 0; a < 4; ++a) inTet[tets[4 * e + a]] = 1;
+    for (uint32_t v = 0; v < V; ++v)
+      if (!anchored[v] && !inTet[v]) stored -= 6u;
+    systemNonZeros = stored;
+    // ---- order: anchored nodes first (they couple to nothing), then nested dissection
+    perm.clear();
+    perm.reserve(V);
+    std::vector<uint32_t> free;
+    for (uint32_t v = 0; v < V; ++v) (anchored[v] ? perm : free).push_back(v);
+    std::vector<uint32_t> mark(V, 0u);
+    uint32_t stamp = 0;
+    dissect(free, adj, rest, mark, stamp);
+    iperm.assign(V, 0u);
+    for (uint32_t i = 0; i < V; ++i) iperm[perm[i]] = i;
+    // ---- elimination tree (Liu, with path compression) and row patterns
+    std::vector<std::vector<uint32_t>> lower(V);  // neighbours of i earlier in the order
+    for (uint32_t v = 0; v < V; ++v)
+      for (uint32_t w : adj[v])
+        if (iperm[w] < iperm[v]) lower[iperm[v]].push_back(iperm[w]);
+    const uint32_t NONE = ~0u;
+    std::vector<uint32_t> parent(V, NONE), ancestor(V, NONE);
+    for (uint32_t i = 0; i < V; ++i)
+      for (uint32_t k : lower[i]) {
+        uint32_t r = k;
+        while (ancestor[r] != NONE && ancestor[r] != i) {
+          const uint32_t next = ancestor[r];
+          ancestor[r] = i;
+          r = next;
+        }
+        if (ancestor[r] == NONE) {
+          ancestor[r] = i;
+          parent[r] = i;
+        }
+      }
+    rowStart.assign(V + 1, 0u);
+    rowCol.clear();
+    std::vector<uint32_t> seen(V, NONE), pattern;
+    for (uint32_t i = 0; i < V; ++i) {
+      pattern.clear();
+      seen[i] = i;
+      for (uint32_t k : lower[i])
+        for (uint32_t r = k; seen[r] != i; r = parent[r]) {  // the path up to a node already reached
+          seen[r] = i;
+          pattern.push_back(r);
+        }
+      std::sort(pattern.begin(), pattern.end());
+      rowCol.insert(rowCol.end(), pattern.begin(), pattern.end());
+      rowStart[i + 1] = uint32_t(rowCol.size());
+    }
+    // ---- the column view
+    colStart.assign(V + 1, 0u);
+    for (uint32_t c : rowCol) ++colStart[c + 1];
+    for (uint32_t i = 0; i < V; ++i) colStart[i + 1] += colStart[i];
+    colRow.assign(rowCol.size(), 0u);
+    std::vector<uint32_t> fill(colStart.begin(), colStart.end() - 1);
+    for (uint32_t i = 0; i < V; ++i)
+      for (uint32_t k = rowStart[i]; k < rowStart[i + 1]; ++k) colRow[fill[rowCol[k]]++] = i;
+    analyzed = true;
+  }
+
+  // Nested dissection of a free node set: split at the median of the widest
+  // coordinate, the separator being the lower side's nodes that touch the
+  // upper side; the two sides first, the separator last.
+  void dissect(std::vector<uint32_t>& set, const std::vector<std::vector<uint32_t>>& adj, const double* rest,
+               std::vector<uint32_t>& mark, uint32_t& stamp) {
+    constexpr size_t LEAF = 64;
+    if (set.size() <= LEAF) {
+      perm.insert(perm.end(), set.begin(), set.end());
+      return;
+    }
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (uint32_t v : set)
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], rest[3 * size_t(v) + k]);
+        hi[k] = std::max(hi[k], rest[3 * size_t(v) + k]);
+      }
+    int axis = 0;
+    for (int k = 1; k < 3; ++k)
+      if (hi[k] - lo[k] > hi[axis] - lo[axis]) axis = k;
+    const size_t half = set.size() / 2;
+    std::nth_element(set.begin(), set.begin() + half, set.end(), [&](uint32_t a, uint32_t b) {
+      const double ca = rest[3 * size_t(a) + axis], cb = rest[3 * size_t(b) + axis];
+      return ca < cb || (ca == cb && a < b);
+    });
+    const uint32_t upper = ++stamp;
+    for (size_t k = half; k < set.size(); ++k) mark[set[k]] = upper;
+    std::vector<uint32_t> left, right(set.begin() + half, set.end()), sep;
+    for (size_t k = 0; k < half; ++k) {
+      const uint32_t v = set[k];
+      bool touches = false;
+      for (uint32_t w : adj[v])
+        if (mark[w] == upper) {
+          touches = true;
+          break;
+        }
+      (touches ? sep : left).push_back(v);
+    }
+    std::vector<uint32_t>().swap(set);
+    dissect(left, adj, rest, mark, stamp);
+    dissect(right, adj, rest, mark, stamp);
+    perm.insert(perm.end(), sep.begin(), sep.end());
+  }
+
+  // Numeric factor.  diag [9 V] and the element blocks blocks[16 per tet][9]
+  // (row-major, block (a, b) of tet e at 16 e + 4 a + b) in node numbering;
+  // couplings that touch an anchored node are left out.  False when a pivot
+  // block is not positive definite (SimplicialLLT's NumericalIssue).
+  bool factor(const uint8_t* anchored, const std::vector<uint32_t>& tets, const std::vector<double>& blocks,
+              const std::vector<double>& diag) {
+    const uint32_t V = nodes;
+    const size_t T = tets.size() / 4;
+    rowBlk.assign(size_t(9) * rowCol.size(), 0.0);
+    colBlk.assign(size_t(9) * rowCol.size(), 0.0);
+    diagInv.assign(size_t(9) * V, 0.0);
+    std::vector<double> permDia(size_t(9) * V);
+    for (uint32_t v = 0; v < V; ++v) std::copy_n(&diag[9 * size_t(v)], 9, &permDia[9 * size_t(iperm[v])]);
+    // the lower blocks of P A P^T into their places in the row pattern
+    for (size_t e = 0; e < T; ++e)
+      for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b) {
+          const uint32_t na = tets[4 * e + a], nb = tets[4 * e + b];
+          if (anchored[na] || anchored[nb]) continue;
+          const uint32_t i = iperm[na], j = iperm[nb];
+          const double* B = &blocks[9 * (16 * e + 4 * a + b)];
+          if (i == j) {
+            for (int q = 0; q < 9; ++q) permDia[9 * size_t(i) + q] += B[q];
+          } else if (j < i) {
+            const uint32_t* c0 = &rowCol[rowStart[i]];
+            const uint32_t k = rowStart[i] + uint32_t(std::lower_bound(c0, c0 + (rowStart[i + 1] - rowStart[i]), j) - c0);
+            for (int q = 0; q < 9; ++q) rowBlk[9 * size_t(k) + q] += B[q];
+          }
+        }
+    std::vector<uint32_t> where(V, 0u), colFill(colStart.begin(), colStart.end() - 1);
+    for (uint32_t i = 0; i < V; ++i) {
+      const uint32_t k0 = rowStart[i], k1 = rowStart[i + 1];
+      for (uint32_t k = k0; k < k1; ++k) where[rowCol[k]] = k;
+      double d[9];
+      std::copy_n(&permDia[9 * size_t(i)], 9, d);
+      for (uint32_t k = k0; k < k1; ++k) {
+        const uint32_t j = rowCol[k];
+        double* x = &rowBlk[9 * size_t(k)];
+        // L_ij = x_j L_jj^-T
+        const double* Di = &diagInv[9 * size_t(j)];
+        double l[9];
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) l[3 * r + c] = x[3 * r] * Di[3 * c] + x[3 * r + 1] * Di[3 * c + 1] + x[3 * r + 2] * Di[3 * c + 2];
+        std::copy_n(l, 9, x);
+        // x_m -= L_ij L_mj^T for the rows m of column j before i
+        for (uint32_t p = colStart[j]; p < colFill[j]; ++p) {
+          double* xm = &rowBlk[9 * size_t(where[colRow[p]])];
+          const double* lm = &colBlk[9 * size_t(p)];
+          for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c)
+              xm[3 * r + c] -= l[3 * r] * lm[3 * c] + l[3 * r + 1] * lm[3 * c + 1] + l[3 * r + 2] * lm[3 * c + 2];
+        }
+        // D -= L_ij L_ij^T
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) d[3 * r + c] -= l[3 * r] * l[3 * c] + l[3 * r + 1] * l[3 * c + 1] + l[3 * r + 2] * l[3 * c + 2];
+      }
+      // L_ii = chol(D), lower; its inverse
+      double L[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      if (!(d[0] > 0.0)) return ready = false;
+      L[0] = std::sqrt(d[0]);
+      L[3] = d[3] / L[0];
+      L[6] = d[6] / L[0];
+      const double d4 = d[4] - L[3] * L[3];
+      if (!(d4 > 0.0)) return ready = false;
+      L[4] = std::sqrt(d4);
+      L[7] = (d[7] - L[6] * L[3]) / L[4];
+      const double d8 = d[8] - L[6] * L[6] - L[7] * L[7];
+      if (!(d8 > 0.0)) return ready = false;
+      L[8] = std::sqrt(d8);
+      double* I = &diagInv[9 * size_t(i)];
+      I[0] = 1.0 / L[0];
+      I[4] = 1.0 / L[4];
+      I[8] = 1.0 / L[8];
+      I[3] = -L[3] * I[0] / L[4];
+      I[7] = -L[7] * I[4] / L[8];
+      I[6] = -(L[6] * I[0] + L[7] * I[3]) / L[8];
+      // row i's blocks join their columns
+      for (uint32_t k = k0; k < k1; ++k) {
+        const uint32_t p = colFill[rowCol[k]]++;
+        std::copy_n(&rowBlk[9 * size_t(k)], 9, &colBlk[9 * size_t(p)]);
+      }
+    }
+    return ready = true;
+  }
+};
+
+}  // namespace tl

@@ -10,9 +10,12 @@
 #include "tl_floating.cuh"
 #include "tl_sell.cuh"
 #include "tl_sell_build.h"
+#include "tl_factor.cuh"
+#include "tl_factor_host.h"
 #include "tl_validate.h"
 
 #include <algorithm>
+#include <chrono>
 #include <condition_variable>
 #include <functional>
 #include <mutex>
@@ -254,6 +257,8 @@ struct SystemBase {
   virtual void tune(uint32_t blocksPerSm, uint32_t graph) = 0;
   virtual void tuneShape(uint32_t knob, uint32_t value) = 0;
   virtual void setSolver(uint32_t form) = 0;
+  virtual void useFactor(uint32_t enable, uint32_t budget) = 0;
+  virtual void factorStats(tl_factor_stats* out) = 0;
   virtual void setPlasticity(uint32_t mode) = 0;
   virtual void expireWait(int32_t solve) = 0;
   virtual bool plasticUsed(uint32_t law) const = 0;
@@ -724,6 +729,15 @@ struct System final : SystemBase {
         if (hTau[e] != S(0)) hasDamping = true;
         if (hMat[laneBase + l].yields) h.anyYields = true;
         if (hasEyoung) hE[e] = d.element_youngs ? d.element_youngs[t] : hMat[laneBase + l].youngs;
+        if (b == 0) {  // the first body's mesh, for a solver state's factor
+          for (int k = 0; k < 4; ++k) fTets.push_back(d.tet_nodes[4 * size_t(t) + k]);
+          fYoungs.push_back(d.element_youngs ? d.element_youngs[t] : (l < d.lanes ? d.materials[l].youngs_modulus : 0.0));
+          fPoisson.push_back(l < d.lanes ? d.materials[l].poissons_ratio : 0.3);
+        }
+      }
+      if (b == 0) {
+        fAnch.assign(d.anchored, d.anchored + d.nodes);
+        fMass.assign(d.node_mass, d.node_mass + d.nodes);
       }
       for (uint32_t t = d.tets; t < bd.elem_tile_end * TILE - bd.elem_begin; ++t) {
         const uint32_t e = bd.elem_begin + t;
@@ -1389,6 +1403,10 @@ struct System final : SystemBase {
       expireSolve = -1;
     }
     ++solveCount;
+    if (factorOn && fPrepared) {  // a solver state with a factor: kPcgFactor
+      pcgFactor(law, X, pass, x0zero, tangent);
+      return;
+    }
     kPcgPrepare<S><<<1, TILE, 0, st>>>(view(), pass);
     check();
     Sys<S> s = view();
@@ -1479,6 +1497,285 @@ struct System final : SystemBase {
       TL_CUDA(cudaStreamSynchronize(st));
       trace.push_back(taken);
     }
+  }
+  // ------------------------------------------------------ solver state ----
+  // The caller-held solver state (DeformableSolverState, factor.h:205-210)
+  // of a one-body system: its factor (made on the host, tl_factor_host.h),
+  // the factor in the device layout of kPcgFactor, the FactorReference and
+  // the SolverStats.
+  bool factorOn = false;
+  uint32_t factorBudget = 32u;
+  BlockFactor fHost;
+  double fStep = 0.0, fInertia = 1.0;  // FactorReference::step, ::inertia
+  bool fPrepared = false;              // a factor is prepared for the current substep
+  uint32_t fBudget = 0u;               // the iteration budget of the substep's factored solves
+  tl_factor_stats fStats{};
+  float fMean = 0.0f;                  // SolverStats::meanIterations is a float
+  std::vector<uint32_t> fTets;         // body 0: tets, per-tet Young's modulus and Poisson ratio, anchors, masses
+  std::vector<double> fYoungs, fPoisson, fMass;
+  std::vector<uint8_t> fAnch;
+  DevBuf<uint32_t> dfPerm, dfIperm, dfRowStart, dfRowCol, dfColStart, dfColRow, dfFlags, dfTicket;
+  DevBuf<double> dfRowBlk, dfColBlk, dfDiagInv, dfFrame, dfPart;
+  DevBuf<Vec4<double>> dfY, dfW, dfRef;
+  DevBuf<Vec4<S>> dfR, dfD, dfQ, dfZ, dfRestart;
+  int factorPerSm = 0;
+
+  void useFactor(uint32_t enable, uint32_t budget) override {
+    if (!enable) {
+      factorOn = false;
+      return;
+    }
+    if (B != 1) throw StatusError{TL_ERR_UNSUPPORTED, "a solver state is held for one-body systems"};
+    if (!sellReady) throw StatusError{TL_ERR_UNSUPPORTED, "the factored PCG needs the assembled operator"};
+    if (hasDamping) throw StatusError{TL_ERR_UNSUPPORTED, "the factor is made without stiffness damping"};
+    if (hencky) throw StatusError{TL_ERR_UNSUPPORTED, "the factor is made for the small-strain path"};
+    factorOn = true;
+    factorBudget = budget;
+    fHost.ready = false;
+    fStats = tl_factor_stats{};
+    fMean = 0.0f;
+    if (!factorPerSm) {
+      TL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&factorPerSm, kPcgFactor<S>, TILE, 0));
+      if (factorPerSm < 1) throw StatusError{TL_ERR_UNSUPPORTED, "the factored PCG grid cannot be resident"};
+    }
+  }
+  void factorStats(tl_factor_stats* out) override {
+    *out = fStats;
+    out->mean_iterations = double(fMean);
+    out->rows = 3u * fHost.nodes;
+    out->ready = fHost.ready ? 1u : 0u;
+    out->system_nonzeros = fHost.systemNonZeros;
+    out->factor_nonzeros = fHost.factorNonZeros();
+  }
+  FactorDev factorView() {
+    FactorDev f;
+    f.nodes = fHost.nodes;
+    f.perm = dfPerm.ptr;
+    f.iperm = dfIperm.ptr;
+    f.row_start = dfRowStart.ptr;
+    f.row_col = dfRowCol.ptr;
+    f.row_blk = dfRowBlk.ptr;
+    f.col_start = dfColStart.ptr;
+    f.col_row = dfColRow.ptr;
+    f.col_blk = dfColBlk.ptr;
+    f.diag_inv = dfDiagInv.ptr;
+    f.y = dfY.ptr;
+    f.w = dfW.ptr;
+    f.fwd_flag = dfFlags.ptr;
+    f.bwd_flag = dfFlags.ptr + fHost.nodes;
+    f.ticket = dfTicket.ptr;
+    f.epoch = dfTicket.ptr + 3;
+    f.frame = dfFrame.ptr;
+    f.part = dfPart.ptr;
+    return f;
+  }
+  double fCurStep = 0.0, fCurInertia = 1.0;  // the current step's h and (1 - alpha_m)
+  uint32_t fCgLimit = 0u;                     // Settings::cgIterations of the current step
+
+  // factor.cc:49-88 preciseTetBlocks: the 16 blocks step^2 R K R^T in FP64,
+  // row-major, with Dm and V recomputed from the rest positions (q: the
+  // tet's nodes, R row-major; preciseLame, factor.cc:21-30).
+  static void preciseTetBlocks(const double* rest, const uint32_t* q, double youngs, double poisson, const double* R,
+                               double step, double* out) {
+    double m[3][3];  // columns: the edges from node 0
+    for (int k = 0; k < 3; ++k)
+      for (int r = 0; r < 3; ++r) m[r][k] = rest[3 * size_t(q[k + 1]) + r] - rest[3 * size_t(q[0]) + r];
+    const double c00 = m[1][1] * m[2][2] - m[1][2] * m[2][1], c01 = m[1][2] * m[2][0] - m[1][0] * m[2][2],
+                 c02 = m[1][0] * m[2][1] - m[1][1] * m[2][0];
+    const double det = m[0][0] * c00 + m[0][1] * c01 + m[0][2] * c02;
+    const double volume = det / 6.0, inv = 1.0 / det;
+    // rows of m^-1 = the gradients of nodes 1..3 (adjugate / determinant)
+    double g[4][3];
+    g[1][0] = c00 * inv;
+    g[2][0] = c01 * inv;
+    g[3][0] = c02 * inv;
+    g[1][1] = (m[0][2] * m[2][1] - m[0][1] * m[2][2]) * inv;
+    g[2][1] = (m[0][0] * m[2][2] - m[0][2] * m[2][0]) * inv;
+    g[3][1] = (m[0][1] * m[2][0] - m[0][0] * m[2][1]) * inv;
+    g[1][2] = (m[0][1] * m[1][2] - m[0][2] * m[1][1]) * inv;
+    g[2][2] = (m[0][2] * m[1][0] - m[0][0] * m[1][2]) * inv;
+    g[3][2] = (m[0][0] * m[1][1] - m[0][1] * m[1][0]) * inv;
+    for (int r = 0; r < 3; ++r) g[0][r] = -(g[1][r] + g[2][r] + g[3][r]);
+    const double nu = std::clamp(poisson, 0.0, 0.49);
+    const double lambda = youngs * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = youngs / (2.0 * (1.0 + nu));
+    const double scale = step * step;
+    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) {
+        const double gab = g[a][0] * g[b][0] + g[a][1] * g[b][1] + g[a][2] * g[b][2];
+        double k[3][3], t[3][3];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j)
+            k[i][j] = volume * (lambda * g[a][i] * g[b][j] + mu * g[b][i] * g[a][j] + (i == j ? mu * gab : 0.0));
+        for (int i = 0; i < 3; ++i)  // t = R k
+          for (int j = 0; j < 3; ++j) t[i][j] = R[3 * i] * k[0][j] + R[3 * i + 1] * k[1][j] + R[3 * i + 2] * k[2][j];
+        double* o = out + 9 * (4 * a + b);
+        for (int i = 0; i < 3; ++i)  // o = step^2 t R^T
+          for (int j = 0; j < 3; ++j)
+            o[3 * i + j] = scale * (t[i][0] * R[3 * j] + t[i][1] * R[3 * j + 1] + t[i][2] * R[3 * j + 2]);
+      }
+  }
+
+  // refreshFactor (factor.cc:567-618) for body 0: the system at the rotations
+  // of the last element pass, factored; the FactorReference positions and
+  // centre are the body's now.
+  void factorRefresh(double step, double inertia) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const BodyDev& bd = bodyHost[0];
+    const HostBody& h = hb[0];
+    const uint32_t V = h.nodes, T = h.tets;
+    std::vector<double> rot(size_t(9) * T), x(size_t(3) * V);
+    fetchElems<double>(bd, h, rot.data(), nullptr, false);
+    getElems<double>(h, rot.data(), nullptr);
+    getNodes(bd, h, u, x.data(), true);
+    if (!fHost.analyzed || fHost.nodes != V) {  // analyzeSystem (factor.cc:549-565), once per mesh
+      fHost.analyze(V, fAnch.data(), fTets, h.rest.data());
+      auto put = [&](DevBuf<uint32_t>& d, const std::vector<uint32_t>& v) {
+        d.alloc(std::max<size_t>(v.size(), 1));
+        d.upload(v.data(), v.size(), st);
+      };
+      put(dfPerm, fHost.perm);
+      put(dfIperm, fHost.iperm);
+      put(dfRowStart, fHost.rowStart);
+      put(dfRowCol, fHost.rowCol);
+      put(dfColStart, fHost.colStart);
+      put(dfColRow, fHost.colRow);
+      dfRowBlk.alloc(std::max<size_t>(size_t(9) * fHost.rowCol.size(), 1));
+      dfColBlk.alloc(std::max<size_t>(size_t(9) * fHost.rowCol.size(), 1));
+      dfDiagInv.alloc(size_t(9) * std::max<uint32_t>(V, 1));
+      dfY.alloc(std::max<uint32_t>(V, 1));
+      dfW.alloc(std::max<uint32_t>(V, 1));
+      dfFlags.alloc(size_t(2) * std::max<uint32_t>(V, 1));
+      dfFlags.zero(st);
+      dfTicket.alloc(4);
+      dfTicket.zero(st);
+      dfFrame.alloc(9);
+      dfPart.alloc(size_t(8) * factorPerSm * ctx->sms);
+      dfRef.alloc(size_t(V) + 1);
+      for (DevBuf<Vec4<S>>* b : {&dfR, &dfD, &dfQ, &dfZ, &dfRestart}) {
+        b->alloc(Vp);
+        b->zero(st);
+      }
+    }
+    std::vector<double> blocks(size_t(144) * T), diag(size_t(9) * V, 0.0);
+    parallelFor(T, [&](size_t e0, size_t e1) {
+      for (size_t e = e0; e < e1; ++e)
+        preciseTetBlocks(h.rest.data(), &fTets[4 * e], fYoungs[e], fPoisson[e], &rot[9 * e], step, &blocks[144 * e]);
+    });
+    for (uint32_t v = 0; v < V; ++v) {
+      const double d = fAnch[v] ? 1.0 : inertia * double(S(fMass[v]));
+      diag[9 * size_t(v)] = diag[9 * size_t(v) + 4] = diag[9 * size_t(v) + 8] = d;
+    }
+    if (fHost.factor(fAnch.data(), fTets, blocks, diag)) {
+      dfRowBlk.upload(fHost.rowBlk.data(), fHost.rowBlk.size(), st);
+      dfColBlk.upload(fHost.colBlk.data(), fHost.colBlk.size(), st);
+      dfDiagInv.upload(fHost.diagInv.data(), fHost.diagInv.size(), st);
+    }
+    ++fStats.generation;
+    fStep = step;
+    fInertia = inertia;
+    std::vector<Vec4<double>> ref(size_t(V) + 1);
+    double total = 0.0, c[3] = {0.0, 0.0, 0.0};
+    for (uint32_t v = 0; v < V; ++v) {
+      ref[v] = Vec4<double>{x[3 * size_t(v)], x[3 * size_t(v) + 1], x[3 * size_t(v) + 2], 0.0};
+      const double m = double(S(fMass[v]));
+      total += m;
+      for (int k = 0; k < 3; ++k) c[k] += m * x[3 * size_t(v) + k];
+    }
+    ref[V] = total > 0.0 ? Vec4<double>{c[0] / total, c[1] / total, c[2] / total, 0.0}
+                         : Vec4<double>{c[0], c[1], c[2], 0.0};
+    dfRef.upload(ref.data(), ref.size(), st);
+    TL_CUDA(cudaStreamSynchronize(st));
+    fStats.refactor_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+
+  // One kPcgFactor solve from X (or zero) with the given cap; its result.
+  CgBodyDev launchFactor(Vec4<S>* X, bool x0zero, uint32_t limit, uint32_t pass) {
+    kPcgPrepare<S><<<1, TILE, 0, st>>>(view(), pass);
+    check();
+    Sys<S> s = view();
+    SellDev<S> g = sellView();
+    FactorDev f = factorView();
+    Vec4<S>*R = dfR.ptr, *D = dfD.ptr, *Q = dfQ.ptr, *Z = dfZ.ptr;
+    uint32_t xz = x0zero ? 1u : 0u, lim = limit;
+    void* args[] = {&s, &g, &f, &X, &R, &D, &Q, &Z, &xz, &lim};
+    TL_CUDA(cudaLaunchCooperativeKernel((const void*)kPcgFactor<S>, dim3(factorPerSm * ctx->sms), dim3(TILE), args,
+                                        0, st));
+    ++launches;
+    CgBodyDev c;
+    TL_CUDA(cudaMemcpyAsync(&c, cg.ptr, sizeof(CgBodyDev), cudaMemcpyDeviceToHost, st));
+    TL_CUDA(cudaStreamSynchronize(st));
+    return c;
+  }
+
+  // solvePrimary (solver.cc:3822-3910) with a prepared factor.  The solves
+  // that may refresh (a substep's first elastic read, a Newton attempt's
+  // first solve, a fallback's first read) are exactly those that start from
+  // a guess; a capped one makes the factor again at the latest rotations and
+  // solves again from the same start with the full iteration cap.
+  void pcgFactor(int law, Vec4<S>* X, uint32_t pass, bool x0zero, bool tangent) {
+    const bool refreshes = !x0zero;
+    Sys<S> s = view();
+    SellDev<S> g = sellView();
+    const unsigned blocks = (sellUpperCount + TILE - 1) / TILE;
+    if (profiling) mark(1, true);
+    assembleSell(s, g, blocks, law == TL_LAW_SNH ? 1 : 0, false, tangent, pass);
+    check();
+    ++launches;
+    if (profiling) {
+      mark(1, false);
+      mark(2, true);
+    }
+    if (refreshes)
+      TL_CUDA(cudaMemcpyAsync(dfRestart.ptr, X, size_t(Vp) * sizeof(Vec4<S>), cudaMemcpyDeviceToDevice, st));
+    CgBodyDev c = launchFactor(X, x0zero, fBudget, pass);
+    if (c.pad0 && refreshes) {
+      ++fStats.refresh_requests;
+      fStats.refreshed_at_age = fStats.substeps_since_refresh;
+      fStats.spent_before_refresh = c.taken;
+      fStats.wasted_iterations += c.taken;
+      fStats.refresh_requested = 1u;
+      TL_CUDA(cudaMemcpyAsync(X, dfRestart.ptr, size_t(Vp) * sizeof(Vec4<S>), cudaMemcpyDeviceToDevice, st));
+      factorRefresh(fCurStep, fCurInertia);
+      ++fStats.refactors;
+      ++fStats.retries;
+      ++fStats.refactor_count;
+      ++fStats.retry_count;
+      fStats.factor_age = 0u;
+      fStats.substeps_since_refresh = 0u;
+      identityFrame();
+      if (fHost.ready) {
+        c = launchFactor(X, x0zero, fCgLimit, pass);
+      } else {  // an empty factor conditions by block Jacobi (solver.cc:1923-1944)
+        if (profiling) mark(2, false);
+        fPrepared = false;
+        pcg(law, X, pass, x0zero, tangent);
+        fPrepared = true;
+        TL_CUDA(cudaMemcpyAsync(&c, cg.ptr, sizeof(CgBodyDev), cudaMemcpyDeviceToHost, st));
+        TL_CUDA(cudaStreamSynchronize(st));
+        fStats.spent_after_refresh = c.taken;
+        if (c.taken == fCgLimit && std::sqrt(c.length) > c.target) {
+          ++fStats.retries_failed;
+          fStats.fresh_retry_failed = 1u;
+        }
+        return;
+      }
+      fStats.spent_after_refresh = c.taken;
+      if (c.pad0) {
+        ++fStats.retries_failed;
+        fStats.fresh_retry_failed = 1u;
+      }
+    }
+    fStats.factor_applications += c.pad1;
+    kFactorRecord<S><<<1, 1, 0, st>>>(view(), tangent ? 1u : 0u);
+    check();
+    if (profiling) mark(2, false);
+    if (tracing) trace.push_back(c.taken);
+  }
+
+  void identityFrame() {
+    const double eye[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    dfFrame.upload(eye, 9, st);
+    TL_CUDA(cudaStreamSynchronize(st));
   }
   void finalize(uint32_t which) {
     kFinalize<<<B, TILE, 0, st>>>(dBody.ptr, epart.ptr, npart.ptr, acc.ptr, which);
@@ -1602,7 +1899,32 @@ struct System final : SystemBase {
     const bool anyYields = std::any_of(hb.begin(), hb.end(), [](const HostBody& h) { return h.anyYields; }) &&
                            law == TL_LAW_COROTATED && !hencky;
     std::vector<tl_step_report> local(B);
+    fPrepared = false;
+    if (factorOn) {
+      if (B != 1 || hasDamping || hencky)
+        throw StatusError{TL_ERR_UNSUPPORTED, "a solver state needs one undamped body on the small-strain path"};
+      // the factor is made at the committed rotations, which the SNH operator state replaces
+      if (law == TL_LAW_SNH) throw StatusError{TL_ERR_UNSUPPORTED, "a solver state is held for the corotated law"};
+      // solver.cc:3639-3655: the factor is made again when it is empty or was
+      // made for another step or inertia
+      fCurStep = hs[0].hstep;
+      fCurInertia = hs[0].inertia;
+      fCgLimit = set.cg_iterations;
+      if (!fHost.ready || fStep != fCurStep || fInertia != fCurInertia) {
+        factorRefresh(fCurStep, fCurInertia);
+        fStats.factor_age = 0u;
+        ++fStats.refactor_count;
+      }
+    }
     for (uint32_t pass = 0; pass < maxSub; ++pass) {
+      if (factorOn) {  // solver.cc:3808-3821: the prepared factor, its frame and budget
+        fPrepared = fHost.ready;
+        if (fPrepared) {
+          kFactorFrame<S><<<1, TILE, 0, st>>>(view(), hb[0].nodes, dfRef.ptr, dfFrame.ptr);
+          check();
+        }
+        fBudget = fPrepared && factorBudget != 0u ? std::min(factorBudget, set.cg_iterations) : set.cg_iterations;
+      }
       if (anyFloating) frameBegin(pass);
       nodeOp(kPredict<S>, pass);
       if (!anyNewton) {
@@ -1612,12 +1934,20 @@ struct System final : SystemBase {
       } else {  // a batch: every yielding body's Newton loop at once, the others' elastic reads
         newtonBatch(law, pass, set, rule, hs, local, newtonBody);
       }
+      if (factorOn) {  // solver.cc:4258-4263
+        CgReportDev rep;
+        TL_CUDA(cudaMemcpyAsync(&rep, cgrep.ptr, sizeof(CgReportDev), cudaMemcpyDeviceToHost, st));
+        TL_CUDA(cudaStreamSynchronize(st));
+        ++fStats.substeps_since_refresh;
+        fMean = 0.9f * fMean + 0.1f * float(rep.pass_iterations);
+      }
       if (anyFloating) frameEnd(pass);
       nodeOp(kUpdate<S>, pass);
       if (anyFloating) frameTurn(pass);
       recordSubstep(pass);
       if (anyYields) element(law, u.ptr, nullptr, pass, EM_MAPPING | EM_COMMIT, 0.0);
     }
+    fPrepared = false;
     if (hencky) {  // flowLattice once per step, after the solve (strainstep.cc:822-825)
       yielding.zero(st);
       kHenckyFlow<S><<<elemTiles, TILE, 0, st>>>(view());
@@ -2522,6 +2852,7 @@ struct System final : SystemBase {
       graphExec = nullptr;
     }
     eyoung.upload(E, h.tets, st, bd.elem_begin);
+    if (b == 0) fYoungs.assign(E, E + h.tets);
     TL_CUDA(cudaStreamSynchronize(st));
   }
 
@@ -2889,6 +3220,23 @@ int32_t tl_system_set_solver(tl_system* system, uint32_t form) {
   if (!system || form > TL_SOLVER_ASSEMBLED_PIPELINED) return TL_ERR_ARG;
   return guarded(system->ctx, [&]() -> int32_t {
     system->impl->setSolver(form);
+    return TL_OK;
+  });
+}
+
+int32_t tl_system_use_factor(tl_system* system, uint32_t enable, uint32_t factor_budget) {
+  if (!system) return TL_ERR_ARG;
+  return guarded(system->ctx, [&]() -> int32_t {
+    TL_CUDA(cudaSetDevice(system->ctx->device));
+    system->impl->useFactor(enable, factor_budget);
+    return TL_OK;
+  });
+}
+
+int32_t tl_system_factor_stats(tl_system* system, tl_factor_stats* out) {
+  if (!system || !out) return TL_ERR_ARG;
+  return guarded(system->ctx, [&]() -> int32_t {
+    system->impl->factorStats(out);
     return TL_OK;
   });
 }

@@ -278,6 +278,20 @@ class System:
         check(capi.lib().tl_system_tune_shape(self.handle, capi.TL_SHAPE_BATCH_BLOCKS, int(batch_blocks)),
               self.context.handle)
 
+    def use_factor(self, enable: bool = True, factor_budget: int = 32):
+        """Hold a solver state for this one-body system (tl_system_use_factor;
+        the DeformableSolverState* of deformable::step): its PCG is then
+        preconditioned by the FP64 Cholesky factor of the system, refreshed as
+        the reference refreshes it.  factor_budget is Settings::factorBudget."""
+        check(capi.lib().tl_system_use_factor(self.handle, 1 if enable else 0, int(factor_budget)),
+              self.context.handle)
+
+    def factor_stats(self) -> dict:
+        """SolverStats, factor size and factor counters (tl_system_factor_stats)."""
+        out = capi.tl_factor_stats()
+        check(capi.lib().tl_system_factor_stats(self.handle, C.byref(out)), self.context.handle)
+        return out.as_dict()
+
     def set_solver(self, form: str = "auto"):
         """PCG operator form of a system (tl_system_set_solver): "auto",
         "assembled" (3x3 node blocks assembled once per solve),
