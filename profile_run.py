@@ -32,15 +32,22 @@ def main():
                     help="PCG operator form (tl_system_set_solver)")
     ap.add_argument("--tolerance", type=float, default=1e-3, help="PCG relative tolerance")
     ap.add_argument("--cap", type=int, default=64, help="PCG iteration cap")
+    ap.add_argument("--factor", type=int, default=-1,
+                    help="hold a solver state with this factor budget (tl_system_use_factor; -1: none)")
+    ap.add_argument("--cells", default="", help="plastic-block lattice cells as NX,NY,NZ (default: the workload's)")
     args = ap.parse_args()
     spec = dict(WORKLOADS[args.workload])
     if args.count and spec.get("batch"):
         spec["count"] = args.count
+    if args.cells:
+        spec["cells"] = tuple(int(c) for c in args.cells.split(","))
     meshes, mats = make_bodies(spec)
     precision = tb.FP32_MIXED if args.precision == "mixed" else tb.FP64
     law = tb.NEO_HOOKEAN if spec["law"] == "snh" else tb.COROTATED
     system = tb.System(meshes, mats, precision)
     system.set_solver(args.solver)
+    if args.factor >= 0:
+        system.use_factor(True, args.factor)
     for i, m in enumerate(meshes):
         system.set_state(tb.rest_state(m), i)
     settings = tb.Settings(law=law, trace=True, tolerance=args.tolerance, cg_iterations=args.cap)
@@ -48,7 +55,9 @@ def main():
     print(json.dumps({"workload": args.workload, "precision": args.precision,
                       "tets": sum(m.tets for m in meshes), "nodes": sum(m.nodes for m in meshes),
                       "pcg_iterations": system.trace(),
-                      "tangent_iterations": sum(r[0]["cg_tangent_iterations"] for r in reports)}))
+                      "tangent_iterations": sum(r[0]["cg_tangent_iterations"] for r in reports),
+                      "device_seconds": [r[0]["device_seconds"] for r in reports],
+                      "factor": system.factor_stats() if args.factor >= 0 else None}))
     system.close()
 
 

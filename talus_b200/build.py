@@ -8,7 +8,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SOURCES = [os.path.join(HERE, "csrc", "tl_system.cu"), os.path.join(HERE, "csrc", "tl_noalloc.cu")]
 HEADERS = [os.path.join(HERE, "csrc", f) for f in ("tl_kernels.cuh", "tl_math.cuh", "tl_adjoint.cuh", "tl_sell.cuh",
-                                                   "tl_sell_build.h", "tl_validate.h", "tl_floating.cuh")] + [
+                                                   "tl_sell_build.h", "tl_validate.h", "tl_floating.cuh",
+                                                   "tl_factor.cuh", "tl_factor_host.h")] + [
     os.path.join(os.path.dirname(HERE), "include", "talus_fem.h")]
 OUTPUT = os.path.join(HERE, "libtalus_fem.so")
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",

@@ -15,11 +15,13 @@
 //   kPcgFactor    persistent cooperative PCG in the reference's order with
 //                 the factor as preconditioner, operator = the assembled block
 //                 matrix of kSellAssemble.  The two triangular solves of each
-//                 application run inside the launch: every warp takes node
-//                 rows by an atomic ticket, forward rows in increasing order,
-//                 then backward rows in decreasing order, and waits (bounded)
-//                 for the flags of the rows its row reads.  Rows are handed out
-//                 only to running warps in dependency order, so the smallest
+//                 application run inside the launch over the supernodes of the
+//                 dissection (its leaves and separators): every block takes
+//                 supernodes by an atomic ticket, children before parents in
+//                 the forward solve and parents before children in the
+//                 backward one, and waits (bounded) for the flags of the
+//                 supernodes it reads.  Supernodes are handed out only to
+//                 running blocks in dependency order, so the smallest
 //                 unfinished ticket can always finish.
 #pragma once
 
@@ -39,11 +41,18 @@ struct FactorDev {
   const uint32_t* col_row;    // [col blocks] their rows
   const double* col_blk;      // [9 per block] L_ji row-major
   const double* diag_inv;     // [9 per node] L_ii^-1 row-major (lower triangular)
+  uint32_t supernodes;
+  const uint32_t* sn_start;   // [supernodes + 1] row range of each supernode (children first)
+  const int32_t* sn_child;    // [2 per supernode] -1: none
+  const int32_t* sn_parent;   // [supernodes] -1: a root
+  const uint32_t* row_split;  // [nodes] first block of row i inside its supernode
+  const uint32_t* col_split;  // [nodes] first block of column i past its supernode
+  Vec4<double>* rhs;          // [nodes] right sides less the finished supernodes' part
   Vec4<double>* y;            // [nodes] forward solve
   Vec4<double>* w;            // [nodes] backward solve
-  uint32_t* fwd_flag;         // [nodes] application epoch of y
-  uint32_t* bwd_flag;         // [nodes] application epoch of w
-  uint32_t* ticket;           // [3] row tickets, by application mod 3
+  uint32_t* fwd_flag;         // [supernodes] application epoch of the supernode's y
+  uint32_t* bwd_flag;         // [supernodes] application epoch of the supernode's w
+  uint32_t* ticket;           // [3] supernode tickets, by application mod 3
   uint32_t* epoch;            // [1] applications made so far (flags start at 0)
   const double* frame;        // [9] row-major rotation the factor is applied in
   double* part;               // [8 G] block partials, two halves
@@ -53,21 +62,40 @@ __device__ __forceinline__ void stRelease(uint32_t* p, uint32_t v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Bounded wait for flag == epoch.  Gives up after TL_BARRIER_LIMIT_NS
-// (recording TL_ERR_TIMEOUT) or once another wait or barrier has given up.
-__device__ __forceinline__ bool waitFlag(const uint32_t* flag, uint32_t epoch, GridSyncDev* sync) {
-  if (ldAcquire(flag) == epoch) return true;
-  const unsigned long long t0 = globalTimer();
-  unsigned int polls = 0;
-  while (ldAcquire(flag) != epoch) {
-    if ((++polls & 255u) == 0u) {
+__device__ __forceinline__ uint32_t ldRelaxed(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Waits until the flags of up to FLAG_BATCH rows all hold epoch: every
+// pending flag is polled at once with relaxed loads, then one acquire fence
+// orders the reads of the rows' values after them.  Bounded: gives up after
+// TL_BARRIER_LIMIT_NS (recording TL_ERR_TIMEOUT) or once another wait or
+// barrier has given up.
+constexpr int FLAG_BATCH = 8;
+__device__ __forceinline__ bool waitFlags(const uint32_t* flags, const uint32_t (&j)[FLAG_BATCH], uint32_t n,
+                                          uint32_t epoch, GridSyncDev* sync) {
+  uint32_t pending = n >= 32u ? 0xffffffffu : (1u << n) - 1u;
+  unsigned long long t0 = 0;
+  unsigned int rounds = 0;
+  for (;;) {
+#pragma unroll
+    for (int b = 0; b < FLAG_BATCH; ++b)
+      if ((pending >> b) & 1u)
+        if (ldRelaxed(&flags[j[b]]) == epoch) pending &= ~(1u << b);
+    if (!pending) break;
+    if (rounds == 0) t0 = globalTimer();
+    if ((++rounds & 63u) == 0u) {
       if (*(volatile int*)&sync->error != 0) return false;
       if (globalTimer() - t0 > TL_BARRIER_LIMIT_NS) {
         atomicExch(&sync->error, 5);  // TL_ERR_TIMEOUT
         return false;
       }
     }
+    __nanosleep(32);
   }
+  asm volatile("fence.acq_rel.gpu;" ::: "memory");
   return true;
 }
 
@@ -81,65 +109,142 @@ __device__ __forceinline__ V3<double> warpSum3(V3<double> v) {
   return v;
 }
 
+// Sum of a V3 over the block; the result in thread 0.
+__device__ __forceinline__ V3<double> blockSum3(V3<double> v, double (&red)[3][TILE / 32]) {
+  v = warpSum3(v);
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[0][warp] = v.x;
+    red[1][warp] = v.y;
+    red[2][warp] = v.z;
+  }
+  __syncthreads();
+  V3<double> sum = {0, 0, 0};
+  if (threadIdx.x == 0)
+    for (int w = 0; w < TILE / 32; ++w) sum = sum + V3<double>{red[0][w], red[1][w], red[2][w]};
+  return sum;
+}
+
+// Rows of a supernode whose solved values a block keeps in shared memory
+// (later rows of larger supernodes read theirs from global memory).
+constexpr uint32_t SN_CACHE = 1024;
+
 // z = frame (L L^T)^-1 P (frame^T r) of applyFactor, y and w in factor order;
-// every warp of the grid takes part.  r is read at the forward rows (written
-// before the launch's last grid barrier); the caller turns w back.
+// every block of the grid takes part.  Blocks take supernodes by an atomic
+// ticket: the forward solve's in increasing order (children first), each
+// after its children's flags; then the backward solve's in decreasing order
+// (parents first), each after its parent's flag (a root: after its own
+// forward flag, which follows every descendant's).  A block first takes the
+// finished supernodes' part of all its rows at once (a warp per row), then
+// solves its rows one after another, all threads on each row's blocks inside
+// the supernode, the values solved so far in shared memory.  r is read at the
+// forward rows (written before the launch's last grid barrier); the caller
+// turns w back.
 template <class S>
 __device__ void factorSolve(const FactorDev& f, GridSyncDev* sync, const Vec4<S>* r, const M3<S>& frame,
                             uint32_t epoch, uint32_t* ticket) {
-  const uint32_t lane = threadIdx.x & 31u, V = f.nodes;
+  __shared__ uint32_t snTicket;
+  __shared__ double red[3][TILE / 32];
+  __shared__ double solved[3][SN_CACHE];
+  const uint32_t SN = f.supernodes, lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   bool ok = true;
   for (;;) {
-    uint32_t t = 0;
-    if (lane == 0) t = atomicAdd(ticket, 1u);
-    t = __shfl_sync(0xffffffffu, t, 0);
-    if (t >= 2u * V) break;
-    V3<double> acc = {0, 0, 0};
-    if (t < V) {  // forward row i: y_i = L_ii^-1 (b_i - sum_j L_ij y_j)
-      const uint32_t i = t, k1 = __ldg(&f.row_start[i + 1]);
-      for (uint32_t k = __ldg(&f.row_start[i]) + lane; k < k1; k += 32u) {
-        const uint32_t j = __ldg(&f.row_col[k]);
-        ok = ok && waitFlag(&f.fwd_flag[j], epoch, sync);
-        const Vec4<double> yj = ld4cg(&f.y[j]);
-        const double* L = f.row_blk + size_t(9) * k;
-        acc.x += __ldg(L) * yj.x + __ldg(L + 1) * yj.y + __ldg(L + 2) * yj.z;
-        acc.y += __ldg(L + 3) * yj.x + __ldg(L + 4) * yj.y + __ldg(L + 5) * yj.z;
-        acc.z += __ldg(L + 6) * yj.x + __ldg(L + 7) * yj.y + __ldg(L + 8) * yj.z;
-      }
-      acc = warpSum3(acc);
-      if (lane == 0) {
-        const uint32_t o = __ldg(&f.perm[i]);
-        const V3<S> turned = mulT(frame, xyz(ld4cg(&r[o])));  // frame^T r in the step's arithmetic
-        const V3<double> b = cvt<double>(turned) - acc;
-        const double* D = f.diag_inv + size_t(9) * i;
-        const V3<double> y = {__ldg(D) * b.x, __ldg(D + 3) * b.x + __ldg(D + 4) * b.y,
-                              __ldg(D + 6) * b.x + __ldg(D + 7) * b.y + __ldg(D + 8) * b.z};
-        f.y[i] = Vec4<double>{y.x, y.y, y.z, 0.0};
-        stRelease(&f.fwd_flag[i], epoch);
-      }
-    } else {  // backward row i: w_i = L_ii^-T (y_i - sum_{j > i} L_ji^T w_j)
-      const uint32_t i = 2u * V - 1u - t, k1 = __ldg(&f.col_start[i + 1]);
-      for (uint32_t k = __ldg(&f.col_start[i]) + lane; k < k1; k += 32u) {
-        const uint32_t j = __ldg(&f.col_row[k]);
-        ok = ok && waitFlag(&f.bwd_flag[j], epoch, sync);
-        const Vec4<double> wj = ld4cg(&f.w[j]);
-        const double* L = f.col_blk + size_t(9) * k;
-        acc.x += __ldg(L) * wj.x + __ldg(L + 3) * wj.y + __ldg(L + 6) * wj.z;
-        acc.y += __ldg(L + 1) * wj.x + __ldg(L + 4) * wj.y + __ldg(L + 7) * wj.z;
-        acc.z += __ldg(L + 2) * wj.x + __ldg(L + 5) * wj.y + __ldg(L + 8) * wj.z;
-      }
-      acc = warpSum3(acc);
-      if (lane == 0) {
-        ok = ok && waitFlag(&f.fwd_flag[i], epoch, sync);
-        const Vec4<double> yi = ld4cg(&f.y[i]);
-        const V3<double> b = {yi.x - acc.x, yi.y - acc.y, yi.z - acc.z};
-        const double* D = f.diag_inv + size_t(9) * i;
-        const V3<double> w = {__ldg(D) * b.x + __ldg(D + 3) * b.y + __ldg(D + 6) * b.z,
-                              __ldg(D + 4) * b.y + __ldg(D + 7) * b.z, __ldg(D + 8) * b.z};
-        f.w[i] = Vec4<double>{w.x, w.y, w.z, 0.0};
-        stRelease(&f.bwd_flag[i], epoch);
+    if (threadIdx.x == 0) snTicket = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint32_t t = snTicket;
+    if (t >= 2u * SN) break;
+    const bool forward = t < SN;
+    const uint32_t p = forward ? t : 2u * SN - 1u - t;
+    if (threadIdx.x == 0) {  // the supernodes this one reads
+      uint32_t wait[FLAG_BATCH] = {0, 0, 0, 0, 0, 0, 0, 0};
+      uint32_t n = 0;
+      if (forward) {
+        for (int c = 0; c < 2; ++c) {
+          const int32_t ch = __ldg(&f.sn_child[2 * p + c]);
+          if (ch >= 0) wait[n++] = uint32_t(ch);
+        }
+        ok = ok && waitFlags(f.fwd_flag, wait, n, epoch, sync);
+      } else {
+        const int32_t parent = __ldg(&f.sn_parent[p]);
+        wait[0] = parent >= 0 ? uint32_t(parent) : p;
+        ok = ok && waitFlags(parent >= 0 ? f.bwd_flag : f.fwd_flag, wait, 1u, epoch, sync);
       }
     }
+    __syncthreads();
+    const uint32_t b = __ldg(&f.sn_start[p]), e = __ldg(&f.sn_start[p + 1]);
+    const uint32_t* start = forward ? f.row_start : f.col_start;
+    const uint32_t* index = forward ? f.row_col : f.col_row;
+    const Vec4<double>* val = forward ? f.y : f.w;
+    const double* blk = forward ? f.row_blk : f.col_blk;
+    // forward: L_ij v; backward: L_ji^T v
+    const auto term = [&](const double* L, const Vec4<double>& v, V3<double>& acc) {
+      if (forward) {
+        acc.x += __ldg(L) * v.x + __ldg(L + 1) * v.y + __ldg(L + 2) * v.z;
+        acc.y += __ldg(L + 3) * v.x + __ldg(L + 4) * v.y + __ldg(L + 5) * v.z;
+        acc.z += __ldg(L + 6) * v.x + __ldg(L + 7) * v.y + __ldg(L + 8) * v.z;
+      } else {
+        acc.x += __ldg(L) * v.x + __ldg(L + 3) * v.y + __ldg(L + 6) * v.z;
+        acc.y += __ldg(L + 1) * v.x + __ldg(L + 4) * v.y + __ldg(L + 7) * v.z;
+        acc.z += __ldg(L + 2) * v.x + __ldg(L + 5) * v.y + __ldg(L + 8) * v.z;
+      }
+    };
+    // ---- the finished supernodes' part of every row: forward the blocks
+    // before the supernode, backward those past it; rhs = b_i - that part
+    for (uint32_t i = b + warp; i < e; i += TILE / 32) {
+      const uint32_t k0 = forward ? __ldg(&start[i]) : __ldg(&f.col_split[i]);
+      const uint32_t k1 = forward ? __ldg(&f.row_split[i]) : __ldg(&start[i + 1]);
+      V3<double> acc = {0, 0, 0};
+      for (uint32_t k = k0 + lane; k < k1; k += 32u) term(blk + size_t(9) * k, ld4cg(&val[__ldg(&index[k])]), acc);
+      acc = warpSum3(acc);
+      if (lane == 0) {
+        V3<double> rhs;
+        if (forward) {  // frame^T r in the step's arithmetic
+          rhs = cvt<double>(mulT(frame, xyz(ld4cg(&r[__ldg(&f.perm[i])]))));
+        } else {
+          const Vec4<double> yi = ld4cg(&f.y[i]);
+          rhs = {yi.x, yi.y, yi.z};
+        }
+        f.rhs[i] = Vec4<double>{rhs.x - acc.x, rhs.y - acc.y, rhs.z - acc.z, 0.0};
+      }
+    }
+    __syncthreads();
+    // ---- the supernode's own rows in order
+    for (uint32_t q = 0; q < e - b; ++q) {
+      const uint32_t i = forward ? b + q : e - 1u - q;
+      const double* D = f.diag_inv + size_t(9) * i;
+      double d[9];
+      Vec4<double> rhs = {0, 0, 0, 0};
+      if (threadIdx.x == 0) {  // requested with the row's blocks
+#pragma unroll
+        for (int m = 0; m < 9; ++m) d[m] = __ldg(D + m);
+        rhs = ld4cg(&f.rhs[i]);
+      }
+      const uint32_t k0 = forward ? __ldg(&f.row_split[i]) : __ldg(&start[i]);
+      const uint32_t k1 = forward ? __ldg(&start[i + 1]) : __ldg(&f.col_split[i]);
+      V3<double> acc = {0, 0, 0};
+      for (uint32_t k = k0 + threadIdx.x; k < k1; k += TILE) {
+        const uint32_t j = __ldg(&index[k]), at = j - b;
+        const Vec4<double> v = at < SN_CACHE ? Vec4<double>{solved[0][at], solved[1][at], solved[2][at], 0.0}
+                                             : ld4cg(&val[j]);
+        term(blk + size_t(9) * k, v, acc);
+      }
+      const V3<double> sum = blockSum3(acc, red);
+      if (threadIdx.x == 0) {
+        const V3<double> bb = {rhs.x - sum.x, rhs.y - sum.y, rhs.z - sum.z};
+        const V3<double> x = forward ? V3<double>{d[0] * bb.x, d[3] * bb.x + d[4] * bb.y,
+                                                  d[6] * bb.x + d[7] * bb.y + d[8] * bb.z}   // L_ii^-1 bb
+                                     : V3<double>{d[0] * bb.x + d[3] * bb.y + d[6] * bb.z,  // L_ii^-T bb
+                                                  d[4] * bb.y + d[7] * bb.z, d[8] * bb.z};
+        (forward ? f.y : f.w)[i] = Vec4<double>{x.x, x.y, x.z, 0.0};
+        if (i - b < SN_CACHE) {
+          solved[0][i - b] = x.x;
+          solved[1][i - b] = x.y;
+          solved[2][i - b] = x.z;
+        }
+      }
+      __syncthreads();  // the row is visible to the block's next rows; red is free again
+    }
+    if (threadIdx.x == 0) stRelease(forward ? &f.fwd_flag[p] : &f.bwd_flag[p], epoch);
   }
   (void)ok;  // a wait that gave up has recorded it; the next grid barrier ends the launch
 }

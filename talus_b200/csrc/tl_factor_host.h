@@ -27,6 +27,17 @@ struct BlockFactor {
   std::vector<uint32_t> rowStart, rowCol;     // strictly lower blocks of L by rows, columns ascending
   std::vector<uint32_t> colStart, colRow;     // the same blocks by columns, rows ascending
   std::vector<double> rowBlk, colBlk, diagInv;  // [9 per block] row-major; L_ii^-1 per node
+  // supernodes: the leaves and separators of the dissection, contiguous row
+  // ranges in factor order, children before parents; a supernode's rows read
+  // only rows of its own range and of its descendants (forward solve)
+  std::vector<uint32_t> snStart;  // [supernodes + 1]
+  std::vector<int32_t> snChild;   // [2 per supernode] -1: none
+  std::vector<int32_t> snParent;  // [supernodes] -1: a root
+  // per row: its first block inside its supernode (row view: columns >= the
+  // supernode's first row) and its first block past it (column view: rows >=
+  // the supernode's end), so that a solve reads the finished supernodes'
+  // values in one pass and its own rows' one by one
+  std::vector<uint32_t> rowSplit, colSplit;
 
   uint64_t factorNonZeros() const {  // scalar entries of L: 9 per off-diagonal block, 6 per diagonal block
     return ready ? uint64_t(9) * rowCol.size() + uint64_t(6) * nodes : 0u;
@@ -61,11 +72,18 @@ struct BlockFactor {
     // ---- order: anchored nodes first (they couple to nothing), then nested dissection
     perm.clear();
     perm.reserve(V);
+    snStart.assign(1, 0u);
+    snChild.clear();
     std::vector<uint32_t> free;
     for (uint32_t v = 0; v < V; ++v) (anchored[v] ? perm : free).push_back(v);
+    if (!perm.empty()) addSupernode(-1, -1);  // the anchored rows: no entries
     std::vector<uint32_t> mark(V, 0u);
     uint32_t stamp = 0;
     dissect(free, adj, rest, mark, stamp);
+    snParent.assign(snStart.size() - 1, -1);
+    for (size_t p = 0; p + 1 < snStart.size(); ++p)
+      for (int c = 0; c < 2; ++c)
+        if (snChild[2 * p + c] >= 0) snParent[snChild[2 * p + c]] = int32_t(p);
     iperm.assign(V, 0u);
     for (uint32_t i = 0; i < V; ++i) iperm[perm[i]] = i;
     // ---- elimination tree (Liu, with path compression) and row patterns
@@ -111,18 +129,36 @@ struct BlockFactor {
     std::vector<uint32_t> fill(colStart.begin(), colStart.end() - 1);
     for (uint32_t i = 0; i < V; ++i)
       for (uint32_t k = rowStart[i]; k < rowStart[i + 1]; ++k) colRow[fill[rowCol[k]]++] = i;
+    rowSplit.assign(V, 0u);
+    colSplit.assign(V, 0u);
+    for (size_t p = 0; p + 1 < snStart.size(); ++p)
+      for (uint32_t i = snStart[p]; i < snStart[p + 1]; ++i) {
+        rowSplit[i] = uint32_t(std::lower_bound(rowCol.begin() + rowStart[i], rowCol.begin() + rowStart[i + 1],
+                                                snStart[p]) - rowCol.begin());
+        colSplit[i] = uint32_t(std::lower_bound(colRow.begin() + colStart[i], colRow.begin() + colStart[i + 1],
+                                                snStart[p + 1]) - colRow.begin());
+      }
     analyzed = true;
   }
 
+  // A supernode of the rows appended to perm since the last one.
+  int32_t addSupernode(int32_t a, int32_t b) {
+    snStart.push_back(uint32_t(perm.size()));
+    snChild.push_back(a);
+    snChild.push_back(b);
+    return int32_t(snStart.size()) - 2;
+  }
   // Nested dissection of a free node set: split at the median of the widest
   // coordinate, the separator being the lower side's nodes that touch the
-  // upper side; the two sides first, the separator last.
-  void dissect(std::vector<uint32_t>& set, const std::vector<std::vector<uint32_t>>& adj, const double* rest,
-               std::vector<uint32_t>& mark, uint32_t& stamp) {
+  // upper side; the two sides first, the separator last.  Returns the
+  // subtree's supernode (-1 for an empty set).
+  int32_t dissect(std::vector<uint32_t>& set, const std::vector<std::vector<uint32_t>>& adj, const double* rest,
+                  std::vector<uint32_t>& mark, uint32_t& stamp) {
     constexpr size_t LEAF = 64;
+    if (set.empty()) return -1;
     if (set.size() <= LEAF) {
       perm.insert(perm.end(), set.begin(), set.end());
-      return;
+      return addSupernode(-1, -1);
     }
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     for (uint32_t v : set)
@@ -152,9 +188,10 @@ struct BlockFactor {
       (touches ? sep : left).push_back(v);
     }
     std::vector<uint32_t>().swap(set);
-    dissect(left, adj, rest, mark, stamp);
-    dissect(right, adj, rest, mark, stamp);
+    const int32_t a = dissect(left, adj, rest, mark, stamp);
+    const int32_t b = dissect(right, adj, rest, mark, stamp);
     perm.insert(perm.end(), sep.begin(), sep.end());
+    return addSupernode(a, b);
   }
 
   // Numeric factor.  diag [9 V] and the element blocks blocks[16 per tet][9]

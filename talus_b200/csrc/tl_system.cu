@@ -1514,9 +1514,11 @@ struct System final : SystemBase {
   std::vector<uint32_t> fTets;         // body 0: tets, per-tet Young's modulus and Poisson ratio, anchors, masses
   std::vector<double> fYoungs, fPoisson, fMass;
   std::vector<uint8_t> fAnch;
-  DevBuf<uint32_t> dfPerm, dfIperm, dfRowStart, dfRowCol, dfColStart, dfColRow, dfFlags, dfTicket;
+  DevBuf<uint32_t> dfPerm, dfIperm, dfRowStart, dfRowCol, dfColStart, dfColRow, dfFlags, dfTicket, dfSnStart,
+      dfRowSplit, dfColSplit;
+  DevBuf<int32_t> dfSnChild, dfSnParent;
   DevBuf<double> dfRowBlk, dfColBlk, dfDiagInv, dfFrame, dfPart;
-  DevBuf<Vec4<double>> dfY, dfW, dfRef;
+  DevBuf<Vec4<double>> dfY, dfW, dfRef, dfRhs;
   DevBuf<Vec4<S>> dfR, dfD, dfQ, dfZ, dfRestart;
   int factorPerSm = 0;
 
@@ -1559,10 +1561,17 @@ struct System final : SystemBase {
     f.col_row = dfColRow.ptr;
     f.col_blk = dfColBlk.ptr;
     f.diag_inv = dfDiagInv.ptr;
+    f.supernodes = uint32_t(fHost.snParent.size());
+    f.sn_start = dfSnStart.ptr;
+    f.sn_child = dfSnChild.ptr;
+    f.sn_parent = dfSnParent.ptr;
+    f.row_split = dfRowSplit.ptr;
+    f.col_split = dfColSplit.ptr;
+    f.rhs = dfRhs.ptr;
     f.y = dfY.ptr;
     f.w = dfW.ptr;
     f.fwd_flag = dfFlags.ptr;
-    f.bwd_flag = dfFlags.ptr + fHost.nodes;
+    f.bwd_flag = dfFlags.ptr + fHost.snParent.size();
     f.ticket = dfTicket.ptr;
     f.epoch = dfTicket.ptr + 3;
     f.frame = dfFrame.ptr;
@@ -1639,12 +1648,22 @@ struct System final : SystemBase {
       put(dfRowCol, fHost.rowCol);
       put(dfColStart, fHost.colStart);
       put(dfColRow, fHost.colRow);
+      put(dfSnStart, fHost.snStart);
+      put(dfRowSplit, fHost.rowSplit);
+      put(dfColSplit, fHost.colSplit);
+      auto puti = [&](DevBuf<int32_t>& d, const std::vector<int32_t>& v) {
+        d.alloc(std::max<size_t>(v.size(), 1));
+        d.upload(v.data(), v.size(), st);
+      };
+      puti(dfSnChild, fHost.snChild);
+      puti(dfSnParent, fHost.snParent);
       dfRowBlk.alloc(std::max<size_t>(size_t(9) * fHost.rowCol.size(), 1));
       dfColBlk.alloc(std::max<size_t>(size_t(9) * fHost.rowCol.size(), 1));
       dfDiagInv.alloc(size_t(9) * std::max<uint32_t>(V, 1));
       dfY.alloc(std::max<uint32_t>(V, 1));
       dfW.alloc(std::max<uint32_t>(V, 1));
-      dfFlags.alloc(size_t(2) * std::max<uint32_t>(V, 1));
+      dfRhs.alloc(std::max<uint32_t>(V, 1));
+      dfFlags.alloc(size_t(2) * std::max<size_t>(fHost.snParent.size(), 1));
       dfFlags.zero(st);
       dfTicket.alloc(4);
       dfTicket.zero(st);
