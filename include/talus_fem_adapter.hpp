@@ -29,6 +29,7 @@ struct DeviceBody {
   uint32_t law = TL_LAW_COROTATED;
   uint32_t nodes = 0u, tets = 0u;
   std::vector<float> rotation, plastic;  // [9 T] committed rotations, [10 T] plastic points
+  bool factored = false;                 // the device holds a solver state's factor for this body
   DeviceBody() = default;
   DeviceBody(const DeviceBody&) = delete;
   DeviceBody& operator=(const DeviceBody&) = delete;
@@ -201,6 +202,53 @@ inline int32_t step(DeviceBody& body, talus::DeformableState& state, const Setti
   if (rc != TL_OK && rc != TL_ERR_NONFINITE) return rc;
   unpackElements(state, T, body.rotation, body.plastic);
   accumulate(report, r, body.system, 0);
+  return rc;
+}
+
+// deformable::step(mesh, state, materials, settings, gravity, dt, {}, {},
+// solver, report) with a caller-held solver state (solver.h:451-462,
+// factor.h:205-210).  The factor itself lives on the device with the body:
+// the first call with a solver state turns it on (tl_system_use_factor with
+// Settings::factorBudget), a call without one turns it off.  After each step
+// the caller's SolverStats (factor.h:28-38) are those of the device state and
+// the step's factor counters are added to the report (solver.cc:3606-3609,
+// 3839-3899).  The reference's Eigen factor inside the caller's state is not
+// built (the device factor takes its place).
+inline int32_t step(DeviceBody& body, talus::DeformableState& state, const Settings& s, const glm::vec3& gravity,
+                    float dt, DeformableSolverState* solver, StepReport& report) {
+  if ((solver != nullptr) != body.factored) {
+    const int32_t rc = tl_system_use_factor(body.system, solver ? 1u : 0u, s.factorBudget);
+    if (rc != TL_OK) return rc;
+    body.factored = solver != nullptr;
+  }
+  tl_factor_stats before{}, after{};
+  if (solver) tl_system_factor_stats(body.system, &before);
+  const int32_t rc = step(body, state, s, gravity, dt, report);
+  if (!solver || (rc != TL_OK && rc != TL_ERR_NONFINITE)) return rc;
+  tl_system_factor_stats(body.system, &after);
+  SolverStats& st = solver->stats;
+  st.factorAge = after.factor_age;
+  st.refactorCount = after.refactor_count;
+  st.retryCount = after.retry_count;
+  st.substepsSinceRefresh = after.substeps_since_refresh;
+  st.meanIterations = float(after.mean_iterations);
+  st.refreshRequested = after.refresh_requested != 0u;
+  st.freshRetryFailed = after.fresh_retry_failed != 0u;
+  report.factorRows = before.rows;  // read before the step's refresh, as the reference reads them
+  report.factorNonZeros = before.factor_nonzeros;
+  report.systemNonZeros = before.system_nonzeros;
+  report.refreshRequests += after.refresh_requests - before.refresh_requests;
+  report.refactors += after.refactors - before.refactors;
+  report.retries += after.retries - before.retries;
+  report.retriesFailed += after.retries_failed - before.retries_failed;
+  report.wastedIterations += after.wasted_iterations - before.wasted_iterations;
+  report.factorApplications += after.factor_applications - before.factor_applications;
+  if (after.refresh_requests != before.refresh_requests) {
+    report.refreshedAtAge = after.refreshed_at_age;
+    report.spentBeforeRefresh = after.spent_before_refresh;
+    report.spentAfterRefresh = after.spent_after_refresh;
+  }
+  report.refactorSeconds += after.refactor_seconds - before.refactor_seconds;
   return rc;
 }
 

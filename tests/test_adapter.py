@@ -71,7 +71,7 @@ struct DeformableState {
 namespace deformable {
 enum class RigidSplit { Off, Unprojected, Projected };
 struct Settings {
-  uint32_t substeps = 1u, cgIterations = 64u, plasticPasses = 40u;
+  uint32_t substeps = 1u, cgIterations = 64u, plasticPasses = 40u, factorBudget = 32u;
   float tolerance = 1.0e-3f, spectralRadius = 0.5f;
   RigidSplit rigidSplit = RigidSplit::Projected;
 };
@@ -87,7 +87,20 @@ struct StepReport {
   uint32_t worstSubstep = 0u;
   std::vector<uint32_t> cgPerSubstep;
   std::vector<float> cgStartResidual, cgEndResidual;
+  uint32_t factorApplications = 0u, factorRows = 0u, refreshRequests = 0u, refreshedAtAge = 0u,
+           spentBeforeRefresh = 0u, spentAfterRefresh = 0u, wastedIterations = 0u, refactors = 0u, retries = 0u,
+           retriesFailed = 0u;
+  uint64_t factorNonZeros = 0u, systemNonZeros = 0u;
+  double refactorSeconds = 0.0;
 };
+struct SolverStats {
+  uint32_t lastIterations = 0u;
+  float lastResidual = 0.0f;
+  uint32_t factorAge = 0u, refactorCount = 0u, retryCount = 0u, substepsSinceRefresh = 0u;
+  float meanIterations = 0.0f;
+  bool refreshRequested = false, freshRetryFailed = false;
+};
+struct DeformableSolverState { SolverStats stats; };
 }  // namespace deformable
 }  // namespace talus
 """
@@ -129,7 +142,12 @@ int main() {
     d::StepReport report;
     const int32_t s = d::b200::step(body, state, d::Settings{}, glm::vec3{0.0f, -9.81f, 0.0f}, 1.0f / 60.0f, report);
     std::printf("step %d cg %u\n", s, report.cgIterations);
-    return s == TL_OK ? 0 : 3;
+    if (s != TL_OK) return 3;
+    d::DeformableSolverState solver;  // the same step with a caller-held solver state
+    const int32_t f = d::b200::step(body, state, d::Settings{}, glm::vec3{0.0f, -9.81f, 0.0f}, 1.0f / 60.0f,
+                                    &solver, report);
+    std::printf("factored %d refactors %u\n", f, solver.stats.refactorCount);
+    return f == TL_OK && solver.stats.refactorCount == 1u ? 0 : 5;
   }
   std::printf("upload %d\n", rc);
   return rc == TL_ERR_NO_DEVICE ? 0 : 2;
