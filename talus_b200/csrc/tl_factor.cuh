@@ -146,6 +146,7 @@ __device__ void factorSolve(const FactorDev& f, GridSyncDev* sync, const Vec4<S>
   __shared__ uint32_t snTicket;
   __shared__ double red[3][TILE / 32];
   __shared__ double solved[3][SN_CACHE];
+  __shared__ uint32_t span[2][SN_CACHE];  // each cached row's own blocks [k0, k1)
   const uint32_t SN = f.supernodes, lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   bool ok = true;
   for (;;) {
@@ -176,25 +177,47 @@ __device__ void factorSolve(const FactorDev& f, GridSyncDev* sync, const Vec4<S>
     const uint32_t* index = forward ? f.row_col : f.col_row;
     const Vec4<double>* val = forward ? f.y : f.w;
     const double* blk = forward ? f.row_blk : f.col_blk;
-    // forward: L_ij v; backward: L_ji^T v
-    const auto term = [&](const double* L, const Vec4<double>& v, V3<double>& acc) {
+    // forward: L_ij v; backward: L_ji^T v (L row-major, in registers)
+    const auto termR = [&](const double (&L)[9], const Vec4<double>& v, V3<double>& acc) {
       if (forward) {
-        acc.x += __ldg(L) * v.x + __ldg(L + 1) * v.y + __ldg(L + 2) * v.z;
-        acc.y += __ldg(L + 3) * v.x + __ldg(L + 4) * v.y + __ldg(L + 5) * v.z;
-        acc.z += __ldg(L + 6) * v.x + __ldg(L + 7) * v.y + __ldg(L + 8) * v.z;
+        acc.x += L[0] * v.x + L[1] * v.y + L[2] * v.z;
+        acc.y += L[3] * v.x + L[4] * v.y + L[5] * v.z;
+        acc.z += L[6] * v.x + L[7] * v.y + L[8] * v.z;
       } else {
-        acc.x += __ldg(L) * v.x + __ldg(L + 3) * v.y + __ldg(L + 6) * v.z;
-        acc.y += __ldg(L + 1) * v.x + __ldg(L + 4) * v.y + __ldg(L + 7) * v.z;
-        acc.z += __ldg(L + 2) * v.x + __ldg(L + 5) * v.y + __ldg(L + 8) * v.z;
+        acc.x += L[0] * v.x + L[3] * v.y + L[6] * v.z;
+        acc.y += L[1] * v.x + L[4] * v.y + L[7] * v.z;
+        acc.z += L[2] * v.x + L[5] * v.y + L[8] * v.z;
       }
+    };
+    const auto term = [&](const double* Lg, const Vec4<double>& v, V3<double>& acc) {
+      double L[9];
+#pragma unroll
+      for (int m = 0; m < 9; ++m) L[m] = __ldg(Lg + m);
+      termR(L, v, acc);
     };
     // ---- the finished supernodes' part of every row: forward the blocks
     // before the supernode, backward those past it; rhs = b_i - that part
     for (uint32_t i = b + warp; i < e; i += TILE / 32) {
       const uint32_t k0 = forward ? __ldg(&start[i]) : __ldg(&f.col_split[i]);
       const uint32_t k1 = forward ? __ldg(&f.row_split[i]) : __ldg(&start[i + 1]);
+      if (lane == 0 && i - b < SN_CACHE) {  // the blocks inside the supernode, for the solve below
+        span[0][i - b] = forward ? k1 : __ldg(&start[i]);
+        span[1][i - b] = forward ? __ldg(&start[i + 1]) : k0;
+      }
       V3<double> acc = {0, 0, 0};
-      for (uint32_t k = k0 + lane; k < k1; k += 32u) term(blk + size_t(9) * k, ld4cg(&val[__ldg(&index[k])]), acc);
+      // a warp per row, several of each lane's blocks in flight at once
+      uint32_t k = k0 + lane;
+      for (; k + 96u < k1; k += 128u) {
+        uint32_t jj[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) jj[u] = __ldg(&index[k + 32u * u]);
+        Vec4<double> vv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) vv[u] = ld4cg(&val[jj[u]]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) term(blk + size_t(9) * (k + 32u * u), vv[u], acc);
+      }
+      for (; k < k1; k += 32u) term(blk + size_t(9) * k, ld4cg(&val[__ldg(&index[k])]), acc);
       acc = warpSum3(acc);
       if (lane == 0) {
         V3<double> rhs;
@@ -208,26 +231,64 @@ __device__ void factorSolve(const FactorDev& f, GridSyncDev* sync, const Vec4<S>
       }
     }
     __syncthreads();
-    // ---- the supernode's own rows in order
-    for (uint32_t q = 0; q < e - b; ++q) {
-      const uint32_t i = forward ? b + q : e - 1u - q;
-      const double* D = f.diag_inv + size_t(9) * i;
-      double d[9];
-      Vec4<double> rhs = {0, 0, 0, 0};
-      if (threadIdx.x == 0) {  // requested with the row's blocks
+    // ---- the supernode's own rows in order.  Each row's first block per
+    // thread, its L_ii^-1 and right side are requested while the row before
+    // it is reduced, so a row costs its reduction and two block barriers.
+    const auto rowOf = [&](uint32_t q) { return forward ? b + q : e - 1u - q; };
+    const auto spanOf = [&](uint32_t q, uint32_t& k0, uint32_t& k1) {
+      const uint32_t i = rowOf(q);
+      if (i - b < SN_CACHE) {
+        k0 = span[0][i - b];
+        k1 = span[1][i - b];
+      } else {
+        k0 = forward ? __ldg(&f.row_split[i]) : __ldg(&start[i]);
+        k1 = forward ? __ldg(&start[i + 1]) : __ldg(&f.col_split[i]);
+      }
+    };
+    uint32_t nj = 0, nk = 0;
+    bool nvalid = false;
+    double nL[9], nd[9];
+    Vec4<double> nrhs = {0, 0, 0, 0};
+    const auto fetch = [&](uint32_t q) {  // requests for row q
+      uint32_t k0, k1;
+      spanOf(q, k0, k1);
+      nk = k0 + threadIdx.x;
+      nvalid = nk < k1;
+      if (nvalid) {
+        nj = __ldg(&index[nk]);
 #pragma unroll
-        for (int m = 0; m < 9; ++m) d[m] = __ldg(D + m);
-        rhs = ld4cg(&f.rhs[i]);
+        for (int m = 0; m < 9; ++m) nL[m] = __ldg(blk + size_t(9) * nk + m);
       }
-      const uint32_t k0 = forward ? __ldg(&f.row_split[i]) : __ldg(&start[i]);
-      const uint32_t k1 = forward ? __ldg(&start[i + 1]) : __ldg(&f.col_split[i]);
+      if (threadIdx.x == 0) {
+        const double* D = f.diag_inv + size_t(9) * rowOf(q);
+#pragma unroll
+        for (int m = 0; m < 9; ++m) nd[m] = __ldg(D + m);
+        nrhs = ld4cg(&f.rhs[rowOf(q)]);
+      }
+    };
+    if (e > b) fetch(0);
+    for (uint32_t q = 0; q < e - b; ++q) {
+      const uint32_t i = rowOf(q);
+      uint32_t k0, k1;
+      spanOf(q, k0, k1);
+      const bool valid = nvalid;
+      const uint32_t j0 = nj;
+      double L0[9], d[9];
+#pragma unroll
+      for (int m = 0; m < 9; ++m) {
+        L0[m] = nL[m];
+        d[m] = nd[m];
+      }
+      const Vec4<double> rhs = nrhs;
+      const auto value = [&](uint32_t j) {
+        const uint32_t at = j - b;
+        return at < SN_CACHE ? Vec4<double>{solved[0][at], solved[1][at], solved[2][at], 0.0} : ld4cg(&val[j]);
+      };
       V3<double> acc = {0, 0, 0};
-      for (uint32_t k = k0 + threadIdx.x; k < k1; k += TILE) {
-        const uint32_t j = __ldg(&index[k]), at = j - b;
-        const Vec4<double> v = at < SN_CACHE ? Vec4<double>{solved[0][at], solved[1][at], solved[2][at], 0.0}
-                                             : ld4cg(&val[j]);
-        term(blk + size_t(9) * k, v, acc);
-      }
+      if (valid) termR(L0, value(j0), acc);
+      for (uint32_t k = k0 + threadIdx.x + TILE; k < k1; k += TILE)
+        term(blk + size_t(9) * k, value(__ldg(&index[k])), acc);
+      if (q + 1 < e - b) fetch(q + 1);
       const V3<double> sum = blockSum3(acc, red);
       if (threadIdx.x == 0) {
         const V3<double> bb = {rhs.x - sum.x, rhs.y - sum.y, rhs.z - sum.z};
