@@ -345,3 +345,25 @@ def test_island_of_anchored_floating_and_yielding_bodies(program):
         if np.isfinite(mat.yield_stress):
             assert (ostate.plastic[:, 9] > 0).any()
             assert np.abs(eq - ostate.plastic[:, 9]).max() <= 1e-4 * ostate.plastic[:, 9].max()
+
+
+def test_solver_state_through_the_adapter(tmp_path):
+    """deformable::step with a caller-held DeformableSolverState*: the adapter
+    turns the device factor on and writes SolverStats back (one refresh for
+    the first factored step)."""
+    from tests.test_adapter import PROGRAM as SMALL
+    if shutil.which("g++") is None:
+        pytest.skip("g++ missing")
+    capi.lib()
+    stub = tmp_path / "talus" / "deformable" / "solver"
+    stub.mkdir(parents=True)
+    (stub / "solver.h").write_text(STAND_IN)
+    (tmp_path / "main.cc").write_text(SMALL)
+    exe = tmp_path / "adapter"
+    libdir = os.path.join(ROOT, "talus_b200")
+    subprocess.run(["g++", "-std=c++20", "-Wall", "-Werror", f"-I{tmp_path}", f"-I{os.path.join(ROOT, 'include')}",
+                    "-o", str(exe), str(tmp_path / "main.cc"), f"-L{libdir}", "-ltalus_fem", f"-Wl,-rpath,{libdir}"],
+                   check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "factored 0 refactors 1" in out.stdout, out.stdout
