@@ -233,8 +233,9 @@ int32_t tl_system_set_solver(tl_system* system, uint32_t form);
  * solver.h:54; 0: the iteration cap).  The factor is made on the host
  * (nested-dissection order, block up-looking Cholesky) and applied on the
  * device inside the PCG launch (kPcgFactor).  Needs a one-body system with
- * the assembled operator available, the corotated law on the small-strain
- * path and no stiffness damping: TL_ERR_UNSUPPORTED otherwise.  enable = 0 drops the state. */
+ * the assembled operator available and the corotated law on the small-strain
+ * path (with or without stiffness damping, whose blocks the factor holds):
+ * TL_ERR_UNSUPPORTED otherwise.  enable = 0 drops the state. */
 int32_t tl_system_use_factor(tl_system* system, uint32_t enable, uint32_t factor_budget);
 
 /* SolverStats (factor.h:28-38), the SystemFactor's size (factor.h:50-62) and

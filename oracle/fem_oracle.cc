@@ -43,7 +43,7 @@ struct or_solver {
   std::vector<uint8_t> anchored;
   std::vector<double> refPosition;     // FactorReference::positions [3 nodes]
   double refCentroid[3] = {0.0, 0.0, 0.0};
-  double refStep = 0.0, refInertia = 1.0;
+  double refStep = 0.0, refInertia = 1.0, refDamping = 0.0;  // FactorReference step, inertia, damping key
   or_solver_stats stats{};
   float meanIterations = 0.0f;         // SolverStats::meanIterations is a float
 };
@@ -1246,7 +1246,7 @@ std::array<M3<double>, 16> preciseTetBlocks(const Solver<R>& s, const Element<R>
 // positions and centroid are the state's.
 template <class R>
 void refreshFactor(or_solver& f, const Solver<R>& s, const std::vector<double>& youngs,
-                   const std::vector<double>& poisson, R step, R inertia) {
+                   const std::vector<double>& poisson, R step, R inertia, R damping) {
   const uint32_t V = s.V;
   const size_t n = size_t(3) * V;
   if (f.analyzed && f.nodes != V) f.analyzed = false;
@@ -1285,7 +1285,24 @@ void refreshFactor(or_solver& f, const Solver<R>& s, const std::vector<double>& 
   auto at = [&](size_t i, size_t j) -> double& { return f.env[f.start[i] + (j - f.first[i])]; };
   for (uint32_t e = 0; e < s.T; ++e) {
     const Element<R>& el = s.elements[e];
-    const std::array<M3<double>, 16> blocks = preciseTetBlocks(s, el, youngs[e], poisson[e], s.rotation[e], step);
+    std::array<M3<double>, 16> blocks = preciseTetBlocks(s, el, youngs[e], poisson[e], s.rotation[e], step);
+    // factor.cc:346-366, 386-389: the damping blocks weight * dampingBlocks(rigidFit(corners), R, K),
+    // the fit at the state's positions, in the step's arithmetic (dampingBlocks, factor.cc:274-298)
+    const R weight = damping * el.tau;
+    if (weight != R(0)) {
+      const RigidFit<R> fit = rigidFit(s.gather(s.position, el));
+      std::array<V3<R>, 4> unit, column;
+      for (int corner = 0; corner < 4; ++corner)
+        for (int axis = 0; axis < 3; ++axis) {
+          unit.fill(V3<R>());
+          unit[corner][axis] = R(1);
+          applyDamping(fit, s.rotation[e], s.store[e], unit, column);
+          for (int row = 0; row < 4; ++row) {
+            const V3<R> scaled = weight * column[row];
+            blocks[4 * row + corner][axis] += V3<double>(double(scaled.x), double(scaled.y), double(scaled.z));
+          }
+        }
+    }
     for (int a = 0; a < 4; ++a)
       for (int b = 0; b < 4; ++b) {
         const uint32_t na = el.nodes[a], nb = el.nodes[b];
@@ -1317,6 +1334,7 @@ void refreshFactor(or_solver& f, const Solver<R>& s, const std::vector<double>& 
   ++f.born;
   f.refStep = double(step);
   f.refInertia = double(inertia);
+  f.refDamping = double(damping);
   f.refPosition.assign(n, 0.0);
   V3<R> centroid;
   R total = 0;
@@ -1422,8 +1440,8 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
   if (s.hencky) anyYields = false;  // each step is elastic from the plastic rest
   // damping is defined with the corotated stiffness and committed rotation
   if (s.damped && s.law == OR_LAW_SNH) return -3;
-  // a factor is restated for undamped bodies on the small-strain path
-  if (solver && (s.damped || s.hencky)) return -3;
+  // a factor is restated for the small-strain path
+  if (solver && s.hencky) return -3;
   if (s.damped) s.fits.assign(T, RigidFit<R>());
   auto sized = [&](std::vector<V3<R>>& v) { v.assign(V, V3<R>()); };
   sized(s.force); sized(s.right); sized(s.residual); sized(s.direction); sized(s.applied); sized(s.conditioned);
@@ -1457,9 +1475,12 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
   bool plasticGrowth = false;
   // solver.cc:3639-3655: the caller's factor is made again when it is empty
   // or was made for another step or inertia
+  // dampingStep (solver.cc:3592): the damping scale when a material damps; the
+  // reference compares the per-lane keys scale * tau, equal exactly when the scales are
+  const R dampingStep = s.damped ? s.dampScale : R(0);
   if (solver && (!solver->ready || solver->refStep != double(effective.step) ||
-                 solver->refInertia != double(effective.inertia))) {
-    refreshFactor(*solver, s, factorYoungs, factorPoisson, effective.step, effective.inertia);
+                 solver->refInertia != double(effective.inertia) || solver->refDamping != double(dampingStep))) {
+    refreshFactor(*solver, s, factorYoungs, factorPoisson, effective.step, effective.inertia, dampingStep);
     solver->stats.factor_age = 0u;
     ++solver->stats.refactor_count;
   }
@@ -1558,7 +1579,7 @@ int stepImpl(const or_mesh* mesh, or_state* st, const or_material* materials, ui
         fs.wasted_iterations += r.iterations;
         fs.refresh_requested = 1u;
         solution = s.restart;
-        refreshFactor(*solver, s, factorYoungs, factorPoisson, effective.step, effective.inertia);
+        refreshFactor(*solver, s, factorYoungs, factorPoisson, effective.step, effective.inertia, dampingStep);
         ++fs.refactors;
         ++fs.retries;
         ++fs.refactor_count;

@@ -17,7 +17,136 @@
 #include <numeric>
 #include <vector>
 
+#include "tl_math.cuh"
+
 namespace tl {
+
+// factor.cc:49-88 preciseTetBlocks: the 16 blocks step^2 R K R^T in FP64,
+// row-major, with Dm and V recomputed from the rest positions (q: the
+// tet's nodes, R row-major; preciseLame, factor.cc:21-30).
+inline void factorTetBlocks(const double* rest, const uint32_t* q, double youngs, double poisson, const double* R,
+                            double step, double* out) {
+  double m[3][3];  // columns: the edges from node 0
+  for (int k = 0; k < 3; ++k)
+    for (int r = 0; r < 3; ++r) m[r][k] = rest[3 * size_t(q[k + 1]) + r] - rest[3 * size_t(q[0]) + r];
+  const double c00 = m[1][1] * m[2][2] - m[1][2] * m[2][1], c01 = m[1][2] * m[2][0] - m[1][0] * m[2][2],
+               c02 = m[1][0] * m[2][1] - m[1][1] * m[2][0];
+  const double det = m[0][0] * c00 + m[0][1] * c01 + m[0][2] * c02;
+  const double volume = det / 6.0, inv = 1.0 / det;
+  // rows of m^-1 = the gradients of nodes 1..3 (adjugate / determinant)
+  double g[4][3];
+  g[1][0] = c00 * inv;
+  g[2][0] = c01 * inv;
+  g[3][0] = c02 * inv;
+  g[1][1] = (m[0][2] * m[2][1] - m[0][1] * m[2][2]) * inv;
+  g[2][1] = (m[0][0] * m[2][2] - m[0][2] * m[2][0]) * inv;
+  g[3][1] = (m[0][1] * m[2][0] - m[0][0] * m[2][1]) * inv;
+  g[1][2] = (m[0][1] * m[1][2] - m[0][2] * m[1][1]) * inv;
+  g[2][2] = (m[0][2] * m[1][0] - m[0][0] * m[1][2]) * inv;
+  g[3][2] = (m[0][0] * m[1][1] - m[0][1] * m[1][0]) * inv;
+  for (int r = 0; r < 3; ++r) g[0][r] = -(g[1][r] + g[2][r] + g[3][r]);
+  const double nu = std::clamp(poisson, 0.0, 0.49);
+  const double lambda = youngs * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = youngs / (2.0 * (1.0 + nu));
+  const double scale = step * step;
+  for (int a = 0; a < 4; ++a)
+    for (int b = 0; b < 4; ++b) {
+      const double gab = g[a][0] * g[b][0] + g[a][1] * g[b][1] + g[a][2] * g[b][2];
+      double k[3][3], t[3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+          k[i][j] = volume * (lambda * g[a][i] * g[b][j] + mu * g[b][i] * g[a][j] + (i == j ? mu * gab : 0.0));
+      for (int i = 0; i < 3; ++i)  // t = R k
+        for (int j = 0; j < 3; ++j) t[i][j] = R[3 * i] * k[0][j] + R[3 * i + 1] * k[1][j] + R[3 * i + 2] * k[2][j];
+      double* o = out + 9 * (4 * a + b);
+      for (int i = 0; i < 3; ++i)  // o = step^2 t R^T
+        for (int j = 0; j < 3; ++j)
+          o[3 * i + j] = scale * (t[i][0] * R[3 * j] + t[i][1] * R[3 * j + 1] + t[i][2] * R[3 * j + 2]);
+    }
+}
+
+// factor.cc:274-298, 780-853 dampingBlocks: the 16 blocks of Pi R K R^T Pi,
+// Pi the removal of the rigid motion fitted to the corners x (rigidFit,
+// factor.cc:780-818: mean translation and the spin I^-1 sum a x v about the
+// centroid, I pseudo-inverted when nearly singular), K from Dm^-1 and V
+// (tetStiffness, material.cc:209-234), in FP64, row-major.
+inline void factorDampingBlocks(const double* x, const double* R, const double* Dm, double volume, double youngs,
+                                double poisson, double* out) {
+  double centre[3] = {0, 0, 0}, arm[4][3], I[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (int c = 0; c < 4; ++c)
+    for (int r = 0; r < 3; ++r) centre[r] += x[3 * c + r];
+  for (int r = 0; r < 3; ++r) centre[r] *= 0.25;
+  for (int c = 0; c < 4; ++c) {
+    for (int r = 0; r < 3; ++r) arm[c][r] = x[3 * c + r] - centre[r];
+    const double aa = arm[c][0] * arm[c][0] + arm[c][1] * arm[c][1] + arm[c][2] * arm[c][2];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) I[i][j] += (i == j ? aa : 0.0) - arm[c][i] * arm[c][j];
+  }
+  const double third = (I[0][0] + I[1][1] + I[2][2]) / 3.0;
+  M3<double> m;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) m.m[i][j] = I[i][j];
+  double inv[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  const double det = det3(m);
+  if (det > 1.0e-6 * third * third * third) {
+    const M3<double> cf = cofactor(m);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) inv[i][j] = cf.m[j][i] / det;
+  } else {
+    double a[3][3], v[3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) a[i][j] = I[i][j];
+    jacobiEigen3(a, v);
+    for (int k = 0; k < 3; ++k) {
+      if (!(a[k][k] > 1.0e-6 * third)) continue;
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) inv[i][j] += v[i][k] * v[j][k] / a[k][k];
+    }
+  }
+  auto removeRigid = [&](double v[4][3]) {
+    double mean[3] = {0, 0, 0}, moment[3] = {0, 0, 0}, spin[3];
+    for (int c = 0; c < 4; ++c)
+      for (int r = 0; r < 3; ++r) {
+        mean[r] += v[c][r];
+        moment[r] += arm[c][(r + 1) % 3] * v[c][(r + 2) % 3] - arm[c][(r + 2) % 3] * v[c][(r + 1) % 3];
+      }
+    for (int r = 0; r < 3; ++r) {
+      mean[r] *= 0.25;
+      spin[r] = inv[r][0] * moment[0] + inv[r][1] * moment[1] + inv[r][2] * moment[2];
+    }
+    for (int c = 0; c < 4; ++c)
+      for (int r = 0; r < 3; ++r)
+        v[c][r] -= mean[r] + spin[(r + 1) % 3] * arm[c][(r + 2) % 3] - spin[(r + 2) % 3] * arm[c][(r + 1) % 3];
+  };
+  double g[4][3];
+  for (int k = 0; k < 3; ++k)
+    for (int r = 0; r < 3; ++r) g[k + 1][r] = Dm[3 * k + r];
+  for (int r = 0; r < 3; ++r) g[0][r] = -(g[1][r] + g[2][r] + g[3][r]);
+  const double nu = std::clamp(poisson, 0.0, 0.49);
+  const double lambda = youngs * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = youngs / (2.0 * (1.0 + nu));
+  for (int corner = 0; corner < 4; ++corner)
+    for (int axis = 0; axis < 3; ++axis) {
+      double v[4][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, un[4][3], y[4][3];
+      v[corner][axis] = 1.0;
+      removeRigid(v);
+      for (int c = 0; c < 4; ++c)  // R^T v
+        for (int r = 0; r < 3; ++r) un[c][r] = R[r] * v[c][0] + R[3 + r] * v[c][1] + R[6 + r] * v[c][2];
+      for (int row = 0; row < 4; ++row) {
+        double sum[3] = {0, 0, 0};
+        for (int col = 0; col < 4; ++col) {
+          const double gab = g[row][0] * g[col][0] + g[row][1] * g[col][1] + g[row][2] * g[col][2];
+          for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+              sum[i] += volume * (lambda * g[row][i] * g[col][j] + mu * g[col][i] * g[row][j] + (i == j ? mu * gab : 0.0)) *
+                        un[col][j];
+        }
+        for (int r = 0; r < 3; ++r) y[row][r] = R[3 * r] * sum[0] + R[3 * r + 1] * sum[1] + R[3 * r + 2] * sum[2];
+      }
+      removeRigid(y);
+      for (int row = 0; row < 4; ++row)
+        for (int r = 0; r < 3; ++r) out[9 * (4 * row + corner) + 3 * r + axis] = y[row][r];
+    }
+}
+
 
 struct BlockFactor {
   uint32_t nodes = 0;

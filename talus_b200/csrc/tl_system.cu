@@ -733,6 +733,9 @@ struct System final : SystemBase {
           for (int k = 0; k < 4; ++k) fTets.push_back(d.tet_nodes[4 * size_t(t) + k]);
           fYoungs.push_back(d.element_youngs ? d.element_youngs[t] : (l < d.lanes ? d.materials[l].youngs_modulus : 0.0));
           fPoisson.push_back(l < d.lanes ? d.materials[l].poissons_ratio : 0.3);
+          fTau.push_back(laneTau[laneBase + l]);
+          fVol.push_back(d.volume[t]);
+          for (int k = 0; k < 9; ++k) fDm.push_back(d.rest_inverse[9 * size_t(t) + k]);
         }
       }
       if (b == 0) {
@@ -1512,7 +1515,7 @@ struct System final : SystemBase {
   tl_factor_stats fStats{};
   float fMean = 0.0f;                  // SolverStats::meanIterations is a float
   std::vector<uint32_t> fTets;         // body 0: tets, per-tet Young's modulus and Poisson ratio, anchors, masses
-  std::vector<double> fYoungs, fPoisson, fMass;
+  std::vector<double> fYoungs, fPoisson, fMass, fTau, fVol, fDm;  // fDm: Dm^-1 row-major
   std::vector<uint8_t> fAnch;
   DevBuf<uint32_t> dfPerm, dfIperm, dfRowStart, dfRowCol, dfColStart, dfColRow, dfFlags, dfTicket, dfSnStart,
       dfRowSplit, dfColSplit;
@@ -1529,7 +1532,6 @@ struct System final : SystemBase {
     }
     if (B != 1) throw StatusError{TL_ERR_UNSUPPORTED, "a solver state is held for one-body systems"};
     if (!sellReady) throw StatusError{TL_ERR_UNSUPPORTED, "the factored PCG needs the assembled operator"};
-    if (hasDamping) throw StatusError{TL_ERR_UNSUPPORTED, "the factor is made without stiffness damping"};
     if (hencky) throw StatusError{TL_ERR_UNSUPPORTED, "the factor is made for the small-strain path"};
     factorOn = true;
     factorBudget = budget;
@@ -1579,55 +1581,14 @@ struct System final : SystemBase {
     return f;
   }
   double fCurStep = 0.0, fCurInertia = 1.0;  // the current step's h and (1 - alpha_m)
+  double fCurDamping = 0.0, fDamping = 0.0;   // the current step's damping scale, the factor's
   uint32_t fCgLimit = 0u;                     // Settings::cgIterations of the current step
 
-  // factor.cc:49-88 preciseTetBlocks: the 16 blocks step^2 R K R^T in FP64,
-  // row-major, with Dm and V recomputed from the rest positions (q: the
-  // tet's nodes, R row-major; preciseLame, factor.cc:21-30).
-  static void preciseTetBlocks(const double* rest, const uint32_t* q, double youngs, double poisson, const double* R,
-                               double step, double* out) {
-    double m[3][3];  // columns: the edges from node 0
-    for (int k = 0; k < 3; ++k)
-      for (int r = 0; r < 3; ++r) m[r][k] = rest[3 * size_t(q[k + 1]) + r] - rest[3 * size_t(q[0]) + r];
-    const double c00 = m[1][1] * m[2][2] - m[1][2] * m[2][1], c01 = m[1][2] * m[2][0] - m[1][0] * m[2][2],
-                 c02 = m[1][0] * m[2][1] - m[1][1] * m[2][0];
-    const double det = m[0][0] * c00 + m[0][1] * c01 + m[0][2] * c02;
-    const double volume = det / 6.0, inv = 1.0 / det;
-    // rows of m^-1 = the gradients of nodes 1..3 (adjugate / determinant)
-    double g[4][3];
-    g[1][0] = c00 * inv;
-    g[2][0] = c01 * inv;
-    g[3][0] = c02 * inv;
-    g[1][1] = (m[0][2] * m[2][1] - m[0][1] * m[2][2]) * inv;
-    g[2][1] = (m[0][0] * m[2][2] - m[0][2] * m[2][0]) * inv;
-    g[3][1] = (m[0][1] * m[2][0] - m[0][0] * m[2][1]) * inv;
-    g[1][2] = (m[0][1] * m[1][2] - m[0][2] * m[1][1]) * inv;
-    g[2][2] = (m[0][2] * m[1][0] - m[0][0] * m[1][2]) * inv;
-    g[3][2] = (m[0][0] * m[1][1] - m[0][1] * m[1][0]) * inv;
-    for (int r = 0; r < 3; ++r) g[0][r] = -(g[1][r] + g[2][r] + g[3][r]);
-    const double nu = std::clamp(poisson, 0.0, 0.49);
-    const double lambda = youngs * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = youngs / (2.0 * (1.0 + nu));
-    const double scale = step * step;
-    for (int a = 0; a < 4; ++a)
-      for (int b = 0; b < 4; ++b) {
-        const double gab = g[a][0] * g[b][0] + g[a][1] * g[b][1] + g[a][2] * g[b][2];
-        double k[3][3], t[3][3];
-        for (int i = 0; i < 3; ++i)
-          for (int j = 0; j < 3; ++j)
-            k[i][j] = volume * (lambda * g[a][i] * g[b][j] + mu * g[b][i] * g[a][j] + (i == j ? mu * gab : 0.0));
-        for (int i = 0; i < 3; ++i)  // t = R k
-          for (int j = 0; j < 3; ++j) t[i][j] = R[3 * i] * k[0][j] + R[3 * i + 1] * k[1][j] + R[3 * i + 2] * k[2][j];
-        double* o = out + 9 * (4 * a + b);
-        for (int i = 0; i < 3; ++i)  // o = step^2 t R^T
-          for (int j = 0; j < 3; ++j)
-            o[3 * i + j] = scale * (t[i][0] * R[3 * j] + t[i][1] * R[3 * j + 1] + t[i][2] * R[3 * j + 2]);
-      }
-  }
-
   // refreshFactor (factor.cc:567-618) for body 0: the system at the rotations
-  // of the last element pass, factored; the FactorReference positions and
+  // of the last element pass, with the damping blocks at the body's positions
+  // when a material damps, factored; the FactorReference positions and
   // centre are the body's now.
-  void factorRefresh(double step, double inertia) {
+  void factorRefresh(double step, double inertia, double damping) {
     const auto t0 = std::chrono::steady_clock::now();
     const BodyDev& bd = bodyHost[0];
     const HostBody& h = hb[0];
@@ -1677,8 +1638,16 @@ struct System final : SystemBase {
     }
     std::vector<double> blocks(size_t(144) * T), diag(size_t(9) * V, 0.0);
     parallelFor(T, [&](size_t e0, size_t e1) {
-      for (size_t e = e0; e < e1; ++e)
-        preciseTetBlocks(h.rest.data(), &fTets[4 * e], fYoungs[e], fPoisson[e], &rot[9 * e], step, &blocks[144 * e]);
+      for (size_t e = e0; e < e1; ++e) {
+        factorTetBlocks(h.rest.data(), &fTets[4 * e], fYoungs[e], fPoisson[e], &rot[9 * e], step, &blocks[144 * e]);
+        const double weight = damping * double(S(fTau[e]));
+        if (weight == 0.0) continue;
+        double corners[12], d[144];
+        for (int c = 0; c < 4; ++c)
+          for (int r = 0; r < 3; ++r) corners[3 * c + r] = x[3 * size_t(fTets[4 * e + c]) + r];
+        factorDampingBlocks(corners, &rot[9 * e], &fDm[9 * e], fVol[e], fYoungs[e], fPoisson[e], d);
+        for (int q = 0; q < 144; ++q) blocks[144 * e + q] += weight * d[q];
+      }
     });
     for (uint32_t v = 0; v < V; ++v) {
       const double d = fAnch[v] ? 1.0 : inertia * double(S(fMass[v]));
@@ -1692,6 +1661,7 @@ struct System final : SystemBase {
     ++fStats.generation;
     fStep = step;
     fInertia = inertia;
+    fDamping = damping;
     std::vector<Vec4<double>> ref(size_t(V) + 1);
     double total = 0.0, c[3] = {0.0, 0.0, 0.0};
     for (uint32_t v = 0; v < V; ++v) {
@@ -1737,7 +1707,7 @@ struct System final : SystemBase {
     SellDev<S> g = sellView();
     const unsigned blocks = (sellUpperCount + TILE - 1) / TILE;
     if (profiling) mark(1, true);
-    assembleSell(s, g, blocks, law == TL_LAW_SNH ? 1 : 0, false, tangent, pass);
+    assembleSell(s, g, blocks, law == TL_LAW_SNH ? 1 : 0, hasDamping && law != TL_LAW_SNH, tangent, pass);
     check();
     ++launches;
     if (profiling) {
@@ -1754,7 +1724,7 @@ struct System final : SystemBase {
       fStats.wasted_iterations += c.taken;
       fStats.refresh_requested = 1u;
       TL_CUDA(cudaMemcpyAsync(X, dfRestart.ptr, size_t(Vp) * sizeof(Vec4<S>), cudaMemcpyDeviceToDevice, st));
-      factorRefresh(fCurStep, fCurInertia);
+      factorRefresh(fCurStep, fCurInertia, fCurDamping);
       ++fStats.refactors;
       ++fStats.retries;
       ++fStats.refactor_count;
@@ -1920,17 +1890,19 @@ struct System final : SystemBase {
     std::vector<tl_step_report> local(B);
     fPrepared = false;
     if (factorOn) {
-      if (B != 1 || hasDamping || hencky)
-        throw StatusError{TL_ERR_UNSUPPORTED, "a solver state needs one undamped body on the small-strain path"};
+      if (B != 1 || hencky)
+        throw StatusError{TL_ERR_UNSUPPORTED, "a solver state needs one body on the small-strain path"};
       // the factor is made at the committed rotations, which the SNH operator state replaces
       if (law == TL_LAW_SNH) throw StatusError{TL_ERR_UNSUPPORTED, "a solver state is held for the corotated law"};
       // solver.cc:3639-3655: the factor is made again when it is empty or was
       // made for another step or inertia
       fCurStep = hs[0].hstep;
       fCurInertia = hs[0].inertia;
+      // dampingStep (solver.cc:3592): (1 - alpha_f) gamma h when a material damps
+      fCurDamping = hasDamping ? (1.0 - rule.alphaForce) * rule.gamma * hs[0].inner : 0.0;
       fCgLimit = set.cg_iterations;
-      if (!fHost.ready || fStep != fCurStep || fInertia != fCurInertia) {
-        factorRefresh(fCurStep, fCurInertia);
+      if (!fHost.ready || fStep != fCurStep || fInertia != fCurInertia || fDamping != fCurDamping) {
+        factorRefresh(fCurStep, fCurInertia, fCurDamping);
         fStats.factor_age = 0u;
         ++fStats.refactor_count;
       }

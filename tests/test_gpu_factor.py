@@ -99,6 +99,17 @@ def test_factored_plastic_block_with_refreshes_fp64_matches_oracle():
     assert gstats["retries"] > 0 and gstats["wasted_iterations"] > 0
 
 
+def test_factored_damped_block_fp64_matches_oracle():
+    """Stiffness damping: the factor holds the damping blocks at the state's
+    positions (factor.cc:346-366), refreshed with the damping scale."""
+    mesh, _ = elastic_block()
+    mat = tb.PhysicalMaterial(density=1000.0, youngs_modulus=1e6, poissons_ratio=0.3, stiffness_damping=0.02)
+    errors, greps, oreps, gstats, ostats, _ = run_factored(tb.FP64, mesh, mat, tb.Settings(), 6, budget=32)
+    assert max(errors) <= 1e-9, errors
+    assert [r["cg_iterations"] for r in greps] == [r["cg_iterations"] for r in oreps]
+    assert_same_counters(gstats, ostats)
+
+
 def test_factored_spinning_free_body_fp64_matches_oracle():
     """A floating body: the factor is applied in the body's rotation since
     the refresh (bodyRotation)."""
@@ -138,16 +149,17 @@ def test_step_change_refreshes_the_factor():
     system.close()
 
 
-def test_solver_state_needs_one_undamped_body():
+def test_solver_state_needs_one_body_and_the_corotated_law():
     mesh, mat = elastic_block((2, 2, 2))
     batch = tb.System([mesh, mesh], [[mat], [mat]], tb.FP64)
     with pytest.raises(capi.TalusError) as e:
         batch.use_factor(True, 32)
     assert e.value.status == capi.TL_ERR_UNSUPPORTED
     batch.close()
-    damped = tb.PhysicalMaterial(density=1000.0, youngs_modulus=1e6, poissons_ratio=0.3, stiffness_damping=0.01)
-    system = tb.System(mesh, [damped], tb.FP64)
+    system = tb.System(mesh, [mat], tb.FP64)
+    system.use_factor(True, 32)
+    system.set_state(tb.rest_state(mesh))
     with pytest.raises(capi.TalusError) as e:
-        system.use_factor(True, 32)
+        system.step(tb.Settings(law=tb.NEO_HOOKEAN), GRAVITY, DT)
     assert e.value.status == capi.TL_ERR_UNSUPPORTED
     system.close()

@@ -66,3 +66,17 @@ def test_a_new_step_length_refreshes_the_factor():
     for dt in (DT, DT, DT / 2):
         po.step(po.F64, om, state, [oracle_material(mat)], oracle_settings(tb.Settings()), GRAVITY, dt, solver=solver)
     assert solver.stats()["refactor_count"] == 2
+
+
+def test_damped_factor_conditions_the_damped_system():
+    """With stiffness damping the factor holds the damping blocks too
+    (factor.cc:346-366): the factored step solves the same damped equations."""
+    mesh, _ = elastic_block((5, 5, 5))
+    mat = tb.PhysicalMaterial(density=1000.0, youngs_modulus=1e6, poissons_ratio=0.3, stiffness_damping=0.02)
+    settings = tb.Settings(tolerance=1e-9, cg_iterations=500)
+    plain, preps = run(mesh, mat, settings, 3)
+    solver = po.Solver(32)
+    fact, freps = run(mesh, mat, settings, 3, solver)
+    assert relative_error(fact.position, plain.position, mesh.rest_positions) <= 1e-6
+    assert sum(r["cg_iterations"] for r in freps) * 4 < sum(r["cg_iterations"] for r in preps)
+    assert solver.stats()["refactor_count"] == 1
