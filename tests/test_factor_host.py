@@ -23,6 +23,11 @@ void fh_damping_blocks(const double* x, const double* R, const double* Dm, doubl
 }
 // A lattice of nx*ny*nz nodes, 6 tets per cube, the j == 0 plane anchored, random SPD element blocks:
 // the factor's solve of A x = b against A x, max |A x - b| / max |b|.
+// The supernode order the device solves rely on: the supernodes cover the rows
+// once in order, every parent comes after its children, and every block of a
+// row's L lies in the row's own supernode or a descendant of it.  0 if it
+// holds; otherwise the number of violations.
+int fh_supernode_violations(int nx, int ny, int nz);
 double fh_solve_residual(int nx, int ny, int nz, unsigned seed) {
   const uint32_t V = nx * ny * nz;
   std::vector<double> rest(3 * V);
@@ -93,6 +98,48 @@ double fh_solve_residual(int nx, int ny, int nz, unsigned seed) {
   for (size_t q = 0; q < 3 * V; ++q) { err = std::max(err, std::abs(ax[q] - b[q])); nb = std::max(nb, std::abs(b[q])); }
   return err / nb;
 }
+int fh_supernode_violations(int nx, int ny, int nz) {
+  const uint32_t V = nx * ny * nz;
+  std::vector<double> rest(3 * V);
+  std::vector<uint8_t> anch(V, 0);
+  auto id = [&](int i, int j, int k) { return uint32_t(i + nx * (j + ny * k)); };
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const uint32_t v = id(i, j, k);
+        rest[3 * v] = i; rest[3 * v + 1] = j; rest[3 * v + 2] = k;
+        anch[v] = j == 0 || j == ny - 1;
+      }
+  std::vector<uint32_t> tets;
+  const int T6[6][4] = {{0, 1, 3, 7}, {0, 1, 5, 7}, {0, 2, 3, 7}, {0, 2, 6, 7}, {0, 4, 5, 7}, {0, 4, 6, 7}};
+  for (int k = 0; k + 1 < nz; ++k)
+    for (int j = 0; j + 1 < ny; ++j)
+      for (int i = 0; i + 1 < nx; ++i) {
+        uint32_t c[8];
+        for (int q = 0; q < 8; ++q) c[q] = id(i + (q & 1), j + ((q >> 1) & 1), k + ((q >> 2) & 1));
+        for (auto& t : T6) for (int q = 0; q < 4; ++q) tets.push_back(c[t[q]]);
+      }
+  BlockFactor f;
+  f.analyze(V, anch.data(), tets, rest.data());
+  const size_t S = f.snParent.size();
+  int bad = 0;
+  if (f.snStart.front() != 0 || f.snStart.back() != V) ++bad;
+  std::vector<int32_t> snOf(V, -1);
+  for (size_t p = 0; p < S; ++p) {
+    if (f.snStart[p] > f.snStart[p + 1]) ++bad;
+    for (uint32_t i = f.snStart[p]; i < f.snStart[p + 1]; ++i) snOf[i] = int32_t(p);
+    if (f.snParent[p] >= 0 && f.snParent[p] <= int32_t(p)) ++bad;
+    for (int c = 0; c < 2; ++c) {
+      const int32_t ch = f.snChild[2 * p + c];
+      if (ch >= 0 && f.snParent[ch] != int32_t(p)) ++bad;
+    }
+  }
+  auto within = [&](int32_t a, int32_t p) { for (; a >= 0; a = f.snParent[a]) if (a == p) return true; return false; };
+  for (uint32_t i = 0; i < V; ++i)
+    for (uint32_t k = f.rowStart[i]; k < f.rowStart[i + 1]; ++k)
+      if (!within(snOf[f.rowCol[k]], snOf[i])) ++bad;
+  return bad;
+}
 }
 """
 
@@ -110,12 +157,21 @@ def fh(tmp_path_factory):
     handle.fh_damping_blocks.argtypes = [C.c_void_p] * 3 + [C.c_double] * 3 + [C.c_void_p]
     handle.fh_solve_residual.argtypes = [C.c_int, C.c_int, C.c_int, C.c_uint]
     handle.fh_solve_residual.restype = C.c_double
+    handle.fh_supernode_violations.argtypes = [C.c_int, C.c_int, C.c_int]
     return handle
 
 
 @pytest.mark.parametrize("dims", [(3, 3, 3), (6, 5, 5), (12, 6, 6)])
 def test_block_factor_solves_its_system(fh, dims):
     assert fh.fh_solve_residual(*dims, 7) <= 1e-10
+
+
+@pytest.mark.parametrize("dims", [(3, 3, 3), (17, 9, 9), (9, 17, 5), (33, 17, 17)])
+def test_supernodes_order_the_solves(fh, dims):
+    """The device solves hand supernodes out children first (forward) and
+    parents first (backward), each waiting on the supernodes it reads: that
+    needs every row's blocks to lie in its own supernode or below it."""
+    assert fh.fh_supernode_violations(*dims) == 0
 
 
 def test_damping_blocks_are_the_oracle_damping_operator(fh):
