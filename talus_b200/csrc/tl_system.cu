@@ -1975,7 +1975,14 @@ struct System final : SystemBase {
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     int32_t status = TL_OK;
-    if (hsy->error != 0) throw StatusError{TL_ERR_TIMEOUT, "a PCG grid barrier ran out of time"};
+    if (hsy->error != 0) {
+      if (dfFlags.ptr) {  // a factored solve may have left mid-application: its flags start over
+        dfFlags.zero(st);
+        dfTicket.zero(st);
+        TL_CUDA(cudaStreamSynchronize(st));
+      }
+      throw StatusError{TL_ERR_TIMEOUT, "a PCG grid barrier ran out of time"};
+    }
     for (uint32_t b = 0; b < B; ++b) {
       if (!reports) continue;
       tl_step_report& r = reports[b];

@@ -57,3 +57,27 @@ def test_a_wait_that_runs_out_in_an_early_solve_is_reported_at_the_step_end(solv
     assert report.cg_iterations > 0
     assert np.isfinite(system.get_state().position).all()
     system.close()
+
+
+@pytest.mark.parametrize("solve", [0, 2])
+def test_factored_solve_reports_an_expired_wait(solve):
+    """The same host-armed expiry on a system with a solver state: the
+    factored PCG (kPcgFactor, whose grid barriers and supernode waits are
+    bounded the same way) leaves at its first barrier, the step returns
+    TL_ERR_TIMEOUT, and the next step runs normally with the factor."""
+    mesh, mat = elastic_block((4, 4, 4), seed=6)
+    system = tb.System(mesh, [mat], tb.FP64)
+    system.use_factor(True, 32)
+    system.set_state(tb.rest_state(mesh))
+    system.step(tb.Settings(), GRAVITY, DT)
+    assert capi.lib().tl_system_expire_wait(system.handle, solve) == capi.TL_OK
+    reports = (tb.StepReport * 1)()
+    g = np.asarray(GRAVITY, np.float64)
+    rc = capi.lib().tl_step(system.handle, C.byref(tb.Settings()._c()), g.ctypes.data, DT, reports)
+    assert rc == capi.TL_ERR_TIMEOUT
+    system.set_state(tb.rest_state(mesh))
+    report = system.step(tb.Settings(), GRAVITY, DT)[0]
+    assert report.cg_iterations > 0
+    assert np.isfinite(system.get_state().position).all()
+    assert system.factor_stats()["ready"] == 1
+    system.close()
