@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol():
 def test_struct_layout_matches_the_header():
     structs = {"tl_material": capi.tl_material, "tl_mesh_desc": capi.tl_mesh_desc,
                "tl_settings": capi.tl_settings, "tl_step_report": capi.tl_step_report,
-               "tl_rollout_desc": capi.tl_rollout_desc}
+               "tl_rollout_desc": capi.tl_rollout_desc, "tl_factor_stats": capi.tl_factor_stats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for name, cls in structs.items():
         lines.append(f'  printf("{name} size %zu\\n", sizeof({name}));')
