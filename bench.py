@@ -635,6 +635,8 @@ def run_ours(args, spec, rank, world, dist):
     yields = any(np.isfinite(m.yield_stress) and m.yield_stress > 0 for ms in mats for m in ms)
     if not args.no_hencky and not spec.get("batch") and yields:
         result["hencky"] = hencky_form(meshes[0], mats[0], settings, context)
+    if not args.no_solver_state and not spec.get("batch") and world == 1:
+        result["solver_state"] = solver_state_form(context)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_sample(spec)
     if rank == 0:
@@ -771,6 +773,45 @@ def hencky_form(mesh, mats, settings, context, warmup=3, steps=10):
     return out
 
 
+def solver_state_form(context, cells=(16, 8, 8), warmup=1, steps=4, budget=32):
+    """A caller-held solver state (tl_system_use_factor: the FP64 Cholesky
+    preconditioner of deformable::step's DeformableSolverState*) on a
+    plastic block of the benchmark's material at reduced size, FP64, against
+    the same steps with block Jacobi: device time per step from the step
+    reports (the first step, which makes the factor on the host, is a warm-up
+    step), PCG iterations, the factor's host time and size."""
+    import talus_b200 as tb
+    from talus_b200.workloads import WORKLOADS, make_bodies
+
+    spec = dict(WORKLOADS["plastic-block"])
+    spec["cells"] = tuple(cells)
+    meshes, mats = make_bodies(spec)
+    mesh = meshes[0]
+    out = {"workload": f"plastic block {cells[0]}x{cells[1]}x{cells[2]} cells ({mesh.tets} tets), FP64",
+           "factor_budget": budget}
+    for name, factored in (("factor", True), ("jacobi", False)):
+        s = tb.System(mesh, mats[0], tb.FP64, context)
+        s.set_solver("assembled")
+        if factored:
+            s.use_factor(True, budget)
+        s.set_state(tb.rest_state(mesh))
+        seconds, iterations = 0.0, 0
+        for k in range(warmup + steps):
+            rep = s.step(tb.Settings())[0]
+            if k >= warmup:
+                seconds += rep.device_seconds
+                iterations += rep.cg_iterations
+        out[name] = {"ms_per_step": seconds * 1e3 / steps, "pcg_iterations_per_step": iterations / steps}
+        if factored:
+            st = s.factor_stats()
+            out[name].update({"refactor_seconds": st["refactor_seconds"], "factor_nonzeros": st["factor_nonzeros"],
+                              "refactor_count": st["refactor_count"], "retries": st["retries"]})
+        s.close()
+    out["note"] = ("the factored solves are latency-bound on the elimination tree's longest path "
+                   "(kPcgFactor); the factor is made on the host at the first step")
+    return out
+
+
 def matrix_blocks(mesh):
     """Nonzero 3x3 blocks of a body's assembled operator: its nodes (the
     diagonal) plus both directions of every distinct edge of its tets."""
@@ -894,6 +935,7 @@ def main():
     ap.add_argument("--no-converged-check", action="store_true")
     ap.add_argument("--no-hencky", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-solver-state", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
