@@ -163,3 +163,17 @@ def test_solver_state_needs_one_body_and_the_corotated_law():
         system.step(tb.Settings(law=tb.NEO_HOOKEAN), GRAVITY, DT)
     assert e.value.status == capi.TL_ERR_UNSUPPORTED
     system.close()
+
+
+@pytest.mark.parametrize("substeps,budget", [(3, 32), (1, 0)])
+def test_factored_substeps_and_budget_rules_match_oracle(substeps, budget):
+    """Several substeps per step (a frame per substep, substepsSinceRefresh
+    and meanIterations per substep) and a budget of 0 (the iteration cap
+    itself, solver.cc:3814-3817) follow the oracle."""
+    mesh, mat = plastic_block((8, 4, 4))
+    settings = tb.Settings(substeps=substeps)
+    errors, greps, oreps, gstats, ostats, _ = run_factored(tb.FP64, mesh, mat, settings, 3, budget=budget)
+    assert max(errors) <= 1e-8, errors
+    assert [r["cg_iterations"] for r in greps] == [r["cg_iterations"] for r in oreps]
+    assert_same_counters(gstats, ostats)
+    assert gstats["substeps_since_refresh"] == 3 * substeps
