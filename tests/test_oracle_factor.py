@@ -80,3 +80,18 @@ def test_damped_factor_conditions_the_damped_system():
     assert relative_error(fact.position, plain.position, mesh.rest_positions) <= 1e-6
     assert sum(r["cg_iterations"] for r in freps) * 4 < sum(r["cg_iterations"] for r in preps)
     assert solver.stats()["refactor_count"] == 1
+
+
+def test_factored_step_in_the_reference_arithmetic_follows_fp64():
+    """The FP32 restatement (the reference's glm arithmetic) with a solver
+    state stays near the FP64 step without one, at the reference's own FP32
+    error level."""
+    mesh, mat = plastic_block((8, 4, 4))
+    om = to_oracle(mesh)
+    st32, st64 = po.State.rest(om), po.State.rest(om)
+    solver = po.Solver(32)
+    for _ in range(3):
+        po.step(po.F32, om, st32, [oracle_material(mat)], oracle_settings(tb.Settings()), GRAVITY, DT, solver=solver)
+        po.step(po.F64, om, st64, [oracle_material(mat)], oracle_settings(tb.Settings()), GRAVITY, DT)
+    assert relative_error(st32.position, st64.position, mesh.rest_positions) <= 1e-4
+    assert solver.stats()["refactor_count"] == 1
