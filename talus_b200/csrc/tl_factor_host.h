@@ -12,9 +12,11 @@
 #pragma once
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include "tl_math.cuh"
@@ -352,8 +354,11 @@ struct BlockFactor {
             for (int q = 0; q < 9; ++q) rowBlk[9 * size_t(k) + q] += B[q];
           }
         }
-    std::vector<uint32_t> where(V, 0u), colFill(colStart.begin(), colStart.end() - 1);
-    for (uint32_t i = 0; i < V; ++i) {
+    std::vector<uint32_t> colFill(colStart.begin(), colStart.end() - 1);
+    // One row of the up-looking factor; `where` is the caller's scratch.  Rows
+    // of supernodes in disjoint subtrees touch disjoint columns, so the
+    // supernodes of one depth of the dissection are factored in parallel.
+    const auto factorRow = [&](uint32_t i, std::vector<uint32_t>& where) -> bool {
       const uint32_t k0 = rowStart[i], k1 = rowStart[i + 1];
       for (uint32_t k = k0; k < k1; ++k) where[rowCol[k]] = k;
       double d[9];
@@ -381,16 +386,16 @@ struct BlockFactor {
       }
       // L_ii = chol(D), lower; its inverse
       double L[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-      if (!(d[0] > 0.0)) return ready = false;
+      if (!(d[0] > 0.0)) return false;
       L[0] = std::sqrt(d[0]);
       L[3] = d[3] / L[0];
       L[6] = d[6] / L[0];
       const double d4 = d[4] - L[3] * L[3];
-      if (!(d4 > 0.0)) return ready = false;
+      if (!(d4 > 0.0)) return false;
       L[4] = std::sqrt(d4);
       L[7] = (d[7] - L[6] * L[3]) / L[4];
       const double d8 = d[8] - L[6] * L[6] - L[7] * L[7];
-      if (!(d8 > 0.0)) return ready = false;
+      if (!(d8 > 0.0)) return false;
       L[8] = std::sqrt(d8);
       double* I = &diagInv[9 * size_t(i)];
       I[0] = 1.0 / L[0];
@@ -404,6 +409,40 @@ struct BlockFactor {
         const uint32_t p = colFill[rowCol[k]]++;
         std::copy_n(&rowBlk[9 * size_t(k)], 9, &colBlk[9 * size_t(p)]);
       }
+      return true;
+    };
+    const size_t S = snParent.size();
+    std::vector<uint32_t> depth(S, 0u);
+    uint32_t deepest = 0;
+    for (size_t p = S; p-- > 0;) {  // parents come after their children
+      depth[p] = snParent[p] >= 0 ? depth[snParent[p]] + 1u : 0u;
+      deepest = std::max(deepest, depth[p]);
+    }
+    std::vector<std::vector<uint32_t>> level(size_t(deepest) + 1);
+    for (size_t p = 0; p < S; ++p) level[depth[p]].push_back(uint32_t(p));
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    std::atomic<bool> failed{false};
+    for (size_t d = level.size(); d-- > 0;) {
+      const std::vector<uint32_t>& here = level[d];
+      std::atomic<size_t> next{0};
+      const auto work = [&]() {
+        std::vector<uint32_t> where(V, 0u);
+        for (size_t q; (q = next.fetch_add(1)) < here.size();)
+          for (uint32_t i = snStart[here[q]]; i < snStart[here[q] + 1]; ++i)
+            if (!factorRow(i, where)) {
+              failed = true;
+              return;
+            }
+      };
+      const unsigned n = unsigned(std::min<size_t>(hw, here.size()));
+      if (n <= 1) {
+        work();
+      } else {
+        std::vector<std::thread> pool;
+        for (unsigned t = 0; t < n; ++t) pool.emplace_back(work);
+        for (std::thread& t : pool) t.join();
+      }
+      if (failed) return ready = false;
     }
     return ready = true;
   }
