@@ -68,11 +68,11 @@ __device__ __forceinline__ uint32_t ldRelaxed(const uint32_t* p) {
   return v;
 }
 
-// Waits until the flags of up to FLAG_BATCH rows all hold epoch: every
-// pending flag is polled at once with relaxed loads, then one acquire fence
-// orders the reads of the rows' values after them.  Bounded: gives up after
-// TL_BARRIER_LIMIT_NS (recording TL_ERR_TIMEOUT) or once another wait or
-// barrier has given up.
+// Waits until flags[j[0..n)] (n <= FLAG_BATCH supernodes) all hold epoch:
+// every pending flag is polled at once with relaxed loads, then one acquire
+// fence orders the reads of those supernodes' values after them.  Bounded:
+// gives up after TL_BARRIER_LIMIT_NS (recording TL_ERR_TIMEOUT) or once
+// another wait or barrier has given up.
 constexpr int FLAG_BATCH = 8;
 __device__ __forceinline__ bool waitFlags(const uint32_t* flags, const uint32_t (&j)[FLAG_BATCH], uint32_t n,
                                           uint32_t epoch, GridSyncDev* sync) {
