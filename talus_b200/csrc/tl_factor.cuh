@@ -286,8 +286,22 @@ __device__ void factorSolve(const FactorDev& f, GridSyncDev* sync, const Vec4<S>
       };
       V3<double> acc = {0, 0, 0};
       if (valid) termR(L0, value(j0), acc);
-      for (uint32_t k = k0 + threadIdx.x + TILE; k < k1; k += TILE)
-        term(blk + size_t(9) * k, value(__ldg(&index[k])), acc);
+      // the thread's further blocks of the row, four at a time with their
+      // loads issued together
+      uint32_t k = k0 + threadIdx.x + TILE;
+      for (; k + 3u * TILE < k1; k += 4u * TILE) {
+        uint32_t jj[4];
+        double Lq[4][9];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          jj[u] = __ldg(&index[k + u * TILE]);
+#pragma unroll
+          for (int m = 0; m < 9; ++m) Lq[u][m] = __ldg(blk + size_t(9) * (k + u * TILE) + m);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) termR(Lq[u], value(jj[u]), acc);
+      }
+      for (; k < k1; k += TILE) term(blk + size_t(9) * k, value(__ldg(&index[k])), acc);
       if (q + 1 < e - b) fetch(q + 1);
       const V3<double> sum = blockSum3(acc, red);
       if (threadIdx.x == 0) {
