@@ -1406,7 +1406,7 @@ struct System final : SystemBase {
       expireSolve = -1;
     }
     ++solveCount;
-    if (factorOn && fPrepared) {  // a solver state with a factor: kPcgFactor
+    if (factorOn && fPrepared && fHost.ready) {  // a solver state with a factor: kPcgFactor
       pcgFactor(law, X, pass, x0zero, tangent);
       return;
     }
